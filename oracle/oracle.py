@@ -1,0 +1,287 @@
+"""ctypes loader for the CPU oracle (``libmrpnn_oracle.so``) and for the
+reference's own sources compiled on the CPU (``_ref/libmrpnn_ref.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline legs of bench.py, never by the product package.
+"""
+import ctypes as C
+import os
+import shutil
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libmrpnn_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmrpnn_ref.so")
+REF_TREE = os.environ.get("MRPNN_REFERENCE", "/root/reference")
+MODEL = os.path.join(os.path.dirname(HERE), "mrpnn_b200", "data", "mrpnn_model.bin")
+
+f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+F3 = C.c_float * 3
+
+
+class Scene(C.Structure):
+    _fields_ = [("density", C.c_void_p), ("res", C.c_int), ("max_density", C.c_float),
+                ("mips", C.c_void_p), ("tr_mips", C.c_void_p), ("hg_lut", C.c_void_p),
+                ("baked_tr", C.c_void_p), ("baked_res", C.c_int),
+                ("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3)]
+
+
+class View(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("ori", F3), ("up", F3), ("right", F3),
+                ("light_dir", F3), ("light_color", F3), ("alpha", C.c_float), ("g", C.c_float),
+                ("multi_scatter", C.c_int), ("spp", C.c_int), ("seed", C.c_uint32), ("frame", C.c_int)]
+
+
+def _build(target):
+    make = shutil.which("make")
+    if make is None:
+        raise RuntimeError("oracle library missing and no make to build it")
+    subprocess.run([make, "-s", "-C", HERE, target], check=True)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            _build("all")
+        L = C.CDLL(ORACLE_SO)
+        L.orc_load_model.argtypes = [C.c_char_p]
+        L.orc_philox4x32_10.argtypes = [np.ctypeslib.ndpointer(np.uint32), np.ctypeslib.ndpointer(np.uint32),
+                                        np.ctypeslib.ndpointer(np.uint32)]
+        L.orc_stream_uniform.argtypes = [C.c_uint32] * 6
+        L.orc_stream_uniform.restype = C.c_float
+        L.orc_fbm_voxel.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_float, C.c_int, C.c_float]
+        L.orc_fbm_voxel.restype = C.c_float
+        L.orc_fbm_volume.argtypes = [f32p, C.c_int, C.c_uint32, C.c_float, C.c_int, C.c_float]
+        L.orc_max_density.argtypes = [f32p, C.c_int64]
+        L.orc_max_density.restype = C.c_float
+        L.orc_build_pyramid.argtypes = [f32p, C.c_int, f32p]
+        L.orc_tr_mip_level.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p]
+        L.orc_hg_lut_texels.argtypes = [C.c_float, C.c_uint32, i32p, C.c_int, f32p]
+        L.orc_baked_tr.argtypes = [C.POINTER(Scene), C.c_float, f32p, C.c_int, C.c_uint32, C.c_int, i64p,
+                                   C.c_int64, f32p]
+        L.orc_tr.argtypes = [C.POINTER(Scene), f32p, f32p, C.c_float, C.c_float] + [C.c_uint32] * 5
+        L.orc_tr.restype = C.c_float
+        L.orc_stencil_tables.argtypes = [f32p, i32p, i32p, i32p, f32p]
+        L.orc_hg.argtypes = [C.c_float, C.c_float]
+        L.orc_hg.restype = C.c_float
+        L.orc_sample_hg.argtypes = [C.c_float, C.c_float, f32p, C.c_float, f32p]
+        L.orc_ray_box_offset.argtypes = [f32p, f32p]
+        L.orc_ray_box_offset.restype = C.c_float
+        L.orc_ray_box_distance.argtypes = [f32p, f32p]
+        L.orc_ray_box_distance.restype = C.c_float
+        L.orc_sample_density.argtypes = [f32p, C.c_int, f32p, C.c_int]
+        L.orc_sample_density.restype = C.c_float
+        L.orc_sample_lut.argtypes = [f32p, C.c_float, C.c_float]
+        L.orc_sample_lut.restype = C.c_float
+        L.orc_camera_ray.argtypes = [C.POINTER(View), C.c_int, C.c_int, f32p]
+        L.orc_first_hit.argtypes = [C.POINTER(Scene), f32p, f32p, C.c_float, f32p]
+        L.orc_basis.argtypes = [f32p, C.c_float, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.POINTER(C.c_uint32), f32p]
+        L.orc_setup_input.argtypes = [C.POINTER(Scene), C.c_int] + [f32p] * 6 + [C.c_float, C.c_float, f32p, f32p]
+        L.orc_mlp_f32.argtypes = [f32p, f32p, C.c_float, f32p, C.c_int, f32p]
+        L.orc_mlp_f64.argtypes = [f32p, f32p, C.c_float, f32p, C.c_int, f64p]
+        L.orc_predict_pixels.argtypes = [C.POINTER(Scene), C.POINTER(View), i32p, C.c_int, f32p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
+        L.orc_trace_pixels.argtypes = [C.POINTER(Scene), C.POINTER(View), i32p, C.c_int, f32p, C.c_void_p,
+                                       C.c_void_p]
+        rc = L.orc_load_model(MODEL.encode())
+        if rc != 0:
+            raise RuntimeError(f"oracle: cannot load model file {MODEL} (rc={rc})")
+        _lib = L
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(REF_SO) or os.path.isdir(os.path.join(REF_TREE, "core"))
+
+
+def ref():
+    """The reference's render sources compiled on the CPU (built on demand)."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            if not os.path.isdir(os.path.join(REF_TREE, "core")):
+                raise RuntimeError("reference checker not built and reference tree absent")
+            subprocess.run([shutil.which("make") or "make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+        R = C.CDLL(REF_SO)
+        vp = C.c_void_p
+        R.ref_bind_scene.argtypes = [vp, C.c_int, C.c_float, vp, vp, vp, vp, C.c_int, f32p, C.c_float, f32p]
+        R.ref_hg.argtypes = [C.c_float, C.c_float]
+        R.ref_hg.restype = C.c_float
+        R.ref_sample_hg.argtypes = [C.c_float, C.c_float, f32p, C.c_float, f32p]
+        R.ref_ray_box_offset.argtypes = [f32p, f32p]
+        R.ref_ray_box_offset.restype = C.c_float
+        R.ref_ray_box_distance.argtypes = [f32p, f32p]
+        R.ref_ray_box_distance.restype = C.c_float
+        R.ref_stencil.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), f32p]
+        R.ref_sample_density.argtypes = [C.c_int, f32p]
+        R.ref_sample_density.restype = C.c_float
+        R.ref_shadow_tr.argtypes = [f32p, f32p, C.c_int]
+        R.ref_shadow_tr.restype = C.c_float
+        R.ref_mlp.argtypes = [f32p, f32p, C.c_float, f32p, C.c_int, f32p]
+        R.ref_setup_input.argtypes = [C.c_int] + [f32p] * 6 + [C.c_float, C.c_float, f32p, f32p]
+        R.ref_first_hit.argtypes = [f32p, f32p, C.c_float, f32p]
+        R.ref_basis.argtypes = [f32p, C.c_float] + [C.c_uint32] * 5 + [f32p]
+        R.ref_tr.argtypes = [f32p, f32p, C.c_float, C.c_float] + [C.c_uint32] * 5
+        R.ref_tr.restype = C.c_float
+        R.ref_predict_pixels.argtypes = [C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_float,
+                                         C.c_uint32, C.c_int, i32p, C.c_int, f32p]
+        R.ref_trace_sample.argtypes = [C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_float,
+                                       C.c_int, C.c_uint32, C.c_int, C.c_int, C.c_int, f32p]
+        _ref = R
+    return _ref
+
+
+# ---------------------------------------------------------------------------
+# numpy-level helpers
+# ---------------------------------------------------------------------------
+def mip_sizes():
+    return [256 >> m for m in range(9)]
+
+
+def tr_sizes():
+    return [128 >> i for i in range(8)]
+
+
+def split_levels(flat, sizes):
+    out, off = [], 0
+    for r in sizes:
+        out.append(flat[off:off + r ** 3].reshape(r, r, r))
+        off += r ** 3
+    return out
+
+
+def fbm_volume(R, seed, base_freq, octaves=6, gain=0.5):
+    out = np.empty(R ** 3, np.float32)
+    lib().orc_fbm_volume(out, R, seed, base_freq, octaves, gain)
+    return out
+
+
+def build_pyramid(data, R):
+    out = np.empty(sum(r ** 3 for r in mip_sizes()), np.float32)
+    lib().orc_build_pyramid(np.ascontiguousarray(data, np.float32).ravel(), R, out)
+    return out
+
+
+def tr_mips(mips, alpha, light_dir, levels=range(8)):
+    out = np.zeros(sum(r ** 3 for r in tr_sizes()), np.float32)
+    offs = np.cumsum([0] + [r ** 3 for r in tr_sizes()])
+    L = np.asarray(light_dir, np.float32)
+    for lv in levels:
+        part = np.empty(tr_sizes()[lv] ** 3, np.float32)
+        lib().orc_tr_mip_level(mips, lv, alpha, L, part)
+        out[offs[lv]:offs[lv + 1]] = part
+    return out
+
+
+def hg_lut_texels(g, seed, texels):
+    t = np.ascontiguousarray(texels, np.int32)
+    out = np.empty(t.size, np.float32)
+    lib().orc_hg_lut_texels(g, seed, t, t.size, out)
+    return out
+
+
+def stencil_tables():
+    off = np.empty(192, np.float32)
+    layer = np.empty(192, np.int32)
+    typ = np.empty(192, np.int32)
+    li = np.empty(192, np.int32)
+    v = np.empty(192, np.float32)
+    lib().orc_stencil_tables(off, layer, typ, li, v)
+    return off, layer, typ, li, v
+
+
+def lut_rows_needed():
+    """LUT texel indices read by the gather: the two rows around each stencil v."""
+    _, _, _, _, v = stencil_tables()
+    rows = set()
+    for vv in v:
+        y = int(np.floor(vv * 512 - 0.5))
+        for r in (y, y + 1):
+            rows.add(min(max(r, 0), 511))
+    rows = sorted(rows)
+    return rows, np.concatenate([np.arange(r * 512, (r + 1) * 512, dtype=np.int32) for r in rows])
+
+
+class SceneBuf:
+    """Host arrays for one scene plus the ctypes struct pointing at them."""
+
+    def __init__(self, density, res, max_density, mips=None, tr=None, lut=None, baked=None, baked_res=0,
+                 scatter_rate=(1.001, 1.001, 1.001), tr_scale=1.0, sky=(0.0, 0.0, 0.0)):
+        keep = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).ravel()
+        self.density, self.mips, self.tr, self.lut, self.baked = map(keep, (density, mips, tr, lut, baked))
+        self.res, self.max_density, self.baked_res = res, float(max_density), baked_res
+        self.scatter_rate = np.asarray(scatter_rate, np.float32)
+        self.tr_scale = float(tr_scale)
+        self.sky = np.asarray(sky, np.float32)
+        ptr = lambda a: None if a is None else a.ctypes.data
+        self.c = Scene(ptr(self.density), res, self.max_density, ptr(self.mips), ptr(self.tr), ptr(self.lut),
+                       ptr(self.baked), baked_res, F3(*self.scatter_rate), self.tr_scale, F3(*self.sky))
+
+    def bind_ref(self):
+        ref().ref_bind_scene(self.c.density, self.res, self.max_density, self.c.mips, self.c.tr_mips,
+                             self.c.hg_lut, self.c.baked_tr, self.baked_res, self.scatter_rate, self.tr_scale,
+                             self.sky)
+
+
+def make_view(width, height, ori, up, right, light_dir, light_color=(1, 1, 1), alpha=64.0, g=0.857,
+              multi_scatter=256, spp=32, seed=0, frame=0):
+    return View(width, height, F3(*ori), F3(*up), F3(*right), F3(*light_dir), F3(*light_color), alpha, g,
+                multi_scatter, spp, seed, frame)
+
+
+def predict_pixels(scene, view, pixels, want_features=False):
+    px = np.ascontiguousarray(pixels, np.int32)
+    n = px.size
+    rgba = np.empty((n, 4), np.float32)
+    feat = np.empty((n, 576), np.float32) if want_features else None
+    gam = np.empty(n, np.float32) if want_features else None
+    hit = np.empty((n, 4), np.float32) if want_features else None
+    p = lambda a: None if a is None else a.ctypes.data
+    lib().orc_predict_pixels(C.byref(scene.c), C.byref(view), px, n, rgba, p(feat), p(gam), p(hit))
+    return (rgba, feat, gam, hit) if want_features else rgba
+
+
+def trace_pixels(scene, view, pixels):
+    px = np.ascontiguousarray(pixels, np.int32)
+    n = px.size
+    rgba = np.empty((n, 4), np.float32)
+    s = np.empty((n, 3), np.float64)
+    s2 = np.empty((n, 3), np.float64)
+    lib().orc_trace_pixels(C.byref(scene.c), C.byref(view), px, n, rgba, s.ctypes.data, s2.ctypes.data)
+    return rgba, s, s2
+
+
+def mlp_f32(feat, gamma, g, sr):
+    feat = np.ascontiguousarray(feat, np.float32)
+    n = feat.shape[0]
+    out = np.empty((n, 3), np.float32)
+    lib().orc_mlp_f32(feat, np.ascontiguousarray(gamma, np.float32), g, np.asarray(sr, np.float32), n, out)
+    return out
+
+
+def mlp_f64(feat, gamma, g, sr):
+    feat = np.ascontiguousarray(feat, np.float32)
+    n = feat.shape[0]
+    out = np.empty((n, 3), np.float64)
+    lib().orc_mlp_f64(feat, np.ascontiguousarray(gamma, np.float32), g, np.asarray(sr, np.float32), n, out)
+    return out
+
+
+def ref_mlp(feat, gamma, g, sr):
+    feat = np.ascontiguousarray(feat, np.float32)
+    n = feat.shape[0]
+    out = np.empty((n, 3), np.float32)
+    ref().ref_mlp(feat, np.ascontiguousarray(gamma, np.float32), g, np.asarray(sr, np.float32), n, out)
+    return out
