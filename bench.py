@@ -1,0 +1,335 @@
+"""Benchmark of the MRPNN render path on B200.
+
+Workload (the headline configuration): MRPNN predictor frames of 1024x1024 over
+a 512^3 fp32 fBm cloud (seed 1, base frequency 6, 6 octaves, gain 0.5),
+9-level pyramid, extinction 64, albedo 0.99, g 0.857, light
+normalize(0.3, 0.8, 0.5), sky 0.05, 45 degree camera at (0.75, 0.75, 0.75),
+one predictor evaluation per pixel.  A step is one frame.
+
+  python bench.py [--gpus N --steps K --warmup W] [--precision fp32|bf16|fp8]
+  python bench.py --impl reference        # CPU port of the reference path
+
+N > 1 runs one process per GPU (torchrun); each GPU renders its own frames
+from its own replica of the volume (the path shards by frame, no collective):
+value = frames of all ranks / max over ranks of the device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1024^2 MRPNN frames/s"
+UNIT = "frames/s"
+W = H = 1024
+RES = 512
+SCENE = dict(seed=1, freq=6.0, octaves=6, gain=0.5, alpha=64.0, g=0.857, albedo=0.99, sky=0.05,
+             light=(0.3, 0.8, 0.5), cam=(0.75, 0.75, 0.75), fov=45.0)
+GATHER_BYTES_PER_PIXEL = 192 * (8 + 8 + 2 * 4) * 4     # density + TR trilinear, 2 LUT bilinear, fp32
+
+
+def light():
+    L = np.asarray(SCENE["light"], np.float32)
+    return (L / np.float32(np.sqrt(np.float32(np.dot(L, L))))).astype(np.float32)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_scene_from_gpu(vol):
+    """Host copies of the GPU resources (bit-identical to the oracle's own
+    construction, which tests/test_gpu_resources.py checks)."""
+    import mrpnn_b200 as M
+    from oracle import oracle as O
+    mips = np.concatenate([vol.read(M.api.RES_MIP, m) for m in range(9)])
+    tr = np.concatenate([vol.read(M.api.RES_TR, i) for i in range(8)])
+    return O.SceneBuf(vol.read(M.api.RES_DENSITY), RES, vol.max_density, mips, tr, vol.read(M.api.RES_LUT),
+                      scatter_rate=(SCENE["albedo"],) * 3, sky=(SCENE["sky"],) * 3)
+
+
+def cpu_scene_oracle():
+    """The scene built by the CPU port alone (reference arm: no GPU code)."""
+    from oracle import oracle as O
+    vol = O.fbm_volume(RES, SCENE["seed"], SCENE["freq"], SCENE["octaves"], SCENE["gain"])
+    md = O.lib().orc_max_density(vol, vol.size)
+    mips = O.build_pyramid(vol, RES)
+    tr = O.tr_mips(mips, SCENE["alpha"], light())
+    _, tex = O.lut_rows_needed()
+    lut = np.zeros(512 * 512, np.float32)
+    lut[tex] = O.hg_lut_texels(SCENE["g"], 0, tex)
+    return O.SceneBuf(vol, RES, md, mips, tr, lut, scatter_rate=(SCENE["albedo"],) * 3, sky=(SCENE["sky"],) * 3)
+
+
+def view_vectors():
+    import mrpnn_b200 as M
+    ori, up, right = M.camera_frame(SCENE["cam"])
+    s = np.float32(np.tan(np.deg2rad(SCENE["fov"]) / 2))
+    return ori, (up * s).astype(np.float32), (right * s).astype(np.float32)
+
+
+def time_cpu_predict(sc, n_pix, seed=0, reps=1):
+    """Oracle predictor on a random sample of the 1024^2 frame -> pixels/s."""
+    from oracle import oracle as O
+    ori, up, right = view_vectors()
+    view = O.make_view(W, H, ori, up, right, light(), alpha=SCENE["alpha"], g=SCENE["g"], seed=seed, frame=0)
+    rng = np.random.default_rng(seed)
+    px = rng.choice(W * H, n_pix, replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.predict_pixels(sc, view, px)
+    dt = time.perf_counter() - t0
+    return n_pix * reps / dt, dt
+
+
+def omp_threads():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    t0 = time.perf_counter()
+    sc = cpu_scene_oracle()
+    setup_s = time.perf_counter() - t0
+    n_pix = args.ref_pixels
+    for _ in range(args.warmup):
+        time_cpu_predict(sc, max(256, n_pix // 8))
+    rates = []
+    for k in range(args.steps):
+        r, _ = time_cpu_predict(sc, n_pix, seed=k + 1)
+        rates.append(r)
+    pix_s = float(np.mean(rates))
+    fps = pix_s / (W * H)
+    cores = omp_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 / fps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"MRPNN predictor, {W}x{H} frame, {RES}^3 fBm (seed 1, freq 6), FP32 MLP",
+                   "sample": f"{n_pix} random pixels per step"},
+        "cpu_baseline": {"value": fps, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n_pix} random pixels of the {W}x{H} frame per step, scene setup {setup_s:.1f}s"},
+        "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_mine(args, rank, world, local):
+    import torch
+
+    import mrpnn_b200 as M
+    M.init(local)
+    prec = {"fp32": M.FP32, "bf16": M.BF16, "fp8": M.FP8}[args.precision]
+    vol = M.VolumeRender(RES)
+    vol.generate_fbm(SCENE["seed"], SCENE["freq"], SCENE["octaves"], SCENE["gain"])
+    vol.Update()
+    vol.SetScatterRate(SCENE["albedo"])
+    vol.SetSky(SCENE["sky"])
+    vol.SetPrecision(prec)
+    ori, up, right = view_vectors()
+    L = light()
+    view = vol.make_view((W, H), ori, up, right, L, SCENE["g"], SCENE["alpha"], seed=rank)
+    dev_out = torch.empty((H, W, 4), dtype=torch.float32, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")   # > L2 (126 MB)
+
+    for i in range(args.warmup):
+        view.frame_offset = i
+        vol.render_view(view, M.VolumeRender.MRPNN, 1, dev_out)
+    torch.cuda.synchronize()
+
+    # -- device-timed region: inputs resident, L2 flushed between steps --------
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = []
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            view.frame_offset = 1000 + k
+            vol.render_view(view, M.VolumeRender.MRPNN, 1, dev_out)
+            ms.append(vol.last_render_ms())
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(float(sum(ms)), world)
+    frames = args.steps * world
+    value = frames / (total_ms / 1000.0)
+    img = dev_out.cpu().numpy()
+    active = int((img[..., 3] > 0).sum())
+
+    # -- end to end through the public API: host (pinned) output every step ------
+    host_out = torch.empty((H, W, 4), dtype=torch.float32).pin_memory().numpy()
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        view.frame_offset = 2000 + k
+        vol.render_view(view, M.VolumeRender.MRPNN, 1, host_out)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = frames / e2e_s
+
+    hbm, bf16, peak_kind = peaks()
+    avg_ms = float(np.mean(ms))
+    alg_bytes = active * GATHER_BYTES_PER_PIXEL + W * H * 16
+    achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            traffic = json.load(f).get(f"predict_{args.precision}_{W}x{H}", {}).get("dram_bytes_per_launch")
+    except Exception:
+        pass
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sc = cpu_scene_from_gpu(vol)
+        pix_s, dt = time_cpu_predict(sc, args.cpu_pixels)
+        cpu = {"value": pix_s / (W * H), "unit": UNIT, "cores": omp_threads(), "kind": "port",
+               "sample": f"{args.cpu_pixels} random pixels of the {W}x{H} frame ({dt:.1f}s), OpenMP oracle"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16", "fp8": "fp8-e4m3"}[args.precision],
+            "data": "synthetic",
+            "config": {"workload": f"MRPNN predictor frame {W}x{H}, {RES}^3 fBm cloud (seed 1, freq 6), 9-level pyramid",
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MiB write) between timed steps", "active_pixels": active},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 96, "d2h_bytes_per_step": W * H * 16},
+            "gpu_launches": args.steps * 1,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "note": f"predict kernel; algorithmic bytes = active pixels x {GATHER_BYTES_PER_PIXEL} B "
+                                 f"gather + 16 B/pixel output; peak {peak_kind}"},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp8"])
+    ap.add_argument("--cpu-pixels", type=int, default=8192)
+    ap.add_argument("--ref-pixels", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = (0, 1, 0)
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", 0))
+        world = int(os.environ.get("WORLD_SIZE", 1))
+        run_reference(args, rank, world)
+        return
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        run_mine(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

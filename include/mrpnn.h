@@ -1,0 +1,179 @@
+/*
+ * mrpnn.h -- C ABI of the MRPNN B200 render path (libmrpnn_b200.so).
+ *
+ * The reference exposes this path only as the C++ classes VolumeRender
+ * (core/volume.hpp:45-155) and Camera (core/camera.hpp:29-43) over
+ * process-global CUDA texture references.  This ABI carries the same
+ * operations with opaque per-volume handles, plain pointers and sizes, and a
+ * status code on every call; include/mrpnn_volume_render.hpp rebuilds the
+ * reference's classes on top of it.  Each entry names the reference
+ * interface it replaces.
+ *
+ * Conventions
+ *   - Every call returns mrp_status; on failure mrp_last_error() holds a
+ *     message (per calling thread).
+ *   - 3D grids are res^3 floats, index (x*res + y)*res + z, z fastest
+ *     (VolumeRender::SetData, core/volume.cu:1178-1180).
+ *   - Buffers are caller-owned.  *_is_device = 0: host memory (pinned or
+ *     pageable), copied inside the call; 1: device memory on the handle's
+ *     device, used in place.
+ *   - A volume handle owns one CUDA stream; calls on one handle are
+ *     serialised by the caller, calls on different handles may run
+ *     concurrently from different threads.  Calls return after the work
+ *     they enqueue has completed unless documented otherwise.
+ *   - Nothing here falls back to the CPU: without a usable sm_100 device
+ *     mrp_init fails with MRP_ERR_NO_DEVICE.
+ */
+#ifndef MRPNN_H
+#define MRPNN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mrp_status {
+    MRP_OK = 0,
+    MRP_ERR_INVALID = 1,       /* bad argument                                 */
+    MRP_ERR_NO_DEVICE = 2,     /* no CUDA device / not sm_100                  */
+    MRP_ERR_CUDA = 3,          /* a CUDA runtime call failed                   */
+    MRP_ERR_OOM = 4,           /* device allocation failed                     */
+    MRP_ERR_NOT_READY = 5,     /* resource not built yet (e.g. no Update)      */
+    MRP_ERR_UNSUPPORTED = 6,   /* e.g. RenderType RPNN (not compiled upstream) */
+    MRP_ERR_IO = 7,            /* file could not be read / written             */
+    MRP_ERR_BUDGET = 8,        /* serving: admission over the memory budget    */
+    MRP_ERR_TIMEOUT = 9        /* serving: bounded wait expired                */
+} mrp_status;
+
+/* VolumeRender::RenderType (core/volume.hpp:98-100) */
+typedef enum mrp_render_type { MRP_PT = 0, MRP_RPNN = 1, MRP_MRPNN = 2 } mrp_render_type;
+
+/* MLP arithmetic of the predictor. FP32 is the drop-in (parity 1e-4 rel). */
+typedef enum mrp_precision { MRP_FP32 = 0, MRP_BF16 = 1, MRP_FP8 = 2 } mrp_precision;
+
+typedef struct mrp_volume mrp_volume;
+
+/* Renderer settings that the reference keeps in __device__ globals
+ * (core/render.cuh:10-18): VolumeRender::SetScatterRate, SetTrScale,
+ * SetEnvExp.  sky is the constant environment radiance standing in for
+ * SkyBox's HDRI (SetHDRI); bake_res is the NEE transmittance grid edge
+ * (Update_CachedTR uses 768). */
+typedef struct mrp_params {
+    float scatter_rate[3];   /* default 1.001, 1.001, 1.001 */
+    float tr_scale;          /* default 1                   */
+    float sky[3];            /* default 0, 0, 0             */
+    float env_exp;           /* default 1 (scales sky)      */
+    int bake_res;            /* default 768                 */
+    int bake_replicate_seeding; /* 1 (default): the reference's per-voxel estimates share one stream */
+    mrp_precision precision; /* predictor MLP arithmetic, default MRP_FP32 */
+    uint32_t seed;           /* RNG key of the LUT and bake streams, default 0 */
+} mrp_params;
+
+/* One camera: VolumeRender::Render(int2 size, ori, up, right, lightDir, rt,
+ * g, alpha, lightColor, multiScatter, sampleNum) (core/volume.cu:487).  The
+ * field of view follows |right| and |up| (unit vectors give 90 degrees). */
+typedef struct mrp_view {
+    int width, height;
+    float ori[3], up[3], right[3];
+    float light_dir[3], light_color[3];
+    float alpha;             /* extinction scale                          */
+    float g;                 /* Henyey-Greenstein asymmetry               */
+    int multi_scatter;       /* PT bounce cap                             */
+    int spp;                 /* PT samples per launch (reference: 32)     */
+    uint32_t seed;           /* RNG key of the pixel streams              */
+    int frame_offset;        /* launch index of the first launch          */
+} mrp_view;
+
+typedef struct mrp_volume_info {
+    int res;
+    float max_density;
+    int has_pyramid, has_lut, has_tr, has_baked_tr;
+    float lut_g, tr_alpha, tr_light[3];
+    size_t device_bytes;
+} mrp_volume_info;
+
+/* Resource selector for mrp_volume_read (readback for checking). */
+typedef enum mrp_resource {
+    MRP_RES_DENSITY = 0, MRP_RES_MIP = 1, MRP_RES_TR = 2, MRP_RES_LUT = 3, MRP_RES_BAKED_TR = 4, MRP_RES_OCCUPANCY = 5
+} mrp_resource;
+
+/* -- library ---------------------------------------------------------------- */
+/* cudaSetDevice + capability check; loads the model file if given (NULL:
+ * the model file installed beside the library). */
+mrp_status mrp_init(int device, const char* model_path);
+const char* mrp_last_error(void);
+const char* mrp_version(void);
+/* Replaces the network weights from a model file (format: mrpnn_b200/data/
+ * make_model.py).  The reference bakes them into __constant__ arrays
+ * (core/NNWeight.cuh, core/radiancePredict.cu:299). */
+mrp_status mrp_load_model(const char* path);
+void mrp_default_params(mrp_params* p);
+
+/* -- volume lifecycle --------------------------------------------------------- */
+/* VolumeRender(int resolution) (core/volume.cu:948-957); allocates exactly
+ * res^3 floats instead of the reference's fixed 1024^3 array. */
+mrp_status mrp_volume_create(int res, mrp_volume** out);
+/* ~VolumeRender (core/volume.cu:1151-1176) */
+mrp_status mrp_volume_destroy(mrp_volume* v);
+/* VolumeRender::SetDatas / SetData storage (core/volume.cu:1178-1184):
+ * copies a full res^3 grid. */
+mrp_status mrp_volume_set_data(mrp_volume* v, const float* data, int res, int is_device);
+/* SetDatas(FillFunc) through ParallelFill (core/omp.cpp:4-18): fn(x,y,z,u,v,w)
+ * with u = (x+0.5)/res, evaluated on host threads. */
+typedef float (*mrp_fill_fn)(int x, int y, int z, float u, float v, float w, void* user);
+mrp_status mrp_volume_fill(mrp_volume* v, mrp_fill_fn fn, void* user);
+/* Synthetic fBm cloud generated on the device (benchmark volumes). */
+mrp_status mrp_volume_generate_fbm(mrp_volume* v, uint32_t seed, float base_freq, int octaves, float gain);
+/* VolumeRender::Update(process_mips) (core/volume.cu:1443-1531): computes the
+ * majorant (max density, which the reference leaves at 1e-5), the 9-level
+ * pyramid (256>>m) and the occupancy bricks, on the device. */
+mrp_status mrp_volume_update(mrp_volume* v, int process_mips);
+/* Overrides the majorant (the reference's max_density field). */
+mrp_status mrp_volume_set_max_density(mrp_volume* v, float max_density);
+mrp_status mrp_volume_get_info(const mrp_volume* v, mrp_volume_info* info);
+mrp_status mrp_set_params(mrp_volume* v, const mrp_params* p);
+mrp_status mrp_get_params(const mrp_volume* v, mrp_params* p);
+/* Copies a resource (level: mip / TR level) to dst; returns its float count
+ * in *count when dst is NULL. */
+mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* dst, size_t* count, int dst_is_device);
+
+/* -- per-render caches ------------------------------------------------------------ */
+/* VolumeRender::UpdateHGLut(g) (core/volume.cu:1401-1423), cached on g. */
+mrp_status mrp_update_hg_lut(mrp_volume* v, float g);
+/* VolumeRender::Update_TR(lightDir, alpha) (core/volume.cu:1589-1667),
+ * cached on (lightDir, alpha). */
+mrp_status mrp_update_tr(mrp_volume* v, const float light_dir[3], float alpha);
+/* VolumeRender::Update_CachedTR(lightDir, alpha) (core/volume.cu:1669-1696),
+ * cached on (lightDir, alpha, bake_res). */
+mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float alpha);
+
+/* -- rendering ---------------------------------------------------------------------- */
+/* VolumeRender::Render(...) -> vector<float4> (core/volume.cu:487-548):
+ * sample_num launches with the running mean of RenderCamera; out holds
+ * width*height float4 (RGB, A = coverage for PT / hit distance for MRPNN). */
+mrp_status mrp_render(mrp_volume* v, const mrp_view* view, mrp_render_type type, int sample_num, float* out_rgba,
+                      int out_is_device);
+/* Device time of the kernels of the last mrp_render on this handle (ms). */
+mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms);
+
+/* -- parity entry points (pieces of the path) ---------------------------------------- */
+/* RadiancePredictInternal (core/radiancePredict.cu:301-422) on n feature
+ * sets: feat [n][576] = X_Val[192], X_Val_Sub[192], X_Val_Hg[192]; gamma [n];
+ * out [n][3]. */
+mrp_status mrp_predict_features(const float* feat, const float* gamma, float g, const float scatter_rate[3], int n,
+                                float* out3, mrp_precision precision, int is_device);
+/* SetupInputData (core/radiancePredict.cu:427-485) for n points: pos [n][3],
+ * bases [n][12] = XMain, YMain, ZMain, LXMain; feat [n][576], gamma [n]. */
+mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bases, const float light_dir[3], float g,
+                               float alpha, int n, float* feat, float* gamma, int is_device);
+/* GetSamplePoint (core/render.cuh:436-462) for n rays: hit4 [n][4] =
+ * (x, y, z, 1 if hit). */
+mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, float alpha, int n, float* hit4,
+                         int is_device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MRPNN_H */

@@ -1,0 +1,9 @@
+"""mrpnn_b200 -- B200-native (sm_100a) MRPNN render path: delta-tracking path
+tracer and the MRPNN neural radiance predictor, behind a C ABI
+(include/mrpnn.h) with a Python mirror of the reference's VolumeRender /
+Camera API."""
+from .api import (BF16, FP8, FP32, Camera, MrpError, VolumeRender, camera_frame, default_params, init, lib,
+                  predict_features)
+
+__all__ = ["VolumeRender", "Camera", "MrpError", "init", "lib", "predict_features", "camera_frame",
+           "default_params", "FP32", "BF16", "FP8"]

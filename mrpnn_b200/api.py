@@ -1,0 +1,393 @@
+"""Python mirror of the reference's render API over the C ABI (include/mrpnn.h).
+
+The reference's public interface is the C++ pair ``VolumeRender``
+(core/volume.hpp:45-155) and ``Camera`` (core/camera.hpp:29-43); this module
+keeps their method names, argument meaning and defaults, so a script written
+against them reads the same.  All work runs in ``libmrpnn_b200.so`` on the
+GPU; importing works without a GPU, but any call that needs the device raises
+``MrpError`` when no sm_100 device is present -- there is no CPU path.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmrpnn_b200.so")
+MODEL_PATH = os.path.join(HERE, "data", "mrpnn_model.bin")
+
+# mrp_status
+OK, ERR_INVALID, ERR_NO_DEVICE, ERR_CUDA, ERR_OOM, ERR_NOT_READY, ERR_UNSUPPORTED, ERR_IO, ERR_BUDGET, ERR_TIMEOUT = range(10)
+STATUS_NAMES = ["OK", "INVALID", "NO_DEVICE", "CUDA", "OOM", "NOT_READY", "UNSUPPORTED", "IO", "BUDGET", "TIMEOUT"]
+FP32, BF16, FP8 = 0, 1, 2
+RES_DENSITY, RES_MIP, RES_TR, RES_LUT, RES_BAKED_TR, RES_OCCUPANCY = range(6)
+
+F3 = C.c_float * 3
+
+
+class MrpError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"mrp {STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else status}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3), ("env_exp", C.c_float),
+                ("bake_res", C.c_int), ("bake_replicate_seeding", C.c_int), ("precision", C.c_int),
+                ("seed", C.c_uint32)]
+
+
+class View(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("ori", F3), ("up", F3), ("right", F3),
+                ("light_dir", F3), ("light_color", F3), ("alpha", C.c_float), ("g", C.c_float),
+                ("multi_scatter", C.c_int), ("spp", C.c_int), ("seed", C.c_uint32), ("frame_offset", C.c_int)]
+
+
+class VolumeInfo(C.Structure):
+    _fields_ = [("res", C.c_int), ("max_density", C.c_float), ("has_pyramid", C.c_int), ("has_lut", C.c_int),
+                ("has_tr", C.c_int), ("has_baked_tr", C.c_int), ("lut_g", C.c_float), ("tr_alpha", C.c_float),
+                ("tr_light", F3), ("device_bytes", C.c_size_t)]
+
+
+FILL_FN = C.CFUNCTYPE(C.c_float, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_void_p)
+
+# Every symbol include/mrpnn.h declares, with its ctypes signature.
+_SIGS = {
+    "mrp_init": ([C.c_int, C.c_char_p], C.c_int),
+    "mrp_last_error": ([], C.c_char_p),
+    "mrp_version": ([], C.c_char_p),
+    "mrp_load_model": ([C.c_char_p], C.c_int),
+    "mrp_default_params": ([C.POINTER(Params)], None),
+    "mrp_volume_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "mrp_volume_destroy": ([C.c_void_p], C.c_int),
+    "mrp_volume_set_data": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "mrp_volume_fill": ([C.c_void_p, FILL_FN, C.c_void_p], C.c_int),
+    "mrp_volume_generate_fbm": ([C.c_void_p, C.c_uint32, C.c_float, C.c_int, C.c_float], C.c_int),
+    "mrp_volume_update": ([C.c_void_p, C.c_int], C.c_int),
+    "mrp_volume_set_max_density": ([C.c_void_p, C.c_float], C.c_int),
+    "mrp_volume_get_info": ([C.c_void_p, C.POINTER(VolumeInfo)], C.c_int),
+    "mrp_set_params": ([C.c_void_p, C.POINTER(Params)], C.c_int),
+    "mrp_get_params": ([C.c_void_p, C.POINTER(Params)], C.c_int),
+    "mrp_volume_read": ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_size_t), C.c_int], C.c_int),
+    "mrp_update_hg_lut": ([C.c_void_p, C.c_float], C.c_int),
+    "mrp_update_tr": ([C.c_void_p, F3, C.c_float], C.c_int),
+    "mrp_update_baked_tr": ([C.c_void_p, F3, C.c_float], C.c_int),
+    "mrp_render": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "mrp_last_render_ms": ([C.c_void_p, C.POINTER(C.c_float)], C.c_int),
+    "mrp_predict_features": ([C.c_void_p, C.c_void_p, C.c_float, F3, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "mrp_gather_features": ([C.c_void_p, C.c_void_p, C.c_void_p, F3, C.c_float, C.c_float, C.c_int, C.c_void_p,
+                             C.c_void_p, C.c_int], C.c_int),
+    "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
+}
+
+_lib = None
+_initialized = False
+
+
+def lib():
+    """Loads libmrpnn_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MrpError(ERR_NOT_READY, f"{LIB_PATH} is missing: build it with `python -m mrpnn_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != OK:
+        raise MrpError(status, lib().mrp_last_error().decode(errors="replace"))
+
+
+def init(device=0, model_path=None):
+    """mrp_init: selects the CUDA device and loads the network weights."""
+    global _initialized
+    _check(lib().mrp_init(device, model_path.encode() if model_path else MODEL_PATH.encode()))
+    _initialized = True
+
+
+def _ensure_init():
+    if not _initialized:
+        init()
+
+
+def _f3(v):
+    v = [float(x) for x in v]
+    return F3(*v)
+
+
+def _ptr(a):
+    """(pointer, is_device) of a numpy array or a CUDA torch tensor."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data, 0
+    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+        return a.data_ptr(), 1
+    raise TypeError("expected a numpy array or a CUDA tensor")
+
+
+def _host_f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def default_params():
+    p = Params()
+    lib().mrp_default_params(C.byref(p))
+    return p
+
+
+def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
+    """RadiancePredictInternal on n feature sets (feat [n, 576] = X_Val, X_Val_Sub,
+    X_Val_Hg; gamma [n]) -> [n, 3].  Accepts numpy arrays (host) or CUDA tensors."""
+    _ensure_init()
+    if isinstance(feat, np.ndarray):
+        feat = _host_f32(feat)
+        gamma = _host_f32(gamma)
+        n = feat.shape[0]
+        out = np.empty((n, 3), np.float32) if out is None else out
+        _check(lib().mrp_predict_features(feat.ctypes.data, gamma.ctypes.data, float(g), _f3(scatter_rate), n,
+                                          out.ctypes.data, int(precision), 0))
+        return out
+    n = feat.shape[0]
+    if out is None:
+        import torch
+        out = torch.empty((n, 3), dtype=torch.float32, device=feat.device)
+    _check(lib().mrp_predict_features(feat.data_ptr(), gamma.data_ptr(), float(g), _f3(scatter_rate), n,
+                                      out.data_ptr(), int(precision), 1))
+    return out
+
+
+class VolumeRender:
+    """VolumeRender (core/volume.hpp:45-155) over a device-resident volume handle."""
+    PT, RPNN, MRPNN = 0, 1, 2
+
+    def __init__(self, resolution):
+        _ensure_init()
+        h = C.c_void_p()
+        _check(lib().mrp_volume_create(int(resolution), C.byref(h)))
+        self._h = h
+        self.resolution = int(resolution)
+        self._params = default_params()
+        self._view_seed = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.mrp_volume_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    # -- data -------------------------------------------------------------
+    def set_data(self, data):
+        """Full grid, index (x*R + y)*R + z (SetData storage, core/volume.cu:1178)."""
+        if isinstance(data, np.ndarray):
+            data = _host_f32(data).ravel()
+            if data.size != self.resolution ** 3:
+                raise ValueError("data size does not match the resolution")
+            _check(lib().mrp_volume_set_data(self._h, data.ctypes.data, self.resolution, 0))
+        else:
+            _check(lib().mrp_volume_set_data(self._h, data.data_ptr(), self.resolution, 1))
+
+    def SetDatas(self, func):
+        """SetDatas(FillFunc) (core/volume.cu:1182): func(x, y, z, u, v, w) -> float.
+        func may take numpy index/coordinate grids (vectorised) or scalars."""
+        R = self.resolution
+        i = np.arange(R)
+        x, y, z = np.meshgrid(i, i, i, indexing="ij")
+        u = ((x + 0.5) / R).astype(np.float32)
+        v = ((y + 0.5) / R).astype(np.float32)
+        w = ((z + 0.5) / R).astype(np.float32)
+        try:
+            vals = np.asarray(func(x, y, z, u, v, w), dtype=np.float32)
+            if vals.shape != x.shape:
+                raise ValueError
+        except Exception:
+            cb = FILL_FN(lambda a, b, c, uu, vv, ww, _u: float(func(a, b, c, uu, vv, ww)))
+            _check(lib().mrp_volume_fill(self._h, cb, None))
+            return
+        self.set_data(vals)
+
+    def generate_fbm(self, seed, base_freq, octaves=6, gain=0.5):
+        """Synthetic fBm cloud on the device (benchmark volumes)."""
+        _check(lib().mrp_volume_generate_fbm(self._h, int(seed), float(base_freq), int(octaves), float(gain)))
+
+    def Update(self, process_mips=True, need_reset_datas_dev=True):
+        _check(lib().mrp_volume_update(self._h, 1 if process_mips else 0))
+
+    @property
+    def max_density(self):
+        return self.info().max_density
+
+    @max_density.setter
+    def max_density(self, value):
+        _check(lib().mrp_volume_set_max_density(self._h, float(value)))
+
+    def info(self):
+        inf = VolumeInfo()
+        _check(lib().mrp_volume_get_info(self._h, C.byref(inf)))
+        return inf
+
+    def read(self, which, level=0):
+        n = C.c_size_t()
+        _check(lib().mrp_volume_read(self._h, which, level, None, C.byref(n), 0))
+        out = np.empty(n.value, np.uint8 if which == RES_OCCUPANCY else np.float32)
+        _check(lib().mrp_volume_read(self._h, which, level, out.ctypes.data, None, 0))
+        return out
+
+    # -- settings (core/volume.cu:1732-1765) ----------------------------------
+    def _push(self):
+        _check(lib().mrp_set_params(self._h, C.byref(self._params)))
+
+    def SetScatterRate(self, rate):
+        r = [rate] * 3 if np.isscalar(rate) else list(rate)
+        self._params.scatter_rate = _f3(r)
+        self._push()
+
+    def SetTrScale(self, scale):
+        self._params.tr_scale = float(scale)
+        self._push()
+
+    def SetEnvExp(self, exp):
+        self._params.env_exp = float(exp)
+        self._push()
+
+    def SetSky(self, radiance):
+        r = [radiance] * 3 if np.isscalar(radiance) else list(radiance)
+        self._params.sky = _f3(r)
+        self._push()
+
+    def SetPrecision(self, precision):
+        self._params.precision = int(precision)
+        self._push()
+
+    def SetBakeResolution(self, res, replicate_reference_seeding=True):
+        self._params.bake_res = int(res)
+        self._params.bake_replicate_seeding = 1 if replicate_reference_seeding else 0
+        self._push()
+
+    def SetSeed(self, seed):
+        self._params.seed = int(seed)
+        self._push()
+
+    # -- caches -------------------------------------------------------------------
+    def UpdateHGLut(self, g):
+        _check(lib().mrp_update_hg_lut(self._h, float(g)))
+
+    def Update_TR(self, lightDir, alpha=64.0, CPU=False):
+        _check(lib().mrp_update_tr(self._h, _f3(lightDir), float(alpha)))
+
+    def Update_CachedTR(self, lightDir, alpha):
+        _check(lib().mrp_update_baked_tr(self._h, _f3(lightDir), float(alpha)))
+
+    # -- rendering ----------------------------------------------------------------
+    def make_view(self, size, ori, up, right, lightDir, g=0.857, alpha=1.0, lightColor=(1, 1, 1), multiScatter=512,
+                  spp=32, seed=0, frame_offset=0):
+        w, h = (size, size) if np.isscalar(size) else size
+        return View(int(w), int(h), _f3(ori), _f3(up), _f3(right), _f3(lightDir), _f3(lightColor), float(alpha),
+                    float(g), int(multiScatter), int(spp), int(seed), int(frame_offset))
+
+    def Render(self, size, ori, up, right, lightDir, rt=PT, g=0.857, alpha=1.0, lightColor=(1, 1, 1),
+               multiScatter=512, sampleNum=1024, spp=32, seed=0, out=None):
+        """VolumeRender::Render (core/volume.cu:487-548) -> float32 [H, W, 4]
+        (or into `out`, a numpy array or CUDA tensor of H*W*4 floats)."""
+        view = self.make_view(size, ori, up, right, lightDir, g, alpha, lightColor, multiScatter, spp, seed)
+        if out is None:
+            out = np.empty((view.height, view.width, 4), np.float32)
+        p, dev = _ptr(out)
+        _check(lib().mrp_render(self._h, C.byref(view), int(rt), int(sampleNum), p, dev))
+        return out
+
+    def render_view(self, view, rt, sample_num, out):
+        p, dev = _ptr(out)
+        _check(lib().mrp_render(self._h, C.byref(view), int(rt), int(sample_num), p, dev))
+        return out
+
+    def last_render_ms(self):
+        ms = C.c_float()
+        _check(lib().mrp_last_render_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    # -- parity pieces ------------------------------------------------------------
+    def gather_features(self, pos, bases, light_dir, g, alpha):
+        pos = _host_f32(pos).reshape(-1, 3)
+        bases = _host_f32(bases).reshape(-1, 12)
+        n = pos.shape[0]
+        feat = np.empty((n, 576), np.float32)
+        gam = np.empty(n, np.float32)
+        _check(lib().mrp_gather_features(self._h, pos.ctypes.data, bases.ctypes.data, _f3(light_dir), float(g),
+                                         float(alpha), n, feat.ctypes.data, gam.ctypes.data, 0))
+        return feat, gam
+
+    def first_hit(self, ori, dirs, alpha):
+        ori = _host_f32(ori).reshape(-1, 3)
+        dirs = _host_f32(dirs).reshape(-1, 3)
+        n = dirs.shape[0]
+        if ori.shape[0] == 1 and n > 1:
+            ori = np.ascontiguousarray(np.repeat(ori, n, axis=0))
+        out = np.empty((n, 4), np.float32)
+        _check(lib().mrp_first_hit(self._h, ori.ctypes.data, dirs.ctypes.data, float(alpha), n, out.ctypes.data, 0))
+        return out
+
+
+def camera_frame(position):
+    """Camera::SetPosition (core/camera.cu:176-192): look-at-origin frame."""
+    ori = np.asarray(position, np.float32)
+    fwd = -ori / np.float32(np.sqrt(np.float32(np.dot(ori, ori))))
+    right = np.cross(np.array([0, 1, 0], np.float32), fwd).astype(np.float32)
+    right = right / np.float32(np.sqrt(np.float32(np.dot(right, right))))
+    up = np.cross(fwd, right).astype(np.float32)
+    if position[0] == 0 and position[2] == 0:
+        right = np.array([1, 0, 0], np.float32)
+        up = np.array([0, 0, 1 if position[1] > 0 else -1], np.float32)
+    return ori, up, right
+
+
+class Camera:
+    """Camera (core/camera.hpp:29-43).  fov_deg scales right/up by tan(fov/2)
+    (the reference's unit vectors give 90 degrees)."""
+
+    def __init__(self, volume, name="test camera", position=(0.75, 0.75, 0.75), resolution=512, fov_deg=90.0):
+        self.volume = volume
+        self.name = name
+        self.resolution = resolution
+        self.fov_deg = fov_deg
+        self.SetPosition(position)
+
+    def SetPosition(self, position):
+        self.ori, self.up, self.right = camera_frame(position)
+
+    def GetPosition(self):
+        return self.ori
+
+    def SetVolume(self, volume):
+        self.volume = volume
+
+    def _scaled(self):
+        s = np.float32(np.tan(np.deg2rad(self.fov_deg) / 2))
+        return (self.up * s).astype(np.float32), (self.right * s).astype(np.float32)
+
+    def Render(self, lightDir, lightColor=(1, 1, 1), alpha=1.0, multiScatter=1, g=0.0, sampleNum=1,
+               rt=VolumeRender.PT, **kw):
+        up, right = self._scaled()
+        return self.volume.Render((self.resolution, self.resolution), self.ori, up, right, lightDir, rt, g, alpha,
+                                  lightColor, multiScatter, sampleNum, **kw)
+
+    def RenderToFile(self, path, lightDir, lightColor=(1, 1, 1), alpha=1.0, multiScatter=1, g=0.0, sampleNum=1,
+                     tone=None, rt=VolumeRender.PT, exp=1.0, **kw):
+        """Camera::RenderToFile (core/camera.cu:229-257): saturate to 8 bit and
+        write `path`.png; like the reference it ignores `tone` and `exp`."""
+        img = self.Render(lightDir, lightColor, alpha, multiScatter, g, sampleNum, rt, **kw)
+        rgb = (np.clip(img[..., :3], 0.0, 1.0) * 255).astype(np.uint8)
+        rgba = np.concatenate([rgb, np.full(rgb.shape[:2] + (1,), 255, np.uint8)], axis=-1)
+        from PIL import Image
+        Image.fromarray(rgba, "RGBA").save(path + ".png")
+        return img

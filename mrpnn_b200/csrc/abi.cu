@@ -1,0 +1,794 @@
+// abi.cu -- host side of the C ABI (include/mrpnn.h): library state, volume
+// handles, resource caches and the render loop of VolumeRender::Render.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <dlfcn.h>
+
+#include "../../include/mrpnn.h"
+#include "kernels.h"
+#include "mlp_tc.h"
+
+using namespace mrp;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string t_err;
+static mrp_status fail(mrp_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return s;
+}
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "%s: %s (%s:%d)", #call, \
+                        cudaGetErrorString(e_), __FILE__, __LINE__);                               \
+    } while (0)
+#define TRY(call)                                                                                  \
+    do {                                                                                           \
+        mrp_status s_ = (call);                                                                    \
+        if (s_ != MRP_OK) return s_;                                                               \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// library state (one device per process)
+// ---------------------------------------------------------------------------
+namespace {
+struct Lib {
+    std::mutex mu;
+    bool ready = false;
+    int device = -1;
+    int sms = 148;
+    cudaStream_t stream = nullptr;   // for handle-less calls
+    std::map<std::string, std::vector<float>> model;
+    float* d_weights = nullptr;      // packed fp32 weights (common.cuh layout)
+    std::vector<float> h_weights;
+    TcWeights tc;                    // tensor-core weight images
+    // scratch for handle-less parity calls
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+};
+Lib g;
+
+std::string default_model_path() {
+    Dl_info info;
+    if (dladdr((void*)&default_model_path, &info) && info.dli_fname) {
+        std::string p = info.dli_fname;
+        size_t s = p.rfind('/');
+        std::string dir = s == std::string::npos ? "." : p.substr(0, s);
+        return dir + "/data/mrpnn_model.bin";
+    }
+    return "mrpnn_model.bin";
+}
+
+uint32_t pcg_host(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+
+// Digit permutations of the scrambled radical inverse for bases 2,3,5,7,11
+// (seeded Fisher-Yates; the reference ships a fixed random table,
+// core/volume.cu:1196).
+void halton_perms(uint32_t perm[28]) {
+    const uint32_t primes[5] = {2, 3, 5, 7, 11}, sums[5] = {0, 2, 5, 10, 17};
+    for (int b = 0; b < 5; ++b) {
+        for (uint32_t i = 0; i < primes[b]; ++i) perm[sums[b] + i] = i;
+        uint32_t h = 0x4D525031u + (uint32_t)b;
+        for (uint32_t i = primes[b] - 1; i > 0; --i) {
+            h = pcg_host(h);
+            uint32_t j = h % (i + 1);
+            std::swap(perm[sums[b] + i], perm[sums[b] + j]);
+        }
+    }
+}
+
+float lerp_h(float a, float b, float v) { return a * (1.0f - v) + b * v; }
+
+// GetSamples23_ (core/vector.cu:304-405): offset and mip layer of stencil
+// point i, plus the HG-LUT row v of SetupInputData (core/radiancePredict.cu:458-464).
+void stencil_tables(StencilTables& t, const std::vector<float>& dirs) {
+    for (int i = 0; i < 192; ++i) {
+        float o, layer;
+        const float sc = 0.6f;
+        if (i < 8) { o = (float)(1.0 / 256.0); o *= lerp_h(sc, 1.0f, 1.0f); layer = 0; }
+        else if (i < 16) { o = (float)(2.5 / 256.0); o *= lerp_h(sc, 1.0f, 0.8f); layer = 1; }
+        else if (i < 32) { o = (float)(5.5 / 256.0); o *= lerp_h(sc, 1.0f, 0.6f); layer = 2; }
+        else if (i < 48) { o = (float)(11.5 / 256.0); o *= lerp_h(sc, 1.0f, 0.4f); layer = 3; }
+        else if (i < 64) { o = (float)(23.5 / 256.0); o *= lerp_h(sc, 1.0f, 0.2f); layer = 4; }
+        else if (i < 96) { o = (float)(47.5 / 256.0); o *= sc; layer = 5; }
+        else if (i < 128) { o = (float)(95.5 / 256.0); o *= sc; layer = 6; }
+        else if (i < 160) { o = (float)(191.5 / 256.0); o *= sc; layer = 7; }
+        else if (i < 168) { o = (float)(i - 160 + 1); o = (float)(o / 256.0); layer = 0; }
+        else if (i < 176) { o = (float)(8.5 + 1 + 2.0 * (i - 168)); o = (float)(o / 256.0); layer = 1; }
+        else if (i < 184) { o = (float)(26.5 + 4.0 * (i - 176)); o = (float)(o / 256.0); layer = 2; }
+        else { o = (float)(60.5 + 8.0 * (i - 184)); o = (float)(o / 256.0); layer = 3; }
+        layer += 0.1f;
+        int l = (int)layer;
+        t.offset[i] = o;
+        t.layer[i] = l;
+        float radius = (float)(1 << l) / 256.0f;
+        float angle = std::atan(0.5f * radius / o);
+        t.lut_v[i] = angle / (3.1415926535f * 60.0f / 180.0f);
+    }
+    std::memcpy(t.dirs, dirs.data(), sizeof t.dirs);
+}
+
+mrp_status read_model(const char* path, std::map<std::string, std::vector<float>>& out) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(MRP_ERR_IO, "cannot open model file %s", path);
+    char magic[8];
+    uint32_t count = 0;
+    if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, "MRPNNMD1", 8) != 0 || std::fread(&count, 4, 1, f) != 1) {
+        std::fclose(f);
+        return fail(MRP_ERR_IO, "%s: not an MRPNN model file", path);
+    }
+    out.clear();
+    for (uint32_t k = 0; k < count; ++k) {
+        uint16_t len = 0;
+        uint32_t n = 0;
+        std::string name;
+        if (std::fread(&len, 2, 1, f) != 1) break;
+        name.resize(len);
+        if (std::fread(&name[0], 1, len, f) != len || std::fread(&n, 4, 1, f) != 1 || n > (1u << 24)) break;
+        std::vector<float> v(n);
+        if (std::fread(v.data(), 4, n, f) != n) break;
+        out[name] = std::move(v);
+    }
+    std::fclose(f);
+    if (out.size() != count) return fail(MRP_ERR_IO, "%s: truncated model file", path);
+    return MRP_OK;
+}
+
+// Packs the named tensors into the kernel layout (common.cuh).
+mrp_status pack_weights(const std::map<std::string, std::vector<float>>& m, std::vector<float>& w) {
+    w.clear();
+    auto put = [&](const std::string& name, size_t n) -> bool {
+        auto it = m.find(name);
+        if (it == m.end() || it->second.size() != n) { t_err = "model tensor " + name + " missing or mis-sized"; return false; }
+        w.insert(w.end(), it->second.begin(), it->second.end());
+        return true;
+    };
+    auto block = [&](const std::string& se, const std::string& d, const std::string& tr, const std::string& hg,
+                     int wdt) -> bool {
+        return put(se + "1W", 64) && put(se + "2W", 24) && put(d + "W", wdt * wdt) && put(d + "B", wdt) &&
+               put(tr + "W", wdt * wdt) && put(tr + "B", wdt) && put(hg + "W", wdt * wdt) && put(hg + "B", wdt);
+    };
+    for (int k = 0; k < 8; ++k) {
+        std::string s = std::to_string(k);
+        if (!block("LSE" + s, "L" + s + "1", "L_Tr" + s + "1", "L_Hg" + s + "1", kMainW[k])) return MRP_ERR_IO;
+    }
+    if (!(put("L81W", 1024) && put("L81B", 32) && put("L_Tr81W", 1024) && put("L_Tr81B", 32) && put("L_Hg81W", 1024) &&
+          put("L_Hg81B", 32)))
+        return MRP_ERR_IO;
+    for (int k = 0; k < 4; ++k) {
+        std::string s = std::to_string(k);
+        if (!block("LDSE" + s, "LD" + s + "1", "LD_Tr" + s + "1", "LD_Hg" + s + "1", 8)) return MRP_ERR_IO;
+    }
+    if (!(put("LD41W", 64) && put("LD41B", 8) && put("LD_Tr41W", 64) && put("LD_Tr41B", 8) && put("LD_Hg41W", 64) &&
+          put("LD_Hg41B", 8)))
+        return MRP_ERR_IO;
+    if (!(put("LGGSW", 24) && put("LGGSB", 8) && put("LSEFin1W", 1200) && put("LSEFin2W", 96) && put("LC0W", 16384) &&
+          put("LC0B", 128) && put("LC1W", 8192) && put("LC1B", 64) && put("LC2W", 2048) && put("LC2B", 32) &&
+          put("LXW", 512) && put("LXB", 16)))
+        return MRP_ERR_IO;
+    for (int k = 0; k < 12; ++k)
+        if (!(put("LX" + std::to_string(k) + "W", 256) && put("LX" + std::to_string(k) + "B", 16))) return MRP_ERR_IO;
+    if (!(put("LX12W", 16) && put("LX12B", 1))) return MRP_ERR_IO;
+    if ((int)w.size() != kWeightCount) return fail(MRP_ERR_IO, "packed %zu weights, expected %d", w.size(), kWeightCount);
+    return MRP_OK;
+}
+
+mrp_status ensure_scratch(size_t bytes) {
+    if (g.scratch_bytes >= bytes) return MRP_OK;
+    if (g.scratch) cudaFree(g.scratch);
+    g.scratch = nullptr;
+    g.scratch_bytes = 0;
+    CU(cudaMalloc(&g.scratch, bytes));
+    g.scratch_bytes = bytes;
+    return MRP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// volume handle
+// ---------------------------------------------------------------------------
+struct mrp_volume {
+    int res = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.0f;
+    float* density = nullptr;
+    float* mips = nullptr;
+    float* trs = nullptr;
+    float* lut = nullptr;
+    float* baked = nullptr;
+    int baked_alloc_res = 0;
+    uint8_t* occ = nullptr;
+    int occ_shift = 3, occ_res = 0;
+    int* d_maxbits = nullptr;
+    bool has_data = false, has_pyramid = false, has_lut = false, has_tr = false, has_baked = false;
+    bool max_override = false;
+    float max_density = 0.00001f;
+    float lut_g = NAN, tr_alpha = NAN, tr_light[3] = {NAN, NAN, NAN};
+    float bk_alpha = NAN, bk_light[3] = {NAN, NAN, NAN};
+    int bk_res = 0;
+    uint32_t lut_seed = 0, bk_seed = 0;
+    mrp_params params;
+    // render buffers
+    float4* accum = nullptr;
+    size_t accum_pix = 0;
+    double* sum3 = nullptr;
+    int* first_pos = nullptr;
+    unsigned long long* counter = nullptr;
+    size_t trace_pix = 0;
+    // tensor-core predictor scratch
+    TcScratch tc;
+
+    VolumeDev dev() const {
+        VolumeDev d{};
+        d.density = density;
+        d.res = res;
+        d.max_density = max_density;
+        d.mips = mips;
+        d.trs = trs;
+        d.lut = lut;
+        d.baked = baked;
+        d.baked_res = bk_res;
+        d.occ = occ;
+        d.occ_shift = occ_shift;
+        d.occ_res = occ_res;
+        d.scatter_rate = {params.scatter_rate[0], params.scatter_rate[1], params.scatter_rate[2]};
+        d.tr_scale = params.tr_scale;
+        d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};
+        return d;
+    }
+};
+
+static mrp_status need_init() {
+    if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");
+    return MRP_OK;
+}
+
+extern "C" {
+
+const char* mrp_last_error(void) { return t_err.c_str(); }
+const char* mrp_version(void) { return "mrpnn_b200 0.1 (sm_100a)"; }
+
+void mrp_default_params(mrp_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->scatter_rate[0] = p->scatter_rate[1] = p->scatter_rate[2] = 1.001f;
+    p->tr_scale = 1.0f;
+    p->env_exp = 1.0f;
+    p->bake_res = 768;
+    p->bake_replicate_seeding = 1;
+    p->precision = MRP_FP32;
+    p->seed = 0;
+}
+
+mrp_status mrp_load_model(const char* path) {
+    std::lock_guard<std::mutex> lk(g.mu);
+    if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");
+    std::map<std::string, std::vector<float>> m;
+    TRY(read_model(path, m));
+    std::vector<float> w;
+    if (pack_weights(m, w) != MRP_OK) return fail(MRP_ERR_IO, "%s: %s", path, t_err.c_str());
+    auto it = m.find("STENCIL_DIRS");
+    if (it == m.end() || it->second.size() != 480) return fail(MRP_ERR_IO, "%s: missing STENCIL_DIRS", path);
+    StencilTables st;
+    stencil_tables(st, it->second);
+    CU(set_stencil_tables(st));
+    if (!g.d_weights) CU(cudaMalloc(&g.d_weights, sizeof(float) * kWeightCount));
+    CU(cudaMemcpy(g.d_weights, w.data(), sizeof(float) * kWeightCount, cudaMemcpyHostToDevice));
+    CU(tc_prepare_weights(w.data(), g.tc));
+    g.model = std::move(m);
+    g.h_weights = std::move(w);
+    return MRP_OK;
+}
+
+mrp_status mrp_init(int device, const char* model_path) {
+    {
+        std::lock_guard<std::mutex> lk(g.mu);
+        if (!g.ready) {
+            int n = 0;
+            cudaError_t e = cudaGetDeviceCount(&n);
+            if (e != cudaSuccess || n == 0)
+                return fail(MRP_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
+            if (device < 0 || device >= n) return fail(MRP_ERR_INVALID, "device %d out of range (%d)", device, n);
+            CU(cudaSetDevice(device));
+            cudaDeviceProp prop;
+            CU(cudaGetDeviceProperties(&prop, device));
+            if (prop.major != 10)
+                return fail(MRP_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                            prop.major, prop.minor);
+            g.device = device;
+            g.sms = prop.multiProcessorCount;
+            CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+            uint32_t perm[28];
+            halton_perms(perm);
+            CU(set_halton_permutations(perm));
+            g.ready = true;
+        } else {
+            CU(cudaSetDevice(g.device));
+        }
+    }
+    if (g.d_weights && !model_path) return MRP_OK;
+    std::string p = model_path ? model_path : default_model_path();
+    return mrp_load_model(p.c_str());
+}
+
+mrp_status mrp_volume_create(int res, mrp_volume** out) {
+    TRY(need_init());
+    if (!out || res < 2 || res > 2048) return fail(MRP_ERR_INVALID, "volume resolution %d out of range [2, 2048]", res);
+    mrp_volume* v = new mrp_volume();
+    v->res = res;
+    mrp_default_params(&v->params);
+    auto cleanup = [&](mrp_status s) { mrp_volume_destroy(v); return s; };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&v->ev0)) != cudaSuccess || (e = cudaEventCreate(&v->ev1)) != cudaSuccess)
+        return cleanup(fail(MRP_ERR_CUDA, "stream/event: %s", cudaGetErrorString(e)));
+    size_t n = (size_t)res * res * res;
+    v->occ_res = (res + (1 << v->occ_shift) - 1) >> v->occ_shift;
+    size_t nocc = (size_t)v->occ_res * v->occ_res * v->occ_res;
+    if ((e = cudaMalloc(&v->density, n * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v->mips, kMipFloats * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v->lut, kLut * kLut * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess)
+        return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
+                            cudaGetErrorString(e)));
+    cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
+    *out = v;
+    return MRP_OK;
+}
+
+mrp_status mrp_volume_destroy(mrp_volume* v) {
+    if (!v) return MRP_OK;
+    if (v->stream) cudaStreamSynchronize(v->stream);
+    cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
+    cudaFree(v->occ); cudaFree(v->d_maxbits); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
+    cudaFree(v->counter);
+    tc_free_scratch(v->tc);
+    if (v->ev0) cudaEventDestroy(v->ev0);
+    if (v->ev1) cudaEventDestroy(v->ev1);
+    if (v->stream) cudaStreamDestroy(v->stream);
+    delete v;
+    return MRP_OK;
+}
+
+static void invalidate(mrp_volume* v) {
+    v->has_pyramid = v->has_tr = v->has_baked = false;
+    v->tr_alpha = NAN; v->bk_alpha = NAN;
+}
+
+mrp_status mrp_volume_set_data(mrp_volume* v, const float* data, int res, int is_device) {
+    TRY(need_init());
+    if (!v || !data || res != v->res) return fail(MRP_ERR_INVALID, "set_data: resolution %d != volume %d", res, v ? v->res : -1);
+    size_t bytes = (size_t)res * res * res * sizeof(float);
+    CU(cudaMemcpyAsync(v->density, data, bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, v->stream));
+    CU(cudaStreamSynchronize(v->stream));
+    v->has_data = true;
+    invalidate(v);
+    return MRP_OK;
+}
+
+mrp_status mrp_volume_fill(mrp_volume* v, mrp_fill_fn fn, void* user) {
+    TRY(need_init());
+    if (!v || !fn) return fail(MRP_ERR_INVALID, "fill: null argument");
+    int R = v->res;
+    std::vector<float> host((size_t)R * R * R);
+    unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (int i = (int)t; i < R; i += (int)nt)
+                for (int j = 0; j < R; ++j)
+                    for (int k = 0; k < R; ++k) {
+                        float u = (float)((i + 0.5) / R), w2 = (float)((j + 0.5) / R), w3 = (float)((k + 0.5) / R);
+                        host[((size_t)i * R + j) * R + k] = fn(i, j, k, u, w2, w3, user);
+                    }
+        });
+    for (auto& t : th) t.join();
+    return mrp_volume_set_data(v, host.data(), R, 0);
+}
+
+mrp_status mrp_volume_generate_fbm(mrp_volume* v, uint32_t seed, float base_freq, int octaves, float gain) {
+    TRY(need_init());
+    if (!v || octaves < 1 || octaves > 16) return fail(MRP_ERR_INVALID, "fbm: bad arguments");
+    CU(launch_fbm(v->density, v->res, seed, base_freq, octaves, gain, g.sms, v->stream));
+    CU(cudaStreamSynchronize(v->stream));
+    v->has_data = true;
+    invalidate(v);
+    return MRP_OK;
+}
+
+mrp_status mrp_volume_set_max_density(mrp_volume* v, float md) {
+    if (!v || !(md > 0)) return fail(MRP_ERR_INVALID, "max density must be > 0");
+    v->max_density = md;
+    v->max_override = true;
+    v->has_baked = false; v->bk_alpha = NAN;
+    return MRP_OK;
+}
+
+mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
+    TRY(need_init());
+    if (!v) return fail(MRP_ERR_INVALID, "null volume");
+    if (!v->has_data) return fail(MRP_ERR_NOT_READY, "update: no data set");
+    int R = v->res;
+    size_t n = (size_t)R * R * R;
+    if (!v->max_override) {
+        int init;
+        { float f0 = 0.00001f; std::memcpy(&init, &f0, sizeof init); }
+        CU(cudaMemcpyAsync(v->d_maxbits, &init, sizeof(int), cudaMemcpyHostToDevice, v->stream));
+        CU(launch_max_density(v->density, n, v->d_maxbits, g.sms, v->stream));
+        int bits = 0;
+        CU(cudaMemcpyAsync(&bits, v->d_maxbits, sizeof(int), cudaMemcpyDeviceToHost, v->stream));
+        CU(cudaStreamSynchronize(v->stream));
+        std::memcpy(&v->max_density, &bits, sizeof(float));
+    }
+    CU(launch_occupancy(v->density, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
+    if (process_mips) {
+        // core/volume.cu:1476-1514: halve to the largest power of two >= 256
+        // below the input, then 9 levels 256 >> m, each from the previous one.
+        int res = 256;
+        while (res * 2 < R) res <<= 1;
+        const float* src = v->density;
+        int src_res = R;
+        float* tmp[2] = {nullptr, nullptr};
+        int which = 0;
+        for (; res > 256; res >>= 1) {
+            float*& t = tmp[which];
+            if (!t) CU(cudaMalloc(&t, (size_t)res * res * res * sizeof(float)));
+            CU(launch_resample(t, res, src, src_res, g.sms, v->stream));
+            src = t;
+            src_res = res;
+            which ^= 1;
+        }
+        for (int m = 0; m < 9; ++m) {
+            int r = 256 >> m;
+            float* dst = v->mips + mip_offset(m);
+            CU(launch_resample(dst, r, src, src_res, g.sms, v->stream));
+            src = dst;
+            src_res = r;
+        }
+        CU(cudaStreamSynchronize(v->stream));
+        cudaFree(tmp[0]);
+        cudaFree(tmp[1]);
+        v->has_pyramid = true;
+    }
+    CU(cudaStreamSynchronize(v->stream));
+    v->has_tr = false; v->tr_alpha = NAN;
+    v->has_baked = false; v->bk_alpha = NAN;
+    return MRP_OK;
+}
+
+mrp_status mrp_volume_get_info(const mrp_volume* v, mrp_volume_info* info) {
+    if (!v || !info) return fail(MRP_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof *info);
+    info->res = v->res;
+    info->max_density = v->max_density;
+    info->has_pyramid = v->has_pyramid;
+    info->has_lut = v->has_lut;
+    info->has_tr = v->has_tr;
+    info->has_baked_tr = v->has_baked;
+    info->lut_g = v->lut_g;
+    info->tr_alpha = v->tr_alpha;
+    for (int i = 0; i < 3; ++i) info->tr_light[i] = v->tr_light[i];
+    size_t R = v->res;
+    info->device_bytes = R * R * R * 4 + kMipFloats * 4 + kTrFloats * 4 + kLut * kLut * 4 +
+                         (size_t)v->baked_alloc_res * v->baked_alloc_res * v->baked_alloc_res * 4;
+    return MRP_OK;
+}
+
+mrp_status mrp_set_params(mrp_volume* v, const mrp_params* p) {
+    if (!v || !p) return fail(MRP_ERR_INVALID, "null argument");
+    if (p->bake_res < 2 || p->bake_res > 2048) return fail(MRP_ERR_INVALID, "bake_res %d out of range", p->bake_res);
+    if (p->precision != MRP_FP32 && p->precision != MRP_BF16 && p->precision != MRP_FP8)
+        return fail(MRP_ERR_INVALID, "unknown precision %d", (int)p->precision);
+    bool bake_changed = p->bake_res != v->params.bake_res || p->tr_scale != v->params.tr_scale ||
+                        p->bake_replicate_seeding != v->params.bake_replicate_seeding || p->seed != v->params.seed;
+    bool lut_changed = p->seed != v->params.seed;
+    v->params = *p;
+    if (bake_changed) { v->has_baked = false; v->bk_alpha = NAN; }
+    if (lut_changed) { v->has_lut = false; v->lut_g = NAN; }
+    return MRP_OK;
+}
+mrp_status mrp_get_params(const mrp_volume* v, mrp_params* p) {
+    if (!v || !p) return fail(MRP_ERR_INVALID, "null argument");
+    *p = v->params;
+    return MRP_OK;
+}
+
+mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* dst, size_t* count, int dst_is_device) {
+    if (!v) return fail(MRP_ERR_INVALID, "null volume");
+    const void* src = nullptr;
+    size_t n = 0, esize = sizeof(float);
+    switch (which) {
+        case MRP_RES_DENSITY: src = v->density; n = (size_t)v->res * v->res * v->res; break;
+        case MRP_RES_MIP:
+            if (level < 0 || level > 8) return fail(MRP_ERR_INVALID, "mip level %d", level);
+            src = v->mips + mip_offset(level); n = (size_t)(256 >> level) * (256 >> level) * (256 >> level); break;
+        case MRP_RES_TR:
+            if (level < 0 || level > 7) return fail(MRP_ERR_INVALID, "TR level %d", level);
+            src = v->trs + tr_offset(level); n = (size_t)(128 >> level) * (128 >> level) * (128 >> level); break;
+        case MRP_RES_LUT: src = v->lut; n = kLut * kLut; break;
+        case MRP_RES_BAKED_TR:
+            if (!v->baked) return fail(MRP_ERR_NOT_READY, "no baked TR");
+            src = v->baked; n = (size_t)v->bk_res * v->bk_res * v->bk_res; break;
+        case MRP_RES_OCCUPANCY: src = v->occ; n = (size_t)v->occ_res * v->occ_res * v->occ_res; esize = 1; break;
+        default: return fail(MRP_ERR_INVALID, "unknown resource %d", (int)which);
+    }
+    if (count) *count = n;
+    if (!dst) return MRP_OK;
+    CU(cudaMemcpyAsync(dst, src, n * esize, dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, v->stream));
+    CU(cudaStreamSynchronize(v->stream));
+    return MRP_OK;
+}
+
+// --- caches ----------------------------------------------------------------
+static mrp_status update_lut_async(mrp_volume* v, float g_) {
+    if (v->has_lut && v->lut_g == g_ && v->lut_seed == v->params.seed) return MRP_OK;
+    CU(launch_hg_lut(v->lut, g_, v->params.seed, v->stream));
+    v->has_lut = true;
+    v->lut_g = g_;
+    v->lut_seed = v->params.seed;
+    return MRP_OK;
+}
+static mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
+    if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "TR mips need the pyramid (call mrp_volume_update)");
+    if (v->has_tr && v->tr_alpha == alpha && v->tr_light[0] == L[0] && v->tr_light[1] == L[1] && v->tr_light[2] == L[2])
+        return MRP_OK;
+    for (int lv = 0; lv < 8; ++lv) {
+        float a = alpha / std::pow(1.73f, (float)lv + 1.0f);
+        CU(launch_tr_level(v->trs + tr_offset(lv), 128 >> lv, v->mips + mip_offset(lv + 1), a, L, g.sms, v->stream));
+    }
+    v->has_tr = true;
+    v->tr_alpha = alpha;
+    std::memcpy(v->tr_light, L, sizeof v->tr_light);
+    return MRP_OK;
+}
+static mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha) {
+    int B = v->params.bake_res;
+    if (v->has_baked && v->bk_alpha == alpha && v->bk_res == B && v->bk_seed == v->params.seed &&
+        v->bk_light[0] == L[0] && v->bk_light[1] == L[1] && v->bk_light[2] == L[2])
+        return MRP_OK;
+    if (v->baked_alloc_res != B) {
+        cudaFree(v->baked);
+        v->baked = nullptr;
+        v->baked_alloc_res = 0;
+        CU(cudaMalloc(&v->baked, (size_t)B * B * B * sizeof(float)));
+        v->baked_alloc_res = B;
+    }
+    v->bk_res = B;
+    VolumeDev d = v->dev();
+    CU(launch_baked_tr(v->baked, d, B, alpha, L, v->params.seed, v->params.bake_replicate_seeding, g.sms, v->stream));
+    v->has_baked = true;
+    v->bk_alpha = alpha;
+    v->bk_seed = v->params.seed;
+    std::memcpy(v->bk_light, L, sizeof v->bk_light);
+    return MRP_OK;
+}
+
+mrp_status mrp_update_hg_lut(mrp_volume* v, float g_) {
+    TRY(need_init());
+    if (!v) return fail(MRP_ERR_INVALID, "null volume");
+    TRY(update_lut_async(v, g_));
+    CU(cudaStreamSynchronize(v->stream));
+    return MRP_OK;
+}
+mrp_status mrp_update_tr(mrp_volume* v, const float light_dir[3], float alpha) {
+    TRY(need_init());
+    if (!v || !light_dir) return fail(MRP_ERR_INVALID, "null argument");
+    TRY(update_tr_async(v, light_dir, alpha));
+    CU(cudaStreamSynchronize(v->stream));
+    return MRP_OK;
+}
+mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float alpha) {
+    TRY(need_init());
+    if (!v || !light_dir) return fail(MRP_ERR_INVALID, "null argument");
+    if (!v->has_data) return fail(MRP_ERR_NOT_READY, "no data");
+    TRY(update_baked_async(v, light_dir, alpha));
+    CU(cudaStreamSynchronize(v->stream));
+    return MRP_OK;
+}
+
+// --- rendering ----------------------------------------------------------------
+static ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k) {
+    ViewDev d{};
+    d.width = w->width;
+    d.height = w->height;
+    d.ori = {w->ori[0], w->ori[1], w->ori[2]};
+    d.up = {w->up[0], w->up[1], w->up[2]};
+    d.right = {w->right[0], w->right[1], w->right[2]};
+    d.light_dir = {w->light_dir[0], w->light_dir[1], w->light_dir[2]};
+    d.light_color = {w->light_color[0], w->light_color[1], w->light_color[2]};
+    d.alpha = w->alpha;
+    d.g = w->g;
+    d.multi_scatter = w->multi_scatter;
+    d.spp = w->spp;
+    d.seed = w->seed;
+    d.frame = frame;
+    d.mean_k = mean_k;
+    float t_step = 2.0f / (float)v->res;
+    float smax = v->max_density * w->alpha;
+    d.pass_rate = std::exp(-t_step * smax);
+    return d;
+}
+
+mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out, int out_is_device) {
+    TRY(need_init());
+    if (!v || !w || !out) return fail(MRP_ERR_INVALID, "null argument");
+    if (w->width <= 0 || w->height <= 0 || (long long)w->width * w->height > (1ll << 28))
+        return fail(MRP_ERR_INVALID, "image size %dx%d", w->width, w->height);
+    if (sample_num < 1) return fail(MRP_ERR_INVALID, "sample_num must be >= 1");
+    if (type == MRP_RPNN) return fail(MRP_ERR_UNSUPPORTED, "RPNN is compiled only with -DCRPNN in the reference");
+    if (type != MRP_PT && type != MRP_MRPNN) return fail(MRP_ERR_INVALID, "unknown render type %d", (int)type);
+    if (!v->has_data) return fail(MRP_ERR_NOT_READY, "no volume data");
+    if (type == MRP_MRPNN && !v->has_pyramid) return fail(MRP_ERR_NOT_READY, "MRPNN needs the pyramid (mrp_volume_update)");
+    if (type == MRP_PT && (w->spp < 1 || w->multi_scatter < 1)) return fail(MRP_ERR_INVALID, "PT needs spp, multi_scatter >= 1");
+    size_t npix = (size_t)w->width * w->height;
+    if (v->accum_pix < npix) {
+        cudaFree(v->accum);
+        v->accum = nullptr;
+        v->accum_pix = 0;
+        CU(cudaMalloc(&v->accum, npix * sizeof(float4)));
+        v->accum_pix = npix;
+    }
+    if (type == MRP_PT && v->trace_pix < npix) {
+        cudaFree(v->sum3); cudaFree(v->first_pos); cudaFree(v->counter);
+        v->sum3 = nullptr; v->first_pos = nullptr; v->counter = nullptr; v->trace_pix = 0;
+        CU(cudaMalloc(&v->sum3, npix * 3 * sizeof(double)));
+        CU(cudaMalloc(&v->first_pos, npix * sizeof(int)));
+        CU(cudaMalloc(&v->counter, sizeof(unsigned long long)));
+        v->trace_pix = npix;
+    }
+    // caches first (the reference updates them inside its launch loop,
+    // core/volume.cu:511-518; they do not change between its launches)
+    if (type == MRP_MRPNN) {
+        TRY(update_lut_async(v, w->g));
+        TRY(update_tr_async(v, w->light_dir, w->alpha));
+    } else {
+        TRY(update_baked_async(v, w->light_dir, w->alpha));
+    }
+    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) TRY(tc_ensure_scratch(v->tc, npix) == cudaSuccess ? MRP_OK
+                                                                        : fail(MRP_ERR_OOM, "tensor-core scratch"));
+    VolumeDev d = v->dev();
+    CU(cudaEventRecord(v->ev0, v->stream));
+    for (int i = 0; i < sample_num; ++i) {
+        ViewDev vd = make_view(v, w, w->frame_offset + i, i);
+        if (type == MRP_MRPNN) {
+            if (v->params.precision == MRP_FP32) {
+                CU(launch_predict_fp32(d, vd, g.d_weights, v->accum, nullptr, nullptr, v->stream));
+            } else {
+                CU(tc_launch_predict(d, vd, g.tc, v->params.precision == MRP_FP8, v->tc, v->accum, g.sms, v->stream));
+            }
+        } else {
+            CU(cudaMemsetAsync(v->sum3, 0, npix * 3 * sizeof(double), v->stream));
+            CU(launch_fill_int(v->first_pos, (int)npix, w->spp, v->stream));
+            CU(cudaMemsetAsync(v->counter, 0, sizeof(unsigned long long), v->stream));
+            CU(launch_trace(d, vd, v->sum3, nullptr, v->first_pos, v->counter, g.sms, v->stream));
+            CU(launch_trace_resolve(v->sum3, v->first_pos, (int)npix, w->spp, i, v->accum, v->stream));
+        }
+    }
+    CU(cudaEventRecord(v->ev1, v->stream));
+    CU(cudaMemcpyAsync(out, v->accum, npix * sizeof(float4), out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       v->stream));
+    CU(cudaStreamSynchronize(v->stream));
+    CU(cudaEventElapsedTime(&v->last_ms, v->ev0, v->ev1));
+    return MRP_OK;
+}
+
+mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms) {
+    if (!v || !ms) return fail(MRP_ERR_INVALID, "null argument");
+    *ms = v->last_ms;
+    return MRP_OK;
+}
+
+// --- parity entry points --------------------------------------------------------
+mrp_status mrp_predict_features(const float* feat, const float* gamma, float g_, const float sr[3], int n, float* out3,
+                                mrp_precision precision, int is_device) {
+    TRY(need_init());
+    if (!feat || !gamma || !sr || !out3 || n < 0) return fail(MRP_ERR_INVALID, "null argument");
+    if (n == 0) return MRP_OK;
+    std::lock_guard<std::mutex> lk(g.mu);
+    const float *df = feat, *dg = gamma;
+    float* dout = out3;
+    if (!is_device) {
+        size_t need = (size_t)n * (576 + 1 + 3) * sizeof(float);
+        TRY(ensure_scratch(need));
+        float* base = (float*)g.scratch;
+        float* f = base;
+        float* gm = base + (size_t)n * 576;
+        dout = gm + n;
+        CU(cudaMemcpyAsync(f, feat, (size_t)n * 576 * sizeof(float), cudaMemcpyHostToDevice, g.stream));
+        CU(cudaMemcpyAsync(gm, gamma, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, g.stream));
+        df = f;
+        dg = gm;
+    }
+    if (precision == MRP_FP32) {
+        CU(launch_mlp_fp32(g.d_weights, df, dg, g_, sr, n, dout, g.stream));
+    } else if (precision == MRP_BF16 || precision == MRP_FP8) {
+        CU(tc_launch_mlp(g.tc, precision == MRP_FP8, df, dg, g_, sr, n, dout, g.sms, g.stream));
+    } else {
+        return fail(MRP_ERR_INVALID, "unknown precision %d", (int)precision);
+    }
+    if (!is_device) CU(cudaMemcpyAsync(out3, dout, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, g.stream));
+    CU(cudaStreamSynchronize(g.stream));
+    return MRP_OK;
+}
+
+mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bases, const float L[3], float g_, float alpha,
+                               int n, float* feat, float* gamma, int is_device) {
+    TRY(need_init());
+    if (!v || !pos || !bases || !L || !feat || !gamma || n < 0) return fail(MRP_ERR_INVALID, "null argument");
+    if (!v->has_pyramid || !v->has_tr || !v->has_lut) return fail(MRP_ERR_NOT_READY, "gather needs pyramid, TR mips and LUT");
+    if (n == 0) return MRP_OK;
+    float* dl = nullptr;
+    float *dp = (float*)pos, *db = (float*)bases, *dfeat = feat, *dgam = gamma;
+    std::vector<void*> allocs;
+    auto alloc = [&](size_t bytes) -> float* { void* p = nullptr; if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr; allocs.push_back(p); return (float*)p; };
+    auto release = [&]() { for (void* p : allocs) cudaFree(p); };
+    dl = alloc(3 * sizeof(float));
+    if (!dl) { release(); return fail(MRP_ERR_OOM, "gather scratch"); }
+    cudaMemcpyAsync(dl, L, 3 * sizeof(float), cudaMemcpyHostToDevice, v->stream);
+    if (!is_device) {
+        dp = alloc((size_t)n * 3 * 4); db = alloc((size_t)n * 12 * 4); dfeat = alloc((size_t)n * 576 * 4); dgam = alloc((size_t)n * 4);
+        if (!dp || !db || !dfeat || !dgam) { release(); return fail(MRP_ERR_OOM, "gather scratch"); }
+        cudaMemcpyAsync(dp, pos, (size_t)n * 3 * 4, cudaMemcpyHostToDevice, v->stream);
+        cudaMemcpyAsync(db, bases, (size_t)n * 12 * 4, cudaMemcpyHostToDevice, v->stream);
+    }
+    cudaError_t e = launch_gather(v->dev(), dp, db, dl, g_, alpha, n, dfeat, dgam, v->stream);
+    if (e == cudaSuccess && !is_device) {
+        cudaMemcpyAsync(feat, dfeat, (size_t)n * 576 * 4, cudaMemcpyDeviceToHost, v->stream);
+        cudaMemcpyAsync(gamma, dgam, (size_t)n * 4, cudaMemcpyDeviceToHost, v->stream);
+    }
+    cudaError_t e2 = cudaStreamSynchronize(v->stream);
+    release();
+    if (e != cudaSuccess || e2 != cudaSuccess)
+        return fail(MRP_ERR_CUDA, "gather: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return MRP_OK;
+}
+
+mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, float alpha, int n, float* hit4, int is_device) {
+    TRY(need_init());
+    if (!v || !ori || !dir || !hit4 || n < 0) return fail(MRP_ERR_INVALID, "null argument");
+    if (!v->has_data) return fail(MRP_ERR_NOT_READY, "no data");
+    if (n == 0) return MRP_OK;
+    float pass_rate = std::exp(-(2.0f / (float)v->res) * (v->max_density * alpha));
+    const float *dori = ori, *ddir = dir;
+    float* dhit = hit4;
+    float* tmp = nullptr;
+    if (!is_device) {
+        CU(cudaMalloc(&tmp, (size_t)n * 10 * sizeof(float)));
+        float* o = tmp; float* d = tmp + 3 * (size_t)n; dhit = tmp + 6 * (size_t)n;
+        cudaMemcpyAsync(o, ori, (size_t)n * 12, cudaMemcpyHostToDevice, v->stream);
+        cudaMemcpyAsync(d, dir, (size_t)n * 12, cudaMemcpyHostToDevice, v->stream);
+        dori = o; ddir = d;
+    }
+    cudaError_t e = launch_first_hit(v->dev(), dori, ddir, alpha, pass_rate, n, dhit, v->stream);
+    if (e == cudaSuccess && !is_device) cudaMemcpyAsync(hit4, dhit, (size_t)n * 16, cudaMemcpyDeviceToHost, v->stream);
+    cudaError_t e2 = cudaStreamSynchronize(v->stream);
+    if (tmp) cudaFree(tmp);
+    if (e != cudaSuccess || e2 != cudaSuccess) return fail(MRP_ERR_CUDA, "first_hit: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return MRP_OK;
+}
+
+}  // extern "C"

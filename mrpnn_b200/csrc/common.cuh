@@ -1,0 +1,248 @@
+// common.cuh -- device building blocks shared by the MRPNN B200 kernels.
+//
+// Rounding order.  The reference path is float arithmetic whose results the
+// build reproduces bit for bit where the operations are +, -, *, /, sqrt and
+// comparisons.  nvcc would otherwise contract a*b+c into FMAs, so every
+// expression that must keep the reference's rounding is written with the
+// IEEE round-to-nearest intrinsics below (which the compiler never fuses).
+// Transcendentals (log, exp, pow, atan, acos, sin, cos, tan) use the
+// non-fast-math CUDA functions; they can differ from the host's libm in the
+// last bit, which the parity tests allow for.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define MRP_HD __host__ __device__ __forceinline__
+#define MRP_D __device__ __forceinline__
+
+namespace mrp {
+
+// ---------------------------------------------------------------------------
+// exact float ops
+// ---------------------------------------------------------------------------
+MRP_D float fa(float a, float b) { return __fadd_rn(a, b); }
+MRP_D float fs(float a, float b) { return __fsub_rn(a, b); }
+MRP_D float fm(float a, float b) { return __fmul_rn(a, b); }
+MRP_D float fd(float a, float b) { return __fdiv_rn(a, b); }
+MRP_D float fsq(float a) { return __fsqrt_rn(a); }
+
+struct f3 { float x, y, z; };
+MRP_HD f3 mk3(float x, float y, float z) { return {x, y, z}; }
+MRP_D f3 add(f3 a, f3 b) { return {fa(a.x, b.x), fa(a.y, b.y), fa(a.z, b.z)}; }
+MRP_D f3 sub(f3 a, f3 b) { return {fs(a.x, b.x), fs(a.y, b.y), fs(a.z, b.z)}; }
+MRP_D f3 mul(f3 a, f3 b) { return {fm(a.x, b.x), fm(a.y, b.y), fm(a.z, b.z)}; }
+MRP_D f3 mul(f3 a, float b) { return {fm(a.x, b), fm(a.y, b), fm(a.z, b)}; }
+MRP_D f3 div(f3 a, float b) { return {fd(a.x, b), fd(a.y, b), fd(a.z, b)}; }
+MRP_D f3 adds(f3 a, float b) { return {fa(a.x, b), fa(a.y, b), fa(a.z, b)}; }
+MRP_D f3 subs(f3 a, float b) { return {fs(a.x, b), fs(a.y, b), fs(a.z, b)}; }
+MRP_D f3 neg(f3 a) { return {-a.x, -a.y, -a.z}; }
+// dot(a,b) = a.x*b.x + a.y*b.y + a.z*b.z, left to right (core/vector.cu:22)
+MRP_D float dot(f3 a, f3 b) { return fa(fa(fm(a.x, b.x), fm(a.y, b.y)), fm(a.z, b.z)); }
+MRP_D f3 normalize(f3 v) { float l = fsq(dot(v, v)); return {fd(v.x, l), fd(v.y, l), fd(v.z, l)}; }
+MRP_D f3 cross(f3 a, f3 b) {
+    return {fs(fm(a.y, b.z), fm(a.z, b.y)), fs(fm(a.z, b.x), fm(a.x, b.z)), fs(fm(a.x, b.y), fm(a.y, b.x))};
+}
+MRP_D float length(f3 a) { return fsq(dot(a, a)); }
+// lerp(a,b,v) = a*(1-v) + b*v (core/vector.cu:33)
+MRP_D float lerp(float a, float b, float v) { return fa(fm(a, fs(1.0f, v)), fm(b, v)); }
+MRP_D f3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+
+// inv / RayBoxOffset / RayBoxDistance (core/vector.cu:19, 46-80)
+MRP_D f3 inv(f3 a) {
+    return {a.x == 0 ? 999999999.0f : fd(1.0f, a.x), a.y == 0 ? 999999999.0f : fd(1.0f, a.y),
+            a.z == 0 ? 999999999.0f : fd(1.0f, a.z)};
+}
+MRP_D float ray_box_offset(f3 p, f3 dir) {
+    dir = inv(dir);
+    f3 to_axil = mul(neg(p), dir);
+    f3 face = mul(mk3(0.4999f, 0.4999f, 0.4999f), dir);
+    f3 d0 = add(to_axil, face), d1 = sub(to_axil, face);
+    float tmi = fmaxf(fminf(d0.x, d1.x), fmaxf(fminf(d0.y, d1.y), fminf(d0.z, d1.z)));
+    float tma = fminf(fmaxf(d0.x, d1.x), fminf(fmaxf(d0.y, d1.y), fmaxf(d0.z, d1.z)));
+    return tma >= tmi ? fmaxf(tmi, 0.0f) : -1.0f;
+}
+MRP_D float ray_box_distance(f3 p, f3 dir) {
+    dir = inv(dir);
+    f3 to_axil = mul(neg(p), dir);
+    f3 face = mul(mk3(0.5f, 0.5f, 0.5f), dir);
+    f3 d0 = add(to_axil, face), d1 = sub(to_axil, face);
+    return fminf(fmaxf(d0.x, d1.x), fminf(fmaxf(d0.y, d1.y), fmaxf(d0.z, d1.z)));
+}
+
+// HenyeyGreenstein (core/vector.cu:210-214): (1-g^2)/(1+g^2-2g cos)^1.5 / 4
+MRP_D float hg(float c, float g) {
+    float g2 = fm(g, g);
+    return fm(fd(fs(1.0f, g2), powf(fs(fa(1.0f, g2), fm(fm(2.0f, g), c)), 1.5f)), 0.25f);
+}
+// SampleHenyeyGreenstein (core/vector.cu:216-242)
+MRP_D f3 sample_hg(float e0, float e1, f3 v, float g) {
+    float cost;
+    if (fabsf(g) < 0.0001) {
+        cost = fs(fm(e0, 2.0f), 1.0f);
+    } else {
+        float g2 = fm(g, g);
+        float t0 = fd(fs(1.0f, g2), fa(fs(1.0f, g), fm(fm(2.0f, g), e0)));
+        cost = fd(fs(fa(1.0f, g2), fm(t0, t0)), fm(2.0f, g));
+    }
+    float phi = (float)(2.0 * 3.14159265359 * (double)e1);
+    float sint = fsq(fmaxf(0.0f, fs(1.0f, fm(cost, cost))));
+    f3 v2 = fabsf(v.z) > 0.70710678118654757 ? normalize(cross(v, mk3(0, 1, 0))) : normalize(cross(v, mk3(0, 0, 1)));
+    f3 v3 = cross(v2, v);
+    return add(add(mul(v3, fm(sint, cosf(phi))), mul(v2, fm(sint, sinf(phi)))), mul(v, cost));
+}
+// UniformSampleSphere (core/vector.cu:195-208)
+MRP_D f3 uniform_sphere(float ex, float ey) {
+    float phi = fm(fm(2.0f, 3.14159265359f), ex);
+    float cost = fs(1.0f, fm(2.0f, ey));
+    float sint = fsq(fs(1.0f, fm(cost, cost)));
+    return {fm(sint, cosf(phi)), fm(sint, sinf(phi)), cost};
+}
+
+// ---------------------------------------------------------------------------
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).  A stream is addressed
+// by (kind, id, sub, frame, seed); its n-th uniform is word n%4 of
+// Philox(counter = (n/4, sub, frame, kind), key = (id, seed ^ kind*0x9E3779B9)).
+// Uniforms are odd multiples of 2^-24, so never 0 and never 1.
+// ---------------------------------------------------------------------------
+MRP_HD void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+#ifdef __CUDA_ARCH__
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+MRP_HD float u01(uint32_t x) { return (float)(((x >> 9) << 1) | 1u) * 5.9604644775390625e-8f; }
+
+enum StreamKind : uint32_t { kPixelStream = 0, kLutStream = 1, kBakeStream = 2 };
+
+struct Stream {
+    uint32_t k0, k1, sub, frame, kind, n;
+    uint32_t blk[4];
+    MRP_D Stream(uint32_t kind_, uint32_t id, uint32_t sub_, uint32_t frame_, uint32_t seed)
+        : k0(id), k1(seed ^ (kind_ * 0x9E3779B9u)), sub(sub_), frame(frame_), kind(kind_), n(0) {}
+    MRP_D void restart() { n = 0; }
+    MRP_D float next() {
+        if ((n & 3) == 0) philox(n >> 2, sub, frame, kind, k0, k1, blk);
+        float r;
+        switch (n & 3) { case 0: r = u01(blk[0]); break; case 1: r = u01(blk[1]); break;
+                         case 2: r = u01(blk[2]); break; default: r = u01(blk[3]); }
+        ++n;
+        return r;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Software linear-filtered fetches with normalized coordinates, standing in
+// for tex3D/tex2D (see the oracle for the exact definition): texel coordinate
+// u*N - 0.5, fastest axis interpolated first, weights in fp32.
+// ---------------------------------------------------------------------------
+MRP_D float fetch_border(const float* __restrict__ g, int n, int x, int y, int z) {
+    if ((unsigned)x >= (unsigned)n || (unsigned)y >= (unsigned)n || (unsigned)z >= (unsigned)n) return 0.0f;
+    return __ldg(g + ((size_t)x * n + y) * n + z);
+}
+MRP_D float fetch_clamp(const float* __restrict__ g, int n, int x, int y, int z) {
+    x = min(max(x, 0), n - 1); y = min(max(y, 0), n - 1); z = min(max(z, 0), n - 1);
+    return __ldg(g + ((size_t)x * n + y) * n + z);
+}
+template <bool Clamp>
+MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
+    f3 uv = adds(pos, 0.5f);
+    float nf = (float)n;
+    float px = fs(fm(uv.x, nf), 0.5f), py = fs(fm(uv.y, nf), 0.5f), pz = fs(fm(uv.z, nf), 0.5f);
+    float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
+    int x = (int)flx, y = (int)fly, z = (int)flz;
+    float wx = fs(px, (float)x), wy = fs(py, (float)y), wz = fs(pz, (float)z);
+    auto F = [&](int a, int b, int c) { return Clamp ? fetch_clamp(g, n, a, b, c) : fetch_border(g, n, a, b, c); };
+    float c00 = lerp(F(x, y, z), F(x, y, z + 1), wz);
+    float c01 = lerp(F(x, y + 1, z), F(x, y + 1, z + 1), wz);
+    float c10 = lerp(F(x + 1, y, z), F(x + 1, y, z + 1), wz);
+    float c11 = lerp(F(x + 1, y + 1, z), F(x + 1, y + 1, z + 1), wz);
+    return lerp(lerp(c00, c01, wy), lerp(c10, c11, wy), wx);
+}
+constexpr int kLut = 512;
+MRP_D float tex_lut(const float* __restrict__ lut, float u, float v) {
+    float px = fs(fm(u, (float)kLut), 0.5f), py = fs(fm(v, (float)kLut), 0.5f);
+    int x = (int)floorf(px), y = (int)floorf(py);
+    float wx = fs(px, (float)x), wy = fs(py, (float)y);
+    int x0 = min(max(x, 0), kLut - 1), x1 = min(max(x + 1, 0), kLut - 1);
+    int y0 = min(max(y, 0), kLut - 1), y1 = min(max(y + 1, 0), kLut - 1);
+    float r0 = lerp(__ldg(lut + y0 * kLut + x0), __ldg(lut + y1 * kLut + x0), wy);
+    float r1 = lerp(__ldg(lut + y0 * kLut + x1), __ldg(lut + y1 * kLut + x1), wy);
+    return lerp(r0, r1, wx);
+}
+
+// ---------------------------------------------------------------------------
+// Device view of one volume's resources (passed by value to kernels).
+// ---------------------------------------------------------------------------
+struct VolumeDev {
+    const float* density;   // res^3, z fastest
+    int res;
+    float max_density;
+    const float* mips;      // 9 levels (256>>m)^3, concatenated (offsets: mip_offset)
+    const float* trs;       // 8 levels (128>>i)^3, concatenated (offsets: tr_offset)
+    const float* lut;       // 512x512 HG LUT
+    const float* baked;     // NEE transmittance grid
+    int baked_res;
+    const uint8_t* occ;     // 1 where a brick (or its trilinear apron) holds density != 0
+    int occ_shift;          // brick edge = 1 << occ_shift voxels
+    int occ_res;            // bricks per axis
+    f3 scatter_rate;
+    float tr_scale;
+    f3 sky;
+};
+
+MRP_HD size_t mip_offset(int m) { size_t o = 0; for (int i = 0; i < m; ++i) { size_t r = 256 >> i; o += r * r * r; } return o; }
+MRP_HD size_t tr_offset(int m) { size_t o = 0; for (int i = 0; i < m; ++i) { size_t r = 128 >> i; o += r * r * r; } return o; }
+constexpr size_t kMipFloats = 19173961;   // sum_{m<9} (256>>m)^3
+constexpr size_t kTrFloats = 2396745;     // sum_{i<8} (128>>i)^3
+
+// One camera launch (RenderCamera's arguments, core/volume.cu:199).
+struct ViewDev {
+    int width, height;
+    f3 ori, up, right, light_dir, light_color;
+    float alpha, g;
+    int multi_scatter, spp;
+    uint32_t seed;
+    int frame;         // RNG launch index ("randNum")
+    int mean_k;        // running-mean index of this launch ("frameNum")
+    float pass_rate;   // exp(-(2/res) * max_density * alpha), host libm (DeterminateEstimatedHit)
+};
+
+// ---------------------------------------------------------------------------
+// Packed MLP weight layout (fp32, one buffer).  Per SE block: the gate MLP
+// 8->8 (no bias) and 8->3 (no bias), then the three branch layers w->w with
+// biases in channel order density, TR, HG.  Then the three final 32->32
+// (main) or 8->8 (direct-illumination) layers, then the tail.  Names follow
+// core/NNWeight.cuh.
+// ---------------------------------------------------------------------------
+constexpr int kMainW[8] = {8, 8, 16, 16, 16, 32, 32, 32};
+constexpr int kMainFrom[8] = {0, 8, 16, 32, 48, 64, 96, 128};
+constexpr bool kMainWiden[8] = {false, true, false, false, true, false, false, false};
+constexpr int kDiFrom[4] = {160, 168, 176, 184};
+constexpr int block_size(int w) { return 64 + 24 + 3 * (w * w + w); }
+constexpr int main_block_off(int k) { int o = 0; for (int i = 0; i < k; ++i) o += block_size(kMainW[i]); return o; }
+constexpr int kMainFinalOff = main_block_off(8);
+constexpr int kDiOff = kMainFinalOff + 3 * (32 * 32 + 32);
+constexpr int di_block_off(int k) { return kDiOff + k * block_size(8); }
+constexpr int kDiFinalOff = di_block_off(4);
+constexpr int kTailOff = kDiFinalOff + 3 * (64 + 8);
+constexpr int kLGGSW = kTailOff, kLGGSB = kLGGSW + 24, kLSEFin1W = kLGGSB + 8, kLSEFin2W = kLSEFin1W + 1200;
+constexpr int kLC0W = kLSEFin2W + 96, kLC0B = kLC0W + 16384, kLC1W = kLC0B + 128, kLC1B = kLC1W + 8192;
+constexpr int kLC2W = kLC1B + 64, kLC2B = kLC2W + 2048, kLXW = kLC2B + 32, kLXB = kLXW + 512;
+constexpr int kLXk = kLXB + 16;   // LX0W, LX0B, ..., LX11W, LX11B (256 + 16 each)
+constexpr int lxw(int k) { return kLXk + k * 272; }
+constexpr int lxb(int k) { return kLXk + k * 272 + 256; }
+constexpr int kLX12W = kLXk + 12 * 272, kLX12B = kLX12W + 16;
+constexpr int kWeightCount = kLX12B + 1;
+static_assert(kWeightCount == 49673, "packed weight count must match core/NNWeight.cuh");
+
+}  // namespace mrp

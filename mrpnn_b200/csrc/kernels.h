@@ -1,0 +1,49 @@
+// kernels.h -- launch entry points of the MRPNN B200 kernels (host side).
+#pragma once
+#include "common.cuh"
+
+namespace mrp {
+
+// volume_kernels.cu
+cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
+                       cudaStream_t s);
+cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s);
+cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s);
+cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
+cudaError_t launch_tr_level(float* out, int res, const float* src, float alpha, const float L[3], int sms,
+                            cudaStream_t s);
+cudaError_t set_halton_permutations(const uint32_t perm[28]);
+cudaError_t launch_hg_lut(float* lut, float g, uint32_t seed, cudaStream_t s);
+cudaError_t launch_baked_tr(float* out, const VolumeDev& v, int bake_res, float alpha, const float L[3], uint32_t seed,
+                            int replicate, int sms, cudaStream_t s);
+
+// predictor_kernels.cu
+struct StencilTables {
+    float offset[192];
+    int layer[192];
+    float lut_v[192];
+    float dirs[160 * 3];
+};
+cudaError_t set_stencil_tables(const StencilTables& t);
+// features: [n][576] (X_Val, X_Val_Sub, X_Val_Hg), gamma [n]
+cudaError_t launch_gather(const VolumeDev& v, const float* pos, const float* bases, const float* light, float g,
+                          float alpha, int n, float* feat, float* gamma, cudaStream_t s);
+cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float* gamma, float g, const float sr[3],
+                            int n, float* out3, cudaStream_t s);
+cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* dir, float alpha, float pass_rate, int n,
+                             float* hit4, cudaStream_t s);
+// One launch of RenderCamera<true, MRPNN>: running mean into accum (float4
+// per pixel) with weight 1/(1+frame).
+cudaError_t launch_predict_fp32(const VolumeDev& v, const ViewDev& view, const float* weights, float4* accum,
+                                float* dbg_feat, float* dbg_hit, cudaStream_t s);
+
+// tracer_kernels.cu: one launch of RenderCamera<false> (spp samples per
+// pixel); FP64 sums of per-sample radiance and of its square per pixel.
+// first_pos[pix] must start at spp and counter at 0.
+cudaError_t launch_trace(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
+                         unsigned long long* counter, int sms, cudaStream_t s);
+cudaError_t launch_fill_int(int* p, int n, int value, cudaStream_t s);
+cudaError_t launch_trace_resolve(const double* sum3, const int* first_pos, int npix, int spp, int frame, float4* accum,
+                                 cudaStream_t s);
+
+}  // namespace mrp

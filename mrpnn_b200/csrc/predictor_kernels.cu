@@ -1,0 +1,472 @@
+// predictor_kernels.cu -- the MRPNN radiance predictor on the GPU, FP32 form.
+//
+// One launch renders one frame of RenderCamera<true, MRPNN>
+// (core/volume.cu:198-228 -> core/render.cuh:808-875):
+//   camera ray -> first estimated hit (DeterminateEstimatedHit) -> random
+//   bases (GetMatrixFromNormal) -> 192-point stencil gather of density, TR
+//   and HG features (SetupInputData) -> SE-gated MLP
+//   (RadiancePredictInternal) -> running mean.
+// Everything up to the features keeps the reference's float rounding order
+// (common.cuh), so hits and features match the CPU oracle to the bit except
+// where a transcendental's last bit differs.  The MLP here is the plain FP32
+// drop-in: one pixel per thread, weights broadcast from L1 (uniform loads).
+#include "kernels.h"
+
+namespace mrp {
+
+// Stencil tables (GetSamples23_ / SphereRandom3, core/vector.cu:82-405),
+// filled from the host: per sample offset, mip layer, and the HG-LUT row
+// coordinate v (depends only on the sample), plus the 160 unit directions of
+// the model file.
+__constant__ float c_offset[192];
+__constant__ int c_layer[192];
+__constant__ float c_lutv[192];
+__constant__ float c_dirs[160 * 3];
+
+cudaError_t set_stencil_tables(const StencilTables& t) {
+    cudaError_t e;
+    if ((e = cudaMemcpyToSymbol(c_offset, t.offset, sizeof t.offset)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_layer, t.layer, sizeof t.layer)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_lutv, t.lut_v, sizeof t.lut_v)) != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_dirs, t.dirs, sizeof t.dirs);
+}
+
+MRP_D float density(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
+MRP_D const float* mip_level(const VolumeDev& v, int m) { return v.mips + mip_offset(m); }
+MRP_D const float* tr_level(const VolumeDev& v, int m) { return v.trs + tr_offset(m); }
+
+// RenderCamera ray (core/volume.cu:208-216): jitter = first two draws of the
+// pixel stream.
+MRP_D f3 camera_ray(const ViewDev& w, int row, int col) {
+    Stream st(kPixelStream, (uint32_t)(row * w.width + col), 0, (uint32_t)w.frame, w.seed);
+    float r0 = st.next(), r1 = st.next();
+    float u = fs(1.0f, fd(fa((float)col, r0), (float)w.width));
+    float vv = fs(1.0f, fd(fa((float)row, r1), (float)w.height));
+    f3 fwd = normalize(neg(w.ori));
+    f3 d = add(add(fwd, mul(w.right, fs(fm(u, 2.0f), 1.0f))), mul(w.up, fs(fm(vv, 2.0f), 1.0f)));
+    return normalize(d);
+}
+
+// DeterminateEstimatedHit(float& alpha, ...) (core/render.cuh:105-197).
+// pass_rate = exp(-t_step * SMax) is computed once on the host.
+MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 pos, f3 dir, float dis, f3* next) {
+    float smax = fm(v.max_density, alpha);
+    float t = 0.0f, last_non_empty_t = 0.0f, prob = 1.0f, last_dens = 0.0f;
+    float rf = (float)v.res;
+    float t_step = fd(2.0f, rf), empty_step = fd(1.0f, rf);
+    int loop = 0;
+    while (loop++ < 10000) {
+        if (t > dis) {
+            if (last_non_empty_t != 0.0f) { t = last_non_empty_t; break; }
+            *next = mk3(0, 0, 0);
+            return false;
+        }
+        float d = density(v, add(pos, mul(dir, t)));
+        if (d > 0) {
+            float S = fm(d, alpha);
+            float step_p = fa(pass_rate, fm(fs(1.0f, pass_rate), fs(1.0f, fd(S, smax))));
+            float next_p = fm(prob, step_p);
+            if (next_p < 0.5f) {
+                float offset = fs(1.0f, fd(logf(fd(0.5f, prob)), logf(step_p)));
+                t = fs(t, fm(t_step, offset));
+                break;
+            }
+            prob = next_p;
+            t = fa(t, t_step);
+        } else {
+            if (last_dens > 0) {
+                float S = fm(last_dens, alpha);
+                float ts = fa(t_step, d);
+                // exp(-(ts*SMax)) == pass_rate when d == 0 (same argument)
+                float pr = d == 0.0f ? pass_rate : expf(-fm(ts, smax));
+                float step_p = fa(pr, fm(fs(1.0f, pr), fs(1.0f, fd(S, smax))));
+                float next_p = fm(prob, step_p);
+                if (next_p < 0.5f) {
+                    float offset = fs(1.0f, fd(logf(fd(0.5f, prob)), logf(step_p)));
+                    t = fs(t, fm(ts, offset));
+                    break;
+                }
+                prob = next_p;
+                last_non_empty_t = fa(t, d);
+            }
+            t = fa(t, fmaxf(fm(-d, 1.0f), empty_step));
+        }
+        last_dens = d;
+    }
+    *next = add(mul(dir, t), pos);
+    return true;
+}
+
+// GetSamplePoint (core/render.cuh:436-462)
+MRP_D bool first_hit(const VolumeDev& v, f3 ori, f3 dir, float alpha, float pass_rate, f3* hit) {
+    dir = normalize(dir);
+    *hit = mk3(0, 0, 0);
+    float dis = ray_box_offset(ori, dir);
+    if (dis < 0) return false;
+    f3 sp = add(ori, mul(dir, dis));
+    float md = ray_box_distance(sp, dir);
+    f3 p;
+    bool in = estimated_hit(v, alpha, pass_rate, sp, dir, md, &p);
+    if (in) *hit = p;
+    return in;
+}
+
+// GetMatrixFromNormal (core/render.cuh:694-708)
+MRP_D void basis(f3 v1, float spread, Stream& st, f3* b0, f3* b1, f3* b2) {
+    v1 = normalize(v1);
+    f3 v2 = mk3(0, 0, 0), v3 = mk3(0, 0, 0);
+    for (int guard = 0; guard < 1000; ++guard) {
+        float ex = fm(st.next(), spread);
+        float ey = fm(st.next(), spread);
+        f3 r = uniform_sphere(ex, ey);
+        if (fabsf(dot(r, v1)) < 0.00001) continue;
+        v2 = normalize(cross(v1, r));
+        v3 = cross(v2, v1);
+        break;
+    }
+    *b0 = v1; *b1 = v2; *b2 = v3;
+}
+
+// ShadowTerm_TRTex(...).x with unit light colour (core/renderResources.cu:254-272)
+MRP_D float shadow_tr(const VolumeDev& v, f3 p, f3 light, int mip) {
+    const float* g = tr_level(v, mip);
+    int n = 128 >> mip;
+    if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
+        float off = ray_box_offset(p, light);
+        if (off >= 0) return fm(1.0f, tex3<true>(g, n, add(p, mul(light, off))));
+        return 1.0f;
+    }
+    return fm(1.0f, tex3<true>(g, n, p));
+}
+
+// SetupInputData (core/radiancePredict.cu:427-485).  Writes feature i of
+// channel c to out[c * stride + i].
+MRP_D void gather(const VolumeDev& v, f3 pos, f3 X, f3 Y, f3 Z, f3 LX, f3 L, float g, float alpha, float* out,
+                  int stride, float* gamma) {
+    for (int i = 0; i < 192; ++i) {
+        float off = c_offset[i];
+        int layer = c_layer[i];
+        f3 cur;
+        if (i < 160) {
+            f3 p = mk3(c_dirs[3 * i], c_dirs[3 * i + 1], c_dirs[3 * i + 2]);
+            cur = add(pos, mul(add(add(mul(X, p.x), mul(Y, p.y)), mul(Z, p.z)), off));
+        } else {
+            cur = add(pos, mul(L, off));
+        }
+        float d = tex3<false>(mip_level(v, layer), 256 >> layer, cur);
+        out[i] = logf(fa(1.0f, fd(fm(alpha, d), 64.0f)));
+        float hv;
+        if (i == 0) {
+            hv = logf(fa(hg(dot(X, L), g), 1.0f));
+        } else {
+            f3 ms = normalize(sub(cur, pos));
+            float c1 = dot(X, ms), c2 = dot(LX, ms);
+            float u = fa(fm(c1, 0.5f), 0.5f), u2 = fa(fm(c2, 0.5f), 0.5f);
+            float lv = c_lutv[i];
+            hv = logf(fa(fm(tex_lut(v.lut, u, lv), tex_lut(v.lut, u2, lv)), 1.0f));
+        }
+        out[2 * stride + i] = hv;
+        out[stride + i] = shadow_tr(v, cur, LX, layer > 1 ? layer - 1 : 0);
+    }
+    float dd = fminf(1.0f, fmaxf(-1.0f, dot(X, LX)));
+    *gamma = acosf(dd);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 MLP, RadiancePredictInternal (core/radiancePredict.cu:301-422).
+// Blocks: in_c = X_c[slice]*gate_c + prev_c; out = relu(b + W in) (bias
+// first); then ADD3 (out += slice) or, for the widening blocks 1 and 4, REP3
+// (next residual = concat(out, slice)).  Weights: packed layout of common.cuh.
+// ---------------------------------------------------------------------------
+MRP_D float wld(const float* __restrict__ w, int i) { return __ldg(w + i); }
+
+MRP_D float sigmoid_ref(float o) { return (float)(1.0 / (1.0 + (double)expf(-o))); }
+
+template <int W, int FROM, bool WIDEN, bool HAS_PREV>
+MRP_D void mlp_block(const float* __restrict__ x, int stride, float g, float gamma, float* pool, int pid,
+                     float (&prev)[3][32], float (&nxt)[3][32], const float* __restrict__ wt) {
+    // SE gate: pool (avg, max) of each channel's slice, 8->8 relu, 8->3 sigmoid
+    float p8[8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float s = 0.0f, m = -10000.0f;
+#pragma unroll
+        for (int i = 0; i < W; ++i) { float xv = x[c * stride + FROM + i]; s += xv; m = fmaxf(m, xv); }
+        s = s / (float)W;
+        pool[pid + c] = s;
+        pool[36 + pid + c] = m;
+        p8[c] = s;
+        p8[3 + c] = m;
+    }
+    p8[6] = g;
+    p8[7] = gamma;
+    float h[8], gate[3];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], wld(wt, o * 8 + j), a);
+        h[o] = a >= 0.0f ? a : 0.0f;
+    }
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = fmaf(h[j], wld(wt, 64 + o * 8 + j), a);
+        gate[o] = sigmoid_ref(a);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float* wc = wt + 88 + c * (W * W + W);
+        float in[W];
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+            float t = x[c * stride + FROM + i] * gate[c];
+            in[i] = HAS_PREV ? t + prev[c][i] : t;
+        }
+#pragma unroll 4
+        for (int o = 0; o < W; ++o) {
+            float a = wld(wc, W * W + o);
+#pragma unroll
+            for (int j = 0; j < W; ++j) a = fmaf(in[j], wld(wc, o * W + j), a);
+            a = a >= 0.0f ? a : 0.0f;
+            if (WIDEN) nxt[c][o] = a;
+            else nxt[c][o] = a + x[c * stride + FROM + o];
+        }
+        if (WIDEN) {
+#pragma unroll
+            for (int i = 0; i < W; ++i) nxt[c][W + i] = x[c * stride + FROM + i];
+        }
+    }
+}
+
+template <int FROM, int TO>
+MRP_D void dense_relu(const float* in, float* out, const float* __restrict__ w, const float* __restrict__ b) {
+#pragma unroll 2
+    for (int o = 0; o < TO; ++o) {
+        float a = wld(b, o);
+#pragma unroll
+        for (int j = 0; j < FROM; ++j) a = fmaf(in[j], wld(w, o * FROM + j), a);
+        out[o] = a >= 0.0f ? a : 0.0f;
+    }
+}
+
+template <int K>
+MRP_D void copy_state(float (&dst)[3][32], const float (&src)[3][32]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int i = 0; i < K; ++i) dst[c][i] = src[c][i];
+}
+
+// x: features of one pixel, channel c at x[c * stride + i]
+MRP_D void mlp_fp32(const float* __restrict__ x, int stride, float gamma, float g, f3 sr, const float* __restrict__ wt,
+                    float out[3]) {
+    float pool[75];
+    pool[72] = g;
+    pool[73] = gamma;
+    float comb[120];
+    {
+        float a[3][32], b[3][32];
+        mlp_block<8, 0, false, false>(x, stride, g, gamma, pool, 0, a, b, wt + main_block_off(0));
+        copy_state<8>(a, b);
+        mlp_block<8, 8, true, true>(x, stride, g, gamma, pool, 3, a, b, wt + main_block_off(1));
+        copy_state<16>(a, b);
+        mlp_block<16, 16, false, true>(x, stride, g, gamma, pool, 6, a, b, wt + main_block_off(2));
+        copy_state<16>(a, b);
+        mlp_block<16, 32, false, true>(x, stride, g, gamma, pool, 9, a, b, wt + main_block_off(3));
+        copy_state<16>(a, b);
+        mlp_block<16, 48, true, true>(x, stride, g, gamma, pool, 12, a, b, wt + main_block_off(4));
+        copy_state<32>(a, b);
+        mlp_block<32, 64, false, true>(x, stride, g, gamma, pool, 15, a, b, wt + main_block_off(5));
+        copy_state<32>(a, b);
+        mlp_block<32, 96, false, true>(x, stride, g, gamma, pool, 18, a, b, wt + main_block_off(6));
+        copy_state<32>(a, b);
+        mlp_block<32, 128, false, true>(x, stride, g, gamma, pool, 21, a, b, wt + main_block_off(7));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float* wf = wt + kMainFinalOff + c * (1024 + 32);
+            dense_relu<32, 32>(b[c], comb + 32 * c, wf, wf + 1024);
+        }
+    }
+    {
+        float a[3][32], b[3][32];
+        mlp_block<8, 160, false, false>(x, stride, g, gamma, pool, 24, a, b, wt + di_block_off(0));
+        copy_state<8>(a, b);
+        mlp_block<8, 168, false, true>(x, stride, g, gamma, pool, 27, a, b, wt + di_block_off(1));
+        copy_state<8>(a, b);
+        mlp_block<8, 176, false, true>(x, stride, g, gamma, pool, 30, a, b, wt + di_block_off(2));
+        copy_state<8>(a, b);
+        mlp_block<8, 184, false, true>(x, stride, g, gamma, pool, 33, a, b, wt + di_block_off(3));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float* wf = wt + kDiFinalOff + c * (64 + 8);
+            dense_relu<8, 8>(b[c], comb + 96 + 8 * c, wf, wf + 64);
+        }
+    }
+    float srv[3] = {sr.x, sr.y, sr.z};
+    float srp[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) srp[c] = powf(srv[c], 4.0f);
+    float P[3];
+#pragma unroll 1
+    for (int ch = 0; ch < 3; ++ch) {
+        if (ch == 1 && srv[1] == srv[0]) { P[1] = P[0]; continue; }
+        if (ch == 2 && srv[2] == srv[0]) { P[2] = P[0]; continue; }
+        if (ch == 2 && srv[2] == srv[1]) { P[2] = P[1]; continue; }
+        pool[74] = srp[ch];
+        float xa[128], xb[128];
+#pragma unroll
+        for (int i = 0; i < 120; ++i) xa[i] = comb[i];
+        // LGGS 3->8: sum first, bias last (LinearReLU, :41-56)
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            float a = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) a = fmaf(pool[72 + j], wld(wt, kLGGSW + o * 3 + j), a);
+            a += wld(wt, kLGGSB + o);
+            xa[120 + o] = a >= 0.0f ? a : 0.0f;
+        }
+        float hf[16], gf[6];
+#pragma unroll 2
+        for (int o = 0; o < 16; ++o) {
+            float a = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 75; ++j) a = fmaf(pool[j], wld(wt, kLSEFin1W + o * 75 + j), a);
+            hf[o] = a >= 0.0f ? a : 0.0f;
+        }
+#pragma unroll
+        for (int o = 0; o < 6; ++o) {
+            float a = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) a = fmaf(hf[j], wld(wt, kLSEFin2W + o * 16 + j), a);
+            gf[o] = sigmoid_ref(a);
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) { xa[i] *= gf[0]; xa[32 + i] *= gf[1]; xa[64 + i] *= gf[2]; }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) { xa[96 + i] *= gf[3]; xa[104 + i] *= gf[4]; xa[112 + i] *= gf[5]; }
+        dense_relu<128, 128>(xa, xb, wt + kLC0W, wt + kLC0B);
+        dense_relu<128, 64>(xb, xa, wt + kLC1W, wt + kLC1B);
+        dense_relu<64, 32>(xa, xb, wt + kLC2W, wt + kLC2B);
+        dense_relu<32, 16>(xb, xa, wt + kLXW, wt + kLXB);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            float y[16], z[16];
+            dense_relu<16, 16>(xa, y, wt + lxw(2 * k), wt + lxb(2 * k));
+            dense_relu<16, 16>(y, z, wt + lxw(2 * k + 1), wt + lxb(2 * k + 1));
+#pragma unroll
+            for (int i = 0; i < 16; ++i) xa[i] += z[i];
+        }
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) a = fmaf(xa[j], wld(wt, kLX12W + j), a);
+        a += wld(wt, kLX12B);
+        P[ch] = a >= 0.0f ? a : 0.0f;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = fmaxf(expf(P[c]) - 1.0f, 0.0f) * srp[c];
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__global__ void k_first_hit(VolumeDev v, const float* __restrict__ ori, const float* __restrict__ dir, float alpha,
+                            float pass_rate, int n, float* __restrict__ hit4) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 h;
+    bool in = first_hit(v, ld3(ori + 3 * i), ld3(dir + 3 * i), alpha, pass_rate, &h);
+    hit4[4 * i] = h.x; hit4[4 * i + 1] = h.y; hit4[4 * i + 2] = h.z; hit4[4 * i + 3] = in ? 1.0f : 0.0f;
+}
+
+// bases: [n][15] = X, Y, Z (main basis), LX (light basis x), unused
+__global__ void k_gather(VolumeDev v, const float* __restrict__ pos, const float* __restrict__ bases,
+                         const float* __restrict__ light, float g, float alpha, int n, float* __restrict__ feat,
+                         float* __restrict__ gamma) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* b = bases + 12 * i;
+    gather(v, ld3(pos + 3 * i), ld3(b), ld3(b + 3), ld3(b + 6), ld3(b + 9), ld3(light), g, alpha, feat + (size_t)576 * i,
+           192, gamma + i);
+}
+
+__global__ void __launch_bounds__(128) k_mlp_fp32(const float* __restrict__ wt, const float* __restrict__ feat,
+                                                  const float* __restrict__ gamma, float g, f3 sr, int n,
+                                                  float* __restrict__ out3) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float o[3];
+    mlp_fp32(feat + (size_t)576 * i, 192, gamma[i], g, sr, wt, o);
+    out3[3 * i] = o[0]; out3[3 * i + 1] = o[1]; out3[3 * i + 2] = o[2];
+}
+
+// One launch of RenderCamera<true, MRPNN>; per-pixel thread.
+__global__ void __launch_bounds__(128) k_predict_fp32(VolumeDev v, ViewDev w, const float* __restrict__ wt,
+                                                      float4* __restrict__ accum, float* __restrict__ dbg_feat,
+                                                      float* __restrict__ dbg_hit) {
+    int pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= w.width * w.height) return;
+    int row = pix / w.width, col = pix % w.width;
+    f3 dir = normalize(camera_ray(w, row, col));        // NNPredict: dir = normalize(dir)
+    f3 L = normalize(w.light_dir);
+    Stream st(kPixelStream, (uint32_t)pix, 0, (uint32_t)w.frame, w.seed);   // InitRand again
+    f3 hit;
+    bool active = first_hit(v, w.ori, dir, w.alpha, w.pass_rate, &hit);
+    f3 X, Y, Z, LX, LY, LZ;
+    basis(dir, 0.1f, st, &X, &Y, &Z);
+    basis(L, 0.1f, st, &LX, &LY, &LZ);
+    float4 res;
+    if (active) {
+        float x[576], gamma;
+        gather(v, hit, X, Y, Z, LX, L, w.g, w.alpha, x, 192, &gamma);
+        if (dbg_feat) {
+            for (int i = 0; i < 576; ++i) dbg_feat[(size_t)pix * 576 + i] = x[i];
+        }
+        f3 sr = div(v.scatter_rate, 1.001f);
+        float o[3];
+        mlp_fp32(x, 192, gamma, w.g, sr, wt, o);
+        f3 pr = mul(mk3(o[0], o[1], o[2]), 1.0f);
+        f3 r = mul(mul(pr, w.light_color), v.scatter_rate);
+        res = make_float4(r.x, r.y, r.z, length(sub(w.ori, hit)));
+    } else {
+        res = make_float4(v.sky.x, v.sky.y, v.sky.z, -1.0f);
+    }
+    if (dbg_hit) {
+        dbg_hit[4 * pix] = hit.x; dbg_hit[4 * pix + 1] = hit.y; dbg_hit[4 * pix + 2] = hit.z;
+        dbg_hit[4 * pix + 3] = active ? 1.0f : 0.0f;
+    }
+    res.x = fmaxf(0.0f, res.x); res.y = fmaxf(0.0f, res.y); res.z = fmaxf(0.0f, res.z); res.w = fmaxf(0.0f, res.w);
+    // result = lerp(result, res, 1/(1+frameNum)) (core/volume.cu:226-227)
+    float rate = fd(1.0f, (float)(1 + w.mean_k));
+    float4 a = w.mean_k == 0 ? make_float4(0, 0, 0, 0) : accum[pix];
+    accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
+}
+
+cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* dir, float alpha, float pass_rate, int n,
+                             float* hit4, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_first_hit<<<(n + 127) / 128, 128, 0, s>>>(v, ori, dir, alpha, pass_rate, n, hit4);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather(const VolumeDev& v, const float* pos, const float* bases, const float* light, float g,
+                          float alpha, int n, float* feat, float* gamma, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_gather<<<(n + 127) / 128, 128, 0, s>>>(v, pos, bases, light, g, alpha, n, feat, gamma);
+    return cudaGetLastError();
+}
+cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float* gamma, float g, const float sr[3],
+                            int n, float* out3, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_mlp_fp32<<<(n + 127) / 128, 128, 0, s>>>(weights, feat, gamma, g, mk3(sr[0], sr[1], sr[2]), n, out3);
+    return cudaGetLastError();
+}
+cudaError_t launch_predict_fp32(const VolumeDev& v, const ViewDev& view, const float* weights, float4* accum,
+                                float* dbg_feat, float* dbg_hit, cudaStream_t s) {
+    int n = view.width * view.height;
+    if (n <= 0) return cudaSuccess;
+    k_predict_fp32<<<(n + 127) / 128, 128, 0, s>>>(v, view, weights, accum, dbg_feat, dbg_hit);
+    return cudaGetLastError();
+}
+
+}  // namespace mrp

@@ -1,0 +1,155 @@
+// tracer_kernels.cu -- the delta-tracking path tracer (PT render mode), the
+// ground-truth oracle of the renderer.
+//
+// Reference: RenderCamera<false> -> CalculateRadiance (core/volume.cu:198-228,
+// core/render.cuh:535-597), free flights by DeterminateNextVertex
+// (core/render.cuh:399-434) with NEE through the baked transmittance grid.
+//
+// B200 form: a persistent kernel pulls (pixel, sample) work items from a
+// global counter, so a lane whose path ended starts the next one instead of
+// idling until the longest path of its warp finishes (per-pixel threads
+// leave most lanes idle: path lengths range from 0 to 256 bounces).  Every
+// sample has its own Philox stream (sub = sample index), so results do not
+// depend on which lane ran it.  Per-sample radiance is computed in fp32 in
+// the reference's order and accumulated per pixel in FP64.
+#include "kernels.h"
+
+namespace mrp {
+
+MRP_D float density_t(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
+
+// DeterminateNextVertex.  SampleHenyeyGreenstein(Rand, Rand, ...) takes the
+// first draw as e1 and the second as e0 (x86-64 g++ argument order).
+MRP_D bool next_vertex(const VolumeDev& v, Stream& st, float alpha, float g, f3 pos, f3 dir, float dis, f3* npos,
+                       f3* ndir) {
+    float smax = fm(v.max_density, alpha);
+    float t = 0.0f;
+    int loop = 0;
+    while (loop++ < 10000) {
+        float rk = st.next();
+        t = fs(t, fd(logf(fs(1.0f, rk)), smax));
+        if (t > dis) { *npos = mk3(0, 0, 0); *ndir = mk3(0, 0, 0); return false; }
+        rk = st.next();
+        float d = density_t(v, add(pos, mul(dir, t)));
+        float S = fm(d, alpha);
+        if (fd(S, smax) > rk) break;
+        if (d < 0) t = fs(t, d);
+    }
+    float e1 = st.next();
+    float e0 = st.next();
+    *ndir = sample_hg(e0, e1, dir, g);
+    *npos = add(mul(dir, t), pos);
+    return true;
+}
+
+MRP_D f3 camera_ray_t(const ViewDev& w, int row, int col) {
+    Stream st(kPixelStream, (uint32_t)(row * w.width + col), 0, (uint32_t)w.frame, w.seed);
+    float r0 = st.next(), r1 = st.next();
+    float u = fs(1.0f, fd(fa((float)col, r0), (float)w.width));
+    float vv = fs(1.0f, fd(fa((float)row, r1), (float)w.height));
+    f3 fwd = normalize(neg(w.ori));
+    f3 d = add(add(fwd, mul(w.right, fs(fm(u, 2.0f), 1.0f))), mul(w.up, fs(fm(vv, 2.0f), 1.0f)));
+    return normalize(d);
+}
+
+// Radiance of sample k of one pixel (CalculateRadiance's loop body).
+MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 ori, f3 dir, float dis, f3 L) {
+    Stream st(kPixelStream, (uint32_t)pix, (uint32_t)k, (uint32_t)w.frame, w.seed);
+    f3 res = mk3(0, 0, 0);
+    f3 p = add(ori, mul(dir, dis)), rd = dir, csr = mk3(1, 1, 1);
+    for (int b = 0; b < w.multi_scatter; ++b) {
+        f3 np, nd;
+        float md = ray_box_distance(p, rd);
+        if (!next_vertex(v, st, w.alpha, w.g, p, rd, md, &np, &nd)) {
+            res = add(res, mul(v.sky, csr));
+            break;
+        }
+        p = np;
+        csr = mul(csr, v.scatter_rate);
+        float ph = hg(dot(rd, L), w.g);
+        float tr = tex3<true>(v.baked, v.baked_res, p);
+        res = add(res, mul(mul(w.light_color, csr), fm(tr, ph)));
+        rd = nd;
+    }
+    return res;
+}
+
+__global__ void __launch_bounds__(128) k_trace(VolumeDev v, ViewDev w, double* __restrict__ sum3,
+                                               double* __restrict__ sumsq3, int* __restrict__ first_pos,
+                                               unsigned long long* __restrict__ counter) {
+    const long long total = (long long)w.width * w.height * w.spp;
+    const int npix = w.width * w.height;
+    f3 L = normalize(w.light_dir);
+    for (;;) {
+        long long item;
+        // one atomic per warp, items handed out in warp-sized runs
+        unsigned lane = threadIdx.x & 31;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        item = (long long)base + lane;
+        if ((long long)base >= total) break;
+        if (item >= total) continue;
+        // sample-major order: consecutive lanes trace neighbouring pixels
+        int k = (int)(item / npix), pix = (int)(item % npix);
+        int row = pix / w.width, col = pix % w.width;
+        f3 dir = normalize(camera_ray_t(w, row, col));
+        float dis = ray_box_offset(w.ori, dir);
+        f3 r;
+        if (dis < 0) {
+            r = v.sky;   // SkyBox(dir), coverage stays 0
+        } else {
+            r = trace_sample(v, w, pix, k, w.ori, dir, dis, L);
+            if (r.x > 0 || r.y > 0 || r.z > 0) atomicMin(first_pos + pix, k);
+        }
+        atomicAdd(sum3 + 3 * pix, (double)r.x);
+        atomicAdd(sum3 + 3 * pix + 1, (double)r.y);
+        atomicAdd(sum3 + 3 * pix + 2, (double)r.z);
+        if (sumsq3) {
+            atomicAdd(sumsq3 + 3 * pix, (double)r.x * r.x);
+            atomicAdd(sumsq3 + 3 * pix + 1, (double)r.y * r.y);
+            atomicAdd(sumsq3 + 3 * pix + 2, (double)r.z * r.z);
+        }
+    }
+}
+
+// (mean radiance, coverage) of the launch, then the running mean over
+// launches (core/volume.cu:224-227).  Coverage: the reference counts samples
+// after which its running radiance sum is positive (core/render.cuh:594).
+__global__ void k_trace_resolve(const double* __restrict__ sum3, const int* __restrict__ first_pos, int npix, int spp,
+                                int frame, float4* __restrict__ accum) {
+    int pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= npix) return;
+    float4 res;
+    res.x = (float)(sum3[3 * pix] / spp);
+    res.y = (float)(sum3[3 * pix + 1] / spp);
+    res.z = (float)(sum3[3 * pix + 2] / spp);
+    int kf = first_pos[pix];
+    res.w = kf < spp ? fd((float)(spp - kf), (float)spp) : 0.0f;
+    res.x = fmaxf(0.0f, res.x); res.y = fmaxf(0.0f, res.y); res.z = fmaxf(0.0f, res.z);
+    float rate = fd(1.0f, (float)(1 + frame));
+    float4 a = frame == 0 ? make_float4(0, 0, 0, 0) : accum[pix];
+    accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
+}
+
+__global__ void k_fill_int(int* __restrict__ p, int n, int value) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = value;
+}
+cudaError_t launch_fill_int(int* p, int n, int value, cudaStream_t s) {
+    if (n > 0) k_fill_int<<<(n + 255) / 256, 256, 0, s>>>(p, n, value);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
+                         unsigned long long* counter, int sms, cudaStream_t s) {
+    k_trace<<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    return cudaGetLastError();
+}
+cudaError_t launch_trace_resolve(const double* sum3, const int* first_pos, int npix, int spp, int frame, float4* accum,
+                                 cudaStream_t s) {
+    k_trace_resolve<<<(npix + 255) / 256, 256, 0, s>>>(sum3, first_pos, npix, spp, frame, accum);
+    return cudaGetLastError();
+}
+
+}  // namespace mrp

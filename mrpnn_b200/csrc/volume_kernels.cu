@@ -1,0 +1,351 @@
+// volume_kernels.cu -- volume ingest and per-volume resources on the GPU:
+// synthetic fBm generation, the 9-level density pyramid, the majorant, the
+// empty-space occupancy bricks, the transmittance (TR) mips, the HG phase LUT
+// and the baked NEE transmittance grid.
+//
+// The reference builds the pyramid on the CPU (VolumeRender::Update,
+// core/volume.cu:1474-1515) and the TR mips / LUT / baked TR with legacy
+// texture + surface references (core/volume.cu:1322-1400, 1535-1696).  Here
+// every resource is a plain z-fastest fp32 array in HBM produced by one
+// kernel launch per level, on the volume's stream.
+#include "kernels.h"
+
+namespace mrp {
+
+// ---------------------------------------------------------------------------
+// fBm value noise (synthetic benchmark volumes; not part of the reference).
+// PCG-RXS-M-XS lattice hash (Jarzynski & Olano, JCGT 2020), quintic fade.
+// ---------------------------------------------------------------------------
+MRP_D uint32_t pcg(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+MRP_D float lattice(uint32_t seed, int ix, int iy, int iz) {
+    uint32_t h = pcg(pcg(pcg(pcg(seed) + (uint32_t)ix) + (uint32_t)iy) + (uint32_t)iz);
+    return fm((float)(h >> 8), 5.9604644775390625e-8f);
+}
+MRP_D float quintic(float f) { return fm(fm(fm(f, f), f), fa(fm(f, fs(fm(f, 6.0f), 15.0f)), 10.0f)); }
+MRP_D float value_noise(float px, float py, float pz, uint32_t seed) {
+    float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+    int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+    float wx = quintic(fs(px, fx)), wy = quintic(fs(py, fy)), wz = quintic(fs(pz, fz));
+    float c00 = lerp(lattice(seed, ix, iy, iz), lattice(seed, ix, iy, iz + 1), wz);
+    float c01 = lerp(lattice(seed, ix, iy + 1, iz), lattice(seed, ix, iy + 1, iz + 1), wz);
+    float c10 = lerp(lattice(seed, ix + 1, iy, iz), lattice(seed, ix + 1, iy, iz + 1), wz);
+    float c11 = lerp(lattice(seed, ix + 1, iy + 1, iz), lattice(seed, ix + 1, iy + 1, iz + 1), wz);
+    return lerp(lerp(c00, c01, wy), lerp(c10, c11, wy), wx);
+}
+MRP_D float fbm_voxel(int R, int x, int y, int z, uint32_t seed, float base_freq, int octaves, float gain) {
+    float Rf = (float)R;
+    float u = fd(fa((float)x, 0.5f), Rf), v = fd(fa((float)y, 0.5f), Rf), w = fd(fa((float)z, 0.5f), Rf);
+    float sum = 0, norm = 0, amp = 1.0f, freq = base_freq;
+    for (int o = 0; o < octaves; ++o) {
+        sum = fa(sum, fm(amp, value_noise(fm(u, freq), fm(v, freq), fm(w, freq), seed + (uint32_t)o * 1013u)));
+        norm = fa(norm, amp);
+        amp = fm(amp, gain);
+        freq = fm(freq, 2.0f);
+    }
+    float n = fd(sum, norm);
+    float dx = fs(u, 0.5f), dy = fs(v, 0.5f), dz = fs(w, 0.5f);
+    float d = fsq(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));
+    float t = fd(fs(d, 0.4f), fs(0.32f, 0.4f));
+    t = fminf(fmaxf(t, 0.0f), 1.0f);
+    float fall = fm(fm(t, t), fs(3.0f, fm(2.0f, t)));
+    return fminf(fmaxf(fm(n, fall), 0.0f), 1.0f);
+}
+__global__ void k_fbm(float* __restrict__ out, int R, uint32_t seed, float base_freq, int octaves, float gain) {
+    size_t n = (size_t)R * R * R;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int z = (int)(i % R), y = (int)((i / R) % R), x = (int)(i / ((size_t)R * R));
+        out[i] = fbm_voxel(R, x, y, z, seed, base_freq, octaves, gain);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pyramid level from a source grid: the reference's CPU trilinear Sample()
+// (border 0, negative values clamped, core/volume.cu:835-863) at texel
+// centres u = (i + 0.5) / res (ParallelFill, core/omp.cpp:11-13).
+// ---------------------------------------------------------------------------
+MRP_D float cpu_fetch(const float* __restrict__ d, int res, int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res) return 0.0f;
+    return fmaxf(0.0f, __ldg(d + ((size_t)x * res + y) * res + z));
+}
+__global__ void k_resample(float* __restrict__ out, int res, const float* __restrict__ src, int src_res) {
+    size_t n = (size_t)res * res * res;
+    float sr = (float)src_res;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int k = (int)(i % res), j = (int)((i / res) % res), q = (int)(i / ((size_t)res * res));
+        float u = (float)(((double)q + 0.5) / res), v = (float)(((double)j + 0.5) / res),
+              w = (float)(((double)k + 0.5) / res);
+        float px = fs(fm(u, sr), 0.5f), py = fs(fm(v, sr), 0.5f), pz = fs(fm(w, sr), 0.5f);
+        int x = (int)floorf(px), y = (int)floorf(py), z = (int)floorf(pz);
+        float wx = fs(px, (float)x), wy = fs(py, (float)y), wz = fs(pz, (float)z);
+        float a = lerp(lerp(cpu_fetch(src, src_res, x, y, z), cpu_fetch(src, src_res, x, y, z + 1), wz),
+                       lerp(cpu_fetch(src, src_res, x, y + 1, z), cpu_fetch(src, src_res, x, y + 1, z + 1), wz), wy);
+        float b = lerp(lerp(cpu_fetch(src, src_res, x + 1, y, z), cpu_fetch(src, src_res, x + 1, y, z + 1), wz),
+                       lerp(cpu_fetch(src, src_res, x + 1, y + 1, z), cpu_fetch(src, src_res, x + 1, y + 1, z + 1), wz), wy);
+        out[i] = lerp(a, b, wx);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// max density (the delta-tracking majorant), floored at the reference's
+// default 1e-5 (core/volume.hpp:104).  Densities are compared as int bits,
+// which orders non-negative floats; negative (SDF) values never win.
+// ---------------------------------------------------------------------------
+__global__ void k_max_density(const float* __restrict__ d, size_t n, int* __restrict__ out_bits) {
+    float m = 0.00001f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, __ldg(d + i));
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_int(m));
+}
+
+// ---------------------------------------------------------------------------
+// Occupancy bricks for exact empty-space skipping in the first-hit march.
+// Brick b covers voxels [b*B, b*B + B) per axis.  A trilinear fetch whose
+// base voxel lies in brick b reads voxels base..base+1, i.e. at most one
+// voxel past the brick, so the brick is marked occupied when any voxel in
+// [b*B - 1, b*B + B] holds a non-zero value.  A zero brick therefore
+// guarantees Density() == 0 exactly for every sample whose base voxel is in
+// it (border texels are 0 by addressing).
+// ---------------------------------------------------------------------------
+__global__ void k_occupancy(const float* __restrict__ d, int R, int shift, int nb, uint8_t* __restrict__ occ) {
+    int total = nb * nb * nb;
+    for (int b = blockIdx.x; b < total; b += gridDim.x) {
+        int bz = b % nb, by = (b / nb) % nb, bx = b / (nb * nb);
+        int B = 1 << shift;
+        int x0 = bx * B - 1, y0 = by * B - 1, z0 = bz * B - 1;
+        int span = B + 2;
+        int any = 0;
+        for (int t = threadIdx.x; t < span * span * span && !any; t += blockDim.x) {
+            int z = z0 + t % span, y = y0 + (t / span) % span, x = x0 + t / (span * span);
+            if ((unsigned)x < (unsigned)R && (unsigned)y < (unsigned)R && (unsigned)z < (unsigned)R)
+                any |= __ldg(d + ((size_t)x * R + y) * R + z) != 0.0f;
+        }
+        any = __syncthreads_or(any);
+        if (threadIdx.x == 0) occ[b] = any ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fill_TR (core/volume.cu:1535-1560): transmittance of TR level `level`
+// (res 128>>level) marched 128 steps toward the light through density level
+// level+1 with alpha scaled by 1.73^(level+1) (core/volume.cu:1636-1653).
+// ---------------------------------------------------------------------------
+__global__ void k_tr_level(float* __restrict__ out, int res, const float* __restrict__ src, float alpha, f3 L) {
+    size_t n = (size_t)res * res * res;
+    float rf = (float)res;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int z = (int)(i % res), y = (int)((i / res) % res), x = (int)(i / ((size_t)res * res));
+        f3 uv = div(adds(mk3((float)x, (float)y, (float)z), 0.5f), rf);
+        f3 ori = subs(uv, 0.5f);
+        float dis = ray_box_distance(ori, L);
+        float step = fd(dis, 128.0f);
+        f3 lp = ori;
+        float acc = 0;
+        for (int s = 0; s < 128; ++s) {
+            lp = add(lp, mul(L, step));
+            acc = fa(acc, tex3<false>(src, res, lp));
+        }
+        out[i] = fm(1.0f, fm(expf(fm(fm(-acc, alpha), step)), 1.0f));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fill_Hg (core/volume.cu:1322-1400): 512x512 LUT of the HG phase averaged
+// over a cone, 1024 scrambled-Halton samples per texel.  The digit
+// permutations come from the host (seeded Fisher-Yates), the per-texel shift
+// bn from the texel's LUT stream instead of a curand draw.
+// ---------------------------------------------------------------------------
+__constant__ uint32_t c_perm[28];
+__constant__ uint32_t c_primes[5] = {2, 3, 5, 7, 11};
+__constant__ uint32_t c_prime_sums[5] = {0, 2, 5, 10, 17};
+
+MRP_D float scrambled_radical_inverse(int bi, uint32_t a) {
+    const uint32_t base = c_primes[bi], off = c_prime_sums[bi];
+    const float inv_base = fd(1.0f, (float)base);
+    uint32_t rev = 0;
+    float inv_base_n = 1.0f;
+    while (a) {
+        uint32_t next = a / base;
+        uint32_t digit = a - next * base;
+        rev = rev * base + c_perm[off + digit];
+        inv_base_n = fm(inv_base_n, inv_base);
+        a = next;
+    }
+    return fminf(fm(inv_base_n, fa((float)rev, fd(fm(inv_base, (float)c_perm[off]), fs(1.0f, inv_base)))), 0.99999994f);
+}
+MRP_D float fracf_(float f) { return fs(f, (float)(long)f); }
+
+__global__ void k_hg_lut(float* __restrict__ lut, float g, uint32_t seed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= kLut || j >= kLut) return;
+    float costheta = (float)((((double)(float)i + 0.5) / kLut) * 2.0 - 1.0);
+    float aa = (float)(((double)(float)j + 0.5) / kLut);
+    float angle = (float)((double)aa * 3.1415926535 * 60.0 / 180.0);
+    Stream st(kLutStream, (uint32_t)(j * kLut + i), 0, 0, seed);
+    float bn = st.next();
+    float h = 0.0f;
+    float radius = tanf(angle);
+    f3 view = mk3(1.0f, 0.0f, 0.0f);
+    f3 dir = mk3(costheta, fsq(fs(1.0f, fm(costheta, costheta))), 0.0f);
+    float mis = 0;
+    {
+        float p = fa(fs(fm(radius, radius), 1.0f), fm(dir.x, dir.x));
+        if (p > 0) {
+            float sdotl = g > 0 ? dir.x : -dir.x;
+            float w = fsq(p);
+            float d0 = fd(fmaxf(0.0f, fs(sdotl, w)), radius);
+            float d1 = fd(fa(sdotl, w), radius);
+            float d = fs(fm(fm(d1, d1), d1), fm(fm(d0, d0), d0));
+            mis = fm((float)(d1 > d0), d);
+        }
+        mis = fminf(fmaxf(mis, 1e-8f), 1.0f);
+        float a = fabsf(g);
+        double ad = a;
+        a = (float)(ad < 0.6 ? 0.0 : (ad < 0.7 ? (ad - 0.6) * 9 : (pow((ad - 0.7) / 0.3, 0.05) * 0.1 + 0.9)));
+        mis = fs(1.0f, fd(1.0f, fa(1.0f, fd(fm(a, mis), fs(1.0f, a)))));
+    }
+    for (uint32_t k = 0; k < 1024; ++k) {
+        if (fracf_(fa(scrambled_radical_inverse(4, k), bn)) < mis) {
+            float rx = fracf_(fa(scrambled_radical_inverse(0, k), bn));
+            float ry = fracf_(fa(scrambled_radical_inverse(1, k), bn));
+            f3 l = sample_hg(rx, ry, view, g);
+            float sdotl = dot(dir, l);
+            float p = fa(fs(fm(radius, radius), 1.0f), fm(sdotl, sdotl));
+            if (p <= 0) continue;
+            float w = fsq(p);
+            float d0 = fs(sdotl, w);
+            float d1 = fd(fa(sdotl, w), radius);
+            d0 = fd(fmaxf(0.0f, d0), radius);
+            float d = fs(fm(fm(d1, d1), d1), fm(fm(d0, d0), d0));
+            h = fa(h, fmaxf(0.0f, fd(d, 4.0f)));
+        } else {
+            float rx = fracf_(fa(scrambled_radical_inverse(0, k), bn));
+            float ry = fracf_(fa(scrambled_radical_inverse(1, k), bn));
+            float rz = fracf_(fa(scrambled_radical_inverse(2, k), bn));
+            float theta = (float)((double)rx * 2.0 * 3.1415926535);
+            float phi = (float)acos(2.0 * (double)ry - 1.0);
+            float r = powf(rz, fd(1.0f, 3.0f));
+            float st_ = sinf(theta), ct = cosf(theta), sp = sinf(phi), cp = cosf(phi);
+            float x = fm(fm(fm(radius, r), sp), ct), y = fm(fm(fm(radius, r), sp), st_), z = fm(fm(radius, r), cp);
+            f3 rp = add(mk3(x, y, z), dir);
+            float c = dot(normalize(rp), view);
+            h = fa(h, hg(c, g));
+        }
+    }
+    lut[j * kLut + i] = fd(h, 1024.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Tr (core/render.cuh:60-103): ratio tracking while tr > 0.5, then delta
+// tracking with termination until tr <= 0.001, through Density().
+// ---------------------------------------------------------------------------
+MRP_D float density(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
+
+MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float dis, float alpha) {
+    float smax = fm(v.max_density, alpha);
+    float tr = 1.0f, t = 0.0f;
+    int loop = 0;
+    while (loop++ < 10000 && tr > 0.5) {
+        float rk = st.next();
+        t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
+        if (t > dis) break;
+        float d = density(v, add(pos, mul(dir, t)));
+        float S = fm(d, alpha);
+        tr = fm(tr, fs(1.0f, fmaxf(0.0f, fd(S, smax))));
+        if (d < 0) t = fs(t, d);
+    }
+    while (loop++ < 10000 && tr > 0.001) {
+        float rk = st.next();
+        t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
+        if (t > dis) break;
+        float d = density(v, add(pos, mul(dir, t)));
+        float S = fm(d, alpha);
+        if (st.next() < fmaxf(0.0f, fd(S, smax))) { tr = 0.0f; break; }
+        if (d < 0) t = fs(t, d);
+    }
+    return tr;
+}
+
+// Fill_BakeTR (core/volume.cu:1562-1587) over voxels [first, first+count).
+// replicate != 0 restarts the voxel's stream for every estimate, as InitRand
+// inside the reference's loop does (the estimates are then identical).
+__global__ void k_baked_tr(float* __restrict__ out, VolumeDev v, int bake_res, float alpha, f3 L, uint32_t seed,
+                           int replicate, int64_t first, int64_t count) {
+    float rf = (float)bake_res;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x) {
+        int64_t vi = first + q;
+        int x = (int)(vi / ((int64_t)bake_res * bake_res)), y = (int)((vi / bake_res) % bake_res), z = (int)(vi % bake_res);
+        f3 uv = div(adds(mk3((float)x, (float)y, (float)z), 0.5f), rf);
+        f3 p = subs(uv, 0.5f);
+        int cnt = density(v, p) > 0 ? 5 : 2;
+        float acc = 0.0f;
+        uint32_t hi = (uint32_t)(vi >> 32) * 8u;
+        for (int i = 0; i < cnt; ++i) {
+            Stream st(kBakeStream, (uint32_t)vi, replicate ? hi : hi + (uint32_t)i, 0, seed);
+            float md = ray_box_distance(p, L);
+            acc = fa(acc, transmittance(v, st, p, L, md, alpha));
+        }
+        out[vi] = fm(1.0f, fd(acc, (float)cnt));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int grid_for(size_t n, int block, int sms) {
+    size_t g = (n + block - 1) / block;
+    size_t cap = (size_t)sms * 32;
+    return (int)(g < cap ? (g ? g : 1) : cap);
+}
+
+cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
+                       cudaStream_t s) {
+    k_fbm<<<grid_for((size_t)R * R * R, 256, sms), 256, 0, s>>>(out, R, seed, base_freq, octaves, gain);
+    return cudaGetLastError();
+}
+cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s) {
+    k_resample<<<grid_for((size_t)res * res * res, 256, sms), 256, 0, s>>>(out, res, src, src_res);
+    return cudaGetLastError();
+}
+cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s) {
+    k_max_density<<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
+    return cudaGetLastError();
+}
+cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s) {
+    int total = nb * nb * nb;
+    k_occupancy<<<total < sms * 16 ? total : sms * 16, 256, 0, s>>>(d, R, shift, nb, occ);
+    return cudaGetLastError();
+}
+cudaError_t launch_tr_level(float* out, int res, const float* src, float alpha, const float L[3], int sms,
+                            cudaStream_t s) {
+    k_tr_level<<<grid_for((size_t)res * res * res, 128, sms), 128, 0, s>>>(out, res, src, alpha, mk3(L[0], L[1], L[2]));
+    return cudaGetLastError();
+}
+cudaError_t set_halton_permutations(const uint32_t perm[28]) {
+    return cudaMemcpyToSymbol(c_perm, perm, sizeof(uint32_t) * 28);
+}
+cudaError_t launch_hg_lut(float* lut, float g, uint32_t seed, cudaStream_t s) {
+    k_hg_lut<<<dim3(kLut / 16, kLut / 16), dim3(16, 16), 0, s>>>(lut, g, seed);
+    return cudaGetLastError();
+}
+cudaError_t launch_baked_tr(float* out, const VolumeDev& v, int bake_res, float alpha, const float L[3], uint32_t seed,
+                            int replicate, int sms, cudaStream_t s) {
+    int64_t total = (int64_t)bake_res * bake_res * bake_res;
+    // bounded chunks keep every launch short
+    const int64_t chunk = (int64_t)1 << 26;
+    for (int64_t first = 0; first < total; first += chunk) {
+        int64_t cnt = total - first < chunk ? total - first : chunk;
+        k_baked_tr<<<grid_for((size_t)cnt, 128, sms), 128, 0, s>>>(out, v, bake_res, alpha, mk3(L[0], L[1], L[2]),
+                                                                   seed, replicate, first, cnt);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace mrp

@@ -1,0 +1,193 @@
+"""Generate tests/golden/ref_pins.npz from the reference's own render code.
+
+The reference's core/vector.cu, core/radiancePredict.cu,
+core/renderResources.cu and core/render.cuh are compiled on the CPU by
+oracle/Makefile ("make -C oracle ref", shims in oracle/ref/shim) into
+oracle/_ref/libmrpnn_ref.so.  This script feeds it seeded inputs and stores
+inputs and outputs, so tests can pin the oracle (oracle/mrpnn_oracle.cpp) to
+the reference without the reference tree being present.
+
+Scene-based cases use a small synthetic scene rebuilt identically by the test
+(fBm 32^3, pyramid, TR mips, the HG-LUT rows the gather reads); checksums of
+those scene arrays are stored too.
+
+Usage: python tests/golden/make_golden.py   (needs /root/reference)
+"""
+import ctypes as C
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import oracle as O  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_pins.npz")
+
+SCENE = dict(R=32, seed=0, freq=4.0, alpha=64.0, g=0.857, lut_seed=7, light=(0.3, 0.8, 0.5),
+             sr=(0.99, 0.99, 0.99), sky=(0.05, 0.05, 0.05))
+
+
+def light_dir():
+    L = np.asarray(SCENE["light"], np.float32)
+    return (L / np.float32(np.sqrt(np.float32(np.dot(L, L))))).astype(np.float32)
+
+
+def build_scene():
+    """The synthetic scene used by the scene-based pins (oracle-built)."""
+    R = SCENE["R"]
+    vol = O.fbm_volume(R, SCENE["seed"], SCENE["freq"])
+    md = O.lib().orc_max_density(vol, vol.size)
+    mips = O.build_pyramid(vol, R)
+    L = light_dir()
+    tr = O.tr_mips(mips, SCENE["alpha"], L)
+    _, tex = O.lut_rows_needed()
+    lut = np.zeros(512 * 512, np.float32)
+    lut[tex] = O.hg_lut_texels(SCENE["g"], SCENE["lut_seed"], tex)
+    baked = tr[:128 ** 3].copy()   # any clamp-sampled grid serves as the NEE table here
+    sc = O.SceneBuf(vol, R, md, mips, tr, lut, baked=baked, baked_res=128, scatter_rate=SCENE["sr"],
+                    sky=SCENE["sky"])
+    return sc
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def camera(W):
+    ori = np.array([0.75, 0.75, 0.75], np.float32)
+    fwd = -ori / np.float32(np.sqrt(np.float32(np.dot(ori, ori))))
+    right = np.cross([0, 1, 0], fwd).astype(np.float32)
+    right /= np.float32(np.sqrt(np.float32(np.dot(right, right))))
+    up = np.cross(fwd, right).astype(np.float32)
+    t = np.float32(np.tan(np.deg2rad(22.5)))
+    return ori, (up * t).astype(np.float32), (right * t).astype(np.float32)
+
+
+def main():
+    R = O.ref()
+    rng = np.random.default_rng(20261203)
+    out = {}
+
+    # -- MLP (RadiancePredictInternal) on random features ---------------------
+    n = 64
+    feat = rng.uniform(0.0, 1.5, (n, 576)).astype(np.float32)
+    gam = rng.uniform(0.0, np.pi, n).astype(np.float32)
+    out["mlp_feat"], out["mlp_gamma"] = feat, gam
+    for tag, sr in (("grey", (1.0, 1.0, 1.0)), ("rgb", (0.99, 0.9, 0.8))):
+        out[f"mlp_out_{tag}"] = O.ref_mlp(feat, gam, 0.857, sr)
+        out[f"mlp_sr_{tag}"] = np.asarray(sr, np.float32)
+
+    # -- stencil tables (GetSamples23_, SphereRandom3) ------------------------
+    offs, layers, types, lidx, dirs = [], [], [], [], []
+    for i in range(192):
+        o, l, t, li = C.c_float(), C.c_float(), C.c_int(), C.c_int()
+        d = np.zeros(3, np.float32)
+        R.ref_stencil(i, C.byref(o), C.byref(l), C.byref(t), C.byref(li), d)
+        offs.append(o.value); layers.append(l.value); types.append(t.value); lidx.append(li.value); dirs.append(d)
+    out["st_offset"] = np.asarray(offs, np.float32)
+    out["st_layer"] = np.asarray(layers, np.float32)
+    out["st_type"] = np.asarray(types, np.int32)
+    out["st_localindex"] = np.asarray(lidx, np.int32)
+    out["st_dirs"] = np.asarray(dirs, np.float32)
+
+    # -- maths -------------------------------------------------------------------
+    m = 512
+    hc = rng.uniform(-1, 1, m).astype(np.float32)
+    hgv = rng.uniform(-0.95, 0.95, m).astype(np.float32)
+    out["hg_in"] = np.stack([hc, hgv], 1)
+    out["hg_out"] = np.array([R.ref_hg(c, g) for c, g in zip(hc, hgv)], np.float32)
+    e = rng.uniform(0, 1, (m, 2)).astype(np.float32)
+    vv = rng.normal(size=(m, 3)).astype(np.float32)
+    vv /= np.linalg.norm(vv, axis=1, keepdims=True).astype(np.float32)
+    out["shg_e"], out["shg_v"], out["shg_g"] = e, vv, hgv
+    res = np.zeros((m, 3), np.float32)
+    for i in range(m):
+        o3 = np.zeros(3, np.float32)
+        R.ref_sample_hg(e[i, 0], e[i, 1], np.ascontiguousarray(vv[i]), hgv[i], o3)
+        res[i] = o3
+    out["shg_out"] = res
+    p = rng.uniform(-1.2, 1.2, (m, 3)).astype(np.float32)
+    d = rng.normal(size=(m, 3)).astype(np.float32)
+    d[rng.uniform(size=m) < 0.1, rng.integers(0, 3)] = 0.0
+    out["rb_p"], out["rb_d"] = p, d
+    out["rb_off"] = np.array([R.ref_ray_box_offset(p[i], d[i]) for i in range(m)], np.float32)
+    out["rb_dist"] = np.array([R.ref_ray_box_distance(p[i], d[i]) for i in range(m)], np.float32)
+
+    # -- scene-based pins ----------------------------------------------------------
+    sc = build_scene()
+    sc.bind_ref()
+    out["scene_digest_mips"] = np.array(digest(sc.mips))
+    out["scene_digest_tr"] = np.array(digest(sc.tr))
+    out["scene_digest_lut"] = np.array(digest(sc.lut))
+    L = light_dir()
+    # first hit
+    k = 256
+    oris = (np.array([0.75, 0.75, 0.75]) + rng.normal(0, 0.05, (k, 3))).astype(np.float32)
+    dirs_ = (-oris + rng.normal(0, 0.2, (k, 3))).astype(np.float32)
+    hits = np.zeros((k, 4), np.float32)
+    for i in range(k):
+        h = np.zeros(3, np.float32)
+        a = R.ref_first_hit(oris[i], dirs_[i], SCENE["alpha"], h)
+        hits[i, :3], hits[i, 3] = h, a
+    out["fh_ori"], out["fh_dir"], out["fh_out"] = oris, dirs_, hits
+    # basis (GetMatrixFromNormal)
+    k = 64
+    bv = rng.normal(size=(k, 3)).astype(np.float32)
+    bo = np.zeros((k, 9), np.float32)
+    for i in range(k):
+        o9 = np.zeros(9, np.float32)
+        R.ref_basis(bv[i], 0.1, i, 0, 3, 11, 0, o9)
+        bo[i] = o9
+    out["basis_v"], out["basis_out"] = bv, bo
+    # SetupInputData
+    k = 32
+    pos = rng.uniform(-0.45, 0.45, (k, 3)).astype(np.float32)
+    bases = np.zeros((k, 12), np.float32)
+    feats = np.zeros((k, 576), np.float32)
+    gams = np.zeros(k, np.float32)
+    for i in range(k):
+        m9 = np.zeros(9, np.float32)
+        l9 = np.zeros(9, np.float32)
+        R.ref_basis(rng.normal(size=3).astype(np.float32), 0.1, i, 0, 0, 0, 0, m9)
+        R.ref_basis(L, 0.1, i, 1, 0, 0, 0, l9)
+        bases[i, :9], bases[i, 9:] = m9, l9[:3]
+        f = np.zeros(576, np.float32)
+        gm = np.zeros(1, np.float32)
+        R.ref_setup_input(1, pos[i], m9[:3], m9[3:6], m9[6:], l9[:3], L, SCENE["g"], SCENE["alpha"], f, gm)
+        feats[i], gams[i] = f, gm[0]
+    out["si_pos"], out["si_bases"], out["si_feat"], out["si_gamma"] = pos, bases, feats, gams
+    # full predictor pixels (RenderCamera<true, MRPNN> ray + NNPredict<MRPNN>)
+    W = 16
+    ori, up, right = camera(W)
+    px = np.arange(W * W, dtype=np.int32)
+    rgba = np.zeros((W * W, 4), np.float32)
+    R.ref_predict_pixels(W, W, ori, up, right, L, np.ones(3, np.float32), SCENE["alpha"], SCENE["g"], 5, 2, px,
+                         W * W, rgba)
+    out["pp_rgba"] = rgba
+    # tracer samples (CalculateRadiance, one sample per call)
+    cases = [(int(p_), int(k_)) for p_, k_ in zip(rng.integers(0, W * W, 48), rng.integers(0, 8, 48))]
+    tr_out = np.zeros((len(cases), 4), np.float32)
+    for i, (p_, k_) in enumerate(cases):
+        o4 = np.zeros(4, np.float32)
+        R.ref_trace_sample(W, W, ori, up, right, L, np.ones(3, np.float32), SCENE["alpha"], SCENE["g"], 64, 5, 2,
+                           p_, k_, o4)
+        tr_out[i] = o4
+    out["ts_cases"], out["ts_out"] = np.asarray(cases, np.int32), tr_out
+    # Tr (ratio + delta tracking)
+    k = 64
+    tp = rng.uniform(-0.45, 0.45, (k, 3)).astype(np.float32)
+    tv = np.zeros(k, np.float32)
+    for i in range(k):
+        dis = R.ref_ray_box_distance(tp[i], L)
+        tv[i] = R.ref_tr(tp[i], L, dis, SCENE["alpha"], i, 0, 0, 9, 2)
+    out["tr_pos"], out["tr_out"] = tp, tv
+
+    np.savez_compressed(OUT, **out)
+    print(OUT, os.path.getsize(OUT), "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,80 @@
+"""The C ABI without a GPU: the library loads, exports every symbol that
+include/mrpnn.h declares, and refuses to run (no CPU fallback)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(mrp_[a-z0-9_]+)\s*\(", text))
+    return names - {"mrp_fill_fn"}
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert {"mrp_init", "mrp_volume_create", "mrp_volume_update", "mrp_render", "mrp_predict_features"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    import mrpnn_b200
+    L = mrpnn_b200.lib()
+    missing = [n for n in sorted(declared_symbols()) if not hasattr(L, n)]
+    assert not missing, missing
+    from mrpnn_b200 import api
+    assert set(api._SIGS) == declared_symbols()
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="a GPU is present")
+def test_fails_loudly_without_gpu():
+    import mrpnn_b200
+    from mrpnn_b200 import api
+    with pytest.raises(mrpnn_b200.MrpError) as e:
+        mrpnn_b200.init()
+    assert e.value.status == api.ERR_NO_DEVICE
+    with pytest.raises(mrpnn_b200.MrpError):
+        mrpnn_b200.predict_features(np.zeros((1, 576), np.float32), np.zeros(1, np.float32), 0.5, (1, 1, 1))
+
+
+def test_default_params():
+    import mrpnn_b200
+    p = mrpnn_b200.default_params()
+    assert list(p.scatter_rate) == pytest.approx([1.001] * 3)
+    assert p.bake_res == 768 and p.tr_scale == 1.0 and p.precision == 0
+
+
+def test_model_file_layout():
+    """The packed model file holds the 146 reference tensors plus the stencil."""
+    import struct
+    path = os.path.join(ROOT, "mrpnn_b200", "data", "mrpnn_model.bin")
+    with open(path, "rb") as f:
+        assert f.read(8) == b"MRPNNMD1"
+        n = struct.unpack("<I", f.read(4))[0]
+        total = 0
+        names = []
+        for _ in range(n):
+            ln = struct.unpack("<H", f.read(2))[0]
+            names.append(f.read(ln).decode())
+            c = struct.unpack("<I", f.read(4))[0]
+            f.seek(4 * c, 1)
+            total += c if names[-1] != "STENCIL_DIRS" else 0
+    assert n == 147 and "STENCIL_DIRS" in names
+    assert total == 49673

@@ -1,0 +1,133 @@
+"""The MRPNN predictor on the GPU against the CPU oracle (itself pinned to
+the reference's own code by tests/test_oracle_pins.py).
+
+Tolerances: first-hit decisions are exact (only +,-,*,/ and comparisons);
+hit positions, features and the MLP differ only through the last bit of
+log/exp/pow/atan/acos, so features agree to 1e-5 relative and the FP32 MLP
+to the 1e-4 relative bound of the drop-in contract."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.gpu_scene import LIGHT, Scene, view_frame
+
+pytestmark = pytest.mark.gpu
+
+MLP_RTOL = 1e-4      # FP32 predictor vs the reference predictor, relative
+MLP_ATOL = 1e-6      # floor for outputs at 0 (relu / exp(x)-1 near 0)
+
+
+@pytest.fixture(scope="module")
+def scene():
+    return Scene(R=64)
+
+
+def test_mlp_fp32_matches_reference_golden(golden):
+    """GPU FP32 MLP vs RadiancePredictInternal compiled from the reference."""
+    import mrpnn_b200 as M
+    M.init()
+    for tag in ("grey", "rgb"):
+        out = M.predict_features(golden["mlp_feat"], golden["mlp_gamma"], 0.857, golden[f"mlp_sr_{tag}"])
+        ref = golden[f"mlp_out_{tag}"]
+        np.testing.assert_allclose(out, ref, rtol=MLP_RTOL, atol=MLP_ATOL)
+
+
+def test_mlp_fp32_random_features():
+    import mrpnn_b200 as M
+    M.init()
+    rng = np.random.default_rng(11)
+    n = 1000
+    feat = np.concatenate([rng.uniform(0, 1.5, (n, 192)), rng.uniform(0, 1, (n, 192)),
+                           rng.uniform(0, 3, (n, 192))], 1).astype(np.float32)
+    gam = rng.uniform(0, np.pi, n).astype(np.float32)
+    for sr in ((1.0, 1.0, 1.0), (0.99, 0.9, 0.8), (0.9, 0.9, 0.7)):
+        out = M.predict_features(feat, gam, 0.857, sr)
+        ref = O.mlp_f32(feat, gam, 0.857, sr)
+        np.testing.assert_allclose(out, ref, rtol=MLP_RTOL, atol=MLP_ATOL)
+
+
+def test_mlp_fp32_device_buffers():
+    import torch
+    import mrpnn_b200 as M
+    M.init()
+    rng = np.random.default_rng(12)
+    feat = rng.uniform(0, 1.5, (300, 576)).astype(np.float32)
+    gam = rng.uniform(0, 3, 300).astype(np.float32)
+    out = M.predict_features(torch.from_numpy(feat).cuda(), torch.from_numpy(gam).cuda(), 0.5, (1, 1, 1))
+    ref = O.mlp_f32(feat, gam, 0.5, (1, 1, 1))
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=MLP_RTOL, atol=MLP_ATOL)
+
+
+def test_first_hit(scene):
+    rng = np.random.default_rng(1)
+    n = 4096
+    ori = (np.array([0.75, 0.75, 0.75]) + rng.normal(0, 0.05, (n, 3))).astype(np.float32)
+    d = (-ori + rng.normal(0, 0.25, (n, 3))).astype(np.float32)
+    got = scene.vol.first_hit(ori, d, scene.alpha)
+    L = O.lib()
+    ref = np.zeros((n, 4), np.float32)
+    h = np.zeros(3, np.float32)
+    for i in range(n):
+        ref[i, 3] = L.orc_first_hit(C.byref(scene.orc.c), ori[i], d[i], scene.alpha, h)
+        ref[i, :3] = h
+    np.testing.assert_array_equal(got[:, 3], ref[:, 3])
+    assert ref[:, 3].sum() > n // 4
+    np.testing.assert_allclose(got[:, :3], ref[:, :3], rtol=0, atol=2e-6)
+    assert np.mean(np.all(got == ref, axis=1)) > 0.9   # most hits are bit-identical
+
+
+def test_gather(scene):
+    rng = np.random.default_rng(2)
+    n = 256
+    pos = rng.uniform(-0.45, 0.45, (n, 3)).astype(np.float32)
+    bases = np.zeros((n, 12), np.float32)
+    L = O.lib()
+    for i in range(n):
+        cur = C.c_uint32(0)
+        m9 = np.zeros(9, np.float32)
+        l9 = np.zeros(9, np.float32)
+        L.orc_basis(rng.normal(size=3).astype(np.float32), 0.1, i, 0, 0, 0, C.byref(cur), m9)
+        cur = C.c_uint32(0)
+        L.orc_basis(LIGHT, 0.1, i, 1, 0, 0, C.byref(cur), l9)
+        bases[i, :9], bases[i, 9:] = m9, l9[:3]
+    feat, gam = scene.vol.gather_features(pos, bases, LIGHT, scene.g, scene.alpha)
+    ref = np.zeros((n, 576), np.float32)
+    rg = np.zeros(n, np.float32)
+    f = np.zeros(576, np.float32)
+    gm = np.zeros(1, np.float32)
+    for i in range(n):
+        b = bases[i]
+        L.orc_setup_input(C.byref(scene.orc.c), 1, pos[i], b[0:3].copy(), b[3:6].copy(), b[6:9].copy(),
+                          b[9:12].copy(), LIGHT, scene.g, scene.alpha, f, gm)
+        ref[i], rg[i] = f, gm[0]
+    np.testing.assert_allclose(feat, ref, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(gam, rg, rtol=0, atol=2e-5)
+
+
+def _render_pair(scene, W, frame=0, launches=1, sr=0.99):
+    import mrpnn_b200 as M
+    ori, up, right = view_frame()
+    out = scene.vol.Render((W, W), ori, up, right, LIGHT, M.VolumeRender.MRPNN, scene.g, scene.alpha,
+                           sampleNum=launches, seed=3)
+    acc = np.zeros((W * W, 4), np.float32)
+    for k in range(launches):
+        view = O.make_view(W, W, ori, up, right, LIGHT, alpha=scene.alpha, g=scene.g, seed=3, frame=frame + k)
+        res = O.predict_pixels(scene.orc, view, np.arange(W * W, dtype=np.int32))
+        rate = np.float32(1.0) / np.float32(1 + k)
+        acc = acc * (np.float32(1) - rate) + res * rate
+    return out.reshape(-1, 4), acc
+
+
+def test_predict_render_one_launch(scene):
+    got, ref = _render_pair(scene, 64)
+    assert np.array_equal(got[:, 3] > 0, ref[:, 3] > 0)      # same pixels hit
+    assert (ref[:, 3] > 0).sum() > 500
+    ok = np.isclose(got, ref, rtol=MLP_RTOL, atol=MLP_ATOL).all(axis=1)
+    assert ok.mean() > 0.999, np.argwhere(~ok)[:5]
+
+
+def test_predict_render_running_mean(scene):
+    got, ref = _render_pair(scene, 32, launches=3)
+    np.testing.assert_allclose(got, ref, rtol=MLP_RTOL, atol=MLP_ATOL)

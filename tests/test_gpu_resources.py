@@ -1,0 +1,84 @@
+"""GPU volume resources against the CPU oracle: fBm volume, pyramid, majorant
+and occupancy are bit-exact; TR mips, HG LUT and the baked TR grid match to
+the last bits their transcendentals allow."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.gpu_scene import LIGHT, Scene
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scene():
+    return Scene(R=64, bake_res=48)
+
+
+def test_fbm_bit_exact(scene):
+    ref = O.fbm_volume(64, 0, 4.0)
+    np.testing.assert_array_equal(scene.density, ref)
+
+
+@pytest.mark.parametrize("R", [64, 200, 520])
+def test_pyramid_bit_exact(R):
+    import mrpnn_b200 as M
+    M.init()
+    rng = np.random.default_rng(R)
+    data = rng.uniform(-0.2, 1.0, R ** 3).astype(np.float32)   # negatives exercise the clamp
+    v = M.VolumeRender(R)
+    v.set_data(data)
+    v.Update()
+    ref = O.split_levels(O.build_pyramid(data, R), O.mip_sizes())
+    for m in range(9):
+        np.testing.assert_array_equal(v.read(M.api.RES_MIP, m), ref[m].ravel(), err_msg=f"mip {m}")
+    assert v.max_density == O.lib().orc_max_density(data, data.size)
+
+
+def test_occupancy_is_conservative(scene):
+    import mrpnn_b200 as M
+    occ = scene.vol.read(M.api.RES_OCCUPANCY)
+    R, B = 64, 8
+    nb = R // B
+    d = scene.density.reshape(R, R, R) != 0
+    pad = np.zeros((R + 2, R + 2, R + 2), bool)
+    pad[1:-1, 1:-1, 1:-1] = d
+    want = np.zeros((nb, nb, nb), np.uint8)
+    for bx in range(nb):
+        for by in range(nb):
+            for bz in range(nb):
+                want[bx, by, bz] = pad[bx * B:bx * B + B + 2, by * B:by * B + B + 2, bz * B:bz * B + B + 2].any()
+    np.testing.assert_array_equal(occ.reshape(nb, nb, nb), want)
+
+
+def test_tr_mips(scene):
+    ref = O.tr_mips(scene.mips, scene.alpha, LIGHT)
+    got = scene.tr
+    np.testing.assert_allclose(got, ref, rtol=2e-6, atol=1e-7)
+
+
+def test_hg_lut_subset(scene):
+    rng = np.random.default_rng(3)
+    tex = rng.choice(512 * 512, 3000, replace=False).astype(np.int32)
+    ref = O.hg_lut_texels(scene.g, 0, tex)
+    got = scene.lut[tex]
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-6)
+    # a texel can flip one of its 1024 samples between the two MIS branches
+    # when a transcendental differs in the last bit
+    assert np.mean(rel < 1e-4) > 0.995, np.sort(rel)[-10:]
+    assert np.max(rel) < 0.05
+
+
+def test_baked_tr_statistics(scene):
+    """Same Philox streams: most voxels reproduce exactly; the rest are the
+    same estimator, so the means agree."""
+    n = 48 ** 3
+    rng = np.random.default_rng(5)
+    vox = rng.choice(n, 4000, replace=False).astype(np.int64)
+    out = np.zeros(vox.size, np.float32)
+    L = O.lib()
+    import ctypes as C
+    L.orc_baked_tr(C.byref(scene.orc.c), scene.alpha, LIGHT, 48, 0, 1, vox, vox.size, out)
+    got = scene.baked[vox]
+    assert np.mean(np.abs(got - out) < 1e-5) > 0.9
+    assert abs(got.mean() - out.mean()) < 0.01

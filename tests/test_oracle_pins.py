@@ -1,0 +1,161 @@
+"""The CPU oracle against the reference's own render code.
+
+Golden vectors in tests/golden/ref_pins.npz come from the reference's
+core/vector.cu, core/radiancePredict.cu, core/renderResources.cu and
+core/render.cuh compiled on the CPU (tests/golden/make_golden.py).  Every
+case here is bit-exact: the oracle keeps the reference's float rounding order.
+"""
+import ctypes as C
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from tests.golden.make_golden import SCENE, build_scene, camera, light_dir
+
+
+def test_mlp_matches_reference(oracle, golden):
+    feat, gam = golden["mlp_feat"], golden["mlp_gamma"]
+    for tag in ("grey", "rgb"):
+        out = oracle.mlp_f32(feat, gam, 0.857, golden[f"mlp_sr_{tag}"])
+        np.testing.assert_array_equal(out, golden[f"mlp_out_{tag}"])
+
+
+def test_mlp_f64_close_to_f32(oracle, golden):
+    feat, gam = golden["mlp_feat"], golden["mlp_gamma"]
+    a = oracle.mlp_f32(feat, gam, 0.857, golden["mlp_sr_rgb"])
+    d = oracle.mlp_f64(feat, gam, 0.857, golden["mlp_sr_rgb"])
+    rel = np.abs(a - d) / np.maximum(np.abs(d), 1e-6)
+    assert rel.max() < 1e-4
+
+
+def test_stencil_tables(oracle, golden):
+    off, layer, typ, li, _ = oracle.stencil_tables()
+    np.testing.assert_array_equal(off, golden["st_offset"])
+    np.testing.assert_array_equal(layer, (golden["st_layer"] + np.float32(0.1)).astype(np.int32))
+    np.testing.assert_array_equal(typ, golden["st_type"])
+    np.testing.assert_array_equal(li, golden["st_localindex"])
+    data = C.POINTER(C.c_float)()
+    cnt = C.c_int()
+    assert oracle.lib().orc_model_tensor(b"STENCIL_DIRS", C.byref(data), C.byref(cnt)) == 0
+    dirs = np.ctypeslib.as_array(data, (cnt.value,)).reshape(160, 3)
+    np.testing.assert_array_equal(dirs, golden["st_dirs"][:160])
+
+
+def test_maths(oracle, golden):
+    L = oracle.lib()
+    hg = np.array([L.orc_hg(c, g) for c, g in golden["hg_in"]], np.float32)
+    np.testing.assert_array_equal(hg, golden["hg_out"])
+    out = np.zeros(3, np.float32)
+    for i in range(len(golden["shg_e"])):
+        e = golden["shg_e"][i]
+        L.orc_sample_hg(e[0], e[1], np.ascontiguousarray(golden["shg_v"][i]), golden["shg_g"][i], out)
+        np.testing.assert_array_equal(out, golden["shg_out"][i])
+    p, d = golden["rb_p"], golden["rb_d"]
+    off = np.array([L.orc_ray_box_offset(p[i], d[i]) for i in range(len(p))], np.float32)
+    dist = np.array([L.orc_ray_box_distance(p[i], d[i]) for i in range(len(p))], np.float32)
+    np.testing.assert_array_equal(off, golden["rb_off"])
+    np.testing.assert_array_equal(dist, golden["rb_dist"])
+
+
+@pytest.fixture(scope="module")
+def scene(oracle):
+    return build_scene()
+
+
+def test_scene_is_reproducible(scene, golden):
+    d = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+    assert d(scene.mips) == str(golden["scene_digest_mips"])
+    assert d(scene.tr) == str(golden["scene_digest_tr"])
+    assert d(scene.lut) == str(golden["scene_digest_lut"])
+
+
+def test_first_hit(oracle, scene, golden):
+    L = oracle.lib()
+    h = np.zeros(3, np.float32)
+    for o, d, ref in zip(golden["fh_ori"], golden["fh_dir"], golden["fh_out"]):
+        a = L.orc_first_hit(C.byref(scene.c), o, d, SCENE["alpha"], h)
+        assert a == int(ref[3])
+        np.testing.assert_array_equal(h, ref[:3])
+
+
+def test_basis(oracle, golden):
+    L = oracle.lib()
+    for i, (v, ref) in enumerate(zip(golden["basis_v"], golden["basis_out"])):
+        cur = C.c_uint32(0)
+        o9 = np.zeros(9, np.float32)
+        L.orc_basis(np.ascontiguousarray(v), 0.1, i, 0, 3, 11, C.byref(cur), o9)
+        np.testing.assert_array_equal(o9, ref)
+
+
+def test_setup_input(oracle, scene, golden):
+    L = oracle.lib()
+    Ld = light_dir()
+    f = np.zeros(576, np.float32)
+    gm = np.zeros(1, np.float32)
+    for p, b, ref_f, ref_g in zip(golden["si_pos"], golden["si_bases"], golden["si_feat"], golden["si_gamma"]):
+        b = np.ascontiguousarray(b)
+        L.orc_setup_input(C.byref(scene.c), 1, p, b[0:3].copy(), b[3:6].copy(), b[6:9].copy(), b[9:12].copy(), Ld,
+                          SCENE["g"], SCENE["alpha"], f, gm)
+        np.testing.assert_array_equal(f, ref_f)
+        assert gm[0] == ref_g
+
+
+def test_predict_pixels(oracle, scene, golden):
+    W = 16
+    ori, up, right = camera(W)
+    view = oracle.make_view(W, W, ori, up, right, light_dir(), alpha=SCENE["alpha"], g=SCENE["g"], seed=5, frame=2)
+    rgba = oracle.predict_pixels(scene, view, np.arange(W * W, dtype=np.int32))
+    np.testing.assert_array_equal(rgba, golden["pp_rgba"])
+    assert (rgba[:, 3] > 0).sum() > 50   # the view actually hits the cloud
+
+
+def test_trace_samples(oracle, scene, golden):
+    W = 16
+    ori, up, right = camera(W)
+    for (pix, k), ref in zip(golden["ts_cases"], golden["ts_out"]):
+        view = oracle.make_view(W, W, ori, up, right, light_dir(), alpha=SCENE["alpha"], g=SCENE["g"],
+                                multi_scatter=64, spp=int(k) + 1, seed=5, frame=2)
+        _, s, _ = oracle.trace_pixels(scene, view, np.array([pix], np.int32))
+        if k > 0:
+            view.spp = int(k)
+            _, s0, _ = oracle.trace_pixels(scene, view, np.array([pix], np.int32))
+            s = s - s0
+        np.testing.assert_array_equal(s[0].astype(np.float32), ref[:3])
+
+
+def test_transmittance(oracle, scene, golden):
+    L = oracle.lib()
+    Ld = light_dir()
+    for i, (p, ref) in enumerate(zip(golden["tr_pos"], golden["tr_out"])):
+        dis = L.orc_ray_box_distance(p, Ld)
+        v = L.orc_tr(C.byref(scene.c), p, Ld, dis, SCENE["alpha"], i, 0, 0, 9, 2)
+        assert np.float32(v) == ref
+
+
+def test_philox_known_answers(oracle):
+    """Philox-4x32-10 known-answer vectors of the Random123 distribution."""
+    L = oracle.lib()
+    out = np.zeros(4, np.uint32)
+    cases = [
+        ([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+        ([0xffffffff] * 4, [0xffffffff] * 2, [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+        ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+         [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]),
+    ]
+    for c, k, want in cases:
+        L.orc_philox4x32_10(np.array(c, np.uint32), np.array(k, np.uint32), out)
+        assert list(out) == want
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                                    "oracle", "_ref", "libmrpnn_ref.so"))
+                    and not os.path.isdir("/root/reference/core"), reason="reference checker not available")
+def test_live_reference_mlp_small(oracle):
+    """Re-run the reference MLP (live build) on fresh random features."""
+    rng = np.random.default_rng(7)
+    feat = rng.uniform(0, 2.0, (32, 576)).astype(np.float32)
+    gam = rng.uniform(0, np.pi, 32).astype(np.float32)
+    np.testing.assert_array_equal(oracle.mlp_f32(feat, gam, 0.6, (0.95, 0.95, 0.95)),
+                                  oracle.ref_mlp(feat, gam, 0.6, (0.95, 0.95, 0.95)))
