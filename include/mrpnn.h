@@ -173,6 +173,14 @@ mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bas
 mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, float alpha, int n, float* hit4,
                          int is_device);
 
+/* One FP32 MRPNN launch of mrp_render (launch index view->frame_offset, no
+ * running mean) that also returns the intermediates of NNPredict per pixel:
+ * aux [w*h][20] = hit x, y, z, hit flag, gamma, XMain, YMain, ZMain, LXMain
+ * (GetSamplePoint, GetMatrixFromNormal, core/render.cuh:808-843) and feat
+ * [w*h][576] (SetupInputData's features; zero where no hit). */
+mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* view, float* rgba, float* aux, float* feat,
+                                    int is_device);
+
 #ifdef __cplusplus
 }
 #endif

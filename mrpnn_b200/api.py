@@ -78,6 +78,7 @@ _SIGS = {
     "mrp_gather_features": ([C.c_void_p, C.c_void_p, C.c_void_p, F3, C.c_float, C.c_float, C.c_int, C.c_void_p,
                              C.c_void_p, C.c_int], C.c_int),
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
 }
 
 _lib = None
@@ -326,6 +327,16 @@ class VolumeRender:
         _check(lib().mrp_gather_features(self._h, pos.ctypes.data, bases.ctypes.data, _f3(light_dir), float(g),
                                          float(alpha), n, feat.ctypes.data, gam.ctypes.data, 0))
         return feat, gam
+
+    def predict_debug(self, view):
+        """One FP32 MRPNN launch with its intermediates: (rgba [n,4], aux [n,20], feat [n,576])."""
+        n = view.width * view.height
+        rgba = np.empty((n, 4), np.float32)
+        aux = np.empty((n, 20), np.float32)
+        feat = np.empty((n, 576), np.float32)
+        _check(lib().mrp_render_predict_debug(self._h, C.byref(view), rgba.ctypes.data, aux.ctypes.data,
+                                              feat.ctypes.data, 0))
+        return rgba, aux, feat
 
     def first_hit(self, ori, dirs, alpha):
         ori = _host_f32(ori).reshape(-1, 3)

@@ -696,6 +696,43 @@ mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, in
     return MRP_OK;
 }
 
+mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgba, float* aux, float* feat,
+                                    int is_device) {
+    TRY(need_init());
+    if (!v || !w || !rgba || !aux || !feat) return fail(MRP_ERR_INVALID, "null argument");
+    if (w->width <= 0 || w->height <= 0 || (long long)w->width * w->height > (1ll << 22))
+        return fail(MRP_ERR_INVALID, "debug render limited to 4M pixels");
+    if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "MRPNN needs the pyramid (mrp_volume_update)");
+    size_t npix = (size_t)w->width * w->height;
+    TRY(update_lut_async(v, w->g));
+    TRY(update_tr_async(v, w->light_dir, w->alpha));
+    float4* acc = nullptr;
+    float *da = aux, *df = feat;
+    std::vector<void*> allocs;
+    auto alloc = [&](size_t b) { void* p = nullptr; if (cudaMalloc(&p, b) == cudaSuccess) allocs.push_back(p); return p; };
+    auto release = [&]() { for (void* p : allocs) cudaFree(p); };
+    acc = (float4*)alloc(npix * sizeof(float4));
+    if (!is_device) { da = (float*)alloc(npix * 20 * 4); df = (float*)alloc(npix * 576 * 4); }
+    if (!acc || !da || !df) { release(); return fail(MRP_ERR_OOM, "debug render buffers"); }
+    cudaMemsetAsync(df, 0, npix * 576 * 4, v->stream);
+    cudaMemsetAsync(da, 0, npix * 20 * 4, v->stream);
+    ViewDev vd = make_view(v, w, w->frame_offset, 0);
+    cudaError_t e = launch_predict_fp32(v->dev(), vd, g.d_weights, acc, df, da, v->stream);
+    cudaMemcpyKind k = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (e == cudaSuccess) {
+        cudaMemcpyAsync(rgba, acc, npix * sizeof(float4), k, v->stream);
+        if (!is_device) {
+            cudaMemcpyAsync(aux, da, npix * 20 * 4, k, v->stream);
+            cudaMemcpyAsync(feat, df, npix * 576 * 4, k, v->stream);
+        }
+    }
+    cudaError_t e2 = cudaStreamSynchronize(v->stream);
+    release();
+    if (e != cudaSuccess || e2 != cudaSuccess)
+        return fail(MRP_ERR_CUDA, "debug render: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return MRP_OK;
+}
+
 mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms) {
     if (!v || !ms) return fail(MRP_ERR_INVALID, "null argument");
     *ms = v->last_ms;

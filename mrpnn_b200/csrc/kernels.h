@@ -33,9 +33,11 @@ cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float
 cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* dir, float alpha, float pass_rate, int n,
                              float* hit4, cudaStream_t s);
 // One launch of RenderCamera<true, MRPNN>: running mean into accum (float4
-// per pixel) with weight 1/(1+frame).
+// per pixel) with weight 1/(1+mean_k).  Optional per-pixel intermediates:
+// dbg_feat [npix][576], dbg_aux [npix][20] = hit xyz, hit flag, gamma, X, Y,
+// Z, LX.
 cudaError_t launch_predict_fp32(const VolumeDev& v, const ViewDev& view, const float* weights, float4* accum,
-                                float* dbg_feat, float* dbg_hit, cudaStream_t s);
+                                float* dbg_feat, float* dbg_aux, cudaStream_t s);
 
 // tracer_kernels.cu: one launch of RenderCamera<false> (spp samples per
 // pixel); FP64 sums of per-sample radiance and of its square per pixel.

@@ -139,38 +139,67 @@ MRP_D float shadow_tr(const VolumeDev& v, f3 p, f3 light, int mip) {
     return fm(1.0f, tex3<true>(g, n, p));
 }
 
-// SetupInputData (core/radiancePredict.cu:427-485).  Writes feature i of
-// channel c to out[c * stride + i].
-MRP_D void gather(const VolumeDev& v, f3 pos, f3 X, f3 Y, f3 Z, f3 LX, f3 L, float g, float alpha, float* out,
-                  int stride, float* gamma) {
-    for (int i = 0; i < 192; ++i) {
-        float off = c_offset[i];
-        int layer = c_layer[i];
-        f3 cur;
-        if (i < 160) {
-            f3 p = mk3(c_dirs[3 * i], c_dirs[3 * i + 1], c_dirs[3 * i + 2]);
-            cur = add(pos, mul(add(add(mul(X, p.x), mul(Y, p.y)), mul(Z, p.z)), off));
-        } else {
-            cur = add(pos, mul(L, off));
-        }
-        float d = tex3<false>(mip_level(v, layer), 256 >> layer, cur);
-        out[i] = logf(fa(1.0f, fd(fm(alpha, d), 64.0f)));
-        float hv;
-        if (i == 0) {
-            hv = logf(fa(hg(dot(X, L), g), 1.0f));
-        } else {
-            f3 ms = normalize(sub(cur, pos));
-            float c1 = dot(X, ms), c2 = dot(LX, ms);
-            float u = fa(fm(c1, 0.5f), 0.5f), u2 = fa(fm(c2, 0.5f), 0.5f);
-            float lv = c_lutv[i];
-            hv = logf(fa(fm(tex_lut(v.lut, u, lv), tex_lut(v.lut, u2, lv)), 1.0f));
-        }
-        out[2 * stride + i] = hv;
-        out[stride + i] = shadow_tr(v, cur, LX, layer > 1 ? layer - 1 : 0);
+// One stencil point of SetupInputData (core/radiancePredict.cu:433-471):
+// density (X_Val), TR (X_Val_Sub) and HG (X_Val_Hg) features of sample i.
+struct PixelFrame { f3 pos, X, Y, Z, LX, L; float g, alpha; };
+
+MRP_D void gather_sample(const VolumeDev& v, const PixelFrame& f, int i, float* fd_, float* fs_, float* fh_) {
+    float off = c_offset[i];
+    int layer = c_layer[i];
+    f3 cur;
+    if (i < 160) {
+        f3 p = mk3(c_dirs[3 * i], c_dirs[3 * i + 1], c_dirs[3 * i + 2]);
+        cur = add(f.pos, mul(add(add(mul(f.X, p.x), mul(f.Y, p.y)), mul(f.Z, p.z)), off));
+    } else {
+        cur = add(f.pos, mul(f.L, off));
     }
-    float dd = fminf(1.0f, fmaxf(-1.0f, dot(X, LX)));
-    *gamma = acosf(dd);
+    float d = tex3<false>(mip_level(v, layer), 256 >> layer, cur);
+    *fd_ = logf(fa(1.0f, fd(fm(f.alpha, d), 64.0f)));
+    if (i == 0) {
+        *fh_ = logf(fa(hg(dot(f.X, f.L), f.g), 1.0f));
+    } else {
+        f3 ms = normalize(sub(cur, f.pos));
+        float c1 = dot(f.X, ms), c2 = dot(f.LX, ms);
+        float u = fa(fm(c1, 0.5f), 0.5f), u2 = fa(fm(c2, 0.5f), 0.5f);
+        float lv = c_lutv[i];
+        *fh_ = logf(fa(fm(tex_lut(v.lut, u, lv), tex_lut(v.lut, u2, lv)), 1.0f));
+    }
+    *fs_ = shadow_tr(v, cur, f.LX, layer > 1 ? layer - 1 : 0);
 }
+MRP_D float gamma_of(const PixelFrame& f) { return acosf(fminf(1.0f, fmaxf(-1.0f, dot(f.X, f.LX)))); }
+
+// All 192 points; feature i of channel c to out[c * stride + i].
+MRP_D void gather(const VolumeDev& v, const PixelFrame& f, float* out, int stride, float* gamma) {
+    for (int i = 0; i < 192; ++i) gather_sample(v, f, i, out + i, out + stride + i, out + 2 * stride + i);
+    *gamma = gamma_of(f);
+}
+
+// Feature sources of the MLP: a block asks for its slice [FROM, FROM+W) of
+// the three channels just before it uses it, so no pixel ever holds all 576.
+struct GlobalFeatures {
+    const float* x;   // channel c at x[c * 192 + i]
+    template <int FROM, int W>
+    MRP_D void load(float (&xs)[3][32]) const {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int i = 0; i < W; ++i) xs[c][i] = __ldg(x + c * 192 + FROM + i);
+    }
+};
+struct GatheredFeatures {
+    const VolumeDev* v;
+    PixelFrame f;
+    template <int FROM, int W>
+    MRP_D void load(float (&xs)[3][32]) const {
+        float t[3][32];
+#pragma unroll 1
+        for (int i = 0; i < W; ++i) gather_sample(*v, f, FROM + i, &t[0][i], &t[1][i], &t[2][i]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int i = 0; i < W; ++i) xs[c][i] = t[c][i];
+    }
+};
 
 // ---------------------------------------------------------------------------
 // FP32 MLP, RadiancePredictInternal (core/radiancePredict.cu:301-422).
@@ -182,16 +211,18 @@ MRP_D float wld(const float* __restrict__ w, int i) { return __ldg(w + i); }
 
 MRP_D float sigmoid_ref(float o) { return (float)(1.0 / (1.0 + (double)expf(-o))); }
 
-template <int W, int FROM, bool WIDEN, bool HAS_PREV>
-MRP_D void mlp_block(const float* __restrict__ x, int stride, float g, float gamma, float* pool, int pid,
-                     float (&prev)[3][32], float (&nxt)[3][32], const float* __restrict__ wt) {
+template <int W, int FROM, bool WIDEN, bool HAS_PREV, class Src>
+MRP_D void mlp_block(const Src& src, float g, float gamma, float* pool, int pid, float (&prev)[3][32],
+                     float (&nxt)[3][32], const float* __restrict__ wt) {
+    float xs[3][32];
+    src.template load<FROM, W>(xs);
     // SE gate: pool (avg, max) of each channel's slice, 8->8 relu, 8->3 sigmoid
     float p8[8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float s = 0.0f, m = -10000.0f;
 #pragma unroll
-        for (int i = 0; i < W; ++i) { float xv = x[c * stride + FROM + i]; s += xv; m = fmaxf(m, xv); }
+        for (int i = 0; i < W; ++i) { float xv = xs[c][i]; s += xv; m = fmaxf(m, xv); }
         s = s / (float)W;
         pool[pid + c] = s;
         pool[36 + pid + c] = m;
@@ -221,7 +252,7 @@ MRP_D void mlp_block(const float* __restrict__ x, int stride, float g, float gam
         float in[W];
 #pragma unroll
         for (int i = 0; i < W; ++i) {
-            float t = x[c * stride + FROM + i] * gate[c];
+            float t = xs[c][i] * gate[c];
             in[i] = HAS_PREV ? t + prev[c][i] : t;
         }
 #pragma unroll 4
@@ -231,11 +262,11 @@ MRP_D void mlp_block(const float* __restrict__ x, int stride, float g, float gam
             for (int j = 0; j < W; ++j) a = fmaf(in[j], wld(wc, o * W + j), a);
             a = a >= 0.0f ? a : 0.0f;
             if (WIDEN) nxt[c][o] = a;
-            else nxt[c][o] = a + x[c * stride + FROM + o];
+            else nxt[c][o] = a + xs[c][o];
         }
         if (WIDEN) {
 #pragma unroll
-            for (int i = 0; i < W; ++i) nxt[c][W + i] = x[c * stride + FROM + i];
+            for (int i = 0; i < W; ++i) nxt[c][W + i] = xs[c][i];
         }
     }
 }
@@ -259,30 +290,29 @@ MRP_D void copy_state(float (&dst)[3][32], const float (&src)[3][32]) {
         for (int i = 0; i < K; ++i) dst[c][i] = src[c][i];
 }
 
-// x: features of one pixel, channel c at x[c * stride + i]
-MRP_D void mlp_fp32(const float* __restrict__ x, int stride, float gamma, float g, f3 sr, const float* __restrict__ wt,
-                    float out[3]) {
+template <class Src>
+MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __restrict__ wt, float out[3]) {
     float pool[75];
     pool[72] = g;
     pool[73] = gamma;
     float comb[120];
     {
         float a[3][32], b[3][32];
-        mlp_block<8, 0, false, false>(x, stride, g, gamma, pool, 0, a, b, wt + main_block_off(0));
+        mlp_block<8, 0, false, false>(x, g, gamma, pool, 0, a, b, wt + main_block_off(0));
         copy_state<8>(a, b);
-        mlp_block<8, 8, true, true>(x, stride, g, gamma, pool, 3, a, b, wt + main_block_off(1));
+        mlp_block<8, 8, true, true>(x, g, gamma, pool, 3, a, b, wt + main_block_off(1));
         copy_state<16>(a, b);
-        mlp_block<16, 16, false, true>(x, stride, g, gamma, pool, 6, a, b, wt + main_block_off(2));
+        mlp_block<16, 16, false, true>(x, g, gamma, pool, 6, a, b, wt + main_block_off(2));
         copy_state<16>(a, b);
-        mlp_block<16, 32, false, true>(x, stride, g, gamma, pool, 9, a, b, wt + main_block_off(3));
+        mlp_block<16, 32, false, true>(x, g, gamma, pool, 9, a, b, wt + main_block_off(3));
         copy_state<16>(a, b);
-        mlp_block<16, 48, true, true>(x, stride, g, gamma, pool, 12, a, b, wt + main_block_off(4));
+        mlp_block<16, 48, true, true>(x, g, gamma, pool, 12, a, b, wt + main_block_off(4));
         copy_state<32>(a, b);
-        mlp_block<32, 64, false, true>(x, stride, g, gamma, pool, 15, a, b, wt + main_block_off(5));
+        mlp_block<32, 64, false, true>(x, g, gamma, pool, 15, a, b, wt + main_block_off(5));
         copy_state<32>(a, b);
-        mlp_block<32, 96, false, true>(x, stride, g, gamma, pool, 18, a, b, wt + main_block_off(6));
+        mlp_block<32, 96, false, true>(x, g, gamma, pool, 18, a, b, wt + main_block_off(6));
         copy_state<32>(a, b);
-        mlp_block<32, 128, false, true>(x, stride, g, gamma, pool, 21, a, b, wt + main_block_off(7));
+        mlp_block<32, 128, false, true>(x, g, gamma, pool, 21, a, b, wt + main_block_off(7));
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float* wf = wt + kMainFinalOff + c * (1024 + 32);
@@ -291,13 +321,13 @@ MRP_D void mlp_fp32(const float* __restrict__ x, int stride, float gamma, float 
     }
     {
         float a[3][32], b[3][32];
-        mlp_block<8, 160, false, false>(x, stride, g, gamma, pool, 24, a, b, wt + di_block_off(0));
+        mlp_block<8, 160, false, false>(x, g, gamma, pool, 24, a, b, wt + di_block_off(0));
         copy_state<8>(a, b);
-        mlp_block<8, 168, false, true>(x, stride, g, gamma, pool, 27, a, b, wt + di_block_off(1));
+        mlp_block<8, 168, false, true>(x, g, gamma, pool, 27, a, b, wt + di_block_off(1));
         copy_state<8>(a, b);
-        mlp_block<8, 176, false, true>(x, stride, g, gamma, pool, 30, a, b, wt + di_block_off(2));
+        mlp_block<8, 176, false, true>(x, g, gamma, pool, 30, a, b, wt + di_block_off(2));
         copy_state<8>(a, b);
-        mlp_block<8, 184, false, true>(x, stride, g, gamma, pool, 33, a, b, wt + di_block_off(3));
+        mlp_block<8, 184, false, true>(x, g, gamma, pool, 33, a, b, wt + di_block_off(3));
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float* wf = wt + kDiFinalOff + c * (64 + 8);
@@ -387,8 +417,8 @@ __global__ void k_gather(VolumeDev v, const float* __restrict__ pos, const float
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* b = bases + 12 * i;
-    gather(v, ld3(pos + 3 * i), ld3(b), ld3(b + 3), ld3(b + 6), ld3(b + 9), ld3(light), g, alpha, feat + (size_t)576 * i,
-           192, gamma + i);
+    PixelFrame f{ld3(pos + 3 * i), ld3(b), ld3(b + 3), ld3(b + 6), ld3(b + 9), ld3(light), g, alpha};
+    gather(v, f, feat + (size_t)576 * i, 192, gamma + i);
 }
 
 __global__ void __launch_bounds__(128) k_mlp_fp32(const float* __restrict__ wt, const float* __restrict__ feat,
@@ -397,14 +427,14 @@ __global__ void __launch_bounds__(128) k_mlp_fp32(const float* __restrict__ wt, 
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float o[3];
-    mlp_fp32(feat + (size_t)576 * i, 192, gamma[i], g, sr, wt, o);
+    mlp_fp32(GlobalFeatures{feat + (size_t)576 * i}, gamma[i], g, sr, wt, o);
     out3[3 * i] = o[0]; out3[3 * i + 1] = o[1]; out3[3 * i + 2] = o[2];
 }
 
 // One launch of RenderCamera<true, MRPNN>; per-pixel thread.
 __global__ void __launch_bounds__(128) k_predict_fp32(VolumeDev v, ViewDev w, const float* __restrict__ wt,
                                                       float4* __restrict__ accum, float* __restrict__ dbg_feat,
-                                                      float* __restrict__ dbg_hit) {
+                                                      float* __restrict__ dbg_aux) {
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= w.width * w.height) return;
     int row = pix / w.width, col = pix % w.width;
@@ -418,23 +448,27 @@ __global__ void __launch_bounds__(128) k_predict_fp32(VolumeDev v, ViewDev w, co
     basis(L, 0.1f, st, &LX, &LY, &LZ);
     float4 res;
     if (active) {
-        float x[576], gamma;
-        gather(v, hit, X, Y, Z, LX, L, w.g, w.alpha, x, 192, &gamma);
+        GatheredFeatures src{&v, PixelFrame{hit, X, Y, Z, LX, L, w.g, w.alpha}};
+        float gamma = gamma_of(src.f);
         if (dbg_feat) {
-            for (int i = 0; i < 576; ++i) dbg_feat[(size_t)pix * 576 + i] = x[i];
+            float gdummy;
+            gather(v, src.f, dbg_feat + (size_t)pix * 576, 192, &gdummy);
         }
+        if (dbg_aux) dbg_aux[(size_t)pix * 20 + 4] = gamma;
         f3 sr = div(v.scatter_rate, 1.001f);
         float o[3];
-        mlp_fp32(x, 192, gamma, w.g, sr, wt, o);
+        mlp_fp32(src, gamma, w.g, sr, wt, o);
         f3 pr = mul(mk3(o[0], o[1], o[2]), 1.0f);
         f3 r = mul(mul(pr, w.light_color), v.scatter_rate);
         res = make_float4(r.x, r.y, r.z, length(sub(w.ori, hit)));
     } else {
         res = make_float4(v.sky.x, v.sky.y, v.sky.z, -1.0f);
     }
-    if (dbg_hit) {
-        dbg_hit[4 * pix] = hit.x; dbg_hit[4 * pix + 1] = hit.y; dbg_hit[4 * pix + 2] = hit.z;
-        dbg_hit[4 * pix + 3] = active ? 1.0f : 0.0f;
+    if (dbg_aux) {   // hit xyz, hit flag, gamma, X, Y, Z, LX (17 floats, stride 20)
+        float* a = dbg_aux + (size_t)pix * 20;
+        a[0] = hit.x; a[1] = hit.y; a[2] = hit.z; a[3] = active ? 1.0f : 0.0f;
+        a[5] = X.x; a[6] = X.y; a[7] = X.z; a[8] = Y.x; a[9] = Y.y; a[10] = Y.z;
+        a[11] = Z.x; a[12] = Z.y; a[13] = Z.z; a[14] = LX.x; a[15] = LX.y; a[16] = LX.z;
     }
     res.x = fmaxf(0.0f, res.x); res.y = fmaxf(0.0f, res.y); res.z = fmaxf(0.0f, res.z); res.w = fmaxf(0.0f, res.w);
     // result = lerp(result, res, 1/(1+frameNum)) (core/volume.cu:226-227)
@@ -462,10 +496,10 @@ cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float
     return cudaGetLastError();
 }
 cudaError_t launch_predict_fp32(const VolumeDev& v, const ViewDev& view, const float* weights, float4* accum,
-                                float* dbg_feat, float* dbg_hit, cudaStream_t s) {
+                                float* dbg_feat, float* dbg_aux, cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;
-    k_predict_fp32<<<(n + 127) / 128, 128, 0, s>>>(v, view, weights, accum, dbg_feat, dbg_hit);
+    k_predict_fp32<<<(n + 127) / 128, 128, 0, s>>>(v, view, weights, accum, dbg_feat, dbg_aux);
     return cudaGetLastError();
 }
 

@@ -131,3 +131,36 @@ def test_predict_render_one_launch(scene):
 def test_predict_render_running_mean(scene):
     got, ref = _render_pair(scene, 32, launches=3)
     np.testing.assert_allclose(got, ref, rtol=MLP_RTOL, atol=MLP_ATOL)
+
+
+def test_predict_intermediates(scene):
+    """Hit points, bases, gamma and features inside the render kernel against
+    the oracle's NNPredict, pixel by pixel."""
+    import mrpnn_b200 as M
+    W = 32
+    ori, up, right = view_frame()
+    view = scene.vol.make_view((W, W), ori, up, right, LIGHT, scene.g, scene.alpha, seed=3)
+    rgba, aux, feat = scene.vol.predict_debug(view)
+    oview = O.make_view(W, W, ori, up, right, LIGHT, alpha=scene.alpha, g=scene.g, seed=3, frame=0)
+    r_rgba, r_feat, r_gamma, r_hit = O.predict_pixels(scene.orc, oview, np.arange(W * W, dtype=np.int32),
+                                                      want_features=True)
+    L = O.lib()
+    hit = r_hit[:, 3] > 0
+    np.testing.assert_array_equal(aux[:, 3], r_hit[:, 3])
+    np.testing.assert_allclose(aux[hit, :3], r_hit[hit, :3], rtol=0, atol=2e-6)
+    # bases from the pixel stream (draws 0.. after InitRand)
+    bases = np.zeros((W * W, 12), np.float32)
+    for p in range(W * W):
+        d0 = np.zeros(3, np.float32)
+        L.orc_camera_ray(C.byref(oview), p // W, p % W, d0)
+        d = d0 / np.float32(np.sqrt(np.float32(np.dot(d0, d0))))
+        cur = C.c_uint32(0)
+        m9 = np.zeros(9, np.float32)
+        l9 = np.zeros(9, np.float32)
+        L.orc_basis(d.astype(np.float32), 0.1, p, 0, 0, 3, C.byref(cur), m9)
+        L.orc_basis(LIGHT, 0.1, p, 0, 0, 3, C.byref(cur), l9)
+        bases[p, :9], bases[p, 9:] = m9, l9[:3]
+    np.testing.assert_allclose(aux[:, 5:17], bases, rtol=0, atol=1e-5, err_msg="bases")
+    np.testing.assert_allclose(aux[hit, 4], r_gamma[hit], rtol=0, atol=2e-5, err_msg="gamma")
+    np.testing.assert_allclose(feat[hit], r_feat[hit], rtol=1e-5, atol=1e-6, err_msg="features")
+    np.testing.assert_allclose(rgba, r_rgba, rtol=MLP_RTOL, atol=MLP_ATOL, err_msg="rgba")
