@@ -242,6 +242,7 @@ def run_mine(args, rank, world, local):
     torch.cuda.synchronize()
     ms = []
     with ClockSampler(local) as clocks:
+        time.sleep(0.3)
         for k in range(args.steps):
             flush.fill_(float(k))
             torch.cuda.synchronize()
@@ -308,14 +309,17 @@ def run_mine(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp8"])
     ap.add_argument("--cpu-pixels", type=int, default=8192)
     ap.add_argument("--ref-pixels", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=1024, help="frame edge (the headline workload is 1024)")
     args = ap.parse_args()
+    global W, H
+    W = H = args.size
     rank, world, local = (0, 1, 0)
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", 0))

@@ -238,8 +238,16 @@ struct mrp_volume {
     int* first_pos = nullptr;
     unsigned long long* counter = nullptr;
     size_t trace_pix = 0;
+    // staged predictor buffers (records of hit pixels, tiled features)
+    int* rec_count = nullptr;
+    int* rec_pix = nullptr;
+    float* rec_f = nullptr;
+    float* feat = nullptr;
+    size_t rec_cap = 0;
     // tensor-core predictor scratch
     TcScratch tc;
+
+    HitRecords records() const { return HitRecords{rec_count, rec_pix, rec_f, rec_cap}; }
 
     VolumeDev dev() const {
         VolumeDev d{};
@@ -366,6 +374,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
     cudaFree(v->occ); cudaFree(v->d_maxbits); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
+    cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     tc_free_scratch(v->tc);
     if (v->ev0) cudaEventDestroy(v->ev0);
     if (v->ev1) cudaEventDestroy(v->ev1);
@@ -611,6 +620,18 @@ mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float al
 }
 
 // --- rendering ----------------------------------------------------------------
+static mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
+    if (v->rec_cap >= npix) return MRP_OK;
+    cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
+    v->rec_count = nullptr; v->rec_pix = nullptr; v->rec_f = nullptr; v->feat = nullptr; v->rec_cap = 0;
+    CU(cudaMalloc(&v->rec_count, sizeof(int)));
+    CU(cudaMalloc(&v->rec_pix, npix * sizeof(int)));
+    CU(cudaMalloc(&v->rec_f, npix * 16 * sizeof(float)));
+    CU(cudaMalloc(&v->feat, tiled_feature_floats(npix) * sizeof(float)));
+    v->rec_cap = npix;
+    return MRP_OK;
+}
+
 static ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k) {
     ViewDev d{};
     d.width = w->width;
@@ -668,17 +689,20 @@ mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, in
     } else {
         TRY(update_baked_async(v, w->light_dir, w->alpha));
     }
-    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) TRY(tc_ensure_scratch(v->tc, npix) == cudaSuccess ? MRP_OK
-                                                                        : fail(MRP_ERR_OOM, "tensor-core scratch"));
+    if (type == MRP_MRPNN) TRY(ensure_predictor_buffers(v, npix));
     VolumeDev d = v->dev();
     CU(cudaEventRecord(v->ev0, v->stream));
     for (int i = 0; i < sample_num; ++i) {
         ViewDev vd = make_view(v, w, w->frame_offset + i, i);
         if (type == MRP_MRPNN) {
+            HitRecords rec = v->records();
+            CU(launch_hit(d, vd, rec, v->accum, v->stream));
+            CU(launch_gather_rec(d, vd, rec, v->feat, v->stream));
             if (v->params.precision == MRP_FP32) {
-                CU(launch_predict_fp32(d, vd, g.d_weights, v->accum, nullptr, nullptr, v->stream));
+                CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, v->accum, v->stream));
             } else {
-                CU(tc_launch_predict(d, vd, g.tc, v->params.precision == MRP_FP8, v->tc, v->accum, g.sms, v->stream));
+                CU(tc_launch_mlp_rec(g.tc, v->params.precision == MRP_FP8, d, vd, rec, v->feat, v->accum, g.sms,
+                                     v->stream));
             }
         } else {
             CU(cudaMemsetAsync(v->sum3, 0, npix * 3 * sizeof(double), v->stream));
@@ -717,7 +741,14 @@ mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgb
     cudaMemsetAsync(df, 0, npix * 576 * 4, v->stream);
     cudaMemsetAsync(da, 0, npix * 20 * 4, v->stream);
     ViewDev vd = make_view(v, w, w->frame_offset, 0);
-    cudaError_t e = launch_predict_fp32(v->dev(), vd, g.d_weights, acc, df, da, v->stream);
+    mrp_status ps = ensure_predictor_buffers(v, npix);
+    if (ps != MRP_OK) { release(); return ps; }
+    HitRecords rec = v->records();
+    VolumeDev dv = v->dev();
+    cudaError_t e = launch_hit(dv, vd, rec, acc, v->stream);
+    if (e == cudaSuccess) e = launch_gather_rec(dv, vd, rec, v->feat, v->stream);
+    if (e == cudaSuccess) e = launch_mlp_rec_fp32(dv, vd, rec, v->feat, g.d_weights, acc, v->stream);
+    if (e == cudaSuccess) e = launch_debug_scatter(rec, v->feat, (int)npix, da, df, v->stream);
     cudaMemcpyKind k = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (e == cudaSuccess) {
         cudaMemcpyAsync(rgba, acc, npix * sizeof(float4), k, v->stream);

@@ -32,12 +32,26 @@ cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float
                             int n, float* out3, cudaStream_t s);
 cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* dir, float alpha, float pass_rate, int n,
                              float* hit4, cudaStream_t s);
-// One launch of RenderCamera<true, MRPNN>: running mean into accum (float4
-// per pixel) with weight 1/(1+mean_k).  Optional per-pixel intermediates:
-// dbg_feat [npix][576], dbg_aux [npix][20] = hit xyz, hit flag, gamma, X, Y,
-// Z, LX.
-cudaError_t launch_predict_fp32(const VolumeDev& v, const ViewDev& view, const float* weights, float4* accum,
-                                float* dbg_feat, float* dbg_aux, cudaStream_t s);
+// Staged predictor (one launch of RenderCamera<true, MRPNN>, running mean
+// into accum with weight 1/(1+mean_k)):
+//   launch_hit         ray + first hit + bases, compact list of hit pixels
+//   launch_gather_rec  stencil features of the hit pixels (tiled layout)
+//   launch_mlp_rec_*   network on the features, result at each pixel
+struct HitRecords {
+    int* count;     // number of records (device)
+    int* pix;       // [cap] pixel index of each record
+    float* f;       // [16][cap]: hit xyz, X, Y, Z, LX, gamma
+    size_t cap;     // >= pixels of the launch
+};
+cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, float4* accum, cudaStream_t s);
+cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s);
+cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitRecords rec, const float* feat,
+                                const float* weights, float4* accum, cudaStream_t s);
+// Scatters records and tiled features to per-pixel layout (debug entry).
+cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, int npix, float* aux, float* feat_out,
+                                 cudaStream_t s);
+// Tiled feature buffer size for n records (floats).
+inline size_t tiled_feature_floats(size_t n) { return ((n + 31) / 32) * 32 * 576; }
 
 // tracer_kernels.cu: one launch of RenderCamera<false> (spp samples per
 // pixel); FP64 sums of per-sample radiance and of its square per pixel.

@@ -11,8 +11,8 @@ cudaError_t tc_launch_mlp(const TcWeights&, bool, const float*, const float*, fl
                           cudaStream_t) {
     return cudaErrorNotSupported;
 }
-cudaError_t tc_launch_predict(const VolumeDev&, const ViewDev&, const TcWeights&, bool, TcScratch&, float4*, int,
-                              cudaStream_t) {
+cudaError_t tc_launch_mlp_rec(const TcWeights&, bool, const VolumeDev&, const ViewDev&, const HitRecords&,
+                              const float*, float4*, int, cudaStream_t) {
     return cudaErrorNotSupported;
 }
 

@@ -24,7 +24,9 @@ cudaError_t tc_ensure_scratch(TcScratch& s, size_t npix);
 void tc_free_scratch(TcScratch& s);
 cudaError_t tc_launch_mlp(const TcWeights& w, bool fp8, const float* feat, const float* gamma, float g, const float sr[3],
                           int n, float* out3, int sms, cudaStream_t s);
-cudaError_t tc_launch_predict(const VolumeDev& v, const ViewDev& view, const TcWeights& w, bool fp8, TcScratch& scratch,
-                              float4* accum, int sms, cudaStream_t s);
+// Network on the staged predictor's records and tiled features (kernels.h).
+struct HitRecords;
+cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
+                              const HitRecords& rec, const float* feat, float4* accum, int sms, cudaStream_t s);
 
 }  // namespace mrp

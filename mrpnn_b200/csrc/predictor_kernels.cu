@@ -47,6 +47,25 @@ MRP_D f3 camera_ray(const ViewDev& w, int row, int col) {
     return normalize(d);
 }
 
+// Density() at p, skipping the 8 texel loads when the occupancy bricks prove
+// the trilinear footprint is all zero: the base voxel of the fetch is
+// floor(uv*R - 0.5) per axis; a base outside [-1, R-1] reads only border
+// texels (0), and a base inside reads voxels base..base+1, which lie in the
+// 1-voxel apron of its brick.  lerp(0, 0, w) is exactly +0, so the skip
+// returns the value the fetch would.
+MRP_D float density_skip(const VolumeDev& v, f3 p) {
+    f3 uv = adds(p, 0.5f);
+    float nf = (float)v.res;
+    int x = (int)floorf(fs(fm(uv.x, nf), 0.5f)), y = (int)floorf(fs(fm(uv.y, nf), 0.5f)),
+        z = (int)floorf(fs(fm(uv.z, nf), 0.5f));
+    int R1 = v.res - 1;
+    if (x < -1 || y < -1 || z < -1 || x > R1 || y > R1 || z > R1) return 0.0f;
+    int nb = v.occ_res;
+    int b = ((max(x, 0) >> v.occ_shift) * nb + (max(y, 0) >> v.occ_shift)) * nb + (max(z, 0) >> v.occ_shift);
+    if (__ldg(v.occ + b) == 0) return 0.0f;
+    return tex3<false>(v.density, v.res, p);
+}
+
 // DeterminateEstimatedHit(float& alpha, ...) (core/render.cuh:105-197).
 // pass_rate = exp(-t_step * SMax) is computed once on the host.
 MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 pos, f3 dir, float dis, f3* next) {
@@ -61,7 +80,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
             *next = mk3(0, 0, 0);
             return false;
         }
-        float d = density(v, add(pos, mul(dir, t)));
+        float d = v.occ ? density_skip(v, add(pos, mul(dir, t))) : density(v, add(pos, mul(dir, t)));
         if (d > 0) {
             float S = fm(d, alpha);
             float step_p = fa(pass_rate, fm(fs(1.0f, pass_rate), fs(1.0f, fd(S, smax))));
@@ -186,6 +205,19 @@ struct GlobalFeatures {
             for (int i = 0; i < W; ++i) xs[c][i] = __ldg(x + c * 192 + FROM + i);
     }
 };
+// Tiled feature layout of the staged predictor: record r, channel c, sample
+// i at x[((r / 32) * 576 + c * 192 + i) * 32 + r % 32] -- a warp of 32
+// records reads or writes 128 contiguous bytes per feature.
+struct TiledFeatures {
+    const float* x;   // already offset to (r / 32) * 576 * 32 + r % 32
+    template <int FROM, int W>
+    MRP_D void load(float (&xs)[3][32]) const {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int i = 0; i < W; ++i) xs[c][i] = __ldg(x + (c * 192 + FROM + i) * 32);
+    }
+};
 struct GatheredFeatures {
     const VolumeDev* v;
     PixelFrame f;
@@ -276,8 +308,15 @@ MRP_D void dense_relu(const float* in, float* out, const float* __restrict__ w, 
 #pragma unroll 2
     for (int o = 0; o < TO; ++o) {
         float a = wld(b, o);
+        const float4* w4 = reinterpret_cast<const float4*>(w + o * FROM);
 #pragma unroll
-        for (int j = 0; j < FROM; ++j) a = fmaf(in[j], wld(w, o * FROM + j), a);
+        for (int j = 0; j < FROM / 4; ++j) {
+            float4 q = __ldg(w4 + j);
+            a = fmaf(in[4 * j], q.x, a);
+            a = fmaf(in[4 * j + 1], q.y, a);
+            a = fmaf(in[4 * j + 2], q.z, a);
+            a = fmaf(in[4 * j + 3], q.w, a);
+        }
         out[o] = a >= 0.0f ? a : 0.0f;
     }
 }
@@ -431,50 +470,116 @@ __global__ void __launch_bounds__(128) k_mlp_fp32(const float* __restrict__ wt, 
     out3[3 * i] = o[0]; out3[3 * i + 1] = o[1]; out3[3 * i + 2] = o[2];
 }
 
-// One launch of RenderCamera<true, MRPNN>; per-pixel thread.
-__global__ void __launch_bounds__(128) k_predict_fp32(VolumeDev v, ViewDev w, const float* __restrict__ wt,
-                                                      float4* __restrict__ accum, float* __restrict__ dbg_feat,
-                                                      float* __restrict__ dbg_aux) {
-    int pix = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pix >= w.width * w.height) return;
-    int row = pix / w.width, col = pix % w.width;
-    f3 dir = normalize(camera_ray(w, row, col));        // NNPredict: dir = normalize(dir)
-    f3 L = normalize(w.light_dir);
-    Stream st(kPixelStream, (uint32_t)pix, 0, (uint32_t)w.frame, w.seed);   // InitRand again
-    f3 hit;
-    bool active = first_hit(v, w.ori, dir, w.alpha, w.pass_rate, &hit);
-    f3 X, Y, Z, LX, LY, LZ;
-    basis(dir, 0.1f, st, &X, &Y, &Z);
-    basis(L, 0.1f, st, &LX, &LY, &LZ);
-    float4 res;
-    if (active) {
-        GatheredFeatures src{&v, PixelFrame{hit, X, Y, Z, LX, L, w.g, w.alpha}};
-        float gamma = gamma_of(src.f);
-        if (dbg_feat) {
-            float gdummy;
-            gather(v, src.f, dbg_feat + (size_t)pix * 576, 192, &gdummy);
-        }
-        if (dbg_aux) dbg_aux[(size_t)pix * 20 + 4] = gamma;
-        f3 sr = div(v.scatter_rate, 1.001f);
-        float o[3];
-        mlp_fp32(src, gamma, w.g, sr, wt, o);
-        f3 pr = mul(mk3(o[0], o[1], o[2]), 1.0f);
-        f3 r = mul(mul(pr, w.light_color), v.scatter_rate);
-        res = make_float4(r.x, r.y, r.z, length(sub(w.ori, hit)));
-    } else {
-        res = make_float4(v.sky.x, v.sky.y, v.sky.z, -1.0f);
-    }
-    if (dbg_aux) {   // hit xyz, hit flag, gamma, X, Y, Z, LX (17 floats, stride 20)
-        float* a = dbg_aux + (size_t)pix * 20;
-        a[0] = hit.x; a[1] = hit.y; a[2] = hit.z; a[3] = active ? 1.0f : 0.0f;
-        a[5] = X.x; a[6] = X.y; a[7] = X.z; a[8] = Y.x; a[9] = Y.y; a[10] = Y.z;
-        a[11] = Z.x; a[12] = Z.y; a[13] = Z.z; a[14] = LX.x; a[15] = LX.y; a[16] = LX.z;
-    }
+// ---------------------------------------------------------------------------
+// Staged predictor: one launch of RenderCamera<true, MRPNN> is
+//   k_hit     per pixel: ray, first hit, bases; hit pixels appended to a
+//             compact record list, missed pixels resolved to the sky;
+//   k_gather  per record: the 192-point stencil -> tiled features;
+//   k_mlp_*   per record: the network -> running mean at the record's pixel.
+// ---------------------------------------------------------------------------
+MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
     res.x = fmaxf(0.0f, res.x); res.y = fmaxf(0.0f, res.y); res.z = fmaxf(0.0f, res.z); res.w = fmaxf(0.0f, res.w);
     // result = lerp(result, res, 1/(1+frameNum)) (core/volume.cu:226-227)
-    float rate = fd(1.0f, (float)(1 + w.mean_k));
-    float4 a = w.mean_k == 0 ? make_float4(0, 0, 0, 0) : accum[pix];
+    float rate = fd(1.0f, (float)(1 + mean_k));
+    float4 a = mean_k == 0 ? make_float4(0, 0, 0, 0) : accum[pix];
     accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
+}
+
+__global__ void __launch_bounds__(256) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
+    int pix = blockIdx.x * blockDim.x + threadIdx.x;
+    int npix = w.width * w.height;
+    bool valid = pix < npix;
+    bool active = false;
+    f3 hit = mk3(0, 0, 0), X, Y, Z, LX;
+    if (valid) {
+        int row = pix / w.width, col = pix % w.width;
+        f3 dir = normalize(camera_ray(w, row, col));        // NNPredict: dir = normalize(dir)
+        f3 L = normalize(w.light_dir);
+        Stream st(kPixelStream, (uint32_t)pix, 0, (uint32_t)w.frame, w.seed);   // InitRand again
+        active = first_hit(v, w.ori, dir, w.alpha, w.pass_rate, &hit);
+        f3 LY, LZ;
+        basis(dir, 0.1f, st, &X, &Y, &Z);
+        basis(L, 0.1f, st, &LX, &LY, &LZ);
+        if (!active) running_mean(accum, pix, w.mean_k, make_float4(v.sky.x, v.sky.y, v.sky.z, -1.0f));
+    }
+    // warp-aggregated append of the hit pixels
+    unsigned lane = threadIdx.x & 31;
+    unsigned m = __ballot_sync(0xffffffffu, active);
+    if (m == 0) return;
+    int base = 0;
+    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(rec.count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (!active) return;
+    int r = base + __popc(m & ((1u << lane) - 1u));
+    size_t cap = rec.cap;
+    rec.pix[r] = pix;
+    float* f = rec.f + r;
+    float vals[16] = {hit.x, hit.y, hit.z, X.x, X.y, X.z, Y.x, Y.y, Y.z, Z.x, Z.y, Z.z, LX.x, LX.y, LX.z,
+                      gamma_of(PixelFrame{hit, X, Y, Z, LX, mk3(0, 0, 0), 0.0f, 0.0f})};
+#pragma unroll
+    for (int k = 0; k < 16; ++k) f[k * cap] = vals[k];
+}
+
+MRP_D PixelFrame record_frame(const HitRecords& rec, int r, f3 L, float g, float alpha) {
+    const float* f = rec.f + r;
+    size_t c = rec.cap;
+    PixelFrame pf;
+    pf.pos = mk3(f[0], f[c], f[2 * c]);
+    pf.X = mk3(f[3 * c], f[4 * c], f[5 * c]);
+    pf.Y = mk3(f[6 * c], f[7 * c], f[8 * c]);
+    pf.Z = mk3(f[9 * c], f[10 * c], f[11 * c]);
+    pf.LX = mk3(f[12 * c], f[13 * c], f[14 * c]);
+    pf.L = L;
+    pf.g = g;
+    pf.alpha = alpha;
+    return pf;
+}
+
+__global__ void __launch_bounds__(128) k_gather_rec(VolumeDev v, ViewDev w, HitRecords rec, float* __restrict__ feat) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= *rec.count) return;
+    PixelFrame pf = record_frame(rec, r, normalize(w.light_dir), w.g, w.alpha);
+    float* out = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
+#pragma unroll 1
+    for (int i = 0; i < 192; ++i) {
+        float a, b, c;
+        gather_sample(v, pf, i, &a, &b, &c);
+        out[i * 32] = a;
+        out[(192 + i) * 32] = b;
+        out[(384 + i) * 32] = c;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_mlp_rec(VolumeDev v, ViewDev w, HitRecords rec, const float* __restrict__ feat,
+                                                const float* __restrict__ wt, float4* __restrict__ accum) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= *rec.count) return;
+    float gamma = rec.f[15 * rec.cap + r];
+    f3 sr = div(v.scatter_rate, 1.001f);
+    float o[3];
+    mlp_fp32(TiledFeatures{feat + (size_t)(r >> 5) * 576 * 32 + (r & 31)}, gamma, w.g, sr, wt, o);
+    int pix = rec.pix[r];
+    f3 hit = mk3(rec.f[r], rec.f[rec.cap + r], rec.f[2 * rec.cap + r]);
+    f3 pr = mul(mk3(o[0], o[1], o[2]), 1.0f);   // alphaMult == 1 (core/render.cuh:844-848)
+    f3 res = mul(mul(pr, w.light_color), v.scatter_rate);
+    running_mean(accum, pix, w.mean_k, make_float4(res.x, res.y, res.z, length(sub(w.ori, hit))));
+}
+
+// Per-pixel intermediates for the debug entry point: aux [npix][20] = hit
+// xyz, hit flag, gamma, X, Y, Z, LX; feat [npix][576].
+__global__ void k_debug_scatter(HitRecords rec, const float* __restrict__ feat, float* __restrict__ aux,
+                                float* __restrict__ feat_out) {
+    int r = blockIdx.x;
+    if (r >= *rec.count) return;
+    int pix = rec.pix[r];
+    const float* f = rec.f + r;
+    float* a = aux + (size_t)pix * 20;
+    if (threadIdx.x == 0) {
+        a[0] = f[0]; a[1] = f[rec.cap]; a[2] = f[2 * rec.cap]; a[3] = 1.0f; a[4] = f[15 * rec.cap];
+        for (int k = 0; k < 12; ++k) a[5 + k] = f[(3 + k) * rec.cap];
+    }
+    const float* src = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
+    for (int i = threadIdx.x; i < 576; i += blockDim.x) feat_out[(size_t)pix * 576 + i] = src[i * 32];
 }
 
 cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* dir, float alpha, float pass_rate, int n,
@@ -495,11 +600,30 @@ cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float
     k_mlp_fp32<<<(n + 127) / 128, 128, 0, s>>>(weights, feat, gamma, g, mk3(sr[0], sr[1], sr[2]), n, out3);
     return cudaGetLastError();
 }
-cudaError_t launch_predict_fp32(const VolumeDev& v, const ViewDev& view, const float* weights, float4* accum,
-                                float* dbg_feat, float* dbg_aux, cudaStream_t s) {
+cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, float4* accum, cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;
-    k_predict_fp32<<<(n + 127) / 128, 128, 0, s>>>(v, view, weights, accum, dbg_feat, dbg_aux);
+    cudaError_t e = cudaMemsetAsync(rec.count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k_hit<<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s) {
+    int n = view.width * view.height;
+    if (n <= 0) return cudaSuccess;
+    k_gather_rec<<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
+    return cudaGetLastError();
+}
+cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitRecords rec, const float* feat,
+                                const float* weights, float4* accum, cudaStream_t s) {
+    int n = view.width * view.height;
+    if (n <= 0) return cudaSuccess;
+    k_mlp_rec<<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat, weights, accum);
+    return cudaGetLastError();
+}
+cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, int npix, float* aux, float* feat_out,
+                                 cudaStream_t s) {
+    if (npix > 0) k_debug_scatter<<<npix, 128, 0, s>>>(rec, feat, aux, feat_out);
     return cudaGetLastError();
 }
 

@@ -160,7 +160,7 @@ def test_predict_intermediates(scene):
         L.orc_basis(d.astype(np.float32), 0.1, p, 0, 0, 3, C.byref(cur), m9)
         L.orc_basis(LIGHT, 0.1, p, 0, 0, 3, C.byref(cur), l9)
         bases[p, :9], bases[p, 9:] = m9, l9[:3]
-    np.testing.assert_allclose(aux[:, 5:17], bases, rtol=0, atol=1e-5, err_msg="bases")
+    np.testing.assert_allclose(aux[hit, 5:17], bases[hit], rtol=0, atol=1e-5, err_msg="bases")
     np.testing.assert_allclose(aux[hit, 4], r_gamma[hit], rtol=0, atol=2e-5, err_msg="gamma")
     np.testing.assert_allclose(feat[hit], r_feat[hit], rtol=1e-5, atol=1e-6, err_msg="features")
     np.testing.assert_allclose(rgba, r_rgba, rtol=MLP_RTOL, atol=MLP_ATOL, err_msg="rgba")
