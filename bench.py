@@ -214,46 +214,71 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+STAGES = ("first hit + bases", "stencil gather", "network")
+# Algorithmic HBM bytes per hit pixel of each predictor stage (fp32 data):
+#   gather : 192 points x (8 density + 8 TR + 2 x 4 LUT texels) x 4 B read,
+#            576 features x 4 B written
+#   network: 576 features x 4 B read + 16 B record + 16 B result
+STAGE_BYTES_PER_HIT = (None, GATHER_BYTES_PER_PIXEL + 576 * 4, 576 * 4 + 32)
+
+
+def time_frames(vol, view, steps, flush, dev_out, frame0):
+    import torch
+
+    import mrpnn_b200 as M
+    ms, stages = [], []
+    for k in range(steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        view.frame_offset = frame0 + k
+        vol.render_view(view, M.VolumeRender.MRPNN, 1, dev_out)
+        ms.append(vol.last_render_ms())
+        stages.append(vol.last_render_stages())
+    return ms, np.mean(np.asarray(stages), axis=0)
+
+
 def run_mine(args, rank, world, local):
     import torch
 
     import mrpnn_b200 as M
     M.init(local)
-    prec = {"fp32": M.FP32, "bf16": M.BF16, "fp8": M.FP8}[args.precision]
+    precs = {"fp32": M.FP32, "bf16": M.BF16, "fp8": M.FP8}
     vol = M.VolumeRender(RES)
     vol.generate_fbm(SCENE["seed"], SCENE["freq"], SCENE["octaves"], SCENE["gain"])
     vol.Update()
     vol.SetScatterRate(SCENE["albedo"])
     vol.SetSky(SCENE["sky"])
-    vol.SetPrecision(prec)
     ori, up, right = view_vectors()
     L = light()
     view = vol.make_view((W, H), ori, up, right, L, SCENE["g"], SCENE["alpha"], seed=rank)
     dev_out = torch.empty((H, W, 4), dtype=torch.float32, device=f"cuda:{local}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")   # > L2 (126 MB)
 
-    for i in range(args.warmup):
-        view.frame_offset = i
-        vol.render_view(view, M.VolumeRender.MRPNN, 1, dev_out)
-    torch.cuda.synchronize()
-
-    # -- device-timed region: inputs resident, L2 flushed between steps --------
-    barrier(world)
-    torch.cuda.synchronize()
-    ms = []
-    with ClockSampler(local) as clocks:
-        time.sleep(0.3)
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            torch.cuda.synchronize()
-            view.frame_offset = 1000 + k
+    # every precision form, same protocol; the headline is args.precision
+    order = [p for p in ("fp32", "bf16", "fp8") if p != args.precision] + [args.precision]
+    forms = {}
+    for p in order:
+        vol.SetPrecision(precs[p])
+        for i in range(args.warmup):
+            view.frame_offset = i
             vol.render_view(view, M.VolumeRender.MRPNN, 1, dev_out)
-            ms.append(vol.last_render_ms())
-    torch.cuda.synchronize()
-    barrier(world)
-    total_ms = max_over_ranks(float(sum(ms)), world)
+        torch.cuda.synchronize()
+        barrier(world)
+        if p == args.precision:
+            with ClockSampler(local) as clocks:
+                time.sleep(0.3)
+                ms, stage_ms = time_frames(vol, view, args.steps, flush, dev_out, 1000)
+        else:
+            ms, stage_ms = time_frames(vol, view, max(3, args.steps // 4), flush, dev_out, 1000)
+        torch.cuda.synchronize()
+        barrier(world)
+        tot = max_over_ranks(float(sum(ms)), world)
+        forms[p] = {"value": len(ms) * world / (tot / 1000.0), "ms_per_frame": tot / len(ms),
+                    "stage_ms": dict(zip(STAGES, [round(float(x), 4) for x in stage_ms]))}
+    head = forms[args.precision]
+    total_ms = head["ms_per_frame"] * args.steps
     frames = args.steps * world
-    value = frames / (total_ms / 1000.0)
+    value = head["value"]
     img = dev_out.cpu().numpy()
     active = int((img[..., 3] > 0).sum())
 
@@ -268,38 +293,45 @@ def run_mine(args, rank, world, local):
     e2e = frames / e2e_s
 
     hbm, bf16, peak_kind = peaks()
-    avg_ms = float(np.mean(ms))
-    alg_bytes = active * GATHER_BYTES_PER_PIXEL + W * H * 16
-    achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
+    st = list(head["stage_ms"].values())
+    dom = int(np.argmax(st))
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            traffic = json.load(f).get(f"predict_{args.precision}_{W}x{H}", {}).get("dram_bytes_per_launch")
+            traffic = json.load(f).get(f"{args.precision}_{W}x{H}", {}).get(["hit", "gather", "network"][dom])
     except Exception:
         pass
+    if STAGE_BYTES_PER_HIT[dom] is not None:
+        alg = active * STAGE_BYTES_PER_HIT[dom]
+        achieved = alg / (st[dom] / 1000.0) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "kernel": STAGES[dom],
+                "note": f"algorithmic bytes = {STAGE_BYTES_PER_HIT[dom]} B x {active} hit pixels per launch; "
+                        f"duration = CUDA events around the stage; peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    else:
+        roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": traffic,
+                "kernel": STAGES[dom], "note": "march lookups are data dependent; see profiles/"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sc = cpu_scene_from_gpu(vol)
         pix_s, dt = time_cpu_predict(sc, args.cpu_pixels)
         cpu = {"value": pix_s / (W * H), "unit": UNIT, "cores": omp_threads(), "kind": "port",
-               "sample": f"{args.cpu_pixels} random pixels of the {W}x{H} frame ({dt:.1f}s), OpenMP oracle"}
+               "sample": f"{args.cpu_pixels} random pixels of the {W}x{H} frame ({dt:.2f}s), OpenMP oracle, FP32 MLP"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16", "fp8": "fp8-e4m3"}[args.precision],
-            "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "bf16": "bf16", "fp8": "fp8-e4m3"}[args.precision], "data": "synthetic",
             "config": {"workload": f"MRPNN predictor frame {W}x{H}, {RES}^3 fBm cloud (seed 1, freq 6), 9-level pyramid",
                        "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MiB write) between timed steps", "active_pixels": active},
+                       "l2": "flushed (256 MiB write) between timed steps", "hit_pixels": active,
+                       "precision_forms": forms},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 96, "d2h_bytes_per_step": W * H * 16},
-            "gpu_launches": args.steps * 1,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic,
-                         "note": f"predict kernel; algorithmic bytes = active pixels x {GATHER_BYTES_PER_PIXEL} B "
-                                 f"gather + 16 B/pixel output; peak {peak_kind}"},
+            "gpu_launches": args.steps * 3,
+            "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
@@ -312,7 +344,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp8"])
+    ap.add_argument("--precision", default="bf16", choices=["fp32", "bf16", "fp8"])
     ap.add_argument("--cpu-pixels", type=int, default=8192)
     ap.add_argument("--ref-pixels", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")

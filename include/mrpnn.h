@@ -155,8 +155,12 @@ mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float al
  * width*height float4 (RGB, A = coverage for PT / hit distance for MRPNN). */
 mrp_status mrp_render(mrp_volume* v, const mrp_view* view, mrp_render_type type, int sample_num, float* out_rgba,
                       int out_is_device);
-/* Device time of the kernels of the last mrp_render on this handle (ms). */
+/* Device time of the kernels of the last mrp_render on this handle (ms;
+ * -1 when it ran more than one launch -- see mrp_last_render_stages). */
 mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms);
+/* Device time of the stages of the last launch of the last mrp_render (ms):
+ * MRPNN = first hit + bases, stencil gather, network; PT = paths, resolve, 0. */
+mrp_status mrp_last_render_stages(const mrp_volume* v, float ms[3]);
 
 /* -- parity entry points (pieces of the path) ---------------------------------------- */
 /* RadiancePredictInternal (core/radiancePredict.cu:301-422) on n feature
@@ -172,6 +176,13 @@ mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bas
  * (x, y, z, 1 if hit). */
 mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, float alpha, int n, float* hit4,
                          int is_device);
+
+/* Tensor-core check: D[128][n] = A[128][k] * B[n][k]^T (row-major fp32 in,
+ * fp32 out) with A and B rounded to BF16 (fp8 = 0) or E4M3 (fp8 = 1) and
+ * accumulated in FP32 by one tcgen05.mma chain -- the operand layout and
+ * descriptors of the tensor-core MLP.  n: 16..128 step 16; k: multiple of 16
+ * (32 for E4M3) up to 128. */
+mrp_status mrp_tc_gemm_check(int fp8, const float* A, const float* B, int n, int k, float* D);
 
 /* One FP32 MRPNN launch of mrp_render (launch index view->frame_offset, no
  * running mean) that also returns the intermediates of NNPredict per pixel:

@@ -74,10 +74,12 @@ _SIGS = {
     "mrp_update_baked_tr": ([C.c_void_p, F3, C.c_float], C.c_int),
     "mrp_render": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_last_render_ms": ([C.c_void_p, C.POINTER(C.c_float)], C.c_int),
+    "mrp_last_render_stages": ([C.c_void_p, C.POINTER(C.c_float)], C.c_int),
     "mrp_predict_features": ([C.c_void_p, C.c_void_p, C.c_float, F3, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "mrp_gather_features": ([C.c_void_p, C.c_void_p, C.c_void_p, F3, C.c_float, C.c_float, C.c_int, C.c_void_p,
                              C.c_void_p, C.c_int], C.c_int),
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
 }
 
@@ -163,6 +165,17 @@ def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
     _check(lib().mrp_predict_features(feat.data_ptr(), gamma.data_ptr(), float(g), _f3(scatter_rate), n,
                                       out.data_ptr(), int(precision), 1))
     return out
+
+
+def tc_gemm_check(A, B, fp8=False):
+    """D = A B^T through one tcgen05.mma chain (A [128, k], B [n, k])."""
+    _ensure_init()
+    A = _host_f32(A)
+    B = _host_f32(B)
+    n, k = B.shape
+    D = np.empty((128, n), np.float32)
+    _check(lib().mrp_tc_gemm_check(1 if fp8 else 0, A.ctypes.data, B.ctypes.data, n, k, D.ctypes.data))
+    return D
 
 
 class VolumeRender:
@@ -316,6 +329,11 @@ class VolumeRender:
         ms = C.c_float()
         _check(lib().mrp_last_render_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def last_render_stages(self):
+        ms = (C.c_float * 3)()
+        _check(lib().mrp_last_render_stages(self._h, ms))
+        return list(ms)
 
     # -- parity pieces ------------------------------------------------------------
     def gather_features(self, pos, bases, light_dir, g, alpha):

@@ -213,7 +213,10 @@ struct mrp_volume {
     int res = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_stage[2] = {nullptr, nullptr};   // stage boundaries of the last launch
     float last_ms = 0.0f;
+    float stage_ms[3] = {0, 0, 0};
+    bool stages_valid = false;
     float* density = nullptr;
     float* mips = nullptr;
     float* trs = nullptr;
@@ -306,6 +309,7 @@ mrp_status mrp_load_model(const char* path) {
     if (!g.d_weights) CU(cudaMalloc(&g.d_weights, sizeof(float) * kWeightCount));
     CU(cudaMemcpy(g.d_weights, w.data(), sizeof(float) * kWeightCount, cudaMemcpyHostToDevice));
     CU(tc_prepare_weights(w.data(), g.tc));
+    g.tc.d_fp32 = g.d_weights;
     g.model = std::move(m);
     g.h_weights = std::move(w);
     return MRP_OK;
@@ -351,7 +355,8 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
     auto cleanup = [&](mrp_status s) { mrp_volume_destroy(v); return s; };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&v->ev0)) != cudaSuccess || (e = cudaEventCreate(&v->ev1)) != cudaSuccess)
+        (e = cudaEventCreate(&v->ev0)) != cudaSuccess || (e = cudaEventCreate(&v->ev1)) != cudaSuccess ||
+        (e = cudaEventCreate(&v->ev_stage[0])) != cudaSuccess || (e = cudaEventCreate(&v->ev_stage[1])) != cudaSuccess)
         return cleanup(fail(MRP_ERR_CUDA, "stream/event: %s", cudaGetErrorString(e)));
     size_t n = (size_t)res * res * res;
     v->occ_res = (res + (1 << v->occ_shift) - 1) >> v->occ_shift;
@@ -378,6 +383,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     tc_free_scratch(v->tc);
     if (v->ev0) cudaEventDestroy(v->ev0);
     if (v->ev1) cudaEventDestroy(v->ev1);
+    for (auto& ev : v->ev_stage) if (ev) cudaEventDestroy(ev);
     if (v->stream) cudaStreamDestroy(v->stream);
     delete v;
     return MRP_OK;
@@ -691,13 +697,18 @@ mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, in
     }
     if (type == MRP_MRPNN) TRY(ensure_predictor_buffers(v, npix));
     VolumeDev d = v->dev();
+    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) CU(cudaMemsetAsync(g.tc.d_err, 0, sizeof(int), v->stream));
     CU(cudaEventRecord(v->ev0, v->stream));
     for (int i = 0; i < sample_num; ++i) {
         ViewDev vd = make_view(v, w, w->frame_offset + i, i);
+        bool last = i == sample_num - 1;
         if (type == MRP_MRPNN) {
             HitRecords rec = v->records();
+            if (last) CU(cudaEventRecord(v->ev0, v->stream));
             CU(launch_hit(d, vd, rec, v->accum, v->stream));
+            if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));
             CU(launch_gather_rec(d, vd, rec, v->feat, v->stream));
+            if (last) CU(cudaEventRecord(v->ev_stage[1], v->stream));
             if (v->params.precision == MRP_FP32) {
                 CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, v->accum, v->stream));
             } else {
@@ -708,15 +719,35 @@ mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, in
             CU(cudaMemsetAsync(v->sum3, 0, npix * 3 * sizeof(double), v->stream));
             CU(launch_fill_int(v->first_pos, (int)npix, w->spp, v->stream));
             CU(cudaMemsetAsync(v->counter, 0, sizeof(unsigned long long), v->stream));
+            if (last) CU(cudaEventRecord(v->ev0, v->stream));
             CU(launch_trace(d, vd, v->sum3, nullptr, v->first_pos, v->counter, g.sms, v->stream));
+            if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));
             CU(launch_trace_resolve(v->sum3, v->first_pos, (int)npix, w->spp, i, v->accum, v->stream));
+            if (last) CU(cudaEventRecord(v->ev_stage[1], v->stream));
         }
     }
     CU(cudaEventRecord(v->ev1, v->stream));
     CU(cudaMemcpyAsync(out, v->accum, npix * sizeof(float4), out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                        v->stream));
     CU(cudaStreamSynchronize(v->stream));
-    CU(cudaEventElapsedTime(&v->last_ms, v->ev0, v->ev1));
+    if (sample_num == 1) CU(cudaEventElapsedTime(&v->last_ms, v->ev0, v->ev1));
+    else v->last_ms = -1.0f;
+    CU(cudaEventElapsedTime(&v->stage_ms[0], v->ev0, v->ev_stage[0]));
+    CU(cudaEventElapsedTime(&v->stage_ms[1], v->ev_stage[0], v->ev_stage[1]));
+    CU(cudaEventElapsedTime(&v->stage_ms[2], v->ev_stage[1], v->ev1));
+    v->stages_valid = true;
+    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) {
+        int herr = 0;
+        CU(cudaMemcpy(&herr, g.tc.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core MLP: MMA completion wait timed out");
+    }
+    return MRP_OK;
+}
+
+mrp_status mrp_last_render_stages(const mrp_volume* v, float ms[3]) {
+    if (!v || !ms) return fail(MRP_ERR_INVALID, "null argument");
+    if (!v->stages_valid) return fail(MRP_ERR_NOT_READY, "no render yet");
+    for (int i = 0; i < 3; ++i) ms[i] = v->stage_ms[i];
     return MRP_OK;
 }
 
@@ -764,6 +795,29 @@ mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgb
     return MRP_OK;
 }
 
+mrp_status mrp_tc_gemm_check(int fp8, const float* A, const float* B, int n, int k, float* D) {
+    TRY(need_init());
+    if (!A || !B || !D || n < 16 || n > 128 || n % 16 || k < 16 || k > 128 || k % (fp8 ? 32 : 16))
+        return fail(MRP_ERR_INVALID, "tc gemm check: n in 16..128 step 16, k multiple of %d up to 128", fp8 ? 32 : 16);
+    std::lock_guard<std::mutex> lk(g.mu);
+    size_t bytes = (size_t)(128 * k + n * k + 128 * n) * sizeof(float) + 64;
+    TRY(ensure_scratch(bytes));
+    float* dA = (float*)g.scratch;
+    float* dB = dA + 128 * k;
+    float* dD = dB + n * k;
+    int* derr = (int*)(dD + 128 * n);
+    CU(cudaMemcpyAsync(dA, A, 128 * k * sizeof(float), cudaMemcpyHostToDevice, g.stream));
+    CU(cudaMemcpyAsync(dB, B, (size_t)n * k * sizeof(float), cudaMemcpyHostToDevice, g.stream));
+    CU(cudaMemsetAsync(derr, 0, sizeof(int), g.stream));
+    CU(tc_gemm_test(fp8 != 0, dA, dB, n, k, dD, derr, g.stream));
+    int herr = 0;
+    CU(cudaMemcpyAsync(D, dD, (size_t)128 * n * sizeof(float), cudaMemcpyDeviceToHost, g.stream));
+    CU(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, g.stream));
+    CU(cudaStreamSynchronize(g.stream));
+    if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core GEMM check: MMA completion wait timed out");
+    return MRP_OK;
+}
+
 mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms) {
     if (!v || !ms) return fail(MRP_ERR_INVALID, "null argument");
     *ms = v->last_ms;
@@ -794,7 +848,12 @@ mrp_status mrp_predict_features(const float* feat, const float* gamma, float g_,
     if (precision == MRP_FP32) {
         CU(launch_mlp_fp32(g.d_weights, df, dg, g_, sr, n, dout, g.stream));
     } else if (precision == MRP_BF16 || precision == MRP_FP8) {
+        CU(cudaMemsetAsync(g.tc.d_err, 0, sizeof(int), g.stream));
         CU(tc_launch_mlp(g.tc, precision == MRP_FP8, df, dg, g_, sr, n, dout, g.sms, g.stream));
+        int herr = 0;
+        CU(cudaMemcpyAsync(&herr, g.tc.d_err, sizeof(int), cudaMemcpyDeviceToHost, g.stream));
+        CU(cudaStreamSynchronize(g.stream));
+        if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core MLP: MMA completion wait timed out");
     } else {
         return fail(MRP_ERR_INVALID, "unknown precision %d", (int)precision);
     }

@@ -1,19 +1,801 @@
-// mlp_tc.cu -- tensor-core MLP (placeholder until the tcgen05 kernels land:
-// every launch reports cudaErrorNotSupported, there is no fallback).
+// mlp_tc.cu -- the MRPNN network (RadiancePredictInternal,
+// core/radiancePredict.cu:301-422) on the 5th-generation tensor cores.
+//
+// Layout of the work.  A persistent kernel with one CTA per SM holds every
+// layer's weights in shared memory as UMMA operand images (K-major, no
+// swizzle: 8-row x 16-byte core matrices).  Two groups of 128 threads each
+// own one 128-pixel tile at a time; thread t of a group owns pixel row t of
+// its tile and TMEM lane t.  Per layer step the group writes its A rows
+// (activations, rounded to BF16 or quantised to FP8-E4M3) to shared memory,
+// one elected thread issues tcgen05.mma into the group's TMEM columns and
+// commits to an mbarrier, and every thread reads its row of the FP32
+// accumulator back with tcgen05.ld for the epilogue (bias, ReLU, residuals,
+// gates), all in FP32 on the CUDA cores.  The SE gate MLPs, pooling, the
+// LSEFin gate and the last 16->1 layer stay in FP32.
+//
+// Layers (58): per SE block three branch layers w x w (main widths 8, 8, 16,
+// 16, 16, 32, 32, 32; direct-illumination 4 x 8), the three final 32x32 and
+// 8x8 layers, then LC0 128x128, LC1 64x128, LC2 32x64, LX 16x32, LX0..LX11
+// 16x16.  N and K are padded to the MMA granularity with zeros.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kernels.h"
 #include "mlp_tc.h"
+#include "tc_ptx.cuh"
 
 namespace mrp {
 
-cudaError_t tc_prepare_weights(const float*, TcWeights& w) { w.ready = false; return cudaSuccess; }
-cudaError_t tc_ensure_scratch(TcScratch&, size_t) { return cudaSuccess; }
-void tc_free_scratch(TcScratch& s) { if (s.buf) cudaFree(s.buf); s.buf = nullptr; s.bytes = 0; }
-cudaError_t tc_launch_mlp(const TcWeights&, bool, const float*, const float*, float, const float*, int, float*, int,
-                          cudaStream_t) {
-    return cudaErrorNotSupported;
+// ---------------------------------------------------------------------------
+// layer table (shared by the host packer and the kernel)
+// ---------------------------------------------------------------------------
+constexpr int kLayers = 58;
+// main SE block widths (kMainW) and packed fp32 offsets, usable at run time in device code
+__host__ __device__ constexpr int mw(int k) { return k < 2 ? 8 : k < 5 ? 16 : 32; }
+__host__ __device__ constexpr int mblk_off(int k) { int o = 0; for (int i = 0; i < k; ++i) o += 64 + 24 + 3 * (mw(i) * mw(i) + mw(i)); return o; }
+static_assert(mblk_off(8) == kMainFinalOff, "block offsets");
+constexpr int kL81 = 24, kLD41 = 39, kLC0 = 42, kLC1 = 43, kLC2 = 44, kLX = 45, kLX0 = 46;
+__host__ __device__ constexpr int layer_n(int i) {
+    return i < 24 ? mw(i / 3) : i < 27 ? 32 : i < 42 ? 8 : i == kLC0 ? 128 : i == kLC1 ? 64 : i == kLC2 ? 32 : 16;
 }
-cudaError_t tc_launch_mlp_rec(const TcWeights&, bool, const VolumeDev&, const ViewDev&, const HitRecords&,
-                              const float*, float4*, int, cudaStream_t) {
-    return cudaErrorNotSupported;
+__host__ __device__ constexpr int layer_k(int i) {
+    return i < 24 ? mw(i / 3) : i < 27 ? 32 : i < 42 ? 8 : i == kLC0 ? 128 : i == kLC1 ? 128 : i == kLC2 ? 64 :
+           i == kLX ? 32 : 16;
+}
+__host__ __device__ constexpr int pad_to(int x, int m) { return (x + m - 1) / m * m; }
+// operand element bytes: 2 (BF16) or 1 (E4M3); K granularity 16 / 32 elements
+__host__ __device__ constexpr int kpad(int i, int eb) { return pad_to(layer_k(i), eb == 2 ? 16 : 32); }
+__host__ __device__ constexpr int npad(int i) { return pad_to(layer_n(i), 16); }
+__host__ __device__ constexpr int layer_bytes(int i, int eb) { return npad(i) * kpad(i, eb) * eb; }
+__host__ __device__ constexpr int layer_off(int i, int eb) {
+    int o = 0;
+    for (int j = 0; j < i; ++j) o += layer_bytes(j, eb);
+    return o;
+}
+__host__ __device__ constexpr int image_bytes(int eb) { return layer_off(kLayers, eb); }
+// FP8 weight scales: one per output channel, layer i's at scale_off(i)
+__host__ __device__ constexpr int scale_off(int i) {
+    int o = 0;
+    for (int j = 0; j < i; ++j) o += npad(j);
+    return o;
+}
+constexpr int kScaleCount = scale_off(kLayers);
+// fp32 weight / bias of layer i in the packed fp32 layout (common.cuh)
+__host__ __device__ constexpr int layer_w32(int i) {
+    return i < 24 ? mblk_off(i / 3) + 88 + (i % 3) * (mw(i / 3) * mw(i / 3) + mw(i / 3))
+         : i < 27 ? kMainFinalOff + (i - 24) * (1024 + 32)
+         : i < 39 ? di_block_off((i - 27) / 3) + 88 + ((i - 27) % 3) * 72
+         : i < 42 ? kDiFinalOff + (i - 39) * 72
+         : i == kLC0 ? kLC0W : i == kLC1 ? kLC1W : i == kLC2 ? kLC2W : i == kLX ? kLXW : lxw(i - kLX0);
+}
+__host__ __device__ constexpr int layer_b32(int i) { return layer_w32(i) + layer_n(i) * layer_k(i); }
+static_assert(layer_b32(kLC0) == kLC0B && layer_b32(kLX0 + 11) == lxb(11), "layer table");
+static_assert(image_bytes(2) <= 110 * 1024, "BF16 weight image must fit shared memory");
+
+// Byte offset of element (row m, k) in a K-major no-swizzle operand tile of
+// padded width Kp: 8-row groups SBO = Kp*eb*8 bytes apart, 16-byte K chunks
+// 128 bytes apart, rows of a core matrix 16 bytes apart.
+__host__ __device__ constexpr int op_off(int m, int k, int kp, int eb) {
+    return (m / 8) * (kp * eb * 8) + (k * eb / 16) * 128 + (m % 8) * 16 + (k * eb) % 16;
+}
+
+// ---------------------------------------------------------------------------
+// host: operand images
+// ---------------------------------------------------------------------------
+static uint16_t bf16_bits(float f) {   // round to nearest even
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16 | ((u & 0xFFFF) ? 0x40 : 0));
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+// E4M3 (bias 7, no infinities, max 448), round to nearest even, saturating.
+static uint8_t e4m3_bits(float f) {
+    uint8_t s = std::signbit(f) ? 0x80 : 0;
+    double a = std::fabs((double)f);
+    if (!(a == a)) return 0x7F;
+    if (a >= 448.0) return s | 0x7E;
+    if (a < std::ldexp(1.0, -10)) return s;   // below half the smallest subnormal
+    int e;
+    std::frexp(a, &e);                        // a = m * 2^e, m in [0.5, 1)
+    int ex = e - 1;                           // a in [2^ex, 2^(ex+1))
+    if (ex < -6) ex = -6;                     // subnormal range shares 2^-6 * 0.mmm
+    double q = std::ldexp(1.0, ex - 3);       // quantum of 3 mantissa bits
+    double n = std::nearbyint(a / q);         // ties to even (default rounding)
+    double v = n * q;
+    if (v >= 448.0) return s | 0x7E;
+    if (v == 0) return s;
+    int vex;
+    std::frexp(v, &vex);
+    vex -= 1;
+    if (vex < -6) return s | (uint8_t)(v / std::ldexp(1.0, -9));   // subnormal: mantissa / 8 * 2^-6
+    uint8_t mant = (uint8_t)(v / std::ldexp(1.0, vex) * 8.0 - 8.0);
+    return s | (uint8_t)((vex + 7) << 3) | mant;
+}
+
+cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
+    std::vector<uint8_t> img16(image_bytes(2), 0), img8(image_bytes(1), 0);
+    // FP8: each output channel (weight row) scaled by its own amax / 448
+    std::vector<float> scales(kScaleCount, 1.0f);
+    for (int i = 0; i < kLayers; ++i) {
+        int n = layer_n(i), k = layer_k(i);
+        const float* W = w32 + layer_w32(i);   // [n][k], row-major (Out, In)
+        for (int r = 0; r < n; ++r) {
+            float amax = 0.0f;
+            for (int c = 0; c < k; ++c) amax = std::fmax(amax, std::fabs(W[r * k + c]));
+            float s = amax > 0 ? amax / 448.0f : 1.0f;
+            scales[scale_off(i) + r] = s;
+            for (int c = 0; c < k; ++c) {
+                uint16_t b = bf16_bits(W[r * k + c]);
+                std::memcpy(&img16[layer_off(i, 2) + op_off(r, c, kpad(i, 2), 2)], &b, 2);
+                img8[layer_off(i, 1) + op_off(r, c, kpad(i, 1), 1)] = e4m3_bits(W[r * k + c] / s);
+            }
+        }
+    }
+    cudaError_t e;
+    if (!w.d_bf16 && (e = cudaMalloc(&w.d_bf16, img16.size())) != cudaSuccess) return e;
+    if (!w.d_fp8 && (e = cudaMalloc(&w.d_fp8, img8.size())) != cudaSuccess) return e;
+    if (!w.d_scales && (e = cudaMalloc(&w.d_scales, kScaleCount * sizeof(float))) != cudaSuccess) return e;
+    if (!w.d_err && (e = cudaMalloc(&w.d_err, sizeof(int))) != cudaSuccess) return e;
+    if (!w.d_counter && (e = cudaMalloc(&w.d_counter, sizeof(int))) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(w.d_bf16, img16.data(), img16.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(w.d_fp8, img8.data(), img8.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(w.d_scales, scales.data(), kScaleCount * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemset(w.d_err, 0, sizeof(int))) != cudaSuccess) return e;
+    w.ready = true;
+    return cudaSuccess;
+}
+cudaError_t tc_ensure_scratch(TcScratch&, size_t) { return cudaSuccess; }
+void tc_free_scratch(TcScratch& s) {
+    if (s.buf) cudaFree(s.buf);
+    s.buf = nullptr;
+    s.bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+// device: group synchronisation and one MMA round
+// ---------------------------------------------------------------------------
+constexpr int kGroupThreads = 128;
+constexpr int kGroups = 2;
+constexpr int kTmemColsPerGroup = 256;
+constexpr uint32_t kWaitLimit = 1u << 22;   // polls before an MMA round is declared lost
+constexpr int kABytes = 128 * 128 * 2;      // one group's A buffer (largest: 128 x 128 BF16)
+
+__device__ __forceinline__ void group_bar(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory");
+}
+
+struct Group {
+    int g, t;             // group index, thread within the group
+    uint8_t* a;           // A buffer (shared)
+    const uint8_t* wimg;  // weight image (shared)
+    uint64_t* mbar;
+    uint32_t phase;
+    uint32_t tmem;        // TMEM address of this thread's lane, column 0 of the group
+    uint32_t tmem_col0;   // TMEM address of lane 0, column 0 of the group (MMA D base)
+    int* err;
+    bool ok;
+};
+
+// One MMA per (layer, A sub-tile, D column); issued after all A rows are in
+// shared memory, awaited by the whole group.
+template <int EB>
+__device__ __forceinline__ void mma_round(Group& G, const int* layers, const int* a_off, const int* dcol, int count) {
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    group_bar(G.g);
+    if (G.t == 0) {
+        tc::fence_after_sync();
+        uint32_t abase = tc::smem_addr(G.a), wbase = tc::smem_addr(G.wimg);
+        for (int q = 0; q < count; ++q) {
+            int L = layers[q];
+            int kp = kpad(L, EB);
+            uint32_t idesc = tc::instr_desc(128, npad(L), EB == 2 ? tc::kFmtBF16 : tc::kFmtE4M3);
+            uint32_t sbo = (uint32_t)(kp * EB * 8);
+            int steps = kp * EB / 32;   // 32 bytes of K per MMA (16 BF16 / 32 E4M3)
+            for (int s = 0; s < steps; ++s) {
+                uint64_t ad = tc::smem_desc(abase + a_off[q] + s * 256, 128, sbo);
+                uint64_t bd = tc::smem_desc(wbase + layer_off(L, EB) + s * 256, 128, sbo);
+                if (EB == 2) tc::mma_bf16(G.tmem_col0 + dcol[q], ad, bd, idesc, s > 0);
+                else tc::mma_fp8(G.tmem_col0 + dcol[q], ad, bd, idesc, s > 0);
+            }
+        }
+        tc::mma_commit(G.mbar);
+    }
+    bool done = tc::mbar_wait(G.mbar, G.phase, kWaitLimit);
+    G.phase ^= 1u;
+    if (!done) {
+        G.ok = false;
+        atomicExch(G.err, 1);
+    }
+    tc::fence_after_sync();
+}
+
+// Writes this thread's row of an A operand: v[0..n) (zero padded to kp) at
+// sub-tile byte offset `off`.  FP8 rows are scaled by 1/s (s = row amax/448),
+// returned so the epilogue can undo it.
+template <int EB, int N, int KP>
+__device__ __forceinline__ float write_row(uint8_t* a, int off, int row, const float* v) {
+    float inv = 1.0f, s = 1.0f;
+    if (EB == 1) {
+        float amax = 0.0f;
+#pragma unroll
+        for (int i = 0; i < N; ++i) amax = fmaxf(amax, fabsf(v[i]));
+        s = amax > 0.0f ? amax * (1.0f / 448.0f) : 1.0f;
+        inv = 1.0f / s;
+    }
+    constexpr int E = 16 / EB;   // elements per 16-byte chunk
+#pragma unroll
+    for (int c = 0; c < KP / E; ++c) {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (EB == 2) {
+                int i0 = c * 8 + 2 * q;
+                float lo = i0 < N ? v[i0] : 0.0f, hi = i0 + 1 < N ? v[i0 + 1] : 0.0f;
+                w[q] = tc::pack_bf16(lo, hi);
+            } else {
+                int i0 = c * 16 + 4 * q;
+                float x0 = i0 < N ? v[i0] * inv : 0.0f, x1 = i0 + 1 < N ? v[i0 + 1] * inv : 0.0f;
+                float x2 = i0 + 2 < N ? v[i0 + 2] * inv : 0.0f, x3 = i0 + 3 < N ? v[i0 + 3] * inv : 0.0f;
+                w[q] = (uint32_t)tc::pack_e4m3(x0, x1) | ((uint32_t)tc::pack_e4m3(x2, x3) << 16);
+            }
+        }
+        *reinterpret_cast<uint4*>(a + off + op_off(row, c * E, KP, EB)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    return s;
+}
+
+// Same from a value functor f(i), i < N (evaluated twice for FP8: amax, then quantise).
+template <int EB, int N, int KP, class F>
+__device__ __forceinline__ float write_row_fn(uint8_t* a, int off, int row, F f) {
+    float inv = 1.0f, s = 1.0f;
+    if (EB == 1) {
+        float amax = 0.0f;
+#pragma unroll
+        for (int i = 0; i < N; ++i) amax = fmaxf(amax, fabsf(f(i)));
+        s = amax > 0.0f ? amax * (1.0f / 448.0f) : 1.0f;
+        inv = 1.0f / s;
+    }
+    constexpr int E = 16 / EB;
+#pragma unroll
+    for (int c = 0; c < KP / E; ++c) {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (EB == 2) {
+                int i0 = c * 8 + 2 * q;
+                w[q] = tc::pack_bf16(i0 < N ? f(i0) : 0.0f, i0 + 1 < N ? f(i0 + 1) : 0.0f);
+            } else {
+                int i0 = c * 16 + 4 * q;
+                float x0 = i0 < N ? f(i0) * inv : 0.0f, x1 = i0 + 1 < N ? f(i0 + 1) * inv : 0.0f;
+                float x2 = i0 + 2 < N ? f(i0 + 2) * inv : 0.0f, x3 = i0 + 3 < N ? f(i0 + 3) * inv : 0.0f;
+                w[q] = (uint32_t)tc::pack_e4m3(x0, x1) | ((uint32_t)tc::pack_e4m3(x2, x3) << 16);
+            }
+        }
+        *reinterpret_cast<uint4*>(a + off + op_off(row, c * E, KP, EB)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    return s;
+}
+
+// Reads N (<= 128, multiple of 16 or 8) accumulator columns of this thread's row.
+template <int N>
+__device__ __forceinline__ void read_cols(const Group& G, int col, float* out) {
+#pragma unroll
+    for (int c = 0; c < (N + 15) / 16; ++c) {
+        float v[16];
+        tc::tmem_ld16(G.tmem + col + 16 * c, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (16 * c + i < N) out[16 * c + i] = v[i];
+    }
+}
+
+MRP_D float wl(const float* __restrict__ w, int i) { return __ldg(w + i); }
+MRP_D float sigmoid_d(float o) { return 1.0f / (1.0f + __expf(-o)); }
+
+// Feature sources (rows may be invalid: zeros).
+struct RowFeatures {           // [n][576] row-major
+    const float* x;
+    bool valid;
+    template <int FROM, int W>
+    MRP_D void load(int c, float (&xs)[32]) const {
+#pragma unroll
+        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + c * 192 + FROM + i) : 0.0f;
+    }
+};
+struct TileFeatures {          // tiled layout of the staged predictor
+    const float* x;
+    bool valid;
+    template <int FROM, int W>
+    MRP_D void load(int c, float (&xs)[32]) const {
+#pragma unroll
+        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + (c * 192 + FROM + i) * 32) : 0.0f;
+    }
+};
+
+// One SE block over the three channels: gate from the slice pools, then the
+// branch layers on the tensor cores.  prev/nxt hold the residual state.
+template <int EB, int W, int FROM, bool WIDEN, bool HAS_PREV, int LAYER0, int DCOL, class Src>
+MRP_D void tc_block(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
+                    int se_off, int pid, float g, float gamma, float (&hf)[16], float (&prev)[3][32]) {
+    constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
+    constexpr int SUB = 128 * KP * EB;   // bytes of one branch's A sub-tile
+    float p8[8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float xs[32];
+        src.template load<FROM, W>(c, xs);
+        float s = 0.0f, m = -10000.0f;
+#pragma unroll
+        for (int i = 0; i < W; ++i) { s += xs[i]; m = fmaxf(m, xs[i]); }
+        s = s / (float)W;
+        p8[c] = s;
+        p8[3 + c] = m;
+    }
+    p8[6] = g;
+    p8[7] = gamma;
+    // LSEFin1 (75 -> 16) accumulated block by block: pool[pid + c] = avg,
+    // pool[36 + pid + c] = max
+#pragma unroll
+    for (int o = 0; o < 16; ++o) {
+        float a = hf[o];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            a = fmaf(wl(w32, kLSEFin1W + o * 75 + pid + c), p8[c], a);
+            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 36 + pid + c), p8[3 + c], a);
+        }
+        hf[o] = a;
+    }
+    float h[8], gate[3];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], wl(w32, se_off + o * 8 + j), a);
+        h[o] = fmaxf(a, 0.0f);
+    }
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = fmaf(h[j], wl(w32, se_off + 64 + o * 8 + j), a);
+        gate[o] = sigmoid_d(a);
+    }
+    float rs[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float xs[32], in[32];
+        src.template load<FROM, W>(c, xs);
+#pragma unroll
+        for (int i = 0; i < W; ++i) in[i] = HAS_PREV ? fmaf(xs[i], gate[c], prev[c][i]) : xs[i] * gate[c];
+        rs[c] = write_row<EB, W, KP>(G.a, c * SUB, G.t, in);
+    }
+    const int layers[3] = {LAYER0, LAYER0 + 1, LAYER0 + 2};
+    const int aoff[3] = {0, SUB, 2 * SUB};
+    const int dcol[3] = {DCOL, DCOL + (W <= 16 ? 16 : 32), DCOL + 2 * (W <= 16 ? 16 : 32)};
+    mma_round<EB>(G, layers, aoff, dcol, 3);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float d[32], xs[32];
+        read_cols<W>(G, dcol[c], d);
+        src.template load<FROM, W>(c, xs);
+        const int L = LAYER0 + c;
+#pragma unroll
+        for (int o = 0; o < W; ++o) {
+            float sc = EB == 1 ? rs[c] * __ldg(scales + scale_off(L) + o) : 1.0f;
+            float a = fmaxf(fmaf(d[o], sc, wl(w32, layer_b32(L) + o)), 0.0f);
+            if (WIDEN) prev[c][o] = a;
+            else prev[c][o] = a + xs[o];
+        }
+        if (WIDEN) {
+#pragma unroll
+            for (int i = 0; i < W; ++i) prev[c][W + i] = xs[i];
+        }
+    }
+}
+
+// Issues layer LAYER on the A row already in shared memory (row scale rs).
+template <int EB, int LAYER, int DCOL>
+MRP_D void tc_issue(Group& G) {
+    const int layers[1] = {LAYER}, aoff[1] = {0}, dcol[1] = {DCOL};
+    mma_round<EB>(G, layers, aoff, dcol, 1);
+}
+// relu(D*scale + b) of layer SRC (at DCOL) written as the A row of layer DST;
+// returns DST's row scale.
+template <int EB, int SRC, int DCOL, int DST>
+MRP_D float tc_chain(Group& G, const float* __restrict__ w32, const float* __restrict__ scales, float rs_src) {
+    constexpr int N = layer_n(SRC);
+    static_assert(N == layer_k(DST), "layer chain");
+    float d[N];
+    read_cols<N>(G, DCOL, d);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        float sc = EB == 1 ? rs_src * __ldg(scales + scale_off(SRC) + i) : 1.0f;
+        d[i] = fmaxf(fmaf(d[i], sc, wl(w32, layer_b32(SRC) + i)), 0.0f);
+    }
+    return write_row<EB, N, kpad(DST, EB)>(G.a, 0, G.t, d);
+}
+// relu(D*scale + b) of layer SRC into out[N].
+template <int EB, int SRC, int DCOL>
+MRP_D void tc_out(Group& G, const float* __restrict__ w32, const float* __restrict__ scales, float rs_src, float* out) {
+    constexpr int N = layer_n(SRC);
+    read_cols<N>(G, DCOL, out);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        float sc = EB == 1 ? rs_src * __ldg(scales + scale_off(SRC) + i) : 1.0f;
+        out[i] = fmaxf(fmaf(out[i], sc, wl(w32, layer_b32(SRC) + i)), 0.0f);
+    }
+}
+template <int EB, int K>
+MRP_D void tc_residual_pair(Group& G, const float* __restrict__ w32, const float* __restrict__ scales, float (&a16)[16]) {
+    float r0 = write_row<EB, 16, kpad(kLX0 + 2 * K, EB)>(G.a, 0, G.t, a16);
+    tc_issue<EB, kLX0 + 2 * K, 64>(G);
+    float r1 = tc_chain<EB, kLX0 + 2 * K, 64, kLX0 + 2 * K + 1>(G, w32, scales, r0);
+    tc_issue<EB, kLX0 + 2 * K + 1, 80>(G);
+    float z[16];
+    tc_out<EB, kLX0 + 2 * K + 1, 80>(G, w32, scales, r1, z);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a16[i] += z[i];
+}
+
+template <int EB, class Src>
+MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
+                      float gamma, float g, f3 sr, float out[3]) {
+    float hf[16];
+#pragma unroll
+    for (int o = 0; o < 16; ++o) hf[o] = 0.0f;
+    float prev[3][32];
+    // main branch, X[0:160]; finals leave comb[0:96) in TMEM columns 0..95
+    tc_block<EB, 8, 0, false, false, 0, 0>(G, src, w32, scales, main_block_off(0), 0, g, gamma, hf, prev);
+    tc_block<EB, 8, 8, true, true, 3, 0>(G, src, w32, scales, main_block_off(1), 3, g, gamma, hf, prev);
+    tc_block<EB, 16, 16, false, true, 6, 0>(G, src, w32, scales, main_block_off(2), 6, g, gamma, hf, prev);
+    tc_block<EB, 16, 32, false, true, 9, 0>(G, src, w32, scales, main_block_off(3), 9, g, gamma, hf, prev);
+    tc_block<EB, 16, 48, true, true, 12, 0>(G, src, w32, scales, main_block_off(4), 12, g, gamma, hf, prev);
+    tc_block<EB, 32, 64, false, true, 15, 0>(G, src, w32, scales, main_block_off(5), 15, g, gamma, hf, prev);
+    tc_block<EB, 32, 96, false, true, 18, 0>(G, src, w32, scales, main_block_off(6), 18, g, gamma, hf, prev);
+    tc_block<EB, 32, 128, false, true, 21, 0>(G, src, w32, scales, main_block_off(7), 21, g, gamma, hf, prev);
+    float rs_main[3];
+    {
+        constexpr int KP = kpad(kL81, EB), SUB = 128 * KP * EB;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rs_main[c] = write_row<EB, 32, KP>(G.a, c * SUB, G.t, prev[c]);
+        const int layers[3] = {kL81, kL81 + 1, kL81 + 2}, aoff[3] = {0, SUB, 2 * SUB}, dcol[3] = {0, 32, 64};
+        mma_round<EB>(G, layers, aoff, dcol, 3);
+    }
+    // direct-illumination branch, X[160:192]; finals at columns 176..223
+    tc_block<EB, 8, 160, false, false, 27, 128>(G, src, w32, scales, di_block_off(0), 24, g, gamma, hf, prev);
+    tc_block<EB, 8, 168, false, true, 30, 128>(G, src, w32, scales, di_block_off(1), 27, g, gamma, hf, prev);
+    tc_block<EB, 8, 176, false, true, 33, 128>(G, src, w32, scales, di_block_off(2), 30, g, gamma, hf, prev);
+    tc_block<EB, 8, 184, false, true, 36, 128>(G, src, w32, scales, di_block_off(3), 33, g, gamma, hf, prev);
+    float rs_di[3];
+    {
+        constexpr int KP = kpad(kLD41, EB), SUB = 128 * KP * EB;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rs_di[c] = write_row<EB, 8, KP>(G.a, c * SUB, G.t, prev[c]);
+        const int layers[3] = {kLD41, kLD41 + 1, kLD41 + 2}, aoff[3] = {0, SUB, 2 * SUB}, dcol[3] = {176, 192, 208};
+        mma_round<EB>(G, layers, aoff, dcol, 3);
+    }
+    // comb[120] = relu(finals + b): main (3 x 32) then direct illumination (3 x 8)
+    float comb[120];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float d[32];
+        read_cols<32>(G, 32 * c, d);
+#pragma unroll
+        for (int o = 0; o < 32; ++o) {
+            float sc = EB == 1 ? rs_main[c] * __ldg(scales + scale_off(kL81 + c) + o) : 1.0f;
+            comb[32 * c + o] = fmaxf(fmaf(d[o], sc, wl(w32, layer_b32(kL81 + c) + o)), 0.0f);
+        }
+        float e[16];
+        tc::tmem_ld16(G.tmem + 176 + 16 * c, e);
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            float se = EB == 1 ? rs_di[c] * __ldg(scales + scale_off(kLD41 + c) + o) : 1.0f;
+            comb[96 + 8 * c + o] = fmaxf(fmaf(e[o], se, wl(w32, layer_b32(kLD41 + c) + o)), 0.0f);
+        }
+    }
+    // tail, once per distinct albedo channel (core/radiancePredict.cu:375-419)
+    float srv[3] = {sr.x, sr.y, sr.z}, P[3];
+#pragma unroll 1
+    for (int ch = 0; ch < 3; ++ch) {
+        if (ch == 1 && srv[1] == srv[0]) { P[1] = P[0]; continue; }
+        if (ch == 2 && srv[2] == srv[0]) { P[2] = P[0]; continue; }
+        if (ch == 2 && srv[2] == srv[1]) { P[2] = P[1]; continue; }
+        float s4 = powf(srv[ch], 4.0f);
+        float h[16], gf[6];
+#pragma unroll
+        for (int o = 0; o < 16; ++o) {
+            float a = hf[o];
+            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 72), g, a);
+            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 73), gamma, a);
+            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 74), s4, a);
+            h[o] = fmaxf(a, 0.0f);
+        }
+#pragma unroll
+        for (int o = 0; o < 6; ++o) {
+            float a = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) a = fmaf(h[j], wl(w32, kLSEFin2W + o * 16 + j), a);
+            gf[o] = sigmoid_d(a);
+        }
+        float lg[8];
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            float a = 0.0f;
+            a = fmaf(g, wl(w32, kLGGSW + o * 3), a);
+            a = fmaf(gamma, wl(w32, kLGGSW + o * 3 + 1), a);
+            a = fmaf(s4, wl(w32, kLGGSW + o * 3 + 2), a);
+            lg[o] = fmaxf(a + wl(w32, kLGGSB + o), 0.0f);
+        }
+        // LC0's A row: [comb * gate segment, LGGS]
+        float r0 = write_row_fn<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, [&](int i) {
+            return i < 120 ? comb[i] * gf[i < 96 ? i / 32 : 3 + (i - 96) / 8] : lg[i - 120];
+        });
+        tc_issue<EB, kLC0, 0>(G);
+        float r1 = tc_chain<EB, kLC0, 0, kLC1>(G, w32, scales, r0);
+        tc_issue<EB, kLC1, 128>(G);
+        float r2 = tc_chain<EB, kLC1, 128, kLC2>(G, w32, scales, r1);
+        tc_issue<EB, kLC2, 0>(G);
+        float r3 = tc_chain<EB, kLC2, 0, kLX>(G, w32, scales, r2);
+        tc_issue<EB, kLX, 32>(G);
+        float a16[16];
+        tc_out<EB, kLX, 32>(G, w32, scales, r3, a16);
+        tc_residual_pair<EB, 0>(G, w32, scales, a16);
+        tc_residual_pair<EB, 1>(G, w32, scales, a16);
+        tc_residual_pair<EB, 2>(G, w32, scales, a16);
+        tc_residual_pair<EB, 3>(G, w32, scales, a16);
+        tc_residual_pair<EB, 4>(G, w32, scales, a16);
+        tc_residual_pair<EB, 5>(G, w32, scales, a16);
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) a = fmaf(a16[j], wl(w32, kLX12W + j), a);
+        P[ch] = fmaxf(a + wl(w32, kLX12B), 0.0f);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = fmaxf(expf(P[c]) - 1.0f, 0.0f) * powf(srv[c], 4.0f);
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+struct TcArgs {
+    const uint8_t* wimg;        // operand image (global)
+    int wimg_bytes;
+    const float* w32;           // fp32 packed weights
+    const float* scales;        // FP8 per-layer weight scales
+    int* err;
+    int* tile_counter;
+    // inputs: either row-major features [n][576] + gamma, or staged records
+    const float* feat;
+    const float* gamma;
+    int n;
+    const int* rec_count;
+    const int* rec_pix;
+    const float* rec_f;
+    size_t rec_cap;
+    float g;
+    f3 sr;
+    // outputs
+    float* out3;                // row-major [n][3]
+    float4* accum;              // staged: running mean at each record's pixel
+    f3 light_color, scatter_rate, ori;
+    int mean_k;
+};
+
+template <int EB, bool STAGED>
+__global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(TcArgs A) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int wbytes = (A.wimg_bytes + 1023) & ~1023;
+    uint8_t* wimg = smem;
+    uint8_t* abuf = smem + wbytes;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(abuf + kGroups * kABytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kGroups);
+    int* tile_slot = reinterpret_cast<int*>(tslot + 1);
+
+    const int tid = threadIdx.x, warp = tid / 32;
+    // weights -> shared memory
+    for (int i = tid * 16; i < A.wimg_bytes; i += blockDim.x * 16)
+        *reinterpret_cast<uint4*>(wimg + i) = __ldg(reinterpret_cast<const uint4*>(A.wimg + i));
+    if (warp == 0) {
+        tc::tmem_alloc(tslot, kGroups * kTmemColsPerGroup);
+        tc::tmem_relinquish();
+    }
+    if (tid < kGroups) tc::mbar_init(mbar + tid, 1);
+    tc::mbar_fence_init();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *tslot;
+
+    Group G;
+    G.g = tid / kGroupThreads;
+    G.t = tid % kGroupThreads;
+    G.a = abuf + G.g * kABytes;
+    G.wimg = wimg;
+    G.mbar = mbar + G.g;
+    G.phase = 0;
+    G.tmem_col0 = tbase + (uint32_t)(G.g * kTmemColsPerGroup);
+    G.tmem = G.tmem_col0 + ((uint32_t)(32 * ((tid / 32) % 4)) << 16);
+    G.err = A.err;
+    G.ok = true;
+
+    const int count = STAGED ? *A.rec_count : A.n;
+    for (;;) {
+        if (G.t == 0) tile_slot[G.g] = atomicAdd(A.tile_counter, 1);
+        group_bar(G.g);
+        int tile = tile_slot[G.g];
+        group_bar(G.g);
+        if (tile * 128 >= count || !G.ok) break;
+        int r = tile * 128 + G.t;
+        bool valid = r < count;
+        float o[3];
+        if (STAGED) {
+            float gamma = valid ? A.rec_f[15 * A.rec_cap + r] : 0.0f;
+            TileFeatures src{A.feat + (size_t)(r >> 5) * 576 * 32 + (r & 31), valid};
+            tc_network<EB>(G, src, A.w32, A.scales, gamma, A.g, A.sr, o);
+            if (valid && G.ok) {
+                int pix = A.rec_pix[r];
+                f3 hit = mk3(A.rec_f[r], A.rec_f[A.rec_cap + r], A.rec_f[2 * A.rec_cap + r]);
+                f3 res = mul(mul(mk3(o[0], o[1], o[2]), A.light_color), A.scatter_rate);
+                float4 v4 = make_float4(fmaxf(res.x, 0.0f), fmaxf(res.y, 0.0f), fmaxf(res.z, 0.0f),
+                                        fmaxf(length(sub(A.ori, hit)), 0.0f));
+                float rate = 1.0f / (float)(1 + A.mean_k);
+                float4 a = A.mean_k == 0 ? make_float4(0, 0, 0, 0) : A.accum[pix];
+                A.accum[pix] = make_float4(lerp(a.x, v4.x, rate), lerp(a.y, v4.y, rate), lerp(a.z, v4.z, rate),
+                                           lerp(a.w, v4.w, rate));
+            }
+        } else {
+            float gamma = valid ? A.gamma[r] : 0.0f;
+            RowFeatures src{A.feat + (size_t)r * 576, valid};
+            tc_network<EB>(G, src, A.w32, A.scales, gamma, A.g, A.sr, o);
+            if (valid && G.ok) {
+                A.out3[3 * (size_t)r] = o[0];
+                A.out3[3 * (size_t)r + 1] = o[1];
+                A.out3[3 * (size_t)r + 2] = o[2];
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tbase, kGroups * kTmemColsPerGroup);
+    }
+}
+
+static size_t tc_smem_bytes(int eb) {
+    return (size_t)((image_bytes(eb) + 1023) & ~1023) + kGroups * kABytes + kGroups * 8 + 16;
+}
+
+template <int EB, bool STAGED>
+static cudaError_t launch_tc(TcArgs& a, int sms, cudaStream_t s) {
+    size_t smem = tc_smem_bytes(EB);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<EB, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.tile_counter, 0, sizeof(int), s)) != cudaSuccess) return e;
+    k_mlp_tc<EB, STAGED><<<sms, kGroups * kGroupThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+static TcArgs base_args(const TcWeights& w, bool fp8) {
+    TcArgs a{};
+    a.wimg = (const uint8_t*)(fp8 ? w.d_fp8 : w.d_bf16);
+    a.wimg_bytes = image_bytes(fp8 ? 1 : 2);
+    a.w32 = w.d_fp32;
+    a.scales = w.d_scales;
+    a.err = w.d_err;
+    a.tile_counter = w.d_counter;
+    return a;
+}
+
+cudaError_t tc_launch_mlp(const TcWeights& w, bool fp8, const float* feat, const float* gamma, float g, const float sr[3],
+                          int n, float* out3, int sms, cudaStream_t s) {
+    if (!w.ready || !w.d_fp32) return cudaErrorNotReady;
+    TcArgs a = base_args(w, fp8);
+    a.feat = feat;
+    a.gamma = gamma;
+    a.n = n;
+    a.g = g;
+    a.sr = mk3(sr[0], sr[1], sr[2]);
+    a.out3 = out3;
+    return fp8 ? launch_tc<1, false>(a, sms, s) : launch_tc<2, false>(a, sms, s);
+}
+
+cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
+                              const HitRecords& rec, const float* feat, float4* accum, int sms, cudaStream_t s) {
+    if (!w.ready || !w.d_fp32) return cudaErrorNotReady;
+    TcArgs a = base_args(w, fp8);
+    a.feat = feat;
+    a.rec_count = rec.count;
+    a.rec_pix = rec.pix;
+    a.rec_f = rec.f;
+    a.rec_cap = rec.cap;
+    a.g = view.g;
+    a.sr = mk3(v.scatter_rate.x / 1.001f, v.scatter_rate.y / 1.001f, v.scatter_rate.z / 1.001f);
+    a.accum = accum;
+    a.light_color = view.light_color;
+    a.scatter_rate = v.scatter_rate;
+    a.ori = view.ori;
+    a.mean_k = view.mean_k;
+    return fp8 ? launch_tc<1, true>(a, sms, s) : launch_tc<2, true>(a, sms, s);
+}
+
+// ---------------------------------------------------------------------------
+// self-test: one M=128 GEMM D = A * B^T through the same descriptors
+// ---------------------------------------------------------------------------
+template <int EB>
+__global__ void __launch_bounds__(128, 1) k_tc_gemm_test(const float* __restrict__ A, const float* __restrict__ B,
+                                                         int n, int k, float* __restrict__ D, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int kp = k;   // multiple of 16 (BF16) / 32 (E4M3)
+    uint8_t* sa = smem;
+    uint8_t* sb = smem + 128 * kp * EB;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sb + 128 * kp * EB);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(mbar + 1);
+    int t = threadIdx.x;
+    if (t < 32) { tc::tmem_alloc(slot, 128); tc::tmem_relinquish(); }
+    if (t == 0) tc::mbar_init(mbar, 1);
+    tc::mbar_fence_init();
+    for (int idx = t; idx < 128 * kp; idx += 128) {
+        int m = idx / kp, kk = idx % kp;
+        float va = A[m * k + kk];
+        float vb = m < n ? B[m * k + kk] : 0.0f;
+        if (EB == 2) {
+            uint32_t pa = tc::pack_bf16(va, 0.0f), pb = tc::pack_bf16(vb, 0.0f);
+            *reinterpret_cast<unsigned short*>(sa + op_off(m, kk, kp, 2)) = (unsigned short)(pa & 0xFFFF);
+            *reinterpret_cast<unsigned short*>(sb + op_off(m, kk, kp, 2)) = (unsigned short)(pb & 0xFFFF);
+        } else {
+            sa[op_off(m, kk, kp, 1)] = (uint8_t)(tc::pack_e4m3(va, 0.0f) & 0xFF);
+            sb[op_off(m, kk, kp, 1)] = (uint8_t)(tc::pack_e4m3(vb, 0.0f) & 0xFF);
+        }
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    uint32_t tbase = *slot;
+    if (t == 0) {
+        uint32_t idesc = tc::instr_desc(128, n, EB == 2 ? tc::kFmtBF16 : tc::kFmtE4M3);
+        uint32_t sbo = (uint32_t)(kp * EB * 8);
+        for (int s = 0; s < kp * EB / 32; ++s) {
+            uint64_t ad = tc::smem_desc(tc::smem_addr(sa) + s * 256, 128, sbo);
+            uint64_t bd = tc::smem_desc(tc::smem_addr(sb) + s * 256, 128, sbo);
+            if (EB == 2) tc::mma_bf16(tbase, ad, bd, idesc, s > 0);
+            else tc::mma_fp8(tbase, ad, bd, idesc, s > 0);
+        }
+        tc::mma_commit(mbar);
+    }
+    bool ok = tc::mbar_wait(mbar, 0, kWaitLimit);
+    if (!ok && t == 0) atomicExch(err, 1);
+    tc::fence_after_sync();
+    if (ok) {
+        uint32_t lane_addr = tbase + ((uint32_t)(32 * (t / 32)) << 16);
+        for (int c0 = 0; c0 < n; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(lane_addr + c0, v);
+            for (int i = 0; i < 16; ++i) D[t * n + c0 + i] = v[i];
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) { tc::fence_after_sync(); tc::tmem_dealloc(tbase, 128); }
+}
+
+cudaError_t tc_gemm_test(bool fp8, const float* A, const float* B, int n, int k, float* D, int* err, cudaStream_t s) {
+    int eb = fp8 ? 1 : 2;
+    size_t smem = (size_t)2 * 128 * k * eb + 64;
+    cudaError_t e;
+    if (fp8) {
+        if ((e = cudaFuncSetAttribute(k_tc_gemm_test<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
+        k_tc_gemm_test<1><<<1, 128, smem, s>>>(A, B, n, k, D, err);
+    } else {
+        if ((e = cudaFuncSetAttribute(k_tc_gemm_test<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
+        k_tc_gemm_test<2><<<1, 128, smem, s>>>(A, B, n, k, D, err);
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace mrp

@@ -7,10 +7,12 @@ namespace mrp {
 
 // Weight images for the tensor-core kernels, built once per model.
 struct TcWeights {
-    void* d_bf16 = nullptr;    // packed BF16 operand tiles
-    void* d_fp8 = nullptr;     // packed FP8 operand tiles
-    float* d_scales = nullptr; // per-layer FP8 dequantisation scales
-    float* d_fp32 = nullptr;   // fp32 weights for the CUDA-core parts (gates)
+    void* d_bf16 = nullptr;    // BF16 operand images of the 58 tensor-core layers
+    void* d_fp8 = nullptr;     // FP8-E4M3 operand images (weights / per-layer scale)
+    float* d_scales = nullptr; // FP8 weight scales per output channel (row amax / 448)
+    const float* d_fp32 = nullptr;   // packed fp32 weights: gates, biases, LSEFin, LX12
+    int* d_err = nullptr;      // set to 1 when an MMA round times out
+    int* d_counter = nullptr;  // tile counter of the persistent kernel
     bool ready = false;
 };
 // Per-handle scratch of the tensor-core predictor.
@@ -28,5 +30,9 @@ cudaError_t tc_launch_mlp(const TcWeights& w, bool fp8, const float* feat, const
 struct HitRecords;
 cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
                               const HitRecords& rec, const float* feat, float4* accum, int sms, cudaStream_t s);
+
+// Self-test: D[128][n] = A[128][k] * B[n][k]^T with operands rounded to BF16
+// (or E4M3), k a multiple of 16 (32), n a multiple of 16 up to 128.
+cudaError_t tc_gemm_test(bool fp8, const float* A, const float* B, int n, int k, float* D, int* err, cudaStream_t s);
 
 }  // namespace mrp
