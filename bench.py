@@ -214,6 +214,55 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+TRACER = dict(res=128, seed=0, freq=4.0, size=256, spp=16, bounces=256, bake_res=768)
+
+
+def run_tracer(args, local):
+    """The delta-tracking path tracer on its own workload: 128^3 fBm (seed 0,
+    freq 4), 256x256, 16 spp, <= 256 bounces, NEE through the 768^3 baked
+    transmittance grid.  Returns a dict for the JSON line."""
+    import torch
+
+    import mrpnn_b200 as M
+    vol = M.VolumeRender(TRACER["res"])
+    vol.generate_fbm(TRACER["seed"], TRACER["freq"])
+    vol.Update()
+    vol.SetScatterRate(SCENE["albedo"])
+    vol.SetSky(SCENE["sky"])
+    vol.SetBakeResolution(TRACER["bake_res"])
+    L = light()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    vol.Update_CachedTR(L, SCENE["alpha"])
+    bake_s = time.perf_counter() - t0
+    ori, up, right = view_vectors()
+    n = TRACER["size"]
+    view = vol.make_view((n, n), ori, up, right, L, SCENE["g"], SCENE["alpha"], multiScatter=TRACER["bounces"],
+                         spp=TRACER["spp"], seed=7)
+    out = torch.empty((n, n, 4), dtype=torch.float32, device=f"cuda:{local}")
+    vol.render_view(view, M.VolumeRender.PT, 1, out)
+    ms = []
+    for k in range(args.tracer_steps):
+        view.frame_offset = 10 + k
+        vol.render_view(view, M.VolumeRender.PT, 1, out)
+        ms.append(vol.last_render_ms())
+    cnt = vol.render_counters(view, M.VolumeRender.PT)   # bounces, fetches, NEE lookups, samples
+    t = float(np.mean(ms))
+    trace_ms = vol.last_render_stages()[0]
+    hbm, _, peak_kind = peaks()
+    alg = (cnt[1] + cnt[2]) * 32 + n * n * 16
+    ach = alg / (trace_ms / 1000.0) / 1e9
+    return {"workload": f"PT {n}x{n}, {TRACER['spp']} spp, <= {TRACER['bounces']} bounces, "
+                        f"{TRACER['res']}^3 fBm (seed 0, freq 4), NEE via {TRACER['bake_res']}^3 baked TR",
+            "ms_per_frame": t, "samples_per_s": n * n * TRACER["spp"] / (t / 1000.0),
+            "density_lookups_per_s": (cnt[1] + cnt[2]) / (trace_ms / 1000.0),
+            "counters": {"bounces": cnt[0], "free_flight_fetches": cnt[1], "nee_lookups": cnt[2], "samples": cnt[3]},
+            "bake_s": bake_s,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "note": f"trace kernel; algorithmic bytes = (fetches + NEE lookups) x 32 B (8 fp32 texels) "
+                                 f"+ 16 B/pixel; peak {peak_kind}; the 8 MiB volume is L2-resident"}}
+
+
 STAGES = ("first hit + bases", "stencil gather", "network")
 # Algorithmic HBM bytes per hit pixel of each predictor stage (fp32 data):
 #   gather : 192 points x (8 density + 8 TR + 2 x 4 LUT texels) x 4 B read,
@@ -312,6 +361,8 @@ def run_mine(args, rank, world, local):
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": traffic,
                 "kernel": STAGES[dom], "note": "march lookups are data dependent; see profiles/"}
 
+    tracer = run_tracer(args, local) if (rank == 0 and args.tracer_steps > 0) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sc = cpu_scene_from_gpu(vol)
@@ -334,6 +385,7 @@ def run_mine(args, rank, world, local):
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
+            "tracer": tracer,
         }
         print(json.dumps(line), flush=True)
 
@@ -349,6 +401,7 @@ def main():
     ap.add_argument("--ref-pixels", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=1024, help="frame edge (the headline workload is 1024)")
+    ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
     args = ap.parse_args()
     global W, H
     W = H = args.size

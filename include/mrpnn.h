@@ -155,6 +155,12 @@ mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float al
  * width*height float4 (RGB, A = coverage for PT / hit distance for MRPNN). */
 mrp_status mrp_render(mrp_volume* v, const mrp_view* view, mrp_render_type type, int sample_num, float* out_rgba,
                       int out_is_device);
+/* One launch of mrp_render (output discarded) that also counts its work:
+ * MRPNN: [0] march steps, [1] density fetches (steps not skipped by the
+ * occupancy bricks), [2] stencil points gathered, [3] hit pixels;
+ * PT: [0] bounces, [1] free-flight density fetches, [2] NEE transmittance
+ * lookups, [3] samples traced.  For roofline accounting; not timed. */
+mrp_status mrp_render_counters(mrp_volume* v, const mrp_view* view, mrp_render_type type, unsigned long long counters[4]);
 /* Device time of the kernels of the last mrp_render on this handle (ms;
  * -1 when it ran more than one launch -- see mrp_last_render_stages). */
 mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms);

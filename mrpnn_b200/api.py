@@ -75,6 +75,7 @@ _SIGS = {
     "mrp_render": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_last_render_ms": ([C.c_void_p, C.POINTER(C.c_float)], C.c_int),
     "mrp_last_render_stages": ([C.c_void_p, C.POINTER(C.c_float)], C.c_int),
+    "mrp_render_counters": ([C.c_void_p, C.POINTER(View), C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
     "mrp_predict_features": ([C.c_void_p, C.c_void_p, C.c_float, F3, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "mrp_gather_features": ([C.c_void_p, C.c_void_p, C.c_void_p, F3, C.c_float, C.c_float, C.c_int, C.c_void_p,
                              C.c_void_p, C.c_int], C.c_int),
@@ -329,6 +330,11 @@ class VolumeRender:
         ms = C.c_float()
         _check(lib().mrp_last_render_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def render_counters(self, view, rt):
+        c = (C.c_ulonglong * 4)()
+        _check(lib().mrp_render_counters(self._h, C.byref(view), int(rt), c))
+        return [int(x) for x in c]
 
     def last_render_stages(self):
         ms = (C.c_float * 3)()

@@ -660,7 +660,32 @@ static ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int 
     return d;
 }
 
+static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out,
+                              int out_is_device, unsigned long long* counters);
+
 mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out, int out_is_device) {
+    return render_impl(v, w, type, sample_num, out, out_is_device, nullptr);
+}
+
+mrp_status mrp_render_counters(mrp_volume* v, const mrp_view* w, mrp_render_type type, unsigned long long counters[4]) {
+    TRY(need_init());
+    if (!counters) return fail(MRP_ERR_INVALID, "null argument");
+    unsigned long long* d = nullptr;
+    CU(cudaMalloc(&d, 4 * sizeof(unsigned long long)));
+    cudaMemset(d, 0, 4 * sizeof(unsigned long long));
+    float* out = nullptr;
+    size_t npix = (size_t)std::max(w ? w->width : 0, 0) * std::max(w ? w->height : 0, 0);
+    if (cudaMalloc(&out, std::max<size_t>(npix, 1) * 16) != cudaSuccess) { cudaFree(d); return fail(MRP_ERR_OOM, "counters"); }
+    mrp_status st = render_impl(v, w, type, 1, out, 1, d);
+    if (st == MRP_OK && cudaMemcpy(counters, d, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = fail(MRP_ERR_CUDA, "counters readback");
+    cudaFree(d);
+    cudaFree(out);
+    return st;
+}
+
+static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out,
+                              int out_is_device, unsigned long long* counters) {
     TRY(need_init());
     if (!v || !w || !out) return fail(MRP_ERR_INVALID, "null argument");
     if (w->width <= 0 || w->height <= 0 || (long long)w->width * w->height > (1ll << 28))
@@ -701,6 +726,7 @@ mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, in
     CU(cudaEventRecord(v->ev0, v->stream));
     for (int i = 0; i < sample_num; ++i) {
         ViewDev vd = make_view(v, w, w->frame_offset + i, i);
+        vd.counters = counters;
         bool last = i == sample_num - 1;
         if (type == MRP_MRPNN) {
             HitRecords rec = v->records();

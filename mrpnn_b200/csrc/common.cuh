@@ -215,7 +215,19 @@ struct ViewDev {
     int frame;         // RNG launch index ("randNum")
     int mean_k;        // running-mean index of this launch ("frameNum")
     float pass_rate;   // exp(-(2/res) * max_density * alpha), host libm (DeterminateEstimatedHit)
+    unsigned long long* counters;   // optional work counters (see launch_hit / launch_trace), else null
 };
+
+// Per-thread work tally, flushed to ViewDev::counters once per thread.
+struct Tally {
+    uint32_t steps = 0, fetches = 0, lookups = 0, events = 0;
+};
+MRP_D void flush_tally(unsigned long long* c, const Tally& t) {
+    atomicAdd(c + 0, (unsigned long long)t.steps);
+    atomicAdd(c + 1, (unsigned long long)t.fetches);
+    atomicAdd(c + 2, (unsigned long long)t.lookups);
+    atomicAdd(c + 3, (unsigned long long)t.events);
+}
 
 // ---------------------------------------------------------------------------
 // Packed MLP weight layout (fp32, one buffer).  Per SE block: the gate MLP

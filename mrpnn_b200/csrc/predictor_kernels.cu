@@ -53,7 +53,7 @@ MRP_D f3 camera_ray(const ViewDev& w, int row, int col) {
 // texels (0), and a base inside reads voxels base..base+1, which lie in the
 // 1-voxel apron of its brick.  lerp(0, 0, w) is exactly +0, so the skip
 // returns the value the fetch would.
-MRP_D float density_skip(const VolumeDev& v, f3 p) {
+MRP_D float density_skip(const VolumeDev& v, f3 p, Tally* tl) {
     f3 uv = adds(p, 0.5f);
     float nf = (float)v.res;
     int x = (int)floorf(fs(fm(uv.x, nf), 0.5f)), y = (int)floorf(fs(fm(uv.y, nf), 0.5f)),
@@ -63,12 +63,14 @@ MRP_D float density_skip(const VolumeDev& v, f3 p) {
     int nb = v.occ_res;
     int b = ((max(x, 0) >> v.occ_shift) * nb + (max(y, 0) >> v.occ_shift)) * nb + (max(z, 0) >> v.occ_shift);
     if (__ldg(v.occ + b) == 0) return 0.0f;
+    if (tl) tl->fetches++;
     return tex3<false>(v.density, v.res, p);
 }
 
 // DeterminateEstimatedHit(float& alpha, ...) (core/render.cuh:105-197).
 // pass_rate = exp(-t_step * SMax) is computed once on the host.
-MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 pos, f3 dir, float dis, f3* next) {
+MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 pos, f3 dir, float dis, f3* next,
+                         Tally* tl = nullptr) {
     float smax = fm(v.max_density, alpha);
     float t = 0.0f, last_non_empty_t = 0.0f, prob = 1.0f, last_dens = 0.0f;
     float rf = (float)v.res;
@@ -80,7 +82,14 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
             *next = mk3(0, 0, 0);
             return false;
         }
-        float d = v.occ ? density_skip(v, add(pos, mul(dir, t))) : density(v, add(pos, mul(dir, t)));
+        if (tl) tl->steps++;
+        float d;
+        if (v.occ) {
+            d = density_skip(v, add(pos, mul(dir, t)), tl);
+        } else {
+            d = density(v, add(pos, mul(dir, t)));
+            if (tl) tl->fetches++;
+        }
         if (d > 0) {
             float S = fm(d, alpha);
             float step_p = fa(pass_rate, fm(fs(1.0f, pass_rate), fs(1.0f, fd(S, smax))));
@@ -117,7 +126,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
 }
 
 // GetSamplePoint (core/render.cuh:436-462)
-MRP_D bool first_hit(const VolumeDev& v, f3 ori, f3 dir, float alpha, float pass_rate, f3* hit) {
+MRP_D bool first_hit(const VolumeDev& v, f3 ori, f3 dir, float alpha, float pass_rate, f3* hit, Tally* tl = nullptr) {
     dir = normalize(dir);
     *hit = mk3(0, 0, 0);
     float dis = ray_box_offset(ori, dir);
@@ -125,7 +134,7 @@ MRP_D bool first_hit(const VolumeDev& v, f3 ori, f3 dir, float alpha, float pass
     f3 sp = add(ori, mul(dir, dis));
     float md = ray_box_distance(sp, dir);
     f3 p;
-    bool in = estimated_hit(v, alpha, pass_rate, sp, dir, md, &p);
+    bool in = estimated_hit(v, alpha, pass_rate, sp, dir, md, &p, tl);
     if (in) *hit = p;
     return in;
 }
@@ -485,7 +494,9 @@ MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
     accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
 }
 
+template <bool COUNT>
 __global__ void __launch_bounds__(256) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
+    Tally tally;
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
     int npix = w.width * w.height;
     bool valid = pix < npix;
@@ -496,7 +507,12 @@ __global__ void __launch_bounds__(256) k_hit(VolumeDev v, ViewDev w, HitRecords 
         f3 dir = normalize(camera_ray(w, row, col));        // NNPredict: dir = normalize(dir)
         f3 L = normalize(w.light_dir);
         Stream st(kPixelStream, (uint32_t)pix, 0, (uint32_t)w.frame, w.seed);   // InitRand again
-        active = first_hit(v, w.ori, dir, w.alpha, w.pass_rate, &hit);
+        active = first_hit(v, w.ori, dir, w.alpha, w.pass_rate, &hit, COUNT ? &tally : nullptr);
+        if (COUNT) {
+            tally.events += active ? 1 : 0;
+            tally.lookups += active ? 192 : 0;
+            flush_tally(w.counters, tally);
+        }
         f3 LY, LZ;
         basis(dir, 0.1f, st, &X, &Y, &Z);
         basis(L, 0.1f, st, &LX, &LY, &LZ);
@@ -605,7 +621,8 @@ cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, 
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(rec.count, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    k_hit<<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
+    if (view.counters) k_hit<true><<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
+    else k_hit<false><<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
     return cudaGetLastError();
 }
 cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s) {

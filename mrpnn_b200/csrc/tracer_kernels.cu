@@ -21,7 +21,7 @@ MRP_D float density_t(const VolumeDev& v, f3 p) { return tex3<false>(v.density, 
 // DeterminateNextVertex.  SampleHenyeyGreenstein(Rand, Rand, ...) takes the
 // first draw as e1 and the second as e0 (x86-64 g++ argument order).
 MRP_D bool next_vertex(const VolumeDev& v, Stream& st, float alpha, float g, f3 pos, f3 dir, float dis, f3* npos,
-                       f3* ndir) {
+                       f3* ndir, Tally* tl) {
     float smax = fm(v.max_density, alpha);
     float t = 0.0f;
     int loop = 0;
@@ -31,6 +31,7 @@ MRP_D bool next_vertex(const VolumeDev& v, Stream& st, float alpha, float g, f3 
         if (t > dis) { *npos = mk3(0, 0, 0); *ndir = mk3(0, 0, 0); return false; }
         rk = st.next();
         float d = density_t(v, add(pos, mul(dir, t)));
+        if (tl) tl->fetches++;
         float S = fm(d, alpha);
         if (fd(S, smax) > rk) break;
         if (d < 0) t = fs(t, d);
@@ -53,14 +54,15 @@ MRP_D f3 camera_ray_t(const ViewDev& w, int row, int col) {
 }
 
 // Radiance of sample k of one pixel (CalculateRadiance's loop body).
-MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 ori, f3 dir, float dis, f3 L) {
+MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 ori, f3 dir, float dis, f3 L, Tally* tl) {
     Stream st(kPixelStream, (uint32_t)pix, (uint32_t)k, (uint32_t)w.frame, w.seed);
     f3 res = mk3(0, 0, 0);
     f3 p = add(ori, mul(dir, dis)), rd = dir, csr = mk3(1, 1, 1);
     for (int b = 0; b < w.multi_scatter; ++b) {
         f3 np, nd;
         float md = ray_box_distance(p, rd);
-        if (!next_vertex(v, st, w.alpha, w.g, p, rd, md, &np, &nd)) {
+        if (tl) tl->steps++;
+        if (!next_vertex(v, st, w.alpha, w.g, p, rd, md, &np, &nd, tl)) {
             res = add(res, mul(v.sky, csr));
             break;
         }
@@ -68,18 +70,21 @@ MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 o
         csr = mul(csr, v.scatter_rate);
         float ph = hg(dot(rd, L), w.g);
         float tr = tex3<true>(v.baked, v.baked_res, p);
+        if (tl) tl->lookups++;
         res = add(res, mul(mul(w.light_color, csr), fm(tr, ph)));
         rd = nd;
     }
     return res;
 }
 
+template <bool COUNT>
 __global__ void __launch_bounds__(128) k_trace(VolumeDev v, ViewDev w, double* __restrict__ sum3,
                                                double* __restrict__ sumsq3, int* __restrict__ first_pos,
                                                unsigned long long* __restrict__ counter) {
     const long long total = (long long)w.width * w.height * w.spp;
     const int npix = w.width * w.height;
     f3 L = normalize(w.light_dir);
+    Tally tally;
     for (;;) {
         long long item;
         // one atomic per warp, items handed out in warp-sized runs
@@ -99,7 +104,8 @@ __global__ void __launch_bounds__(128) k_trace(VolumeDev v, ViewDev w, double* _
         if (dis < 0) {
             r = v.sky;   // SkyBox(dir), coverage stays 0
         } else {
-            r = trace_sample(v, w, pix, k, w.ori, dir, dis, L);
+            r = trace_sample(v, w, pix, k, w.ori, dir, dis, L, COUNT ? &tally : nullptr);
+            if (COUNT) tally.events++;
             if (r.x > 0 || r.y > 0 || r.z > 0) atomicMin(first_pos + pix, k);
         }
         atomicAdd(sum3 + 3 * pix, (double)r.x);
@@ -111,6 +117,7 @@ __global__ void __launch_bounds__(128) k_trace(VolumeDev v, ViewDev w, double* _
             atomicAdd(sumsq3 + 3 * pix + 2, (double)r.z * r.z);
         }
     }
+    if (COUNT) flush_tally(w.counters, tally);
 }
 
 // (mean radiance, coverage) of the launch, then the running mean over
@@ -143,7 +150,8 @@ cudaError_t launch_fill_int(int* p, int n, int value, cudaStream_t s) {
 
 cudaError_t launch_trace(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
                          unsigned long long* counter, int sms, cudaStream_t s) {
-    k_trace<<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    if (view.counters) k_trace<true><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    else k_trace<false><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
     return cudaGetLastError();
 }
 cudaError_t launch_trace_resolve(const double* sum3, const int* first_pos, int npix, int spp, int frame, float4* accum,
