@@ -114,6 +114,7 @@ static uint8_t e4m3_bits(float f) {
     return s | (uint8_t)((vex + 7) << 3) | mant;
 }
 
+static cudaError_t upload_layer_descs();
 cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
     std::vector<uint8_t> img16(image_bytes(2), 0), img8(image_bytes(1), 0);
     // FP8: each output channel (weight row) scaled by its own amax / 448
@@ -144,6 +145,7 @@ cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
     if ((e = cudaMemcpy(w.d_scales, scales.data(), kScaleCount * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
         return e;
     if ((e = cudaMemset(w.d_err, 0, sizeof(int))) != cudaSuccess) return e;
+    if ((e = upload_layer_descs()) != cudaSuccess) return e;
     w.ready = true;
     return cudaSuccess;
 }
@@ -155,13 +157,46 @@ void tc_free_scratch(TcScratch& s) {
 }
 
 // ---------------------------------------------------------------------------
-// device: group synchronisation and one MMA round
+// device: layer descriptors, group synchronisation, one MMA round
+//
+// Code size matters here: the whole network runs inside one kernel and two
+// groups execute different layers at once, so every layer of one shape
+// shares one routine and takes its layer index at run time from a constant
+// table (instead of one template instance per layer).
 // ---------------------------------------------------------------------------
 constexpr int kGroupThreads = 128;
 constexpr int kGroups = 2;
 constexpr int kTmemColsPerGroup = 256;
 constexpr uint32_t kWaitLimit = 1u << 22;   // polls before an MMA round is declared lost
 constexpr int kABytes = 128 * 128 * 2;      // one group's A buffer (largest: 128 x 128 BF16)
+
+struct LayerDesc {
+    int b_off[2];   // byte offset of the weight image, [0] BF16, [1] E4M3
+    int kp[2];      // padded K
+    int n, np;      // logical / padded N
+    int b32;        // fp32 bias offset (packed weights)
+    int soff;       // FP8 scale offset
+};
+__constant__ LayerDesc c_layer_desc[kLayers];
+
+static void fill_layer_descs(LayerDesc* d) {
+    for (int i = 0; i < kLayers; ++i) {
+        d[i].b_off[0] = layer_off(i, 2);
+        d[i].b_off[1] = layer_off(i, 1);
+        d[i].kp[0] = kpad(i, 2);
+        d[i].kp[1] = kpad(i, 1);
+        d[i].n = layer_n(i);
+        d[i].np = npad(i);
+        d[i].b32 = layer_b32(i);
+        d[i].soff = scale_off(i);
+    }
+}
+
+static cudaError_t upload_layer_descs() {
+    LayerDesc descs[kLayers];
+    fill_layer_descs(descs);
+    return cudaMemcpyToSymbol(c_layer_desc, descs, sizeof descs);
+}
 
 __device__ __forceinline__ void group_bar(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory");
@@ -179,27 +214,34 @@ struct Group {
     bool ok;
 };
 
-// One MMA per (layer, A sub-tile, D column); issued after all A rows are in
-// shared memory, awaited by the whole group.
+// Up to three MMAs (layer, A sub-tile byte offset, D column), issued after
+// all A rows are in shared memory and awaited by the whole group.
 template <int EB>
-__device__ __forceinline__ void mma_round(Group& G, const int* layers, const int* a_off, const int* dcol, int count) {
+__device__ __noinline__ void mma_round(Group& G, int count, int l0, int a0, int d0, int l1, int a1, int d1, int l2,
+                                       int a2, int d2) {
     tc::fence_proxy_async();
     tc::fence_before_sync();
     group_bar(G.g);
     if (G.t == 0) {
         tc::fence_after_sync();
         uint32_t abase = tc::smem_addr(G.a), wbase = tc::smem_addr(G.wimg);
+        const int e = EB == 2 ? 0 : 1;
+#pragma unroll 1
         for (int q = 0; q < count; ++q) {
-            int L = layers[q];
-            int kp = kpad(L, EB);
-            uint32_t idesc = tc::instr_desc(128, npad(L), EB == 2 ? tc::kFmtBF16 : tc::kFmtE4M3);
+            int L = q == 0 ? l0 : (q == 1 ? l1 : l2);
+            int ao = q == 0 ? a0 : (q == 1 ? a1 : a2);
+            int dc = q == 0 ? d0 : (q == 1 ? d1 : d2);
+            int kp = c_layer_desc[L].kp[e];
+            uint32_t idesc = tc::instr_desc(128, c_layer_desc[L].np, EB == 2 ? tc::kFmtBF16 : tc::kFmtE4M3);
             uint32_t sbo = (uint32_t)(kp * EB * 8);
             int steps = kp * EB / 32;   // 32 bytes of K per MMA (16 BF16 / 32 E4M3)
+            uint32_t bb = wbase + (uint32_t)c_layer_desc[L].b_off[e];
+#pragma unroll 1
             for (int s = 0; s < steps; ++s) {
-                uint64_t ad = tc::smem_desc(abase + a_off[q] + s * 256, 128, sbo);
-                uint64_t bd = tc::smem_desc(wbase + layer_off(L, EB) + s * 256, 128, sbo);
-                if (EB == 2) tc::mma_bf16(G.tmem_col0 + dcol[q], ad, bd, idesc, s > 0);
-                else tc::mma_fp8(G.tmem_col0 + dcol[q], ad, bd, idesc, s > 0);
+                uint64_t ad = tc::smem_desc(abase + ao + s * 256, 128, sbo);
+                uint64_t bd = tc::smem_desc(bb + s * 256, 128, sbo);
+                if (EB == 2) tc::mma_bf16(G.tmem_col0 + dc, ad, bd, idesc, s > 0);
+                else tc::mma_fp8(G.tmem_col0 + dc, ad, bd, idesc, s > 0);
             }
         }
         tc::mma_commit(G.mbar);
@@ -248,39 +290,7 @@ __device__ __forceinline__ float write_row(uint8_t* a, int off, int row, const f
     return s;
 }
 
-// Same from a value functor f(i), i < N (evaluated twice for FP8: amax, then quantise).
-template <int EB, int N, int KP, class F>
-__device__ __forceinline__ float write_row_fn(uint8_t* a, int off, int row, F f) {
-    float inv = 1.0f, s = 1.0f;
-    if (EB == 1) {
-        float amax = 0.0f;
-#pragma unroll
-        for (int i = 0; i < N; ++i) amax = fmaxf(amax, fabsf(f(i)));
-        s = amax > 0.0f ? amax * (1.0f / 448.0f) : 1.0f;
-        inv = 1.0f / s;
-    }
-    constexpr int E = 16 / EB;
-#pragma unroll
-    for (int c = 0; c < KP / E; ++c) {
-        uint32_t w[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (EB == 2) {
-                int i0 = c * 8 + 2 * q;
-                w[q] = tc::pack_bf16(i0 < N ? f(i0) : 0.0f, i0 + 1 < N ? f(i0 + 1) : 0.0f);
-            } else {
-                int i0 = c * 16 + 4 * q;
-                float x0 = i0 < N ? f(i0) * inv : 0.0f, x1 = i0 + 1 < N ? f(i0 + 1) * inv : 0.0f;
-                float x2 = i0 + 2 < N ? f(i0 + 2) * inv : 0.0f, x3 = i0 + 3 < N ? f(i0 + 3) * inv : 0.0f;
-                w[q] = (uint32_t)tc::pack_e4m3(x0, x1) | ((uint32_t)tc::pack_e4m3(x2, x3) << 16);
-            }
-        }
-        *reinterpret_cast<uint4*>(a + off + op_off(row, c * E, KP, EB)) = make_uint4(w[0], w[1], w[2], w[3]);
-    }
-    return s;
-}
-
-// Reads N (<= 128, multiple of 16 or 8) accumulator columns of this thread's row.
+// Reads N (<= 128) accumulator columns of this thread's row.
 template <int N>
 __device__ __forceinline__ void read_cols(const Group& G, int col, float* out) {
 #pragma unroll
@@ -296,56 +306,72 @@ __device__ __forceinline__ void read_cols(const Group& G, int col, float* out) {
 MRP_D float wl(const float* __restrict__ w, int i) { return __ldg(w + i); }
 MRP_D float sigmoid_d(float o) { return 1.0f / (1.0f + __expf(-o)); }
 
-// Feature sources (rows may be invalid: zeros).
+// relu(D * scale + b) for N columns of layer L (runtime), in place.
+template <int EB, int N>
+MRP_D void bias_relu(float* d, int L, float rs, const float* __restrict__ w32, const float* __restrict__ scales) {
+    const int b32 = c_layer_desc[L].b32, so = c_layer_desc[L].soff;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        float sc = EB == 1 ? rs * __ldg(scales + so + i) : 1.0f;
+        d[i] = fmaxf(fmaf(d[i], sc, wl(w32, b32 + i)), 0.0f);
+    }
+}
+
+// Feature sources (rows may be invalid: zeros); FROM is a run-time offset.
 struct RowFeatures {           // [n][576] row-major
     const float* x;
     bool valid;
-    template <int FROM, int W>
-    MRP_D void load(int c, float (&xs)[32]) const {
+    template <int W>
+    MRP_D void load(int c, int from, float (&xs)[32]) const {
 #pragma unroll
-        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + c * 192 + FROM + i) : 0.0f;
+        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + c * 192 + from + i) : 0.0f;
     }
 };
 struct TileFeatures {          // tiled layout of the staged predictor
     const float* x;
     bool valid;
-    template <int FROM, int W>
-    MRP_D void load(int c, float (&xs)[32]) const {
+    template <int W>
+    MRP_D void load(int c, int from, float (&xs)[32]) const {
 #pragma unroll
-        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + (c * 192 + FROM + i) * 32) : 0.0f;
+        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + (c * 192 + from + i) * 32) : 0.0f;
     }
 };
 
-// One SE block over the three channels: gate from the slice pools, then the
-// branch layers on the tensor cores.  prev/nxt hold the residual state.
-template <int EB, int W, int FROM, bool WIDEN, bool HAS_PREV, int LAYER0, int DCOL, class Src>
-MRP_D void tc_block(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
-                    int se_off, int pid, float g, float gamma, float (&hf)[16], float (&prev)[3][32]) {
+// One SE block over the three channels (SE / SERES + ADD3 / REP3,
+// core/radiancePredict.cu:240-294): gate from the slice pools, branch layers
+// l0..l0+2 on the tensor cores (D at dcol, dcol+stride, dcol+2*stride), then
+// prev <- relu(D + b) + slice (ADD3) or concat(relu(D + b), slice) (REP3).
+template <int EB, int W, class Src>
+__device__ __noinline__ void tc_block(Group& G, const Src& src, const float* __restrict__ w32,
+                                      const float* __restrict__ scales, int from, int widen, int has_prev, int l0,
+                                      int dcol, int se_off, int pid, float g, float gamma, float (&hf)[16],
+                                      float (&prev)[3][32]) {
     constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
     constexpr int SUB = 128 * KP * EB;   // bytes of one branch's A sub-tile
+    constexpr int DSTR = W <= 16 ? 16 : 32;
     float p8[8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float xs[32];
-        src.template load<FROM, W>(c, xs);
+        src.template load<W>(c, from, xs);
         float s = 0.0f, m = -10000.0f;
 #pragma unroll
         for (int i = 0; i < W; ++i) { s += xs[i]; m = fmaxf(m, xs[i]); }
-        s = s / (float)W;
-        p8[c] = s;
+        p8[c] = s / (float)W;
         p8[3 + c] = m;
     }
     p8[6] = g;
     p8[7] = gamma;
     // LSEFin1 (75 -> 16) accumulated block by block: pool[pid + c] = avg,
     // pool[36 + pid + c] = max
-#pragma unroll
+#pragma unroll 4
     for (int o = 0; o < 16; ++o) {
         float a = hf[o];
+        const float* w1 = w32 + kLSEFin1W + o * 75 + pid;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            a = fmaf(wl(w32, kLSEFin1W + o * 75 + pid + c), p8[c], a);
-            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 36 + pid + c), p8[3 + c], a);
+            a = fmaf(__ldg(w1 + c), p8[c], a);
+            a = fmaf(__ldg(w1 + 36 + c), p8[3 + c], a);
         }
         hf[o] = a;
     }
@@ -368,77 +394,68 @@ MRP_D void tc_block(Group& G, const Src& src, const float* __restrict__ w32, con
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float xs[32], in[32];
-        src.template load<FROM, W>(c, xs);
+        src.template load<W>(c, from, xs);
 #pragma unroll
-        for (int i = 0; i < W; ++i) in[i] = HAS_PREV ? fmaf(xs[i], gate[c], prev[c][i]) : xs[i] * gate[c];
+        for (int i = 0; i < W; ++i) in[i] = has_prev ? fmaf(xs[i], gate[c], prev[c][i]) : xs[i] * gate[c];
         rs[c] = write_row<EB, W, KP>(G.a, c * SUB, G.t, in);
     }
-    const int layers[3] = {LAYER0, LAYER0 + 1, LAYER0 + 2};
-    const int aoff[3] = {0, SUB, 2 * SUB};
-    const int dcol[3] = {DCOL, DCOL + (W <= 16 ? 16 : 32), DCOL + 2 * (W <= 16 ? 16 : 32)};
-    mma_round<EB>(G, layers, aoff, dcol, 3);
+    mma_round<EB>(G, 3, l0, 0, dcol, l0 + 1, SUB, dcol + DSTR, l0 + 2, 2 * SUB, dcol + 2 * DSTR);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float d[32], xs[32];
-        read_cols<W>(G, dcol[c], d);
-        src.template load<FROM, W>(c, xs);
-        const int L = LAYER0 + c;
+        read_cols<W>(G, dcol + c * DSTR, d);
+        bias_relu<EB, W>(d, l0 + c, rs[c], w32, scales);
+        src.template load<W>(c, from, xs);
+        if (widen) {
 #pragma unroll
-        for (int o = 0; o < W; ++o) {
-            float sc = EB == 1 ? rs[c] * __ldg(scales + scale_off(L) + o) : 1.0f;
-            float a = fmaxf(fmaf(d[o], sc, wl(w32, layer_b32(L) + o)), 0.0f);
-            if (WIDEN) prev[c][o] = a;
-            else prev[c][o] = a + xs[o];
-        }
-        if (WIDEN) {
+            for (int o = 0; o < W; ++o) { prev[c][o] = d[o]; prev[c][W + o] = xs[o]; }
+        } else {
 #pragma unroll
-            for (int i = 0; i < W; ++i) prev[c][W + i] = xs[i];
+            for (int o = 0; o < W; ++o) prev[c][o] = d[o] + xs[o];
         }
     }
 }
 
-// Issues layer LAYER on the A row already in shared memory (row scale rs).
-template <int EB, int LAYER, int DCOL>
-MRP_D void tc_issue(Group& G) {
-    const int layers[1] = {LAYER}, aoff[1] = {0}, dcol[1] = {DCOL};
-    mma_round<EB>(G, layers, aoff, dcol, 1);
-}
-// relu(D*scale + b) of layer SRC (at DCOL) written as the A row of layer DST;
-// returns DST's row scale.
-template <int EB, int SRC, int DCOL, int DST>
-MRP_D float tc_chain(Group& G, const float* __restrict__ w32, const float* __restrict__ scales, float rs_src) {
-    constexpr int N = layer_n(SRC);
-    static_assert(N == layer_k(DST), "layer chain");
-    float d[N];
-    read_cols<N>(G, DCOL, d);
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-        float sc = EB == 1 ? rs_src * __ldg(scales + scale_off(SRC) + i) : 1.0f;
-        d[i] = fmaxf(fmaf(d[i], sc, wl(w32, layer_b32(SRC) + i)), 0.0f);
-    }
-    return write_row<EB, N, kpad(DST, EB)>(G.a, 0, G.t, d);
-}
-// relu(D*scale + b) of layer SRC into out[N].
-template <int EB, int SRC, int DCOL>
-MRP_D void tc_out(Group& G, const float* __restrict__ w32, const float* __restrict__ scales, float rs_src, float* out) {
-    constexpr int N = layer_n(SRC);
-    read_cols<N>(G, DCOL, out);
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-        float sc = EB == 1 ? rs_src * __ldg(scales + scale_off(SRC) + i) : 1.0f;
-        out[i] = fmaxf(fmaf(out[i], sc, wl(w32, layer_b32(SRC) + i)), 0.0f);
-    }
-}
-template <int EB, int K>
-MRP_D void tc_residual_pair(Group& G, const float* __restrict__ w32, const float* __restrict__ scales, float (&a16)[16]) {
-    float r0 = write_row<EB, 16, kpad(kLX0 + 2 * K, EB)>(G.a, 0, G.t, a16);
-    tc_issue<EB, kLX0 + 2 * K, 64>(G);
-    float r1 = tc_chain<EB, kLX0 + 2 * K, 64, kLX0 + 2 * K + 1>(G, w32, scales, r0);
-    tc_issue<EB, kLX0 + 2 * K + 1, 80>(G);
+// Residual pair k of the tail: a += relu(LX(2k+1) relu(LX(2k) a + b) + b).
+template <int EB>
+__device__ __noinline__ void tc_residual_pair(Group& G, const float* __restrict__ w32, const float* __restrict__ scales,
+                                              int k, float (&a16)[16]) {
+    constexpr int KP = EB == 2 ? 16 : 32;
+    const int La = kLX0 + 2 * k, Lb = La + 1;
+    float r0 = write_row<EB, 16, KP>(G.a, 0, G.t, a16);
+    mma_round<EB>(G, 1, La, 0, 64, 0, 0, 0, 0, 0, 0);
+    float u[16];
+    read_cols<16>(G, 64, u);
+    bias_relu<EB, 16>(u, La, r0, w32, scales);
+    float r1 = write_row<EB, 16, KP>(G.a, 0, G.t, u);
+    mma_round<EB>(G, 1, Lb, 0, 80, 0, 0, 0, 0, 0, 0);
     float z[16];
-    tc_out<EB, kLX0 + 2 * K + 1, 80>(G, w32, scales, r1, z);
+    read_cols<16>(G, 80, z);
+    bias_relu<EB, 16>(z, Lb, r1, w32, scales);
 #pragma unroll
     for (int i = 0; i < 16; ++i) a16[i] += z[i];
+}
+
+struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid; };
+__constant__ BlockDesc c_blocks[12] = {
+    {8, 0, 0, 0, 0, 0, mblk_off(0), 0},      {8, 8, 1, 1, 3, 0, mblk_off(1), 3},
+    {16, 16, 0, 1, 6, 0, mblk_off(2), 6},    {16, 32, 0, 1, 9, 0, mblk_off(3), 9},
+    {16, 48, 1, 1, 12, 0, mblk_off(4), 12},  {32, 64, 0, 1, 15, 0, mblk_off(5), 15},
+    {32, 96, 0, 1, 18, 0, mblk_off(6), 18},  {32, 128, 0, 1, 21, 0, mblk_off(7), 21},
+    {8, 160, 0, 0, 27, 128, di_block_off(0), 24}, {8, 168, 0, 1, 30, 128, di_block_off(1), 27},
+    {8, 176, 0, 1, 33, 128, di_block_off(2), 30}, {8, 184, 0, 1, 36, 128, di_block_off(3), 33},
+};
+
+template <int EB, class Src>
+MRP_D void run_block(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales, int b,
+                     float g, float gamma, float (&hf)[16], float (&prev)[3][32]) {
+    const BlockDesc d = c_blocks[b];
+    if (d.w == 8)
+        tc_block<EB, 8>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma, hf, prev);
+    else if (d.w == 16)
+        tc_block<EB, 16>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma, hf, prev);
+    else
+        tc_block<EB, 32>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma, hf, prev);
 }
 
 template <int EB, class Src>
@@ -448,54 +465,37 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
 #pragma unroll
     for (int o = 0; o < 16; ++o) hf[o] = 0.0f;
     float prev[3][32];
-    // main branch, X[0:160]; finals leave comb[0:96) in TMEM columns 0..95
-    tc_block<EB, 8, 0, false, false, 0, 0>(G, src, w32, scales, main_block_off(0), 0, g, gamma, hf, prev);
-    tc_block<EB, 8, 8, true, true, 3, 0>(G, src, w32, scales, main_block_off(1), 3, g, gamma, hf, prev);
-    tc_block<EB, 16, 16, false, true, 6, 0>(G, src, w32, scales, main_block_off(2), 6, g, gamma, hf, prev);
-    tc_block<EB, 16, 32, false, true, 9, 0>(G, src, w32, scales, main_block_off(3), 9, g, gamma, hf, prev);
-    tc_block<EB, 16, 48, true, true, 12, 0>(G, src, w32, scales, main_block_off(4), 12, g, gamma, hf, prev);
-    tc_block<EB, 32, 64, false, true, 15, 0>(G, src, w32, scales, main_block_off(5), 15, g, gamma, hf, prev);
-    tc_block<EB, 32, 96, false, true, 18, 0>(G, src, w32, scales, main_block_off(6), 18, g, gamma, hf, prev);
-    tc_block<EB, 32, 128, false, true, 21, 0>(G, src, w32, scales, main_block_off(7), 21, g, gamma, hf, prev);
+    // main branch, X[0:160]; the three 32x32 finals leave comb[0:96) in TMEM columns 0..95
+#pragma unroll 1
+    for (int b = 0; b < 8; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma, hf, prev);
     float rs_main[3];
     {
-        constexpr int KP = kpad(kL81, EB), SUB = 128 * KP * EB;
+        constexpr int KP = pad_to(32, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
 #pragma unroll
         for (int c = 0; c < 3; ++c) rs_main[c] = write_row<EB, 32, KP>(G.a, c * SUB, G.t, prev[c]);
-        const int layers[3] = {kL81, kL81 + 1, kL81 + 2}, aoff[3] = {0, SUB, 2 * SUB}, dcol[3] = {0, 32, 64};
-        mma_round<EB>(G, layers, aoff, dcol, 3);
+        mma_round<EB>(G, 3, kL81, 0, 0, kL81 + 1, SUB, 32, kL81 + 2, 2 * SUB, 64);
     }
-    // direct-illumination branch, X[160:192]; finals at columns 176..223
-    tc_block<EB, 8, 160, false, false, 27, 128>(G, src, w32, scales, di_block_off(0), 24, g, gamma, hf, prev);
-    tc_block<EB, 8, 168, false, true, 30, 128>(G, src, w32, scales, di_block_off(1), 27, g, gamma, hf, prev);
-    tc_block<EB, 8, 176, false, true, 33, 128>(G, src, w32, scales, di_block_off(2), 30, g, gamma, hf, prev);
-    tc_block<EB, 8, 184, false, true, 36, 128>(G, src, w32, scales, di_block_off(3), 33, g, gamma, hf, prev);
+    // direct-illumination branch, X[160:192]; the 8x8 finals at columns 176..223
+#pragma unroll 1
+    for (int b = 8; b < 12; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma, hf, prev);
     float rs_di[3];
     {
-        constexpr int KP = kpad(kLD41, EB), SUB = 128 * KP * EB;
+        constexpr int KP = pad_to(8, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
 #pragma unroll
         for (int c = 0; c < 3; ++c) rs_di[c] = write_row<EB, 8, KP>(G.a, c * SUB, G.t, prev[c]);
-        const int layers[3] = {kLD41, kLD41 + 1, kLD41 + 2}, aoff[3] = {0, SUB, 2 * SUB}, dcol[3] = {176, 192, 208};
-        mma_round<EB>(G, layers, aoff, dcol, 3);
+        mma_round<EB>(G, 3, kLD41, 0, 176, kLD41 + 1, SUB, 192, kLD41 + 2, 2 * SUB, 208);
     }
     // comb[120] = relu(finals + b): main (3 x 32) then direct illumination (3 x 8)
     float comb[120];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float d[32];
-        read_cols<32>(G, 32 * c, d);
-#pragma unroll
-        for (int o = 0; o < 32; ++o) {
-            float sc = EB == 1 ? rs_main[c] * __ldg(scales + scale_off(kL81 + c) + o) : 1.0f;
-            comb[32 * c + o] = fmaxf(fmaf(d[o], sc, wl(w32, layer_b32(kL81 + c) + o)), 0.0f);
-        }
+        read_cols<32>(G, 32 * c, comb + 32 * c);
+        bias_relu<EB, 32>(comb + 32 * c, kL81 + c, rs_main[c], w32, scales);
         float e[16];
         tc::tmem_ld16(G.tmem + 176 + 16 * c, e);
+        bias_relu<EB, 8>(e, kLD41 + c, rs_di[c], w32, scales);
 #pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            float se = EB == 1 ? rs_di[c] * __ldg(scales + scale_off(kLD41 + c) + o) : 1.0f;
-            comb[96 + 8 * c + o] = fmaxf(fmaf(e[o], se, wl(w32, layer_b32(kLD41 + c) + o)), 0.0f);
-        }
+        for (int o = 0; o < 8; ++o) comb[96 + 8 * c + o] = e[o];
     }
     // tail, once per distinct albedo channel (core/radiancePredict.cu:375-419)
     float srv[3] = {sr.x, sr.y, sr.z}, P[3];
@@ -521,34 +521,37 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
             for (int j = 0; j < 16; ++j) a = fmaf(h[j], wl(w32, kLSEFin2W + o * 16 + j), a);
             gf[o] = sigmoid_d(a);
         }
-        float lg[8];
+        // LC0's A row: [comb * gate segment, LGGS (3 -> 8)]
+        float x[128];
+#pragma unroll
+        for (int i = 0; i < 120; ++i) x[i] = comb[i] * gf[i < 96 ? i / 32 : 3 + (i - 96) / 8];
 #pragma unroll
         for (int o = 0; o < 8; ++o) {
             float a = 0.0f;
             a = fmaf(g, wl(w32, kLGGSW + o * 3), a);
             a = fmaf(gamma, wl(w32, kLGGSW + o * 3 + 1), a);
             a = fmaf(s4, wl(w32, kLGGSW + o * 3 + 2), a);
-            lg[o] = fmaxf(a + wl(w32, kLGGSB + o), 0.0f);
+            x[120 + o] = fmaxf(a + wl(w32, kLGGSB + o), 0.0f);
         }
-        // LC0's A row: [comb * gate segment, LGGS]
-        float r0 = write_row_fn<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, [&](int i) {
-            return i < 120 ? comb[i] * gf[i < 96 ? i / 32 : 3 + (i - 96) / 8] : lg[i - 120];
-        });
-        tc_issue<EB, kLC0, 0>(G);
-        float r1 = tc_chain<EB, kLC0, 0, kLC1>(G, w32, scales, r0);
-        tc_issue<EB, kLC1, 128>(G);
-        float r2 = tc_chain<EB, kLC1, 128, kLC2>(G, w32, scales, r1);
-        tc_issue<EB, kLC2, 0>(G);
-        float r3 = tc_chain<EB, kLC2, 0, kLX>(G, w32, scales, r2);
-        tc_issue<EB, kLX, 32>(G);
+        float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, x);
+        mma_round<EB>(G, 1, kLC0, 0, 0, 0, 0, 0, 0, 0, 0);
+        read_cols<128>(G, 0, x);
+        bias_relu<EB, 128>(x, kLC0, r, w32, scales);
+        r = write_row<EB, 128, kpad(kLC1, EB)>(G.a, 0, G.t, x);
+        mma_round<EB>(G, 1, kLC1, 0, 128, 0, 0, 0, 0, 0, 0);
+        read_cols<64>(G, 128, x);
+        bias_relu<EB, 64>(x, kLC1, r, w32, scales);
+        r = write_row<EB, 64, kpad(kLC2, EB)>(G.a, 0, G.t, x);
+        mma_round<EB>(G, 1, kLC2, 0, 0, 0, 0, 0, 0, 0, 0);
+        read_cols<32>(G, 0, x);
+        bias_relu<EB, 32>(x, kLC2, r, w32, scales);
+        r = write_row<EB, 32, kpad(kLX, EB)>(G.a, 0, G.t, x);
+        mma_round<EB>(G, 1, kLX, 0, 32, 0, 0, 0, 0, 0, 0);
         float a16[16];
-        tc_out<EB, kLX, 32>(G, w32, scales, r3, a16);
-        tc_residual_pair<EB, 0>(G, w32, scales, a16);
-        tc_residual_pair<EB, 1>(G, w32, scales, a16);
-        tc_residual_pair<EB, 2>(G, w32, scales, a16);
-        tc_residual_pair<EB, 3>(G, w32, scales, a16);
-        tc_residual_pair<EB, 4>(G, w32, scales, a16);
-        tc_residual_pair<EB, 5>(G, w32, scales, a16);
+        read_cols<16>(G, 32, a16);
+        bias_relu<EB, 16>(a16, kLX, r, w32, scales);
+#pragma unroll 1
+        for (int k = 0; k < 6; ++k) tc_residual_pair<EB>(G, w32, scales, k, a16);
         float a = 0.0f;
 #pragma unroll
         for (int j = 0; j < 16; ++j) a = fmaf(a16[j], wl(w32, kLX12W + j), a);
