@@ -174,6 +174,32 @@ mrp_status mrp_last_render_stages(const mrp_volume* v, float ms[3]);
  * out [n][3]. */
 mrp_status mrp_predict_features(const float* feat, const float* gamma, float g, const float scatter_rate[3], int n,
                                 float* out3, mrp_precision precision, int is_device);
+/* No counterpart in the reference.  mrp_predict_features for host buffers
+ * that allocates nothing.  It is for callers that must not allocate while
+ * they render: a frame loop that cannot afford the device-wide
+ * synchronisation cudaFree implies, or a process whose memory pool
+ * (PyTorch's caching allocator, say) already holds the HBM, so that a
+ * cudaMalloc could fail in the middle of a frame.  The device copies of feat
+ * and gamma, the output, and the tensor-core network's tile counter and error
+ * flag live in one fixed array in the library's device image,
+ * MRP_NOALLOC_SCRATCH_BYTES (about 4.5 MiB), which every GPU that loads the
+ * library holds until the process exits.
+ *   - n <= MRP_NOALLOC_MAX_POINTS; a larger n returns MRP_ERR_INVALID and
+ *     does nothing -- split the batch.
+ *   - The array keeps the last call's contents.  The tile counter and the
+ *     error flag must start at zero, and each call clears both on its stream
+ *     before it launches; the feature area needs no clearing.
+ *   - The first call on a device looks the array's device address up
+ *     (cudaGetSymbolAddress, which may load the module); make that first call
+ *     before any stream capture begins.
+ *   - All calls share the array, so calls that overlapped on the GPU would
+ *     race on it.  The library holds its lock for the whole call and returns
+ *     only after its stream has drained, so calls from several host threads
+ *     run one after another. */
+#define MRP_NOALLOC_MAX_POINTS 2048
+#define MRP_NOALLOC_SCRATCH_BYTES (256 + (size_t)MRP_NOALLOC_MAX_POINTS * (576 + 1 + 3) * 4)
+mrp_status mrp_predict_features_noalloc(const float* feat, const float* gamma, float g, const float scatter_rate[3],
+                                        int n, float* out3, mrp_precision precision);
 /* SetupInputData (core/radiancePredict.cu:427-485) for n points: pos [n][3],
  * bases [n][12] = XMain, YMain, ZMain, LXMain; feat [n][576], gamma [n]. */
 mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bases, const float light_dir[3], float g,

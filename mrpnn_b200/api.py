@@ -77,6 +77,7 @@ _SIGS = {
     "mrp_last_render_stages": ([C.c_void_p, C.POINTER(C.c_float)], C.c_int),
     "mrp_render_counters": ([C.c_void_p, C.POINTER(View), C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
     "mrp_predict_features": ([C.c_void_p, C.c_void_p, C.c_float, F3, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "mrp_predict_features_noalloc": ([C.c_void_p, C.c_void_p, C.c_float, F3, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_gather_features": ([C.c_void_p, C.c_void_p, C.c_void_p, F3, C.c_float, C.c_float, C.c_int, C.c_void_p,
                              C.c_void_p, C.c_int], C.c_int),
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
@@ -165,6 +166,25 @@ def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
         out = torch.empty((n, 3), dtype=torch.float32, device=feat.device)
     _check(lib().mrp_predict_features(feat.data_ptr(), gamma.data_ptr(), float(g), _f3(scatter_rate), n,
                                       out.data_ptr(), int(precision), 1))
+    return out
+
+
+NOALLOC_MAX_POINTS = 2048   # MRP_NOALLOC_MAX_POINTS in include/mrpnn.h
+
+
+def predict_features_noalloc(feat, gamma, g, scatter_rate, precision=FP32):
+    """predict_features for host arrays through mrp_predict_features_noalloc,
+    for callers that must not allocate device memory mid-render: the device
+    copies, the output and the tensor-core network's counters sit in the
+    library's fixed device array.  At most NOALLOC_MAX_POINTS feature sets
+    per call."""
+    _ensure_init()
+    feat = _host_f32(feat)
+    gamma = _host_f32(gamma)
+    n = feat.shape[0]
+    out = np.empty((n, 3), np.float32)
+    _check(lib().mrp_predict_features_noalloc(feat.ctypes.data, gamma.ctypes.data, float(g), _f3(scatter_rate), n,
+                                              out.ctypes.data, int(precision)))
     return out
 
 

@@ -888,6 +888,85 @@ mrp_status mrp_predict_features(const float* feat, const float* gamma, float g_,
     return MRP_OK;
 }
 
+}  // extern "C"
+
+// --- mrp_predict_features_noalloc ----------------------------------------------------
+// One fixed scratch array per device, part of this library's device image.
+// Host code must not hand `g_noalloc_scratch` itself to a kernel: on the host
+// that name is only a stand-in for the device symbol.  Its device address is
+// looked up once per device (cudaGetSymbolAddress, with the device current)
+// and passed on.  Layout, every part on a 256-byte boundary:
+//   [0, 4)     tile counter of the tensor-core network  (zeroed before each launch)
+//   [4, 8)     error flag of the tensor-core network    (zeroed before each launch)
+//   [256, ..)  feat  [MRP_NOALLOC_MAX_POINTS][576] fp32 (copied in; no clearing)
+//   then       gamma [MRP_NOALLOC_MAX_POINTS] fp32
+//   then       out   [MRP_NOALLOC_MAX_POINTS][3] fp32
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MRP_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr size_t kNoAllocFeat = 256;
+constexpr size_t kNoAllocGamma = kNoAllocFeat + (size_t)MRP_NOALLOC_MAX_POINTS * 576 * sizeof(float);
+constexpr size_t kNoAllocOut = kNoAllocGamma + (size_t)MRP_NOALLOC_MAX_POINTS * sizeof(float);
+static_assert(kNoAllocOut + (size_t)MRP_NOALLOC_MAX_POINTS * 3 * sizeof(float) == MRP_NOALLOC_SCRATCH_BYTES,
+              "scratch layout");
+static_assert(kNoAllocGamma % 256 == 0 && kNoAllocOut % 256 == 0, "scratch alignment");
+constexpr int kNoAllocDevices = 64;
+unsigned char* g_noalloc_addr[kNoAllocDevices] = {};   // device address per device, set under g.mu
+
+// Makes `dev` current for the scope and restores the caller's device after.
+struct CurrentDevice {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit CurrentDevice(int dev) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
+    }
+    ~CurrentDevice() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+}  // namespace
+
+extern "C" {
+
+mrp_status mrp_predict_features_noalloc(const float* feat, const float* gamma, float g_, const float sr[3], int n,
+                                        float* out3, mrp_precision precision) {
+    TRY(need_init());
+    if (!feat || !gamma || !sr || !out3 || n < 0) return fail(MRP_ERR_INVALID, "null argument");
+    if (n > MRP_NOALLOC_MAX_POINTS)
+        return fail(MRP_ERR_INVALID,
+                    "mrp_predict_features_noalloc: %d points exceed its fixed scratch of %d points; split the batch",
+                    n, MRP_NOALLOC_MAX_POINTS);
+    if (precision != MRP_FP32 && precision != MRP_BF16 && precision != MRP_FP8)
+        return fail(MRP_ERR_INVALID, "unknown precision %d", (int)precision);
+    if (n == 0) return MRP_OK;
+    std::lock_guard<std::mutex> lk(g.mu);
+    if (g.device < 0 || g.device >= kNoAllocDevices) return fail(MRP_ERR_INVALID, "device %d", g.device);
+    CurrentDevice cd(g.device);
+    CU(cd.err);
+    unsigned char*& base = g_noalloc_addr[g.device];
+    if (!base) CU(cudaGetSymbolAddress((void**)&base, g_noalloc_scratch));
+    int* counter = (int*)base;
+    int* err = (int*)(base + 4);
+    float* f = (float*)(base + kNoAllocFeat);
+    float* gm = (float*)(base + kNoAllocGamma);
+    float* dout = (float*)(base + kNoAllocOut);
+    CU(cudaMemcpyAsync(f, feat, (size_t)n * 576 * sizeof(float), cudaMemcpyHostToDevice, g.stream));
+    CU(cudaMemcpyAsync(gm, gamma, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, g.stream));
+    int herr = 0;
+    if (precision == MRP_FP32) {
+        CU(launch_mlp_fp32(g.d_weights, f, gm, g_, sr, n, dout, g.stream));
+    } else {
+        CU(tc_launch_mlp_at(g.tc, precision == MRP_FP8, f, gm, g_, sr, n, dout, counter, err, g.sms, g.stream));
+        CU(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, g.stream));
+    }
+    CU(cudaMemcpyAsync(out3, dout, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, g.stream));
+    CU(cudaStreamSynchronize(g.stream));
+    if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core MLP: MMA completion wait timed out");
+    return MRP_OK;
+}
+
 mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bases, const float L[3], float g_, float alpha,
                                int n, float* feat, float* gamma, int is_device) {
     TRY(need_init());

@@ -707,6 +707,24 @@ cudaError_t tc_launch_mlp(const TcWeights& w, bool fp8, const float* feat, const
     return fp8 ? launch_tc<1, false>(a, sms, s) : launch_tc<2, false>(a, sms, s);
 }
 
+cudaError_t tc_launch_mlp_at(const TcWeights& w, bool fp8, const float* feat, const float* gamma, float g,
+                             const float sr[3], int n, float* out3, int* tile_counter, int* err, int sms,
+                             cudaStream_t s) {
+    if (!w.ready || !w.d_fp32 || !tile_counter || !err) return cudaErrorNotReady;
+    TcArgs a = base_args(w, fp8);
+    a.err = err;
+    a.tile_counter = tile_counter;
+    a.feat = feat;
+    a.gamma = gamma;
+    a.n = n;
+    a.g = g;
+    a.sr = mk3(sr[0], sr[1], sr[2]);
+    a.out3 = out3;
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    return fp8 ? launch_tc<1, false>(a, sms, s) : launch_tc<2, false>(a, sms, s);
+}
+
 cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
                               const HitRecords& rec, const float* feat, float4* accum, int sms, cudaStream_t s) {
     if (!w.ready || !w.d_fp32) return cudaErrorNotReady;

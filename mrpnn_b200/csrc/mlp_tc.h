@@ -26,6 +26,11 @@ cudaError_t tc_ensure_scratch(TcScratch& s, size_t npix);
 void tc_free_scratch(TcScratch& s);
 cudaError_t tc_launch_mlp(const TcWeights& w, bool fp8, const float* feat, const float* gamma, float g, const float sr[3],
                           int n, float* out3, int sms, cudaStream_t s);
+// Same launch with the tile counter and the error flag at caller-given device
+// addresses instead of the ones in TcWeights (both zeroed on `s` first).
+cudaError_t tc_launch_mlp_at(const TcWeights& w, bool fp8, const float* feat, const float* gamma, float g,
+                             const float sr[3], int n, float* out3, int* tile_counter, int* err, int sms,
+                             cudaStream_t s);
 // Network on the staged predictor's records and tiled features (kernels.h).
 struct HitRecords;
 cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
