@@ -263,11 +263,160 @@ def run_tracer(args, local):
                                  f"+ 16 B/pixel; peak {peak_kind}; the 8 MiB volume is L2-resident"}}
 
 
+SERVE = dict(volumes=16, sizes=(128, 256, 512), seeds=range(10, 26), alpha=(16.0, 256.0), freq=4.0, rate=200.0,
+             images=((256, 256), (512, 512), (1024, 1024), (1920, 1080)), radius=(0.8, 2.0), budget=120 << 30,
+             slots=16)
+
+
+def run_serving(args, local):
+    """Serving workload: 16 resident fBm volumes (edges drawn from 128/256/512,
+    seeds 10-25, extinction 16-256), a seeded Poisson stream of MRPNN requests
+    at 200 req/s with images drawn from 256^2 / 512^2 / 1024^2 / 1920x1080,
+    random orbit cameras (radius 0.8-2) and random lights, BF16 network,
+    120 GB admission budget.  Latency = submit -> result in the caller's
+    (device) buffer, from the server's own clock."""
+    import threading
+
+    import torch
+
+    import mrpnn_b200 as M
+    rng = np.random.default_rng(2024)
+    vols = []
+    for seed in SERVE["seeds"]:
+        R = int(rng.choice(SERVE["sizes"]))
+        v = M.VolumeRender(R)
+        v.generate_fbm(int(seed), SERVE["freq"])
+        v.Update()
+        v.SetScatterRate(SCENE["albedo"])
+        v.SetSky(SCENE["sky"])
+        vols.append((v, R, float(rng.uniform(*SERVE["alpha"]))))
+    n_req = args.serve_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / SERVE["rate"], n_req))
+    reqs = []
+    for i in range(n_req):
+        vi = int(rng.integers(len(vols)))
+        v, R, alpha = vols[vi]
+        Wq, Hq = SERVE["images"][int(rng.integers(len(SERVE["images"])))]
+        r = rng.uniform(*SERVE["radius"])
+        d = rng.normal(size=3)
+        pos = r * d / np.linalg.norm(d)
+        ori, up, right = M.camera_frame(tuple(float(x) for x in pos))
+        sc = np.float32(np.tan(np.deg2rad(SCENE["fov"]) / 2))
+        L = rng.normal(size=3)
+        L = (L / np.linalg.norm(L)).astype(np.float32)
+        view = v.make_view((Wq, Hq), ori, (up * sc).astype(np.float32), (right * sc).astype(np.float32), L,
+                           SCENE["g"], alpha, seed=i)
+        reqs.append((vi, view))
+    pool = [torch.empty(1920 * 1080 * 4, dtype=torch.float32, device=f"cuda:{local}") for _ in range(64)]
+    srv = M.Server(memory_budget=SERVE["budget"], max_slots=SERVE["slots"], precision=M.BF16)
+    try:
+        # warm-up: one request of each image size (LUT, slot buffers)
+        for k, (Wq, Hq) in enumerate(SERVE["images"]):
+            v = vols[k][0]
+            vw = v.make_view((Wq, Hq), *view_vectors(), light(), SCENE["g"], vols[k][2])
+            srv.wait(srv.submit(v, vw, pool[k][:Wq * Hq * 4]))
+        tickets = [None] * n_req
+        done = [False] * n_req
+        t_start = time.perf_counter()
+
+        def producer():
+            for i, (vi, view) in enumerate(reqs):
+                dt = t_start + arrivals[i] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                if i >= len(pool):   # buffer reuse: request i - 64 must be done
+                    while not done[i - len(pool)]:
+                        time.sleep(1e-4)
+                tickets[i] = srv.submit(vols[vi][0], view, pool[i % len(pool)][:view.width * view.height * 4])
+
+        th = threading.Thread(target=producer)
+        th.start()
+        lat, parts, pix = [], [], 0
+        first_submit, last_done = None, None
+        for i in range(n_req):
+            while tickets[i] is None:
+                time.sleep(1e-4)
+            _, tm = srv.wait(tickets[i])
+            done[i] = True
+            lat.append(tm["done_ms"] - tm["submit_ms"])
+            parts.append((tm["admit_ms"] - tm["submit_ms"], tm["features_ms"] - tm["admit_ms"],
+                          tm["network_ms"] - tm["features_ms"], tm["done_ms"] - tm["network_ms"]))
+            first_submit = tm["submit_ms"] if first_submit is None else min(first_submit, tm["submit_ms"])
+            last_done = tm["done_ms"] if last_done is None else max(last_done, tm["done_ms"])
+            pix += reqs[i][1].width * reqs[i][1].height
+        th.join()
+        st = srv.stats()
+    finally:
+        srv.close()
+    span_s = (last_done - first_submit) / 1000.0
+    lat = np.asarray(lat)
+    pm = np.median(np.asarray(parts), axis=0)
+    return {"workload": "16 resident fBm volumes (128/256/512^3, seeds 10-25, alpha 16-256), Poisson "
+                        f"{SERVE['rate']:.0f} req/s, images 256^2/512^2/1024^2/1920x1080, orbit cameras, random "
+                        "lights, BF16 network, 120 GB budget, 16 slots, results in device buffers",
+            "requests": n_req, "offered_req_s": SERVE["rate"], "achieved_req_s": n_req / span_s,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "frames_per_s_1024eq": pix / (1024 * 1024) / span_s,
+            "median_split_ms": {"queue": float(pm[0]), "tr+hit+gather": float(pm[1]), "network": float(pm[2]),
+                                "result copy": float(pm[3])},
+            "batches": st["batches"], "mean_batch": st["batched_requests"] / max(1, st["batches"]),
+            "max_batch": st["max_batch"], "peak_bytes": st["peak_bytes"]}
+
+
+def lum_rmse_x100(a, b):
+    """The reference's tools/Compare.py metric: both images saturated to 8 bit,
+    Rec.601 luminance / 255, RMSE over all pixels, x100."""
+    def lum(x):
+        q = np.round(np.clip(x[..., :3], 0.0, 1.0) * 255.0)
+        return (q[..., 0] * 0.299 + q[..., 1] * 0.587 + q[..., 2] * 0.114) / 255.0
+    return float(np.sqrt(np.mean((lum(a) - lum(b)) ** 2)) * 100.0)
+
+
+def run_precision(args, vol, local):
+    """Error of each precision form against the path tracer: the C2 scene seen
+    through the headline camera (rendered at 512^2) and through a 1920x1080
+    camera (rendered at 480x270, same 16:9 framing).  Reference: one PT launch
+    of 4096 spp per pixel, FP64-accumulated, unbiased NEE (one ratio-tracking
+    Tr() estimate per vertex), <= 512 bounces.  Predictor: MRPNN running mean
+    over 1 and 16 launches."""
+    import mrpnn_b200 as M
+    ori, up, right = view_vectors()
+    views = {"headline camera @512x512": ((512, 512), up, right),
+             "1920x1080 camera @480x270": ((480, 270), up, (right * np.float32(16.0 / 9.0)).astype(np.float32))}
+    out = {"reference": f"PT, {args.rmse_spp} spp in one launch (FP64 per-pixel sums), unbiased NEE, <= 512 bounces",
+           "metrics": "rel_rmse = RMS(pred - PT) / RMS(PT) over linear RGB; lum_rmse_x100 = tools/Compare.py",
+           "views": {}}
+    prec = {"fp32": M.FP32, "bf16": M.BF16, "fp8": M.FP8}
+    L = light()
+    for name, (size, u, r) in views.items():
+        vol.SetNeeMode(True)
+        t0 = time.perf_counter()
+        ref = vol.Render(size, ori, u, r, L, M.VolumeRender.PT, SCENE["g"], SCENE["alpha"], multiScatter=512,
+                         sampleNum=1, spp=args.rmse_spp, seed=99)
+        pt_s = time.perf_counter() - t0
+        vol.SetNeeMode(False)
+        den = float(np.sqrt(np.mean(ref[..., :3].astype(np.float64) ** 2)))
+        res = {"pt_seconds": pt_s}
+        for pname, pv in prec.items():
+            vol.SetPrecision(pv)
+            for n in (1, 16):
+                img = vol.Render(size, ori, u, r, L, M.VolumeRender.MRPNN, SCENE["g"], SCENE["alpha"], sampleNum=n,
+                                 seed=5)
+                d = img[..., :3].astype(np.float64) - ref[..., :3]
+                res[f"{pname}_x{n}"] = {"rel_rmse": float(np.sqrt(np.mean(d ** 2)) / den),
+                                        "lum_rmse_x100": lum_rmse_x100(img, ref)}
+        out["views"][name] = res
+    vol.SetPrecision(prec[args.precision])
+    return out
+
+
 STAGES = ("first hit + bases", "stencil gather", "network")
 # Algorithmic HBM bytes per hit pixel of each predictor stage (fp32 data):
 #   gather : 192 points x (8 density + 8 TR + 2 x 4 LUT texels) x 4 B read,
 #            576 features x 4 B written
 #   network: 576 features x 4 B read + 16 B record + 16 B result
+FLOP_PER_HIT = 97072   # 2 x 48,536 MACs of RadiancePredictInternal, grey albedo
 STAGE_BYTES_PER_HIT = (None, GATHER_BYTES_PER_PIXEL + 576 * 4, 576 * 4 + 32)
 
 
@@ -350,7 +499,18 @@ def run_mine(args, rank, world, local):
             traffic = json.load(f).get(f"{args.precision}_{W}x{H}", {}).get(["hit", "gather", "network"][dom])
     except Exception:
         pass
-    if STAGE_BYTES_PER_HIT[dom] is not None:
+    if dom == 2 and args.precision != "fp32":
+        # the tcgen05 network: a GEMM chain, roofline = dense BF16 tensor peak
+        flop = active * FLOP_PER_HIT
+        achieved = flop / (st[dom] / 1000.0) / 1e12
+        dram = (traffic / (st[dom] / 1000.0) / 1e9) if traffic else None
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                "traffic": traffic, "kernel": STAGES[dom],
+                "note": f"algorithmic FLOP = {FLOP_PER_HIT} x {active} hit pixels per launch (grey albedo); "
+                        f"duration = CUDA events around the stage; peak {peak_kind} burst bf16 "
+                        f"(MEASURED_PEAKS.json bf16_tflops); DRAM from the ncu traffic "
+                        f"{'%.0f GB/s' % dram if dram else 'n/a'} of {hbm:.0f}"}
+    elif STAGE_BYTES_PER_HIT[dom] is not None:
         alg = active * STAGE_BYTES_PER_HIT[dom]
         achieved = alg / (st[dom] / 1000.0) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -362,6 +522,8 @@ def run_mine(args, rank, world, local):
                 "kernel": STAGES[dom], "note": "march lookups are data dependent; see profiles/"}
 
     tracer = run_tracer(args, local) if (rank == 0 and args.tracer_steps > 0) else None
+    serving = run_serving(args, local) if (rank == 0 and args.serve_requests > 0) else None
+    precision_error = run_precision(args, vol, local) if (rank == 0 and args.rmse_spp > 0) else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -386,6 +548,8 @@ def run_mine(args, rank, world, local):
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "tracer": tracer,
+            "serving": serving,
+            "precision_error": precision_error,
         }
         print(json.dumps(line), flush=True)
 
@@ -402,6 +566,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=1024, help="frame edge (the headline workload is 1024)")
     ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving workload (0: skip)")
+    ap.add_argument("--rmse-spp", type=int, default=4096, help="spp of the PT reference image (0: skip)")
     args = ap.parse_args()
     global W, H
     W = H = args.size

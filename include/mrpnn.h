@@ -69,6 +69,9 @@ typedef struct mrp_params {
     int bake_replicate_seeding; /* 1 (default): the reference's per-voxel estimates share one stream */
     mrp_precision precision; /* predictor MLP arithmetic, default MRP_FP32 */
     uint32_t seed;           /* RNG key of the LUT and bake streams, default 0 */
+    int nee_mode;            /* PT next-event estimation: 0 (default) the baked
+                                TR grid, as the reference; 1 one ratio-tracking
+                                Tr() estimate per vertex (unbiased, no bake) */
 } mrp_params;
 
 /* One camera: VolumeRender::Render(int2 size, ori, up, right, lightDir, rt,
@@ -223,6 +226,57 @@ mrp_status mrp_tc_gemm_check(int fp8, const float* A, const float* B, int n, int
  * [w*h][576] (SetupInputData's features; zero where no hit). */
 mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* view, float* rgba, float* aux, float* feat,
                                     int is_device);
+
+/* -- serving --------------------------------------------------------------------------
+ * The reference renders one frame per synchronous Render call
+ * (core/volume.cu:487-548); its viewer (core/GUI.hpp:1002-1030) and data
+ * generator (dataGen.cu:246-328) loop over it.  A server keeps any number of
+ * resident volumes (ordinary mrp_volume handles after mrp_volume_update) and
+ * renders MRPNN requests on them with continuous batching: a worker thread
+ * admits requests into slots while slots and the memory budget allow; each
+ * admitted request builds its own TR mips for its light and alpha and runs
+ * the first hit and the stencil gather on its slot's stream, overlapping the
+ * requests already on the device; the network of every request whose
+ * features are ready runs in one batched persistent launch; results go to
+ * the caller's buffer.  Each result equals mrp_render of the same view with
+ * sample_num 1 (same kernels, same per-pixel streams).
+ * Volumes must not be changed (set_data / update / params) while requests on
+ * them are pending. */
+typedef struct mrp_server mrp_server;
+typedef struct mrp_serve_config {
+    size_t memory_budget;    /* device bytes for request slots and LUTs (default 120 GB) */
+    int max_slots;           /* requests on the device at once, 1..64 (default 16) */
+    mrp_precision precision; /* network arithmetic (default MRP_BF16)              */
+} mrp_serve_config;
+typedef struct mrp_request {
+    mrp_volume* volume;      /* resident volume (pyramid built)                    */
+    mrp_view view;           /* camera, light, alpha, g, seed, frame_offset        */
+    float* out_rgba;         /* width*height*4 floats, as mrp_render writes them   */
+    int out_is_device;       /* 0: host memory (pinned or pageable), 1: device     */
+} mrp_request;
+/* Milliseconds since mrp_serve_open of each step of one request. */
+typedef struct mrp_request_timing {
+    double submit_ms, admit_ms, features_ms, network_ms, done_ms;
+} mrp_request_timing;
+typedef struct mrp_serve_stats {
+    unsigned long long submitted, completed, failed, batches, batched_requests;
+    int max_batch;           /* most requests in one network launch               */
+    size_t bytes_in_use, peak_bytes;
+} mrp_serve_stats;
+void mrp_serve_default_config(mrp_serve_config* cfg);
+mrp_status mrp_serve_open(const mrp_serve_config* cfg, mrp_server** out);
+/* Queues a request; returns at once with its ticket.  A request larger than
+ * the whole budget fails with MRP_ERR_BUDGET here. */
+mrp_status mrp_serve_submit(mrp_server* s, const mrp_request* req, uint64_t* ticket);
+/* Waits up to wait_ms (0: poll; < 0: until done) for a ticket.  *done = 1
+ * when the result is in the caller's buffer; the return value is then the
+ * request's own status and the ticket is released.  *done = 0: still
+ * running, MRP_OK. */
+mrp_status mrp_serve_poll(mrp_server* s, uint64_t ticket, int wait_ms, int* done, mrp_request_timing* timing);
+mrp_status mrp_serve_stats_get(mrp_server* s, mrp_serve_stats* stats);
+/* Finishes every submitted request, then stops the worker and frees the
+ * server's device memory. */
+mrp_status mrp_serve_close(mrp_server* s);
 
 #ifdef __cplusplus
 }

@@ -2,8 +2,8 @@
 tracer and the MRPNN neural radiance predictor, behind a C ABI
 (include/mrpnn.h) with a Python mirror of the reference's VolumeRender /
 Camera API."""
-from .api import (BF16, FP8, FP32, NOALLOC_MAX_POINTS, Camera, MrpError, VolumeRender, camera_frame, default_params,
-                  init, lib, predict_features, predict_features_noalloc)
+from .api import (BF16, FP8, FP32, NOALLOC_MAX_POINTS, Camera, MrpError, Server, VolumeRender, camera_frame,
+                  default_params, init, lib, predict_features, predict_features_noalloc)
 
 __all__ = ["VolumeRender", "Camera", "MrpError", "init", "lib", "predict_features", "predict_features_noalloc",
-           "NOALLOC_MAX_POINTS", "camera_frame", "default_params", "FP32", "BF16", "FP8"]
+           "NOALLOC_MAX_POINTS", "Server", "camera_frame", "default_params", "FP32", "BF16", "FP8"]

@@ -34,7 +34,7 @@ class MrpError(RuntimeError):
 class Params(C.Structure):
     _fields_ = [("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3), ("env_exp", C.c_float),
                 ("bake_res", C.c_int), ("bake_replicate_seeding", C.c_int), ("precision", C.c_int),
-                ("seed", C.c_uint32)]
+                ("seed", C.c_uint32), ("nee_mode", C.c_int)]
 
 
 class View(C.Structure):
@@ -47,6 +47,24 @@ class VolumeInfo(C.Structure):
     _fields_ = [("res", C.c_int), ("max_density", C.c_float), ("has_pyramid", C.c_int), ("has_lut", C.c_int),
                 ("has_tr", C.c_int), ("has_baked_tr", C.c_int), ("lut_g", C.c_float), ("tr_alpha", C.c_float),
                 ("tr_light", F3), ("device_bytes", C.c_size_t)]
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [("memory_budget", C.c_size_t), ("max_slots", C.c_int), ("precision", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("volume", C.c_void_p), ("view", View), ("out_rgba", C.c_void_p), ("out_is_device", C.c_int)]
+
+
+class RequestTiming(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("submit_ms", "admit_ms", "features_ms", "network_ms", "done_ms")]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_ulonglong), ("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
+                ("batches", C.c_ulonglong), ("batched_requests", C.c_ulonglong), ("max_batch", C.c_int),
+                ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t)]
 
 
 FILL_FN = C.CFUNCTYPE(C.c_float, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_void_p)
@@ -83,6 +101,12 @@ _SIGS = {
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "mrp_serve_default_config": ([C.POINTER(ServeConfig)], None),
+    "mrp_serve_open": ([C.POINTER(ServeConfig), C.POINTER(C.c_void_p)], C.c_int),
+    "mrp_serve_submit": ([C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
+    "mrp_serve_poll": ([C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_int), C.POINTER(RequestTiming)], C.c_int),
+    "mrp_serve_stats_get": ([C.c_void_p, C.POINTER(ServeStats)], C.c_int),
+    "mrp_serve_close": ([C.c_void_p], C.c_int),
 }
 
 _lib = None
@@ -313,6 +337,13 @@ class VolumeRender:
         self._params.seed = int(seed)
         self._push()
 
+    def SetNeeMode(self, unbiased):
+        """PT next-event estimation: False (default) samples the baked TR grid
+        like the reference; True takes one ratio-tracking Tr() estimate per
+        vertex (unbiased; no bake)."""
+        self._params.nee_mode = 1 if unbiased else 0
+        self._push()
+
     # -- caches -------------------------------------------------------------------
     def UpdateHGLut(self, g):
         _check(lib().mrp_update_hg_lut(self._h, float(g)))
@@ -446,3 +477,67 @@ class Camera:
         from PIL import Image
         Image.fromarray(rgba, "RGBA").save(path + ".png")
         return img
+
+
+class Server:
+    """The serving loop (mrp_serve_*): MRPNN requests on resident volumes with
+    memory-budget admission and batched network launches.  Output buffers are
+    numpy arrays (pinned or pageable) or CUDA tensors; they must stay alive
+    until the ticket is polled done, which this wrapper takes care of."""
+
+    def __init__(self, memory_budget=None, max_slots=16, precision=BF16):
+        _ensure_init()
+        cfg = ServeConfig()
+        lib().mrp_serve_default_config(C.byref(cfg))
+        if memory_budget is not None:
+            cfg.memory_budget = int(memory_budget)
+        cfg.max_slots = int(max_slots)
+        cfg.precision = int(precision)
+        h = C.c_void_p()
+        _check(lib().mrp_serve_open(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._outs = {}
+
+    def submit(self, volume, view, out=None):
+        """Queues `view` (a View) on `volume` (a VolumeRender); returns the ticket."""
+        if out is None:
+            out = np.empty((view.height, view.width, 4), np.float32)
+        p, dev = _ptr(out)
+        req = Request(volume._h, view, p, dev)
+        t = C.c_uint64()
+        _check(lib().mrp_serve_submit(self._h, C.byref(req), C.byref(t)))
+        self._outs[t.value] = out
+        return t.value
+
+    def poll(self, ticket, wait_ms=-1):
+        """(done, timing dict); raises MrpError if the request failed."""
+        done = C.c_int()
+        tm = RequestTiming()
+        st = lib().mrp_serve_poll(self._h, ticket, int(wait_ms), C.byref(done), C.byref(tm))
+        if done.value:
+            out = self._outs.pop(ticket, None)
+            _check(st)
+            return True, {k: getattr(tm, k) for k, _ in RequestTiming._fields_}, out
+        _check(st)
+        return False, None, None
+
+    def wait(self, ticket):
+        """Blocks until done; returns (output, timing)."""
+        done, tm, out = self.poll(ticket, -1)
+        return out, tm
+
+    def stats(self):
+        st = ServeStats()
+        _check(lib().mrp_serve_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+    def close(self):
+        if self._h:
+            _check(lib().mrp_serve_close(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

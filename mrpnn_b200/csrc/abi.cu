@@ -13,9 +13,7 @@
 
 #include <dlfcn.h>
 
-#include "../../include/mrpnn.h"
-#include "kernels.h"
-#include "mlp_tc.h"
+#include "abi_internal.h"
 
 using namespace mrp;
 
@@ -23,7 +21,9 @@ using namespace mrp;
 // errors
 // ---------------------------------------------------------------------------
 static thread_local std::string t_err;
-static mrp_status fail(mrp_status s, const char* fmt, ...) {
+namespace mrpi {
+Lib g;
+mrp_status fail(mrp_status s, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -32,38 +32,13 @@ static mrp_status fail(mrp_status s, const char* fmt, ...) {
     t_err = buf;
     return s;
 }
-#define CU(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess)                                                                     \
-            return fail(e_ == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "%s: %s (%s:%d)", #call, \
-                        cudaGetErrorString(e_), __FILE__, __LINE__);                               \
-    } while (0)
-#define TRY(call)                                                                                  \
-    do {                                                                                           \
-        mrp_status s_ = (call);                                                                    \
-        if (s_ != MRP_OK) return s_;                                                               \
-    } while (0)
+}  // namespace mrpi
+using namespace mrpi;
 
 // ---------------------------------------------------------------------------
 // library state (one device per process)
 // ---------------------------------------------------------------------------
 namespace {
-struct Lib {
-    std::mutex mu;
-    bool ready = false;
-    int device = -1;
-    int sms = 148;
-    cudaStream_t stream = nullptr;   // for handle-less calls
-    std::map<std::string, std::vector<float>> model;
-    float* d_weights = nullptr;      // packed fp32 weights (common.cuh layout)
-    std::vector<float> h_weights;
-    TcWeights tc;                    // tensor-core weight images
-    // scratch for handle-less parity calls
-    void* scratch = nullptr;
-    size_t scratch_bytes = 0;
-};
-Lib g;
 
 std::string default_model_path() {
     Dl_info info;
@@ -205,77 +180,6 @@ mrp_status ensure_scratch(size_t bytes) {
 }
 
 }  // namespace
-
-// ---------------------------------------------------------------------------
-// volume handle
-// ---------------------------------------------------------------------------
-struct mrp_volume {
-    int res = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t ev_stage[2] = {nullptr, nullptr};   // stage boundaries of the last launch
-    float last_ms = 0.0f;
-    float stage_ms[3] = {0, 0, 0};
-    bool stages_valid = false;
-    float* density = nullptr;
-    float* mips = nullptr;
-    float* trs = nullptr;
-    float* lut = nullptr;
-    float* baked = nullptr;
-    int baked_alloc_res = 0;
-    uint8_t* occ = nullptr;
-    int occ_shift = 3, occ_res = 0;
-    int* d_maxbits = nullptr;
-    bool has_data = false, has_pyramid = false, has_lut = false, has_tr = false, has_baked = false;
-    bool max_override = false;
-    float max_density = 0.00001f;
-    float lut_g = NAN, tr_alpha = NAN, tr_light[3] = {NAN, NAN, NAN};
-    float bk_alpha = NAN, bk_light[3] = {NAN, NAN, NAN};
-    int bk_res = 0;
-    uint32_t lut_seed = 0, bk_seed = 0;
-    mrp_params params;
-    // render buffers
-    float4* accum = nullptr;
-    size_t accum_pix = 0;
-    double* sum3 = nullptr;
-    int* first_pos = nullptr;
-    unsigned long long* counter = nullptr;
-    size_t trace_pix = 0;
-    // staged predictor buffers (records of hit pixels, tiled features)
-    int* rec_count = nullptr;
-    int* rec_pix = nullptr;
-    float* rec_f = nullptr;
-    float* feat = nullptr;
-    size_t rec_cap = 0;
-    // tensor-core predictor scratch
-    TcScratch tc;
-
-    HitRecords records() const { return HitRecords{rec_count, rec_pix, rec_f, rec_cap}; }
-
-    VolumeDev dev() const {
-        VolumeDev d{};
-        d.density = density;
-        d.res = res;
-        d.max_density = max_density;
-        d.mips = mips;
-        d.trs = trs;
-        d.lut = lut;
-        d.baked = baked;
-        d.baked_res = bk_res;
-        d.occ = occ;
-        d.occ_shift = occ_shift;
-        d.occ_res = occ_res;
-        d.scatter_rate = {params.scatter_rate[0], params.scatter_rate[1], params.scatter_rate[2]};
-        d.tr_scale = params.tr_scale;
-        d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};
-        return d;
-    }
-};
-
-static mrp_status need_init() {
-    if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");
-    return MRP_OK;
-}
 
 extern "C" {
 
@@ -518,6 +422,7 @@ mrp_status mrp_set_params(mrp_volume* v, const mrp_params* p) {
     if (p->bake_res < 2 || p->bake_res > 2048) return fail(MRP_ERR_INVALID, "bake_res %d out of range", p->bake_res);
     if (p->precision != MRP_FP32 && p->precision != MRP_BF16 && p->precision != MRP_FP8)
         return fail(MRP_ERR_INVALID, "unknown precision %d", (int)p->precision);
+    if (p->nee_mode != 0 && p->nee_mode != 1) return fail(MRP_ERR_INVALID, "nee_mode %d (0 or 1)", p->nee_mode);
     bool bake_changed = p->bake_res != v->params.bake_res || p->tr_scale != v->params.tr_scale ||
                         p->bake_replicate_seeding != v->params.bake_replicate_seeding || p->seed != v->params.seed;
     bool lut_changed = p->seed != v->params.seed;
@@ -559,6 +464,20 @@ mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* 
 }
 
 // --- caches ----------------------------------------------------------------
+}  // extern "C"
+namespace mrpi {
+// Fill_TR for all 8 TR levels: level lv (res 128 >> lv) through density mip
+// lv + 1 with alpha / 1.73^(lv + 1) (core/volume.cu:1535-1560).
+cudaError_t build_tr_levels(float* trs, const float* mips, const float L[3], float alpha, cudaStream_t s) {
+    for (int lv = 0; lv < 8; ++lv) {
+        float a = alpha / std::pow(1.73f, (float)lv + 1.0f);
+        cudaError_t e = launch_tr_level(trs + tr_offset(lv), 128 >> lv, mips + mip_offset(lv + 1), a, L, g.sms, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+}  // namespace mrpi
+extern "C" {
 static mrp_status update_lut_async(mrp_volume* v, float g_) {
     if (v->has_lut && v->lut_g == g_ && v->lut_seed == v->params.seed) return MRP_OK;
     CU(launch_hg_lut(v->lut, g_, v->params.seed, v->stream));
@@ -571,10 +490,7 @@ static mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) 
     if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "TR mips need the pyramid (call mrp_volume_update)");
     if (v->has_tr && v->tr_alpha == alpha && v->tr_light[0] == L[0] && v->tr_light[1] == L[1] && v->tr_light[2] == L[2])
         return MRP_OK;
-    for (int lv = 0; lv < 8; ++lv) {
-        float a = alpha / std::pow(1.73f, (float)lv + 1.0f);
-        CU(launch_tr_level(v->trs + tr_offset(lv), 128 >> lv, v->mips + mip_offset(lv + 1), a, L, g.sms, v->stream));
-    }
+    CU(build_tr_levels(v->trs, v->mips, L, alpha, v->stream));
     v->has_tr = true;
     v->tr_alpha = alpha;
     std::memcpy(v->tr_light, L, sizeof v->tr_light);
@@ -634,11 +550,14 @@ static mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
     CU(cudaMalloc(&v->rec_pix, npix * sizeof(int)));
     CU(cudaMalloc(&v->rec_f, npix * 16 * sizeof(float)));
     CU(cudaMalloc(&v->feat, tiled_feature_floats(npix) * sizeof(float)));
+    CU(tc_ensure_scratch(v->tc));
     v->rec_cap = npix;
     return MRP_OK;
 }
 
-static ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k) {
+}  // extern "C"
+namespace mrpi {
+ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k) {
     ViewDev d{};
     d.width = w->width;
     d.height = w->height;
@@ -659,6 +578,8 @@ static ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int 
     d.pass_rate = std::exp(-t_step * smax);
     return d;
 }
+}  // namespace mrpi
+extern "C" {
 
 static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out,
                               int out_is_device, unsigned long long* counters);
@@ -717,12 +638,12 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     if (type == MRP_MRPNN) {
         TRY(update_lut_async(v, w->g));
         TRY(update_tr_async(v, w->light_dir, w->alpha));
-    } else {
+    } else if (v->params.nee_mode == 0) {
         TRY(update_baked_async(v, w->light_dir, w->alpha));
     }
     if (type == MRP_MRPNN) TRY(ensure_predictor_buffers(v, npix));
     VolumeDev d = v->dev();
-    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) CU(cudaMemsetAsync(g.tc.d_err, 0, sizeof(int), v->stream));
+    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) CU(cudaMemsetAsync(v->tc.d + 1, 0, sizeof(int), v->stream));
     CU(cudaEventRecord(v->ev0, v->stream));
     for (int i = 0; i < sample_num; ++i) {
         ViewDev vd = make_view(v, w, w->frame_offset + i, i);
@@ -738,7 +659,7 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
             if (v->params.precision == MRP_FP32) {
                 CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, v->accum, v->stream));
             } else {
-                CU(tc_launch_mlp_rec(g.tc, v->params.precision == MRP_FP8, d, vd, rec, v->feat, v->accum, g.sms,
+                CU(tc_launch_mlp_rec(g.tc, v->params.precision == MRP_FP8, d, vd, rec, v->feat, v->accum, v->tc, g.sms,
                                      v->stream));
             }
         } else {
@@ -764,7 +685,7 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     v->stages_valid = true;
     if (type == MRP_MRPNN && v->params.precision != MRP_FP32) {
         int herr = 0;
-        CU(cudaMemcpy(&herr, g.tc.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(&herr, v->tc.d + 1, sizeof(int), cudaMemcpyDeviceToHost));
         if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core MLP: MMA completion wait timed out");
     }
     return MRP_OK;

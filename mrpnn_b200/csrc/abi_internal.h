@@ -1,0 +1,131 @@
+// abi_internal.h -- state shared by the C ABI's translation units (abi.cu,
+// serve.cu): the library singleton, the volume handle, error reporting.
+#pragma once
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mrpnn.h"
+#include "kernels.h"
+#include "mlp_tc.h"
+
+struct mrp_volume;
+namespace mrpi {
+using namespace mrp;
+
+// Sets the calling thread's last error (mrp_last_error) and returns s.
+mrp_status fail(mrp_status s, const char* fmt, ...);
+
+struct Lib {
+    std::mutex mu;
+    bool ready = false;
+    int device = -1;
+    int sms = 148;
+    cudaStream_t stream = nullptr;   // for handle-less calls
+    std::map<std::string, std::vector<float>> model;
+    float* d_weights = nullptr;      // packed fp32 weights (common.cuh layout)
+    std::vector<float> h_weights;
+    TcWeights tc;                    // tensor-core weight images
+    // scratch for handle-less parity calls
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+};
+extern Lib g;
+
+// Device view of one camera launch (RenderCamera's arguments).
+ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k);
+// Fill_TR for the 8 TR levels of a pyramid into trs (kTrFloats floats).
+cudaError_t build_tr_levels(float* trs, const float* mips, const float L[3], float alpha, cudaStream_t s);
+
+inline mrp_status need_init() {
+    if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");
+    return MRP_OK;
+}
+
+}  // namespace mrpi
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return mrpi::fail(e_ == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "%s: %s (%s:%d)", #call, \
+                              cudaGetErrorString(e_), __FILE__, __LINE__);                         \
+    } while (0)
+#define TRY(call)                                                                                  \
+    do {                                                                                           \
+        mrp_status s_ = (call);                                                                    \
+        if (s_ != MRP_OK) return s_;                                                               \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// volume handle
+// ---------------------------------------------------------------------------
+struct mrp_volume {
+    using VolumeDev = mrp::VolumeDev;
+    using HitRecords = mrp::HitRecords;
+    using TcScratch = mrp::TcScratch;
+    int res = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_stage[2] = {nullptr, nullptr};   // stage boundaries of the last launch
+    float last_ms = 0.0f;
+    float stage_ms[3] = {0, 0, 0};
+    bool stages_valid = false;
+    float* density = nullptr;
+    float* mips = nullptr;
+    float* trs = nullptr;
+    float* lut = nullptr;
+    float* baked = nullptr;
+    int baked_alloc_res = 0;
+    uint8_t* occ = nullptr;
+    int occ_shift = 3, occ_res = 0;
+    int* d_maxbits = nullptr;
+    bool has_data = false, has_pyramid = false, has_lut = false, has_tr = false, has_baked = false;
+    bool max_override = false;
+    float max_density = 0.00001f;
+    float lut_g = NAN, tr_alpha = NAN, tr_light[3] = {NAN, NAN, NAN};
+    float bk_alpha = NAN, bk_light[3] = {NAN, NAN, NAN};
+    int bk_res = 0;
+    uint32_t lut_seed = 0, bk_seed = 0;
+    mrp_params params;
+    // render buffers
+    float4* accum = nullptr;
+    size_t accum_pix = 0;
+    double* sum3 = nullptr;
+    int* first_pos = nullptr;
+    unsigned long long* counter = nullptr;
+    size_t trace_pix = 0;
+    // staged predictor buffers (records of hit pixels, tiled features)
+    int* rec_count = nullptr;
+    int* rec_pix = nullptr;
+    float* rec_f = nullptr;
+    float* feat = nullptr;
+    size_t rec_cap = 0;
+    // tensor-core predictor scratch
+    TcScratch tc;
+
+    HitRecords records() const { return HitRecords{rec_count, rec_pix, rec_f, rec_cap}; }
+
+    VolumeDev dev() const {
+        VolumeDev d{};
+        d.density = density;
+        d.res = res;
+        d.max_density = max_density;
+        d.mips = mips;
+        d.trs = trs;
+        d.lut = lut;
+        d.baked = baked;
+        d.baked_res = bk_res;
+        d.occ = occ;
+        d.occ_shift = occ_shift;
+        d.occ_res = occ_res;
+        d.scatter_rate = {params.scatter_rate[0], params.scatter_rate[1], params.scatter_rate[2]};
+        d.tr_scale = params.tr_scale;
+        d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};
+        d.nee_mode = params.nee_mode;
+        return d;
+    }
+};
+

@@ -122,7 +122,7 @@ MRP_HD void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t 
 }
 MRP_HD float u01(uint32_t x) { return (float)(((x >> 9) << 1) | 1u) * 5.9604644775390625e-8f; }
 
-enum StreamKind : uint32_t { kPixelStream = 0, kLutStream = 1, kBakeStream = 2 };
+enum StreamKind : uint32_t { kPixelStream = 0, kLutStream = 1, kBakeStream = 2, kNeeStream = 3 };
 
 struct Stream {
     uint32_t k0, k1, sub, frame, kind, n;
@@ -153,6 +153,12 @@ MRP_D float fetch_clamp(const float* __restrict__ g, int n, int x, int y, int z)
     x = min(max(x, 0), n - 1); y = min(max(y, 0), n - 1); z = min(max(z, 0), n - 1);
     return __ldg(g + ((size_t)x * n + y) * n + z);
 }
+// lerp with 1 - v computed once by the caller (same operations, same result).
+MRP_D float lerp_w(float a, float b, float v, float omv) { return fa(fm(a, omv), fm(b, v)); }
+// Trilinear fetch.  The eight texels come from per-axis clamped coordinates
+// (so every load is in bounds); border mode then zeroes the texels whose
+// unclamped coordinate lies outside [0, n).  Values and the order of the
+// seven lerps are those of fetch_border / fetch_clamp above.
 template <bool Clamp>
 MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
     f3 uv = adds(pos, 0.5f);
@@ -160,13 +166,31 @@ MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
     float px = fs(fm(uv.x, nf), 0.5f), py = fs(fm(uv.y, nf), 0.5f), pz = fs(fm(uv.z, nf), 0.5f);
     float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
     int x = (int)flx, y = (int)fly, z = (int)flz;
-    float wx = fs(px, (float)x), wy = fs(py, (float)y), wz = fs(pz, (float)z);
-    auto F = [&](int a, int b, int c) { return Clamp ? fetch_clamp(g, n, a, b, c) : fetch_border(g, n, a, b, c); };
-    float c00 = lerp(F(x, y, z), F(x, y, z + 1), wz);
-    float c01 = lerp(F(x, y + 1, z), F(x, y + 1, z + 1), wz);
-    float c10 = lerp(F(x + 1, y, z), F(x + 1, y, z + 1), wz);
-    float c11 = lerp(F(x + 1, y + 1, z), F(x + 1, y + 1, z + 1), wz);
-    return lerp(lerp(c00, c01, wy), lerp(c10, c11, wy), wx);
+    float wx = fs(px, flx), wy = fs(py, fly), wz = fs(pz, flz);
+    float ox = fs(1.0f, wx), oy = fs(1.0f, wy), oz = fs(1.0f, wz);
+    int x0 = min(max(x, 0), n - 1), x1 = min(max(x + 1, 0), n - 1);
+    int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
+    int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
+    const float* p0 = g + (size_t)x0 * n * n;
+    const float* p1 = g + (size_t)x1 * n * n;
+    float t000 = __ldg(p0 + y0 + z0), t001 = __ldg(p0 + y0 + z1), t010 = __ldg(p0 + y1 + z0), t011 = __ldg(p0 + y1 + z1);
+    float t100 = __ldg(p1 + y0 + z0), t101 = __ldg(p1 + y0 + z1), t110 = __ldg(p1 + y1 + z0), t111 = __ldg(p1 + y1 + z1);
+    if (!Clamp) {
+        bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
+        bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
+        bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
+        if (!(vx0 && vx1 && vy0 && vy1 && vz0 && vz1)) {
+            t000 = vx0 && vy0 && vz0 ? t000 : 0.0f; t001 = vx0 && vy0 && vz1 ? t001 : 0.0f;
+            t010 = vx0 && vy1 && vz0 ? t010 : 0.0f; t011 = vx0 && vy1 && vz1 ? t011 : 0.0f;
+            t100 = vx1 && vy0 && vz0 ? t100 : 0.0f; t101 = vx1 && vy0 && vz1 ? t101 : 0.0f;
+            t110 = vx1 && vy1 && vz0 ? t110 : 0.0f; t111 = vx1 && vy1 && vz1 ? t111 : 0.0f;
+        }
+    }
+    float c00 = lerp_w(t000, t001, wz, oz);
+    float c01 = lerp_w(t010, t011, wz, oz);
+    float c10 = lerp_w(t100, t101, wz, oz);
+    float c11 = lerp_w(t110, t111, wz, oz);
+    return lerp_w(lerp_w(c00, c01, wy, oy), lerp_w(c10, c11, wy, oy), wx, ox);
 }
 constexpr int kLut = 512;
 MRP_D float tex_lut(const float* __restrict__ lut, float u, float v) {
@@ -198,10 +222,43 @@ struct VolumeDev {
     f3 scatter_rate;
     float tr_scale;
     f3 sky;
+    int nee_mode;           // tracer NEE: 0 baked grid (reference), 1 one Tr() estimate per vertex
 };
 
-MRP_HD size_t mip_offset(int m) { size_t o = 0; for (int i = 0; i < m; ++i) { size_t r = 256 >> i; o += r * r * r; } return o; }
-MRP_HD size_t tr_offset(int m) { size_t o = 0; for (int i = 0; i < m; ++i) { size_t r = 128 >> i; o += r * r * r; } return o; }
+// ---------------------------------------------------------------------------
+// Tr (core/render.cuh:60-103): ratio tracking while tr > 0.5, then delta
+// tracking with termination until tr <= 0.001, through the full-resolution
+// density.  Both loops share the reference's 10000-iteration bound.
+// ---------------------------------------------------------------------------
+MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float dis, float alpha) {
+    float smax = fm(v.max_density, alpha);
+    float tr = 1.0f, t = 0.0f;
+    int loop = 0;
+    while (loop++ < 10000 && tr > 0.5) {
+        float rk = st.next();
+        t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
+        if (t > dis) break;
+        float d = tex3<false>(v.density, v.res, add(pos, mul(dir, t)));
+        float S = fm(d, alpha);
+        tr = fm(tr, fs(1.0f, fmaxf(0.0f, fd(S, smax))));
+        if (d < 0) t = fs(t, d);
+    }
+    while (loop++ < 10000 && tr > 0.001) {
+        float rk = st.next();
+        t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
+        if (t > dis) break;
+        float d = tex3<false>(v.density, v.res, add(pos, mul(dir, t)));
+        float S = fm(d, alpha);
+        if (st.next() < fmaxf(0.0f, fd(S, smax))) { tr = 0.0f; break; }
+        if (d < 0) t = fs(t, d);
+    }
+    return tr;
+}
+
+// sum_{i<m} (256>>i)^3 = (2^27 - 2^(27-3m)) / 7 and sum_{i<m} (128>>i)^3 =
+// (2^24 - 2^(24-3m)) / 7, both exact in 32 bits for the levels that exist.
+MRP_HD size_t mip_offset(int m) { return (size_t)(((1u << 27) - (1u << (27 - 3 * m))) / 7u); }
+MRP_HD size_t tr_offset(int m) { return (size_t)(((1u << 24) - (1u << (24 - 3 * m))) / 7u); }
 constexpr size_t kMipFloats = 19173961;   // sum_{m<9} (256>>m)^3
 constexpr size_t kTrFloats = 2396745;     // sum_{i<8} (128>>i)^3
 

@@ -149,11 +149,15 @@ cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
     w.ready = true;
     return cudaSuccess;
 }
-cudaError_t tc_ensure_scratch(TcScratch&, size_t) { return cudaSuccess; }
+cudaError_t tc_ensure_scratch(TcScratch& s) {
+    if (s.d) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&s.d, 2 * sizeof(int));
+    if (e != cudaSuccess) { s.d = nullptr; return e; }
+    return cudaMemset(s.d, 0, 2 * sizeof(int));
+}
 void tc_free_scratch(TcScratch& s) {
-    if (s.buf) cudaFree(s.buf);
-    s.buf = nullptr;
-    s.bytes = 0;
+    if (s.d) cudaFree(s.d);
+    s.d = nullptr;
 }
 
 // ---------------------------------------------------------------------------
@@ -575,21 +579,17 @@ struct TcArgs {
     const float* feat;
     const float* gamma;
     int n;
-    const int* rec_count;
-    const int* rec_pix;
-    const float* rec_f;
-    size_t rec_cap;
     float g;
     f3 sr;
-    // outputs
     float* out3;                // row-major [n][3]
-    float4* accum;              // staged: running mean at each record's pixel
-    f3 light_color, scatter_rate, ori;
-    int mean_k;
+    // staged records: segs[0, nseg), or seg0 alone when segs is null
+    const TcSegment* segs;
+    int nseg;
+    TcSegment seg0;
 };
 
 template <int EB, bool STAGED>
-__global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(TcArgs A) {
+__global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __grid_constant__ TcArgs A) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int wbytes = (A.wimg_bytes + 1023) & ~1023;
     uint8_t* wimg = smem;
@@ -597,6 +597,9 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(TcArgs A)
     uint64_t* mbar = reinterpret_cast<uint64_t*>(abuf + kGroups * kABytes);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kGroups);
     int* tile_slot = reinterpret_cast<int*>(tslot + 1);
+    int* seg_start = tile_slot + kGroups;   // staged: first tile of each segment, [nseg + 1]
+    const TcSegment* segs = A.segs ? A.segs : &A.seg0;
+    const int nseg = A.segs ? A.nseg : 1;
 
     const int tid = threadIdx.x, warp = tid / 32;
     // weights -> shared memory
@@ -607,6 +610,14 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(TcArgs A)
         tc::tmem_relinquish();
     }
     if (tid < kGroups) tc::mbar_init(mbar + tid, 1);
+    if (STAGED && tid == 32) {
+        int acc = 0;
+        for (int q = 0; q < nseg; ++q) {
+            seg_start[q] = acc;
+            acc += (*segs[q].rec_count + 127) / 128;
+        }
+        seg_start[nseg] = acc;
+    }
     tc::mbar_fence_init();
     tc::fence_before_sync();
     __syncthreads();
@@ -625,32 +636,39 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(TcArgs A)
     G.err = A.err;
     G.ok = true;
 
-    const int count = STAGED ? *A.rec_count : A.n;
+    const int total_tiles = STAGED ? seg_start[nseg] : (A.n + 127) / 128;
     for (;;) {
         if (G.t == 0) tile_slot[G.g] = atomicAdd(A.tile_counter, 1);
         group_bar(G.g);
         int tile = tile_slot[G.g];
         group_bar(G.g);
-        if (tile * 128 >= count || !G.ok) break;
-        int r = tile * 128 + G.t;
-        bool valid = r < count;
+        if (tile >= total_tiles || !G.ok) break;
         float o[3];
         if (STAGED) {
-            float gamma = valid ? A.rec_f[15 * A.rec_cap + r] : 0.0f;
-            TileFeatures src{A.feat + (size_t)(r >> 5) * 576 * 32 + (r & 31), valid};
-            tc_network<EB>(G, src, A.w32, A.scales, gamma, A.g, A.sr, o);
+            int q = 0;
+            while (tile >= seg_start[q + 1]) ++q;
+            const TcSegment* S = segs + q;
+            const int r = (tile - seg_start[q]) * 128 + G.t;
+            const bool valid = r < *S->rec_count;
+            const size_t cap = S->rec_cap;
+            float gamma = valid ? S->rec_f[15 * cap + r] : 0.0f;
+            TileFeatures src{S->feat + (size_t)(r >> 5) * 576 * 32 + (r & 31), valid};
+            tc_network<EB>(G, src, A.w32, A.scales, gamma, S->g, S->sr, o);
             if (valid && G.ok) {
-                int pix = A.rec_pix[r];
-                f3 hit = mk3(A.rec_f[r], A.rec_f[A.rec_cap + r], A.rec_f[2 * A.rec_cap + r]);
-                f3 res = mul(mul(mk3(o[0], o[1], o[2]), A.light_color), A.scatter_rate);
+                int pix = S->rec_pix[r];
+                f3 hit = mk3(S->rec_f[r], S->rec_f[cap + r], S->rec_f[2 * cap + r]);
+                f3 res = mul(mul(mk3(o[0], o[1], o[2]), S->light_color), S->scatter_rate);
                 float4 v4 = make_float4(fmaxf(res.x, 0.0f), fmaxf(res.y, 0.0f), fmaxf(res.z, 0.0f),
-                                        fmaxf(length(sub(A.ori, hit)), 0.0f));
-                float rate = 1.0f / (float)(1 + A.mean_k);
-                float4 a = A.mean_k == 0 ? make_float4(0, 0, 0, 0) : A.accum[pix];
-                A.accum[pix] = make_float4(lerp(a.x, v4.x, rate), lerp(a.y, v4.y, rate), lerp(a.z, v4.z, rate),
-                                           lerp(a.w, v4.w, rate));
+                                        fmaxf(length(sub(S->ori, hit)), 0.0f));
+                const int mean_k = S->mean_k;
+                float rate = 1.0f / (float)(1 + mean_k);
+                float4 a = mean_k == 0 ? make_float4(0, 0, 0, 0) : S->accum[pix];
+                S->accum[pix] = make_float4(lerp(a.x, v4.x, rate), lerp(a.y, v4.y, rate), lerp(a.z, v4.z, rate),
+                                            lerp(a.w, v4.w, rate));
             }
         } else {
+            const int r = tile * 128 + G.t;
+            const bool valid = r < A.n;
             float gamma = valid ? A.gamma[r] : 0.0f;
             RowFeatures src{A.feat + (size_t)r * 576, valid};
             tc_network<EB>(G, src, A.w32, A.scales, gamma, A.g, A.sr, o);
@@ -670,7 +688,8 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(TcArgs A)
 }
 
 static size_t tc_smem_bytes(int eb) {
-    return (size_t)((image_bytes(eb) + 1023) & ~1023) + kGroups * kABytes + kGroups * 8 + 16;
+    return (size_t)((image_bytes(eb) + 1023) & ~1023) + kGroups * kABytes + kGroups * 8 + 16 +
+           (kTcMaxSegments + 1) * sizeof(int);
 }
 
 template <int EB, bool STAGED>
@@ -725,22 +744,46 @@ cudaError_t tc_launch_mlp_at(const TcWeights& w, bool fp8, const float* feat, co
     return fp8 ? launch_tc<1, false>(a, sms, s) : launch_tc<2, false>(a, sms, s);
 }
 
+TcSegment tc_segment(const VolumeDev& v, const ViewDev& view, const HitRecords& rec, const float* feat,
+                     float4* accum) {
+    TcSegment q{};
+    q.feat = feat;
+    q.rec_count = rec.count;
+    q.rec_pix = rec.pix;
+    q.rec_f = rec.f;
+    q.rec_cap = rec.cap;
+    q.accum = accum;
+    q.sr = mk3(v.scatter_rate.x / 1.001f, v.scatter_rate.y / 1.001f, v.scatter_rate.z / 1.001f);
+    q.light_color = view.light_color;
+    q.scatter_rate = v.scatter_rate;
+    q.ori = view.ori;
+    q.g = view.g;
+    q.mean_k = view.mean_k;
+    return q;
+}
+
 cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
-                              const HitRecords& rec, const float* feat, float4* accum, int sms, cudaStream_t s) {
-    if (!w.ready || !w.d_fp32) return cudaErrorNotReady;
+                              const HitRecords& rec, const float* feat, float4* accum, const TcScratch& sc, int sms,
+                              cudaStream_t s) {
+    if (!w.ready || !w.d_fp32 || !sc.d) return cudaErrorNotReady;
     TcArgs a = base_args(w, fp8);
-    a.feat = feat;
-    a.rec_count = rec.count;
-    a.rec_pix = rec.pix;
-    a.rec_f = rec.f;
-    a.rec_cap = rec.cap;
-    a.g = view.g;
-    a.sr = mk3(v.scatter_rate.x / 1.001f, v.scatter_rate.y / 1.001f, v.scatter_rate.z / 1.001f);
-    a.accum = accum;
-    a.light_color = view.light_color;
-    a.scatter_rate = v.scatter_rate;
-    a.ori = view.ori;
-    a.mean_k = view.mean_k;
+    a.tile_counter = sc.d;
+    a.err = sc.d + 1;
+    a.segs = nullptr;
+    a.nseg = 1;
+    a.seg0 = tc_segment(v, view, rec, feat, accum);
+    return fp8 ? launch_tc<1, true>(a, sms, s) : launch_tc<2, true>(a, sms, s);
+}
+
+cudaError_t tc_launch_mlp_segments(const TcWeights& w, bool fp8, const TcSegment* d_segs, int nseg,
+                                   const TcScratch& sc, int sms, cudaStream_t s) {
+    if (!w.ready || !w.d_fp32 || !sc.d || !d_segs) return cudaErrorNotReady;
+    if (nseg < 1 || nseg > kTcMaxSegments) return cudaErrorInvalidValue;
+    TcArgs a = base_args(w, fp8);
+    a.tile_counter = sc.d;
+    a.err = sc.d + 1;
+    a.segs = d_segs;
+    a.nseg = nseg;
     return fp8 ? launch_tc<1, true>(a, sms, s) : launch_tc<2, true>(a, sms, s);
 }
 

@@ -15,14 +15,33 @@ struct TcWeights {
     int* d_counter = nullptr;  // tile counter of the persistent kernel
     bool ready = false;
 };
-// Per-handle scratch of the tensor-core predictor.
+// Per-handle scratch of the tensor-core predictor: the persistent kernel's
+// tile counter (d[0]) and error flag (d[1]).  Every stream that launches the
+// network needs its own, or two launches would share one tile counter.
 struct TcScratch {
-    void* buf = nullptr;
-    size_t bytes = 0;
+    int* d = nullptr;
 };
-
+// One request's staged records for the network: hit records, tiled features,
+// running-mean image and the constants of its launch.  The batched launch
+// takes up to kTcMaxSegments of them (each request's tiles stay separate).
+struct TcSegment {
+    const float* feat;
+    const int* rec_count;
+    const int* rec_pix;
+    const float* rec_f;
+    size_t rec_cap;
+    float4* accum;
+    f3 sr;                       // network input sigma = scatter_rate / 1.001
+    f3 light_color, scatter_rate, ori;
+    float g;
+    int mean_k;
+};
+constexpr int kTcMaxSegments = 64;
+struct HitRecords;
+TcSegment tc_segment(const VolumeDev& v, const ViewDev& view, const HitRecords& rec, const float* feat,
+                     float4* accum);
 cudaError_t tc_prepare_weights(const float* packed_fp32_host, TcWeights& w);
-cudaError_t tc_ensure_scratch(TcScratch& s, size_t npix);
+cudaError_t tc_ensure_scratch(TcScratch& s);
 void tc_free_scratch(TcScratch& s);
 cudaError_t tc_launch_mlp(const TcWeights& w, bool fp8, const float* feat, const float* gamma, float g, const float sr[3],
                           int n, float* out3, int sms, cudaStream_t s);
@@ -32,9 +51,13 @@ cudaError_t tc_launch_mlp_at(const TcWeights& w, bool fp8, const float* feat, co
                              const float sr[3], int n, float* out3, int* tile_counter, int* err, int sms,
                              cudaStream_t s);
 // Network on the staged predictor's records and tiled features (kernels.h).
-struct HitRecords;
 cudaError_t tc_launch_mlp_rec(const TcWeights& w, bool fp8, const VolumeDev& v, const ViewDev& view,
-                              const HitRecords& rec, const float* feat, float4* accum, int sms, cudaStream_t s);
+                              const HitRecords& rec, const float* feat, float4* accum, const TcScratch& sc, int sms,
+                              cudaStream_t s);
+// The network over several requests' records in one persistent launch:
+// d_segs[0, nseg) in device memory (nseg <= kTcMaxSegments).
+cudaError_t tc_launch_mlp_segments(const TcWeights& w, bool fp8, const TcSegment* d_segs, int nseg,
+                                   const TcScratch& sc, int sms, cudaStream_t s);
 
 // Self-test: D[128][n] = A[128][k] * B[n][k]^T with operands rounded to BF16
 // (or E4M3), k a multiple of 16 (32), n a multiple of 16 up to 128.

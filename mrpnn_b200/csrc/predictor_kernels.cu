@@ -182,7 +182,8 @@ MRP_D void gather_sample(const VolumeDev& v, const PixelFrame& f, int i, float* 
         cur = add(f.pos, mul(f.L, off));
     }
     float d = tex3<false>(mip_level(v, layer), 256 >> layer, cur);
-    *fd_ = logf(fa(1.0f, fd(fm(f.alpha, d), 64.0f)));
+    // x / 64 == x * 2^-6 exactly (both round the same real number)
+    *fd_ = logf(fa(1.0f, fm(fm(f.alpha, d), 0.015625f)));
     if (i == 0) {
         *fh_ = logf(fa(hg(dot(f.X, f.L), f.g), 1.0f));
     } else {

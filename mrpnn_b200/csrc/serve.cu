@@ -1,0 +1,543 @@
+// serve.cu -- the serving loop of include/mrpnn.h (mrp_serve_*): resident
+// volumes, MRPNN render requests admitted into device slots by a memory
+// budget, per-request first hit + gather on the slot's stream, and the
+// network of every request whose features are ready in one batched
+// persistent tcgen05 launch (continuous batching).
+//
+// The reference has no counterpart: VolumeRender::Render renders one frame
+// per synchronous call (core/volume.cu:487-548).  Each result here is the
+// one mrp_render gives for the same view with sample_num 1: the same
+// kernels on the same per-pixel streams; only the network launch is shared.
+//
+// Threads.  API calls only touch the ticket table under `mu`; one worker
+// thread owns every CUDA call of the server.  The worker polls events
+// (cudaEventQuery) and sleeps 20 us when nothing moved, so no wait of the
+// server can hang: the GPU work it waits for is ordinary bounded kernels.
+#include <chrono>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <thread>
+#include <unordered_map>
+
+#include "abi_internal.h"
+
+using namespace mrpi;
+
+namespace {
+using Clock = std::chrono::steady_clock;
+
+struct Ticket {
+    uint64_t id = 0;
+    mrp_request req{};
+    size_t npix = 0;
+    bool done = false;
+    mrp_status status = MRP_OK;
+    std::string error;
+    mrp_request_timing t{};
+};
+
+enum SlotState { kFree, kFeatures, kNetwork, kOutput };
+
+// Device working set of one admitted request.  Buffers grow to the largest
+// request the slot has held and are kept; the budget counts what is held.
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_feat = nullptr, ev_done = nullptr;
+    size_t cap = 0, bytes = 0;
+    float* trs = nullptr;          // this request's TR mips (kTrFloats)
+    int* rec_count = nullptr;
+    int* rec_pix = nullptr;
+    float* rec_f = nullptr;
+    float* feat = nullptr;
+    float4* accum = nullptr;
+    float* staging = nullptr;      // pinned host copy for pageable outputs
+    size_t staging_cap = 0;
+    bool staged_out = false;
+    SlotState state = kFree;
+    std::shared_ptr<Ticket> t;
+    VolumeDev vd{};
+    ViewDev view{};
+    HitRecords records() const { return HitRecords{rec_count, rec_pix, rec_f, cap}; }
+};
+
+size_t slot_bytes(size_t npix) {
+    return kTrFloats * sizeof(float) + sizeof(int) + npix * (sizeof(int) + 16 * sizeof(float) + sizeof(float4)) +
+           tiled_feature_floats(npix) * sizeof(float);
+}
+constexpr size_t kLutBytes = 512 * 512 * sizeof(float);
+
+struct Lut {
+    float g;
+    uint32_t seed;
+    float* d;
+    cudaEvent_t ready;
+};
+
+double ms_since(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
+}  // namespace
+
+struct mrp_server {
+    mrp_serve_config cfg{};
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Ticket>> incoming;                    // guarded by mu
+    std::unordered_map<uint64_t, std::shared_ptr<Ticket>> tickets;   // guarded by mu
+    uint64_t next_id = 1;
+    bool stopping = false;                                           // guarded by mu
+    mrp_serve_stats stats{};                                         // guarded by mu
+    Clock::time_point t0;
+    // worker-only state
+    std::deque<std::shared_ptr<Ticket>> pending;
+    std::vector<Slot> slots;
+    std::vector<Lut> luts;
+    size_t used = 0;
+    cudaStream_t net = nullptr;
+    cudaEvent_t ev_net = nullptr;
+    TcScratch sc;
+    TcSegment* d_segs = nullptr;
+    TcSegment* h_segs = nullptr;   // pinned
+    int* h_err = nullptr;          // pinned
+    std::vector<int> batch;        // slots in the network launch in flight
+    bool net_busy = false;
+
+    void complete(const std::shared_ptr<Ticket>& T, mrp_status st, const std::string& err) {
+        std::lock_guard<std::mutex> lk(mu);
+        T->status = st;
+        T->error = err;
+        T->done = true;
+        T->t.done_ms = ms_since(t0);
+        if (st == MRP_OK) stats.completed++;
+        else stats.failed++;
+        stats.bytes_in_use = used;
+        cv_done.notify_all();
+    }
+    void release(Slot& s) {
+        s.state = kFree;
+        s.t.reset();
+        s.staged_out = false;
+    }
+    void free_buffers(Slot& s) {
+        cudaFree(s.trs); cudaFree(s.rec_count); cudaFree(s.rec_pix); cudaFree(s.rec_f); cudaFree(s.feat);
+        cudaFree(s.accum);
+        s.trs = nullptr; s.rec_count = nullptr; s.rec_pix = nullptr; s.rec_f = nullptr; s.feat = nullptr;
+        s.accum = nullptr;
+        used -= s.bytes;
+        s.bytes = 0;
+        s.cap = 0;
+    }
+    cudaError_t grow(Slot& s, size_t npix) {
+        free_buffers(s);
+        cudaError_t e;
+        if ((e = cudaMalloc(&s.trs, kTrFloats * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&s.rec_count, sizeof(int))) != cudaSuccess ||
+            (e = cudaMalloc(&s.rec_pix, npix * sizeof(int))) != cudaSuccess ||
+            (e = cudaMalloc(&s.rec_f, npix * 16 * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&s.feat, tiled_feature_floats(npix) * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&s.accum, npix * sizeof(float4))) != cudaSuccess) {
+            free_buffers(s);
+            return e;
+        }
+        s.cap = npix;
+        s.bytes = slot_bytes(npix);
+        used += s.bytes;
+        return cudaSuccess;
+    }
+
+    bool admit();
+    bool launch_network();
+    bool finish_network();
+    bool finish_outputs();
+    void enqueue_output(Slot& s, bool after_net);
+    const Lut* lut_for(float g_, uint32_t seed, cudaStream_t s, std::string* err);
+    void run();
+};
+
+// The LUT of (g, seed), shared by every request that asks for it; built once
+// on the stream of the first such request, which the others then wait for.
+const Lut* mrp_server::lut_for(float g_, uint32_t seed, cudaStream_t s, std::string* err) {
+    for (const Lut& l : luts)
+        if (l.g == g_ && l.seed == seed) {
+            cudaStreamWaitEvent(s, l.ready, 0);
+            return &l;
+        }
+    Lut l{g_, seed, nullptr, nullptr};
+    cudaError_t e;
+    if ((e = cudaMalloc(&l.d, kLutBytes)) != cudaSuccess) { *err = cuda_msg("LUT", e); return nullptr; }
+    if ((e = cudaEventCreateWithFlags(&l.ready, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = launch_hg_lut(l.d, g_, seed, s)) != cudaSuccess || (e = cudaEventRecord(l.ready, s)) != cudaSuccess) {
+        cudaFree(l.d);
+        if (l.ready) cudaEventDestroy(l.ready);
+        *err = cuda_msg("LUT", e);
+        return nullptr;
+    }
+    used += kLutBytes;
+    luts.push_back(l);
+    return &luts.back();
+}
+
+// Admission, first come first served: the head request enters when a slot
+// is free and its working set fits the budget (idle slots give their buffers
+// back first if needed).  Then its TR mips, first hit and gather are queued
+// on the slot's stream.
+bool mrp_server::admit() {
+    bool moved = false;
+    while (!pending.empty()) {
+        std::shared_ptr<Ticket> T = pending.front();
+        // a free slot whose buffers already hold the request (the smallest
+        // such), else the free slot with the largest buffers (least growth)
+        int pick = -1;
+        for (int i = 0; i < (int)slots.size(); ++i) {
+            const Slot& c = slots[i];
+            if (c.state != kFree) continue;
+            if (pick < 0) { pick = i; continue; }
+            const Slot& b = slots[pick];
+            bool c_fits = c.cap >= T->npix, b_fits = b.cap >= T->npix;
+            if (c_fits != b_fits ? c_fits : (c_fits ? c.cap < b.cap : c.cap > b.cap)) pick = i;
+        }
+        if (pick < 0) break;
+        Slot& s = slots[pick];
+        mrp_volume* v = T->req.volume;
+        const mrp_view& w = T->req.view;
+        bool need_lut = true;
+        for (const Lut& l : luts)
+            if (l.g == w.g && l.seed == v->params.seed) need_lut = false;
+        size_t need = (s.cap >= T->npix ? 0 : slot_bytes(T->npix) - s.bytes) + (need_lut ? kLutBytes : 0);
+        if (used + need > cfg.memory_budget) {
+            for (Slot& o : slots)   // idle slots give their buffers back
+                if (&o != &s && o.state == kFree && o.bytes && used + need > cfg.memory_budget) free_buffers(o);
+            if (used + need > cfg.memory_budget) break;   // wait for running requests to finish
+        }
+        pending.pop_front();
+        moved = true;
+        T->t.admit_ms = ms_since(t0);
+        cudaError_t e = cudaSuccess;
+        if (s.cap < T->npix && (e = grow(s, T->npix)) != cudaSuccess) {
+            complete(T, MRP_ERR_OOM, cuda_msg("slot buffers", e));
+            continue;
+        }
+        std::string err;
+        const Lut* lut = lut_for(w.g, v->params.seed, s.stream, &err);
+        if (!lut) { complete(T, MRP_ERR_CUDA, err); continue; }
+        s.t = T;
+        s.vd = v->dev();
+        s.vd.trs = s.trs;
+        s.vd.lut = lut->d;
+        s.view = make_view(v, &w, w.frame_offset, 0);
+        HitRecords rec = s.records();
+        if ((e = build_tr_levels(s.trs, v->mips, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
+            (e = launch_hit(s.vd, s.view, rec, s.accum, s.stream)) != cudaSuccess ||
+            (e = launch_gather_rec(s.vd, s.view, rec, s.feat, s.stream)) != cudaSuccess) {
+            complete(T, MRP_ERR_CUDA, cuda_msg("request launch", e));
+            release(s);
+            continue;
+        }
+        if (cfg.precision == MRP_FP32) {   // FP32 network per request, no batching
+            if ((e = launch_mlp_rec_fp32(s.vd, s.view, rec, s.feat, g.d_weights, s.accum, s.stream)) != cudaSuccess) {
+                complete(T, MRP_ERR_CUDA, cuda_msg("network", e));
+                release(s);
+                continue;
+            }
+            T->t.features_ms = T->t.network_ms = ms_since(t0);
+            enqueue_output(s, false);
+        } else {
+            cudaEventRecord(s.ev_feat, s.stream);
+            s.state = kFeatures;
+        }
+    }
+    if (moved) {
+        std::lock_guard<std::mutex> lk(mu);
+        stats.bytes_in_use = used;
+        if (used > stats.peak_bytes) stats.peak_bytes = used;
+    }
+    return moved;
+}
+
+// One persistent launch over every request whose features are ready.
+bool mrp_server::launch_network() {
+    if (net_busy) return false;
+    batch.clear();
+    for (int i = 0; i < (int)slots.size() && (int)batch.size() < kTcMaxSegments; ++i) {
+        Slot& s = slots[i];
+        if (s.state != kFeatures) continue;
+        cudaError_t q = cudaEventQuery(s.ev_feat);
+        if (q == cudaErrorNotReady) continue;
+        if (q != cudaSuccess) {
+            complete(s.t, MRP_ERR_CUDA, cuda_msg("features", q));
+            release(s);
+            continue;
+        }
+        s.t->t.features_ms = ms_since(t0);
+        h_segs[batch.size()] = tc_segment(s.vd, s.view, s.records(), s.feat, s.accum);
+        batch.push_back(i);
+    }
+    if (batch.empty()) return false;
+    int n = (int)batch.size();
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(d_segs, h_segs, n * sizeof(TcSegment), cudaMemcpyHostToDevice, net)) != cudaSuccess ||
+        (e = cudaMemsetAsync(sc.d + 1, 0, sizeof(int), net)) != cudaSuccess ||
+        (e = tc_launch_mlp_segments(g.tc, cfg.precision == MRP_FP8, d_segs, n, sc, g.sms, net)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h_err, sc.d + 1, sizeof(int), cudaMemcpyDeviceToHost, net)) != cudaSuccess ||
+        (e = cudaEventRecord(ev_net, net)) != cudaSuccess) {
+        for (int i : batch) {
+            complete(slots[i].t, MRP_ERR_CUDA, cuda_msg("batched network", e));
+            release(slots[i]);
+        }
+        batch.clear();
+        return true;
+    }
+    for (int i : batch) slots[i].state = kNetwork;
+    net_busy = true;
+    std::lock_guard<std::mutex> lk(mu);
+    stats.batches++;
+    stats.batched_requests += n;
+    if (n > stats.max_batch) stats.max_batch = n;
+    return true;
+}
+
+bool mrp_server::finish_network() {
+    if (!net_busy) return false;
+    cudaError_t q = cudaEventQuery(ev_net);
+    if (q == cudaErrorNotReady) return false;
+    net_busy = false;
+    for (int i : batch) {
+        Slot& s = slots[i];
+        s.t->t.network_ms = ms_since(t0);
+        if (q != cudaSuccess || *h_err) {
+            complete(s.t, q != cudaSuccess ? MRP_ERR_CUDA : MRP_ERR_TIMEOUT,
+                     q != cudaSuccess ? cuda_msg("batched network", q) : "tensor-core MLP: MMA completion wait timed out");
+            release(s);
+            continue;
+        }
+        enqueue_output(s, true);
+    }
+    batch.clear();
+    return true;
+}
+
+// Result to the caller's buffer on the slot's stream: device and pinned host
+// buffers directly, pageable host memory through the slot's pinned staging.
+void mrp_server::enqueue_output(Slot& s, bool after_net) {
+    const size_t bytes = s.t->npix * sizeof(float4);
+    float* out = s.t->req.out_rgba;
+    cudaError_t e = cudaSuccess;
+    if (after_net) e = cudaStreamWaitEvent(s.stream, ev_net, 0);
+    s.staged_out = false;
+    if (e == cudaSuccess) {
+        if (s.t->req.out_is_device) {
+            e = cudaMemcpyAsync(out, s.accum, bytes, cudaMemcpyDeviceToDevice, s.stream);
+        } else {
+            cudaPointerAttributes at{};
+            bool pinned = cudaPointerGetAttributes(&at, out) == cudaSuccess && at.type == cudaMemoryTypeHost;
+            cudaGetLastError();
+            if (pinned) {
+                e = cudaMemcpyAsync(out, s.accum, bytes, cudaMemcpyDeviceToHost, s.stream);
+            } else {
+                if (s.staging_cap < bytes) {
+                    if (s.staging) cudaFreeHost(s.staging);
+                    s.staging = nullptr;
+                    s.staging_cap = 0;
+                    e = cudaMallocHost(&s.staging, bytes);
+                    if (e == cudaSuccess) s.staging_cap = bytes;
+                }
+                if (e == cudaSuccess) e = cudaMemcpyAsync(s.staging, s.accum, bytes, cudaMemcpyDeviceToHost, s.stream);
+                s.staged_out = true;
+            }
+        }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(s.ev_done, s.stream);
+    if (e != cudaSuccess) {
+        complete(s.t, MRP_ERR_CUDA, cuda_msg("result copy", e));
+        release(s);
+        return;
+    }
+    s.state = kOutput;
+}
+
+bool mrp_server::finish_outputs() {
+    bool moved = false;
+    for (Slot& s : slots) {
+        if (s.state != kOutput) continue;
+        cudaError_t q = cudaEventQuery(s.ev_done);
+        if (q == cudaErrorNotReady) continue;
+        moved = true;
+        if (q == cudaSuccess && s.staged_out) std::memcpy(s.t->req.out_rgba, s.staging, s.t->npix * sizeof(float4));
+        std::shared_ptr<Ticket> T = s.t;
+        release(s);
+        complete(T, q == cudaSuccess ? MRP_OK : MRP_ERR_CUDA, q == cudaSuccess ? "" : cuda_msg("result copy", q));
+    }
+    return moved;
+}
+
+void mrp_server::run() {
+    cudaSetDevice(g.device);
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            while (!incoming.empty()) {
+                pending.push_back(incoming.front());
+                incoming.pop_front();
+            }
+            bool busy = !pending.empty() || net_busy;
+            for (const Slot& s : slots) busy = busy || s.state != kFree;
+            if (!busy) {
+                if (stopping) return;
+                cv_work.wait_for(lk, std::chrono::milliseconds(20));
+                continue;
+            }
+        }
+        bool moved = finish_outputs();
+        moved = finish_network() || moved;
+        moved = launch_network() || moved;
+        moved = admit() || moved;
+        if (!moved) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+extern "C" {
+
+void mrp_serve_default_config(mrp_serve_config* c) {
+    if (!c) return;
+    c->memory_budget = (size_t)120 << 30;
+    c->max_slots = 16;
+    c->precision = MRP_BF16;
+}
+
+mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
+    TRY(need_init());
+    if (!out) return fail(MRP_ERR_INVALID, "null argument");
+    mrp_serve_config cfg;
+    mrp_serve_default_config(&cfg);
+    if (cfg_in) cfg = *cfg_in;
+    if (cfg.max_slots < 1 || cfg.max_slots > kTcMaxSegments)
+        return fail(MRP_ERR_INVALID, "max_slots %d out of range [1, %d]", cfg.max_slots, kTcMaxSegments);
+    if (cfg.precision != MRP_FP32 && cfg.precision != MRP_BF16 && cfg.precision != MRP_FP8)
+        return fail(MRP_ERR_INVALID, "unknown precision %d", (int)cfg.precision);
+    std::unique_ptr<mrp_server> S(new mrp_server());
+    S->cfg = cfg;
+    S->t0 = Clock::now();
+    auto cleanup = [&](mrp_status st) {
+        mrp_server* p = S.release();
+        p->stopping = true;
+        for (Slot& s : p->slots) {
+            p->free_buffers(s);
+            if (s.stream) cudaStreamDestroy(s.stream);
+            if (s.ev_feat) cudaEventDestroy(s.ev_feat);
+            if (s.ev_done) cudaEventDestroy(s.ev_done);
+        }
+        if (p->net) cudaStreamDestroy(p->net);
+        if (p->ev_net) cudaEventDestroy(p->ev_net);
+        tc_free_scratch(p->sc);
+        cudaFree(p->d_segs);
+        if (p->h_segs) cudaFreeHost(p->h_segs);
+        if (p->h_err) cudaFreeHost(p->h_err);
+        delete p;
+        return st;
+    };
+    cudaError_t e;
+    S->slots.resize(cfg.max_slots);
+    for (Slot& s : S->slots)
+        if ((e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&s.ev_feat, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&s.ev_done, cudaEventDisableTiming)) != cudaSuccess)
+            return cleanup(fail(MRP_ERR_CUDA, "slot streams: %s", cudaGetErrorString(e)));
+    if ((e = cudaStreamCreateWithFlags(&S->net, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&S->ev_net, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = tc_ensure_scratch(S->sc)) != cudaSuccess ||
+        (e = cudaMalloc(&S->d_segs, kTcMaxSegments * sizeof(TcSegment))) != cudaSuccess ||
+        (e = cudaMallocHost(&S->h_segs, kTcMaxSegments * sizeof(TcSegment))) != cudaSuccess ||
+        (e = cudaMallocHost(&S->h_err, sizeof(int))) != cudaSuccess)
+        return cleanup(fail(MRP_ERR_CUDA, "server set-up: %s", cudaGetErrorString(e)));
+    *S->h_err = 0;
+    mrp_server* p = S.release();
+    p->worker = std::thread([p] { p->run(); });
+    *out = p;
+    return MRP_OK;
+}
+
+mrp_status mrp_serve_submit(mrp_server* S, const mrp_request* r, uint64_t* ticket) {
+    if (!S || !r || !ticket) return fail(MRP_ERR_INVALID, "null argument");
+    const mrp_view& w = r->view;
+    if (!r->volume || !r->out_rgba) return fail(MRP_ERR_INVALID, "request needs a volume and an output buffer");
+    if (!r->volume->has_pyramid) return fail(MRP_ERR_NOT_READY, "volume has no pyramid (call mrp_volume_update)");
+    if (w.width <= 0 || w.height <= 0 || (long long)w.width * w.height > (1ll << 26))
+        return fail(MRP_ERR_INVALID, "image size %dx%d", w.width, w.height);
+    auto T = std::make_shared<Ticket>();
+    T->req = *r;
+    T->npix = (size_t)w.width * w.height;
+    size_t need = slot_bytes(T->npix) + kLutBytes;
+    if (need > S->cfg.memory_budget)
+        return fail(MRP_ERR_BUDGET, "request needs %zu bytes, budget is %zu", need, S->cfg.memory_budget);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stopping) return fail(MRP_ERR_NOT_READY, "server is closing");
+    T->id = S->next_id++;
+    T->t.submit_ms = ms_since(S->t0);
+    S->tickets[T->id] = T;
+    S->incoming.push_back(T);
+    S->stats.submitted++;
+    *ticket = T->id;
+    S->cv_work.notify_one();
+    return MRP_OK;
+}
+
+mrp_status mrp_serve_poll(mrp_server* S, uint64_t ticket, int wait_ms, int* done, mrp_request_timing* timing) {
+    if (!S || !done) return fail(MRP_ERR_INVALID, "null argument");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->tickets.find(ticket);
+    if (it == S->tickets.end()) return fail(MRP_ERR_INVALID, "unknown ticket %llu", (unsigned long long)ticket);
+    std::shared_ptr<Ticket> T = it->second;
+    if (!T->done && wait_ms != 0) {
+        if (wait_ms < 0) S->cv_done.wait(lk, [&] { return T->done; });
+        else S->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return T->done; });
+    }
+    *done = T->done ? 1 : 0;
+    if (!T->done) return MRP_OK;
+    if (timing) *timing = T->t;
+    S->tickets.erase(it);
+    if (T->status != MRP_OK) return fail(T->status, "%s", T->error.c_str());
+    return MRP_OK;
+}
+
+mrp_status mrp_serve_stats_get(mrp_server* S, mrp_serve_stats* st) {
+    if (!S || !st) return fail(MRP_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    *st = S->stats;
+    return MRP_OK;
+}
+
+mrp_status mrp_serve_close(mrp_server* S) {
+    if (!S) return fail(MRP_ERR_INVALID, "null server");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stopping = true;
+        S->cv_work.notify_all();
+    }
+    if (S->worker.joinable()) S->worker.join();
+    for (Slot& s : S->slots) {
+        S->free_buffers(s);
+        if (s.staging) cudaFreeHost(s.staging);
+        cudaStreamDestroy(s.stream);
+        cudaEventDestroy(s.ev_feat);
+        cudaEventDestroy(s.ev_done);
+    }
+    for (Lut& l : S->luts) {
+        cudaFree(l.d);
+        cudaEventDestroy(l.ready);
+    }
+    cudaStreamDestroy(S->net);
+    cudaEventDestroy(S->ev_net);
+    tc_free_scratch(S->sc);
+    cudaFree(S->d_segs);
+    cudaFreeHost(S->h_segs);
+    cudaFreeHost(S->h_err);
+    delete S;
+    return MRP_OK;
+}
+
+}  // extern "C"

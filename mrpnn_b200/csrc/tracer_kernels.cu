@@ -3,7 +3,9 @@
 //
 // Reference: RenderCamera<false> -> CalculateRadiance (core/volume.cu:198-228,
 // core/render.cuh:535-597), free flights by DeterminateNextVertex
-// (core/render.cuh:399-434) with NEE through the baked transmittance grid.
+// (core/render.cuh:399-434) with NEE through the baked transmittance grid
+// (nee_mode 0, the reference) or one unbiased Tr() estimate per vertex from
+// the sample's own NEE stream (nee_mode 1; the error reference).
 //
 // B200 form: a persistent kernel pulls (pixel, sample) work items from a
 // global counter, so a lane whose path ended starts the next one instead of
@@ -56,6 +58,7 @@ MRP_D f3 camera_ray_t(const ViewDev& w, int row, int col) {
 // Radiance of sample k of one pixel (CalculateRadiance's loop body).
 MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 ori, f3 dir, float dis, f3 L, Tally* tl) {
     Stream st(kPixelStream, (uint32_t)pix, (uint32_t)k, (uint32_t)w.frame, w.seed);
+    Stream nst(kNeeStream, (uint32_t)pix, (uint32_t)k, (uint32_t)w.frame, w.seed);   // nee_mode 1 only
     f3 res = mk3(0, 0, 0);
     f3 p = add(ori, mul(dir, dis)), rd = dir, csr = mk3(1, 1, 1);
     for (int b = 0; b < w.multi_scatter; ++b) {
@@ -69,7 +72,8 @@ MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 o
         p = np;
         csr = mul(csr, v.scatter_rate);
         float ph = hg(dot(rd, L), w.g);
-        float tr = tex3<true>(v.baked, v.baked_res, p);
+        float tr = v.nee_mode ? transmittance(v, nst, p, L, ray_box_distance(p, L), w.alpha)
+                              : tex3<true>(v.baked, v.baked_res, p);
         if (tl) tl->lookups++;
         res = add(res, mul(mul(w.light_color, csr), fm(tr, ph)));
         rd = nd;

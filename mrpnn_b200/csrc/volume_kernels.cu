@@ -240,36 +240,7 @@ __global__ void k_hg_lut(float* __restrict__ lut, float g, uint32_t seed) {
     lut[j * kLut + i] = fd(h, 1024.0f);
 }
 
-// ---------------------------------------------------------------------------
-// Tr (core/render.cuh:60-103): ratio tracking while tr > 0.5, then delta
-// tracking with termination until tr <= 0.001, through Density().
-// ---------------------------------------------------------------------------
 MRP_D float density(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
-
-MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float dis, float alpha) {
-    float smax = fm(v.max_density, alpha);
-    float tr = 1.0f, t = 0.0f;
-    int loop = 0;
-    while (loop++ < 10000 && tr > 0.5) {
-        float rk = st.next();
-        t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
-        if (t > dis) break;
-        float d = density(v, add(pos, mul(dir, t)));
-        float S = fm(d, alpha);
-        tr = fm(tr, fs(1.0f, fmaxf(0.0f, fd(S, smax))));
-        if (d < 0) t = fs(t, d);
-    }
-    while (loop++ < 10000 && tr > 0.001) {
-        float rk = st.next();
-        t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
-        if (t > dis) break;
-        float d = density(v, add(pos, mul(dir, t)));
-        float S = fm(d, alpha);
-        if (st.next() < fmaxf(0.0f, fd(S, smax))) { tr = 0.0f; break; }
-        if (d < 0) t = fs(t, d);
-    }
-    return tr;
-}
 
 // Fill_BakeTR (core/volume.cu:1562-1587) over voxels [first, first+count).
 // replicate != 0 restarts the voxel's stream for every estimate, as InitRand

@@ -1050,6 +1050,9 @@ void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, 
             bool any = false;
             for (int k = 0; k < v->spp; ++k) {
                 Stream st(0, (uint32_t)pix, (uint32_t)k, (uint32_t)v->frame, v->seed);
+                // unbiased NEE (no baked grid): one Tr() estimate per vertex
+                // from the sample's own NEE stream (kind 3)
+                Stream nst(3, (uint32_t)pix, (uint32_t)k, (uint32_t)v->frame, v->seed);
                 f3 res = {0, 0, 0};
                 f3 p = ori + dir * dis, rd = dir, csr = {1, 1, 1};
                 for (int b = 0; b < v->multi_scatter; ++b) {
@@ -1062,7 +1065,8 @@ void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, 
                     p = np;
                     csr = csr * srate;
                     float ph = hg(dot(rd, L), v->g);
-                    float tr = tex3(s->baked_tr, s->baked_res, p, true);
+                    float tr = s->baked_tr ? tex3(s->baked_tr, s->baked_res, p, true)
+                                           : transmittance(s, nst, p, L, ray_box_distance(p, L), v->alpha);
                     res = res + (lc * csr) * (tr * ph);
                     rd = nd;
                 }

@@ -38,7 +38,8 @@ typedef struct orc_scene {
     const float* mips;      /* 9 levels, level m is (256>>m)^3, concatenated    */
     const float* tr_mips;   /* 8 levels, level i is (128>>i)^3, concatenated    */
     const float* hg_lut;    /* 512x512, index v_row*512 + u_col                 */
-    const float* baked_tr;  /* NEE transmittance grid used by the tracer        */
+    const float* baked_tr;  /* NEE transmittance grid used by the tracer; NULL:
+                               one Tr() estimate per vertex instead (unbiased)   */
     int baked_res;
     float scatter_rate[3];  /* "scatter_rate" (core/render.cuh:17)              */
     float tr_scale;         /* "tr_scale" (core/render.cuh:16)                  */

@@ -61,6 +61,20 @@ def test_default_params():
     assert p.bake_res == 768 and p.tr_scale == 1.0 and p.precision == 0
 
 
+def test_serve_defaults_and_no_gpu_refusal():
+    import ctypes as C
+    import mrpnn_b200
+    from mrpnn_b200 import api
+    cfg = api.ServeConfig()
+    api.lib().mrp_serve_default_config(C.byref(cfg))
+    assert cfg.memory_budget == 120 << 30 and cfg.max_slots == 16 and cfg.precision == api.BF16
+    p = mrpnn_b200.default_params()
+    assert p.nee_mode == 0
+    if not _has_gpu():
+        h = C.c_void_p()
+        assert api.lib().mrp_serve_open(C.byref(cfg), C.byref(h)) == api.ERR_NOT_READY
+
+
 def test_model_file_layout():
     """The packed model file holds the 146 reference tensors plus the stencil."""
     import struct

@@ -47,3 +47,27 @@ def test_tracer_deterministic(scene):
     b = scene.vol.Render((32, 32), ori, up, right, LIGHT, M.VolumeRender.PT, scene.g, scene.alpha,
                          multiScatter=32, sampleNum=2, spp=8, seed=1)
     np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-7)
+
+
+def test_tracer_unbiased_nee_zscore():
+    """nee_mode 1 (one Tr() estimate per vertex, no baked grid) against the
+    oracle run without a baked grid, same streams, same z-score bar."""
+    import mrpnn_b200 as M
+    sc = Scene(R=64)
+    sc.vol.SetNeeMode(True)
+    W, spp = 40, 32
+    ori, up, right = view_frame()
+    got = sc.vol.Render((W, W), ori, up, right, LIGHT, M.VolumeRender.PT, sc.g, sc.alpha,
+                        multiScatter=64, sampleNum=1, spp=spp, seed=5).reshape(-1, 4)
+    assert not sc.vol.info().has_baked_tr
+    view = O.make_view(W, W, ori, up, right, LIGHT, alpha=sc.alpha, g=sc.g, multi_scatter=64, spp=spp,
+                       seed=5, frame=0)
+    rgba, s, s2 = O.trace_pixels(sc.orc, view, np.arange(W * W, dtype=np.int32))
+    mean = s / spp
+    var = np.maximum(s2 / spp - mean ** 2, 0) * spp / max(spp - 1, 1)
+    se = np.sqrt(2 * var / spp) + 1e-7
+    z = (got[:, :3] - mean) / se
+    zf = z[np.isfinite(z)]
+    assert np.mean(np.abs(zf) < 4) >= 0.999
+    assert abs(zf.mean()) < 0.1
+    assert np.mean(np.isclose(got[:, :3], rgba[:, :3], rtol=1e-5, atol=1e-7).all(axis=1)) > 0.5
