@@ -142,6 +142,21 @@ mrp_status mrp_get_params(const mrp_volume* v, mrp_params* p);
  * in *count when dst is NULL. */
 mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* dst, size_t* count, int dst_is_device);
 
+/* -- volume files: VolumeRender(string path, bool cacheTR) / LoadData
+ * (core/volume.cu:970-1149) --------------------------------------------------------- */
+/* .bin (int32 R, R^3 float32, z fastest), .txt (R then R^3 floats) or .vox
+ * (256^3 integers x 64/255); a path without a .bin suffix reads path + ".bin"
+ * when that cache exists.  Host only (no device needed).  dst == NULL: only
+ * *res is returned. */
+mrp_status mrp_volume_file_read(const char* path, int* res, float* dst, size_t dst_floats);
+/* Writes the .bin format (the reference's cache file). */
+mrp_status mrp_volume_file_write_bin(const char* path, const float* data, int res);
+/* Reads a volume file into a new handle and runs mrp_volume_update.  The
+ * reference's four datasets (path containing CLOUD0, CLOUD1, MODEL0, MODEL1)
+ * keep its hard-coded majorants; write_cache = 1 writes path + ".bin" after
+ * parsing a .txt / .vox file, as LoadData does. */
+mrp_status mrp_volume_load(const char* path, int write_cache, mrp_volume** out);
+
 /* -- per-render caches ------------------------------------------------------------ */
 /* VolumeRender::UpdateHGLut(g) (core/volume.cu:1401-1423), cached on g. */
 mrp_status mrp_update_hg_lut(mrp_volume* v, float g);
@@ -247,6 +262,9 @@ typedef struct mrp_serve_config {
     size_t memory_budget;    /* device bytes for request slots and LUTs (default 120 GB) */
     int max_slots;           /* requests on the device at once, 1..64 (default 16) */
     mrp_precision precision; /* network arithmetic (default MRP_BF16)              */
+    size_t slot_pixels;      /* size every slot for this many pixels at open, so
+                                admission never allocates (default 0: slots grow
+                                on demand, stream-ordered, and keep their size) */
 } mrp_serve_config;
 typedef struct mrp_request {
     mrp_volume* volume;      /* resident volume (pyramid built)                    */

@@ -50,7 +50,8 @@ class VolumeInfo(C.Structure):
 
 
 class ServeConfig(C.Structure):
-    _fields_ = [("memory_budget", C.c_size_t), ("max_slots", C.c_int), ("precision", C.c_int)]
+    _fields_ = [("memory_budget", C.c_size_t), ("max_slots", C.c_int), ("precision", C.c_int),
+                ("slot_pixels", C.c_size_t)]
 
 
 class Request(C.Structure):
@@ -101,6 +102,9 @@ _SIGS = {
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "mrp_volume_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
+    "mrp_volume_file_write_bin": ([C.c_char_p, C.c_void_p, C.c_int], C.c_int),
+    "mrp_volume_load": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "mrp_serve_default_config": ([C.POINTER(ServeConfig)], None),
     "mrp_serve_open": ([C.POINTER(ServeConfig), C.POINTER(C.c_void_p)], C.c_int),
     "mrp_serve_submit": ([C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
@@ -193,6 +197,24 @@ def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
     return out
 
 
+def read_volume_file(path):
+    """mrp_volume_file_read: a .bin / .txt / .vox volume as float32 [R, R, R]
+    (z fastest), on the host; no device needed."""
+    r = C.c_int()
+    _check(lib().mrp_volume_file_read(path.encode(), C.byref(r), None, 0))
+    out = np.empty((r.value,) * 3, np.float32)
+    _check(lib().mrp_volume_file_read(path.encode(), C.byref(r), out.ctypes.data, out.size))
+    return out
+
+
+def write_volume_bin(path, data):
+    """mrp_volume_file_write_bin: the reference's .bin cache format."""
+    data = _host_f32(data)
+    R = data.shape[0]
+    assert data.shape == (R, R, R)
+    _check(lib().mrp_volume_file_write_bin(path.encode(), data.ctypes.data, R))
+
+
 NOALLOC_MAX_POINTS = 2048   # MRP_NOALLOC_MAX_POINTS in include/mrpnn.h
 
 
@@ -227,12 +249,21 @@ class VolumeRender:
     """VolumeRender (core/volume.hpp:45-155) over a device-resident volume handle."""
     PT, RPNN, MRPNN = 0, 1, 2
 
-    def __init__(self, resolution):
+    def __init__(self, resolution, cacheTR=False, write_cache=True):
+        """VolumeRender(int resolution) or VolumeRender(string path, bool
+        cacheTR) (core/volume.cu:948-967): a path loads a .bin / .txt / .vox
+        file (LoadData) and runs Update; cacheTR has no effect here (the baked
+        TR grid is sized by SetBakeResolution, not by the load)."""
         _ensure_init()
         h = C.c_void_p()
-        _check(lib().mrp_volume_create(int(resolution), C.byref(h)))
-        self._h = h
-        self.resolution = int(resolution)
+        if isinstance(resolution, (str, bytes, os.PathLike)):
+            _check(lib().mrp_volume_load(os.fsencode(resolution), 1 if write_cache else 0, C.byref(h)))
+            self._h = h
+            self.resolution = int(self.info().res)
+        else:
+            _check(lib().mrp_volume_create(int(resolution), C.byref(h)))
+            self._h = h
+            self.resolution = int(resolution)
         self._params = default_params()
         self._view_seed = 0
 
@@ -485,7 +516,7 @@ class Server:
     numpy arrays (pinned or pageable) or CUDA tensors; they must stay alive
     until the ticket is polled done, which this wrapper takes care of."""
 
-    def __init__(self, memory_budget=None, max_slots=16, precision=BF16):
+    def __init__(self, memory_budget=None, max_slots=16, precision=BF16, slot_pixels=0):
         _ensure_init()
         cfg = ServeConfig()
         lib().mrp_serve_default_config(C.byref(cfg))
@@ -493,6 +524,7 @@ class Server:
             cfg.memory_budget = int(memory_budget)
         cfg.max_slots = int(max_slots)
         cfg.precision = int(precision)
+        cfg.slot_pixels = int(slot_pixels)
         h = C.c_void_p()
         _check(lib().mrp_serve_open(C.byref(cfg), C.byref(h)))
         self._h = h

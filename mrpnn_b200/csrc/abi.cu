@@ -269,7 +269,8 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
         (e = cudaMalloc(&v->mips, kMipFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->lut, kLut * kLut * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess)
+        (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
+        (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
                             cudaGetErrorString(e)));
     cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
@@ -281,7 +282,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
     cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
-    cudaFree(v->occ); cudaFree(v->d_maxbits); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
+    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     tc_free_scratch(v->tc);
@@ -388,6 +389,9 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
             src = dst;
             src_res = r;
         }
+        for (int m = 0; m < kOccMips; ++m)
+            CU(launch_occupancy(v->mips + mip_offset(m), 256 >> m, 3, 32 >> m, v->mip_occ + mip_occ_offset(m), g.sms,
+                                v->stream));
         CU(cudaStreamSynchronize(v->stream));
         cudaFree(tmp[0]);
         cudaFree(tmp[1]);
@@ -468,10 +472,12 @@ mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* 
 namespace mrpi {
 // Fill_TR for all 8 TR levels: level lv (res 128 >> lv) through density mip
 // lv + 1 with alpha / 1.73^(lv + 1) (core/volume.cu:1535-1560).
-cudaError_t build_tr_levels(float* trs, const float* mips, const float L[3], float alpha, cudaStream_t s) {
+cudaError_t build_tr_levels(float* trs, const float* mips, const uint8_t* mip_occ, const float L[3], float alpha,
+                            cudaStream_t s) {
     for (int lv = 0; lv < 8; ++lv) {
         float a = alpha / std::pow(1.73f, (float)lv + 1.0f);
-        cudaError_t e = launch_tr_level(trs + tr_offset(lv), 128 >> lv, mips + mip_offset(lv + 1), a, L, g.sms, s);
+        const uint8_t* occ = mip_occ && lv + 1 < kOccMips ? mip_occ + mip_occ_offset(lv + 1) : nullptr;
+        cudaError_t e = launch_tr_level(trs + tr_offset(lv), 128 >> lv, mips + mip_offset(lv + 1), occ, a, L, g.sms, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -490,7 +496,7 @@ static mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) 
     if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "TR mips need the pyramid (call mrp_volume_update)");
     if (v->has_tr && v->tr_alpha == alpha && v->tr_light[0] == L[0] && v->tr_light[1] == L[1] && v->tr_light[2] == L[2])
         return MRP_OK;
-    CU(build_tr_levels(v->trs, v->mips, L, alpha, v->stream));
+    CU(build_tr_levels(v->trs, v->mips, v->mip_occ, L, alpha, v->stream));
     v->has_tr = true;
     v->tr_alpha = alpha;
     std::memcpy(v->tr_light, L, sizeof v->tr_light);

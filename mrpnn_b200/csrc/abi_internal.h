@@ -37,7 +37,8 @@ extern Lib g;
 // Device view of one camera launch (RenderCamera's arguments).
 ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k);
 // Fill_TR for the 8 TR levels of a pyramid into trs (kTrFloats floats).
-cudaError_t build_tr_levels(float* trs, const float* mips, const float L[3], float alpha, cudaStream_t s);
+cudaError_t build_tr_levels(float* trs, const float* mips, const uint8_t* mip_occ, const float L[3], float alpha,
+                            cudaStream_t s);
 
 inline mrp_status need_init() {
     if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");
@@ -80,6 +81,7 @@ struct mrp_volume {
     float* baked = nullptr;
     int baked_alloc_res = 0;
     uint8_t* occ = nullptr;
+    uint8_t* mip_occ = nullptr;   // bricks of mip levels 0..kOccMips-1
     int occ_shift = 3, occ_res = 0;
     int* d_maxbits = nullptr;
     bool has_data = false, has_pyramid = false, has_lut = false, has_tr = false, has_baked = false;
@@ -125,6 +127,7 @@ struct mrp_volume {
         d.tr_scale = params.tr_scale;
         d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};
         d.nee_mode = params.nee_mode;
+        d.mip_occ = has_pyramid ? mip_occ : nullptr;
         return d;
     }
 };

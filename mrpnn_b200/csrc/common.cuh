@@ -204,6 +204,13 @@ MRP_D float tex_lut(const float* __restrict__ lut, float u, float v) {
     return lerp(r0, r1, wx);
 }
 
+// sum_{i<m} (256>>i)^3 = (2^27 - 2^(27-3m)) / 7 and sum_{i<m} (128>>i)^3 =
+// (2^24 - 2^(24-3m)) / 7, both exact in 32 bits for the levels that exist.
+MRP_HD size_t mip_offset(int m) { return (size_t)(((1u << 27) - (1u << (27 - 3 * m))) / 7u); }
+MRP_HD size_t tr_offset(int m) { return (size_t)(((1u << 24) - (1u << (24 - 3 * m))) / 7u); }
+constexpr size_t kMipFloats = 19173961;   // sum_{m<9} (256>>m)^3
+constexpr size_t kTrFloats = 2396745;     // sum_{i<8} (128>>i)^3
+
 // ---------------------------------------------------------------------------
 // Device view of one volume's resources (passed by value to kernels).
 // ---------------------------------------------------------------------------
@@ -223,7 +230,43 @@ struct VolumeDev {
     float tr_scale;
     f3 sky;
     int nee_mode;           // tracer NEE: 0 baked grid (reference), 1 one Tr() estimate per vertex
+    const uint8_t* mip_occ; // occupancy of mip levels 0..kOccMips-1 (8^3 bricks, offsets mip_occ_offset)
 };
+
+// ---------------------------------------------------------------------------
+// Empty-space skipping that keeps every result bit-identical: an 8^3 brick
+// is flagged empty only when it and its one-texel apron hold no nonzero
+// texel, so any trilinear footprint whose low corner lies in it reads eight
+// zeros and the filter returns exactly +0 -- the fetch is skipped, never
+// approximated.
+// ---------------------------------------------------------------------------
+constexpr int kOccMips = 5;   // mip levels 0..4 (256^3 .. 16^3) carry bricks
+MRP_HD int mip_occ_offset(int m) { int o = 0; for (int i = 0; i < m; ++i) { int nb = 32 >> i; o += nb * nb * nb; } return o; }
+constexpr int kMipOccBytes = 32 * 32 * 32 + 16 * 16 * 16 + 8 * 8 * 8 + 4 * 4 * 4 + 2 * 2 * 2;
+
+// tex3<false> of an n^3 grid with brick flags occ (nb = ceil(n / 8) per
+// axis, shift 3); returns 0 without touching the grid for empty bricks.
+MRP_D float tex3_occ(const float* __restrict__ g, int n, const uint8_t* __restrict__ occ, int nb, f3 pos) {
+    f3 uv = adds(pos, 0.5f);
+    float nf = (float)n;
+    int x = (int)floorf(fs(fm(uv.x, nf), 0.5f)), y = (int)floorf(fs(fm(uv.y, nf), 0.5f)),
+        z = (int)floorf(fs(fm(uv.z, nf), 0.5f));
+    if (x < -1 || y < -1 || z < -1 || x > n - 1 || y > n - 1 || z > n - 1) return 0.0f;   // footprint outside
+    int b = ((max(x, 0) >> 3) * nb + (max(y, 0) >> 3)) * nb + (max(z, 0) >> 3);
+    if (__ldg(occ + b) == 0) return 0.0f;
+    return tex3<false>(g, n, pos);
+}
+// Density() of the full-resolution grid with its bricks.
+MRP_D float density_occ(const VolumeDev& v, f3 p) {
+    return v.occ ? tex3_occ(v.density, v.res, v.occ, v.occ_res, p) : tex3<false>(v.density, v.res, p);
+}
+// Mip level m of the pyramid (256 >> m) at p, with bricks for m < kOccMips.
+MRP_D float mip_density(const VolumeDev& v, int m, f3 p) {
+    const float* g = v.mips + mip_offset(m);
+    int n = 256 >> m;
+    if (v.mip_occ && m < kOccMips) return tex3_occ(g, n, v.mip_occ + mip_occ_offset(m), 32 >> m, p);
+    return tex3<false>(g, n, p);
+}
 
 // ---------------------------------------------------------------------------
 // Tr (core/render.cuh:60-103): ratio tracking while tr > 0.5, then delta
@@ -238,7 +281,7 @@ MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float 
         float rk = st.next();
         t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
         if (t > dis) break;
-        float d = tex3<false>(v.density, v.res, add(pos, mul(dir, t)));
+        float d = density_occ(v, add(pos, mul(dir, t)));
         float S = fm(d, alpha);
         tr = fm(tr, fs(1.0f, fmaxf(0.0f, fd(S, smax))));
         if (d < 0) t = fs(t, d);
@@ -247,7 +290,7 @@ MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float 
         float rk = st.next();
         t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
         if (t > dis) break;
-        float d = tex3<false>(v.density, v.res, add(pos, mul(dir, t)));
+        float d = density_occ(v, add(pos, mul(dir, t)));
         float S = fm(d, alpha);
         if (st.next() < fmaxf(0.0f, fd(S, smax))) { tr = 0.0f; break; }
         if (d < 0) t = fs(t, d);
@@ -255,12 +298,6 @@ MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float 
     return tr;
 }
 
-// sum_{i<m} (256>>i)^3 = (2^27 - 2^(27-3m)) / 7 and sum_{i<m} (128>>i)^3 =
-// (2^24 - 2^(24-3m)) / 7, both exact in 32 bits for the levels that exist.
-MRP_HD size_t mip_offset(int m) { return (size_t)(((1u << 27) - (1u << (27 - 3 * m))) / 7u); }
-MRP_HD size_t tr_offset(int m) { return (size_t)(((1u << 24) - (1u << (24 - 3 * m))) / 7u); }
-constexpr size_t kMipFloats = 19173961;   // sum_{m<9} (256>>m)^3
-constexpr size_t kTrFloats = 2396745;     // sum_{i<8} (128>>i)^3
 
 // One camera launch (RenderCamera's arguments, core/volume.cu:199).
 struct ViewDev {

@@ -123,9 +123,13 @@ struct mrp_server {
         s.t.reset();
         s.staged_out = false;
     }
+    // Slot buffers are stream-ordered allocations on the slot's stream: a
+    // slot that grows frees and allocates in stream order, without the
+    // device-wide synchronisation of cudaFree.
     void free_buffers(Slot& s) {
-        cudaFree(s.trs); cudaFree(s.rec_count); cudaFree(s.rec_pix); cudaFree(s.rec_f); cudaFree(s.feat);
-        cudaFree(s.accum);
+        for (void* p : {(void*)s.trs, (void*)s.rec_count, (void*)s.rec_pix, (void*)s.rec_f, (void*)s.feat,
+                        (void*)s.accum})
+            if (p) cudaFreeAsync(p, s.stream);
         s.trs = nullptr; s.rec_count = nullptr; s.rec_pix = nullptr; s.rec_f = nullptr; s.feat = nullptr;
         s.accum = nullptr;
         used -= s.bytes;
@@ -135,12 +139,12 @@ struct mrp_server {
     cudaError_t grow(Slot& s, size_t npix) {
         free_buffers(s);
         cudaError_t e;
-        if ((e = cudaMalloc(&s.trs, kTrFloats * sizeof(float))) != cudaSuccess ||
-            (e = cudaMalloc(&s.rec_count, sizeof(int))) != cudaSuccess ||
-            (e = cudaMalloc(&s.rec_pix, npix * sizeof(int))) != cudaSuccess ||
-            (e = cudaMalloc(&s.rec_f, npix * 16 * sizeof(float))) != cudaSuccess ||
-            (e = cudaMalloc(&s.feat, tiled_feature_floats(npix) * sizeof(float))) != cudaSuccess ||
-            (e = cudaMalloc(&s.accum, npix * sizeof(float4))) != cudaSuccess) {
+        if ((e = cudaMallocAsync(&s.trs, kTrFloats * sizeof(float), s.stream)) != cudaSuccess ||
+            (e = cudaMallocAsync(&s.rec_count, sizeof(int), s.stream)) != cudaSuccess ||
+            (e = cudaMallocAsync(&s.rec_pix, npix * sizeof(int), s.stream)) != cudaSuccess ||
+            (e = cudaMallocAsync(&s.rec_f, npix * 16 * sizeof(float), s.stream)) != cudaSuccess ||
+            (e = cudaMallocAsync(&s.feat, tiled_feature_floats(npix) * sizeof(float), s.stream)) != cudaSuccess ||
+            (e = cudaMallocAsync(&s.accum, npix * sizeof(float4), s.stream)) != cudaSuccess) {
             free_buffers(s);
             return e;
         }
@@ -231,7 +235,7 @@ bool mrp_server::admit() {
         s.vd.lut = lut->d;
         s.view = make_view(v, &w, w.frame_offset, 0);
         HitRecords rec = s.records();
-        if ((e = build_tr_levels(s.trs, v->mips, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
+        if ((e = build_tr_levels(s.trs, v->mips, v->mip_occ, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
             (e = launch_hit(s.vd, s.view, rec, s.accum, s.stream)) != cudaSuccess ||
             (e = launch_gather_rec(s.vd, s.view, rec, s.feat, s.stream)) != cudaSuccess) {
             complete(T, MRP_ERR_CUDA, cuda_msg("request launch", e));
@@ -407,6 +411,7 @@ void mrp_serve_default_config(mrp_serve_config* c) {
     c->memory_budget = (size_t)120 << 30;
     c->max_slots = 16;
     c->precision = MRP_BF16;
+    c->slot_pixels = 0;
 }
 
 mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
@@ -419,6 +424,10 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
         return fail(MRP_ERR_INVALID, "max_slots %d out of range [1, %d]", cfg.max_slots, kTcMaxSegments);
     if (cfg.precision != MRP_FP32 && cfg.precision != MRP_BF16 && cfg.precision != MRP_FP8)
         return fail(MRP_ERR_INVALID, "unknown precision %d", (int)cfg.precision);
+    if (cfg.slot_pixels > (1ull << 26)) return fail(MRP_ERR_INVALID, "slot_pixels %zu too large", cfg.slot_pixels);
+    if (cfg.slot_pixels && (slot_bytes(cfg.slot_pixels) + kLutBytes) * (size_t)cfg.max_slots > cfg.memory_budget)
+        return fail(MRP_ERR_BUDGET, "%d slots of %zu pixels exceed the budget of %zu bytes", cfg.max_slots,
+                    cfg.slot_pixels, cfg.memory_budget);
     std::unique_ptr<mrp_server> S(new mrp_server());
     S->cfg = cfg;
     S->t0 = Clock::now();
@@ -455,6 +464,22 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
         (e = cudaMallocHost(&S->h_err, sizeof(int))) != cudaSuccess)
         return cleanup(fail(MRP_ERR_CUDA, "server set-up: %s", cudaGetErrorString(e)));
     *S->h_err = 0;
+    {   // keep freed slot memory in the device pool instead of returning it
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, g.device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
+    if (cfg.slot_pixels) {
+        for (Slot& s : S->slots)
+            if ((e = S->grow(s, cfg.slot_pixels)) != cudaSuccess)
+                return cleanup(fail(MRP_ERR_OOM, "slot buffers: %s", cudaGetErrorString(e)));
+        for (Slot& s : S->slots)
+            if ((e = cudaStreamSynchronize(s.stream)) != cudaSuccess)
+                return cleanup(fail(MRP_ERR_CUDA, "slot buffers: %s", cudaGetErrorString(e)));
+        S->stats.peak_bytes = S->stats.bytes_in_use = S->used;
+    }
     mrp_server* p = S.release();
     p->worker = std::thread([p] { p->run(); });
     *out = p;
@@ -521,6 +546,7 @@ mrp_status mrp_serve_close(mrp_server* S) {
     if (S->worker.joinable()) S->worker.join();
     for (Slot& s : S->slots) {
         S->free_buffers(s);
+        cudaStreamSynchronize(s.stream);
         if (s.staging) cudaFreeHost(s.staging);
         cudaStreamDestroy(s.stream);
         cudaEventDestroy(s.ev_feat);
@@ -536,6 +562,8 @@ mrp_status mrp_serve_close(mrp_server* S) {
     cudaFree(S->d_segs);
     cudaFreeHost(S->h_segs);
     cudaFreeHost(S->h_err);
+    cudaMemPool_t pool;   // give the slots' memory back to the device
+    if (cudaDeviceGetDefaultMemPool(&pool, g.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     delete S;
     return MRP_OK;
 }

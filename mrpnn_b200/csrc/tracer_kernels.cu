@@ -18,6 +18,8 @@
 
 namespace mrp {
 
+// Free-flight lookups stay plain: delta tracking takes few steps in empty
+// bricks, so the brick test cost more than it saved (measured).
 MRP_D float density_t(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
 
 // DeterminateNextVertex.  SampleHenyeyGreenstein(Rand, Rand, ...) takes the

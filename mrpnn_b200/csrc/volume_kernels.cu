@@ -134,7 +134,9 @@ __global__ void k_occupancy(const float* __restrict__ d, int R, int shift, int n
 // (res 128>>level) marched 128 steps toward the light through density level
 // level+1 with alpha scaled by 1.73^(level+1) (core/volume.cu:1636-1653).
 // ---------------------------------------------------------------------------
-__global__ void k_tr_level(float* __restrict__ out, int res, const float* __restrict__ src, float alpha, f3 L) {
+// src_occ (may be null): 8^3 brick flags of src; empty bricks add exactly 0.
+__global__ void k_tr_level(float* __restrict__ out, int res, const float* __restrict__ src,
+                           const uint8_t* __restrict__ src_occ, float alpha, f3 L) {
     size_t n = (size_t)res * res * res;
     float rf = (float)res;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -147,7 +149,7 @@ __global__ void k_tr_level(float* __restrict__ out, int res, const float* __rest
         float acc = 0;
         for (int s = 0; s < 128; ++s) {
             lp = add(lp, mul(L, step));
-            acc = fa(acc, tex3<false>(src, res, lp));
+            acc = fa(acc, src_occ ? tex3_occ(src, res, src_occ, (res + 7) >> 3, lp) : tex3<false>(src, res, lp));
         }
         out[i] = fm(1.0f, fm(expf(fm(fm(-acc, alpha), step)), 1.0f));
     }
@@ -292,9 +294,10 @@ cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* 
     k_occupancy<<<total < sms * 16 ? total : sms * 16, 256, 0, s>>>(d, R, shift, nb, occ);
     return cudaGetLastError();
 }
-cudaError_t launch_tr_level(float* out, int res, const float* src, float alpha, const float L[3], int sms,
-                            cudaStream_t s) {
-    k_tr_level<<<grid_for((size_t)res * res * res, 128, sms), 128, 0, s>>>(out, res, src, alpha, mk3(L[0], L[1], L[2]));
+cudaError_t launch_tr_level(float* out, int res, const float* src, const uint8_t* src_occ, float alpha,
+                            const float L[3], int sms, cudaStream_t s) {
+    k_tr_level<<<grid_for((size_t)res * res * res, 128, sms), 128, 0, s>>>(out, res, src, src_occ, alpha,
+                                                                           mk3(L[0], L[1], L[2]));
     return cudaGetLastError();
 }
 cudaError_t set_halton_permutations(const uint32_t perm[28]) {

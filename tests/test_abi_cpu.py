@@ -68,6 +68,7 @@ def test_serve_defaults_and_no_gpu_refusal():
     cfg = api.ServeConfig()
     api.lib().mrp_serve_default_config(C.byref(cfg))
     assert cfg.memory_budget == 120 << 30 and cfg.max_slots == 16 and cfg.precision == api.BF16
+    assert cfg.slot_pixels == 0
     p = mrpnn_b200.default_params()
     assert p.nee_mode == 0
     if not _has_gpu():

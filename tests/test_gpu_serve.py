@@ -56,7 +56,7 @@ def test_serve_mix_equals_alone(precision):
     reqs = _requests(M, vols, 14, rng)
     alone = [v.render_view(view, M.VolumeRender.MRPNN, 1, np.empty((view.height, view.width, 4), np.float32))
              for v, view in reqs]
-    srv = M.Server(max_slots=4, precision=prec)
+    srv = M.Server(max_slots=4, precision=prec, slot_pixels=128 * 128 if precision == "BF16" else 0)
     try:
         tickets = [srv.submit(v, view) for v, view in reqs]
         for k, t in enumerate(tickets):
