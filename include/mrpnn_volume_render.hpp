@@ -61,6 +61,22 @@ class VolumeRender {
         mrp_default_params(&params);
         datas.assign((size_t)resolution * resolution * resolution, 0.0f);
     }
+    // VolumeRender(string path, bool cacheTR) -> LoadData (core/volume.cu:959-1149):
+    // .bin / .txt / .vox (and the .bin cache beside a parsed file); Update
+    // has run.  cacheTR has no effect: the baked TR grid is sized by
+    // SetBakeResolution, not by the load.
+    explicit VolumeRender(const std::string& path, bool /*cacheTR*/ = false) {
+        mrpnn::ensure_init();
+        mrpnn::check(mrp_volume_file_read(path.c_str(), &resolution, nullptr, 0), "VolumeRender(path)");
+        datas.assign((size_t)resolution * resolution * resolution, 0.0f);
+        mrpnn::check(mrp_volume_file_read(path.c_str(), &resolution, datas.data(), datas.size()), "VolumeRender(path)");
+        mrpnn::check(mrp_volume_load(path.c_str(), 1, &h), "VolumeRender(path)");
+        mrp_default_params(&params);
+        mrp_volume_info info;
+        mrpnn::check(mrp_volume_get_info(h, &info), "VolumeRender(path)");
+        max_density = info.max_density;
+        dirty = false;
+    }
     ~VolumeRender() { mrp_volume_destroy(h); }
     VolumeRender(const VolumeRender&) = delete;
     VolumeRender& operator=(const VolumeRender&) = delete;
