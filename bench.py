@@ -412,6 +412,85 @@ def run_precision(args, vol, local):
     return out
 
 
+LARGE = dict(res=1024, seed=2, freq=8.0, alpha=512.0, albedo=0.999, views=64, size=512, judged=4, judge_size=256,
+             judge_spp=1024, radius=(0.8, 2.0))
+
+
+def run_large(args, local):
+    """Large high-order scattering: 1024^3 fBm (seed 2, freq 8), extinction
+    512, albedo 0.999, g 0.857; a batch of 64 random orbit views at 512^2 in
+    one mrp_render_views call (one FP8 network launch for all views); 4 of
+    the views judged against a 1024-spp path-traced image (baked NEE as the
+    reference renders, <= 512 bounces), both at 256^2."""
+    import torch
+
+    import mrpnn_b200 as M
+    t0 = time.perf_counter()
+    vol = M.VolumeRender(LARGE["res"])
+    vol.generate_fbm(LARGE["seed"], LARGE["freq"])
+    vol.Update()
+    vol.SetScatterRate(LARGE["albedo"])
+    vol.SetSky(SCENE["sky"])
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(77)
+    L = light()
+    sc = np.float32(np.tan(np.deg2rad(SCENE["fov"]) / 2))
+    cams = []
+    for k in range(LARGE["views"]):
+        d = rng.normal(size=3)
+        pos = rng.uniform(*LARGE["radius"]) * d / np.linalg.norm(d)
+        ori, up, right = M.camera_frame(tuple(float(x) for x in pos))
+        cams.append((ori, (up * sc).astype(np.float32), (right * sc).astype(np.float32)))
+    n = LARGE["size"]
+    views = [vol.make_view((n, n), o, u, r, L, SCENE["g"], LARGE["alpha"], seed=k) for k, (o, u, r) in enumerate(cams)]
+    outs = [torch.empty((n, n, 4), dtype=torch.float32, device=f"cuda:{local}") for _ in views]
+    res = {"workload": f"{LARGE['res']}^3 fBm (seed 2, freq 8), alpha {LARGE['alpha']:.0f}, albedo {LARGE['albedo']}, "
+                       f"g {SCENE['g']}, {LARGE['views']} random orbit views at {n}^2 per mrp_render_views call "
+                       "(one batched network launch)", "setup_s": setup_s}
+    for pname, pv in (("fp8", M.FP8), ("bf16", M.BF16), ("fp32", M.FP32)):
+        vol.SetPrecision(pv)
+        vol.render_views(views, outs)
+        ms, st = [], []
+        for _ in range(3):
+            vol.render_views(views, outs)
+            ms.append(vol.last_render_ms())
+            st.append(vol.last_render_stages())
+        t = float(np.median(ms))
+        stg = np.median(np.asarray(st), axis=0)
+        res[pname] = {"ms_per_batch": t, "views_per_s": LARGE["views"] / (t / 1000.0),
+                      "pixels_per_s": LARGE["views"] * n * n / (t / 1000.0),
+                      "stage_ms": {"hit + gather (all views)": float(stg[0]), "network (one launch)": float(stg[1]),
+                                   "copies": float(stg[2])}}
+    # judged views
+    if args.large_judge:
+        vol.SetBakeResolution(768)
+        t1 = time.perf_counter()
+        vol.Update_CachedTR(L, LARGE["alpha"])
+        bake_s = time.perf_counter() - t1
+        m = LARGE["judge_size"]
+        judged = {"reference": f"PT {LARGE['judge_spp']} spp (FP64 per-pixel sums), baked 768^3 NEE, <= 512 bounces, "
+                               f"{m}^2", "bake_s": bake_s, "views": []}
+        for k in range(LARGE["judged"]):
+            o, u, r = cams[k]
+            t1 = time.perf_counter()
+            ref = vol.Render((m, m), o, u, r, L, M.VolumeRender.PT, SCENE["g"], LARGE["alpha"], multiScatter=512,
+                             sampleNum=1, spp=LARGE["judge_spp"], seed=500 + k)
+            pt_s = time.perf_counter() - t1
+            den = float(np.sqrt(np.mean(ref[..., :3].astype(np.float64) ** 2)))
+            one = {"pt_seconds": pt_s}
+            for pname, pv in (("fp32", M.FP32), ("fp8", M.FP8)):
+                vol.SetPrecision(pv)
+                img = vol.Render((m, m), o, u, r, L, M.VolumeRender.MRPNN, SCENE["g"], LARGE["alpha"], sampleNum=16,
+                                 seed=k)
+                dd = img[..., :3].astype(np.float64) - ref[..., :3]
+                one[pname] = {"rel_rmse": float(np.sqrt(np.mean(dd ** 2)) / den),
+                              "lum_rmse_x100": lum_rmse_x100(img, ref)}
+            judged["views"].append(one)
+        res["judged"] = judged
+    vol.close()
+    return res
+
+
 STAGES = ("first hit + bases", "stencil gather", "network")
 # Algorithmic HBM bytes per hit pixel of each predictor stage (fp32 data):
 #   gather : 192 points x (8 density + 8 TR + 2 x 4 LUT texels) x 4 B read,
@@ -525,6 +604,7 @@ def run_mine(args, rank, world, local):
     tracer = run_tracer(args, local) if (rank == 0 and args.tracer_steps > 0) else None
     serving = run_serving(args, local) if (rank == 0 and args.serve_requests > 0) else None
     precision_error = run_precision(args, vol, local) if (rank == 0 and args.rmse_spp > 0) else None
+    large = run_large(args, local) if (rank == 0 and args.large) else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -551,6 +631,7 @@ def run_mine(args, rank, world, local):
             "tracer": tracer,
             "serving": serving,
             "precision_error": precision_error,
+            "large": large,
         }
         print(json.dumps(line), flush=True)
 
@@ -569,6 +650,8 @@ def main():
     ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving workload (0: skip)")
     ap.add_argument("--rmse-spp", type=int, default=4096, help="spp of the PT reference image (0: skip)")
+    ap.add_argument("--large", type=int, default=1, help="run the 1024^3 / 64-view workload (0: skip)")
+    ap.add_argument("--large-judge", type=int, default=1, help="judge 4 large views against the tracer (0: skip)")
     args = ap.parse_args()
     global W, H
     W = H = args.size

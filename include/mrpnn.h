@@ -186,6 +186,15 @@ mrp_status mrp_last_render_ms(const mrp_volume* v, float* ms);
  * MRPNN = first hit + bases, stencil gather, network; PT = paths, resolve, 0. */
 mrp_status mrp_last_render_stages(const mrp_volume* v, float ms[3]);
 
+/* n (1..64) MRPNN views of one volume in one call, the network of all views
+ * in one batched persistent launch.  No counterpart in the reference (its
+ * data generator calls Render once per camera, dataGen.cu:246-328).  The
+ * views share light_dir, alpha and g (one TR / LUT state); each image equals
+ * mrp_render of that view with sample_num 1.  outs[i]: width*height*4
+ * floats.  Stage times (mrp_last_render_stages): hit + gather of all views,
+ * network, result copies. */
+mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* const* outs, int outs_are_device);
+
 /* -- parity entry points (pieces of the path) ---------------------------------------- */
 /* RadiancePredictInternal (core/radiancePredict.cu:301-422) on n feature
  * sets: feat [n][576] = X_Val[192], X_Val_Sub[192], X_Val_Hg[192]; gamma [n];

@@ -105,6 +105,7 @@ _SIGS = {
     "mrp_volume_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
     "mrp_volume_file_write_bin": ([C.c_char_p, C.c_void_p, C.c_int], C.c_int),
     "mrp_volume_load": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "mrp_render_views": ([C.c_void_p, C.POINTER(View), C.c_int, C.POINTER(C.c_void_p), C.c_int], C.c_int),
     "mrp_serve_default_config": ([C.POINTER(ServeConfig)], None),
     "mrp_serve_open": ([C.POINTER(ServeConfig), C.POINTER(C.c_void_p)], C.c_int),
     "mrp_serve_submit": ([C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
@@ -407,6 +408,21 @@ class VolumeRender:
         p, dev = _ptr(out)
         _check(lib().mrp_render(self._h, C.byref(view), int(rt), int(sample_num), p, dev))
         return out
+
+    def render_views(self, views, outs=None):
+        """mrp_render_views: MRPNN images of several views (sharing light,
+        alpha and g) with one batched network launch; numpy outputs by
+        default, or a list of CUDA tensors."""
+        n = len(views)
+        arr = (View * n)(*views)
+        if outs is None:
+            outs = [np.empty((w.height, w.width, 4), np.float32) for w in views]
+        ptrs, devs = zip(*[_ptr(o) for o in outs])
+        if len(set(devs)) != 1:
+            raise ValueError("outputs must be all host or all device buffers")
+        parr = (C.c_void_p * n)(*ptrs)
+        _check(lib().mrp_render_views(self._h, arr, n, parr, devs[0]))
+        return outs
 
     def last_render_ms(self):
         ms = C.c_float()

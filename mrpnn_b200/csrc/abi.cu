@@ -286,6 +286,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     cudaFree(v->counter);
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     tc_free_scratch(v->tc);
+    free_multiview(v);
     if (v->ev0) cudaEventDestroy(v->ev0);
     if (v->ev1) cudaEventDestroy(v->ev1);
     for (auto& ev : v->ev_stage) if (ev) cudaEventDestroy(ev);
@@ -484,7 +485,9 @@ cudaError_t build_tr_levels(float* trs, const float* mips, const uint8_t* mip_oc
 }
 }  // namespace mrpi
 extern "C" {
-static mrp_status update_lut_async(mrp_volume* v, float g_) {
+}  // extern "C"
+namespace mrpi {
+mrp_status update_lut_async(mrp_volume* v, float g_) {
     if (v->has_lut && v->lut_g == g_ && v->lut_seed == v->params.seed) return MRP_OK;
     CU(launch_hg_lut(v->lut, g_, v->params.seed, v->stream));
     v->has_lut = true;
@@ -492,7 +495,7 @@ static mrp_status update_lut_async(mrp_volume* v, float g_) {
     v->lut_seed = v->params.seed;
     return MRP_OK;
 }
-static mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
+mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
     if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "TR mips need the pyramid (call mrp_volume_update)");
     if (v->has_tr && v->tr_alpha == alpha && v->tr_light[0] == L[0] && v->tr_light[1] == L[1] && v->tr_light[2] == L[2])
         return MRP_OK;
@@ -502,6 +505,8 @@ static mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) 
     std::memcpy(v->tr_light, L, sizeof v->tr_light);
     return MRP_OK;
 }
+}  // namespace mrpi
+extern "C" {
 static mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha) {
     int B = v->params.bake_res;
     if (v->has_baked && v->bk_alpha == alpha && v->bk_res == B && v->bk_seed == v->params.seed &&

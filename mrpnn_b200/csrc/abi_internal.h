@@ -15,6 +15,20 @@ struct mrp_volume;
 namespace mrpi {
 using namespace mrp;
 
+// Device buffers of mrp_render_views, kept per volume between calls (grown,
+// never shrunk): records and tiled features of all views concatenated.
+struct MultiViewBuffers {
+    int* rec_count = nullptr;   // [kTcMaxSegments]
+    int* rec_pix = nullptr;     // [total pixels]
+    float* rec_f = nullptr;     // [16 x total pixels]
+    float* feat = nullptr;
+    float4* accum = nullptr;    // [total pixels]
+    TcSegment* d_segs = nullptr;
+    size_t cap_pix = 0, cap_feat = 0;
+    int cap_views = 0;
+};
+void free_multiview(mrp_volume* v);
+
 // Sets the calling thread's last error (mrp_last_error) and returns s.
 mrp_status fail(mrp_status s, const char* fmt, ...);
 
@@ -39,6 +53,11 @@ ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k)
 // Fill_TR for the 8 TR levels of a pyramid into trs (kTrFloats floats).
 cudaError_t build_tr_levels(float* trs, const float* mips, const uint8_t* mip_occ, const float L[3], float alpha,
                             cudaStream_t s);
+
+// Per-volume caches of the predictor, queued on the volume's stream: the HG
+// LUT for g (UpdateHGLut) and the TR mips for (light, alpha) (Update_TR).
+mrp_status update_lut_async(mrp_volume* v, float g);
+mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha);
 
 inline mrp_status need_init() {
     if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");
@@ -107,6 +126,8 @@ struct mrp_volume {
     size_t rec_cap = 0;
     // tensor-core predictor scratch
     TcScratch tc;
+    // mrp_render_views
+    mrpi::MultiViewBuffers mv;
 
     HitRecords records() const { return HitRecords{rec_count, rec_pix, rec_f, rec_cap}; }
 
