@@ -195,6 +195,28 @@ mrp_status mrp_last_render_stages(const mrp_volume* v, float ms[3]);
  * network, result copies. */
 mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* const* outs, int outs_are_device);
 
+/* -- batch ray APIs (core/volume.cu:405-479, 710-834) ---------------------------------
+ * ori / dir / light_dirs: [n][3]; outputs [n][3]; is_device covers inputs and
+ * output alike. */
+/* VolumeRender::GetRadiances: CalculateRadiance (PT, sample_num samples, NEE
+ * as mrp_params.nee_mode) or NNPredict<MRPNN> (network precision as the
+ * volume's params) for each ray; RGB only. */
+mrp_status mrp_get_radiances(mrp_volume* v, const float* ori, const float* dir, int n, const float light_dir[3],
+                             const float light_color[3], float alpha, int multi_scatter, float g, int sample_num,
+                             mrp_render_type type, float* out3, int is_device);
+/* VolumeRender::GetSamples (GetSample, core/render.cuh:615-655), the training
+ * data generator: per task alpha, origin in the medium, view direction,
+ * light direction, g and scatter rate. */
+mrp_status mrp_get_samples(mrp_volume* v, const float* alpha, const float* ori, const float* dir,
+                           const float* light_dirs, const float* g, const float* scatter, int n,
+                           const float light_color[3], int multi_scatter, int sample_num, uint32_t seed, float* out3,
+                           int is_device);
+/* VolumeRender::GetTrs (ShadowTerm_TRs, core/render.cuh:668-680): light
+ * colour x pi x mean of Tr() x HG toward the light. */
+mrp_status mrp_get_trs(mrp_volume* v, float alpha, const float* ori, const float* dir, int n,
+                       const float light_dir[3], const float light_color[3], float g, int sample_num, uint32_t seed,
+                       float* out3, int is_device);
+
 /* -- parity entry points (pieces of the path) ---------------------------------------- */
 /* RadiancePredictInternal (core/radiancePredict.cu:301-422) on n feature
  * sets: feat [n][576] = X_Val[192], X_Val_Sub[192], X_Val_Hg[192]; gamma [n];

@@ -106,6 +106,12 @@ _SIGS = {
     "mrp_volume_file_write_bin": ([C.c_char_p, C.c_void_p, C.c_int], C.c_int),
     "mrp_volume_load": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "mrp_render_views": ([C.c_void_p, C.POINTER(View), C.c_int, C.POINTER(C.c_void_p), C.c_int], C.c_int),
+    "mrp_get_radiances": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, F3, F3, C.c_float, C.c_int, C.c_float,
+                           C.c_int, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "mrp_get_samples": ([C.c_void_p] + [C.c_void_p] * 6 + [C.c_int, F3, C.c_int, C.c_int, C.c_uint32, C.c_void_p,
+                                                            C.c_int], C.c_int),
+    "mrp_get_trs": ([C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_int, F3, F3, C.c_float, C.c_int, C.c_uint32,
+                     C.c_void_p, C.c_int], C.c_int),
     "mrp_serve_default_config": ([C.POINTER(ServeConfig)], None),
     "mrp_serve_open": ([C.POINTER(ServeConfig), C.POINTER(C.c_void_p)], C.c_int),
     "mrp_serve_submit": ([C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
@@ -407,6 +413,45 @@ class VolumeRender:
     def render_view(self, view, rt, sample_num, out):
         p, dev = _ptr(out)
         _check(lib().mrp_render(self._h, C.byref(view), int(rt), int(sample_num), p, dev))
+        return out
+
+    # -- batch ray APIs (core/volume.cu:405-479, 710-834) ---------------------
+    def GetRadiances(self, ori, dir, lightDir, lightColor=(1, 1, 1), alpha=1.0, multiScatter=1, g=0.0, sampleNum=1,
+                     rt=None):
+        """GetRadiances: radiance of explicit rays (PT or MRPNN), [n, 3]."""
+        rt = self.PT if rt is None else rt
+        ori = _host_f32(ori).reshape(-1, 3)
+        dir = _host_f32(dir).reshape(-1, 3)
+        out = np.empty((ori.shape[0], 3), np.float32)
+        _check(lib().mrp_get_radiances(self._h, ori.ctypes.data, dir.ctypes.data, ori.shape[0], _f3(lightDir),
+                                       _f3(lightColor), float(alpha), int(multiScatter), float(g), int(sampleNum),
+                                       int(rt), out.ctypes.data, 0))
+        return out
+
+    def GetSamples(self, alpha, ori, dir, lightDir, g, scatter, lightColor=(1, 1, 1), multiScatter=1, sampleNum=1,
+                   seed=0):
+        """GetSamples: the training-data generator, per-task arrays, [n, 3]."""
+        ori = _host_f32(ori).reshape(-1, 3)
+        n = ori.shape[0]
+        dir = _host_f32(dir).reshape(n, 3)
+        L = _host_f32(lightDir).reshape(n, 3)
+        a = _host_f32(np.broadcast_to(np.asarray(alpha, np.float32), (n,)))
+        gg = _host_f32(np.broadcast_to(np.asarray(g, np.float32), (n,)))
+        sc = _host_f32(np.broadcast_to(np.asarray(scatter, np.float32), (n,)))
+        out = np.empty((n, 3), np.float32)
+        _check(lib().mrp_get_samples(self._h, a.ctypes.data, ori.ctypes.data, dir.ctypes.data, L.ctypes.data,
+                                     gg.ctypes.data, sc.ctypes.data, n, _f3(lightColor), int(multiScatter),
+                                     int(sampleNum), int(seed), out.ctypes.data, 0))
+        return out
+
+    def GetTrs(self, alpha, ori, dir, lightDir, lightColor=(1, 1, 1), g=0.0, sampleNum=1, seed=0):
+        """GetTrs: light colour x pi x mean Tr() x HG toward the light, [n, 3]."""
+        ori = _host_f32(ori).reshape(-1, 3)
+        dir = _host_f32(dir).reshape(-1, 3)
+        out = np.empty((ori.shape[0], 3), np.float32)
+        _check(lib().mrp_get_trs(self._h, float(alpha), ori.ctypes.data, dir.ctypes.data, ori.shape[0],
+                                 _f3(lightDir), _f3(lightColor), float(g), int(sampleNum), int(seed),
+                                 out.ctypes.data, 0))
         return out
 
     def render_views(self, views, outs=None):

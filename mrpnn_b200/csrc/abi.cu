@@ -507,7 +507,9 @@ mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
 }
 }  // namespace mrpi
 extern "C" {
-static mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha) {
+}  // extern "C"
+namespace mrpi {
+mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha) {
     int B = v->params.bake_res;
     if (v->has_baked && v->bk_alpha == alpha && v->bk_res == B && v->bk_seed == v->params.seed &&
         v->bk_light[0] == L[0] && v->bk_light[1] == L[1] && v->bk_light[2] == L[2])
@@ -528,6 +530,9 @@ static mrp_status update_baked_async(mrp_volume* v, const float L[3], float alph
     std::memcpy(v->bk_light, L, sizeof v->bk_light);
     return MRP_OK;
 }
+
+}  // namespace mrpi
+extern "C" {
 
 mrp_status mrp_update_hg_lut(mrp_volume* v, float g_) {
     TRY(need_init());

@@ -58,6 +58,8 @@ cudaError_t build_tr_levels(float* trs, const float* mips, const uint8_t* mip_oc
 // LUT for g (UpdateHGLut) and the TR mips for (light, alpha) (Update_TR).
 mrp_status update_lut_async(mrp_volume* v, float g);
 mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha);
+// The baked NEE grid for (light, alpha) (Update_CachedTR), on the volume's stream.
+mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha);
 
 inline mrp_status need_init() {
     if (!g.ready) return fail(MRP_ERR_NOT_READY, "mrp_init has not been called");

@@ -122,7 +122,8 @@ MRP_HD void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t 
 }
 MRP_HD float u01(uint32_t x) { return (float)(((x >> 9) << 1) | 1u) * 5.9604644775390625e-8f; }
 
-enum StreamKind : uint32_t { kPixelStream = 0, kLutStream = 1, kBakeStream = 2, kNeeStream = 3 };
+enum StreamKind : uint32_t { kPixelStream = 0, kLutStream = 1, kBakeStream = 2, kNeeStream = 3, kSampleStream = 4,
+                             kTrStream = 5 };
 
 struct Stream {
     uint32_t k0, k1, sub, frame, kind, n;
@@ -310,6 +311,10 @@ struct ViewDev {
     int mean_k;        // running-mean index of this launch ("frameNum")
     float pass_rate;   // exp(-(2/res) * max_density * alpha), host libm (DeterminateEstimatedHit)
     unsigned long long* counters;   // optional work counters (see launch_hit / launch_trace), else null
+    // explicit rays instead of the camera (GetRadiances): ray q = pixel q of a
+    // width x 1 launch, origin ray_ori[3q..], direction ray_dir[3q..]
+    const float* ray_ori;
+    const float* ray_dir;
 };
 
 // Per-thread work tally, flushed to ViewDev::counters once per thread.

@@ -59,6 +59,12 @@ inline size_t tiled_feature_floats(size_t n) { return ((n + 31) / 32) * 32 * 576
 cudaError_t launch_trace(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
                          unsigned long long* counter, int sms, cudaStream_t s);
 cudaError_t launch_fill_int(int* p, int n, int value, cudaStream_t s);
+// GetSamples / GetTrs (core/volume.cu:710-834): one thread per task.
+cudaError_t launch_get_samples(const VolumeDev& v, const float* alpha, const float* ori, const float* dir,
+                               const float* ldir, const float* g, const float* scatter, int n, const float lc[3],
+                               int multi_scatter, int spp, uint32_t seed, float* out3, cudaStream_t s);
+cudaError_t launch_get_trs(const VolumeDev& v, float alpha, const float* ori, const float* dir, int n, const float L[3],
+                           const float lc[3], float g, int spp, uint32_t seed, float* out3, cudaStream_t s);
 cudaError_t launch_trace_resolve(const double* sum3, const int* first_pos, int npix, int spp, int frame, float4* accum,
                                  cudaStream_t s);
 

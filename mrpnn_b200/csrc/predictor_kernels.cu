@@ -506,10 +506,16 @@ __global__ void __launch_bounds__(256) k_hit(VolumeDev v, ViewDev w, HitRecords 
     f3 hit = mk3(0, 0, 0), X, Y, Z, LX;
     if (valid) {
         int row = pix / w.width, col = pix % w.width;
-        f3 dir = normalize(camera_ray(w, row, col));        // NNPredict: dir = normalize(dir)
+        f3 ori = w.ori, dir;
+        if (w.ray_dir) {                                     // GetRadiances: explicit rays
+            ori = mk3(w.ray_ori[3 * pix], w.ray_ori[3 * pix + 1], w.ray_ori[3 * pix + 2]);
+            dir = normalize(mk3(w.ray_dir[3 * pix], w.ray_dir[3 * pix + 1], w.ray_dir[3 * pix + 2]));
+        } else {
+            dir = normalize(camera_ray(w, row, col));        // NNPredict: dir = normalize(dir)
+        }
         f3 L = normalize(w.light_dir);
         Stream st(kPixelStream, (uint32_t)pix, 0, (uint32_t)w.frame, w.seed);   // InitRand again
-        active = first_hit(v, w.ori, dir, w.alpha, w.pass_rate, &hit, COUNT ? &tally : nullptr);
+        active = first_hit(v, ori, dir, w.alpha, w.pass_rate, &hit, COUNT ? &tally : nullptr);
         if (COUNT) {
             tally.events += active ? 1 : 0;
             tally.lookups += active ? 192 : 0;

@@ -1022,6 +1022,33 @@ void orc_predict_pixels(const orc_scene* s, const orc_view* v, const int* pixels
     }
 }
 
+// One sample of CalculateRadiance's loop (core/render.cuh:553-592) from the
+// box entry ori + dir * dis; NEE through the baked grid, or one Tr()
+// estimate per vertex from nst when the scene has no baked grid.
+static f3 trace_sample(const orc_scene* s, const orc_view* v, f3 ori, f3 dir, float dis, f3 L, Stream& st,
+                       Stream& nst) {
+    f3 lc = load3(v->light_color);
+    f3 srate = load3(s->scatter_rate);
+    f3 res = {0, 0, 0};
+    f3 p = ori + dir * dis, rd = dir, csr = {1, 1, 1};
+    for (int b = 0; b < v->multi_scatter; ++b) {
+        f3 np, nd;
+        float md = ray_box_distance(p, rd);
+        if (!next_vertex(s, st, v->alpha, v->g, p, rd, md, &np, &nd)) {
+            res = res + sky(s) * csr;
+            break;
+        }
+        p = np;
+        csr = csr * srate;
+        float ph = hg(dot(rd, L), v->g);
+        float tr = s->baked_tr ? tex3(s->baked_tr, s->baked_res, p, true)
+                               : transmittance(s, nst, p, L, ray_box_distance(p, L), v->alpha);
+        res = res + (lc * csr) * (tr * ph);
+        rd = nd;
+    }
+    return res;
+}
+
 // RenderCamera<false> + CalculateRadiance, core/volume.cu:198-228 and
 // core/render.cuh:535-597.  Sample k of a launch draws from its own stream
 // (sub = k); the first sample restarts the pixel stream like InitRand does.
@@ -1036,8 +1063,6 @@ void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, 
         f3 ori = load3(v->ori);
         f3 dir = normalize(load3(d0));
         f3 L = normalize(load3(v->light_dir));
-        f3 lc = load3(v->light_color);
-        f3 srate = load3(s->scatter_rate);
         float dis = ray_box_offset(ori, dir);
         double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
         float out[4];
@@ -1053,23 +1078,7 @@ void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, 
                 // unbiased NEE (no baked grid): one Tr() estimate per vertex
                 // from the sample's own NEE stream (kind 3)
                 Stream nst(3, (uint32_t)pix, (uint32_t)k, (uint32_t)v->frame, v->seed);
-                f3 res = {0, 0, 0};
-                f3 p = ori + dir * dis, rd = dir, csr = {1, 1, 1};
-                for (int b = 0; b < v->multi_scatter; ++b) {
-                    f3 np, nd;
-                    float md = ray_box_distance(p, rd);
-                    if (!next_vertex(s, st, v->alpha, v->g, p, rd, md, &np, &nd)) {
-                        res = res + sky(s) * csr;
-                        break;
-                    }
-                    p = np;
-                    csr = csr * srate;
-                    float ph = hg(dot(rd, L), v->g);
-                    float tr = s->baked_tr ? tex3(s->baked_tr, s->baked_res, p, true)
-                                           : transmittance(s, nst, p, L, ray_box_distance(p, L), v->alpha);
-                    res = res + (lc * csr) * (tr * ph);
-                    rd = nd;
-                }
+                f3 res = trace_sample(s, v, ori, dir, dis, L, st, nst);
                 for (int c = 0; c < 3; ++c) { double x = (&res.x)[c]; acc[c] += x; acc2[c] += x * x; }
                 // coverage: the reference tests its running sum (render.cuh:594)
                 any = any || res.x > 0 || res.y > 0 || res.z > 0;
@@ -1083,4 +1092,88 @@ void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, 
     }
 }
 
+
+// GetRadiances with RenderType PT (core/volume.cu:405-479 ->
+// CalculateRadianceMulti<0> -> CalculateRadiance) for explicit rays: ray q,
+// sample k draws from stream (0, q, k, frame, seed).  FP64 sums per channel.
+void orc_trace_rays(const orc_scene* s, const orc_view* v, const float* ori_, const float* dir_, int n, double* sum3,
+                    double* sumsq3) {
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int q = 0; q < n; ++q) {
+        f3 ori = load3(ori_ + 3 * q), dir = normalize(load3(dir_ + 3 * q));
+        f3 L = normalize(load3(v->light_dir));
+        float dis = ray_box_offset(ori, dir);
+        double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
+        for (int k = 0; k < v->spp; ++k) {
+            f3 res = sky(s);
+            if (dis >= 0) {
+                Stream st(0, (uint32_t)q, (uint32_t)k, (uint32_t)v->frame, v->seed);
+                Stream nst(3, (uint32_t)q, (uint32_t)k, (uint32_t)v->frame, v->seed);
+                res = trace_sample(s, v, ori, dir, dis, L, st, nst);
+            }
+            for (int c = 0; c < 3; ++c) { double x = (&res.x)[c]; acc[c] += x; acc2[c] += x * x; }
+        }
+        for (int c = 0; c < 3; ++c) { sum3[3 * q + c] = acc[c]; sumsq3[3 * q + c] = acc2[c]; }
+    }
+}
+
+// GetSample (core/render.cuh:615-655), the training-data generator: from a
+// point in the medium, the first direction HG-sampled around dir, up to
+// multi_scatter bounces, NEE by Tr() on the same stream.  Task q draws from
+// one stream (4, q, 0, 0, seed) across its samples, as the reference's one
+// InitRand per thread.
+void orc_get_samples(const orc_scene* s, const float* alpha, const float* ori, const float* dir, const float* ldir,
+                     const float* g, const float* scatter, int n, const float lc_[3], int multi_scatter, int spp,
+                     uint32_t seed, float* out3) {
+    f3 lc = load3(lc_);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int q = 0; q < n; ++q) {
+        Stream st(4, (uint32_t)q, 0, 0, seed);
+        f3 o = load3(ori + 3 * q), d = load3(dir + 3 * q), L = load3(ldir + 3 * q);
+        float a = alpha[q], gq = g[q], sc = scatter[q];
+        f3 res = {0, 0, 0};
+        for (int i = 0; i < spp; ++i) {
+            f3 pos = o;
+            float e1 = st.next();
+            float e0 = st.next();
+            f3 rd = sample_hg(e0, e1, d, gq);
+            f3 csr = {1, 1, 1};
+            for (int b = 0; b < multi_scatter; ++b) {
+                f3 np, nd;
+                float dis = ray_box_distance(pos, rd);
+                if (!next_vertex(s, st, a, gq, pos, rd, dis, &np, &nd)) {
+                    res = res + sky(s) * csr;
+                    break;
+                }
+                pos = np;
+                csr = (csr * 1.001f) * sc;
+                dis = ray_box_distance(pos, L);
+                float phase = hg(dot(rd, L), gq);
+                res = res + (lc * csr) * (transmittance(s, st, pos, L, dis, a) * phase);
+                rd = nd;
+            }
+        }
+        store3(out3 + 3 * q, f3{res.x / (float)spp, res.y / (float)spp, res.z / (float)spp});
+    }
+}
+
+// GetTrs -> ShadowTerm_TRs (core/render.cuh:668-680): light colour x pi x the
+// mean of Tr() x HG over spp estimates; task q draws from stream (5, q, 0, 0, seed).
+void orc_get_trs(const orc_scene* s, float alpha, const float* ori, const float* dir, int n, const float L_[3],
+                 const float lc_[3], float g, int spp, uint32_t seed, float* out3) {
+    f3 L = load3(L_), lc = load3(lc_);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int q = 0; q < n; ++q) {
+        Stream st(5, (uint32_t)q, 0, 0, seed);
+        f3 o = load3(ori + 3 * q), d = load3(dir + 3 * q);
+        float res = 0;
+        for (int i = 0; i < spp; ++i) {
+            float dis = ray_box_distance(o, L);
+            float phase = hg(dot(d, L), g);
+            res = res + transmittance(s, st, o, L, dis, alpha) * phase;
+        }
+        f3 r = lc * 3.1415926535f;
+        store3(out3 + 3 * q, f3{r.x * res / (float)spp, r.y * res / (float)spp, r.z * res / (float)spp});
+    }
+}
 }  // extern "C"

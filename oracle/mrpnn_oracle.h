@@ -126,6 +126,16 @@ void orc_predict_pixels(const orc_scene* s, const orc_view* v, const int* pixels
  * samples (float4, as the reference) plus FP64 sums of L and L^2 per channel. */
 void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, int n,
                       float* rgba_out, double* sum3, double* sumsq3);
+/* GetRadiances (PT) for explicit rays ori/dir [n][3]: FP64 sums over v->spp. */
+void orc_trace_rays(const orc_scene* s, const orc_view* v, const float* ori, const float* dir, int n, double* sum3,
+                    double* sumsq3);
+/* GetSamples: per task alpha, ori, dir, light dir, g, scatter; out [n][3]. */
+void orc_get_samples(const orc_scene* s, const float* alpha, const float* ori, const float* dir, const float* ldir,
+                     const float* g, const float* scatter, int n, const float lc[3], int multi_scatter, int spp,
+                     uint32_t seed, float* out3);
+/* GetTrs: ShadowTerm_TRs per task; out [n][3]. */
+void orc_get_trs(const orc_scene* s, float alpha, const float* ori, const float* dir, int n, const float L[3],
+                 const float lc[3], float g, int spp, uint32_t seed, float* out3);
 
 #ifdef __cplusplus
 }

@@ -94,6 +94,12 @@ def lib():
                                          C.c_void_p, C.c_void_p]
         L.orc_trace_pixels.argtypes = [C.POINTER(Scene), C.POINTER(View), i32p, C.c_int, f32p, C.c_void_p,
                                        C.c_void_p]
+        L.orc_trace_rays.argtypes = [C.POINTER(Scene), C.POINTER(View), C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_void_p, C.c_void_p]
+        L.orc_get_samples.argtypes = [C.POINTER(Scene)] + [C.c_void_p] * 6 + [C.c_int, F3, C.c_int, C.c_int,
+                                                                               C.c_uint32, C.c_void_p]
+        L.orc_get_trs.argtypes = [C.POINTER(Scene), C.c_float, C.c_void_p, C.c_void_p, C.c_int, F3, F3, C.c_float,
+                                  C.c_int, C.c_uint32, C.c_void_p]
         rc = L.orc_load_model(MODEL.encode())
         if rc != 0:
             raise RuntimeError(f"oracle: cannot load model file {MODEL} (rc={rc})")
@@ -261,6 +267,40 @@ def trace_pixels(scene, view, pixels):
     s2 = np.empty((n, 3), np.float64)
     lib().orc_trace_pixels(C.byref(scene.c), C.byref(view), px, n, rgba, s.ctypes.data, s2.ctypes.data)
     return rgba, s, s2
+
+
+def trace_rays(scene, view, ori, dir):
+    """GetRadiances (PT) for explicit rays: FP64 sums of L and L^2 over view.spp."""
+    ori = np.ascontiguousarray(ori, np.float32).reshape(-1, 3)
+    dir = np.ascontiguousarray(dir, np.float32).reshape(-1, 3)
+    n = ori.shape[0]
+    s = np.empty((n, 3), np.float64)
+    s2 = np.empty((n, 3), np.float64)
+    lib().orc_trace_rays(C.byref(scene.c), C.byref(view), ori.ctypes.data, dir.ctypes.data, n, s.ctypes.data,
+                         s2.ctypes.data)
+    return s, s2
+
+
+def get_samples(scene, alpha, ori, dir, ldir, g, scatter, light_color, multi_scatter, spp, seed):
+    ori = np.ascontiguousarray(ori, np.float32).reshape(-1, 3)
+    n = ori.shape[0]
+    arr = lambda x, k: np.ascontiguousarray(np.broadcast_to(np.asarray(x, np.float32), (n, k) if k > 1 else (n,)))
+    a, d, L, gg, sc = arr(alpha, 1), arr(dir, 3), arr(ldir, 3), arr(g, 1), arr(scatter, 1)
+    out = np.empty((n, 3), np.float32)
+    lib().orc_get_samples(C.byref(scene.c), a.ctypes.data, ori.ctypes.data, d.ctypes.data, L.ctypes.data,
+                          gg.ctypes.data, sc.ctypes.data, n, F3(*light_color), multi_scatter, spp, seed,
+                          out.ctypes.data)
+    return out
+
+
+def get_trs(scene, alpha, ori, dir, light_dir, light_color, g, spp, seed):
+    ori = np.ascontiguousarray(ori, np.float32).reshape(-1, 3)
+    dir = np.ascontiguousarray(dir, np.float32).reshape(-1, 3)
+    n = ori.shape[0]
+    out = np.empty((n, 3), np.float32)
+    lib().orc_get_trs(C.byref(scene.c), alpha, ori.ctypes.data, dir.ctypes.data, n, F3(*light_dir),
+                      F3(*light_color), g, spp, seed, out.ctypes.data)
+    return out
 
 
 def mlp_f32(feat, gamma, g, sr):
