@@ -195,6 +195,30 @@ mrp_status mrp_last_render_stages(const mrp_volume* v, float ms[3]);
  * network, result copies. */
 mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* const* outs, int outs_are_device);
 
+/* -- interactive frames: VolumeRender::Render(float3*, Histogram*, unsigned*, ...)
+ * (core/volume.cu:550-628) ------------------------------------------------------------ */
+/* Histogram (core/volume.hpp:12-19): 10 bins per channel of L / (L + 1), the
+ * sample count and running means of the luminance and its square. */
+typedef struct mrp_histogram {
+    float bin[30];
+    float total, x2, x;
+} mrp_histogram;
+/* One viewer frame.  PT: one sample per (checkerboard-selected) pixel into
+ * the running mean `target` and the histograms, then Denoise (histogram-
+ * weighted 11 x 11 filter when denoise != 0 and the pixel's variance > 0.01;
+ * checkerboard fill on frame 0); MRPNN: target = the prediction at the
+ * selected pixels, then ReprojectionDenoise.  Both end in exposure, tone
+ * (0 none, 1 Gamma, 2 ACES) and an RGBA8 pack 0xff000000 | r<<16 | g<<8 | b.
+ * frame_num is the reference's frameNum (running-mean index; halved with
+ * checkerboard), flip its checkerboard parity; view->frame_offset keys the
+ * RNG.  target (w*h*3 floats) and histo (w*h) are device buffers the caller
+ * owns and keeps between frames (zero them before frame 0); rgba8 (w*h) is
+ * device or host memory.  Images follow the interactive kernel's framing
+ * (v = (row + r) / H). */
+mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_render_type type, int frame_num,
+                                  int checkerboard, int flip, int tone, int denoise, float exposure, float* target,
+                                  mrp_histogram* histo, uint32_t* rgba8, int rgba8_is_device);
+
 /* -- batch ray APIs (core/volume.cu:405-479, 710-834) ---------------------------------
  * ori / dir / light_dirs: [n][3]; outputs [n][3]; is_device covers inputs and
  * output alike. */

@@ -112,6 +112,8 @@ _SIGS = {
                                                             C.c_int], C.c_int),
     "mrp_get_trs": ([C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_int, F3, F3, C.c_float, C.c_int, C.c_uint32,
                      C.c_void_p, C.c_int], C.c_int),
+    "mrp_render_interactive": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "mrp_serve_default_config": ([C.POINTER(ServeConfig)], None),
     "mrp_serve_open": ([C.POINTER(ServeConfig), C.POINTER(C.c_void_p)], C.c_int),
     "mrp_serve_submit": ([C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
@@ -634,3 +636,37 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class Viewer:
+    """The reference's real-time viewer loop, VolumeRender::Render(float3*
+    target, Histogram*, unsigned* target2, ...) (core/volume.cu:550-628), over
+    mrp_render_interactive: the running-mean image and the per-pixel
+    histograms are device buffers (CUDA tensors) kept between frames; each
+    frame returns the RGBA8 image ([H, W] uint32, 0xAARRGGBB)."""
+
+    def __init__(self, volume, width, height, checkerboard=False):
+        import torch
+        self.volume, self.width, self.height = volume, int(width), int(height)
+        self.target = torch.zeros((self.height, self.width, 3), dtype=torch.float32, device="cuda")
+        self.histo = torch.zeros((self.height, self.width, 33), dtype=torch.float32, device="cuda")
+        self.checkerboard = bool(checkerboard)
+        self.frame_num = 0   # the reference's frameNum (reset when the camera moves)
+        self.flip = 0
+        self.rng_frame = 0   # randNum
+
+    def reset(self):
+        self.frame_num = 0
+
+    def frame(self, view, rt, tone=2, denoise=False, exposure=1.0):
+        view.width, view.height = self.width, self.height
+        view.frame_offset = self.rng_frame
+        out = np.empty((self.height, self.width), np.uint32)
+        _check(lib().mrp_render_interactive(self.volume._h, C.byref(view), int(rt), self.frame_num,
+                                            1 if self.checkerboard else 0, self.flip, int(tone),
+                                            1 if denoise else 0, float(exposure), self.target.data_ptr(),
+                                            self.histo.data_ptr(), out.ctypes.data, 0))
+        self.frame_num += 1
+        self.flip ^= 1
+        self.rng_frame += 1
+        return out

@@ -558,7 +558,9 @@ mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float al
 }
 
 // --- rendering ----------------------------------------------------------------
-static mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
+}  // extern "C"
+namespace mrpi {
+mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
     if (v->rec_cap >= npix) return MRP_OK;
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     v->rec_count = nullptr; v->rec_pix = nullptr; v->rec_f = nullptr; v->feat = nullptr; v->rec_cap = 0;
@@ -570,6 +572,17 @@ static mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
     v->rec_cap = npix;
     return MRP_OK;
 }
+mrp_status ensure_accum(mrp_volume* v, size_t npix) {
+    if (v->accum_pix >= npix) return MRP_OK;
+    cudaFree(v->accum);
+    v->accum = nullptr;
+    v->accum_pix = 0;
+    CU(cudaMalloc(&v->accum, npix * sizeof(float4)));
+    v->accum_pix = npix;
+    return MRP_OK;
+}
+}  // namespace mrpi
+extern "C" {
 
 }  // extern "C"
 namespace mrpi {
@@ -634,13 +647,7 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     if (type == MRP_MRPNN && !v->has_pyramid) return fail(MRP_ERR_NOT_READY, "MRPNN needs the pyramid (mrp_volume_update)");
     if (type == MRP_PT && (w->spp < 1 || w->multi_scatter < 1)) return fail(MRP_ERR_INVALID, "PT needs spp, multi_scatter >= 1");
     size_t npix = (size_t)w->width * w->height;
-    if (v->accum_pix < npix) {
-        cudaFree(v->accum);
-        v->accum = nullptr;
-        v->accum_pix = 0;
-        CU(cudaMalloc(&v->accum, npix * sizeof(float4)));
-        v->accum_pix = npix;
-    }
+    TRY(ensure_accum(v, npix));
     if (type == MRP_PT && v->trace_pix < npix) {
         cudaFree(v->sum3); cudaFree(v->first_pos); cudaFree(v->counter);
         v->sum3 = nullptr; v->first_pos = nullptr; v->counter = nullptr; v->trace_pix = 0;

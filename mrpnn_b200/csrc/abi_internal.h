@@ -58,6 +58,10 @@ cudaError_t build_tr_levels(float* trs, const float* mips, const uint8_t* mip_oc
 // LUT for g (UpdateHGLut) and the TR mips for (light, alpha) (Update_TR).
 mrp_status update_lut_async(mrp_volume* v, float g);
 mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha);
+// Staged-predictor records / features and the running-mean image of a volume,
+// grown to npix pixels.
+mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix);
+mrp_status ensure_accum(mrp_volume* v, size_t npix);
 // The baked NEE grid for (light, alpha) (Update_CachedTR), on the volume's stream.
 mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha);
 

@@ -315,7 +315,26 @@ struct ViewDev {
     // width x 1 launch, origin ray_ori[3q..], direction ray_dir[3q..]
     const float* ray_ori;
     const float* ray_dir;
+    // interactive frames (VolumeRender::Render(float3*, Histogram*, ...)):
+    // cam_mode 1 uses that kernel's v = (row + r) / H instead of
+    // RenderCamera<float4>'s 1 - (row + r) / H; checker renders only the
+    // pixels with (row + col + flip) even
+    int cam_mode, checker, flip;
 };
+
+// Camera ray of pixel (row, col): jitter = the first two draws of the pixel
+// stream (RenderCamera, core/volume.cu:208-216 and 67-81).
+MRP_D f3 camera_ray_dir(const ViewDev& w, int row, int col) {
+    Stream st(kPixelStream, (uint32_t)(row * w.width + col), 0, (uint32_t)w.frame, w.seed);
+    float r0 = st.next(), r1 = st.next();
+    float u = fs(1.0f, fd(fa((float)col, r0), (float)w.width));
+    float vq = fd(fa((float)row, r1), (float)w.height);
+    float vv = w.cam_mode ? vq : fs(1.0f, vq);
+    f3 fwd = normalize(neg(w.ori));
+    f3 d = add(add(fwd, mul(w.right, fs(fm(u, 2.0f), 1.0f))), mul(w.up, fs(fm(vv, 2.0f), 1.0f)));
+    return normalize(d);
+}
+MRP_D bool pixel_selected(const ViewDev& w, int row, int col) { return !w.checker || ((row + col + w.flip) & 1) == 0; }
 
 // Per-thread work tally, flushed to ViewDev::counters once per thread.
 struct Tally {

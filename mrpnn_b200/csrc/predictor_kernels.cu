@@ -37,15 +37,7 @@ MRP_D const float* tr_level(const VolumeDev& v, int m) { return v.trs + tr_offse
 
 // RenderCamera ray (core/volume.cu:208-216): jitter = first two draws of the
 // pixel stream.
-MRP_D f3 camera_ray(const ViewDev& w, int row, int col) {
-    Stream st(kPixelStream, (uint32_t)(row * w.width + col), 0, (uint32_t)w.frame, w.seed);
-    float r0 = st.next(), r1 = st.next();
-    float u = fs(1.0f, fd(fa((float)col, r0), (float)w.width));
-    float vv = fs(1.0f, fd(fa((float)row, r1), (float)w.height));
-    f3 fwd = normalize(neg(w.ori));
-    f3 d = add(add(fwd, mul(w.right, fs(fm(u, 2.0f), 1.0f))), mul(w.up, fs(fm(vv, 2.0f), 1.0f)));
-    return normalize(d);
-}
+MRP_D f3 camera_ray(const ViewDev& w, int row, int col) { return camera_ray_dir(w, row, col); }
 
 // Density() at p, skipping the 8 texel loads when the occupancy bricks prove
 // the trilinear footprint is all zero: the base voxel of the fetch is
@@ -501,7 +493,7 @@ __global__ void __launch_bounds__(256) k_hit(VolumeDev v, ViewDev w, HitRecords 
     Tally tally;
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
     int npix = w.width * w.height;
-    bool valid = pix < npix;
+    bool valid = pix < npix && pixel_selected(w, pix / w.width, pix % w.width);
     bool active = false;
     f3 hit = mk3(0, 0, 0), X, Y, Z, LX;
     if (valid) {

@@ -1176,4 +1176,161 @@ void orc_get_trs(const orc_scene* s, float alpha, const float* ori, const float*
         store3(out3 + 3 * q, f3{r.x * res / (float)spp, r.y * res / (float)spp, r.z * res / (float)spp});
     }
 }
+
+// ---------------------------------------------------------------------------
+// Interactive frame (VolumeRender::Render(float3*, Histogram*, ...),
+// core/volume.cu:57-196, 230-353, 550-628; tone maps core/render.cuh:1144-1236).
+// Histogram layout: bin[30], total, x2, x (33 floats per pixel).
+// ---------------------------------------------------------------------------
+static f3 mat3(f3 r0, f3 r1, f3 r2, f3 v) { return f3{dot(r0, v), dot(r1, v), dot(r2, v)}; }
+static f3 lerp3(f3 a, f3 b, float t) { return f3{lerpf(a.x, b.x, t), lerpf(a.y, b.y, t), lerpf(a.z, b.z, t)}; }
+static f3 gamma_tone(f3 c) {
+    float e = 1.0f / 2.2f;
+    return f3{std::pow(c.x, e), std::pow(c.y, e), std::pow(c.z, e)};
+}
+static f3 aces_tone(f3 color) {
+    const f3 A0 = {0.6624541811f, 0.1340042065f, 0.1561876870f}, A1 = {0.2722287168f, 0.6740817658f, 0.0536895174f},
+             A2 = {-0.0055746495f, 0.0040607335f, 1.0103391003f};
+    f3 aces = mat3({0.4397010f, 0.3829780f, 0.1773350f}, {0.0897923f, 0.8134230f, 0.0967616f},
+                   {0.0175440f, 0.1115440f, 0.8707040f}, color);
+    const f3 Y = {0.272229f, 0.674082f, 0.0536895f};
+    f3 cg = mat3({1.4514393161f, -0.2365107469f, -0.2149285693f}, {-0.0765537734f, 1.1762296998f, -0.0996759264f},
+                 {0.0083161484f, -0.0060324498f, 0.9977163014f}, aces);
+    float tmp = dot(cg, Y);
+    cg = lerp3(f3{tmp, tmp, tmp}, cg, 0.96f);
+    const float a = 278.5085f, b = 10.7772f, c = 293.6045f, d = 88.7122f, e = 80.6889f;
+    f3 x = cg;
+    f3 num = x * ((x * a) + f3{b, b, b});
+    f3 den = (x * ((x * c) + f3{d, d, d})) + f3{e, e, e};
+    f3 post = {num.x / den.x, num.y / den.y, num.z / den.z};
+    f3 XYZ = mat3(A0, A1, A2, post);
+    float divisor = fmax_(dot(XYZ, f3{1, 1, 1}), 1e-4f);
+    f3 xyY = {XYZ.x / divisor, XYZ.y / divisor, XYZ.y};
+    xyY.z = fmin_(fmax_(xyY.z, 0.0f), 65504.0f);
+    xyY.z = std::pow(xyY.z, 0.9811f);
+    float m = xyY.z / fmax_(xyY.y, 1e-4f);
+    XYZ = f3{xyY.x * m, xyY.z, ((1.0f - xyY.x) - xyY.y) * m};
+    f3 lin = mat3({1.6410233797f, -0.3248032942f, -0.2364246952f}, {-0.6636628587f, 1.6153315917f, 0.0167563477f},
+                  {0.0117218943f, -0.0082844420f, 0.9883948585f}, XYZ);
+    tmp = dot(lin, Y);
+    lin = lerp3(f3{tmp, tmp, tmp}, lin, 0.93f);
+    XYZ = mat3(A0, A1, A2, lin);
+    XYZ = mat3({0.98722400f, -0.00611327f, 0.0159533f}, {-0.00759836f, 1.00186000f, 0.0053302f},
+               {0.00307257f, -0.00509595f, 1.0816800f}, XYZ);
+    lin = mat3({3.2409699419f, -1.5373831776f, -0.4986107603f}, {-0.9692436363f, 1.8759675015f, 0.0415550574f},
+               {0.0556300797f, -0.2039769589f, 1.0569715142f}, XYZ);
+    return gamma_tone(lin);
+}
+static float saturate1(float v) { return fmin_(fmax_(v, 0.0f), 1.0f); }
+static int unroll(int row, int col, int W, int H) {
+    col = std::min(std::max(0, col), W - 1);
+    row = std::min(std::max(0, row), H - 1);
+    return col + W * row;
+}
+static float compare_histo(const float* x, const float* y) {
+    float nx = x[30], ny = y[30];
+    float sy = std::sqrt(ny / nx), sx = std::sqrt(nx / ny);
+    float p = 0, res = 0;
+    for (int i = 0; i < 30; ++i) {
+        float hx = x[i], hy = y[i];
+        if (hx != 0 || hy != 0) {
+            p += 1;
+            float t = sy * hx - sx * hy;
+            res += t * t / (hx + hy);
+        }
+    }
+    return p == 0 ? 0 : res / p;
+}
+
+void orc_frame_pt(const orc_scene* s, const orc_view* v, int fnum, int checker, int flip, float* target,
+                  float* histo) {
+    const int W = v->width, H = v->height;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int idx = 0; idx < W * H; ++idx) {
+        int row = idx / W, col = idx % W;
+        if (checker && ((row + col + flip) & 1)) continue;
+        Stream st(0, (uint32_t)idx, 0, (uint32_t)v->frame, v->seed);
+        float r0 = st.next(), r1 = st.next();
+        float u = 1 - ((float)col + r0) / (float)W;
+        float w = ((float)row + r1) / (float)H;
+        f3 ori = load3(v->ori);
+        f3 fwd = normalize(neg(ori));
+        f3 dir = normalize(fwd + (load3(v->right) * (u * 2 - 1)) + (load3(v->up) * (w * 2 - 1)));
+        f3 L = normalize(load3(v->light_dir));
+        float dis = ray_box_offset(ori, dir);
+        f3 res = sky(s);
+        if (dis >= 0) {
+            Stream s0(0, (uint32_t)idx, 0, (uint32_t)v->frame, v->seed);
+            Stream nst(3, (uint32_t)idx, 0, (uint32_t)v->frame, v->seed);
+            res = trace_sample(s, v, ori, dir, dis, L, s0, nst);
+        }
+        res = f3{fmax_(0.0f, res.x), fmax_(0.0f, res.y), fmax_(0.0f, res.z)};
+        float* h = histo + 33 * (size_t)idx;
+        if (fnum == 0) for (int k = 0; k < 33; ++k) h[k] = 0;
+        float rate = 1.0f / (float)(1 + fnum);
+        f3 t = lerp3(load3(target + 3 * (size_t)idx), res, rate);
+        store3(target + 3 * (size_t)idx, t);
+        res = f3{res.x / (res.x + 1), res.y / (res.y + 1), res.z / (res.z + 1)};
+        h[30] += 1;
+        int bx = (int)std::floor(fmin_(res.x, 0.999f) * 10.0f), by = (int)std::floor(fmin_(res.y, 0.999f) * 10.0f),
+            bz = (int)std::floor(fmin_(res.z, 0.999f) * 10.0f);
+        h[bx] += 1;
+        h[by + 10] += 1;
+        h[bz + 20] += 1;
+        float l = dot(res, f3{1, 1, 1});
+        h[32] = lerpf(h[32], l, rate);
+        h[31] = lerpf(h[31], l * l, rate);
+    }
+}
+
+void orc_frame_finish(const float* target, float* histo, int W, int H, int frame_num, int flip, int predict,
+                      int denoise, float exposure, int tone, uint32_t* rgba8) {
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < W * H; ++id) {
+        int row = id / W, col = id % W;
+        auto T = [&](int i) { return load3(target + 3 * (size_t)i); };
+        f3 res;
+        if (predict) {
+            res = T(id);
+        } else if (frame_num == 0) {
+            if ((((row + flip) % 2) + col) % 2 == 0) {
+                res = T(id);
+            } else {
+                res = ((T(unroll(row - 1, col, W, H)) + T(unroll(row + 1, col, W, H))) + T(unroll(row, col - 1, W, H))) +
+                      T(unroll(row, col + 1, W, H));
+                res = f3{res.x / 4.0f, res.y / 4.0f, res.z / 4.0f};
+            }
+        } else {
+            const float* c = histo + 33 * (size_t)id;
+            float variance = std::fabs(c[31] - c[32] * c[32]);
+            if (denoise && variance > 0.01) {
+                res = f3{0, 0, 0};
+                float ws = 0;
+                for (int i = -5; i <= 5; ++i)
+                    for (int j = -5; j <= 5; ++j) {
+                        int t = unroll(row + i, col + j, W, H);
+                        float w = (float)std::fmax(0.0, 1.0 - 1.2 * (double)compare_histo(c, histo + 33 * (size_t)t));
+                        res = res + T(t) * w;
+                        ws += w;
+                    }
+                res = f3{res.x / ws, res.y / ws, res.z / ws};
+            } else {
+                res = T(id);
+            }
+        }
+        f3 val = res * exposure;
+        if (tone == 1) val = gamma_tone(val);
+        else if (tone == 2) val = aces_tone(val);
+        uint32_t r = (uint32_t)(255.0f * saturate1(val.x)), g = (uint32_t)(255.0f * saturate1(val.y)),
+                 b = (uint32_t)(255.0f * saturate1(val.z));
+        rgba8[id] = 0xff000000u | (r << 16) | (g << 8) | b;
+    }
+    if (predict)
+        for (int id = 0; id < W * H; ++id) {
+            f3 t = load3(target + 3 * (size_t)id);
+            histo[33 * (size_t)id + 30] = t.x;
+            histo[33 * (size_t)id + 32] = t.y;
+            histo[33 * (size_t)id + 31] = t.z;
+        }
+}
 }  // extern "C"

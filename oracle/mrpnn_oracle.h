@@ -133,6 +133,13 @@ void orc_trace_rays(const orc_scene* s, const orc_view* v, const float* ori, con
 void orc_get_samples(const orc_scene* s, const float* alpha, const float* ori, const float* dir, const float* ldir,
                      const float* g, const float* scatter, int n, const float lc[3], int multi_scatter, int spp,
                      uint32_t seed, float* out3);
+/* Interactive frame: PT sample + running mean + histograms at the
+ * (checkerboard-)selected pixels (histo: 33 floats per pixel: bin[30],
+ * total, x2, x), and the Denoise / ReprojectionDenoise + tone + RGBA8 pass. */
+void orc_frame_pt(const orc_scene* s, const orc_view* v, int fnum, int checker, int flip, float* target,
+                  float* histo);
+void orc_frame_finish(const float* target, float* histo, int W, int H, int frame_num, int flip, int predict,
+                      int denoise, float exposure, int tone, uint32_t* rgba8);
 /* GetTrs: ShadowTerm_TRs per task; out [n][3]. */
 void orc_get_trs(const orc_scene* s, float alpha, const float* ori, const float* dir, int n, const float L[3],
                  const float lc[3], float g, int spp, uint32_t seed, float* out3);

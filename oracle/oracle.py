@@ -94,6 +94,10 @@ def lib():
                                          C.c_void_p, C.c_void_p]
         L.orc_trace_pixels.argtypes = [C.POINTER(Scene), C.POINTER(View), i32p, C.c_int, f32p, C.c_void_p,
                                        C.c_void_p]
+        L.orc_frame_pt.argtypes = [C.POINTER(Scene), C.POINTER(View), C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_void_p]
+        L.orc_frame_finish.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_float, C.c_int, C.c_void_p]
         L.orc_trace_rays.argtypes = [C.POINTER(Scene), C.POINTER(View), C.c_void_p, C.c_void_p, C.c_int,
                                      C.c_void_p, C.c_void_p]
         L.orc_get_samples.argtypes = [C.POINTER(Scene)] + [C.c_void_p] * 6 + [C.c_int, F3, C.c_int, C.c_int,
@@ -301,6 +305,24 @@ def get_trs(scene, alpha, ori, dir, light_dir, light_color, g, spp, seed):
     lib().orc_get_trs(C.byref(scene.c), alpha, ori.ctypes.data, dir.ctypes.data, n, F3(*light_dir),
                       F3(*light_color), g, spp, seed, out.ctypes.data)
     return out
+
+
+def frame_pt(scene, view, fnum, checker, flip, target, histo):
+    """Interactive PT frame on copies of (target [H, W, 3], histo [H, W, 33])."""
+    t = np.ascontiguousarray(target, np.float32).copy()
+    h = np.ascontiguousarray(histo, np.float32).copy()
+    lib().orc_frame_pt(C.byref(scene.c), C.byref(view), fnum, checker, flip, t.ctypes.data, h.ctypes.data)
+    return t, h
+
+
+def frame_finish(target, histo, frame_num, flip, predict, denoise, exposure, tone):
+    t = np.ascontiguousarray(target, np.float32)
+    h = np.ascontiguousarray(histo, np.float32).copy()
+    H, W = t.shape[:2]
+    out = np.empty((H, W), np.uint32)
+    lib().orc_frame_finish(t.ctypes.data, h.ctypes.data, W, H, frame_num, flip, predict, denoise, exposure, tone,
+                           out.ctypes.data)
+    return out, h
 
 
 def mlp_f32(feat, gamma, g, sr):
