@@ -241,6 +241,15 @@ mrp_status mrp_get_trs(mrp_volume* v, float alpha, const float* ori, const float
                        const float light_dir[3], const float light_color[3], float g, int sample_num, uint32_t seed,
                        float* out3, int is_device);
 
+/* VolumeRender::GatherData (core/volume.cu:630-700 -> GatherSamples ->
+ * NNGatherSamples, core/render.cuh:1006-1142): the input of the tile network
+ * for a view->width x view->height grid of 8 x 8-pixel tiles, sub-pixel offset
+ * (px, py) in eighths of a tile.  out [tiles][773]: X_Val[192],
+ * X_Val_Hg[192], X_Val_Sub[192] (SetupInputData2 of 16 depth samples), 5
+ * angle / depth-gradient terms, 192 t-grid values; a tile whose 64 rays all
+ * miss has out[0] = -1000 (the rest zero apart from its t-grid). */
+mrp_status mrp_gather_tiles(mrp_volume* v, const mrp_view* view, int px, int py, float* out, int is_device);
+
 /* -- parity entry points (pieces of the path) ---------------------------------------- */
 /* RadiancePredictInternal (core/radiancePredict.cu:301-422) on n feature
  * sets: feat [n][576] = X_Val[192], X_Val_Sub[192], X_Val_Hg[192]; gamma [n];

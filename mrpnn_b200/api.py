@@ -114,6 +114,7 @@ _SIGS = {
                      C.c_void_p, C.c_int], C.c_int),
     "mrp_render_interactive": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                 C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "mrp_gather_tiles": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_serve_default_config": ([C.POINTER(ServeConfig)], None),
     "mrp_serve_open": ([C.POINTER(ServeConfig), C.POINTER(C.c_void_p)], C.c_int),
     "mrp_serve_submit": ([C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
@@ -454,6 +455,15 @@ class VolumeRender:
         _check(lib().mrp_get_trs(self._h, float(alpha), ori.ctypes.data, dir.ctypes.data, ori.shape[0],
                                  _f3(lightDir), _f3(lightColor), float(g), int(sampleNum), int(seed),
                                  out.ctypes.data, 0))
+        return out
+
+    def GatherData(self, size, ori, up, right, lightDir, alpha=1.0, g=0.0, pixelOffset=(0, 0), seed=0, frame=0):
+        """GatherData (core/volume.cu:630-700): [tiles_y * tiles_x, 773] tile
+        features for a size = (tiles_x, tiles_y) grid of 8 x 8-pixel tiles."""
+        view = self.make_view(size, ori, up, right, lightDir, g, alpha, seed=seed, frame_offset=frame)
+        out = np.empty((view.width * view.height, 773), np.float32)
+        _check(lib().mrp_gather_tiles(self._h, C.byref(view), int(pixelOffset[0]), int(pixelOffset[1]),
+                                      out.ctypes.data, 0))
         return out
 
     def render_views(self, views, outs=None):

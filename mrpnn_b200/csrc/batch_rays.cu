@@ -6,6 +6,7 @@
 // buffers, work runs on the volume's stream, and the kernels are the
 // renderer's own (explicit-ray mode of k_trace / k_hit, k_get_samples,
 // k_get_trs).
+#include <cmath>
 #include <vector>
 
 #include "abi_internal.h"
@@ -179,6 +180,30 @@ mrp_status mrp_get_trs(mrp_volume* v, float alpha, const float* ori, const float
     if (!is_device) CU(S.scratch((size_t)n * 12, (void**)&out));
     CU(launch_get_trs(v->dev(), alpha, o, d, n, light_dir, light_color, g, sample_num, seed, out, v->stream));
     if (!is_device) CU(cudaMemcpyAsync(out3, out, (size_t)n * 12, cudaMemcpyDeviceToHost, v->stream));
+    CU(cudaStreamSynchronize(v->stream));
+    return MRP_OK;
+}
+
+mrp_status mrp_gather_tiles(mrp_volume* v, const mrp_view* view, int px, int py, float* out, int is_device) {
+    TRY(need_init());
+    if (!v || !view || !out) return fail(MRP_ERR_INVALID, "null argument");
+    if (view->width <= 0 || view->height <= 0 || (long long)view->width * view->height > (1ll << 22))
+        return fail(MRP_ERR_INVALID, "tile grid %dx%d", view->width, view->height);
+    if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "the tile gather needs the pyramid");
+    // GatherData updates the LUT and the TR mips first (core/volume.cu:655-657)
+    TRY(update_lut_async(v, view->g));
+    TRY(update_tr_async(v, view->light_dir, view->alpha));
+    const size_t n = (size_t)view->width * view->height, bytes = n * 773 * sizeof(float);
+    Staging S;
+    float* d_out = out;
+    if (!is_device) CU(S.scratch(bytes, (void**)&d_out));
+    CU(cudaMemsetAsync(d_out, 0, bytes, v->stream));
+    // DeterminateEstimatedHit's thresholds, -logf(0.76 / 0.75 / 0.25), as the
+    // host computes them
+    const float nl[3] = {-std::log(0.76f), -std::log(0.75f), -std::log(0.25f)};
+    ViewDev vd = make_view(v, view, view->frame_offset, 0);
+    CU(launch_gather_tiles(v->dev(), vd, px, py, nl, d_out, v->stream));
+    if (!is_device) CU(cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, v->stream));
     CU(cudaStreamSynchronize(v->stream));
     return MRP_OK;
 }

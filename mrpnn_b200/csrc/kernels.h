@@ -44,6 +44,9 @@ struct HitRecords {
     size_t cap;     // >= pixels of the launch
 };
 cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, float4* accum, cudaStream_t s);
+// GatherData: 773 tile features per tile of a view.width x view.height grid.
+cudaError_t launch_gather_tiles(const VolumeDev& v, const ViewDev& view, int px, int py, const float nl[3], float* out,
+                                cudaStream_t s);
 cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s);
 cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitRecords rec, const float* feat,
                                 const float* weights, float4* accum, cudaStream_t s);

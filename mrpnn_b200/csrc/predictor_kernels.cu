@@ -10,6 +10,8 @@
 // (common.cuh), so hits and features match the CPU oracle to the bit except
 // where a transcendental's last bit differs.  The MLP here is the plain FP32
 // drop-in: one pixel per thread, weights broadcast from L1 (uniform loads).
+#include <cfloat>
+
 #include "kernels.h"
 
 namespace mrp {
@@ -625,6 +627,241 @@ cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, 
     else k_hit<false><<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
     return cudaGetLastError();
 }
+// ---------------------------------------------------------------------------
+// Tile gather of the tile network (GatherData -> GatherSamples ->
+// NNGatherSamples, core/volume.cu:257-282; core/render.cuh:199-397, 464-485,
+// 1006-1142; SetupInputData2, core/radiancePredict.cu:487-553): one thread
+// per 8 x 8-pixel tile, 773 floats: X_Val[192], X_Val_Hg[192], X_Val_Sub[192],
+// 5 angle / depth-gradient terms, 192 t-grid values.  nl = {-log 0.76,
+// -log 0.75, -log 0.25} from the host's logf.
+// ---------------------------------------------------------------------------
+struct TauState { float tau, target; bool first; };
+
+// CheckExitCondition (core/render.cuh:199-297): trapezoid optical depth over
+// the step; the crossing of the 50 % (then 25 %) survival threshold solved in
+// the step.
+MRP_D float exit_offset(float A, float B, float C, float dq, float dt, float S, float lastS) {
+    if (fabsf(A) < 1e-6f) return fd(dq, fm(fm(dt, fa(S, lastS)), 0.5f));
+    float D = fs(fm(B, B), fm(fm(4.0f, A), C));
+    D = fmaxf(D, 0.0f);
+    float sq = fsq(D);
+    float q = fm(-0.5f, fa(B, sq));   // (float)(-0.5 * (double)(B + sq)): exact halving
+    float u1 = fd(q, A), u2 = fd(C, q);
+    return u1 == fminf(fmaxf(u1, 0.0f), 1.0f) ? u1 : u2;
+}
+MRP_D bool check_exit(float S, float lastS, float dt, float t, TauState& st, float ts[4], float tau_second) {
+    float tau_next = fa(st.tau, fm(fm(fa(S, lastS), 0.5f), dt));
+    if (tau_next >= st.target) {
+        float dtau = fs(st.target, st.tau);
+        float A = fm(fm(0.5f, dt), fs(S, lastS)), B = fm(dt, lastS);
+        float off = exit_offset(A, B, -dtau, dtau, dt, S, lastS);
+        off = fminf(fmaxf(off, 0.0f), 1.0f);
+        float hit_t = fs(t, fm(dt, fs(1.0f, off)));
+        if (st.first) {
+            ts[0] = hit_t;
+            st.target = tau_second;
+            st.first = false;
+            if (tau_next >= st.target) {
+                float d2 = fs(st.target, st.tau);
+                float off2 = exit_offset(A, B, -d2, d2, dt, S, lastS);
+                ts[1] = fs(t, fm(dt, fs(1.0f, off2)));
+                return true;
+            }
+        } else {
+            ts[1] = hit_t;
+            return true;
+        }
+    }
+    st.tau = tau_next;
+    return false;
+}
+
+// DeterminateEstimatedHit(alpha, pos, dir, dis) -> float4 (core/render.cuh:298-397)
+MRP_D void estimated_hit_ts(const VolumeDev& v, float alpha, f3 pos, f3 dir, float dis, const float nl[3],
+                            float ts[4]) {
+    float smax = fm(v.max_density, alpha);
+    float t = 0.0f;
+    ts[0] = 0.0f; ts[1] = 0.0f; ts[2] = FLT_MAX; ts[3] = 0.0f;
+    float last_non_empty_t = 0.0f;
+    float rf = (float)v.res;
+    float t_step = fd(1.0f, rf);
+    if (fm(smax, t_step) > nl[0]) t_step = fd(nl[0], smax);
+    TauState st{0.0f, nl[1], true};
+    int loop = 0;
+    float last = 0.0f;
+    while (loop++ < 10000) {
+        if (t > dis) {
+            if (st.first) ts[0] = last_non_empty_t;
+            else ts[1] = last_non_empty_t;
+            break;
+        }
+        float d = density(v, add(pos, mul(dir, t)));
+        if (d > 0) {
+            float S = fm(d, alpha);
+            if (check_exit(S, last, t_step, t, st, ts, nl[2])) break;
+            ts[2] = fminf(t, ts[2]);
+            t = fa(t, t_step);
+            last = S;
+        } else {
+            if (last > 0) {
+                float ts_ = fa(t_step, d);
+                if (ts_ > 0) {
+                    if (check_exit(0.0f, last, ts_, t, st, ts, nl[2])) break;
+                    last_non_empty_t = fa(t, ts_);
+                } else {
+                    last_non_empty_t = t;
+                }
+            }
+            t = fa(t, fmaxf(fm(-d, 1.0f), fd(0.5f, rf)));
+            last = 0.0f;
+        }
+    }
+    if (ts[2] == FLT_MAX) ts[2] = 0.0f;
+    float survival = expf(-st.tau);
+    ts[3] = fminf(fd(fmaxf(fs(1.0f, survival), 0.0f), 0.75f), 1.0f);
+}
+
+// GetSampleT (core/render.cuh:464-485)
+MRP_D void sample_t(const VolumeDev& v, f3 ori, f3 dir, float alpha, const float nl[3], float ts[4]) {
+    float dis = ray_box_offset(ori, dir);
+    if (dis < 0) { ts[0] = ts[1] = ts[2] = ts[3] = 0.0f; return; }
+    f3 sp = add(ori, mul(dir, dis));
+    float md = ray_box_distance(sp, dir);
+    estimated_hit_ts(v, alpha, sp, dir, md, nl, ts);
+    if (ts[0] > 0) { ts[0] = fa(ts[0], dis); ts[2] = fa(ts[2], dis); }
+    if (ts[1] > 0) ts[1] = fa(ts[1], dis);
+}
+
+struct TileAcc {
+    float minx, miny, maxx, maxy;
+    f3 avg;
+};
+
+// PrepareRay (core/render.cuh:1006-1040)
+MRP_D void prepare_ray(const VolumeDev& v, float ox, float oy, f3 dir, f3 ro, f3 uo, f3 ori, float alpha,
+                       const float nl[3], bool p25, int gid, float* tg, TileAcc& acc, float& hd, float& vd,
+                       float ray[4]) {
+    f3 sd = normalize(add(add(dir, mul(ro, ox)), mul(uo, oy)));
+    float ts[4];
+    sample_t(v, ori, sd, alpha, nl, ts);
+    ray[0] = sd.x; ray[1] = sd.y; ray[2] = sd.z; ray[3] = p25 ? ts[1] : ts[0];
+    const float rn = fd(1.0f, 3.0f);
+    float min_t = fm(ts[2], rn), max_t = fm(fmaxf(ts[0], ts[1]), rn);
+    tg[gid] = fm(fa(min_t, max_t), 0.5f);
+    tg[gid + 1] = fs(max_t, min_t);
+    tg[gid / 2 + 128] = ts[3];
+    if (ray[3] != 0) {
+        acc.minx = fminf(acc.minx, ox); acc.miny = fminf(acc.miny, oy);
+        acc.maxx = fmaxf(acc.maxx, ox); acc.maxy = fmaxf(acc.maxy, oy);
+        acc.avg = add(acc.avg, ts[1] > 0 ? mul(sd, 2.0f) : sd);
+        float sum_t = fa(ts[0], ts[1]);
+        hd = fa(hd, sum_t);
+        vd = fa(vd, sum_t);
+    }
+}
+
+struct TileView {
+    int W, H, px, py, frame;
+    uint32_t seed;
+    f3 ori, up, right, L;
+    float alpha, g;
+    float nl[3];
+};
+
+__global__ void __launch_bounds__(64) k_gather_tiles(VolumeDev v, TileView T, float* __restrict__ out) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= T.W * T.H) return;
+    int i = idx / T.W, j = idx % T.W;
+    float* ob = out + (size_t)idx * 773;
+    float u = fs(1.0f, fd(fa(fa((float)j, fd((float)T.px, 8.0f)), 0.5f), (float)T.W));
+    float w = fs(1.0f, fd(fa(fa((float)i, fd((float)T.py, 8.0f)), 0.5f), (float)T.H));
+    f3 fwd = normalize(neg(T.ori));
+    f3 dir = add(add(fwd, mul(T.right, fs(fm(u, 2.0f), 1.0f))), mul(T.up, fs(fm(w, 2.0f), 1.0f)));
+    const float rw = fm((float)T.W, 4.0f), rh = fm((float)T.H, 4.0f);
+    f3 ro = mk3(fd(-T.right.x, rw), fd(-T.right.y, rw), fd(-T.right.z, rw));
+    f3 uo = mk3(fd(-T.up.x, rh), fd(-T.up.y, rh), fd(-T.up.z, rh));
+    float samples[16][4];
+    TileAcc acc{FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, mk3(0, 0, 0)};
+    float hor = 0.0f, vert = 0.0f;
+    float* tg = ob + 192 * 3 + 5;
+    if (idx == 0) ob[0] = fm(ob[0], 1.00001f);
+    for (int y = -3, sid = 0, gid = 0, cb = 0; y <= 3; y += 2, cb = (cb + 1) & 1, gid += 16)
+        for (int x = -3; x <= 3; x += 2, sid++, gid += 4) {
+            bool p25 = ((sid + cb) & 1) != 0;
+            float h_ = 0.0f, v_ = 0.0f;
+            float r[4], c[4];
+            prepare_ray(v, (float)x - 0.5f, (float)y - 0.5f, dir, ro, uo, T.ori, T.alpha, T.nl, p25, gid, tg, acc, h_,
+                        v_, r);
+#pragma unroll 1
+            for (int q = 0; q < 3; ++q) {
+                float ox = q == 1 ? -0.5f : 0.5f, oy = q == 0 ? -0.5f : 0.5f;
+                int go = q == 0 ? 2 : q == 1 ? 16 : 18;
+                prepare_ray(v, (float)x + ox, (float)y + oy, dir, ro, uo, T.ori, T.alpha, T.nl, p25, gid + go, tg, acc,
+                            h_, v_, c);
+                if ((c[3] != 0 && ((c[3] < r[3]) != p25)) || r[3] == 0)
+                    for (int k = 0; k < 4; ++k) r[k] = c[k];
+            }
+            hor = fa(hor, x > 0 ? h_ : -h_);
+            vert = fa(vert, y > 0 ? v_ : -v_);
+            int fill = sid / 2 + (p25 ? 8 : 0);
+            for (int k = 0; k < 4; ++k) samples[fill][k] = r[k];
+        }
+    if (idx == 0) ob[0] = fm(ob[0], 1.00001f);
+    if (acc.minx == FLT_MAX) { ob[0] = -1000.0f; return; }
+    Stream st(kPixelStream, (uint32_t)idx, 0, (uint32_t)T.frame, T.seed);
+    f3 X, Y, Z, LX, LY, LZ;
+    basis(acc.avg, 0.0f, st, &X, &Y, &Z);
+    basis(T.L, 0.0f, st, &LX, &LY, &LZ);
+    float minx = fs(acc.minx, 0.5f), miny = fs(acc.miny, 0.5f), maxx = fa(acc.maxx, 0.5f), maxy = fa(acc.maxy, 0.5f);
+    f3 blc = normalize(add(add(dir, mul(ro, minx)), mul(uo, miny)));
+    f3 rc = normalize(add(dir, mul(ro, maxx))), uc = normalize(add(dir, mul(uo, maxy)));
+    auto cl = [](float x) { return fmaxf(-1.0f, fminf(1.0f, x)); };
+    float* go = ob + 192 * 3;
+    go[0] = acosf(cl(dot(X, T.L)));
+    float gbl = acosf(cl(dot(blc, T.L)));
+    go[1] = fs(acosf(cl(dot(rc, T.L))), gbl);
+    go[2] = fs(acosf(cl(dot(uc, T.L))), gbl);
+    go[3] = hor;
+    go[4] = vert;
+    // SetupInputData2: X_Val [0, 192), X_Val_Hg [192, 384), X_Val_Sub [384, 576)
+    for (int k = 0; k < 16; ++k) {
+        const float* sm = samples[k];
+        if (sm[3] != 0) {
+            f3 sd = mk3(sm[0], sm[1], sm[2]);
+            f3 sp = add(T.ori, mul(sd, sm[3]));
+            float d = tex3<false>(mip_level(v, 0), 256, sp);
+            ob[k] = logf(fa(1.0f, fm(fm(T.alpha, d), 0.015625f)));
+            ob[192 + k] = logf(fa(hg(dot(sd, T.L), T.g), 1.0f));
+            ob[384 + k] = shadow_tr(v, sp, T.L, 0);
+        } else {
+            ob[k] = 0.0f; ob[192 + k] = 0.0f; ob[384 + k] = 0.0f;
+        }
+    }
+    int sid = 0;
+    for (int k = 16; k < 192; ++k) {
+        while (samples[sid][3] == 0) sid = (sid + 1) & 0xf;
+        const float* sm = samples[sid];
+        sid = (sid + 1) & 0xf;
+        PixelFrame pf{add(T.ori, mul(mk3(sm[0], sm[1], sm[2]), sm[3])), X, Y, Z, T.L, T.L, T.g, T.alpha};
+        float fdv, fsv, fhv;
+        gather_sample(v, pf, k, &fdv, &fsv, &fhv);
+        ob[k] = fdv;
+        ob[192 + k] = fhv;
+        ob[384 + k] = fsv;
+    }
+    if (idx == 0) ob[0] = fm(ob[0], 1.00001f);
+}
+
+cudaError_t launch_gather_tiles(const VolumeDev& v, const ViewDev& view, int px, int py, const float nl[3], float* out,
+                                cudaStream_t s) {
+    int n = view.width * view.height;
+    if (n <= 0) return cudaSuccess;
+    TileView T{view.width, view.height, px, py, view.frame, view.seed, view.ori, view.up, view.right,
+               view.light_dir, view.alpha, view.g, {nl[0], nl[1], nl[2]}};
+    k_gather_tiles<<<(n + 63) / 64, 64, 0, s>>>(v, T, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;

@@ -9,6 +9,7 @@
 #include "mrpnn_oracle.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1332,5 +1333,238 @@ void orc_frame_finish(const float* target, float* histo, int W, int H, int frame
             histo[33 * (size_t)id + 32] = t.y;
             histo[33 * (size_t)id + 31] = t.z;
         }
+}
+
+// ---------------------------------------------------------------------------
+// Tile gather of the tile network (GatherData -> GatherSamples ->
+// NNGatherSamples, core/volume.cu:257-282, 630-700; core/render.cuh:298-397,
+// 464-485, 1006-1142; SetupInputData2, core/radiancePredict.cu:487-553).
+// 773 floats per tile: X_Val[192], X_Val_Hg[192], X_Val_Sub[192], 5 angle /
+// depth-gradient terms, 192 t-grid values.  neg_logs = {-log 0.76, -log 0.75,
+// -log 0.25} (host logf, as the reference computes them in the loop).
+// ---------------------------------------------------------------------------
+static bool check_exit(float S, float lastS, float dt, float t, float& tau, float& tau_target, float ts[4],
+                       bool& first_hit, float tau_second) {
+    float tau_next = tau + (S + lastS) * 0.5f * dt;
+    if (tau_next >= tau_target) {
+        float dtau = tau_target - tau;
+        float A = 0.5f * dt * (S - lastS), B = dt * lastS, C = -dtau;
+        auto solve = [&](float Cq, float dq) {
+            float off;
+            if (std::fabs(A) < 1e-6f) {
+                off = dq / (dt * (S + lastS) * 0.5f);
+            } else {
+                float D = B * B - 4.0f * A * Cq;
+                D = fmax_(D, 0.0f);
+                float sq = std::sqrt(D);
+                float q = (float)(-0.5 * (double)(B + sq));
+                float u1 = q / A, u2 = Cq / q;
+                off = (u1 == fmin_(fmax_(u1, 0.0f), 1.0f)) ? u1 : u2;
+            }
+            return off;
+        };
+        float off = solve(C, dtau);
+        off = fmin_(fmax_(off, 0.0f), 1.0f);
+        float hit_t = t - dt * (1.0f - off);
+        if (first_hit) {
+            ts[0] = hit_t;
+            tau_target = tau_second;
+            first_hit = false;
+            if (tau_next >= tau_target) {
+                float d2 = tau_target - tau;
+                float off2 = solve(-d2, d2);
+                ts[1] = t - dt * (1.0f - off2);
+                return true;
+            }
+        } else {
+            ts[1] = hit_t;
+            return true;
+        }
+    }
+    tau = tau_next;
+    return false;
+}
+
+static void estimated_hit_ts(const orc_scene* s, float alpha, f3 pos, f3 dir, float dis, const float nl[3],
+                             float ts[4]) {
+    float smax = s->max_density * alpha;
+    float t = 0;
+    ts[0] = 0; ts[1] = 0; ts[2] = FLT_MAX; ts[3] = 0;
+    float last_non_empty_t = 0;
+    float t_step = 1.0f / (float)s->res;
+    if (smax * t_step > nl[0]) t_step = nl[0] / smax;
+    float tau = 0, tau_target = nl[1];
+    bool first = true;
+    int loop = 0;
+    float last = 0;
+    while (loop++ < 10000) {
+        if (t > dis) {
+            if (first) ts[0] = last_non_empty_t;
+            else ts[1] = last_non_empty_t;
+            break;
+        }
+        float d = density(s, pos + dir * t);
+        if (d > 0) {
+            float S = d * alpha;
+            if (check_exit(S, last, t_step, t, tau, tau_target, ts, first, nl[2])) break;
+            ts[2] = fmin_(t, ts[2]);
+            t += t_step;
+            last = S;
+        } else {
+            if (last > 0) {
+                float ts_ = t_step + d;
+                if (ts_ > 0) {
+                    if (check_exit(0.0f, last, ts_, t, tau, tau_target, ts, first, nl[2])) break;
+                    last_non_empty_t = t + ts_;
+                } else {
+                    last_non_empty_t = t;
+                }
+            }
+            t += fmax_(-d * 1.0f, 0.5f / (float)s->res);
+            last = 0.0f;
+        }
+    }
+    if (ts[2] == FLT_MAX) ts[2] = 0.0f;
+    float survival = std::exp(-tau);
+    ts[3] = fmin_(fmax_(1.0f - survival, 0.0f) / 0.75f, 1.0f);
+}
+
+static void sample_t(const orc_scene* s, f3 ori, f3 dir, float alpha, const float nl[3], float ts[4]) {
+    float dis = ray_box_offset(ori, dir);
+    if (dis < 0) { ts[0] = ts[1] = ts[2] = ts[3] = 0; return; }
+    f3 sp = ori + dir * dis;
+    float md = ray_box_distance(sp, dir);
+    estimated_hit_ts(s, alpha, sp, dir, md, nl, ts);
+    if (ts[0] > 0) { ts[0] += dis; ts[2] += dis; }
+    if (ts[1] > 0) ts[1] += dis;
+}
+
+struct TileAcc {
+    float minx = FLT_MAX, miny = FLT_MAX, maxx = -FLT_MAX, maxy = -FLT_MAX;
+    f3 avg = {0, 0, 0};
+};
+
+static void prepare_ray(const orc_scene* s, float ox, float oy, f3 dir, f3 ro, f3 uo, f3 ori, float alpha,
+                        const float nl[3], bool p25, int gid, float* tg, TileAcc& acc, float& hd, float& vd,
+                        float ray[4]) {
+    f3 sd = normalize((dir + ro * ox) + uo * oy);
+    float ts[4];
+    sample_t(s, ori, sd, alpha, nl, ts);
+    ray[0] = sd.x; ray[1] = sd.y; ray[2] = sd.z; ray[3] = p25 ? ts[1] : ts[0];
+    const float rn = 1.0f / 3.0f;
+    float min_t = ts[2] * rn, max_t = fmax_(ts[0], ts[1]) * rn;
+    tg[gid] = (min_t + max_t) * 0.5f;
+    tg[gid + 1] = max_t - min_t;
+    tg[gid / 2 + 128] = ts[3];
+    if (ray[3] != 0) {
+        acc.minx = fmin_(acc.minx, ox); acc.miny = fmin_(acc.miny, oy);
+        acc.maxx = fmax_(acc.maxx, ox); acc.maxy = fmax_(acc.maxy, oy);
+        acc.avg = acc.avg + ((ts[1] > 0) ? sd * 2.0f : sd);
+        float sum_t = ts[0] + ts[1];
+        hd += sum_t;
+        vd += sum_t;
+    }
+}
+
+void orc_gather_tiles(const orc_scene* s, const orc_view* v, int px, int py, float* out) {
+    const int W = v->width, H = v->height;
+    const float neg_logs[3] = {-std::log(0.76f), -std::log(0.75f), -std::log(0.25f)};
+    const float* dirs_tab = T("STENCIL_DIRS");
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int idx = 0; idx < W * H; ++idx) {
+        int i = idx / W, j = idx % W;
+        float* ob = out + (size_t)idx * 773;
+        for (int k = 0; k < 773; ++k) ob[k] = 0;
+        float u = 1.0f - ((float)j + (float)px / 8.0f + 0.5f) / (float)W;
+        float w = 1.0f - ((float)i + (float)py / 8.0f + 0.5f) / (float)H;
+        f3 ori = load3(v->ori), L = load3(v->light_dir);
+        f3 fwd = normalize(neg(ori));
+        f3 dir = (fwd + (load3(v->right) * (u * 2 - 1))) + (load3(v->up) * (w * 2 - 1));
+        f3 ro = f3{-v->right[0] / ((float)W * 4.0f), -v->right[1] / ((float)W * 4.0f), -v->right[2] / ((float)W * 4.0f)};
+        f3 uo = f3{-v->up[0] / ((float)H * 4.0f), -v->up[1] / ((float)H * 4.0f), -v->up[2] / ((float)H * 4.0f)};
+        float samples[16][4];
+        TileAcc acc;
+        float hor = 0, vert = 0;
+        float* tg = ob + 192 * 3 + 5;
+        if (idx == 0) ob[0] *= 1.00001f;
+        for (int y = -3, sid = 0, gid = 0, cb = 0; y <= 3; y += 2, cb = (cb + 1) & 1, gid += 16)
+            for (int x = -3; x <= 3; x += 2, sid++, gid += 4) {
+                bool p25 = ((sid + cb) & 1) != 0;
+                float h_ = 0, v_ = 0;
+                float r[4], c[4];
+                prepare_ray(s, x - 0.5f, y - 0.5f, dir, ro, uo, ori, v->alpha, neg_logs, p25, gid, tg, acc, h_, v_, r);
+                const int offs[3][3] = {{1, -1, 2}, {-1, 1, 16}, {1, 1, 18}};
+                for (int q = 0; q < 3; ++q) {
+                    prepare_ray(s, x + 0.5f * offs[q][0], y + 0.5f * offs[q][1], dir, ro, uo, ori, v->alpha, neg_logs,
+                                p25, gid + offs[q][2], tg, acc, h_, v_, c);
+                    if ((c[3] != 0 && ((c[3] < r[3]) != p25)) || r[3] == 0)
+                        for (int k = 0; k < 4; ++k) r[k] = c[k];
+                }
+                hor += (x > 0) ? h_ : -h_;
+                vert += (y > 0) ? v_ : -v_;
+                int fill = sid / 2 + (p25 ? 8 : 0);
+                for (int k = 0; k < 4; ++k) samples[fill][k] = r[k];
+            }
+        if (idx == 0) ob[0] *= 1.00001f;
+        if (acc.minx == FLT_MAX) { ob[0] = -1000; continue; }
+        Stream st(0, (uint32_t)idx, 0, (uint32_t)v->frame, v->seed);
+        f3 bm[3], bl[3];
+        basis(acc.avg, 0.0f, st, bm);
+        basis(L, 0.0f, st, bl);
+        float minx = acc.minx - 0.5f, miny = acc.miny - 0.5f, maxx = acc.maxx + 0.5f, maxy = acc.maxy + 0.5f;
+        f3 blc = normalize((dir + ro * minx) + uo * miny), rc = normalize(dir + ro * maxx), uc = normalize(dir + uo * maxy);
+        auto sc = [](float x) { return fmax_(-1.0f, fmin_(1.0f, x)); };
+        float* go = ob + 192 * 3;
+        go[0] = std::acos(sc(dot(bm[0], L)));
+        float gbl = std::acos(sc(dot(blc, L)));
+        go[1] = std::acos(sc(dot(rc, L))) - gbl;
+        go[2] = std::acos(sc(dot(uc, L))) - gbl;
+        go[3] = hor;
+        go[4] = vert;
+        // SetupInputData2: X_Val at [0, 192), X_Val_Hg at [192, 384), X_Val_Sub at [384, 576)
+        float* xv = ob;
+        float* xh = ob + 192;
+        float* xs = ob + 384;
+        f3 X = bm[0], Y = bm[1], Z = bm[2];
+        for (int k = 0; k < 16; ++k) {
+            const float* sm = samples[k];
+            if (sm[3] != 0) {
+                f3 sd = {sm[0], sm[1], sm[2]};
+                f3 sp = ori + sd * sm[3];
+                xv[k] = std::log(1.0f + v->alpha * tex3(mip_ptr(s->mips, 0), 256, sp, false) / 64.0f);
+                xh[k] = std::log(hg(dot(sd, L), v->g) + 1.0f);
+                xs[k] = shadow_tr(s, sp, L, 0);
+            } else {
+                xv[k] = xh[k] = xs[k] = 0;
+            }
+        }
+        int sid = 0;
+        for (int k = 16; k < 192; ++k) {
+            while (samples[sid][3] == 0) sid = (sid + 1) & 0xf;
+            const float* sm = samples[sid];
+            sid = (sid + 1) & 0xf;
+            f3 sp = ori + f3{sm[0], sm[1], sm[2]} * sm[3];
+            StencilEntry e = stencil(k);
+            e.layer += 0.1f;
+            int layer = (int)e.layer;
+            f3 cur;
+            if (e.type >= 4) {
+                f3 p = load3(dirs_tab + 3 * k);
+                cur = sp + ((X * p.x + Y * p.y + Z * p.z) * e.offset);
+            } else {
+                cur = sp + L * e.offset;
+            }
+            xv[k] = std::log(1.0f + v->alpha * tex3(mip_ptr(s->mips, layer), 256 >> layer, cur, false) / 64.0f);
+            f3 ms = normalize(cur - sp);
+            float radius = (float)(1 << layer) / 256.0f;
+            float angle = std::atan(0.5f * radius / e.offset);
+            float c1 = dot(X, ms), c2 = dot(L, ms);
+            float uu = c1 * 0.5f + 0.5f, uu2 = c2 * 0.5f + 0.5f;
+            float vv = angle / (3.1415926535f * 60.0f / 180.0f);
+            xh[k] = std::log(tex_lut(s->hg_lut, uu, vv) * tex_lut(s->hg_lut, uu2, vv) + 1.0f);
+            xs[k] = shadow_tr(s, cur, L, std::max(layer - 1, 0));
+        }
+        if (idx == 0) ob[0] *= 1.00001f;
+    }
 }
 }  // extern "C"

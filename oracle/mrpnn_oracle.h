@@ -140,6 +140,9 @@ void orc_frame_pt(const orc_scene* s, const orc_view* v, int fnum, int checker, 
                   float* histo);
 void orc_frame_finish(const float* target, float* histo, int W, int H, int frame_num, int flip, int predict,
                       int denoise, float exposure, int tone, uint32_t* rgba8);
+/* GatherData (tile features of the tile network): v->width x v->height tiles,
+ * sub-pixel offset (px, py) in 1/8 tile; out [tiles][773]. */
+void orc_gather_tiles(const orc_scene* s, const orc_view* v, int px, int py, float* out);
 /* GetTrs: ShadowTerm_TRs per task; out [n][3]. */
 void orc_get_trs(const orc_scene* s, float alpha, const float* ori, const float* dir, int n, const float L[3],
                  const float lc[3], float g, int spp, uint32_t seed, float* out3);

@@ -98,6 +98,7 @@ def lib():
                                    C.c_void_p]
         L.orc_frame_finish.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_float, C.c_int, C.c_void_p]
+        L.orc_gather_tiles.argtypes = [C.POINTER(Scene), C.POINTER(View), C.c_int, C.c_int, C.c_void_p]
         L.orc_trace_rays.argtypes = [C.POINTER(Scene), C.POINTER(View), C.c_void_p, C.c_void_p, C.c_int,
                                      C.c_void_p, C.c_void_p]
         L.orc_get_samples.argtypes = [C.POINTER(Scene)] + [C.c_void_p] * 6 + [C.c_int, F3, C.c_int, C.c_int,
@@ -149,6 +150,8 @@ def ref():
                                          C.c_uint32, C.c_int, i32p, C.c_int, f32p]
         R.ref_trace_sample.argtypes = [C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_float,
                                        C.c_int, C.c_uint32, C.c_int, C.c_int, C.c_int, f32p]
+        R.ref_gather_tile.argtypes = [C.c_int, C.c_int, f32p, f32p, f32p, f32p, C.c_float, C.c_float, C.c_uint32,
+                                      C.c_int, C.c_int, C.c_int, C.c_int, f32p]
         _ref = R
     return _ref
 
@@ -323,6 +326,13 @@ def frame_finish(target, histo, frame_num, flip, predict, denoise, exposure, ton
     lib().orc_frame_finish(t.ctypes.data, h.ctypes.data, W, H, frame_num, flip, predict, denoise, exposure, tone,
                            out.ctypes.data)
     return out, h
+
+
+def gather_tiles(scene, view, px, py):
+    """GatherData: [view.width * view.height, 773] tile features."""
+    out = np.empty((view.width * view.height, 773), np.float32)
+    lib().orc_gather_tiles(C.byref(scene.c), C.byref(view), px, py, out.ctypes.data)
+    return out
 
 
 def mlp_f32(feat, gamma, g, sr):

@@ -280,6 +280,27 @@ void ref_predict_pixels(int W, int H, const float ori[3], const float up[3], con
     });
 }
 
+// GatherSamples (core/volume.cu:257-282) for tile idx of a W x H tile grid:
+// its ray set-up restated here (volume.cu does not build on the CPU), then
+// NNGatherSamples as the reference writes it.  The block index marks tile 0
+// as the kernel's block (0, 0) / thread (0, 0) for its debug multiplies.
+void ref_gather_tile(int W, int H, const float ori[3], const float up[3], const float right[3],
+                     const float light_dir[3], float alpha, float g, uint32_t seed, int frame, int px, int py, int idx,
+                     float* out773) {
+    int i = idx / W, j = idx % W;
+    blockIdx.x = idx == 0 ? 0u : 1u;
+    blockIdx.y = blockIdx.z = 0u;
+    threadIdx.x = threadIdx.y = threadIdx.z = 0u;
+    float u = 1.0f - ((float)j + (float)px / 8.0f + 0.5f) / (float)W;
+    float v = 1.0f - ((float)i + (float)py / 8.0f + 0.5f) / (float)H;
+    float3 forward = normalize(-ld3(ori));
+    float3 dir = forward + (ld3(right) * (u * 2 - 1)) + (ld3(up) * (v * 2 - 1));
+    float3 right_offset = -ld3(right) / (W * 4.0f);
+    float3 up_offset = -ld3(up) / (H * 4.0f);
+    set_stream(0, (uint32_t)idx, 0, (uint32_t)frame, seed);
+    NNGatherSamples(out773, ld3(ori), dir, ld3(light_dir), right_offset, up_offset, alpha, g);
+}
+
 // CalculateRadiance with sampleNum = 1 for sample k of pixel pix (stream sub k).
 void ref_trace_sample(int W, int H, const float ori[3], const float up[3], const float right[3],
                       const float light_dir[3], const float light_color[3], float alpha, float g, int multi_scatter,

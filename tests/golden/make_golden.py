@@ -185,6 +185,16 @@ def main():
         tv[i] = R.ref_tr(tp[i], L, dis, SCENE["alpha"], i, 0, 0, 9, 2)
     out["tr_pos"], out["tr_out"] = tp, tv
 
+    # tile gather of the tile network (GatherSamples -> NNGatherSamples)
+    TW = 6
+    tori, tup, tright = camera(TW)
+    tiles = np.zeros((TW * TW, 773), np.float32)
+    for idx in range(TW * TW):
+        o = np.zeros(773, np.float32)
+        R.ref_gather_tile(TW, TW, tori, tup, tright, L, SCENE["alpha"], SCENE["g"], 5, 2, 3, 5, idx, o)
+        tiles[idx] = o
+    out["tile_out"] = tiles
+
     np.savez_compressed(OUT, **out)
     print(OUT, os.path.getsize(OUT), "bytes")
 

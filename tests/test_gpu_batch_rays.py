@@ -95,3 +95,18 @@ def test_get_radiances_mrpnn_equals_frame(scene):
     oris = np.broadcast_to(np.asarray(ori, np.float32), (W * W, 3))
     got = scene.vol.GetRadiances(oris, dirs, LIGHT, (1, 1, 1), scene.alpha, 1, scene.g, 1, M.VolumeRender.MRPNN)
     np.testing.assert_allclose(got, frame[:, :3], rtol=1e-5, atol=1e-6)
+
+
+def test_gather_tiles_matches_oracle(scene):
+    """GatherData (773 tile features) on the GPU against the oracle, itself
+    pinned bit for bit to the reference's NNGatherSamples: the depth marches
+    use only +, -, *, /, sqrt, so only the last bits of log / acos / exp may
+    differ."""
+    TW = 12
+    ori, up, right = view_frame()
+    got = scene.vol.GatherData((TW, TW), ori, up, right, LIGHT, alpha=scene.alpha, g=scene.g, pixelOffset=(3, 5),
+                               seed=5, frame=2)
+    view = O.make_view(TW, TW, ori, up, right, LIGHT, alpha=scene.alpha, g=scene.g, seed=5, frame=2)
+    ref = O.gather_tiles(scene.orc, view, 3, 5)
+    assert (ref[:, 0] != -1000).sum() > 40
+    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-5)

@@ -159,3 +159,15 @@ def test_live_reference_mlp_small(oracle):
     gam = rng.uniform(0, np.pi, 32).astype(np.float32)
     np.testing.assert_array_equal(oracle.mlp_f32(feat, gam, 0.6, (0.95, 0.95, 0.95)),
                                   oracle.ref_mlp(feat, gam, 0.6, (0.95, 0.95, 0.95)))
+
+
+def test_gather_tiles(oracle, scene, golden):
+    """GatherData / NNGatherSamples (773 floats per tile) against the
+    reference's own code; tile 0 carries the kernel's debug multiplies."""
+    TW = 6
+    ori, up, right = camera(TW)
+    view = oracle.make_view(TW, TW, ori, up, right, light_dir(), alpha=SCENE["alpha"], g=SCENE["g"], seed=5, frame=2)
+    got = oracle.gather_tiles(scene, view, 3, 5)
+    ref = golden["tile_out"]
+    np.testing.assert_array_equal(got, ref)
+    assert (ref[:, 0] != -1000).sum() > 20     # most tiles see the cloud
