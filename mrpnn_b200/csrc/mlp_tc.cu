@@ -326,7 +326,7 @@ struct RowFeatures {           // [n][576] row-major
     const float* x;
     bool valid;
     template <int W>
-    MRP_D void load(int c, int from, float (&xs)[32]) const {
+    MRP_D void load(int c, int from, float* xs) const {
 #pragma unroll
         for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + c * 192 + from + i) : 0.0f;
     }
@@ -335,11 +335,56 @@ struct TileFeatures {          // tiled layout of the staged predictor
     const float* x;
     bool valid;
     template <int W>
-    MRP_D void load(int c, int from, float (&xs)[32]) const {
+    MRP_D void load(int c, int from, float* xs) const {
 #pragma unroll
         for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + (c * 192 + from + i) * 32) : 0.0f;
     }
 };
+
+// Per-row state that lives in TMEM between blocks (columns of the group's
+// 256; the MMA accumulators use 0..95 (main blocks, finals), 128..175 (DI
+// blocks), 176..223 (DI finals)): the LSEFin1 partial sums and the residual
+// of the main (3 x 32) and direct-illumination (3 x 8) chains.  Keeping them
+// out of registers leaves the per-block routines without a stack frame for
+// them.
+constexpr int kColHf = 96, kColPrevMain = 160, kColPrevDi = 232;
+
+template <int N>
+MRP_D void tmem_get(const Group& G, int col, float* out) {
+    if constexpr (N == 8) {
+        uint32_t r[8];
+        tc::tmem_ld8_nowait(G.tmem + col, r);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) out[i] = __uint_as_float(r[i]);
+    } else {
+        uint32_t r[N / 16][16];
+#pragma unroll
+        for (int c = 0; c < N / 16; ++c) tc::tmem_ld16_nowait(G.tmem + col + 16 * c, r[c]);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < N / 16; ++c)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) out[16 * c + i] = __uint_as_float(r[c][i]);
+    }
+}
+template <int N>
+MRP_D void tmem_put(const Group& G, int col, const float* v) {
+    if constexpr (N == 8) {
+        float t[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t[i] = v[i];
+        tc::tmem_st8(G.tmem + col, t);
+    } else {
+#pragma unroll
+        for (int c = 0; c < N / 16; ++c) {
+            float t[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) t[i] = v[16 * c + i];
+            tc::tmem_st16(G.tmem + col + 16 * c, t);
+        }
+    }
+}
 
 // One SE block over the three channels (SE / SERES + ADD3 / REP3,
 // core/radiancePredict.cu:240-294): gate from the slice pools, branch layers
@@ -348,36 +393,40 @@ struct TileFeatures {          // tiled layout of the staged predictor
 template <int EB, int W, class Src>
 __device__ __noinline__ void tc_block(Group& G, const Src& src, const float* __restrict__ w32,
                                       const float* __restrict__ scales, int from, int widen, int has_prev, int l0,
-                                      int dcol, int se_off, int pid, float g, float gamma, float (&hf)[16],
-                                      float (&prev)[3][32]) {
+                                      int dcol, int se_off, int pid, float g, float gamma, int pcol, int pstride) {
     constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
     constexpr int SUB = 128 * KP * EB;   // bytes of one branch's A sub-tile
     constexpr int DSTR = W <= 16 ? 16 : 32;
+    float xs[3][W];                      // the block's feature slice, loaded once
     float p8[8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float xs[32];
-        src.template load<W>(c, from, xs);
+        src.template load<W>(c, from, xs[c]);
         float s = 0.0f, m = -10000.0f;
 #pragma unroll
-        for (int i = 0; i < W; ++i) { s += xs[i]; m = fmaxf(m, xs[i]); }
+        for (int i = 0; i < W; ++i) { s += xs[c][i]; m = fmaxf(m, xs[c][i]); }
         p8[c] = s / (float)W;
         p8[3 + c] = m;
     }
     p8[6] = g;
     p8[7] = gamma;
-    // LSEFin1 (75 -> 16) accumulated block by block: pool[pid + c] = avg,
-    // pool[36 + pid + c] = max
+    // LSEFin1 (75 -> 16) accumulated block by block in TMEM: pool[pid + c] =
+    // avg, pool[36 + pid + c] = max
+    {
+        float hf[16];
+        tmem_get<16>(G, kColHf, hf);
 #pragma unroll 4
-    for (int o = 0; o < 16; ++o) {
-        float a = hf[o];
-        const float* w1 = w32 + kLSEFin1W + o * 75 + pid;
+        for (int o = 0; o < 16; ++o) {
+            float a = hf[o];
+            const float* w1 = w32 + kLSEFin1W + o * 75 + pid;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            a = fmaf(__ldg(w1 + c), p8[c], a);
-            a = fmaf(__ldg(w1 + 36 + c), p8[3 + c], a);
+            for (int c = 0; c < 3; ++c) {
+                a = fmaf(__ldg(w1 + c), p8[c], a);
+                a = fmaf(__ldg(w1 + 36 + c), p8[3 + c], a);
+            }
+            hf[o] = a;
         }
-        hf[o] = a;
+        tmem_put<16>(G, kColHf, hf);
     }
     float h[8], gate[3];
 #pragma unroll
@@ -397,27 +446,36 @@ __device__ __noinline__ void tc_block(Group& G, const Src& src, const float* __r
     float rs[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float xs[32], in[32];
-        src.template load<W>(c, from, xs);
+        float in[W];
+        if (has_prev) {
+            float pv[W];
+            tmem_get<W>(G, pcol + c * pstride, pv);
 #pragma unroll
-        for (int i = 0; i < W; ++i) in[i] = has_prev ? fmaf(xs[i], gate[c], prev[c][i]) : xs[i] * gate[c];
+            for (int i = 0; i < W; ++i) in[i] = fmaf(xs[c][i], gate[c], pv[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < W; ++i) in[i] = xs[c][i] * gate[c];
+        }
         rs[c] = write_row<EB, W, KP>(G.a, c * SUB, G.t, in);
     }
     mma_round<EB>(G, 3, l0, 0, dcol, l0 + 1, SUB, dcol + DSTR, l0 + 2, 2 * SUB, dcol + 2 * DSTR);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float d[32], xs[32];
+        float d[W];
         read_cols<W>(G, dcol + c * DSTR, d);
         bias_relu<EB, W>(d, l0 + c, rs[c], w32, scales);
-        src.template load<W>(c, from, xs);
         if (widen) {
+            float nv[2 * W];
 #pragma unroll
-            for (int o = 0; o < W; ++o) { prev[c][o] = d[o]; prev[c][W + o] = xs[o]; }
+            for (int o = 0; o < W; ++o) { nv[o] = d[o]; nv[W + o] = xs[c][o]; }
+            tmem_put<2 * W>(G, pcol + c * pstride, nv);
         } else {
 #pragma unroll
-            for (int o = 0; o < W; ++o) prev[c][o] = d[o] + xs[o];
+            for (int o = 0; o < W; ++o) d[o] = d[o] + xs[c][o];
+            tmem_put<W>(G, pcol + c * pstride, d);
         }
     }
+    tc::tmem_wait_st();
 }
 
 // Residual pair k of the tail: a += relu(LX(2k+1) relu(LX(2k) a + b) + b).
@@ -440,55 +498,71 @@ __device__ __noinline__ void tc_residual_pair(Group& G, const float* __restrict_
     for (int i = 0; i < 16; ++i) a16[i] += z[i];
 }
 
-struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid; };
+struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid, pcol, pstride; };
 __constant__ BlockDesc c_blocks[12] = {
-    {8, 0, 0, 0, 0, 0, mblk_off(0), 0},      {8, 8, 1, 1, 3, 0, mblk_off(1), 3},
-    {16, 16, 0, 1, 6, 0, mblk_off(2), 6},    {16, 32, 0, 1, 9, 0, mblk_off(3), 9},
-    {16, 48, 1, 1, 12, 0, mblk_off(4), 12},  {32, 64, 0, 1, 15, 0, mblk_off(5), 15},
-    {32, 96, 0, 1, 18, 0, mblk_off(6), 18},  {32, 128, 0, 1, 21, 0, mblk_off(7), 21},
-    {8, 160, 0, 0, 27, 128, di_block_off(0), 24}, {8, 168, 0, 1, 30, 128, di_block_off(1), 27},
-    {8, 176, 0, 1, 33, 128, di_block_off(2), 30}, {8, 184, 0, 1, 36, 128, di_block_off(3), 33},
+    {8, 0, 0, 0, 0, 0, mblk_off(0), 0, kColPrevMain, 32},      {8, 8, 1, 1, 3, 0, mblk_off(1), 3, kColPrevMain, 32},
+    {16, 16, 0, 1, 6, 0, mblk_off(2), 6, kColPrevMain, 32},    {16, 32, 0, 1, 9, 0, mblk_off(3), 9, kColPrevMain, 32},
+    {16, 48, 1, 1, 12, 0, mblk_off(4), 12, kColPrevMain, 32},  {32, 64, 0, 1, 15, 0, mblk_off(5), 15, kColPrevMain, 32},
+    {32, 96, 0, 1, 18, 0, mblk_off(6), 18, kColPrevMain, 32},  {32, 128, 0, 1, 21, 0, mblk_off(7), 21, kColPrevMain, 32},
+    {8, 160, 0, 0, 27, 128, di_block_off(0), 24, kColPrevDi, 8}, {8, 168, 0, 1, 30, 128, di_block_off(1), 27, kColPrevDi, 8},
+    {8, 176, 0, 1, 33, 128, di_block_off(2), 30, kColPrevDi, 8}, {8, 184, 0, 1, 36, 128, di_block_off(3), 33, kColPrevDi, 8},
 };
 
 template <int EB, class Src>
 MRP_D void run_block(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales, int b,
-                     float g, float gamma, float (&hf)[16], float (&prev)[3][32]) {
+                     float g, float gamma) {
     const BlockDesc d = c_blocks[b];
     if (d.w == 8)
-        tc_block<EB, 8>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma, hf, prev);
+        tc_block<EB, 8>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+                        d.pcol, d.pstride);
     else if (d.w == 16)
-        tc_block<EB, 16>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma, hf, prev);
+        tc_block<EB, 16>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+                         d.pcol, d.pstride);
     else
-        tc_block<EB, 32>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma, hf, prev);
+        tc_block<EB, 32>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+                         d.pcol, d.pstride);
 }
 
 template <int EB, class Src>
 MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
                       float gamma, float g, f3 sr, float out[3]) {
-    float hf[16];
+    {
+        float z[16];
 #pragma unroll
-    for (int o = 0; o < 16; ++o) hf[o] = 0.0f;
-    float prev[3][32];
+        for (int o = 0; o < 16; ++o) z[o] = 0.0f;
+        tmem_put<16>(G, kColHf, z);
+        tc::tmem_wait_st();
+    }
     // main branch, X[0:160]; the three 32x32 finals leave comb[0:96) in TMEM columns 0..95
 #pragma unroll 1
-    for (int b = 0; b < 8; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma, hf, prev);
+    for (int b = 0; b < 8; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma);
     float rs_main[3];
     {
         constexpr int KP = pad_to(32, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) rs_main[c] = write_row<EB, 32, KP>(G.a, c * SUB, G.t, prev[c]);
+        for (int c = 0; c < 3; ++c) {
+            float pv[32];
+            tmem_get<32>(G, kColPrevMain + 32 * c, pv);
+            rs_main[c] = write_row<EB, 32, KP>(G.a, c * SUB, G.t, pv);
+        }
         mma_round<EB>(G, 3, kL81, 0, 0, kL81 + 1, SUB, 32, kL81 + 2, 2 * SUB, 64);
     }
     // direct-illumination branch, X[160:192]; the 8x8 finals at columns 176..223
 #pragma unroll 1
-    for (int b = 8; b < 12; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma, hf, prev);
+    for (int b = 8; b < 12; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma);
     float rs_di[3];
     {
         constexpr int KP = pad_to(8, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) rs_di[c] = write_row<EB, 8, KP>(G.a, c * SUB, G.t, prev[c]);
+        for (int c = 0; c < 3; ++c) {
+            float pv[8];
+            tmem_get<8>(G, kColPrevDi + 8 * c, pv);
+            rs_di[c] = write_row<EB, 8, KP>(G.a, c * SUB, G.t, pv);
+        }
         mma_round<EB>(G, 3, kLD41, 0, 176, kLD41 + 1, SUB, 192, kLD41 + 2, 2 * SUB, 208);
     }
+    float hf[16];
+    tmem_get<16>(G, kColHf, hf);   // before LC0's accumulator covers columns 0..127
     // comb[120] = relu(finals + b): main (3 x 32) then direct illumination (3 x 8)
     float comb[120];
 #pragma unroll
