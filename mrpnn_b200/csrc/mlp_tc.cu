@@ -206,22 +206,25 @@ __device__ __forceinline__ void group_bar(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory");
 }
 
+// Per-thread constants of a group, passed by value into the per-block
+// routines (a reference would put them in local memory and make every use a
+// load).  The mutable part -- mbarrier phase (bit 0) and "a wait timed out"
+// (bit 1) -- travels as an int through the calls.
 struct Group {
     int g, t;             // group index, thread within the group
     uint8_t* a;           // A buffer (shared)
     const uint8_t* wimg;  // weight image (shared)
     uint64_t* mbar;
-    uint32_t phase;
     uint32_t tmem;        // TMEM address of this thread's lane, column 0 of the group
     uint32_t tmem_col0;   // TMEM address of lane 0, column 0 of the group (MMA D base)
     int* err;
-    bool ok;
 };
+constexpr int kStFailed = 2;
 
 // Up to three MMAs (layer, A sub-tile byte offset, D column), issued after
 // all A rows are in shared memory and awaited by the whole group.
 template <int EB>
-__device__ __noinline__ void mma_round(Group& G, int count, int l0, int a0, int d0, int l1, int a1, int d1, int l2,
+__device__ __noinline__ int mma_round(const Group G, int st, int count, int l0, int a0, int d0, int l1, int a1, int d1, int l2,
                                        int a2, int d2) {
     tc::fence_proxy_async();
     tc::fence_before_sync();
@@ -250,13 +253,14 @@ __device__ __noinline__ void mma_round(Group& G, int count, int l0, int a0, int 
         }
         tc::mma_commit(G.mbar);
     }
-    bool done = tc::mbar_wait(G.mbar, G.phase, kWaitLimit);
-    G.phase ^= 1u;
+    bool done = tc::mbar_wait(G.mbar, (uint32_t)(st & 1), kWaitLimit);
+    st ^= 1;
     if (!done) {
-        G.ok = false;
+        st |= kStFailed;
         atomicExch(G.err, 1);
     }
     tc::fence_after_sync();
+    return st;
 }
 
 // Writes this thread's row of an A operand: v[0..n) (zero padded to kp) at
@@ -391,7 +395,7 @@ MRP_D void tmem_put(const Group& G, int col, const float* v) {
 // l0..l0+2 on the tensor cores (D at dcol, dcol+stride, dcol+2*stride), then
 // prev <- relu(D + b) + slice (ADD3) or concat(relu(D + b), slice) (REP3).
 template <int EB, int W, class Src>
-__device__ __noinline__ void tc_block(Group& G, const Src& src, const float* __restrict__ w32,
+__device__ __noinline__ int tc_block(const Group G, int st, const Src src, const float* __restrict__ w32,
                                       const float* __restrict__ scales, int from, int widen, int has_prev, int l0,
                                       int dcol, int se_off, int pid, float g, float gamma, int pcol, int pstride) {
     constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
@@ -458,7 +462,7 @@ __device__ __noinline__ void tc_block(Group& G, const Src& src, const float* __r
         }
         rs[c] = write_row<EB, W, KP>(G.a, c * SUB, G.t, in);
     }
-    mma_round<EB>(G, 3, l0, 0, dcol, l0 + 1, SUB, dcol + DSTR, l0 + 2, 2 * SUB, dcol + 2 * DSTR);
+    st = mma_round<EB>(G, st, 3, l0, 0, dcol, l0 + 1, SUB, dcol + DSTR, l0 + 2, 2 * SUB, dcol + 2 * DSTR);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float d[W];
@@ -476,26 +480,34 @@ __device__ __noinline__ void tc_block(Group& G, const Src& src, const float* __r
         }
     }
     tc::tmem_wait_st();
+    return st;
 }
 
-// Residual pair k of the tail: a += relu(LX(2k+1) relu(LX(2k) a + b) + b).
+// Residual pair k of the tail: a += relu(LX(2k+1) relu(LX(2k) a + b) + b),
+// a (16 values) kept in TMEM columns kColA16.
+constexpr int kColA16 = 96;
 template <int EB>
-__device__ __noinline__ void tc_residual_pair(Group& G, const float* __restrict__ w32, const float* __restrict__ scales,
-                                              int k, float (&a16)[16]) {
+__device__ __noinline__ int tc_residual_pair(const Group G, int st, const float* __restrict__ w32,
+                                             const float* __restrict__ scales, int k) {
     constexpr int KP = EB == 2 ? 16 : 32;
     const int La = kLX0 + 2 * k, Lb = La + 1;
+    float a16[16];
+    tmem_get<16>(G, kColA16, a16);
     float r0 = write_row<EB, 16, KP>(G.a, 0, G.t, a16);
-    mma_round<EB>(G, 1, La, 0, 64, 0, 0, 0, 0, 0, 0);
+    st = mma_round<EB>(G, st, 1, La, 0, 64, 0, 0, 0, 0, 0, 0);
     float u[16];
     read_cols<16>(G, 64, u);
     bias_relu<EB, 16>(u, La, r0, w32, scales);
     float r1 = write_row<EB, 16, KP>(G.a, 0, G.t, u);
-    mma_round<EB>(G, 1, Lb, 0, 80, 0, 0, 0, 0, 0, 0);
+    st = mma_round<EB>(G, st, 1, Lb, 0, 80, 0, 0, 0, 0, 0, 0);
     float z[16];
     read_cols<16>(G, 80, z);
     bias_relu<EB, 16>(z, Lb, r1, w32, scales);
 #pragma unroll
     for (int i = 0; i < 16; ++i) a16[i] += z[i];
+    tmem_put<16>(G, kColA16, a16);
+    tc::tmem_wait_st();
+    return st;
 }
 
 struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid, pcol, pstride; };
@@ -509,22 +521,21 @@ __constant__ BlockDesc c_blocks[12] = {
 };
 
 template <int EB, class Src>
-MRP_D void run_block(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales, int b,
-                     float g, float gamma) {
+MRP_D int run_block(const Group& G, int st, const Src& src, const float* __restrict__ w32,
+                    const float* __restrict__ scales, int b, float g, float gamma) {
     const BlockDesc d = c_blocks[b];
     if (d.w == 8)
-        tc_block<EB, 8>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+        return tc_block<EB, 8>(G, st, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
                         d.pcol, d.pstride);
     else if (d.w == 16)
-        tc_block<EB, 16>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+        return tc_block<EB, 16>(G, st, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
                          d.pcol, d.pstride);
-    else
-        tc_block<EB, 32>(G, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+    return tc_block<EB, 32>(G, st, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
                          d.pcol, d.pstride);
 }
 
 template <int EB, class Src>
-MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
+MRP_D int tc_network(const Group& G, int st, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
                       float gamma, float g, f3 sr, float out[3]) {
     {
         float z[16];
@@ -535,7 +546,7 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
     }
     // main branch, X[0:160]; the three 32x32 finals leave comb[0:96) in TMEM columns 0..95
 #pragma unroll 1
-    for (int b = 0; b < 8; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma);
+    for (int b = 0; b < 8; ++b) st = run_block<EB>(G, st, src, w32, scales, b, g, gamma);
     float rs_main[3];
     {
         constexpr int KP = pad_to(32, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
@@ -545,11 +556,11 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
             tmem_get<32>(G, kColPrevMain + 32 * c, pv);
             rs_main[c] = write_row<EB, 32, KP>(G.a, c * SUB, G.t, pv);
         }
-        mma_round<EB>(G, 3, kL81, 0, 0, kL81 + 1, SUB, 32, kL81 + 2, 2 * SUB, 64);
+        st = mma_round<EB>(G, st, 3, kL81, 0, 0, kL81 + 1, SUB, 32, kL81 + 2, 2 * SUB, 64);
     }
     // direct-illumination branch, X[160:192]; the 8x8 finals at columns 176..223
 #pragma unroll 1
-    for (int b = 8; b < 12; ++b) run_block<EB>(G, src, w32, scales, b, g, gamma);
+    for (int b = 8; b < 12; ++b) st = run_block<EB>(G, st, src, w32, scales, b, g, gamma);
     float rs_di[3];
     {
         constexpr int KP = pad_to(8, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
@@ -559,7 +570,7 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
             tmem_get<8>(G, kColPrevDi + 8 * c, pv);
             rs_di[c] = write_row<EB, 8, KP>(G.a, c * SUB, G.t, pv);
         }
-        mma_round<EB>(G, 3, kLD41, 0, 176, kLD41 + 1, SUB, 192, kLD41 + 2, 2 * SUB, 208);
+        st = mma_round<EB>(G, st, 3, kLD41, 0, 176, kLD41 + 1, SUB, 192, kLD41 + 2, 2 * SUB, 208);
     }
     float hf[16];
     tmem_get<16>(G, kColHf, hf);   // before LC0's accumulator covers columns 0..127
@@ -612,24 +623,27 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
             x[120 + o] = fmaxf(a + wl(w32, kLGGSB + o), 0.0f);
         }
         float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, x);
-        mma_round<EB>(G, 1, kLC0, 0, 0, 0, 0, 0, 0, 0, 0);
+        st = mma_round<EB>(G, st, 1, kLC0, 0, 0, 0, 0, 0, 0, 0, 0);
         read_cols<128>(G, 0, x);
         bias_relu<EB, 128>(x, kLC0, r, w32, scales);
         r = write_row<EB, 128, kpad(kLC1, EB)>(G.a, 0, G.t, x);
-        mma_round<EB>(G, 1, kLC1, 0, 128, 0, 0, 0, 0, 0, 0);
+        st = mma_round<EB>(G, st, 1, kLC1, 0, 128, 0, 0, 0, 0, 0, 0);
         read_cols<64>(G, 128, x);
         bias_relu<EB, 64>(x, kLC1, r, w32, scales);
         r = write_row<EB, 64, kpad(kLC2, EB)>(G.a, 0, G.t, x);
-        mma_round<EB>(G, 1, kLC2, 0, 0, 0, 0, 0, 0, 0, 0);
+        st = mma_round<EB>(G, st, 1, kLC2, 0, 0, 0, 0, 0, 0, 0, 0);
         read_cols<32>(G, 0, x);
         bias_relu<EB, 32>(x, kLC2, r, w32, scales);
         r = write_row<EB, 32, kpad(kLX, EB)>(G.a, 0, G.t, x);
-        mma_round<EB>(G, 1, kLX, 0, 32, 0, 0, 0, 0, 0, 0);
+        st = mma_round<EB>(G, st, 1, kLX, 0, 32, 0, 0, 0, 0, 0, 0);
         float a16[16];
         read_cols<16>(G, 32, a16);
         bias_relu<EB, 16>(a16, kLX, r, w32, scales);
+        tmem_put<16>(G, kColA16, a16);
+        tc::tmem_wait_st();
 #pragma unroll 1
-        for (int k = 0; k < 6; ++k) tc_residual_pair<EB>(G, w32, scales, k, a16);
+        for (int k = 0; k < 6; ++k) st = tc_residual_pair<EB>(G, st, w32, scales, k);
+        tmem_get<16>(G, kColA16, a16);
         float a = 0.0f;
 #pragma unroll
         for (int j = 0; j < 16; ++j) a = fmaf(a16[j], wl(w32, kLX12W + j), a);
@@ -637,6 +651,7 @@ MRP_D void tc_network(Group& G, const Src& src, const float* __restrict__ w32, c
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c] = fmaxf(expf(P[c]) - 1.0f, 0.0f) * powf(srv[c], 4.0f);
+    return st;
 }
 
 // ---------------------------------------------------------------------------
@@ -704,11 +719,10 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
     G.a = abuf + G.g * kABytes;
     G.wimg = wimg;
     G.mbar = mbar + G.g;
-    G.phase = 0;
     G.tmem_col0 = tbase + (uint32_t)(G.g * kTmemColsPerGroup);
     G.tmem = G.tmem_col0 + ((uint32_t)(32 * ((tid / 32) % 4)) << 16);
     G.err = A.err;
-    G.ok = true;
+    int st = 0;
 
     const int total_tiles = STAGED ? seg_start[nseg] : (A.n + 127) / 128;
     for (;;) {
@@ -716,7 +730,7 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
         group_bar(G.g);
         int tile = tile_slot[G.g];
         group_bar(G.g);
-        if (tile >= total_tiles || !G.ok) break;
+        if (tile >= total_tiles || (st & kStFailed)) break;
         float o[3];
         if (STAGED) {
             int q = 0;
@@ -727,8 +741,8 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
             const size_t cap = S->rec_cap;
             float gamma = valid ? S->rec_f[15 * cap + r] : 0.0f;
             TileFeatures src{S->feat + (size_t)(r >> 5) * 576 * 32 + (r & 31), valid};
-            tc_network<EB>(G, src, A.w32, A.scales, gamma, S->g, S->sr, o);
-            if (valid && G.ok) {
+            st = tc_network<EB>(G, st, src, A.w32, A.scales, gamma, S->g, S->sr, o);
+            if (valid && !(st & kStFailed)) {
                 int pix = S->rec_pix[r];
                 f3 hit = mk3(S->rec_f[r], S->rec_f[cap + r], S->rec_f[2 * cap + r]);
                 f3 res = mul(mul(mk3(o[0], o[1], o[2]), S->light_color), S->scatter_rate);
@@ -745,8 +759,8 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
             const bool valid = r < A.n;
             float gamma = valid ? A.gamma[r] : 0.0f;
             RowFeatures src{A.feat + (size_t)r * 576, valid};
-            tc_network<EB>(G, src, A.w32, A.scales, gamma, A.g, A.sr, o);
-            if (valid && G.ok) {
+            st = tc_network<EB>(G, st, src, A.w32, A.scales, gamma, A.g, A.sr, o);
+            if (valid && !(st & kStFailed)) {
                 A.out3[3 * (size_t)r] = o[0];
                 A.out3[3 * (size_t)r + 1] = o[1];
                 A.out3[3 * (size_t)r + 2] = o[2];
