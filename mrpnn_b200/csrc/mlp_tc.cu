@@ -61,6 +61,12 @@ __host__ __device__ constexpr int scale_off(int i) {
     return o;
 }
 constexpr int kScaleCount = scale_off(kLayers);
+// The fp32 constants the CUDA-core parts read, packed for shared memory:
+// FP8 weight scales, layer biases (both indexed by scale_off), the 12 SE gate
+// MLPs (8x8 + 3x8 each), LSEFin1 / LSEFin2, LGGS and the 16 -> 1 head.
+constexpr int kAuxScale = 0, kAuxBias = kScaleCount, kAuxSE = 2 * kScaleCount, kAuxLSE1 = kAuxSE + 12 * 88,
+              kAuxLSE2 = kAuxLSE1 + 1200, kAuxLGGSW = kAuxLSE2 + 96, kAuxLGGSB = kAuxLGGSW + 24,
+              kAuxLX12W = kAuxLGGSB + 8, kAuxLX12B = kAuxLX12W + 16, kAuxCount = (kAuxLX12B + 1 + 3) / 4 * 4;
 // fp32 weight / bias of layer i in the packed fp32 layout (common.cuh)
 __host__ __device__ constexpr int layer_w32(int i) {
     return i < 24 ? mblk_off(i / 3) + 88 + (i % 3) * (mw(i / 3) * mw(i / 3) + mw(i / 3))
@@ -134,7 +140,24 @@ cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
             }
         }
     }
+    std::vector<float> aux(kAuxCount, 0.0f);
+    for (int i = 0; i < kScaleCount; ++i) aux[kAuxScale + i] = scales[i];
+    for (int i = 0; i < kLayers; ++i)
+        for (int r = 0; r < layer_n(i); ++r) aux[kAuxBias + scale_off(i) + r] = w32[layer_b32(i) + r];
+    for (int b = 0; b < 12; ++b) {
+        const float* src = w32 + (b < 8 ? mblk_off(b) : di_block_off(b - 8));
+        std::memcpy(&aux[kAuxSE + 88 * b], src, 88 * sizeof(float));
+    }
+    std::memcpy(&aux[kAuxLSE1], w32 + kLSEFin1W, 1200 * sizeof(float));
+    std::memcpy(&aux[kAuxLSE2], w32 + kLSEFin2W, 96 * sizeof(float));
+    std::memcpy(&aux[kAuxLGGSW], w32 + kLGGSW, 24 * sizeof(float));
+    std::memcpy(&aux[kAuxLGGSB], w32 + kLGGSB, 8 * sizeof(float));
+    std::memcpy(&aux[kAuxLX12W], w32 + kLX12W, 16 * sizeof(float));
+    aux[kAuxLX12B] = w32[kLX12B];
     cudaError_t e;
+    if (!w.d_aux && (e = cudaMalloc(&w.d_aux, kAuxCount * sizeof(float))) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(w.d_aux, aux.data(), kAuxCount * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
     if (!w.d_bf16 && (e = cudaMalloc(&w.d_bf16, img16.size())) != cudaSuccess) return e;
     if (!w.d_fp8 && (e = cudaMalloc(&w.d_fp8, img8.size())) != cudaSuccess) return e;
     if (!w.d_scales && (e = cudaMalloc(&w.d_scales, kScaleCount * sizeof(float))) != cudaSuccess) return e;
@@ -178,7 +201,7 @@ struct LayerDesc {
     int b_off[2];   // byte offset of the weight image, [0] BF16, [1] E4M3
     int kp[2];      // padded K
     int n, np;      // logical / padded N
-    int b32;        // fp32 bias offset (packed weights)
+    int abias;      // bias offset in the shared-memory constants (kAuxBias + scale_off)
     int soff;       // FP8 scale offset
 };
 __constant__ LayerDesc c_layer_desc[kLayers];
@@ -191,7 +214,7 @@ static void fill_layer_descs(LayerDesc* d) {
         d[i].kp[1] = kpad(i, 1);
         d[i].n = layer_n(i);
         d[i].np = npad(i);
-        d[i].b32 = layer_b32(i);
+        d[i].abias = kAuxBias + scale_off(i);
         d[i].soff = scale_off(i);
     }
 }
@@ -316,12 +339,12 @@ MRP_D float sigmoid_d(float o) { return 1.0f / (1.0f + __expf(-o)); }
 
 // relu(D * scale + b) for N columns of layer L (runtime), in place.
 template <int EB, int N>
-MRP_D void bias_relu(float* d, int L, float rs, const float* __restrict__ w32, const float* __restrict__ scales) {
-    const int b32 = c_layer_desc[L].b32, so = c_layer_desc[L].soff;
+MRP_D void bias_relu(float* d, int L, float rs, const float* aux) {
+    const int ab = c_layer_desc[L].abias, so = c_layer_desc[L].soff;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-        float sc = EB == 1 ? rs * __ldg(scales + so + i) : 1.0f;
-        d[i] = fmaxf(fmaf(d[i], sc, wl(w32, b32 + i)), 0.0f);
+        float sc = EB == 1 ? rs * aux[kAuxScale + so + i] : 1.0f;
+        d[i] = fmaxf(fmaf(d[i], sc, aux[ab + i]), 0.0f);
     }
 }
 
@@ -395,8 +418,7 @@ MRP_D void tmem_put(const Group& G, int col, const float* v) {
 // l0..l0+2 on the tensor cores (D at dcol, dcol+stride, dcol+2*stride), then
 // prev <- relu(D + b) + slice (ADD3) or concat(relu(D + b), slice) (REP3).
 template <int EB, int W, class Src>
-__device__ __noinline__ int tc_block(const Group G, int st, const Src src, const float* __restrict__ w32,
-                                      const float* __restrict__ scales, int from, int widen, int has_prev, int l0,
+__device__ __noinline__ int tc_block(const Group G, int st, const Src src, const float* aux, int from, int widen, int has_prev, int l0,
                                       int dcol, int se_off, int pid, float g, float gamma, int pcol, int pstride) {
     constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
     constexpr int SUB = 128 * KP * EB;   // bytes of one branch's A sub-tile
@@ -422,11 +444,11 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
 #pragma unroll 4
         for (int o = 0; o < 16; ++o) {
             float a = hf[o];
-            const float* w1 = w32 + kLSEFin1W + o * 75 + pid;
+            const float* w1 = aux + kAuxLSE1 + o * 75 + pid;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                a = fmaf(__ldg(w1 + c), p8[c], a);
-                a = fmaf(__ldg(w1 + 36 + c), p8[3 + c], a);
+                a = fmaf(w1[c], p8[c], a);
+                a = fmaf(w1[36 + c], p8[3 + c], a);
             }
             hf[o] = a;
         }
@@ -437,14 +459,14 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
     for (int o = 0; o < 8; ++o) {
         float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], wl(w32, se_off + o * 8 + j), a);
+        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], aux[se_off + o * 8 + j], a);
         h[o] = fmaxf(a, 0.0f);
     }
 #pragma unroll
     for (int o = 0; o < 3; ++o) {
         float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a = fmaf(h[j], wl(w32, se_off + 64 + o * 8 + j), a);
+        for (int j = 0; j < 8; ++j) a = fmaf(h[j], aux[se_off + 64 + o * 8 + j], a);
         gate[o] = sigmoid_d(a);
     }
     float rs[3];
@@ -467,7 +489,7 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
     for (int c = 0; c < 3; ++c) {
         float d[W];
         read_cols<W>(G, dcol + c * DSTR, d);
-        bias_relu<EB, W>(d, l0 + c, rs[c], w32, scales);
+        bias_relu<EB, W>(d, l0 + c, rs[c], aux);
         if (widen) {
             float nv[2 * W];
 #pragma unroll
@@ -487,8 +509,7 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
 // a (16 values) kept in TMEM columns kColA16.
 constexpr int kColA16 = 96;
 template <int EB>
-__device__ __noinline__ int tc_residual_pair(const Group G, int st, const float* __restrict__ w32,
-                                             const float* __restrict__ scales, int k) {
+__device__ __noinline__ int tc_residual_pair(const Group G, int st, const float* aux, int k) {
     constexpr int KP = EB == 2 ? 16 : 32;
     const int La = kLX0 + 2 * k, Lb = La + 1;
     float a16[16];
@@ -497,12 +518,12 @@ __device__ __noinline__ int tc_residual_pair(const Group G, int st, const float*
     st = mma_round<EB>(G, st, 1, La, 0, 64, 0, 0, 0, 0, 0, 0);
     float u[16];
     read_cols<16>(G, 64, u);
-    bias_relu<EB, 16>(u, La, r0, w32, scales);
+    bias_relu<EB, 16>(u, La, r0, aux);
     float r1 = write_row<EB, 16, KP>(G.a, 0, G.t, u);
     st = mma_round<EB>(G, st, 1, Lb, 0, 80, 0, 0, 0, 0, 0, 0);
     float z[16];
     read_cols<16>(G, 80, z);
-    bias_relu<EB, 16>(z, Lb, r1, w32, scales);
+    bias_relu<EB, 16>(z, Lb, r1, aux);
 #pragma unroll
     for (int i = 0; i < 16; ++i) a16[i] += z[i];
     tmem_put<16>(G, kColA16, a16);
@@ -510,32 +531,103 @@ __device__ __noinline__ int tc_residual_pair(const Group G, int st, const float*
     return st;
 }
 
+// The tail of one albedo channel (core/radiancePredict.cu:375-419): LSEFin
+// gate, LC0 over [comb * gate, LGGS], LC1, LC2, LX, six residual pairs and
+// the 16 -> 1 head.  comb comes from TMEM (kColComb); the accumulators use
+// columns 0..127 only, so comb survives for the next channel.
+constexpr int kColComb = 136;
+struct Hf16 { float v[16]; };
+struct TailOut { float p; int st; };
+template <int EB>
+__device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux, Hf16 hf, float g, float gamma,
+                                        float s4) {
+    float h[16], gf[6];
+#pragma unroll
+    for (int o = 0; o < 16; ++o) {
+        float a = hf.v[o];
+        a = fmaf(aux[kAuxLSE1 + o * 75 + 72], g, a);
+        a = fmaf(aux[kAuxLSE1 + o * 75 + 73], gamma, a);
+        a = fmaf(aux[kAuxLSE1 + o * 75 + 74], s4, a);
+        h[o] = fmaxf(a, 0.0f);
+    }
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) a = fmaf(h[j], aux[kAuxLSE2 + o * 16 + j], a);
+        gf[o] = sigmoid_d(a);
+    }
+    // LC0's A row: [comb * gate segment, LGGS (3 -> 8)]
+    float x[128];
+    tmem_get<32>(G, kColComb, x);
+    tmem_get<32>(G, kColComb + 32, x + 32);
+    tmem_get<32>(G, kColComb + 64, x + 64);
+    tmem_get<8>(G, kColComb + 96, x + 96);
+    tmem_get<8>(G, kColComb + 104, x + 104);
+    tmem_get<8>(G, kColComb + 112, x + 112);
+#pragma unroll
+    for (int i = 0; i < 120; ++i) x[i] = x[i] * gf[i < 96 ? i / 32 : 3 + (i - 96) / 8];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        float a = 0.0f;
+        a = fmaf(g, aux[kAuxLGGSW + o * 3], a);
+        a = fmaf(gamma, aux[kAuxLGGSW + o * 3 + 1], a);
+        a = fmaf(s4, aux[kAuxLGGSW + o * 3 + 2], a);
+        x[120 + o] = fmaxf(a + aux[kAuxLGGSB + o], 0.0f);
+    }
+    float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLC0, 0, 0, 0, 0, 0, 0, 0, 0);
+    read_cols<128>(G, 0, x);
+    bias_relu<EB, 128>(x, kLC0, r, aux);
+    r = write_row<EB, 128, kpad(kLC1, EB)>(G.a, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLC1, 0, 0, 0, 0, 0, 0, 0, 0);
+    read_cols<64>(G, 0, x);
+    bias_relu<EB, 64>(x, kLC1, r, aux);
+    r = write_row<EB, 64, kpad(kLC2, EB)>(G.a, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLC2, 0, 0, 0, 0, 0, 0, 0, 0);
+    read_cols<32>(G, 0, x);
+    bias_relu<EB, 32>(x, kLC2, r, aux);
+    r = write_row<EB, 32, kpad(kLX, EB)>(G.a, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLX, 0, 32, 0, 0, 0, 0, 0, 0);
+    float a16[16];
+    read_cols<16>(G, 32, a16);
+    bias_relu<EB, 16>(a16, kLX, r, aux);
+    tmem_put<16>(G, kColA16, a16);
+    tc::tmem_wait_st();
+#pragma unroll 1
+    for (int k = 0; k < 6; ++k) st = tc_residual_pair<EB>(G, st, aux, k);
+    tmem_get<16>(G, kColA16, a16);
+    float a = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) a = fmaf(a16[j], aux[kAuxLX12W + j], a);
+    return TailOut{fmaxf(a + aux[kAuxLX12B], 0.0f), st};
+}
+
 struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid, pcol, pstride; };
 __constant__ BlockDesc c_blocks[12] = {
-    {8, 0, 0, 0, 0, 0, mblk_off(0), 0, kColPrevMain, 32},      {8, 8, 1, 1, 3, 0, mblk_off(1), 3, kColPrevMain, 32},
-    {16, 16, 0, 1, 6, 0, mblk_off(2), 6, kColPrevMain, 32},    {16, 32, 0, 1, 9, 0, mblk_off(3), 9, kColPrevMain, 32},
-    {16, 48, 1, 1, 12, 0, mblk_off(4), 12, kColPrevMain, 32},  {32, 64, 0, 1, 15, 0, mblk_off(5), 15, kColPrevMain, 32},
-    {32, 96, 0, 1, 18, 0, mblk_off(6), 18, kColPrevMain, 32},  {32, 128, 0, 1, 21, 0, mblk_off(7), 21, kColPrevMain, 32},
-    {8, 160, 0, 0, 27, 128, di_block_off(0), 24, kColPrevDi, 8}, {8, 168, 0, 1, 30, 128, di_block_off(1), 27, kColPrevDi, 8},
-    {8, 176, 0, 1, 33, 128, di_block_off(2), 30, kColPrevDi, 8}, {8, 184, 0, 1, 36, 128, di_block_off(3), 33, kColPrevDi, 8},
+    {8, 0, 0, 0, 0, 0, kAuxSE + 88 * 0, 0, kColPrevMain, 32},      {8, 8, 1, 1, 3, 0, kAuxSE + 88 * 1, 3, kColPrevMain, 32},
+    {16, 16, 0, 1, 6, 0, kAuxSE + 88 * 2, 6, kColPrevMain, 32},    {16, 32, 0, 1, 9, 0, kAuxSE + 88 * 3, 9, kColPrevMain, 32},
+    {16, 48, 1, 1, 12, 0, kAuxSE + 88 * 4, 12, kColPrevMain, 32},  {32, 64, 0, 1, 15, 0, kAuxSE + 88 * 5, 15, kColPrevMain, 32},
+    {32, 96, 0, 1, 18, 0, kAuxSE + 88 * 6, 18, kColPrevMain, 32},  {32, 128, 0, 1, 21, 0, kAuxSE + 88 * 7, 21, kColPrevMain, 32},
+    {8, 160, 0, 0, 27, 128, kAuxSE + 88 * 8, 24, kColPrevDi, 8}, {8, 168, 0, 1, 30, 128, kAuxSE + 88 * 9, 27, kColPrevDi, 8},
+    {8, 176, 0, 1, 33, 128, kAuxSE + 88 * 10, 30, kColPrevDi, 8}, {8, 184, 0, 1, 36, 128, kAuxSE + 88 * 11, 33, kColPrevDi, 8},
 };
 
 template <int EB, class Src>
-MRP_D int run_block(const Group& G, int st, const Src& src, const float* __restrict__ w32,
-                    const float* __restrict__ scales, int b, float g, float gamma) {
+MRP_D int run_block(const Group& G, int st, const Src& src, const float* aux, int b, float g, float gamma) {
     const BlockDesc d = c_blocks[b];
     if (d.w == 8)
-        return tc_block<EB, 8>(G, st, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+        return tc_block<EB, 8>(G, st, src, aux, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
                         d.pcol, d.pstride);
     else if (d.w == 16)
-        return tc_block<EB, 16>(G, st, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+        return tc_block<EB, 16>(G, st, src, aux, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
                          d.pcol, d.pstride);
-    return tc_block<EB, 32>(G, st, src, w32, scales, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
+    return tc_block<EB, 32>(G, st, src, aux, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
                          d.pcol, d.pstride);
 }
 
 template <int EB, class Src>
-MRP_D int tc_network(const Group& G, int st, const Src& src, const float* __restrict__ w32, const float* __restrict__ scales,
+MRP_D int tc_network(const Group& G, int st, const Src& src, const float* aux,
                       float gamma, float g, f3 sr, float out[3]) {
     {
         float z[16];
@@ -546,7 +638,7 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* __rest
     }
     // main branch, X[0:160]; the three 32x32 finals leave comb[0:96) in TMEM columns 0..95
 #pragma unroll 1
-    for (int b = 0; b < 8; ++b) st = run_block<EB>(G, st, src, w32, scales, b, g, gamma);
+    for (int b = 0; b < 8; ++b) st = run_block<EB>(G, st, src, aux, b, g, gamma);
     float rs_main[3];
     {
         constexpr int KP = pad_to(32, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
@@ -560,7 +652,7 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* __rest
     }
     // direct-illumination branch, X[160:192]; the 8x8 finals at columns 176..223
 #pragma unroll 1
-    for (int b = 8; b < 12; ++b) st = run_block<EB>(G, st, src, w32, scales, b, g, gamma);
+    for (int b = 8; b < 12; ++b) st = run_block<EB>(G, st, src, aux, b, g, gamma);
     float rs_di[3];
     {
         constexpr int KP = pad_to(8, EB == 2 ? 16 : 32), SUB = 128 * KP * EB;
@@ -574,80 +666,37 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* __rest
     }
     float hf[16];
     tmem_get<16>(G, kColHf, hf);   // before LC0's accumulator covers columns 0..127
-    // comb[120] = relu(finals + b): main (3 x 32) then direct illumination (3 x 8)
-    float comb[120];
+    // comb[120] = relu(finals + b) -> TMEM columns kColComb..+119: the DI
+    // finals (176..223) first, then the main ones (0..95) -- the main comb
+    // lands on 136..231, over DI columns already read.
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        read_cols<32>(G, 32 * c, comb + 32 * c);
-        bias_relu<EB, 32>(comb + 32 * c, kL81 + c, rs_main[c], w32, scales);
-        float e[16];
-        tc::tmem_ld16(G.tmem + 176 + 16 * c, e);
-        bias_relu<EB, 8>(e, kLD41 + c, rs_di[c], w32, scales);
-#pragma unroll
-        for (int o = 0; o < 8; ++o) comb[96 + 8 * c + o] = e[o];
+        float e[8];
+        read_cols<8>(G, 176 + 16 * c, e);
+        bias_relu<EB, 8>(e, kLD41 + c, rs_di[c], aux);
+        tmem_put<8>(G, kColComb + 96 + 8 * c, e);
     }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float m[32];
+        read_cols<32>(G, 32 * c, m);
+        bias_relu<EB, 32>(m, kL81 + c, rs_main[c], aux);
+        tmem_put<32>(G, kColComb + 32 * c, m);
+    }
+    tc::tmem_wait_st();
     // tail, once per distinct albedo channel (core/radiancePredict.cu:375-419)
     float srv[3] = {sr.x, sr.y, sr.z}, P[3];
+    Hf16 hv;
+#pragma unroll
+    for (int o = 0; o < 16; ++o) hv.v[o] = hf[o];
 #pragma unroll 1
     for (int ch = 0; ch < 3; ++ch) {
         if (ch == 1 && srv[1] == srv[0]) { P[1] = P[0]; continue; }
         if (ch == 2 && srv[2] == srv[0]) { P[2] = P[0]; continue; }
         if (ch == 2 && srv[2] == srv[1]) { P[2] = P[1]; continue; }
-        float s4 = powf(srv[ch], 4.0f);
-        float h[16], gf[6];
-#pragma unroll
-        for (int o = 0; o < 16; ++o) {
-            float a = hf[o];
-            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 72), g, a);
-            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 73), gamma, a);
-            a = fmaf(wl(w32, kLSEFin1W + o * 75 + 74), s4, a);
-            h[o] = fmaxf(a, 0.0f);
-        }
-#pragma unroll
-        for (int o = 0; o < 6; ++o) {
-            float a = 0.0f;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) a = fmaf(h[j], wl(w32, kLSEFin2W + o * 16 + j), a);
-            gf[o] = sigmoid_d(a);
-        }
-        // LC0's A row: [comb * gate segment, LGGS (3 -> 8)]
-        float x[128];
-#pragma unroll
-        for (int i = 0; i < 120; ++i) x[i] = comb[i] * gf[i < 96 ? i / 32 : 3 + (i - 96) / 8];
-#pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            float a = 0.0f;
-            a = fmaf(g, wl(w32, kLGGSW + o * 3), a);
-            a = fmaf(gamma, wl(w32, kLGGSW + o * 3 + 1), a);
-            a = fmaf(s4, wl(w32, kLGGSW + o * 3 + 2), a);
-            x[120 + o] = fmaxf(a + wl(w32, kLGGSB + o), 0.0f);
-        }
-        float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, x);
-        st = mma_round<EB>(G, st, 1, kLC0, 0, 0, 0, 0, 0, 0, 0, 0);
-        read_cols<128>(G, 0, x);
-        bias_relu<EB, 128>(x, kLC0, r, w32, scales);
-        r = write_row<EB, 128, kpad(kLC1, EB)>(G.a, 0, G.t, x);
-        st = mma_round<EB>(G, st, 1, kLC1, 0, 128, 0, 0, 0, 0, 0, 0);
-        read_cols<64>(G, 128, x);
-        bias_relu<EB, 64>(x, kLC1, r, w32, scales);
-        r = write_row<EB, 64, kpad(kLC2, EB)>(G.a, 0, G.t, x);
-        st = mma_round<EB>(G, st, 1, kLC2, 0, 0, 0, 0, 0, 0, 0, 0);
-        read_cols<32>(G, 0, x);
-        bias_relu<EB, 32>(x, kLC2, r, w32, scales);
-        r = write_row<EB, 32, kpad(kLX, EB)>(G.a, 0, G.t, x);
-        st = mma_round<EB>(G, st, 1, kLX, 0, 32, 0, 0, 0, 0, 0, 0);
-        float a16[16];
-        read_cols<16>(G, 32, a16);
-        bias_relu<EB, 16>(a16, kLX, r, w32, scales);
-        tmem_put<16>(G, kColA16, a16);
-        tc::tmem_wait_st();
-#pragma unroll 1
-        for (int k = 0; k < 6; ++k) st = tc_residual_pair<EB>(G, st, w32, scales, k);
-        tmem_get<16>(G, kColA16, a16);
-        float a = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) a = fmaf(a16[j], wl(w32, kLX12W + j), a);
-        P[ch] = fmaxf(a + wl(w32, kLX12B), 0.0f);
+        TailOut t = tc_tail<EB>(G, st, aux, hv, g, gamma, powf(srv[ch], 4.0f));
+        st = t.st;
+        P[ch] = t.p;
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c] = fmaxf(expf(P[c]) - 1.0f, 0.0f) * powf(srv[c], 4.0f);
@@ -660,8 +709,7 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* __rest
 struct TcArgs {
     const uint8_t* wimg;        // operand image (global)
     int wimg_bytes;
-    const float* w32;           // fp32 packed weights
-    const float* scales;        // FP8 per-layer weight scales
+    const float* aux;           // fp32 constants of the CUDA-core parts (kAux* layout)
     int* err;
     int* tile_counter;
     // inputs: either row-major features [n][576] + gamma, or staged records
@@ -687,6 +735,7 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kGroups);
     int* tile_slot = reinterpret_cast<int*>(tslot + 1);
     int* seg_start = tile_slot + kGroups;   // staged: first tile of each segment, [nseg + 1]
+    float* aux_s = reinterpret_cast<float*>(seg_start + kTcMaxSegments + 1 + 3);   // 16-byte aligned below
     const TcSegment* segs = A.segs ? A.segs : &A.seg0;
     const int nseg = A.segs ? A.nseg : 1;
 
@@ -694,6 +743,9 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
     // weights -> shared memory
     for (int i = tid * 16; i < A.wimg_bytes; i += blockDim.x * 16)
         *reinterpret_cast<uint4*>(wimg + i) = __ldg(reinterpret_cast<const uint4*>(A.wimg + i));
+    aux_s = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(aux_s) + 15) & ~(uintptr_t)15);
+    for (int i = tid * 4; i < kAuxCount; i += blockDim.x * 4)
+        *reinterpret_cast<float4*>(aux_s + i) = __ldg(reinterpret_cast<const float4*>(A.aux + i));
     if (warp == 0) {
         tc::tmem_alloc(tslot, kGroups * kTmemColsPerGroup);
         tc::tmem_relinquish();
@@ -741,7 +793,7 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
             const size_t cap = S->rec_cap;
             float gamma = valid ? S->rec_f[15 * cap + r] : 0.0f;
             TileFeatures src{S->feat + (size_t)(r >> 5) * 576 * 32 + (r & 31), valid};
-            st = tc_network<EB>(G, st, src, A.w32, A.scales, gamma, S->g, S->sr, o);
+            st = tc_network<EB>(G, st, src, aux_s, gamma, S->g, S->sr, o);
             if (valid && !(st & kStFailed)) {
                 int pix = S->rec_pix[r];
                 f3 hit = mk3(S->rec_f[r], S->rec_f[cap + r], S->rec_f[2 * cap + r]);
@@ -759,7 +811,7 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
             const bool valid = r < A.n;
             float gamma = valid ? A.gamma[r] : 0.0f;
             RowFeatures src{A.feat + (size_t)r * 576, valid};
-            st = tc_network<EB>(G, st, src, A.w32, A.scales, gamma, A.g, A.sr, o);
+            st = tc_network<EB>(G, st, src, aux_s, gamma, A.g, A.sr, o);
             if (valid && !(st & kStFailed)) {
                 A.out3[3 * (size_t)r] = o[0];
                 A.out3[3 * (size_t)r + 1] = o[1];
@@ -777,7 +829,7 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
 
 static size_t tc_smem_bytes(int eb) {
     return (size_t)((image_bytes(eb) + 1023) & ~1023) + kGroups * kABytes + kGroups * 8 + 16 +
-           (kTcMaxSegments + 1) * sizeof(int);
+           (kTcMaxSegments + 1 + 3) * sizeof(int) + 16 + kAuxCount * sizeof(float);
 }
 
 template <int EB, bool STAGED>
@@ -794,8 +846,7 @@ static TcArgs base_args(const TcWeights& w, bool fp8) {
     TcArgs a{};
     a.wimg = (const uint8_t*)(fp8 ? w.d_fp8 : w.d_bf16);
     a.wimg_bytes = image_bytes(fp8 ? 1 : 2);
-    a.w32 = w.d_fp32;
-    a.scales = w.d_scales;
+    a.aux = w.d_aux;
     a.err = w.d_err;
     a.tile_counter = w.d_counter;
     return a;

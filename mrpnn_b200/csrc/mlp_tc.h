@@ -11,6 +11,7 @@ struct TcWeights {
     void* d_fp8 = nullptr;     // FP8-E4M3 operand images (weights / per-layer scale)
     float* d_scales = nullptr; // FP8 weight scales per output channel (row amax / 448)
     const float* d_fp32 = nullptr;   // packed fp32 weights: gates, biases, LSEFin, LX12
+    float* d_aux = nullptr;    // fp32 constants of the CUDA-core parts, staged into shared memory
     int* d_err = nullptr;      // set to 1 when an MMA round times out
     int* d_counter = nullptr;  // tile counter of the persistent kernel
     bool ready = false;
