@@ -235,11 +235,10 @@ __device__ __forceinline__ void group_bar(int g) {
 // (bit 1) -- travels as an int through the calls.
 struct Group {
     int g, t;             // group index, thread within the group
-    uint8_t* a;           // A buffer (shared)
-    const uint8_t* wimg;  // weight image (shared)
-    uint64_t* mbar;
+    uint32_t a_s;         // A buffer (shared address)
+    uint32_t wimg_s;      // weight image (shared address)
+    uint32_t mbar_s;      // the group's mbarrier (shared address)
     uint32_t tmem;        // TMEM address of this thread's lane, column 0 of the group
-    uint32_t tmem_col0;   // TMEM address of lane 0, column 0 of the group (MMA D base)
     int* err;
 };
 constexpr int kStFailed = 2;
@@ -247,36 +246,34 @@ constexpr int kStFailed = 2;
 // Up to three MMAs (layer, A sub-tile byte offset, D column), issued after
 // all A rows are in shared memory and awaited by the whole group.
 template <int EB>
-__device__ __noinline__ int mma_round(const Group G, int st, int count, int l0, int a0, int d0, int l1, int a1, int d1, int l2,
-                                       int a2, int d2) {
+__device__ __noinline__ int mma_round(const Group G, int st, int count, int l0, int a_stride, int d0, int d_stride) {
     tc::fence_proxy_async();
     tc::fence_before_sync();
     group_bar(G.g);
     if (G.t == 0) {
         tc::fence_after_sync();
-        uint32_t abase = tc::smem_addr(G.a), wbase = tc::smem_addr(G.wimg);
+        const uint32_t col0 = G.tmem & 0xFFFFu;   // lane 0, the group's column 0
         const int e = EB == 2 ? 0 : 1;
 #pragma unroll 1
         for (int q = 0; q < count; ++q) {
-            int L = q == 0 ? l0 : (q == 1 ? l1 : l2);
-            int ao = q == 0 ? a0 : (q == 1 ? a1 : a2);
-            int dc = q == 0 ? d0 : (q == 1 ? d1 : d2);
+            const int L = l0 + q;
             int kp = c_layer_desc[L].kp[e];
             uint32_t idesc = tc::instr_desc(128, c_layer_desc[L].np, EB == 2 ? tc::kFmtBF16 : tc::kFmtE4M3);
             uint32_t sbo = (uint32_t)(kp * EB * 8);
             int steps = kp * EB / 32;   // 32 bytes of K per MMA (16 BF16 / 32 E4M3)
-            uint32_t bb = wbase + (uint32_t)c_layer_desc[L].b_off[e];
+            uint32_t ab = G.a_s + (uint32_t)(q * a_stride), bb = G.wimg_s + (uint32_t)c_layer_desc[L].b_off[e];
+            uint32_t dc = col0 + (uint32_t)(d0 + q * d_stride);
 #pragma unroll 1
             for (int s = 0; s < steps; ++s) {
-                uint64_t ad = tc::smem_desc(abase + ao + s * 256, 128, sbo);
+                uint64_t ad = tc::smem_desc(ab + s * 256, 128, sbo);
                 uint64_t bd = tc::smem_desc(bb + s * 256, 128, sbo);
-                if (EB == 2) tc::mma_bf16(G.tmem_col0 + dc, ad, bd, idesc, s > 0);
-                else tc::mma_fp8(G.tmem_col0 + dc, ad, bd, idesc, s > 0);
+                if (EB == 2) tc::mma_bf16(dc, ad, bd, idesc, s > 0);
+                else tc::mma_fp8(dc, ad, bd, idesc, s > 0);
             }
         }
-        tc::mma_commit(G.mbar);
+        tc::mma_commit_s(G.mbar_s);
     }
-    bool done = tc::mbar_wait(G.mbar, (uint32_t)(st & 1), kWaitLimit);
+    bool done = tc::mbar_wait_s(G.mbar_s, (uint32_t)(st & 1), kWaitLimit);
     st ^= 1;
     if (!done) {
         st |= kStFailed;
@@ -290,7 +287,7 @@ __device__ __noinline__ int mma_round(const Group G, int st, int count, int l0, 
 // sub-tile byte offset `off`.  FP8 rows are scaled by 1/s (s = row amax/448),
 // returned so the epilogue can undo it.
 template <int EB, int N, int KP>
-__device__ __forceinline__ float write_row(uint8_t* a, int off, int row, const float* v) {
+__device__ __forceinline__ float write_row(uint32_t a_s, int off, int row, const float* v) {
     float inv = 1.0f, s = 1.0f;
     if (EB == 1) {
         float amax = 0.0f;
@@ -316,7 +313,7 @@ __device__ __forceinline__ float write_row(uint8_t* a, int off, int row, const f
                 w[q] = (uint32_t)tc::pack_e4m3(x0, x1) | ((uint32_t)tc::pack_e4m3(x2, x3) << 16);
             }
         }
-        *reinterpret_cast<uint4*>(a + off + op_off(row, c * E, KP, EB)) = make_uint4(w[0], w[1], w[2], w[3]);
+        tc::st_shared_v4(a_s + (uint32_t)(off + op_off(row, c * E, KP, EB)), w[0], w[1], w[2], w[3]);
     }
     return s;
 }
@@ -413,13 +410,26 @@ MRP_D void tmem_put(const Group& G, int col, const float* v) {
     }
 }
 
+struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid, pcol, pstride; };
+__constant__ BlockDesc c_blocks[12] = {
+    {8, 0, 0, 0, 0, 0, kAuxSE + 88 * 0, 0, kColPrevMain, 32},      {8, 8, 1, 1, 3, 0, kAuxSE + 88 * 1, 3, kColPrevMain, 32},
+    {16, 16, 0, 1, 6, 0, kAuxSE + 88 * 2, 6, kColPrevMain, 32},    {16, 32, 0, 1, 9, 0, kAuxSE + 88 * 3, 9, kColPrevMain, 32},
+    {16, 48, 1, 1, 12, 0, kAuxSE + 88 * 4, 12, kColPrevMain, 32},  {32, 64, 0, 1, 15, 0, kAuxSE + 88 * 5, 15, kColPrevMain, 32},
+    {32, 96, 0, 1, 18, 0, kAuxSE + 88 * 6, 18, kColPrevMain, 32},  {32, 128, 0, 1, 21, 0, kAuxSE + 88 * 7, 21, kColPrevMain, 32},
+    {8, 160, 0, 0, 27, 128, kAuxSE + 88 * 8, 24, kColPrevDi, 8}, {8, 168, 0, 1, 30, 128, kAuxSE + 88 * 9, 27, kColPrevDi, 8},
+    {8, 176, 0, 1, 33, 128, kAuxSE + 88 * 10, 30, kColPrevDi, 8}, {8, 184, 0, 1, 36, 128, kAuxSE + 88 * 11, 33, kColPrevDi, 8},
+};
+
 // One SE block over the three channels (SE / SERES + ADD3 / REP3,
 // core/radiancePredict.cu:240-294): gate from the slice pools, branch layers
 // l0..l0+2 on the tensor cores (D at dcol, dcol+stride, dcol+2*stride), then
 // prev <- relu(D + b) + slice (ADD3) or concat(relu(D + b), slice) (REP3).
 template <int EB, int W, class Src>
-__device__ __noinline__ int tc_block(const Group G, int st, const Src src, const float* aux, int from, int widen, int has_prev, int l0,
-                                      int dcol, int se_off, int pid, float g, float gamma, int pcol, int pstride) {
+__device__ __noinline__ int tc_block(const Group G, int st, const Src src, const float* aux, int b, float g,
+                                     float gamma) {
+    const BlockDesc bd = c_blocks[b];
+    const int from = bd.from, widen = bd.widen, has_prev = bd.has_prev, l0 = bd.l0, dcol = bd.dcol,
+              se_off = bd.se_off, pid = bd.pid, pcol = bd.pcol, pstride = bd.pstride;
     constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
     constexpr int SUB = 128 * KP * EB;   // bytes of one branch's A sub-tile
     constexpr int DSTR = W <= 16 ? 16 : 32;
@@ -482,9 +492,9 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
 #pragma unroll
             for (int i = 0; i < W; ++i) in[i] = xs[c][i] * gate[c];
         }
-        rs[c] = write_row<EB, W, KP>(G.a, c * SUB, G.t, in);
+        rs[c] = write_row<EB, W, KP>(G.a_s, c * SUB, G.t, in);
     }
-    st = mma_round<EB>(G, st, 3, l0, 0, dcol, l0 + 1, SUB, dcol + DSTR, l0 + 2, 2 * SUB, dcol + 2 * DSTR);
+    st = mma_round<EB>(G, st, 3, l0, SUB, dcol, DSTR);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float d[W];
@@ -514,13 +524,13 @@ __device__ __noinline__ int tc_residual_pair(const Group G, int st, const float*
     const int La = kLX0 + 2 * k, Lb = La + 1;
     float a16[16];
     tmem_get<16>(G, kColA16, a16);
-    float r0 = write_row<EB, 16, KP>(G.a, 0, G.t, a16);
-    st = mma_round<EB>(G, st, 1, La, 0, 64, 0, 0, 0, 0, 0, 0);
+    float r0 = write_row<EB, 16, KP>(G.a_s, 0, G.t, a16);
+    st = mma_round<EB>(G, st, 1, La, 0, 64, 0);
     float u[16];
     read_cols<16>(G, 64, u);
     bias_relu<EB, 16>(u, La, r0, aux);
-    float r1 = write_row<EB, 16, KP>(G.a, 0, G.t, u);
-    st = mma_round<EB>(G, st, 1, Lb, 0, 80, 0, 0, 0, 0, 0, 0);
+    float r1 = write_row<EB, 16, KP>(G.a_s, 0, G.t, u);
+    st = mma_round<EB>(G, st, 1, Lb, 0, 80, 0);
     float z[16];
     read_cols<16>(G, 80, z);
     bias_relu<EB, 16>(z, Lb, r1, aux);
@@ -536,15 +546,15 @@ __device__ __noinline__ int tc_residual_pair(const Group G, int st, const float*
 // the 16 -> 1 head.  comb comes from TMEM (kColComb); the accumulators use
 // columns 0..127 only, so comb survives for the next channel.
 constexpr int kColComb = 136;
-struct Hf16 { float v[16]; };
 struct TailOut { float p; int st; };
+// hf (the LSEFin1 partial sums) is read from TMEM columns kColHf first thing.
 template <int EB>
-__device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux, Hf16 hf, float g, float gamma,
-                                        float s4) {
+__device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux, float g, float gamma, float s4) {
     float h[16], gf[6];
+    tmem_get<16>(G, kColHf, h);
 #pragma unroll
     for (int o = 0; o < 16; ++o) {
-        float a = hf.v[o];
+        float a = h[o];
         a = fmaf(aux[kAuxLSE1 + o * 75 + 72], g, a);
         a = fmaf(aux[kAuxLSE1 + o * 75 + 73], gamma, a);
         a = fmaf(aux[kAuxLSE1 + o * 75 + 74], s4, a);
@@ -575,20 +585,20 @@ __device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux,
         a = fmaf(s4, aux[kAuxLGGSW + o * 3 + 2], a);
         x[120 + o] = fmaxf(a + aux[kAuxLGGSB + o], 0.0f);
     }
-    float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a, 0, G.t, x);
-    st = mma_round<EB>(G, st, 1, kLC0, 0, 0, 0, 0, 0, 0, 0, 0);
+    float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a_s, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLC0, 0, 0, 0);
     read_cols<128>(G, 0, x);
     bias_relu<EB, 128>(x, kLC0, r, aux);
-    r = write_row<EB, 128, kpad(kLC1, EB)>(G.a, 0, G.t, x);
-    st = mma_round<EB>(G, st, 1, kLC1, 0, 0, 0, 0, 0, 0, 0, 0);
+    r = write_row<EB, 128, kpad(kLC1, EB)>(G.a_s, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLC1, 0, 0, 0);
     read_cols<64>(G, 0, x);
     bias_relu<EB, 64>(x, kLC1, r, aux);
-    r = write_row<EB, 64, kpad(kLC2, EB)>(G.a, 0, G.t, x);
-    st = mma_round<EB>(G, st, 1, kLC2, 0, 0, 0, 0, 0, 0, 0, 0);
+    r = write_row<EB, 64, kpad(kLC2, EB)>(G.a_s, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLC2, 0, 0, 0);
     read_cols<32>(G, 0, x);
     bias_relu<EB, 32>(x, kLC2, r, aux);
-    r = write_row<EB, 32, kpad(kLX, EB)>(G.a, 0, G.t, x);
-    st = mma_round<EB>(G, st, 1, kLX, 0, 32, 0, 0, 0, 0, 0, 0);
+    r = write_row<EB, 32, kpad(kLX, EB)>(G.a_s, 0, G.t, x);
+    st = mma_round<EB>(G, st, 1, kLX, 0, 32, 0);
     float a16[16];
     read_cols<16>(G, 32, a16);
     bias_relu<EB, 16>(a16, kLX, r, aux);
@@ -603,27 +613,13 @@ __device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux,
     return TailOut{fmaxf(a + aux[kAuxLX12B], 0.0f), st};
 }
 
-struct BlockDesc { int w, from, widen, has_prev, l0, dcol, se_off, pid, pcol, pstride; };
-__constant__ BlockDesc c_blocks[12] = {
-    {8, 0, 0, 0, 0, 0, kAuxSE + 88 * 0, 0, kColPrevMain, 32},      {8, 8, 1, 1, 3, 0, kAuxSE + 88 * 1, 3, kColPrevMain, 32},
-    {16, 16, 0, 1, 6, 0, kAuxSE + 88 * 2, 6, kColPrevMain, 32},    {16, 32, 0, 1, 9, 0, kAuxSE + 88 * 3, 9, kColPrevMain, 32},
-    {16, 48, 1, 1, 12, 0, kAuxSE + 88 * 4, 12, kColPrevMain, 32},  {32, 64, 0, 1, 15, 0, kAuxSE + 88 * 5, 15, kColPrevMain, 32},
-    {32, 96, 0, 1, 18, 0, kAuxSE + 88 * 6, 18, kColPrevMain, 32},  {32, 128, 0, 1, 21, 0, kAuxSE + 88 * 7, 21, kColPrevMain, 32},
-    {8, 160, 0, 0, 27, 128, kAuxSE + 88 * 8, 24, kColPrevDi, 8}, {8, 168, 0, 1, 30, 128, kAuxSE + 88 * 9, 27, kColPrevDi, 8},
-    {8, 176, 0, 1, 33, 128, kAuxSE + 88 * 10, 30, kColPrevDi, 8}, {8, 184, 0, 1, 36, 128, kAuxSE + 88 * 11, 33, kColPrevDi, 8},
-};
 
 template <int EB, class Src>
 MRP_D int run_block(const Group& G, int st, const Src& src, const float* aux, int b, float g, float gamma) {
-    const BlockDesc d = c_blocks[b];
-    if (d.w == 8)
-        return tc_block<EB, 8>(G, st, src, aux, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
-                        d.pcol, d.pstride);
-    else if (d.w == 16)
-        return tc_block<EB, 16>(G, st, src, aux, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
-                         d.pcol, d.pstride);
-    return tc_block<EB, 32>(G, st, src, aux, d.from, d.widen, d.has_prev, d.l0, d.dcol, d.se_off, d.pid, g, gamma,
-                         d.pcol, d.pstride);
+    const int w = c_blocks[b].w;
+    if (w == 8) return tc_block<EB, 8>(G, st, src, aux, b, g, gamma);
+    if (w == 16) return tc_block<EB, 16>(G, st, src, aux, b, g, gamma);
+    return tc_block<EB, 32>(G, st, src, aux, b, g, gamma);
 }
 
 template <int EB, class Src>
@@ -646,9 +642,9 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* aux,
         for (int c = 0; c < 3; ++c) {
             float pv[32];
             tmem_get<32>(G, kColPrevMain + 32 * c, pv);
-            rs_main[c] = write_row<EB, 32, KP>(G.a, c * SUB, G.t, pv);
+            rs_main[c] = write_row<EB, 32, KP>(G.a_s, c * SUB, G.t, pv);
         }
-        st = mma_round<EB>(G, st, 3, kL81, 0, 0, kL81 + 1, SUB, 32, kL81 + 2, 2 * SUB, 64);
+        st = mma_round<EB>(G, st, 3, kL81, SUB, 0, 32);
     }
     // direct-illumination branch, X[160:192]; the 8x8 finals at columns 176..223
 #pragma unroll 1
@@ -660,9 +656,9 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* aux,
         for (int c = 0; c < 3; ++c) {
             float pv[8];
             tmem_get<8>(G, kColPrevDi + 8 * c, pv);
-            rs_di[c] = write_row<EB, 8, KP>(G.a, c * SUB, G.t, pv);
+            rs_di[c] = write_row<EB, 8, KP>(G.a_s, c * SUB, G.t, pv);
         }
-        st = mma_round<EB>(G, st, 3, kLD41, 0, 176, kLD41 + 1, SUB, 192, kLD41 + 2, 2 * SUB, 208);
+        st = mma_round<EB>(G, st, 3, kLD41, SUB, 176, 16);
     }
     float hf[16];
     tmem_get<16>(G, kColHf, hf);   // before LC0's accumulator covers columns 0..127
@@ -686,15 +682,16 @@ MRP_D int tc_network(const Group& G, int st, const Src& src, const float* aux,
     tc::tmem_wait_st();
     // tail, once per distinct albedo channel (core/radiancePredict.cu:375-419)
     float srv[3] = {sr.x, sr.y, sr.z}, P[3];
-    Hf16 hv;
 #pragma unroll
-    for (int o = 0; o < 16; ++o) hv.v[o] = hf[o];
-#pragma unroll 1
     for (int ch = 0; ch < 3; ++ch) {
         if (ch == 1 && srv[1] == srv[0]) { P[1] = P[0]; continue; }
         if (ch == 2 && srv[2] == srv[0]) { P[2] = P[0]; continue; }
         if (ch == 2 && srv[2] == srv[1]) { P[2] = P[1]; continue; }
-        TailOut t = tc_tail<EB>(G, st, aux, hv, g, gamma, powf(srv[ch], 4.0f));
+        if (ch > 0) {   // the previous tail's accumulators covered kColHf
+            tmem_put<16>(G, kColHf, hf);
+            tc::tmem_wait_st();
+        }
+        TailOut t = tc_tail<EB>(G, st, aux, g, gamma, powf(srv[ch], 4.0f));
         st = t.st;
         P[ch] = t.p;
     }
@@ -768,11 +765,10 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
     Group G;
     G.g = tid / kGroupThreads;
     G.t = tid % kGroupThreads;
-    G.a = abuf + G.g * kABytes;
-    G.wimg = wimg;
-    G.mbar = mbar + G.g;
-    G.tmem_col0 = tbase + (uint32_t)(G.g * kTmemColsPerGroup);
-    G.tmem = G.tmem_col0 + ((uint32_t)(32 * ((tid / 32) % 4)) << 16);
+    G.a_s = tc::smem_addr(abuf + G.g * kABytes);
+    G.wimg_s = tc::smem_addr(wimg);
+    G.mbar_s = tc::smem_addr(mbar + G.g);
+    G.tmem = tbase + (uint32_t)(G.g * kTmemColsPerGroup) + ((uint32_t)(32 * ((tid / 32) % 4)) << 16);
     G.err = A.err;
     int st = 0;
 
