@@ -193,6 +193,41 @@ MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
     float c11 = lerp_w(t110, t111, wz, oz);
     return lerp_w(lerp_w(c00, c01, wy, oy), lerp_w(c10, c11, wy, oy), wx, ox);
 }
+// Contracted forms for the stencil gather, whose outputs are features (held
+// to 1e-5 relative, not bit for bit): fused multiply-adds in the coordinate
+// and lerp arithmetic.  The march keeps the exact forms above -- its
+// accept / stop decisions must match the reference's float order.
+MRP_D float lerp_fast(float a, float b, float v) { return fmaf(v, b - a, a); }
+template <bool Clamp>
+MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
+    float nf = (float)n;
+    float px = fmaf(pos.x + 0.5f, nf, -0.5f), py = fmaf(pos.y + 0.5f, nf, -0.5f), pz = fmaf(pos.z + 0.5f, nf, -0.5f);
+    float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
+    int x = (int)flx, y = (int)fly, z = (int)flz;
+    float wx = px - flx, wy = py - fly, wz = pz - flz;
+    int x0 = min(max(x, 0), n - 1), x1 = min(max(x + 1, 0), n - 1);
+    int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
+    int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
+    const float* p0 = g + (size_t)x0 * n * n;
+    const float* p1 = g + (size_t)x1 * n * n;
+    float t000 = __ldg(p0 + y0 + z0), t001 = __ldg(p0 + y0 + z1), t010 = __ldg(p0 + y1 + z0), t011 = __ldg(p0 + y1 + z1);
+    float t100 = __ldg(p1 + y0 + z0), t101 = __ldg(p1 + y0 + z1), t110 = __ldg(p1 + y1 + z0), t111 = __ldg(p1 + y1 + z1);
+    if (!Clamp) {
+        bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
+        bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
+        bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
+        if (!(vx0 && vx1 && vy0 && vy1 && vz0 && vz1)) {
+            t000 = vx0 && vy0 && vz0 ? t000 : 0.0f; t001 = vx0 && vy0 && vz1 ? t001 : 0.0f;
+            t010 = vx0 && vy1 && vz0 ? t010 : 0.0f; t011 = vx0 && vy1 && vz1 ? t011 : 0.0f;
+            t100 = vx1 && vy0 && vz0 ? t100 : 0.0f; t101 = vx1 && vy0 && vz1 ? t101 : 0.0f;
+            t110 = vx1 && vy1 && vz0 ? t110 : 0.0f; t111 = vx1 && vy1 && vz1 ? t111 : 0.0f;
+        }
+    }
+    float c00 = lerp_fast(t000, t001, wz), c01 = lerp_fast(t010, t011, wz);
+    float c10 = lerp_fast(t100, t101, wz), c11 = lerp_fast(t110, t111, wz);
+    return lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+}
+
 constexpr int kLut = 512;
 MRP_D float tex_lut(const float* __restrict__ lut, float u, float v) {
     float px = fs(fm(u, (float)kLut), 0.5f), py = fs(fm(v, (float)kLut), 0.5f);
@@ -211,6 +246,18 @@ MRP_HD size_t mip_offset(int m) { return (size_t)(((1u << 27) - (1u << (27 - 3 *
 MRP_HD size_t tr_offset(int m) { return (size_t)(((1u << 24) - (1u << (24 - 3 * m))) / 7u); }
 constexpr size_t kMipFloats = 19173961;   // sum_{m<9} (256>>m)^3
 constexpr size_t kTrFloats = 2396745;     // sum_{i<8} (128>>i)^3
+
+MRP_D float tex_lut_fast(const float* __restrict__ lut, float u, float v) {
+    float px = fmaf(u, (float)kLut, -0.5f), py = fmaf(v, (float)kLut, -0.5f);
+    float flx = floorf(px), fly = floorf(py);
+    int x = (int)flx, y = (int)fly;
+    float wx = px - flx, wy = py - fly;
+    int x0 = min(max(x, 0), kLut - 1), x1 = min(max(x + 1, 0), kLut - 1);
+    int y0 = min(max(y, 0), kLut - 1) * kLut, y1 = min(max(y + 1, 0), kLut - 1) * kLut;
+    float r0 = lerp_fast(__ldg(lut + y0 + x0), __ldg(lut + y1 + x0), wy);
+    float r1 = lerp_fast(__ldg(lut + y0 + x1), __ldg(lut + y1 + x1), wy);
+    return lerp_fast(r0, r1, wx);
+}
 
 // ---------------------------------------------------------------------------
 // Device view of one volume's resources (passed by value to kernels).
