@@ -596,7 +596,9 @@ def run_mine(args, rank, world, local):
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": STAGES[dom],
                 "note": f"algorithmic bytes = {STAGE_BYTES_PER_HIT[dom]} B x {active} hit pixels per launch; "
-                        f"duration = CUDA events around the stage; peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+                        f"duration = CUDA events around the stage; peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs); "
+                        f"the texel reads are served from L1/L2 (the 64 MiB mip-0 level and the TR levels), so "
+                        f"algorithmic bytes can exceed what DRAM moves: traffic is the ncu DRAM bytes per launch"}
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": traffic,
                 "kernel": STAGES[dom], "note": "march lookups are data dependent; see profiles/"}

@@ -169,18 +169,25 @@ MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
     int x = (int)flx, y = (int)fly, z = (int)flz;
     float wx = fs(px, flx), wy = fs(py, fly), wz = fs(pz, flz);
     float ox = fs(1.0f, wx), oy = fs(1.0f, wy), oz = fs(1.0f, wz);
-    int x0 = min(max(x, 0), n - 1), x1 = min(max(x + 1, 0), n - 1);
-    int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
-    int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
-    const float* p0 = g + (size_t)x0 * n * n;
-    const float* p1 = g + (size_t)x1 * n * n;
-    float t000 = __ldg(p0 + y0 + z0), t001 = __ldg(p0 + y0 + z1), t010 = __ldg(p0 + y1 + z0), t011 = __ldg(p0 + y1 + z1);
-    float t100 = __ldg(p1 + y0 + z0), t101 = __ldg(p1 + y0 + z1), t110 = __ldg(p1 + y1 + z0), t111 = __ldg(p1 + y1 + z1);
-    if (!Clamp) {
-        bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
-        bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
-        bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
-        if (!(vx0 && vx1 && vy0 && vy1 && vz0 && vz1)) {
+    const int nn = n * n;
+    float t000, t001, t010, t011, t100, t101, t110, t111;
+    if ((unsigned)x < (unsigned)(n - 1) && (unsigned)y < (unsigned)(n - 1) && (unsigned)z < (unsigned)(n - 1)) {
+        // footprint inside the grid: the clamps and border selects are no-ops
+        const float* b = g + ((size_t)x * n + y) * n + z;
+        t000 = __ldg(b); t001 = __ldg(b + 1); t010 = __ldg(b + n); t011 = __ldg(b + n + 1);
+        t100 = __ldg(b + nn); t101 = __ldg(b + nn + 1); t110 = __ldg(b + nn + n); t111 = __ldg(b + nn + n + 1);
+    } else {
+        int x0 = min(max(x, 0), n - 1), x1 = min(max(x + 1, 0), n - 1);
+        int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
+        int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
+        const float* p0 = g + (size_t)x0 * nn;
+        const float* p1 = g + (size_t)x1 * nn;
+        t000 = __ldg(p0 + y0 + z0); t001 = __ldg(p0 + y0 + z1); t010 = __ldg(p0 + y1 + z0); t011 = __ldg(p0 + y1 + z1);
+        t100 = __ldg(p1 + y0 + z0); t101 = __ldg(p1 + y0 + z1); t110 = __ldg(p1 + y1 + z0); t111 = __ldg(p1 + y1 + z1);
+        if (!Clamp) {
+            bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
+            bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
+            bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
             t000 = vx0 && vy0 && vz0 ? t000 : 0.0f; t001 = vx0 && vy0 && vz1 ? t001 : 0.0f;
             t010 = vx0 && vy1 && vz0 ? t010 : 0.0f; t011 = vx0 && vy1 && vz1 ? t011 : 0.0f;
             t100 = vx1 && vy0 && vz0 ? t100 : 0.0f; t101 = vx1 && vy0 && vz1 ? t101 : 0.0f;
@@ -198,6 +205,9 @@ MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
 // and lerp arithmetic.  The march keeps the exact forms above -- its
 // accept / stop decisions must match the reference's float order.
 MRP_D float lerp_fast(float a, float b, float v) { return fmaf(v, b - a, a); }
+// n^3 must stay below 2^31 (the pyramid and TR levels: n <= 256): 32-bit
+// offsets.  Footprints inside the grid (the common case) skip the clamps and
+// the border selects.
 template <bool Clamp>
 MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float nf = (float)n;
@@ -205,18 +215,24 @@ MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
     int x = (int)flx, y = (int)fly, z = (int)flz;
     float wx = px - flx, wy = py - fly, wz = pz - flz;
-    int x0 = min(max(x, 0), n - 1), x1 = min(max(x + 1, 0), n - 1);
-    int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
-    int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
-    const float* p0 = g + (size_t)x0 * n * n;
-    const float* p1 = g + (size_t)x1 * n * n;
-    float t000 = __ldg(p0 + y0 + z0), t001 = __ldg(p0 + y0 + z1), t010 = __ldg(p0 + y1 + z0), t011 = __ldg(p0 + y1 + z1);
-    float t100 = __ldg(p1 + y0 + z0), t101 = __ldg(p1 + y0 + z1), t110 = __ldg(p1 + y1 + z0), t111 = __ldg(p1 + y1 + z1);
-    if (!Clamp) {
-        bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
-        bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
-        bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
-        if (!(vx0 && vx1 && vy0 && vy1 && vz0 && vz1)) {
+    const int nn = n * n;
+    float t000, t001, t010, t011, t100, t101, t110, t111;
+    if ((unsigned)x < (unsigned)(n - 1) && (unsigned)y < (unsigned)(n - 1) && (unsigned)z < (unsigned)(n - 1)) {
+        const float* b = g + (x * n + y) * n + z;
+        t000 = __ldg(b); t001 = __ldg(b + 1); t010 = __ldg(b + n); t011 = __ldg(b + n + 1);
+        t100 = __ldg(b + nn); t101 = __ldg(b + nn + 1); t110 = __ldg(b + nn + n); t111 = __ldg(b + nn + n + 1);
+    } else {
+        int x0 = min(max(x, 0), n - 1) * nn, x1 = min(max(x + 1, 0), n - 1) * nn;
+        int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
+        int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
+        t000 = __ldg(g + x0 + y0 + z0); t001 = __ldg(g + x0 + y0 + z1);
+        t010 = __ldg(g + x0 + y1 + z0); t011 = __ldg(g + x0 + y1 + z1);
+        t100 = __ldg(g + x1 + y0 + z0); t101 = __ldg(g + x1 + y0 + z1);
+        t110 = __ldg(g + x1 + y1 + z0); t111 = __ldg(g + x1 + y1 + z1);
+        if (!Clamp) {
+            bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
+            bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
+            bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
             t000 = vx0 && vy0 && vz0 ? t000 : 0.0f; t001 = vx0 && vy0 && vz1 ? t001 : 0.0f;
             t010 = vx0 && vy1 && vz0 ? t010 : 0.0f; t011 = vx0 && vy1 && vz1 ? t011 : 0.0f;
             t100 = vx1 && vy0 && vz0 ? t100 : 0.0f; t101 = vx1 && vy0 && vz1 ? t101 : 0.0f;
@@ -252,11 +268,16 @@ MRP_D float tex_lut_fast(const float* __restrict__ lut, float u, float v) {
     float flx = floorf(px), fly = floorf(py);
     int x = (int)flx, y = (int)fly;
     float wx = px - flx, wy = py - fly;
-    int x0 = min(max(x, 0), kLut - 1), x1 = min(max(x + 1, 0), kLut - 1);
-    int y0 = min(max(y, 0), kLut - 1) * kLut, y1 = min(max(y + 1, 0), kLut - 1) * kLut;
-    float r0 = lerp_fast(__ldg(lut + y0 + x0), __ldg(lut + y1 + x0), wy);
-    float r1 = lerp_fast(__ldg(lut + y0 + x1), __ldg(lut + y1 + x1), wy);
-    return lerp_fast(r0, r1, wx);
+    float a, b, c, d;   // (x, y), (x, y + 1), (x + 1, y), (x + 1, y + 1)
+    if ((unsigned)x < (unsigned)(kLut - 1) && (unsigned)y < (unsigned)(kLut - 1)) {
+        const float* p = lut + y * kLut + x;
+        a = __ldg(p); b = __ldg(p + kLut); c = __ldg(p + 1); d = __ldg(p + kLut + 1);
+    } else {
+        int x0 = min(max(x, 0), kLut - 1), x1 = min(max(x + 1, 0), kLut - 1);
+        int y0 = min(max(y, 0), kLut - 1) * kLut, y1 = min(max(y + 1, 0), kLut - 1) * kLut;
+        a = __ldg(lut + y0 + x0); b = __ldg(lut + y1 + x0); c = __ldg(lut + y0 + x1); d = __ldg(lut + y1 + x1);
+    }
+    return lerp_fast(lerp_fast(a, b, wy), lerp_fast(c, d, wy), wx);
 }
 
 // ---------------------------------------------------------------------------
