@@ -21,7 +21,7 @@ namespace mrp {
 
 
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_trace(VolumeDev v, ViewDev w, double* __restrict__ sum3,
+__global__ void __launch_bounds__(128, 8) k_trace(VolumeDev v, ViewDev w, double* __restrict__ sum3,
                                                double* __restrict__ sumsq3, int* __restrict__ first_pos,
                                                unsigned long long* __restrict__ counter) {
     const long long total = (long long)w.width * w.height * w.spp;
