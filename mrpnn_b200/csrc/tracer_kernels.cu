@@ -7,63 +7,181 @@
 // (nee_mode 0, the reference) or one unbiased Tr() estimate per vertex from
 // the sample's own NEE stream (nee_mode 1; the error reference).
 //
-// B200 form: a persistent kernel pulls (pixel, sample) work items from a
-// global counter, so a lane whose path ended starts the next one instead of
-// idling until the longest path of its warp finishes (per-pixel threads
-// leave most lanes idle: path lengths range from 0 to 256 bounces).  Every
-// sample has its own Philox stream (sub = sample index), so results do not
-// depend on which lane ran it.  Per-sample radiance is computed in fp32 in
-// the reference's order and accumulated per pixel in FP64.
+// B200 form: a persistent kernel runs an event loop per lane.  A lane holds
+// one (pixel, sample) item; one loop iteration of a warp is either a
+// free-flight step (two draws, one density fetch, one comparison) of every
+// lane that is in flight, or the real-collision work (phase sampling, NEE,
+// next flight) of every lane that has collided.  Collided lanes wait until
+// kScatterBatch of them are pending (or no lane can step), so the long
+// collision branch runs with many lanes at once instead of with the one or
+// two that collide in a given step.  A lane whose sample ends takes the next
+// item from a global counter at once (one atomic per warp for all lanes
+// that need work).  Every sample has its own Philox stream (sub = sample
+// index) and its arithmetic is CalculateRadiance's, in the reference's order,
+// so results do not depend on which lane ran it or when.  Per-sample
+// radiance is fp32, accumulated per pixel in FP64.
 #include "kernels.h"
 #include "tracing.cuh"
 
 namespace mrp {
 
+namespace {
+constexpr int kScatterBatch = 8;
+
+// The sample's kPixelStream: the state of Stream(kPixelStream, pix, k,
+// frame, seed) without its constant fields (same draws).
+struct LaneStream {
+    uint32_t n, blk[4];
+    MRP_D float next(uint32_t pix, uint32_t k, uint32_t frame, uint32_t seed) {
+        if ((n & 3) == 0) philox(n >> 2, k, frame, kPixelStream, pix, seed ^ (kPixelStream * 0x9E3779B9u), blk);
+        uint32_t x = (n & 2) ? ((n & 1) ? blk[3] : blk[2]) : ((n & 1) ? blk[1] : blk[0]);
+        ++n;
+        return u01(x);
+    }
+};
+
+// nee_mode 1: one unbiased Tr() estimate from the sample's NEE stream,
+// positioned at draw *n.
+__device__ __forceinline__ float nee_tr(const VolumeDev& v, const ViewDev& w, int pix, int k, uint32_t* n, f3 p, f3 L) {
+    Stream s(kNeeStream, (uint32_t)pix, (uint32_t)k, (uint32_t)w.frame, w.seed);
+    s.n = *n;
+    if (s.n & 3) philox(s.n >> 2, s.sub, s.frame, s.kind, s.k0, s.k1, s.blk);
+    float tr = transmittance(v, s, p, L, ray_box_distance(p, L), w.alpha);
+    *n = s.n;
+    return tr;
+}
+
+MRP_D void deposit(double* __restrict__ sum3, double* __restrict__ sumsq3, int* __restrict__ first_pos, int pix, int k,
+                   f3 r, bool hit) {
+    if (hit && (r.x > 0 || r.y > 0 || r.z > 0)) atomicMin(first_pos + pix, k);
+    atomicAdd(sum3 + 3 * pix, (double)r.x);
+    atomicAdd(sum3 + 3 * pix + 1, (double)r.y);
+    atomicAdd(sum3 + 3 * pix + 2, (double)r.z);
+    if (sumsq3) {
+        atomicAdd(sumsq3 + 3 * pix, (double)r.x * r.x);
+        atomicAdd(sumsq3 + 3 * pix + 1, (double)r.y * r.y);
+        atomicAdd(sumsq3 + 3 * pix + 2, (double)r.z * r.z);
+    }
+}
+}  // namespace
 
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 8) k_trace(VolumeDev v, ViewDev w, double* __restrict__ sum3,
+__global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ VolumeDev v,
+                                               const __grid_constant__ ViewDev w, double* __restrict__ sum3,
                                                double* __restrict__ sumsq3, int* __restrict__ first_pos,
                                                unsigned long long* __restrict__ counter) {
-    const long long total = (long long)w.width * w.height * w.spp;
+    const unsigned long long total = (unsigned long long)w.width * w.height * w.spp;
     const int npix = w.width * w.height;
-    f3 L = normalize(w.light_dir);
+    const f3 L = normalize(w.light_dir);
+    const float smax = fm(v.max_density, w.alpha);
+    const uint32_t frame = (uint32_t)w.frame, seed = w.seed;
+    const unsigned lane = threadIdx.x & 31, lt_mask = (1u << lane) - 1u;
     Tally tally;
+    // the lane's sample: pixel, index, stream, vertex, direction, throughput,
+    // radiance, bounce, free-flight distance / limit / iteration
+    bool live = false, dry = false, hit = false;
+    int pix = 0, k = 0, b = 0, loop = 0;
+    uint32_t nee_n = 0;
+    LaneStream st{0, {0, 0, 0, 0}};
+    f3 p = mk3(0, 0, 0), rd = p, csr = p, res = p;
+    float t = 0.0f, md = 0.0f;
     for (;;) {
-        long long item;
-        // one atomic per warp, items handed out in warp-sized runs
-        unsigned lane = threadIdx.x & 31;
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(counter, 32ull);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        item = (long long)base + lane;
-        if ((long long)base >= total) break;
-        if (item >= total) continue;
-        // sample-major order: consecutive lanes trace neighbouring pixels
-        int k = (int)(item / npix), pix = (int)(item % npix);
-        int row = pix / w.width, col = pix % w.width;
-        f3 ori = w.ori, dir;
-        if (w.ray_dir) {   // GetRadiances: explicit rays
-            ori = mk3(w.ray_ori[3 * pix], w.ray_ori[3 * pix + 1], w.ray_ori[3 * pix + 2]);
-            dir = normalize(mk3(w.ray_dir[3 * pix], w.ray_dir[3 * pix + 1], w.ray_dir[3 * pix + 2]));
-        } else {
-            dir = normalize(camera_ray_t(w, row, col));
+        // refill: every lane without a sample takes the next item (rays that
+        // miss the box are resolved to the sky here and refilled again)
+        for (;;) {
+            const unsigned need = __ballot_sync(0xffffffffu, !live && !dry);
+            if (!need) break;
+            const int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!live && !dry) {
+                const unsigned long long item = base + __popc(need & lt_mask);
+                if (item >= total) {
+                    dry = true;
+                } else {
+                    // sample-major order: consecutive items trace neighbouring pixels
+                    k = (int)(item / npix);
+                    pix = (int)(item % npix);
+                    int row = pix / w.width, col = pix % w.width;
+                    f3 ori = w.ori, dir;
+                    if (w.ray_dir) {   // GetRadiances: explicit rays
+                        ori = mk3(w.ray_ori[3 * pix], w.ray_ori[3 * pix + 1], w.ray_ori[3 * pix + 2]);
+                        dir = normalize(mk3(w.ray_dir[3 * pix], w.ray_dir[3 * pix + 1], w.ray_dir[3 * pix + 2]));
+                    } else {
+                        dir = normalize(camera_ray_t(w, row, col));
+                    }
+                    float dis = ray_box_offset(ori, dir);
+                    if (dis < 0) {
+                        deposit(sum3, sumsq3, first_pos, pix, k, v.sky, false);   // SkyBox(dir), coverage stays 0
+                    } else {
+                        if (COUNT) tally.events++;
+                        if (w.multi_scatter < 1) {
+                            deposit(sum3, sumsq3, first_pos, pix, k, mk3(0, 0, 0), true);
+                        } else {
+                            st.n = 0;
+                            nee_n = 0;
+                            res = mk3(0, 0, 0);
+                            p = add(ori, mul(dir, dis));
+                            rd = dir;
+                            csr = mk3(1, 1, 1);
+                            b = 0;
+                            md = ray_box_distance(p, rd);
+                            t = 0.0f;
+                            loop = 0;
+                            hit = false;
+                            if (COUNT) tally.steps++;
+                            live = true;
+                        }
+                    }
+                }
+            }
         }
-        float dis = ray_box_offset(ori, dir);
-        f3 r;
-        if (dis < 0) {
-            r = v.sky;   // SkyBox(dir), coverage stays 0
-        } else {
-            r = trace_sample(v, w, pix, k, ori, dir, dis, L, COUNT ? &tally : nullptr);
-            if (COUNT) tally.events++;
-            if (r.x > 0 || r.y > 0 || r.z > 0) atomicMin(first_pos + pix, k);
+        const unsigned pend = __ballot_sync(0xffffffffu, live && hit);
+        const unsigned fly = __ballot_sync(0xffffffffu, live && !hit);
+        if (!(pend | fly)) break;
+        if (fly && __popc(pend) < kScatterBatch) {
+            if (!live || hit) continue;
+            // one iteration of DeterminateNextVertex's loop (while (loop++ < 10000))
+            if (loop >= 10000) { hit = true; continue; }
+            ++loop;
+            float rk = st.next(pix, k, frame, seed);
+            t = fs(t, fd(logf(fs(1.0f, rk)), smax));
+            if (t > md) {   // left the box: sky radiance, the sample ends
+                res = add(res, mul(v.sky, csr));
+                deposit(sum3, sumsq3, first_pos, pix, k, res, true);
+                live = false;
+                continue;
+            }
+            rk = st.next(pix, k, frame, seed);
+            float d = density_t(v, add(p, mul(rd, t)));
+            if (COUNT) tally.fetches++;
+            float S = fm(d, w.alpha);
+            hit = fd(S, smax) > rk;
+            if (!hit && d < 0) t = fs(t, d);
+            continue;
         }
-        atomicAdd(sum3 + 3 * pix, (double)r.x);
-        atomicAdd(sum3 + 3 * pix + 1, (double)r.y);
-        atomicAdd(sum3 + 3 * pix + 2, (double)r.z);
-        if (sumsq3) {
-            atomicAdd(sumsq3 + 3 * pix, (double)r.x * r.x);
-            atomicAdd(sumsq3 + 3 * pix + 1, (double)r.y * r.y);
-            atomicAdd(sumsq3 + 3 * pix + 2, (double)r.z * r.z);
+        if (!live || !hit) continue;
+        // real collision: phase sampling, NEE, next flight
+        float e1 = st.next(pix, k, frame, seed);
+        float e0 = st.next(pix, k, frame, seed);
+        f3 nd = sample_hg(e0, e1, rd, w.g);
+        p = add(mul(rd, t), p);
+        csr = mul(csr, v.scatter_rate);
+        float ph = hg(dot(rd, L), w.g);
+        float tr = v.nee_mode ? nee_tr(v, w, pix, k, &nee_n, p, L) : tex3<true>(v.baked, v.baked_res, p);
+        if (COUNT) tally.lookups++;
+        res = add(res, mul(mul(w.light_color, csr), fm(tr, ph)));
+        rd = nd;
+        hit = false;
+        if (++b >= w.multi_scatter) {
+            deposit(sum3, sumsq3, first_pos, pix, k, res, true);
+            live = false;
+        } else {
+            md = ray_box_distance(p, rd);
+            t = 0.0f;
+            loop = 0;
+            if (COUNT) tally.steps++;
         }
     }
     if (COUNT) flush_tally(w.counters, tally);
