@@ -25,8 +25,22 @@ __constant__ int c_layer[192];
 __constant__ float c_lutv[192];
 __constant__ float c_dirs[160 * 3];
 
+// The 192 points as the runs of GetSamples23_'s layout: layers 0..7 over the
+// 160 rotated directions (8, 8, 16, 16, 16, 32, 32, 32 points), then layers
+// 0..3 on the light ray (8 points each).  set_stencil_tables checks that the
+// tables it loads have this layout.
+constexpr int kStencilRuns[12][3] = {{0, 0, 8},     {1, 8, 16},    {2, 16, 32},   {3, 32, 48},
+                                     {4, 48, 64},   {5, 64, 96},   {6, 96, 128},  {7, 128, 160},
+                                     {0, 160, 168}, {1, 168, 176}, {2, 176, 184}, {3, 184, 192}};
+__constant__ int c_stencil_runs[12][3] = {{0, 0, 8},     {1, 8, 16},    {2, 16, 32},   {3, 32, 48},
+                                          {4, 48, 64},   {5, 64, 96},   {6, 96, 128},  {7, 128, 160},
+                                          {0, 160, 168}, {1, 168, 176}, {2, 176, 184}, {3, 184, 192}};
 cudaError_t set_stencil_tables(const StencilTables& t) {
     cudaError_t e;
+    // the staged gather is compiled for the runs of kStencilRuns
+    for (const auto& run : kStencilRuns)
+        for (int i = run[1]; i < run[2]; ++i)
+            if (t.layer[i] != run[0]) return cudaErrorInvalidValue;
     if ((e = cudaMemcpyToSymbol(c_offset, t.offset, sizeof t.offset)) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_layer, t.layer, sizeof t.layer)) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_lutv, t.lut_v, sizeof t.lut_v)) != cudaSuccess) return e;
@@ -193,21 +207,20 @@ MRP_D void gather_sample(const VolumeDev& v, const PixelFrame& f, int i, float* 
 // The same stencil point with contracted arithmetic (FMA positions and
 // lerps, rsqrt direction), used by the staged gather of the render path:
 // the features stay within 1e-5 relative of gather_sample.
-MRP_D float shadow_tr_fast(const VolumeDev& v, f3 p, f3 light, int mip) {
-    const float* g = tr_level(v, mip);
-    int n = 128 >> mip;
-    if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
-        float off = ray_box_offset(p, light);
-        if (off >= 0) return tex3_fast<true>(g, n, mk3(fmaf(light.x, off, p.x), fmaf(light.y, off, p.y), fmaf(light.z, off, p.z)));
-        return 1.0f;
-    }
-    return tex3_fast<true>(g, n, p);
-}
-MRP_D void gather_sample_fast(const VolumeDev& v, const PixelFrame& f, int i, float* fd_, float* fs_, float* fh_) {
+// Stencil point i with the sizes and levels of its run hoisted by the
+// caller: mip level m (n^3 texels), TR level (tn^3), and whether the point
+// lies on the light ray (i >= 160) rather than along a rotated direction.
+struct RunLevels {
+    const float* mip;
+    const float* tr;
+    int n, tn;
+    bool light;
+};
+MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunLevels& R, int i, float* fd_, float* fs_,
+                             float* fh_) {
     const float off = c_offset[i];
-    const int layer = c_layer[i];
     f3 d;   // offset from the point
-    if (i < 160) {
+    if (!R.light) {
         const float px = c_dirs[3 * i], py = c_dirs[3 * i + 1], pz = c_dirs[3 * i + 2];
         d = mk3(fmaf(f.Z.x, pz, fmaf(f.Y.x, py, f.X.x * px)) * off, fmaf(f.Z.y, pz, fmaf(f.Y.y, py, f.X.y * px)) * off,
                 fmaf(f.Z.z, pz, fmaf(f.Y.z, py, f.X.z * px)) * off);
@@ -215,7 +228,7 @@ MRP_D void gather_sample_fast(const VolumeDev& v, const PixelFrame& f, int i, fl
         d = mk3(f.L.x * off, f.L.y * off, f.L.z * off);
     }
     const f3 cur = mk3(f.pos.x + d.x, f.pos.y + d.y, f.pos.z + d.z);
-    const float dens = tex3_fast<false>(mip_level(v, layer), 256 >> layer, cur);
+    const float dens = tex3_fast<false>(R.mip, R.n, cur);
     *fd_ = logf(fmaf(f.alpha * dens, 0.015625f, 1.0f));
     if (i == 0) {
         *fh_ = logf(hg(dot(f.X, f.L), f.g) + 1.0f);
@@ -229,7 +242,36 @@ MRP_D void gather_sample_fast(const VolumeDev& v, const PixelFrame& f, int i, fl
         *fh_ = logf(fmaf(tex_lut_fast(v.lut, fmaf(c1, 0.5f, 0.5f), lv), tex_lut_fast(v.lut, fmaf(c2, 0.5f, 0.5f), lv),
                          1.0f));
     }
-    *fs_ = shadow_tr_fast(v, cur, f.LX, layer > 1 ? layer - 1 : 0);
+    // ShadowTerm_TRs: outside the box, the TR where the light ray enters it
+    const f3 p = cur, light = f.LX;
+    float tr = 1.0f;
+    if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
+        float o = ray_box_offset(p, light);
+        if (o >= 0)
+            tr = tex3_fast<true>(R.tr, R.tn, mk3(fmaf(light.x, o, p.x), fmaf(light.y, o, p.y), fmaf(light.z, o, p.z)));
+    } else {
+        tr = tex3_fast<true>(R.tr, R.tn, p);
+    }
+    *fs_ = tr;
+}
+// All 192 points, run by run (GetSamples23_'s layout: layers 0..7 over the
+// 160 rotated directions, then layers 0..3 on the light ray), into the tiled
+// feature layout.
+MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* out) {
+#pragma unroll 1
+    for (int run = 0; run < 12; ++run) {
+        const int layer = c_stencil_runs[run][0], from = c_stencil_runs[run][1], to = c_stencil_runs[run][2];
+        const int tl = layer > 1 ? layer - 1 : 0;
+        const RunLevels R{mip_level(v, layer), tr_level(v, tl), 256 >> layer, 128 >> tl, from >= 160};
+#pragma unroll 1
+        for (int i = from; i < to; ++i) {
+            float a, b, c;
+            gather_point_fast(v, f, R, i, &a, &b, &c);
+            out[i * 32] = a;
+            out[(192 + i) * 32] = b;
+            out[(384 + i) * 32] = c;
+        }
+    }
 }
 MRP_D float gamma_of(const PixelFrame& f) { return acosf(fminf(1.0f, fmaxf(-1.0f, dot(f.X, f.LX)))); }
 
@@ -598,15 +640,7 @@ __global__ void __launch_bounds__(128) k_gather_rec(VolumeDev v, ViewDev w, HitR
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *rec.count) return;
     PixelFrame pf = record_frame(rec, r, normalize(w.light_dir), w.g, w.alpha);
-    float* out = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
-#pragma unroll 1
-    for (int i = 0; i < 192; ++i) {
-        float a, b, c;
-        gather_sample_fast(v, pf, i, &a, &b, &c);
-        out[i * 32] = a;
-        out[(192 + i) * 32] = b;
-        out[(384 + i) * 32] = c;
-    }
+    gather_all_fast(v, pf, feat + (size_t)(r >> 5) * 576 * 32 + (r & 31));
 }
 
 __global__ void __launch_bounds__(128) k_mlp_rec(VolumeDev v, ViewDev w, HitRecords rec, const float* __restrict__ feat,
