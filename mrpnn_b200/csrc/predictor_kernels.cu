@@ -55,24 +55,36 @@ MRP_D const float* tr_level(const VolumeDev& v, int m) { return v.trs + tr_offse
 // pixel stream.
 MRP_D f3 camera_ray(const ViewDev& w, int row, int col) { return camera_ray_dir(w, row, col); }
 
-// Density() at p, skipping the 8 texel loads when the occupancy bricks prove
-// the trilinear footprint is all zero: the base voxel of the fetch is
-// floor(uv*R - 0.5) per axis; a base outside [-1, R-1] reads only border
-// texels (0), and a base inside reads voxels base..base+1, which lie in the
-// 1-voxel apron of its brick.  lerp(0, 0, w) is exactly +0, so the skip
-// returns the value the fetch would.
-MRP_D float density_skip(const VolumeDev& v, f3 p, Tally* tl) {
-    f3 uv = adds(p, 0.5f);
-    float nf = (float)v.res;
-    int x = (int)floorf(fs(fm(uv.x, nf), 0.5f)), y = (int)floorf(fs(fm(uv.y, nf), 0.5f)),
-        z = (int)floorf(fs(fm(uv.z, nf), 0.5f));
-    int R1 = v.res - 1;
-    if (x < -1 || y < -1 || z < -1 || x > R1 || y > R1 || z > R1) return 0.0f;
-    int nb = v.occ_res;
-    int b = ((max(x, 0) >> v.occ_shift) * nb + (max(y, 0) >> v.occ_shift)) * nb + (max(z, 0) >> v.occ_shift);
-    if (__ldg(v.occ + b) == 0) return 0.0f;
+// Density() at pos + dir * t for the march, skipping the 8 texel loads when
+// an occupancy brick proves the trilinear footprint all zero.  The brick is
+// found from X = c + sR * t per axis (c = (pos + 0.5) * R - 0.5, sR = dir *
+// R, one FMA), which differs from the fetch's own texel coordinate by far
+// less than one voxel; the bricks carry one voxel of apron more than a
+// fetch needs, so the brick of floor(X) (clamped to the grid) holds the
+// fetch's whole footprint either way.  lerp(0, 0, w) is exactly +0, so the
+// skip returns the value the fetch would, and otherwise the fetch runs on
+// the exact position.
+struct MarchRay {
+    f3 pos, dir;
+    f3 c, sR;   // texel coordinate X(t) = c + sR * t, per axis
+};
+MRP_D MarchRay march_ray(const VolumeDev& v, f3 pos, f3 dir) {
+    const float nf = (float)v.res;
+    MarchRay m;
+    m.pos = pos;
+    m.dir = dir;
+    m.c = mk3((pos.x + 0.5f) * nf - 0.5f, (pos.y + 0.5f) * nf - 0.5f, (pos.z + 0.5f) * nf - 0.5f);
+    m.sR = mk3(dir.x * nf, dir.y * nf, dir.z * nf);
+    return m;
+}
+MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* tl) {
+    const int R1 = v.res - 1, sh = v.occ_shift, nb = v.occ_res;
+    const int x = min(max(__float2int_rd(fmaf(m.sR.x, t, m.c.x)), 0), R1) >> sh;
+    const int y = min(max(__float2int_rd(fmaf(m.sR.y, t, m.c.y)), 0), R1) >> sh;
+    const int z = min(max(__float2int_rd(fmaf(m.sR.z, t, m.c.z)), 0), R1) >> sh;
+    if (__ldg(v.occ + (x * nb + y) * nb + z) == 0) return 0.0f;
     if (tl) tl->fetches++;
-    return tex3<false>(v.density, v.res, p);
+    return tex3<false>(v.density, v.res, add(m.pos, mul(m.dir, t)));
 }
 
 // DeterminateEstimatedHit(float& alpha, ...) (core/render.cuh:105-197).
@@ -83,6 +95,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
     float t = 0.0f, last_non_empty_t = 0.0f, prob = 1.0f, last_dens = 0.0f;
     float rf = (float)v.res;
     float t_step = fd(2.0f, rf), empty_step = fd(1.0f, rf);
+    const MarchRay mr = march_ray(v, pos, dir);
     int loop = 0;
     while (loop++ < 10000) {
         if (t > dis) {
@@ -93,7 +106,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
         if (tl) tl->steps++;
         float d;
         if (v.occ) {
-            d = density_skip(v, add(pos, mul(dir, t)), tl);
+            d = density_skip(v, mr, t, tl);
         } else {
             d = density(v, add(pos, mul(dir, t)));
             if (tl) tl->fetches++;

@@ -106,10 +106,13 @@ __global__ void k_max_density(const float* __restrict__ d, size_t n, int* __rest
 // Occupancy bricks for exact empty-space skipping in the first-hit march.
 // Brick b covers voxels [b*B, b*B + B) per axis.  A trilinear fetch whose
 // base voxel lies in brick b reads voxels base..base+1, i.e. at most one
-// voxel past the brick, so the brick is marked occupied when any voxel in
-// [b*B - 1, b*B + B] holds a non-zero value.  A zero brick therefore
-// guarantees Density() == 0 exactly for every sample whose base voxel is in
-// it (border texels are 0 by addressing).
+// voxel past the brick; the brick is marked occupied when any voxel in
+// [b*B - 1, b*B + B + 1] holds a non-zero value, one voxel more on each
+// side than the fetch needs, so that a base voxel found from a coordinate
+// that may be off by less than one voxel still picks a brick whose apron
+// holds the whole footprint.  A zero brick therefore guarantees Density() ==
+// 0 exactly for every sample whose base voxel is in it or within one voxel
+// of it (border texels are 0 by addressing).
 // ---------------------------------------------------------------------------
 __global__ void k_occupancy(const float* __restrict__ d, int R, int shift, int nb, uint8_t* __restrict__ occ) {
     int total = nb * nb * nb;
@@ -117,7 +120,7 @@ __global__ void k_occupancy(const float* __restrict__ d, int R, int shift, int n
         int bz = b % nb, by = (b / nb) % nb, bx = b / (nb * nb);
         int B = 1 << shift;
         int x0 = bx * B - 1, y0 = by * B - 1, z0 = bz * B - 1;
-        int span = B + 2;
+        int span = B + 3;
         int any = 0;
         for (int t = threadIdx.x; t < span * span * span && !any; t += blockDim.x) {
             int z = z0 + t % span, y = y0 + (t / span) % span, x = x0 + t / (span * span);

@@ -41,13 +41,15 @@ def test_occupancy_is_conservative(scene):
     R, B = 64, 8
     nb = R // B
     d = scene.density.reshape(R, R, R) != 0
-    pad = np.zeros((R + 2, R + 2, R + 2), bool)
-    pad[1:-1, 1:-1, 1:-1] = d
+    pad = np.zeros((R + 3, R + 3, R + 3), bool)
+    pad[1:-2, 1:-2, 1:-2] = d
     want = np.zeros((nb, nb, nb), np.uint8)
+    # brick b: voxels [b*B - 1, b*B + B + 1] (the fetch's one-voxel apron plus
+    # one voxel of slack for the march's approximate brick lookup)
     for bx in range(nb):
         for by in range(nb):
             for bz in range(nb):
-                want[bx, by, bz] = pad[bx * B:bx * B + B + 2, by * B:by * B + B + 2, bz * B:bz * B + B + 2].any()
+                want[bx, by, bz] = pad[bx * B:bx * B + B + 3, by * B:by * B + B + 3, bz * B:bz * B + B + 3].any()
     np.testing.assert_array_equal(occ.reshape(nb, nb, nb), want)
 
 
