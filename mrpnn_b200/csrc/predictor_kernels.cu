@@ -586,8 +586,11 @@ MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
     accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
 }
 
+// 128-thread blocks, ten resident per SM (48 registers): a block retires as
+// soon as its slowest ray ends, and march lengths vary from 0 to ~1000 steps.
+constexpr int kHitThreads = 128;
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
+__global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
     Tally tally;
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
     int npix = w.width * w.height;
@@ -711,8 +714,9 @@ cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, 
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(rec.count, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    if (view.counters) k_hit<true><<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
-    else k_hit<false><<<(n + 255) / 256, 256, 0, s>>>(v, view, rec, accum);
+    const int blocks = (n + kHitThreads - 1) / kHitThreads;
+    if (view.counters) k_hit<true><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+    else k_hit<false><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
     return cudaGetLastError();
 }
 // ---------------------------------------------------------------------------
