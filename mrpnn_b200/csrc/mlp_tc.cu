@@ -78,6 +78,8 @@ __host__ __device__ constexpr int layer_w32(int i) {
 __host__ __device__ constexpr int layer_b32(int i) { return layer_w32(i) + layer_n(i) * layer_k(i); }
 static_assert(layer_b32(kLC0) == kLC0B && layer_b32(kLX0 + 11) == lxb(11), "layer table");
 static_assert(image_bytes(2) <= 110 * 1024, "BF16 weight image must fit shared memory");
+static_assert(kAuxBias % 4 == 0 && kAuxSE % 4 == 0 && kAuxLSE1 % 4 == 0 && kAuxLSE2 % 4 == 0 && 88 % 4 == 0,
+              "constants read as float4 start on 16-byte boundaries");
 
 // Byte offset of element (row m, k) in a K-major no-swizzle operand tile of
 // padded width Kp: 8-row groups SBO = Kp*eb*8 bytes apart, 16-byte K chunks
@@ -148,7 +150,9 @@ cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
         const float* src = w32 + (b < 8 ? mblk_off(b) : di_block_off(b - 8));
         std::memcpy(&aux[kAuxSE + 88 * b], src, 88 * sizeof(float));
     }
-    std::memcpy(&aux[kAuxLSE1], w32 + kLSEFin1W, 1200 * sizeof(float));
+    // LSEFin1 [16][75] (out, in) stored input-major [75][16]
+    for (int o = 0; o < 16; ++o)
+        for (int j = 0; j < 75; ++j) aux[kAuxLSE1 + 16 * j + o] = w32[kLSEFin1W + o * 75 + j];
     std::memcpy(&aux[kAuxLSE2], w32 + kLSEFin2W, 96 * sizeof(float));
     std::memcpy(&aux[kAuxLGGSW], w32 + kLGGSW, 24 * sizeof(float));
     std::memcpy(&aux[kAuxLGGSB], w32 + kLGGSB, 8 * sizeof(float));
@@ -335,13 +339,36 @@ MRP_D float wl(const float* __restrict__ w, int i) { return __ldg(w + i); }
 MRP_D float sigmoid_d(float o) { return 1.0f / (1.0f + __expf(-o)); }
 
 // relu(D * scale + b) for N columns of layer L (runtime), in place.
+// Biases and scales start on 16-float boundaries (scale_off), so they are
+// read four at a time.
 template <int EB, int N>
 MRP_D void bias_relu(float* d, int L, float rs, const float* aux) {
+    static_assert(N % 4 == 0, "layer widths are multiples of 4");
     const int ab = c_layer_desc[L].abias, so = c_layer_desc[L].soff;
+    const float4* b4 = reinterpret_cast<const float4*>(aux + ab);
+    const float4* s4 = reinterpret_cast<const float4*>(aux + kAuxScale + so);
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-        float sc = EB == 1 ? rs * aux[kAuxScale + so + i] : 1.0f;
-        d[i] = fmaxf(fmaf(d[i], sc, aux[ab + i]), 0.0f);
+    for (int q = 0; q < N / 4; ++q) {
+        const float4 b = b4[q];
+        float4 sc = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        if (EB == 1) {
+            const float4 w = s4[q];
+            sc = make_float4(rs * w.x, rs * w.y, rs * w.z, rs * w.w);
+        }
+        d[4 * q] = fmaxf(fmaf(d[4 * q], sc.x, b.x), 0.0f);
+        d[4 * q + 1] = fmaxf(fmaf(d[4 * q + 1], sc.y, b.y), 0.0f);
+        d[4 * q + 2] = fmaxf(fmaf(d[4 * q + 2], sc.z, b.z), 0.0f);
+        d[4 * q + 3] = fmaxf(fmaf(d[4 * q + 3], sc.w, b.w), 0.0f);
+    }
+}
+// n consecutive constants (16-byte aligned, n a multiple of 4) into registers.
+template <int N>
+MRP_D void aux_row(const float* aux, int off, float* out) {
+    const float4* p = reinterpret_cast<const float4*>(aux + off);
+#pragma unroll
+    for (int q = 0; q < N / 4; ++q) {
+        const float4 v = p[q];
+        out[4 * q] = v.x; out[4 * q + 1] = v.y; out[4 * q + 2] = v.z; out[4 * q + 3] = v.w;
     }
 }
 
@@ -451,32 +478,38 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
     {
         float hf[16];
         tmem_get<16>(G, kColHf, hf);
-#pragma unroll 4
-        for (int o = 0; o < 16; ++o) {
-            float a = hf[o];
-            const float* w1 = aux + kAuxLSE1 + o * 75 + pid;
+        // (LSEFin1 is stored input-major: the 16 weights of input j at
+        // kAuxLSE1 + 16 j; per output the same sequence of FMAs as o-major)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                a = fmaf(w1[c], p8[c], a);
-                a = fmaf(w1[36 + c], p8[3 + c], a);
+        for (int c = 0; c < 3; ++c) {
+            float wa[16], wm[16];
+            aux_row<16>(aux, kAuxLSE1 + 16 * (pid + c), wa);
+            aux_row<16>(aux, kAuxLSE1 + 16 * (36 + pid + c), wm);
+#pragma unroll
+            for (int o = 0; o < 16; ++o) {
+                hf[o] = fmaf(wa[o], p8[c], hf[o]);
+                hf[o] = fmaf(wm[o], p8[3 + c], hf[o]);
             }
-            hf[o] = a;
         }
         tmem_put<16>(G, kColHf, hf);
     }
     float h[8], gate[3];
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
+        float w[8];
+        aux_row<8>(aux, se_off + o * 8, w);
         float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], aux[se_off + o * 8 + j], a);
+        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], w[j], a);
         h[o] = fmaxf(a, 0.0f);
     }
 #pragma unroll
     for (int o = 0; o < 3; ++o) {
+        float w[8];
+        aux_row<8>(aux, se_off + 64 + o * 8, w);
         float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a = fmaf(h[j], aux[se_off + 64 + o * 8 + j], a);
+        for (int j = 0; j < 8; ++j) a = fmaf(h[j], w[j], a);
         gate[o] = sigmoid_d(a);
     }
     float rs[3];
@@ -555,16 +588,18 @@ __device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux,
 #pragma unroll
     for (int o = 0; o < 16; ++o) {
         float a = h[o];
-        a = fmaf(aux[kAuxLSE1 + o * 75 + 72], g, a);
-        a = fmaf(aux[kAuxLSE1 + o * 75 + 73], gamma, a);
-        a = fmaf(aux[kAuxLSE1 + o * 75 + 74], s4, a);
+        a = fmaf(aux[kAuxLSE1 + 16 * 72 + o], g, a);
+        a = fmaf(aux[kAuxLSE1 + 16 * 73 + o], gamma, a);
+        a = fmaf(aux[kAuxLSE1 + 16 * 74 + o], s4, a);
         h[o] = fmaxf(a, 0.0f);
     }
 #pragma unroll
     for (int o = 0; o < 6; ++o) {
+        float w[16];
+        aux_row<16>(aux, kAuxLSE2 + o * 16, w);
         float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) a = fmaf(h[j], aux[kAuxLSE2 + o * 16 + j], a);
+        for (int j = 0; j < 16; ++j) a = fmaf(h[j], w[j], a);
         gf[o] = sigmoid_d(a);
     }
     // LC0's A row: [comb * gate segment, LGGS (3 -> 8)]
