@@ -498,7 +498,10 @@ STAGES = ("first hit + bases", "stencil gather", "network")
 #            576 features x 4 B written
 #   network: 576 features x 4 B read + 16 B record + 16 B result
 FLOP_PER_HIT = 97072   # 2 x 48,536 MACs of RadiancePredictInternal, grey albedo
-STAGE_BYTES_PER_HIT = (None, GATHER_BYTES_PER_PIXEL + 576 * 4, 576 * 4 + 32)
+# features are fp32 for the FP32 network and FP16 pairs for the tensor-core ones
+def stage_bytes_per_hit(precision):
+    fb = 4 if precision == "fp32" else 2
+    return (None, GATHER_BYTES_PER_PIXEL + 576 * fb, 576 * fb + 32)
 
 
 def time_frames(vol, view, steps, flush, dev_out, frame0):
@@ -591,12 +594,12 @@ def run_mine(args, rank, world, local):
                         f"duration = CUDA events around the stage; peak {peak_kind} burst bf16 "
                         f"(MEASURED_PEAKS.json bf16_tflops); DRAM from the ncu traffic "
                         f"{'%.0f GB/s' % dram if dram else 'n/a'} of {hbm:.0f}"}
-    elif STAGE_BYTES_PER_HIT[dom] is not None:
-        alg = active * STAGE_BYTES_PER_HIT[dom]
+    elif stage_bytes_per_hit(args.precision)[dom] is not None:
+        alg = active * stage_bytes_per_hit(args.precision)[dom]
         achieved = alg / (st[dom] / 1000.0) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": STAGES[dom],
-                "note": f"algorithmic bytes = {STAGE_BYTES_PER_HIT[dom]} B x {active} hit pixels per launch; "
+                "note": f"algorithmic bytes = {stage_bytes_per_hit(args.precision)[dom]} B x {active} hit pixels per launch; "
                         f"duration = CUDA events around the stage; peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs); "
                         f"the texel reads are served from L1/L2 (the 64 MiB mip-0 level and the TR levels), so "
                         f"algorithmic bytes can exceed what DRAM moves: traffic is the ncu DRAM bytes per launch"}

@@ -677,7 +677,7 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
             if (last) CU(cudaEventRecord(v->ev0, v->stream));
             CU(launch_hit(d, vd, rec, v->accum, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));
-            CU(launch_gather_rec(d, vd, rec, v->feat, v->stream));
+            CU(launch_gather_rec(d, vd, rec, v->feat, v->params.precision != MRP_FP32, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[1], v->stream));
             if (v->params.precision == MRP_FP32) {
                 CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, v->accum, v->stream));
@@ -747,7 +747,7 @@ mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgb
     HitRecords rec = v->records();
     VolumeDev dv = v->dev();
     cudaError_t e = launch_hit(dv, vd, rec, acc, v->stream);
-    if (e == cudaSuccess) e = launch_gather_rec(dv, vd, rec, v->feat, v->stream);
+    if (e == cudaSuccess) e = launch_gather_rec(dv, vd, rec, v->feat, false, v->stream);
     if (e == cudaSuccess) e = launch_mlp_rec_fp32(dv, vd, rec, v->feat, g.d_weights, acc, v->stream);
     if (e == cudaSuccess) e = launch_debug_scatter(rec, v->feat, (int)npix, da, df, v->stream);
     cudaMemcpyKind k = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

@@ -111,7 +111,7 @@ mrp_status mrp_get_radiances(mrp_volume* v, const float* ori, const float* dir, 
         CU(S.scratch(tiled_feature_floats(n) * sizeof(float), (void**)&feat));
         HitRecords rec{rc, rp, rf, (size_t)n};
         CU(launch_hit(d, vd, rec, acc, v->stream));
-        CU(launch_gather_rec(d, vd, rec, feat, v->stream));
+        CU(launch_gather_rec(d, vd, rec, feat, v->params.precision != MRP_FP32, v->stream));
         if (v->params.precision == MRP_FP32) {
             CU(launch_mlp_rec_fp32(d, vd, rec, feat, mrpi::g.d_weights, acc, v->stream));
         } else {

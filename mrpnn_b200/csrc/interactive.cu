@@ -218,7 +218,7 @@ mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_rende
             VolumeDev d = v->dev();
             HitRecords rec = v->records();
             CU(launch_hit(d, vd, rec, v->accum, v->stream));
-            CU(launch_gather_rec(d, vd, rec, v->feat, v->stream));
+            CU(launch_gather_rec(d, vd, rec, v->feat, v->params.precision != MRP_FP32, v->stream));
             if (v->params.precision == MRP_FP32) {
                 CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, v->accum, v->stream));
             } else {

@@ -47,7 +47,10 @@ cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, 
 // GatherData: 773 tile features per tile of a view.width x view.height grid.
 cudaError_t launch_gather_tiles(const VolumeDev& v, const ViewDev& view, int px, int py, const float nl[3], float* out,
                                 cudaStream_t s);
-cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s);
+// fp16 = false: fp32 features (the FP32 network's input); true: fp16 pairs
+// (the tensor-core networks' input, half the bytes), in the same buffer.
+cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, bool fp16,
+                              cudaStream_t s);
 cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitRecords rec, const float* feat,
                                 const float* weights, float4* accum, cudaStream_t s);
 // Scatters records and tiled features to per-pixel layout (debug entry).

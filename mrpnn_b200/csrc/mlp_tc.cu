@@ -21,6 +21,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "kernels.h"
 #include "mlp_tc.h"
 #include "tc_ptx.cuh"
@@ -382,13 +384,17 @@ struct RowFeatures {           // [n][576] row-major
         for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + c * 192 + from + i) : 0.0f;
     }
 };
-struct TileFeatures {          // tiled layout of the staged predictor
-    const float* x;
+struct TileFeatures {          // FP16 pairs of the staged predictor's tiled layout
+    const __half2* x;          // already offset to (r / 32) * 288 * 32 + r % 32
     bool valid;
     template <int W>
     MRP_D void load(int c, int from, float* xs) const {
 #pragma unroll
-        for (int i = 0; i < W; ++i) xs[i] = valid ? __ldg(x + (c * 192 + from + i) * 32) : 0.0f;
+        for (int k = 0; k < W / 2; ++k) {
+            const float2 p = valid ? __half22float2(__ldg(x + (c * 96 + (from >> 1) + k) * 32)) : make_float2(0.0f, 0.0f);
+            xs[2 * k] = p.x;
+            xs[2 * k + 1] = p.y;
+        }
     }
 };
 
@@ -823,7 +829,7 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
             const bool valid = r < *S->rec_count;
             const size_t cap = S->rec_cap;
             float gamma = valid ? S->rec_f[15 * cap + r] : 0.0f;
-            TileFeatures src{S->feat + (size_t)(r >> 5) * 576 * 32 + (r & 31), valid};
+            TileFeatures src{reinterpret_cast<const __half2*>(S->feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31), valid};
             st = tc_network<EB>(G, st, src, aux_s, gamma, S->g, S->sr, o);
             if (valid && !(st & kStFailed)) {
                 int pix = S->rec_pix[r];

@@ -26,7 +26,7 @@ struct TcScratch {
 // running-mean image and the constants of its launch.  The batched launch
 // takes up to kTcMaxSegments of them (each request's tiles stay separate).
 struct TcSegment {
-    const float* feat;
+    const float* feat;           // the gather's FP16-pair tiled features (launch_gather_rec, fp16)
     const int* rec_count;
     const int* rec_pix;
     const float* rec_f;

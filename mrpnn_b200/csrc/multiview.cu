@@ -74,7 +74,7 @@ mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* 
         float4* acc = B.accum + pix_off[i];
         float* ft = B.feat + feat_off[i];
         CU(launch_hit(d, vd, rec, acc, v->stream));
-        CU(launch_gather_rec(d, vd, rec, ft, v->stream));
+        CU(launch_gather_rec(d, vd, rec, ft, tc, v->stream));
         if (tc) segs[i] = tc_segment(d, vd, rec, ft, acc);
         else CU(launch_mlp_rec_fp32(d, vd, rec, ft, g.d_weights, acc, v->stream));
     }

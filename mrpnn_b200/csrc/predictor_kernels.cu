@@ -12,6 +12,8 @@
 // drop-in: one pixel per thread, weights broadcast from L1 (uniform loads).
 #include <cfloat>
 
+#include <cuda_fp16.h>
+
 #include "kernels.h"
 
 namespace mrp {
@@ -268,9 +270,16 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
     *fs_ = tr;
 }
 // All 192 points, run by run (GetSamples23_'s layout: layers 0..7 over the
-// 160 rotated directions, then layers 0..3 on the light ray), into the tiled
-// feature layout.
-MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* out) {
+// 160 rotated directions, then layers 0..3 on the light ray), into a tiled
+// feature layout: fp32 (record r, channel c, sample i at word
+// ((r / 32) * 576 + c * 192 + i) * 32 + r % 32), or FP16 pairs (samples 2k,
+// 2k + 1 of channel c as one half2 at word ((r / 32) * 288 + c * 96 + k) * 32
+// + r % 32).  Either way a warp of 32 records writes 128 contiguous bytes.
+template <bool FP16>
+MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat, int r) {
+    float* out = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
+    __half2* out2 = reinterpret_cast<__half2*>(feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31);
+    float pa = 0.0f, pb = 0.0f, pc = 0.0f;   // the even sample of a pair
 #pragma unroll 1
     for (int run = 0; run < 12; ++run) {
         const int layer = c_stencil_runs[run][0], from = c_stencil_runs[run][1], to = c_stencil_runs[run][2];
@@ -280,9 +289,18 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* out) 
         for (int i = from; i < to; ++i) {
             float a, b, c;
             gather_point_fast(v, f, R, i, &a, &b, &c);
-            out[i * 32] = a;
-            out[(192 + i) * 32] = b;
-            out[(384 + i) * 32] = c;
+            if (!FP16) {
+                out[i * 32] = a;
+                out[(192 + i) * 32] = b;
+                out[(384 + i) * 32] = c;
+            } else if (i & 1) {   // runs start on even samples
+                const int k = i >> 1;
+                out2[k * 32] = __floats2half2_rn(pa, a);
+                out2[(96 + k) * 32] = __floats2half2_rn(pb, b);
+                out2[(192 + k) * 32] = __floats2half2_rn(pc, c);
+            } else {
+                pa = a; pb = b; pc = c;
+            }
         }
     }
 }
@@ -652,11 +670,12 @@ MRP_D PixelFrame record_frame(const HitRecords& rec, int r, f3 L, float g, float
     return pf;
 }
 
+template <bool FP16>
 __global__ void __launch_bounds__(128) k_gather_rec(VolumeDev v, ViewDev w, HitRecords rec, float* __restrict__ feat) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *rec.count) return;
     PixelFrame pf = record_frame(rec, r, normalize(w.light_dir), w.g, w.alpha);
-    gather_all_fast(v, pf, feat + (size_t)(r >> 5) * 576 * 32 + (r & 31));
+    gather_all_fast<FP16>(v, pf, feat, r);
 }
 
 __global__ void __launch_bounds__(128) k_mlp_rec(VolumeDev v, ViewDev w, HitRecords rec, const float* __restrict__ feat,
@@ -954,10 +973,12 @@ cudaError_t launch_gather_tiles(const VolumeDev& v, const ViewDev& view, int px,
     return cudaGetLastError();
 }
 
-cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, cudaStream_t s) {
+cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecords rec, float* feat, bool fp16,
+                              cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;
-    k_gather_rec<<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
+    if (fp16) k_gather_rec<true><<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
+    else k_gather_rec<false><<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
     return cudaGetLastError();
 }
 cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitRecords rec, const float* feat,

@@ -237,7 +237,7 @@ bool mrp_server::admit() {
         HitRecords rec = s.records();
         if ((e = build_tr_levels(s.trs, v->mips, v->mip_occ, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
             (e = launch_hit(s.vd, s.view, rec, s.accum, s.stream)) != cudaSuccess ||
-            (e = launch_gather_rec(s.vd, s.view, rec, s.feat, s.stream)) != cudaSuccess) {
+            (e = launch_gather_rec(s.vd, s.view, rec, s.feat, cfg.precision != MRP_FP32, s.stream)) != cudaSuccess) {
             complete(T, MRP_ERR_CUDA, cuda_msg("request launch", e));
             release(s);
             continue;
