@@ -270,7 +270,8 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
         (e = cudaMalloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->lut, kLut * kLut * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
-        (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess)
+        (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
                             cudaGetErrorString(e)));
     cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
@@ -282,7 +283,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
     cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
-    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
+    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     tc_free_scratch(v->tc);
@@ -297,6 +298,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
 
 static void invalidate(mrp_volume* v) {
     v->has_pyramid = v->has_tr = v->has_baked = false;
+    v->has_bounds = false;
     v->tr_alpha = NAN; v->bk_alpha = NAN;
 }
 
@@ -366,6 +368,14 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         std::memcpy(&v->max_density, &bits, sizeof(float));
     }
     CU(launch_occupancy(v->density, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
+    {
+        const int init[6] = {R, R, R, -1, -1, -1};
+        CU(cudaMemcpyAsync(v->d_bounds, init, sizeof init, cudaMemcpyHostToDevice, v->stream));
+        CU(launch_nonzero_bounds(v->density, R, v->d_bounds, g.sms, v->stream));
+        CU(cudaMemcpyAsync(v->nz_bounds, v->d_bounds, sizeof v->nz_bounds, cudaMemcpyDeviceToHost, v->stream));
+        CU(cudaStreamSynchronize(v->stream));
+        v->has_bounds = true;
+    }
     if (process_mips) {
         // core/volume.cu:1476-1514: halve to the largest power of two >= 256
         // below the input, then 9 levels 256 >> m, each from the previous one.

@@ -109,6 +109,9 @@ struct mrp_volume {
     uint8_t* mip_occ = nullptr;   // bricks of mip levels 0..kOccMips-1
     int occ_shift = 3, occ_res = 0;
     int* d_maxbits = nullptr;
+    int* d_bounds = nullptr;      // nonzero-voxel index bounds (6 ints) of the last update
+    int nz_bounds[6] = {0, 0, 0, -1, -1, -1};
+    bool has_bounds = false;
     bool has_data = false, has_pyramid = false, has_lut = false, has_tr = false, has_baked = false;
     bool max_override = false;
     float max_density = 0.00001f;
@@ -155,6 +158,17 @@ struct mrp_volume {
         d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};
         d.nee_mode = params.nee_mode;
         d.mip_occ = has_pyramid ? mip_occ : nullptr;
+        d.has_bounds = has_bounds ? 1 : 0;
+        if (has_bounds) {
+            // Density() at p reads base voxel floor((p + 0.5) R - 0.5) and the
+            // next one: nonzero only for base voxels in [min - 1, max]; one
+            // voxel of margin more on each side covers any rounding
+            const float R = (float)res;
+            d.nz_lo = {(nz_bounds[0] - 1.5f) / R - 0.5f, (nz_bounds[1] - 1.5f) / R - 0.5f,
+                       (nz_bounds[2] - 1.5f) / R - 0.5f};
+            d.nz_hi = {(nz_bounds[3] + 2.5f) / R - 0.5f, (nz_bounds[4] + 2.5f) / R - 0.5f,
+                       (nz_bounds[5] + 2.5f) / R - 0.5f};
+        }
         return d;
     }
 };

@@ -300,6 +300,11 @@ struct VolumeDev {
     f3 sky;
     int nee_mode;           // tracer NEE: 0 baked grid (reference), 1 one Tr() estimate per vertex
     const uint8_t* mip_occ; // occupancy of mip levels 0..kOccMips-1 (8^3 bricks, offsets mip_occ_offset)
+    // Box (world coordinates) outside which Density() is exactly 0: the
+    // nonzero voxels' bounds grown by the fetch footprint and one voxel more
+    // (lo > hi for an all-zero grid); has_bounds = 0 when not computed.
+    f3 nz_lo, nz_hi;
+    int has_bounds;
 };
 
 // ---------------------------------------------------------------------------

@@ -10,6 +10,9 @@ cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int oc
 cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s);
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s);
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
+// Index bounds of the nonzero voxels: out6 = {min x, min y, min z, max x,
+// max y, max z}, which must start at {R, R, R, -1, -1, -1}.
+cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s);
 cudaError_t launch_tr_level(float* out, int res, const float* src, const uint8_t* src_occ, float alpha, const float L[3], int sms,
                             cudaStream_t s);
 cudaError_t set_halton_permutations(const uint32_t perm[28]);

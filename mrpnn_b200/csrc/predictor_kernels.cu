@@ -99,6 +99,36 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
     float t_step = fd(2.0f, rf), empty_step = fd(1.0f, rf);
     const MarchRay mr = march_ray(v, pos, dir);
     int loop = 0;
+    if (v.has_bounds) {
+        // Up to where the ray enters the box outside which Density() is 0,
+        // every step reads 0 and only advances t by empty_step (last_dens,
+        // prob and last_non_empty_t stay at their initial values), so those
+        // steps are replayed as additions alone, in the same float order.
+        float t0 = 0.0f, t1 = dis;
+        const float o[3] = {pos.x, pos.y, pos.z}, dd[3] = {dir.x, dir.y, dir.z};
+        const float lo[3] = {v.nz_lo.x, v.nz_lo.y, v.nz_lo.z}, hi[3] = {v.nz_hi.x, v.nz_hi.y, v.nz_hi.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (dd[a] == 0.0f) {
+                if (o[a] < lo[a] || o[a] > hi[a]) t0 = 3.0e38f;
+            } else {
+                const float ta = (lo[a] - o[a]) / dd[a], tb = (hi[a] - o[a]) / dd[a];
+                t0 = fmaxf(t0, fminf(ta, tb));
+                t1 = fminf(t1, fmaxf(ta, tb));
+            }
+        }
+        const bool never = t0 > t1;   // the march segment [0, dis] stays where the density is 0
+        if (never && !tl) {           // it would step until t > dis and report no hit
+            *next = mk3(0, 0, 0);
+            return false;
+        }
+        const float t_enter = never ? 3.0e38f : t0;
+        while (loop < 10000 && t <= dis && t < t_enter) {
+            ++loop;
+            if (tl) tl->steps++;
+            t = fa(t, empty_step);
+        }
+    }
     while (loop++ < 10000) {
         if (t > dis) {
             if (last_non_empty_t != 0.0f) { t = last_non_empty_t; break; }

@@ -102,6 +102,35 @@ __global__ void k_max_density(const float* __restrict__ d, size_t n, int* __rest
     if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_int(m));
 }
 
+// One warp per grid row (x, y): the lanes scan z, the warp keeps the bounds
+// of the nonzero voxels it saw and adds them with six atomics at the end.
+__global__ void k_nonzero_bounds(const float* __restrict__ d, int R, int* __restrict__ out6) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+    int lo[3] = {R, R, R}, hi[3] = {-1, -1, -1};
+    for (long long row = blockIdx.x * (long long)(blockDim.x / 32) + threadIdx.x / 32; row < (long long)R * R;
+         row += warps) {
+        const float* p = d + row * R;
+        int zlo = R, zhi = -1;
+        for (int z = lane; z < R; z += 32)
+            if (__ldg(p + z) != 0.0f) { zlo = min(zlo, z); zhi = max(zhi, z); }
+        zlo = __reduce_min_sync(0xffffffffu, zlo);
+        zhi = __reduce_max_sync(0xffffffffu, zhi);
+        if (zhi >= 0) {
+            const int x = (int)(row / R), y = (int)(row % R);
+            lo[0] = min(lo[0], x); hi[0] = max(hi[0], x);
+            lo[1] = min(lo[1], y); hi[1] = max(hi[1], y);
+            lo[2] = min(lo[2], zlo); hi[2] = max(hi[2], zhi);
+        }
+    }
+    if (lane == 0 && hi[0] >= 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(out6 + a, lo[a]);
+            atomicMax(out6 + 3 + a, hi[a]);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Occupancy bricks for exact empty-space skipping in the first-hit march.
 // Brick b covers voxels [b*B, b*B + B) per axis.  A trilinear fetch whose
@@ -290,6 +319,12 @@ cudaError_t launch_resample(float* out, int res, const float* src, int src_res, 
 }
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s) {
     k_max_density<<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
+    return cudaGetLastError();
+}
+cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s) {
+    long long rows = (long long)R * R;
+    int blocks = (int)((rows + 7) / 8 < sms * 16 ? (rows + 7) / 8 : sms * 16);
+    k_nonzero_bounds<<<blocks, 256, 0, s>>>(d, R, out6);
     return cudaGetLastError();
 }
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s) {
