@@ -164,3 +164,44 @@ def test_predict_intermediates(scene):
     np.testing.assert_allclose(aux[hit, 4], r_gamma[hit], rtol=0, atol=2e-5, err_msg="gamma")
     np.testing.assert_allclose(feat[hit], r_feat[hit], rtol=1e-5, atol=1e-6, err_msg="features")
     np.testing.assert_allclose(rgba, r_rgba, rtol=MLP_RTOL, atol=MLP_ATOL, err_msg="rgba")
+
+
+@pytest.mark.parametrize("case", ["empty", "corner", "full_face", "sdf"])
+def test_first_hit_empty_space_replay(case):
+    """The march replays its steps in front of the box of nonzero voxels as
+    additions alone and drops rays that never reach it; the hits must stay
+    those of the oracle's full march: an all-zero grid, one dense corner
+    block, density touching a face of the grid, and negative (SDF) values."""
+    import mrpnn_b200 as M
+    M.init()
+    R = 48
+    grid = np.zeros((R, R, R), np.float32)
+    if case == "corner":
+        grid[R - 6:, R - 6:, R - 6:] = 1.0
+    elif case == "full_face":
+        grid[:, :, 0:5] = 0.8
+    elif case == "sdf":
+        grid[10:30, 12:30, 14:30] = -0.02
+        grid[18:22, 18:22, 18:22] = 1.0
+    vol = M.VolumeRender(R)
+    vol.set_data(grid)
+    vol.Update()
+    alpha = 64.0
+    rng = np.random.default_rng(7)
+    n = 3000
+    ori = (np.array([0.75, 0.75, 0.75]) + rng.normal(0, 0.1, (n, 3))).astype(np.float32)
+    d = (-ori + rng.normal(0, 0.3, (n, 3))).astype(np.float32)
+    got = vol.first_hit(ori, d, alpha)
+    sc = O.SceneBuf(vol.read(M.api.RES_DENSITY), R, vol.max_density)
+    L = O.lib()
+    ref = np.zeros((n, 4), np.float32)
+    h = np.zeros(3, np.float32)
+    for i in range(n):
+        ref[i, 3] = L.orc_first_hit(C.byref(sc.c), ori[i], d[i], alpha, h)
+        ref[i, :3] = h
+    np.testing.assert_array_equal(got[:, 3], ref[:, 3])
+    if case == "empty":
+        assert ref[:, 3].sum() == 0
+    else:
+        assert ref[:, 3].sum() > 0
+    np.testing.assert_allclose(got[:, :3], ref[:, :3], rtol=0, atol=2e-6)
