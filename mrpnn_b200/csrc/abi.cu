@@ -271,7 +271,9 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
         (e = cudaMalloc(&v->lut, kLut * kLut * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
         (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess ||
-        (e = cudaMalloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess)
+        (e = cudaMalloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&v->mips_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v->trs_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
                             cudaGetErrorString(e)));
     cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
@@ -283,7 +285,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
     cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
-    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
+    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->mips_pad); cudaFree(v->trs_pad); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     tc_free_scratch(v->tc);
@@ -403,6 +405,8 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         for (int m = 0; m < kOccMips; ++m)
             CU(launch_occupancy(v->mips + mip_offset(m), 256 >> m, 3, 32 >> m, v->mip_occ + mip_occ_offset(m), g.sms,
                                 v->stream));
+        CU(launch_pad_levels(v->mips + mip_offset(5), v->mips + mip_offset(6), v->mips + mip_offset(7), false,
+                             v->mips_pad, v->stream));
         CU(cudaStreamSynchronize(v->stream));
         cudaFree(tmp[0]);
         cudaFree(tmp[1]);
@@ -510,6 +514,8 @@ mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
     if (v->has_tr && v->tr_alpha == alpha && v->tr_light[0] == L[0] && v->tr_light[1] == L[1] && v->tr_light[2] == L[2])
         return MRP_OK;
     CU(build_tr_levels(v->trs, v->mips, v->mip_occ, L, alpha, v->stream));
+    CU(launch_pad_levels(v->trs + tr_offset(4), v->trs + tr_offset(5), v->trs + tr_offset(6), true, v->trs_pad,
+                         v->stream));
     v->has_tr = true;
     v->tr_alpha = alpha;
     std::memcpy(v->tr_light, L, sizeof v->tr_light);

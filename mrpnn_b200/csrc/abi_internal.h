@@ -109,6 +109,8 @@ struct mrp_volume {
     uint8_t* mip_occ = nullptr;   // bricks of mip levels 0..kOccMips-1
     int occ_shift = 3, occ_res = 0;
     int* d_maxbits = nullptr;
+    float* mips_pad = nullptr;    // padded mips 5..7 (pad_offset layout), built with the pyramid
+    float* trs_pad = nullptr;     // padded TR levels 4..6, built with the TR levels
     int* d_bounds = nullptr;      // nonzero-voxel index bounds (6 ints) of the last update
     int nz_bounds[6] = {0, 0, 0, -1, -1, -1};
     bool has_bounds = false;
@@ -158,6 +160,8 @@ struct mrp_volume {
         d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};
         d.nee_mode = params.nee_mode;
         d.mip_occ = has_pyramid ? mip_occ : nullptr;
+        d.mips_pad = has_pyramid ? mips_pad : nullptr;
+        d.trs_pad = has_tr ? trs_pad : nullptr;
         d.has_bounds = has_bounds ? 1 : 0;
         if (has_bounds) {
             // Density() at p reads base voxel floor((p + 0.5) R - 0.5) and the

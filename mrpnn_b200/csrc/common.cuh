@@ -208,6 +208,31 @@ MRP_D float lerp_fast(float a, float b, float v) { return fmaf(v, b - a, a); }
 // n^3 must stay below 2^31 (the pyramid and TR levels: n <= 256): 32-bit
 // offsets.  Footprints inside the grid (the common case) skip the clamps and
 // the border selects.
+// tex3_fast on a padded level (pad_offset): the texel coordinate is clamped
+// to [-1, n] per axis, after which every footprint lies inside the padded
+// grid, so there is no branch and no per-texel clamp or border select.  The
+// value is tex3_fast's: beyond -1 (or n) both texels of an axis hold the same
+// margin value, and lerp_fast(a, a, w) = a for every weight, so moving the
+// coordinate to the margin (weight 0) changes nothing.
+MRP_D float tex3_padded(const float* __restrict__ g, int n, f3 pos) {
+    const float nf = (float)n;
+    float px = fmaf(pos.x + 0.5f, nf, -0.5f), py = fmaf(pos.y + 0.5f, nf, -0.5f), pz = fmaf(pos.z + 0.5f, nf, -0.5f);
+    px = fminf(fmaxf(px, -1.0f), nf);
+    py = fminf(fmaxf(py, -1.0f), nf);
+    pz = fminf(fmaxf(pz, -1.0f), nf);
+    const float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
+    const int P = n + 3;
+    const int x = (int)flx + 1, y = (int)fly + 1, z = (int)flz + 1;
+    const float wx = px - flx, wy = py - fly, wz = pz - flz;
+    const float* b = g + (x * P + y) * P + z;
+    const int PP = P * P;
+    const float t000 = __ldg(b), t001 = __ldg(b + 1), t010 = __ldg(b + P), t011 = __ldg(b + P + 1);
+    const float t100 = __ldg(b + PP), t101 = __ldg(b + PP + 1), t110 = __ldg(b + PP + P), t111 = __ldg(b + PP + P + 1);
+    const float c00 = lerp_fast(t000, t001, wz), c01 = lerp_fast(t010, t011, wz);
+    const float c10 = lerp_fast(t100, t101, wz), c11 = lerp_fast(t110, t111, wz);
+    return lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+}
+
 template <bool Clamp>
 MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float nf = (float)n;
@@ -305,7 +330,18 @@ struct VolumeDev {
     // (lo > hi for an all-zero grid); has_bounds = 0 when not computed.
     f3 nz_lo, nz_hi;
     int has_bounds;
+    // Padded copies of the small levels (edge 8, 4, 2: mips 5..7, TR levels
+    // 4..6) for the stencil gather, or null: see pad_offset / tex3_padded.
+    const float* mips_pad;
+    const float* trs_pad;
 };
+// A level of edge n (n <= 8) stored with one texel of margin below and two
+// above per axis, (n + 3)^3 floats, texel (x, y, z) at ((x + 1) P + y + 1) P
+// + z + 1 (P = n + 3).  The margin holds what the fetch reads outside the
+// grid: 0 (border addressing, the density mips) or the nearest edge texel
+// (clamp addressing, the TR levels).  Levels of edge 8, 4, 2 in that order.
+constexpr int kPadLevelFloats = 11 * 11 * 11 + 7 * 7 * 7 + 5 * 5 * 5;
+MRP_HD int pad_offset(int n) { return n == 8 ? 0 : n == 4 ? 11 * 11 * 11 : 11 * 11 * 11 + 7 * 7 * 7; }
 
 // ---------------------------------------------------------------------------
 // Empty-space skipping that keeps every result bit-identical: an 8^3 brick

@@ -10,6 +10,10 @@ cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int oc
 cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s);
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s);
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
+// Padded copies (pad_offset layout, kPadLevelFloats floats) of three levels
+// of edge 8, 4, 2; clamp: TR-level addressing, else border (density mips).
+cudaError_t launch_pad_levels(const float* l8, const float* l4, const float* l2, bool clamp, float* out,
+                              cudaStream_t s);
 // Index bounds of the nonzero voxels: out6 = {min x, min y, min z, max x,
 // max y, max z}, which must start at {R, R, R, -1, -1, -1}.
 cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s);

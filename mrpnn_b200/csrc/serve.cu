@@ -232,6 +232,7 @@ bool mrp_server::admit() {
         s.t = T;
         s.vd = v->dev();
         s.vd.trs = s.trs;
+        s.vd.trs_pad = nullptr;   // the slot's own TR levels have no padded copy
         s.vd.lut = lut->d;
         s.view = make_view(v, &w, w.frame_offset, 0);
         HitRecords rec = s.records();

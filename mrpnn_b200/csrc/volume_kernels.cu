@@ -102,6 +102,28 @@ __global__ void k_max_density(const float* __restrict__ d, size_t n, int* __rest
     if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_int(m));
 }
 
+// Padded copies of three levels of edge 8, 4, 2 (blockIdx.y picks one): the
+// texel of (x, y, z) in [-1, n + 1]^3 is the level's texel under border
+// addressing (0 outside) or clamp addressing (nearest edge texel).
+__global__ void k_pad_levels(const float* __restrict__ l8, const float* __restrict__ l4, const float* __restrict__ l2,
+                             int clamp, float* __restrict__ out) {
+    const int n = 8 >> blockIdx.y, P = n + 3;
+    const float* src = blockIdx.y == 0 ? l8 : blockIdx.y == 1 ? l4 : l2;
+    float* dst = out + pad_offset(n);
+    for (int i = threadIdx.x; i < P * P * P; i += blockDim.x) {
+        int x = i / (P * P) - 1, y = (i / P) % P - 1, z = i % P - 1;
+        float val;
+        if (clamp) {
+            x = min(max(x, 0), n - 1); y = min(max(y, 0), n - 1); z = min(max(z, 0), n - 1);
+            val = src[(x * n + y) * n + z];
+        } else {
+            const bool in = (unsigned)x < (unsigned)n && (unsigned)y < (unsigned)n && (unsigned)z < (unsigned)n;
+            val = in ? src[(x * n + y) * n + z] : 0.0f;
+        }
+        dst[i] = val;
+    }
+}
+
 // One warp per grid row (x, y): the lanes scan z, the warp keeps the bounds
 // of the nonzero voxels it saw and adds them with six atomics at the end.
 __global__ void k_nonzero_bounds(const float* __restrict__ d, int R, int* __restrict__ out6) {
@@ -319,6 +341,11 @@ cudaError_t launch_resample(float* out, int res, const float* src, int src_res, 
 }
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s) {
     k_max_density<<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
+    return cudaGetLastError();
+}
+cudaError_t launch_pad_levels(const float* l8, const float* l4, const float* l2, bool clamp, float* out,
+                              cudaStream_t s) {
+    k_pad_levels<<<dim3(1, 3), 256, 0, s>>>(l8, l4, l2, clamp ? 1 : 0, out);
     return cudaGetLastError();
 }
 cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s) {
