@@ -268,7 +268,7 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
     if ((e = cudaMalloc(&v->density, n * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->mips, kMipFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->lut, kLut * kLut * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v->lut, kLutAlloc * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
         (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess ||
         (e = cudaMalloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess ||
@@ -504,6 +504,7 @@ namespace mrpi {
 mrp_status update_lut_async(mrp_volume* v, float g_) {
     if (v->has_lut && v->lut_g == g_ && v->lut_seed == v->params.seed) return MRP_OK;
     CU(launch_hg_lut(v->lut, g_, v->params.seed, v->stream));
+    CU(launch_lut_dirs(v->lut, v->lut + kLut * kLut, v->stream));
     v->has_lut = true;
     v->lut_g = g_;
     v->lut_seed = v->params.seed;

@@ -162,6 +162,7 @@ struct mrp_volume {
         d.mip_occ = has_pyramid ? mip_occ : nullptr;
         d.mips_pad = has_pyramid ? mips_pad : nullptr;
         d.trs_pad = has_tr ? trs_pad : nullptr;
+        d.lut_dirs = has_lut ? lut + mrp::kLut * mrp::kLut : nullptr;
         d.has_bounds = has_bounds ? 1 : 0;
         if (has_bounds) {
             // Density() at p reads base voxel floor((p + 0.5) R - 0.5) and the

@@ -270,6 +270,7 @@ MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
 }
 
 constexpr int kLut = 512;
+constexpr int kLutAlloc = kLut * kLut + 160;   // the LUT and its lut_dirs table
 MRP_D float tex_lut(const float* __restrict__ lut, float u, float v) {
     float px = fs(fm(u, (float)kLut), 0.5f), py = fs(fm(v, (float)kLut), 0.5f);
     int x = (int)floorf(px), y = (int)floorf(py);
@@ -334,6 +335,10 @@ struct VolumeDev {
     // 4..6) for the stencil gather, or null: see pad_offset / tex3_padded.
     const float* mips_pad;
     const float* trs_pad;
+    // 160 HG-LUT values of the rotated stencil points' own direction (the
+    // first LUT factor of X_Hg, which depends only on the point and g), or
+    // null; stored right after the LUT (kLutAlloc floats per LUT buffer).
+    const float* lut_dirs;
 };
 // A level of edge n (n <= 8) stored with one texel of margin below and two
 // above per axis, (n + 3)^3 floats, texel (x, y, z) at ((x + 1) P + y + 1) P

@@ -32,6 +32,9 @@ struct StencilTables {
     float dirs[160 * 3];
 };
 cudaError_t set_stencil_tables(const StencilTables& t);
+// lut_dirs (160 floats) of the LUT at lut (the table VolumeDev::lut_dirs
+// points at), after the LUT is built on the same stream.
+cudaError_t launch_lut_dirs(const float* lut, float* out, cudaStream_t s);
 // features: [n][576] (X_Val, X_Val_Sub, X_Val_Hg), gamma [n]
 cudaError_t launch_gather(const VolumeDev& v, const float* pos, const float* bases, const float* light, float g,
                           float alpha, int n, float* feat, float* gamma, cudaStream_t s);

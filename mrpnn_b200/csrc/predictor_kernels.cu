@@ -11,6 +11,7 @@
 // where a transcendental's last bit differs.  The MLP here is the plain FP32
 // drop-in: one pixel per thread, weights broadcast from L1 (uniform loads).
 #include <cfloat>
+#include <cmath>
 
 #include <cuda_fp16.h>
 
@@ -26,6 +27,7 @@ __constant__ float c_offset[192];
 __constant__ int c_layer[192];
 __constant__ float c_lutv[192];
 __constant__ float c_dirs[160 * 3];
+__constant__ float c_udirs[160 * 3];   // the same directions normalised (host, double precision)
 
 // The 192 points as the runs of GetSamples23_'s layout: layers 0..7 over the
 // 160 rotated directions (8, 8, 16, 16, 16, 32, 32, 32 points), then layers
@@ -46,6 +48,17 @@ cudaError_t set_stencil_tables(const StencilTables& t) {
     if ((e = cudaMemcpyToSymbol(c_offset, t.offset, sizeof t.offset)) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_layer, t.layer, sizeof t.layer)) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_lutv, t.lut_v, sizeof t.lut_v)) != cudaSuccess) return e;
+    float ud[160 * 3];
+    for (int i = 0; i < 160; ++i) {
+        double x = t.dirs[3 * i], y = t.dirs[3 * i + 1], z = t.dirs[3 * i + 2];
+        double l = std::sqrt(x * x + y * y + z * z);
+        if (!(l > 0)) {   // the hit point itself (point 0, whose X_Hg is HG(X . L))
+            if (i != 0) return cudaErrorInvalidValue;
+            l = 1.0;
+        }
+        ud[3 * i] = (float)(x / l); ud[3 * i + 1] = (float)(y / l); ud[3 * i + 2] = (float)(z / l);
+    }
+    if ((e = cudaMemcpyToSymbol(c_udirs, ud, sizeof ud)) != cudaSuccess) return e;
     return cudaMemcpyToSymbol(c_dirs, t.dirs, sizeof t.dirs);
 }
 
@@ -252,6 +265,35 @@ MRP_D void gather_sample(const VolumeDev& v, const PixelFrame& f, int i, float* 
 // The same stencil point with contracted arithmetic (FMA positions and
 // lerps, rsqrt direction), used by the staged gather of the render path:
 // the features stay within 1e-5 relative of gather_sample.
+// The fp16 path's per-record constants of X_Hg.  A rotated point's
+// direction from the hit is X px + Y py + Z pz for its unit stencil
+// direction (px, py, pz), so its cosine with X is px (a per-point constant:
+// its LUT factor is lut_dirs[i]) and its cosine with LX is q . (px, py, pz),
+// q = (LX.X, LX.Y, LX.Z); a light-ray point's direction is L itself.  The
+// exact form normalises cur - pos; the two differ by rounding (< 1e-6 in
+// the cosine), far below an fp16 step of the feature.
+struct HgFast {
+    f3 q;
+    float u1L, u2L;          // LUT coordinates of the light-ray points
+    const float* lut_dirs;   // null: compute X_Hg the exact way
+};
+MRP_D HgFast hg_fast(const VolumeDev& v, const PixelFrame& f) {
+    HgFast h;
+    h.q = mk3(dot(f.LX, f.X), dot(f.LX, f.Y), dot(f.LX, f.Z));
+    h.u1L = fmaf(dot(f.X, f.L), 0.5f, 0.5f);
+    h.u2L = fmaf(dot(f.LX, f.L), 0.5f, 0.5f);
+    h.lut_dirs = v.lut_dirs;
+    return h;
+}
+__global__ void k_lut_dirs(const float* __restrict__ lut, float* __restrict__ out) {
+    int i = threadIdx.x;
+    if (i < 160) out[i] = tex_lut_fast(lut, fmaf(c_udirs[3 * i], 0.5f, 0.5f), c_lutv[i]);
+}
+cudaError_t launch_lut_dirs(const float* lut, float* out, cudaStream_t s) {
+    k_lut_dirs<<<1, 160, 0, s>>>(lut, out);
+    return cudaGetLastError();
+}
+
 // Stencil point i with the sizes and levels of its run hoisted by the
 // caller: mip level m (n^3 texels), TR level (tn^3), and whether the point
 // lies on the light ray (i >= 160) rather than along a rotated direction.
@@ -269,8 +311,8 @@ template <bool FP16>
 MRP_D float feature_log(float x) { return FP16 ? __logf(x) : logf(x); }
 
 template <bool FP16>
-MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunLevels& R, int i, float* fd_, float* fs_,
-                             float* fh_) {
+MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunLevels& R, const HgFast& H, int i,
+                             float* fd_, float* fs_, float* fh_) {
     const float off = c_offset[i];
     f3 d;   // offset from the point
     if (!R.light) {
@@ -285,6 +327,18 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
     *fd_ = feature_log<FP16>(fmaf(f.alpha * dens, 0.015625f, 1.0f));
     if (i == 0) {
         *fh_ = feature_log<FP16>(hg(dot(f.X, f.L), f.g) + 1.0f);
+    } else if (FP16 && H.lut_dirs) {
+        const float lv = c_lutv[i];
+        float a, b;
+        if (!R.light) {
+            const float c2 = fmaf(H.q.z, c_udirs[3 * i + 2], fmaf(H.q.y, c_udirs[3 * i + 1], H.q.x * c_udirs[3 * i]));
+            a = __ldg(H.lut_dirs + i);
+            b = tex_lut_fast(v.lut, fmaf(c2, 0.5f, 0.5f), lv);
+        } else {
+            a = tex_lut_fast(v.lut, H.u1L, lv);
+            b = tex_lut_fast(v.lut, H.u2L, lv);
+        }
+        *fh_ = feature_log<FP16>(fmaf(a, b, 1.0f));
     } else {
         f3 ms = mk3(cur.x - f.pos.x, cur.y - f.pos.y, cur.z - f.pos.z);
         float rl = rsqrtf(fmaf(ms.z, ms.z, fmaf(ms.y, ms.y, ms.x * ms.x)));
@@ -319,6 +373,7 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
     float* out = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
     __half2* out2 = reinterpret_cast<__half2*>(feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31);
     float pa = 0.0f, pb = 0.0f, pc = 0.0f;   // the even sample of a pair
+    const HgFast H = FP16 ? hg_fast(v, f) : HgFast{mk3(0, 0, 0), 0.0f, 0.0f, nullptr};
 #pragma unroll 1
     for (int run = 0; run < 12; ++run) {
         const int layer = c_stencil_runs[run][0], from = c_stencil_runs[run][1], to = c_stencil_runs[run][2];
@@ -332,7 +387,7 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
 #pragma unroll 1
         for (int i = from; i < to; ++i) {
             float a, b, c;
-            gather_point_fast<FP16>(v, f, R, i, &a, &b, &c);
+            gather_point_fast<FP16>(v, f, R, H, i, &a, &b, &c);
             if (!FP16) {
                 out[i * 32] = a;
                 out[(192 + i) * 32] = b;

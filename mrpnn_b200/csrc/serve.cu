@@ -67,7 +67,7 @@ size_t slot_bytes(size_t npix) {
     return kTrFloats * sizeof(float) + sizeof(int) + npix * (sizeof(int) + 16 * sizeof(float) + sizeof(float4)) +
            tiled_feature_floats(npix) * sizeof(float);
 }
-constexpr size_t kLutBytes = 512 * 512 * sizeof(float);
+constexpr size_t kLutBytes = kLutAlloc * sizeof(float);   // the LUT and its lut_dirs table
 
 struct Lut {
     float g;
@@ -175,7 +175,8 @@ const Lut* mrp_server::lut_for(float g_, uint32_t seed, cudaStream_t s, std::str
     cudaError_t e;
     if ((e = cudaMalloc(&l.d, kLutBytes)) != cudaSuccess) { *err = cuda_msg("LUT", e); return nullptr; }
     if ((e = cudaEventCreateWithFlags(&l.ready, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = launch_hg_lut(l.d, g_, seed, s)) != cudaSuccess || (e = cudaEventRecord(l.ready, s)) != cudaSuccess) {
+        (e = launch_hg_lut(l.d, g_, seed, s)) != cudaSuccess ||
+        (e = launch_lut_dirs(l.d, l.d + kLut * kLut, s)) != cudaSuccess || (e = cudaEventRecord(l.ready, s)) != cudaSuccess) {
         cudaFree(l.d);
         if (l.ready) cudaEventDestroy(l.ready);
         *err = cuda_msg("LUT", e);
@@ -234,6 +235,7 @@ bool mrp_server::admit() {
         s.vd.trs = s.trs;
         s.vd.trs_pad = nullptr;   // the slot's own TR levels have no padded copy
         s.vd.lut = lut->d;
+        s.vd.lut_dirs = lut->d + kLut * kLut;
         s.view = make_view(v, &w, w.frame_offset, 0);
         HitRecords rec = s.records();
         if ((e = build_tr_levels(s.trs, v->mips, v->mip_occ, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
