@@ -597,12 +597,17 @@ def run_mine(args, rank, world, local):
     elif stage_bytes_per_hit(args.precision)[dom] is not None:
         alg = active * stage_bytes_per_hit(args.precision)[dom]
         achieved = alg / (st[dom] / 1000.0) / 1e9
+        dram = traffic / (st[dom] / 1000.0) / 1e9 if traffic else None
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": STAGES[dom],
-                "note": f"algorithmic bytes = {stage_bytes_per_hit(args.precision)[dom]} B x {active} hit pixels per launch; "
-                        f"duration = CUDA events around the stage; peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs); "
-                        f"the texel reads are served from L1/L2 (the 64 MiB mip-0 level and the TR levels), so "
-                        f"algorithmic bytes can exceed what DRAM moves: traffic is the ncu DRAM bytes per launch"}
+                "dram_achieved": dram, "dram_frac": dram / hbm if dram else None,
+                "note": f"algorithmic bytes = {stage_bytes_per_hit(args.precision)[dom]} B x {active} hit pixels per launch "
+                        f"(every texel the stencil's trilinear and bilinear fetches read, plus the features written); "
+                        f"duration = CUDA events around the stage; peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs).  "
+                        f"The texel reads are served from L1/L2 (the 64 MiB mip-0 level and the TR levels), so "
+                        f"algorithmic bytes exceed what DRAM moves and frac can pass 1: traffic is the ncu DRAM bytes "
+                        f"per launch and dram_frac what DRAM actually carries; the kernel is issue-bound "
+                        f"(profiles/k_gather_rec_512x512.md)"}
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": traffic,
                 "kernel": STAGES[dom], "note": "march lookups are data dependent; see profiles/"}
