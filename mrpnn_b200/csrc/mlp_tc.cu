@@ -341,20 +341,35 @@ MRP_D float wl(const float* __restrict__ w, int i) { return __ldg(w + i); }
 MRP_D float sigmoid_d(float o) { return 1.0f / (1.0f + __expf(-o)); }
 
 // relu(D * scale + b) for N columns of layer L (runtime), in place.
+// The constants live in shared memory but reach the routines as a generic
+// pointer; reading them with shared-space loads (the address converted once
+// per access) keeps them off the generic load path, whose results the
+// scheduler tracks like global loads.
+MRP_D float4 lds4(const float* p) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+MRP_D float lds1(const float* p) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+
 // Biases and scales start on 16-float boundaries (scale_off), so they are
 // read four at a time.
 template <int EB, int N>
 MRP_D void bias_relu(float* d, int L, float rs, const float* aux) {
     static_assert(N % 4 == 0, "layer widths are multiples of 4");
     const int ab = c_layer_desc[L].abias, so = c_layer_desc[L].soff;
-    const float4* b4 = reinterpret_cast<const float4*>(aux + ab);
-    const float4* s4 = reinterpret_cast<const float4*>(aux + kAuxScale + so);
 #pragma unroll
     for (int q = 0; q < N / 4; ++q) {
-        const float4 b = b4[q];
+        const float4 b = lds4(aux + ab + 4 * q);
         float4 sc = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         if (EB == 1) {
-            const float4 w = s4[q];
+            const float4 w = lds4(aux + kAuxScale + so + 4 * q);
             sc = make_float4(rs * w.x, rs * w.y, rs * w.z, rs * w.w);
         }
         d[4 * q] = fmaxf(fmaf(d[4 * q], sc.x, b.x), 0.0f);
@@ -366,10 +381,9 @@ MRP_D void bias_relu(float* d, int L, float rs, const float* aux) {
 // n consecutive constants (16-byte aligned, n a multiple of 4) into registers.
 template <int N>
 MRP_D void aux_row(const float* aux, int off, float* out) {
-    const float4* p = reinterpret_cast<const float4*>(aux + off);
 #pragma unroll
     for (int q = 0; q < N / 4; ++q) {
-        const float4 v = p[q];
+        const float4 v = lds4(aux + off + 4 * q);
         out[4 * q] = v.x; out[4 * q + 1] = v.y; out[4 * q + 2] = v.z; out[4 * q + 3] = v.w;
     }
 }
@@ -594,9 +608,9 @@ __device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux,
 #pragma unroll
     for (int o = 0; o < 16; ++o) {
         float a = h[o];
-        a = fmaf(aux[kAuxLSE1 + 16 * 72 + o], g, a);
-        a = fmaf(aux[kAuxLSE1 + 16 * 73 + o], gamma, a);
-        a = fmaf(aux[kAuxLSE1 + 16 * 74 + o], s4, a);
+        a = fmaf(lds1(aux + kAuxLSE1 + 16 * 72 + o), g, a);
+        a = fmaf(lds1(aux + kAuxLSE1 + 16 * 73 + o), gamma, a);
+        a = fmaf(lds1(aux + kAuxLSE1 + 16 * 74 + o), s4, a);
         h[o] = fmaxf(a, 0.0f);
     }
 #pragma unroll
@@ -621,10 +635,10 @@ __device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux,
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
         float a = 0.0f;
-        a = fmaf(g, aux[kAuxLGGSW + o * 3], a);
-        a = fmaf(gamma, aux[kAuxLGGSW + o * 3 + 1], a);
-        a = fmaf(s4, aux[kAuxLGGSW + o * 3 + 2], a);
-        x[120 + o] = fmaxf(a + aux[kAuxLGGSB + o], 0.0f);
+        a = fmaf(g, lds1(aux + kAuxLGGSW + o * 3), a);
+        a = fmaf(gamma, lds1(aux + kAuxLGGSW + o * 3 + 1), a);
+        a = fmaf(s4, lds1(aux + kAuxLGGSW + o * 3 + 2), a);
+        x[120 + o] = fmaxf(a + lds1(aux + kAuxLGGSB + o), 0.0f);
     }
     float r = write_row<EB, 128, kpad(kLC0, EB)>(G.a_s, 0, G.t, x);
     st = mma_round<EB>(G, st, 1, kLC0, 0, 0, 0);
@@ -650,8 +664,8 @@ __device__ __noinline__ TailOut tc_tail(const Group G, int st, const float* aux,
     tmem_get<16>(G, kColA16, a16);
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 16; ++j) a = fmaf(a16[j], aux[kAuxLX12W + j], a);
-    return TailOut{fmaxf(a + aux[kAuxLX12B], 0.0f), st};
+    for (int j = 0; j < 16; ++j) a = fmaf(a16[j], lds1(aux + kAuxLX12W + j), a);
+    return TailOut{fmaxf(a + lds1(aux + kAuxLX12B), 0.0f), st};
 }
 
 
