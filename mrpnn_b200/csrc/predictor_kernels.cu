@@ -112,6 +112,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
     float t_step = fd(2.0f, rf), empty_step = fd(1.0f, rf);
     const MarchRay mr = march_ray(v, pos, dir);
     int loop = 0;
+    float t_exit = 3.0e38f;   // beyond it (and within dis) every step reads 0
     if (v.has_bounds) {
         // Up to where the ray enters the box outside which Density() is 0,
         // every step reads 0 and only advances t by empty_step (last_dens,
@@ -136,6 +137,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
             return false;
         }
         const float t_enter = never ? 3.0e38f : t0;
+        if (!never) t_exit = t1;
         while (loop < 10000 && t <= dis && t < t_enter) {
             ++loop;
             if (tl) tl->steps++;
@@ -144,6 +146,16 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
     }
     while (loop++ < 10000) {
         if (t > dis) {
+            if (last_non_empty_t != 0.0f) { t = last_non_empty_t; break; }
+            *next = mk3(0, 0, 0);
+            return false;
+        }
+        if (!tl && t > t_exit && !(last_dens > 0.0f)) {
+            // Past the nonzero box every step reads 0 and, with no pending
+            // transition from density, only advances t by empty_step; each
+            // step advances t by at least empty_step, so the loop cannot
+            // reach its iteration bound before t > dis: the outcome is the
+            // one the t > dis test above gives.
             if (last_non_empty_t != 0.0f) { t = last_non_empty_t; break; }
             *next = mk3(0, 0, 0);
             return false;
