@@ -298,11 +298,14 @@ mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, floa
  * (32 for E4M3) up to 128. */
 mrp_status mrp_tc_gemm_check(int fp8, const float* A, const float* B, int n, int k, float* D);
 
-/* One FP32 MRPNN launch of mrp_render (launch index view->frame_offset, no
+/* One MRPNN launch of mrp_render (launch index view->frame_offset, no
  * running mean) that also returns the intermediates of NNPredict per pixel:
  * aux [w*h][20] = hit x, y, z, hit flag, gamma, XMain, YMain, ZMain, LXMain
  * (GetSamplePoint, GetMatrixFromNormal, core/render.cuh:808-843) and feat
- * [w*h][576] (SetupInputData's features; zero where no hit). */
+ * [w*h][576] (SetupInputData's features; zero where no hit).  It runs the
+ * volume's precision: with MRP_FP32 the fp32 features and network, with
+ * MRP_BF16 / MRP_FP8 the fp16 features (returned widened to float) and the
+ * tensor-core network, so rgba equals mrp_render's image of that launch. */
 mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* view, float* rgba, float* aux, float* feat,
                                     int is_device);
 

@@ -508,7 +508,9 @@ class VolumeRender:
         return feat, gam
 
     def predict_debug(self, view):
-        """One FP32 MRPNN launch with its intermediates: (rgba [n,4], aux [n,20], feat [n,576])."""
+        """One MRPNN launch at the volume's precision with its intermediates:
+        (rgba [n,4], aux [n,20], feat [n,576]); BF16 / FP8 return the fp16
+        features their tensor-core network reads, widened to float."""
         n = view.width * view.height
         rgba = np.empty((n, 4), np.float32)
         aux = np.empty((n, 20), np.float32)

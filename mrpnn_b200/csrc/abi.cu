@@ -763,10 +763,19 @@ mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgb
     if (ps != MRP_OK) { release(); return ps; }
     HitRecords rec = v->records();
     VolumeDev dv = v->dev();
-    cudaError_t e = launch_hit(dv, vd, rec, acc, v->stream);
-    if (e == cudaSuccess) e = launch_gather_rec(dv, vd, rec, v->feat, false, v->stream);
-    if (e == cudaSuccess) e = launch_mlp_rec_fp32(dv, vd, rec, v->feat, g.d_weights, acc, v->stream);
-    if (e == cudaSuccess) e = launch_debug_scatter(rec, v->feat, (int)npix, da, df, v->stream);
+    // the volume's precision: fp32 features and the FP32 network, or the
+    // fp16 features and the tensor-core network of mrp_render
+    const bool tc = v->params.precision != MRP_FP32;
+    cudaError_t e = tc ? tc_ensure_scratch(v->tc) : cudaSuccess;
+    if (e == cudaSuccess && tc) e = cudaMemsetAsync(v->tc.d + 1, 0, sizeof(int), v->stream);
+    if (e == cudaSuccess) e = launch_hit(dv, vd, rec, acc, v->stream);
+    if (e == cudaSuccess) e = launch_gather_rec(dv, vd, rec, v->feat, tc, v->stream);
+    if (e == cudaSuccess) {
+        e = tc ? tc_launch_mlp_rec(g.tc, v->params.precision == MRP_FP8, dv, vd, rec, v->feat, acc, v->tc, g.sms,
+                                   v->stream)
+               : launch_mlp_rec_fp32(dv, vd, rec, v->feat, g.d_weights, acc, v->stream);
+    }
+    if (e == cudaSuccess) e = launch_debug_scatter(rec, v->feat, tc, (int)npix, da, df, v->stream);
     cudaMemcpyKind k = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (e == cudaSuccess) {
         cudaMemcpyAsync(rgba, acc, npix * sizeof(float4), k, v->stream);
@@ -779,6 +788,11 @@ mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgb
     release();
     if (e != cudaSuccess || e2 != cudaSuccess)
         return fail(MRP_ERR_CUDA, "debug render: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    if (tc) {
+        int herr = 0;
+        CU(cudaMemcpy(&herr, v->tc.d + 1, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core MLP: MMA completion wait timed out");
+    }
     return MRP_OK;
 }
 

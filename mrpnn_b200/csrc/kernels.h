@@ -64,7 +64,8 @@ cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecord
 cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitRecords rec, const float* feat,
                                 const float* weights, float4* accum, cudaStream_t s);
 // Scatters records and tiled features to per-pixel layout (debug entry).
-cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, int npix, float* aux, float* feat_out,
+// feat in the gather's fp32 or fp16-pair layout (launch_gather_rec)
+cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, bool fp16, int npix, float* aux, float* feat_out,
                                  cudaStream_t s);
 // Tiled feature buffer size for n records (floats).
 inline size_t tiled_feature_floats(size_t n) { return ((n + 31) / 32) * 32 * 576; }

@@ -806,6 +806,7 @@ __global__ void __launch_bounds__(128) k_mlp_rec(VolumeDev v, ViewDev w, HitReco
 
 // Per-pixel intermediates for the debug entry point: aux [npix][20] = hit
 // xyz, hit flag, gamma, X, Y, Z, LX; feat [npix][576].
+template <bool FP16>
 __global__ void k_debug_scatter(HitRecords rec, const float* __restrict__ feat, float* __restrict__ aux,
                                 float* __restrict__ feat_out) {
     int r = blockIdx.x;
@@ -817,8 +818,17 @@ __global__ void k_debug_scatter(HitRecords rec, const float* __restrict__ feat, 
         a[0] = f[0]; a[1] = f[rec.cap]; a[2] = f[2 * rec.cap]; a[3] = 1.0f; a[4] = f[15 * rec.cap];
         for (int k = 0; k < 12; ++k) a[5 + k] = f[(3 + k) * rec.cap];
     }
-    const float* src = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
-    for (int i = threadIdx.x; i < 576; i += blockDim.x) feat_out[(size_t)pix * 576 + i] = src[i * 32];
+    if (FP16) {   // fp16 pairs: word ((r / 32) * 288 + c * 96 + k) * 32 + r % 32 holds samples 2k, 2k + 1
+        const __half2* src = reinterpret_cast<const __half2*>(feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31);
+        for (int j = threadIdx.x; j < 288; j += blockDim.x) {
+            const float2 p = __half22float2(src[j * 32]);
+            feat_out[(size_t)pix * 576 + 2 * j] = p.x;
+            feat_out[(size_t)pix * 576 + 2 * j + 1] = p.y;
+        }
+    } else {
+        const float* src = feat + (size_t)(r >> 5) * 576 * 32 + (r & 31);
+        for (int i = threadIdx.x; i < 576; i += blockDim.x) feat_out[(size_t)pix * 576 + i] = src[i * 32];
+    }
 }
 
 cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* dir, float alpha, float pass_rate, int n,
@@ -1099,9 +1109,12 @@ cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitReco
     k_mlp_rec<<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat, weights, accum);
     return cudaGetLastError();
 }
-cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, int npix, float* aux, float* feat_out,
+cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, bool fp16, int npix, float* aux, float* feat_out,
                                  cudaStream_t s) {
-    if (npix > 0) k_debug_scatter<<<npix, 128, 0, s>>>(rec, feat, aux, feat_out);
+    if (npix > 0) {
+        if (fp16) k_debug_scatter<true><<<npix, 128, 0, s>>>(rec, feat, aux, feat_out);
+        else k_debug_scatter<false><<<npix, 128, 0, s>>>(rec, feat, aux, feat_out);
+    }
     return cudaGetLastError();
 }
 

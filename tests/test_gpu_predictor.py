@@ -205,3 +205,29 @@ def test_first_hit_empty_space_replay(case):
     else:
         assert ref[:, 3].sum() > 0
     np.testing.assert_allclose(got[:, :3], ref[:, :3], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("prec", ["BF16", "FP8"])
+def test_fp16_features(scene, prec):
+    """The tensor-core forms' stencil features -- fp16, the hardware log2 and
+    the per-point LUT factor of X_Hg -- against the oracle's exact features
+    (fp16 rounding is 2^-11 relative), and the debug launch's image against
+    mrp_render's image of the same launch."""
+    import mrpnn_b200 as M
+    W = 48
+    ori, up, right = view_frame()
+    view = scene.vol.make_view((W, W), ori, up, right, LIGHT, scene.g, scene.alpha, seed=3)
+    scene.vol.SetPrecision(getattr(M, prec))
+    try:
+        rgba, aux, feat = scene.vol.predict_debug(view)
+        img = np.empty((W, W, 4), np.float32)
+        scene.vol.render_view(view, M.VolumeRender.MRPNN, 1, img)
+    finally:
+        scene.vol.SetPrecision(M.FP32)
+    oview = O.make_view(W, W, ori, up, right, LIGHT, alpha=scene.alpha, g=scene.g, seed=3, frame=0)
+    _, r_feat, _, r_hit = O.predict_pixels(scene.orc, oview, np.arange(W * W, dtype=np.int32), want_features=True)
+    hit = r_hit[:, 3] > 0
+    assert hit.sum() > 100
+    np.testing.assert_array_equal(aux[:, 3], r_hit[:, 3])
+    np.testing.assert_allclose(feat[hit], r_feat[hit], rtol=2e-3, atol=2e-5)
+    np.testing.assert_array_equal(rgba.reshape(W, W, 4), img)
