@@ -233,6 +233,35 @@ MRP_D float tex3_padded(const float* __restrict__ g, int n, f3 pos) {
     return lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
 }
 
+// Two trilinear fetches at one position from texel pairs (mip_tr): the
+// values tex3_fast gives for each array, when the footprint is inside the
+// grid (where border and clamp addressing read the same texels); false (and
+// nothing read) otherwise.
+MRP_D bool tex3_pair_interior(const float2* __restrict__ g, int n, f3 pos, float* a, float* b) {
+    float nf = (float)n;
+    float px = fmaf(pos.x + 0.5f, nf, -0.5f), py = fmaf(pos.y + 0.5f, nf, -0.5f), pz = fmaf(pos.z + 0.5f, nf, -0.5f);
+    float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
+    int x = (int)flx, y = (int)fly, z = (int)flz;
+    if (!((unsigned)x < (unsigned)(n - 1) && (unsigned)y < (unsigned)(n - 1) && (unsigned)z < (unsigned)(n - 1)))
+        return false;
+    float wx = px - flx, wy = py - fly, wz = pz - flz;
+    const int nn = n * n;
+    const float2* q = g + (x * n + y) * n + z;
+    const float2 t000 = __ldg(q), t001 = __ldg(q + 1), t010 = __ldg(q + n), t011 = __ldg(q + n + 1);
+    const float2 t100 = __ldg(q + nn), t101 = __ldg(q + nn + 1), t110 = __ldg(q + nn + n), t111 = __ldg(q + nn + n + 1);
+    {
+        float c00 = lerp_fast(t000.x, t001.x, wz), c01 = lerp_fast(t010.x, t011.x, wz);
+        float c10 = lerp_fast(t100.x, t101.x, wz), c11 = lerp_fast(t110.x, t111.x, wz);
+        *a = lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+    }
+    {
+        float c00 = lerp_fast(t000.y, t001.y, wz), c01 = lerp_fast(t010.y, t011.y, wz);
+        float c10 = lerp_fast(t100.y, t101.y, wz), c11 = lerp_fast(t110.y, t111.y, wz);
+        *b = lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+    }
+    return true;
+}
+
 template <bool Clamp>
 MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float nf = (float)n;
@@ -335,6 +364,10 @@ struct VolumeDev {
     // 4..6) for the stencil gather, or null: see pad_offset / tex3_padded.
     const float* mips_pad;
     const float* trs_pad;
+    // Mip level L and TR level L - 1 (same edge, 256 >> L) side by side per
+    // texel for L = 1..4 (mip_tr_offset), or null: the gather reads both
+    // values of a stencil point with one 8-byte load per texel.
+    const float2* mip_tr;
     // 160 HG-LUT values of the rotated stencil points' own direction (the
     // first LUT factor of X_Hg, which depends only on the point and g), or
     // null; stored right after the LUT (kLutAlloc floats per LUT buffer).
@@ -346,6 +379,8 @@ struct VolumeDev {
 // grid: 0 (border addressing, the density mips) or the nearest edge texel
 // (clamp addressing, the TR levels).  Levels of edge 8, 4, 2 in that order.
 constexpr int kPadLevelFloats = 11 * 11 * 11 + 7 * 7 * 7 + 5 * 5 * 5;
+// Texel offset of level L (1..4) of VolumeDev::mip_tr; L = 5 gives the size.
+MRP_HD int mip_tr_offset(int L) { int o = 0; for (int l = 1; l < L; ++l) { int n = 256 >> l; o += n * n * n; } return o; }
 MRP_HD int pad_offset(int n) { return n == 8 ? 0 : n == 4 ? 11 * 11 * 11 : 11 * 11 * 11 + 7 * 7 * 7; }
 
 // ---------------------------------------------------------------------------

@@ -315,6 +315,7 @@ struct RunLevels {
     int n, tn;
     bool light;
     bool mip_pad, tr_pad;   // mip / tr point at a padded copy (tex3_padded)
+    const float2* pair;     // the run's (mip, TR) texel pairs (mip_tr), or null
 };
 // FP16: the features are stored as fp16, so the two logs use the hardware
 // log2 (__logf, absolute error < 4e-7 on the arguments here, all >= 1), which
@@ -335,7 +336,12 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
         d = mk3(f.L.x * off, f.L.y * off, f.L.z * off);
     }
     const f3 cur = mk3(f.pos.x + d.x, f.pos.y + d.y, f.pos.z + d.z);
-    const float dens = R.mip_pad ? tex3_padded(R.mip, R.n, cur) : tex3_fast<false>(R.mip, R.n, cur);
+    // ShadowTerm_TRs reads the TR at the point itself inside the box, else
+    // where the light ray enters the box
+    const bool outside = cur.x < -0.5f || cur.y < -0.5f || cur.z < -0.5f || cur.x > 0.5f || cur.y > 0.5f || cur.z > 0.5f;
+    float dens, tr_pair = 0.0f;
+    const bool paired = R.pair && !outside && tex3_pair_interior(R.pair, R.n, cur, &dens, &tr_pair);
+    if (!paired) dens = R.mip_pad ? tex3_padded(R.mip, R.n, cur) : tex3_fast<false>(R.mip, R.n, cur);
     *fd_ = feature_log<FP16>(fmaf(f.alpha * dens, 0.015625f, 1.0f));
     if (i == 0) {
         *fh_ = feature_log<FP16>(hg(dot(f.X, f.L), f.g) + 1.0f);
@@ -364,14 +370,18 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
     // ShadowTerm_TRs: outside the box, the TR where the light ray enters it
     const f3 p = cur, light = f.LX;
     float tr = 1.0f;
-    f3 q = p;
-    bool fetch = true;
-    if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
-        float o = ray_box_offset(p, light);
-        fetch = o >= 0;
-        q = mk3(fmaf(light.x, o, p.x), fmaf(light.y, o, p.y), fmaf(light.z, o, p.z));
+    if (paired) {
+        tr = tr_pair;
+    } else {
+        f3 q = p;
+        bool fetch = true;
+        if (outside) {
+            float o = ray_box_offset(p, light);
+            fetch = o >= 0;
+            q = mk3(fmaf(light.x, o, p.x), fmaf(light.y, o, p.y), fmaf(light.z, o, p.z));
+        }
+        if (fetch) tr = R.tr_pad ? tex3_padded(R.tr, R.tn, q) : tex3_fast<true>(R.tr, R.tn, q);
     }
-    if (fetch) tr = R.tr_pad ? tex3_padded(R.tr, R.tn, q) : tex3_fast<true>(R.tr, R.tn, q);
     *fs_ = tr;
 }
 // All 192 points, run by run (GetSamples23_'s layout: layers 0..7 over the
@@ -393,9 +403,11 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
         // edge <= 8 (mips 5..7, TR levels 4..6): most footprints touch the
         // grid's edge, so those runs read the padded copies when present
         const bool mp = v.mips_pad && layer >= 5, tp = v.trs_pad && tl >= 4;
+        // layers 1..4: mip level and TR level share the edge 256 >> layer
+        const float2* pr = v.mip_tr && layer >= 1 && layer <= 4 ? v.mip_tr + mip_tr_offset(layer) : nullptr;
         const RunLevels R{mp ? v.mips_pad + pad_offset(256 >> layer) : mip_level(v, layer),
                           tp ? v.trs_pad + pad_offset(128 >> tl) : tr_level(v, tl), 256 >> layer, 128 >> tl,
-                          from >= 160, mp, tp};
+                          from >= 160, mp, tp, pr};
 #pragma unroll 1
         for (int i = from; i < to; ++i) {
             float a, b, c;

@@ -233,7 +233,8 @@ bool mrp_server::admit() {
         s.t = T;
         s.vd = v->dev();
         s.vd.trs = s.trs;
-        s.vd.trs_pad = nullptr;   // the slot's own TR levels have no padded copy
+        s.vd.trs_pad = nullptr;   // the slot's own TR levels have no padded or paired copy
+        s.vd.mip_tr = nullptr;
         s.vd.lut = lut->d;
         s.vd.lut_dirs = lut->d + kLut * kLut;
         s.view = make_view(v, &w, w.frame_offset, 0);

@@ -102,6 +102,19 @@ __global__ void k_max_density(const float* __restrict__ d, size_t n, int* __rest
     if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_int(m));
 }
 
+// Mip level L and TR level L - 1 side by side per texel, L = 1..4
+// (VolumeDev::mip_tr).
+__global__ void k_interleave_mip_tr(const float* __restrict__ mips, const float* __restrict__ trs,
+                                    float2* __restrict__ out) {
+    const int total = mip_tr_offset(5);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int L = 1;
+        while (L < 4 && i >= mip_tr_offset(L + 1)) ++L;
+        const int j = i - mip_tr_offset(L);
+        out[i] = make_float2(mips[mip_offset(L) + j], trs[tr_offset(L - 1) + j]);
+    }
+}
+
 // Padded copies of three levels of edge 8, 4, 2 (blockIdx.y picks one): the
 // texel of (x, y, z) in [-1, n + 1]^3 is the level's texel under border
 // addressing (0 outside) or clamp addressing (nearest edge texel).
@@ -341,6 +354,10 @@ cudaError_t launch_resample(float* out, int res, const float* src, int src_res, 
 }
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s) {
     k_max_density<<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
+    return cudaGetLastError();
+}
+cudaError_t launch_interleave_mip_tr(const float* mips, const float* trs, float2* out, int sms, cudaStream_t s) {
+    k_interleave_mip_tr<<<sms * 8, 256, 0, s>>>(mips, trs, out);
     return cudaGetLastError();
 }
 cudaError_t launch_pad_levels(const float* l8, const float* l4, const float* l2, bool clamp, float* out,
