@@ -274,7 +274,8 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
         (e = cudaMalloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess ||
         (e = cudaMalloc(&v->mips_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->trs_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->mip_tr, mip_tr_offset(5) * sizeof(float2))) != cudaSuccess)
+        (e = cudaMalloc(&v->mip_tr, mip_tr_offset(5) * sizeof(float2))) != cudaSuccess ||
+        (e = cudaMalloc(&v->pad_pair, kPadLevelFloats * sizeof(float2))) != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
                             cudaGetErrorString(e)));
     cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
@@ -286,7 +287,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
     cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
-    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->mips_pad); cudaFree(v->trs_pad); cudaFree(v->mip_tr); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
+    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->mips_pad); cudaFree(v->trs_pad); cudaFree(v->mip_tr); cudaFree(v->pad_pair); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
     tc_free_scratch(v->tc);
@@ -519,6 +520,7 @@ mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
     CU(launch_pad_levels(v->trs + tr_offset(4), v->trs + tr_offset(5), v->trs + tr_offset(6), true, v->trs_pad,
                          v->stream));
     CU(launch_interleave_mip_tr(v->mips, v->trs, v->mip_tr, g.sms, v->stream));
+    CU(launch_pair_padded(v->mips_pad, v->trs_pad, v->pad_pair, v->stream));
     v->has_tr = true;
     v->tr_alpha = alpha;
     std::memcpy(v->tr_light, L, sizeof v->tr_light);

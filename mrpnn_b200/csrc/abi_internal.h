@@ -112,6 +112,7 @@ struct mrp_volume {
     float* mips_pad = nullptr;    // padded mips 5..7 (pad_offset layout), built with the pyramid
     float* trs_pad = nullptr;     // padded TR levels 4..6, built with the TR levels
     float2* mip_tr = nullptr;     // (mip L, TR L - 1) texel pairs, L = 1..4, built with the TR levels
+    float2* pad_pair = nullptr;   // (padded mip, padded TR) pairs, built with the TR levels
     int* d_bounds = nullptr;      // nonzero-voxel index bounds (6 ints) of the last update
     int nz_bounds[6] = {0, 0, 0, -1, -1, -1};
     bool has_bounds = false;
@@ -164,6 +165,7 @@ struct mrp_volume {
         d.mips_pad = has_pyramid ? mips_pad : nullptr;
         d.trs_pad = has_tr ? trs_pad : nullptr;
         d.mip_tr = has_tr ? mip_tr : nullptr;
+        d.pad_pair = has_tr && has_pyramid ? pad_pair : nullptr;
         d.lut_dirs = has_lut ? lut + mrp::kLut * mrp::kLut : nullptr;
         d.has_bounds = has_bounds ? 1 : 0;
         if (has_bounds) {

@@ -262,6 +262,33 @@ MRP_D bool tex3_pair_interior(const float2* __restrict__ g, int n, f3 pos, float
     return true;
 }
 
+// tex3_padded of both channels of a padded pair array (pad_pair).
+MRP_D void tex3_padded_pair(const float2* __restrict__ g, int n, f3 pos, float* a, float* b) {
+    const float nf = (float)n;
+    float px = fmaf(pos.x + 0.5f, nf, -0.5f), py = fmaf(pos.y + 0.5f, nf, -0.5f), pz = fmaf(pos.z + 0.5f, nf, -0.5f);
+    px = fminf(fmaxf(px, -1.0f), nf);
+    py = fminf(fmaxf(py, -1.0f), nf);
+    pz = fminf(fmaxf(pz, -1.0f), nf);
+    const float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
+    const int P = n + 3;
+    const int x = (int)flx + 1, y = (int)fly + 1, z = (int)flz + 1;
+    const float wx = px - flx, wy = py - fly, wz = pz - flz;
+    const float2* q = g + (x * P + y) * P + z;
+    const int PP = P * P;
+    const float2 t000 = __ldg(q), t001 = __ldg(q + 1), t010 = __ldg(q + P), t011 = __ldg(q + P + 1);
+    const float2 t100 = __ldg(q + PP), t101 = __ldg(q + PP + 1), t110 = __ldg(q + PP + P), t111 = __ldg(q + PP + P + 1);
+    {
+        float c00 = lerp_fast(t000.x, t001.x, wz), c01 = lerp_fast(t010.x, t011.x, wz);
+        float c10 = lerp_fast(t100.x, t101.x, wz), c11 = lerp_fast(t110.x, t111.x, wz);
+        *a = lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+    }
+    {
+        float c00 = lerp_fast(t000.y, t001.y, wz), c01 = lerp_fast(t010.y, t011.y, wz);
+        float c10 = lerp_fast(t100.y, t101.y, wz), c11 = lerp_fast(t110.y, t111.y, wz);
+        *b = lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+    }
+}
+
 template <bool Clamp>
 MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float nf = (float)n;
@@ -368,6 +395,9 @@ struct VolumeDev {
     // texel for L = 1..4 (mip_tr_offset), or null: the gather reads both
     // values of a stencil point with one 8-byte load per texel.
     const float2* mip_tr;
+    // The same pairing for the padded levels (mips 5..7 with TR levels 4..6,
+    // pad_offset layout, each channel with its own margin), or null.
+    const float2* pad_pair;
     // 160 HG-LUT values of the rotated stencil points' own direction (the
     // first LUT factor of X_Hg, which depends only on the point and g), or
     // null; stored right after the LUT (kLutAlloc floats per LUT buffer).

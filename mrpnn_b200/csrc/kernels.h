@@ -10,6 +10,8 @@ cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int oc
 cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s);
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s);
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
+// VolumeDev::pad_pair from the padded mips and TR levels (kPadLevelFloats pairs).
+cudaError_t launch_pair_padded(const float* mips_pad, const float* trs_pad, float2* out, cudaStream_t s);
 // VolumeDev::mip_tr from the pyramid and the TR levels (mip_tr_offset(5) pairs).
 cudaError_t launch_interleave_mip_tr(const float* mips, const float* trs, float2* out, int sms, cudaStream_t s);
 // Padded copies (pad_offset layout, kPadLevelFloats floats) of three levels

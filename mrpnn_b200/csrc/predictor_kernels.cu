@@ -315,7 +315,8 @@ struct RunLevels {
     int n, tn;
     bool light;
     bool mip_pad, tr_pad;   // mip / tr point at a padded copy (tex3_padded)
-    const float2* pair;     // the run's (mip, TR) texel pairs (mip_tr), or null
+    const float2* pair;     // the run's (mip, TR) texel pairs (mip_tr or pad_pair), or null
+    bool pair_pad;          // pair is a padded pair level
 };
 // FP16: the features are stored as fp16, so the two logs use the hardware
 // log2 (__logf, absolute error < 4e-7 on the arguments here, all >= 1), which
@@ -340,7 +341,15 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
     // where the light ray enters the box
     const bool outside = cur.x < -0.5f || cur.y < -0.5f || cur.z < -0.5f || cur.x > 0.5f || cur.y > 0.5f || cur.z > 0.5f;
     float dens, tr_pair = 0.0f;
-    const bool paired = R.pair && !outside && tex3_pair_interior(R.pair, R.n, cur, &dens, &tr_pair);
+    bool paired = false;
+    if (R.pair && !outside) {
+        if (R.pair_pad) {
+            tex3_padded_pair(R.pair, R.n, cur, &dens, &tr_pair);
+            paired = true;
+        } else {
+            paired = tex3_pair_interior(R.pair, R.n, cur, &dens, &tr_pair);
+        }
+    }
     if (!paired) dens = R.mip_pad ? tex3_padded(R.mip, R.n, cur) : tex3_fast<false>(R.mip, R.n, cur);
     *fd_ = feature_log<FP16>(fmaf(f.alpha * dens, 0.015625f, 1.0f));
     if (i == 0) {
@@ -404,10 +413,13 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
         // grid's edge, so those runs read the padded copies when present
         const bool mp = v.mips_pad && layer >= 5, tp = v.trs_pad && tl >= 4;
         // layers 1..4: mip level and TR level share the edge 256 >> layer
-        const float2* pr = v.mip_tr && layer >= 1 && layer <= 4 ? v.mip_tr + mip_tr_offset(layer) : nullptr;
+        // layers 5..7: the padded pairs (mips 5..7 with TR levels 4..6)
+        const bool pp = mp && tp && v.pad_pair;
+        const float2* pr = pp ? v.pad_pair + pad_offset(256 >> layer)
+                           : v.mip_tr && layer >= 1 && layer <= 4 ? v.mip_tr + mip_tr_offset(layer) : nullptr;
         const RunLevels R{mp ? v.mips_pad + pad_offset(256 >> layer) : mip_level(v, layer),
                           tp ? v.trs_pad + pad_offset(128 >> tl) : tr_level(v, tl), 256 >> layer, 128 >> tl,
-                          from >= 160, mp, tp, pr};
+                          from >= 160, mp, tp, pr, pp};
 #pragma unroll 1
         for (int i = from; i < to; ++i) {
             float a, b, c;

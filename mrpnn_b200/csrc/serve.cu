@@ -235,6 +235,7 @@ bool mrp_server::admit() {
         s.vd.trs = s.trs;
         s.vd.trs_pad = nullptr;   // the slot's own TR levels have no padded or paired copy
         s.vd.mip_tr = nullptr;
+        s.vd.pad_pair = nullptr;
         s.vd.lut = lut->d;
         s.vd.lut_dirs = lut->d + kLut * kLut;
         s.view = make_view(v, &w, w.frame_offset, 0);

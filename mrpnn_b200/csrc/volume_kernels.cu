@@ -115,6 +115,12 @@ __global__ void k_interleave_mip_tr(const float* __restrict__ mips, const float*
     }
 }
 
+// The padded mips and TR levels side by side (VolumeDev::pad_pair).
+__global__ void k_pair_padded(const float* __restrict__ a, const float* __restrict__ b, float2* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kPadLevelFloats; i += gridDim.x * blockDim.x)
+        out[i] = make_float2(a[i], b[i]);
+}
+
 // Padded copies of three levels of edge 8, 4, 2 (blockIdx.y picks one): the
 // texel of (x, y, z) in [-1, n + 1]^3 is the level's texel under border
 // addressing (0 outside) or clamp addressing (nearest edge texel).
@@ -358,6 +364,10 @@ cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms,
 }
 cudaError_t launch_interleave_mip_tr(const float* mips, const float* trs, float2* out, int sms, cudaStream_t s) {
     k_interleave_mip_tr<<<sms * 8, 256, 0, s>>>(mips, trs, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_pair_padded(const float* mips_pad, const float* trs_pad, float2* out, cudaStream_t s) {
+    k_pair_padded<<<(kPadLevelFloats + 255) / 256, 256, 0, s>>>(mips_pad, trs_pad, out);
     return cudaGetLastError();
 }
 cudaError_t launch_pad_levels(const float* l8, const float* l4, const float* l2, bool clamp, float* out,
