@@ -82,6 +82,7 @@ MRP_D f3 camera_ray(const ViewDev& w, int row, int col) { return camera_ray_dir(
 struct MarchRay {
     f3 pos, dir;
     f3 c, sR;   // texel coordinate X(t) = c + sR * t, per axis
+    f3 isR;     // 1 / sR (0 where sR == 0)
 };
 MRP_D MarchRay march_ray(const VolumeDev& v, f3 pos, f3 dir) {
     const float nf = (float)v.res;
@@ -90,14 +91,36 @@ MRP_D MarchRay march_ray(const VolumeDev& v, f3 pos, f3 dir) {
     m.dir = dir;
     m.c = mk3((pos.x + 0.5f) * nf - 0.5f, (pos.y + 0.5f) * nf - 0.5f, (pos.z + 0.5f) * nf - 0.5f);
     m.sR = mk3(dir.x * nf, dir.y * nf, dir.z * nf);
+    m.isR = mk3(m.sR.x != 0.0f ? 1.0f / m.sR.x : 0.0f, m.sR.y != 0.0f ? 1.0f / m.sR.y : 0.0f,
+                m.sR.z != 0.0f ? 1.0f / m.sR.z : 0.0f);
     return m;
 }
-MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* tl) {
+// The largest t up to which X(t) stays inside brick b (base voxels
+// [b << sh, (b + 1) << sh)) on one axis, with a 1/64-voxel margin: X(t) is
+// a single rounded FMA, monotone in t, and the margin is far above the
+// rounding of X or of this bound.
+MRP_D float brick_exit(float c, float sR, float isR, int b, int sh) {
+    const float m = 1.0f / 64.0f;
+    if (sR > 0.0f) return ((float)((b + 1) << sh) - m - c) * isR;
+    if (sR < 0.0f) return ((float)(b << sh) + m - c) * isR;
+    return 3.0e38f;
+}
+// *t_brick: when the brick proves the value 0 and the base voxel lies inside
+// the grid, the t up to which the ray stays in that brick (the march's next
+// steps there read 0 as well); else -1.
+MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* tl, float* t_brick) {
     const int R1 = v.res - 1, sh = v.occ_shift, nb = v.occ_res;
-    const int x = min(max(__float2int_rd(fmaf(m.sR.x, t, m.c.x)), 0), R1) >> sh;
-    const int y = min(max(__float2int_rd(fmaf(m.sR.y, t, m.c.y)), 0), R1) >> sh;
-    const int z = min(max(__float2int_rd(fmaf(m.sR.z, t, m.c.z)), 0), R1) >> sh;
-    if (__ldg(v.occ + (x * nb + y) * nb + z) == 0) return 0.0f;
+    const int xi = __float2int_rd(fmaf(m.sR.x, t, m.c.x));
+    const int yi = __float2int_rd(fmaf(m.sR.y, t, m.c.y));
+    const int zi = __float2int_rd(fmaf(m.sR.z, t, m.c.z));
+    const int x = min(max(xi, 0), R1) >> sh, y = min(max(yi, 0), R1) >> sh, z = min(max(zi, 0), R1) >> sh;
+    *t_brick = -1.0f;
+    if (__ldg(v.occ + (x * nb + y) * nb + z) == 0) {
+        if ((unsigned)xi <= (unsigned)R1 && (unsigned)yi <= (unsigned)R1 && (unsigned)zi <= (unsigned)R1)
+            *t_brick = fminf(brick_exit(m.c.x, m.sR.x, m.isR.x, x, sh),
+                             fminf(brick_exit(m.c.y, m.sR.y, m.isR.y, y, sh), brick_exit(m.c.z, m.sR.z, m.isR.z, z, sh)));
+        return 0.0f;
+    }
     if (tl) tl->fetches++;
     return tex3<false>(v.density, v.res, add(m.pos, mul(m.dir, t)));
 }
@@ -161,9 +184,9 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
             return false;
         }
         if (tl) tl->steps++;
-        float d;
+        float d, t_brick = -1.0f;
         if (v.occ) {
-            d = density_skip(v, mr, t, tl);
+            d = density_skip(v, mr, t, tl, &t_brick);
         } else {
             d = density(v, add(pos, mul(dir, t)));
             if (tl) tl->fetches++;
@@ -198,6 +221,14 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
             t = fa(t, fmaxf(fm(-d, 1.0f), empty_step));
         }
         last_dens = d;
+        // The step read 0 from an empty brick: the following steps that
+        // start inside the brick read 0 too and, last_dens being 0, only
+        // advance t by empty_step -- replayed as additions alone.
+        while (t <= t_brick && t <= dis && loop < 10000) {
+            ++loop;
+            if (tl) tl->steps++;
+            t = fa(t, empty_step);
+        }
     }
     *next = add(mul(dir, t), pos);
     return true;
