@@ -52,8 +52,9 @@ MRP_D f3 inv(f3 a) {
     return {a.x == 0 ? 999999999.0f : fd(1.0f, a.x), a.y == 0 ? 999999999.0f : fd(1.0f, a.y),
             a.z == 0 ? 999999999.0f : fd(1.0f, a.z)};
 }
-MRP_D float ray_box_offset(f3 p, f3 dir) {
-    dir = inv(dir);
+// ray_box_offset with inv(dir) already taken (for a direction shared by many
+// points; same operations after the inverse).
+MRP_D float ray_box_offset_inv(f3 p, f3 dir) {
     f3 to_axil = mul(neg(p), dir);
     f3 face = mul(mk3(0.4999f, 0.4999f, 0.4999f), dir);
     f3 d0 = add(to_axil, face), d1 = sub(to_axil, face);
@@ -61,6 +62,7 @@ MRP_D float ray_box_offset(f3 p, f3 dir) {
     float tma = fminf(fmaxf(d0.x, d1.x), fminf(fmaxf(d0.y, d1.y), fmaxf(d0.z, d1.z)));
     return tma >= tmi ? fmaxf(tmi, 0.0f) : -1.0f;
 }
+MRP_D float ray_box_offset(f3 p, f3 dir) { return ray_box_offset_inv(p, inv(dir)); }
 MRP_D float ray_box_distance(f3 p, f3 dir) {
     dir = inv(dir);
     f3 to_axil = mul(neg(p), dir);

@@ -356,8 +356,8 @@ template <bool FP16>
 MRP_D float feature_log(float x) { return FP16 ? __logf(x) : logf(x); }
 
 template <bool FP16>
-MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunLevels& R, const HgFast& H, int i,
-                             float* fd_, float* fs_, float* fh_) {
+MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunLevels& R, const HgFast& H, f3 iLX,
+                             int i, float* fd_, float* fs_, float* fh_) {
     const float off = c_offset[i];
     f3 d;   // offset from the point
     if (!R.light) {
@@ -416,7 +416,7 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
         f3 q = p;
         bool fetch = true;
         if (outside) {
-            float o = ray_box_offset(p, light);
+            float o = ray_box_offset_inv(p, iLX);   // iLX = inv(light), once per record
             fetch = o >= 0;
             q = mk3(fmaf(light.x, o, p.x), fmaf(light.y, o, p.y), fmaf(light.z, o, p.z));
         }
@@ -436,6 +436,7 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
     __half2* out2 = reinterpret_cast<__half2*>(feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31);
     float pa = 0.0f, pb = 0.0f, pc = 0.0f;   // the even sample of a pair
     const HgFast H = FP16 ? hg_fast(v, f) : HgFast{mk3(0, 0, 0), 0.0f, 0.0f, nullptr};
+    const f3 iLX = inv(f.LX);
 #pragma unroll 1
     for (int run = 0; run < 12; ++run) {
         const int layer = c_stencil_runs[run][0], from = c_stencil_runs[run][1], to = c_stencil_runs[run][2];
@@ -454,7 +455,7 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
 #pragma unroll 1
         for (int i = from; i < to; ++i) {
             float a, b, c;
-            gather_point_fast<FP16>(v, f, R, H, i, &a, &b, &c);
+            gather_point_fast<FP16>(v, f, R, H, iLX, i, &a, &b, &c);
             if (!FP16) {
                 out[i * 32] = a;
                 out[(192 + i) * 32] = b;
