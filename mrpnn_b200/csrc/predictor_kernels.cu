@@ -28,6 +28,10 @@ __constant__ int c_layer[192];
 __constant__ float c_lutv[192];
 __constant__ float c_dirs[160 * 3];
 __constant__ float c_udirs[160 * 3];   // the same directions normalised (host, double precision)
+// The fast gather's per-point constants packed for one 16-byte load each:
+// (direction x, y, z, offset) and (unit direction x, y, z, LUT row v); the
+// directions are 0 for the light-ray points 160..191.
+__constant__ float4 c_pt0[192], c_pt1[192];
 
 // The 192 points as the runs of GetSamples23_'s layout: layers 0..7 over the
 // 160 rotated directions (8, 8, 16, 16, 16, 32, 32, 32 points), then layers
@@ -59,6 +63,15 @@ cudaError_t set_stencil_tables(const StencilTables& t) {
         ud[3 * i] = (float)(x / l); ud[3 * i + 1] = (float)(y / l); ud[3 * i + 2] = (float)(z / l);
     }
     if ((e = cudaMemcpyToSymbol(c_udirs, ud, sizeof ud)) != cudaSuccess) return e;
+    float4 p0[192], p1[192];
+    for (int i = 0; i < 192; ++i) {
+        const bool rot = i < 160;
+        p0[i] = make_float4(rot ? t.dirs[3 * i] : 0.0f, rot ? t.dirs[3 * i + 1] : 0.0f, rot ? t.dirs[3 * i + 2] : 0.0f,
+                            t.offset[i]);
+        p1[i] = make_float4(rot ? ud[3 * i] : 0.0f, rot ? ud[3 * i + 1] : 0.0f, rot ? ud[3 * i + 2] : 0.0f, t.lut_v[i]);
+    }
+    if ((e = cudaMemcpyToSymbol(c_pt0, p0, sizeof p0)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_pt1, p1, sizeof p1)) != cudaSuccess) return e;
     return cudaMemcpyToSymbol(c_dirs, t.dirs, sizeof t.dirs);
 }
 
@@ -358,10 +371,11 @@ MRP_D float feature_log(float x) { return FP16 ? __logf(x) : logf(x); }
 template <bool FP16>
 MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunLevels& R, const HgFast& H, f3 iLX,
                              int i, float* fd_, float* fs_, float* fh_) {
-    const float off = c_offset[i];
+    const float4 p0 = c_pt0[i], p1 = c_pt1[i];
+    const float off = p0.w;
     f3 d;   // offset from the point
     if (!R.light) {
-        const float px = c_dirs[3 * i], py = c_dirs[3 * i + 1], pz = c_dirs[3 * i + 2];
+        const float px = p0.x, py = p0.y, pz = p0.z;
         d = mk3(fmaf(f.Z.x, pz, fmaf(f.Y.x, py, f.X.x * px)) * off, fmaf(f.Z.y, pz, fmaf(f.Y.y, py, f.X.y * px)) * off,
                 fmaf(f.Z.z, pz, fmaf(f.Y.z, py, f.X.z * px)) * off);
     } else {
@@ -386,10 +400,10 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
     if (i == 0) {
         *fh_ = feature_log<FP16>(hg(dot(f.X, f.L), f.g) + 1.0f);
     } else if (FP16 && H.lut_dirs) {
-        const float lv = c_lutv[i];
+        const float lv = p1.w;
         float a, b;
         if (!R.light) {
-            const float c2 = fmaf(H.q.z, c_udirs[3 * i + 2], fmaf(H.q.y, c_udirs[3 * i + 1], H.q.x * c_udirs[3 * i]));
+            const float c2 = fmaf(H.q.z, p1.z, fmaf(H.q.y, p1.y, H.q.x * p1.x));
             a = __ldg(H.lut_dirs + i);
             b = tex_lut_fast(v.lut, fmaf(c2, 0.5f, 0.5f), lv);
         } else {
@@ -403,7 +417,7 @@ MRP_D void gather_point_fast(const VolumeDev& v, const PixelFrame& f, const RunL
         ms = mk3(ms.x * rl, ms.y * rl, ms.z * rl);
         float c1 = fmaf(f.X.z, ms.z, fmaf(f.X.y, ms.y, f.X.x * ms.x));
         float c2 = fmaf(f.LX.z, ms.z, fmaf(f.LX.y, ms.y, f.LX.x * ms.x));
-        float lv = c_lutv[i];
+        float lv = p1.w;
         *fh_ = feature_log<FP16>(fmaf(tex_lut_fast(v.lut, fmaf(c1, 0.5f, 0.5f), lv), tex_lut_fast(v.lut, fmaf(c2, 0.5f, 0.5f), lv),
                          1.0f));
     }
