@@ -291,6 +291,33 @@ MRP_D void tex3_padded_pair(const float2* __restrict__ g, int n, f3 pos, float* 
     }
 }
 
+// tex3_fast's footprints that touch the grid's edge: clamped texels, and
+// under border addressing the ones outside the grid zeroed.  Out of line:
+// rare, and it keeps the fetch's common path short in the loops that call it.
+template <bool Clamp>
+__device__ __noinline__ float tex3_edge(const float* __restrict__ g, int n, int x, int y, int z, float wx, float wy,
+                                        float wz) {
+    const int nn = n * n;
+    int x0 = min(max(x, 0), n - 1) * nn, x1 = min(max(x + 1, 0), n - 1) * nn;
+    int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
+    int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
+    float t000 = __ldg(g + x0 + y0 + z0), t001 = __ldg(g + x0 + y0 + z1);
+    float t010 = __ldg(g + x0 + y1 + z0), t011 = __ldg(g + x0 + y1 + z1);
+    float t100 = __ldg(g + x1 + y0 + z0), t101 = __ldg(g + x1 + y0 + z1);
+    float t110 = __ldg(g + x1 + y1 + z0), t111 = __ldg(g + x1 + y1 + z1);
+    if (!Clamp) {
+        bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
+        bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
+        bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
+        t000 = vx0 && vy0 && vz0 ? t000 : 0.0f; t001 = vx0 && vy0 && vz1 ? t001 : 0.0f;
+        t010 = vx0 && vy1 && vz0 ? t010 : 0.0f; t011 = vx0 && vy1 && vz1 ? t011 : 0.0f;
+        t100 = vx1 && vy0 && vz0 ? t100 : 0.0f; t101 = vx1 && vy0 && vz1 ? t101 : 0.0f;
+        t110 = vx1 && vy1 && vz0 ? t110 : 0.0f; t111 = vx1 && vy1 && vz1 ? t111 : 0.0f;
+    }
+    float c00 = lerp_fast(t000, t001, wz), c01 = lerp_fast(t010, t011, wz);
+    float c10 = lerp_fast(t100, t101, wz), c11 = lerp_fast(t110, t111, wz);
+    return lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
+}
 template <bool Clamp>
 MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float nf = (float)n;
@@ -298,30 +325,12 @@ MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
     float flx = floorf(px), fly = floorf(py), flz = floorf(pz);
     int x = (int)flx, y = (int)fly, z = (int)flz;
     float wx = px - flx, wy = py - fly, wz = pz - flz;
+    if (!((unsigned)x < (unsigned)(n - 1) && (unsigned)y < (unsigned)(n - 1) && (unsigned)z < (unsigned)(n - 1)))
+        return tex3_edge<Clamp>(g, n, x, y, z, wx, wy, wz);
     const int nn = n * n;
-    float t000, t001, t010, t011, t100, t101, t110, t111;
-    if ((unsigned)x < (unsigned)(n - 1) && (unsigned)y < (unsigned)(n - 1) && (unsigned)z < (unsigned)(n - 1)) {
-        const float* b = g + (x * n + y) * n + z;
-        t000 = __ldg(b); t001 = __ldg(b + 1); t010 = __ldg(b + n); t011 = __ldg(b + n + 1);
-        t100 = __ldg(b + nn); t101 = __ldg(b + nn + 1); t110 = __ldg(b + nn + n); t111 = __ldg(b + nn + n + 1);
-    } else {
-        int x0 = min(max(x, 0), n - 1) * nn, x1 = min(max(x + 1, 0), n - 1) * nn;
-        int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
-        int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
-        t000 = __ldg(g + x0 + y0 + z0); t001 = __ldg(g + x0 + y0 + z1);
-        t010 = __ldg(g + x0 + y1 + z0); t011 = __ldg(g + x0 + y1 + z1);
-        t100 = __ldg(g + x1 + y0 + z0); t101 = __ldg(g + x1 + y0 + z1);
-        t110 = __ldg(g + x1 + y1 + z0); t111 = __ldg(g + x1 + y1 + z1);
-        if (!Clamp) {
-            bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
-            bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
-            bool vz0 = (unsigned)z < (unsigned)n, vz1 = (unsigned)(z + 1) < (unsigned)n;
-            t000 = vx0 && vy0 && vz0 ? t000 : 0.0f; t001 = vx0 && vy0 && vz1 ? t001 : 0.0f;
-            t010 = vx0 && vy1 && vz0 ? t010 : 0.0f; t011 = vx0 && vy1 && vz1 ? t011 : 0.0f;
-            t100 = vx1 && vy0 && vz0 ? t100 : 0.0f; t101 = vx1 && vy0 && vz1 ? t101 : 0.0f;
-            t110 = vx1 && vy1 && vz0 ? t110 : 0.0f; t111 = vx1 && vy1 && vz1 ? t111 : 0.0f;
-        }
-    }
+    const float* b = g + (x * n + y) * n + z;
+    const float t000 = __ldg(b), t001 = __ldg(b + 1), t010 = __ldg(b + n), t011 = __ldg(b + n + 1);
+    const float t100 = __ldg(b + nn), t101 = __ldg(b + nn + 1), t110 = __ldg(b + nn + n), t111 = __ldg(b + nn + n + 1);
     float c00 = lerp_fast(t000, t001, wz), c01 = lerp_fast(t010, t011, wz);
     float c10 = lerp_fast(t100, t101, wz), c11 = lerp_fast(t110, t111, wz);
     return lerp_fast(lerp_fast(c00, c01, wy), lerp_fast(c10, c11, wy), wx);
