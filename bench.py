@@ -289,7 +289,7 @@ def run_serving(args, local):
     vols = []
     for seed in SERVE["seeds"]:
         R = int(rng.choice(SERVE["sizes"]))
-        v = M.VolumeRender(R)
+        v = M.VolumeRender(R, storage="fp16")   # fp16 density grids
         v.generate_fbm(int(seed), SERVE["freq"])
         v.Update()
         v.SetScatterRate(SCENE["albedo"])
@@ -357,7 +357,7 @@ def run_serving(args, local):
     span_s = (last_done - first_submit) / 1000.0
     lat = np.asarray(lat)
     pm = np.median(np.asarray(parts), axis=0)
-    return {"workload": "16 resident fBm volumes (128/256/512^3, seeds 10-25, alpha 16-256), Poisson "
+    return {"workload": "16 resident fp16 fBm volumes (128/256/512^3, seeds 10-25, alpha 16-256), Poisson "
                         f"{SERVE['rate']:.0f} req/s, images 256^2/512^2/1024^2/1920x1080, orbit cameras, random "
                         "lights, BF16 network, 120 GB budget, 16 slots sized for 1920x1080 at open, results in device buffers",
             "requests": n_req, "offered_req_s": SERVE["rate"], "achieved_req_s": n_req / span_s,
@@ -431,7 +431,7 @@ def run_large(args, local):
 
     import mrpnn_b200 as M
     t0 = time.perf_counter()
-    vol = M.VolumeRender(LARGE["res"])
+    vol = M.VolumeRender(LARGE["res"], storage="fp16")   # fp16 density grid (2 GiB)
     vol.generate_fbm(LARGE["seed"], LARGE["freq"])
     vol.Update()
     vol.SetScatterRate(LARGE["albedo"])
@@ -449,7 +449,7 @@ def run_large(args, local):
     n = LARGE["size"]
     views = [vol.make_view((n, n), o, u, r, L, SCENE["g"], LARGE["alpha"], seed=k) for k, (o, u, r) in enumerate(cams)]
     outs = [torch.empty((n, n, 4), dtype=torch.float32, device=f"cuda:{local}") for _ in views]
-    res = {"workload": f"{LARGE['res']}^3 fBm (seed 2, freq 8), alpha {LARGE['alpha']:.0f}, albedo {LARGE['albedo']}, "
+    res = {"workload": f"{LARGE['res']}^3 fp16 fBm (seed 2, freq 8), alpha {LARGE['alpha']:.0f}, albedo {LARGE['albedo']}, "
                        f"g {SCENE['g']}, {LARGE['views']} random orbit views at {n}^2 per mrp_render_views call "
                        "(one batched network launch)", "setup_s": setup_s}
     for pname, pv in (("fp8", M.FP8), ("bf16", M.BF16), ("fp32", M.FP32)):

@@ -118,6 +118,14 @@ void mrp_default_params(mrp_params* p);
 /* VolumeRender(int resolution) (core/volume.cu:948-957); allocates exactly
  * res^3 floats instead of the reference's fixed 1024^3 array. */
 mrp_status mrp_volume_create(int res, mrp_volume** out);
+/* Storage type of the density grid.  FP16 halves the grid's HBM (a 1024^3
+ * volume: 2 GiB instead of 4); values are rounded to nearest on the way in
+ * (set_data, fill, generate_fbm) and widened exactly on every read, so an
+ * FP16 volume renders exactly as an FP32 volume holding the rounded values.
+ * The pyramid, TR levels, LUT and baked grid stay fp32.  The reference keeps
+ * the grid as float only (core/volume.hpp:47, datas). */
+typedef enum mrp_storage { MRP_STORAGE_FP32 = 0, MRP_STORAGE_FP16 = 1 } mrp_storage;
+mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out);
 /* ~VolumeRender (core/volume.cu:1151-1176) */
 mrp_status mrp_volume_destroy(mrp_volume* v);
 /* VolumeRender::SetDatas / SetData storage (core/volume.cu:1178-1184):

@@ -61,6 +61,14 @@ class VolumeRender {
         mrp_default_params(&params);
         datas.assign((size_t)resolution * resolution * resolution, 0.0f);
     }
+    // The same with the device grid in fp16 (MRP_STORAGE_FP16): half the
+    // HBM; the host copy `datas` stays float, as the reference's.
+    VolumeRender(int resolution, mrp_storage storage) : resolution(resolution) {
+        mrpnn::ensure_init();
+        mrpnn::check(mrp_volume_create_ex(resolution, storage, &h), "VolumeRender");
+        mrp_default_params(&params);
+        datas.assign((size_t)resolution * resolution * resolution, 0.0f);
+    }
     // VolumeRender(string path, bool cacheTR) -> LoadData (core/volume.cu:959-1149):
     // .bin / .txt / .vox (and the .bin cache beside a parsed file); Update
     // has run.  cacheTR has no effect: the baked TR grid is sized by

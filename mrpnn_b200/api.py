@@ -78,6 +78,7 @@ _SIGS = {
     "mrp_load_model": ([C.c_char_p], C.c_int),
     "mrp_default_params": ([C.POINTER(Params)], None),
     "mrp_volume_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "mrp_volume_create_ex": ([C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "mrp_volume_destroy": ([C.c_void_p], C.c_int),
     "mrp_volume_set_data": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "mrp_volume_fill": ([C.c_void_p, FILL_FN, C.c_void_p], C.c_int),
@@ -255,15 +256,23 @@ def tc_gemm_check(A, B, fp8=False):
     return D
 
 
+# density grid storage (mrp_storage)
+STORAGE = {"fp32": 0, "fp16": 1}
+
+
 class VolumeRender:
     """VolumeRender (core/volume.hpp:45-155) over a device-resident volume handle."""
     PT, RPNN, MRPNN = 0, 1, 2
 
-    def __init__(self, resolution, cacheTR=False, write_cache=True):
+    def __init__(self, resolution, cacheTR=False, write_cache=True, storage="fp32"):
         """VolumeRender(int resolution) or VolumeRender(string path, bool
         cacheTR) (core/volume.cu:948-967): a path loads a .bin / .txt / .vox
         file (LoadData) and runs Update; cacheTR has no effect here (the baked
-        TR grid is sized by SetBakeResolution, not by the load)."""
+        TR grid is sized by SetBakeResolution, not by the load).  storage
+        "fp16" keeps a new grid in half precision (values rounded to nearest
+        on the way in; renders as an fp32 grid of the rounded values)."""
+        if storage not in STORAGE:
+            raise ValueError(f"storage must be one of {sorted(STORAGE)}")
         _ensure_init()
         h = C.c_void_p()
         if isinstance(resolution, (str, bytes, os.PathLike)):
@@ -271,7 +280,7 @@ class VolumeRender:
             self._h = h
             self.resolution = int(self.info().res)
         else:
-            _check(lib().mrp_volume_create(int(resolution), C.byref(h)))
+            _check(lib().mrp_volume_create_ex(int(resolution), STORAGE[storage], C.byref(h)))
             self._h = h
             self.resolution = int(resolution)
         self._params = default_params()

@@ -250,9 +250,13 @@ mrp_status mrp_init(int device, const char* model_path) {
     return mrp_load_model(p.c_str());
 }
 
-mrp_status mrp_volume_create(int res, mrp_volume** out) {
+mrp_status mrp_volume_create(int res, mrp_volume** out) { return mrp_volume_create_ex(res, MRP_STORAGE_FP32, out); }
+
+mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) {
     TRY(need_init());
     if (!out || res < 2 || res > 2048) return fail(MRP_ERR_INVALID, "volume resolution %d out of range [2, 2048]", res);
+    if (storage != MRP_STORAGE_FP32 && storage != MRP_STORAGE_FP16)
+        return fail(MRP_ERR_INVALID, "unknown density storage %d", (int)storage);
     mrp_volume* v = new mrp_volume();
     v->res = res;
     mrp_default_params(&v->params);
@@ -265,7 +269,8 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
     size_t n = (size_t)res * res * res;
     v->occ_res = (res + (1 << v->occ_shift) - 1) >> v->occ_shift;
     size_t nocc = (size_t)v->occ_res * v->occ_res * v->occ_res;
-    if ((e = cudaMalloc(&v->density, n * sizeof(float))) != cudaSuccess ||
+    if ((storage == MRP_STORAGE_FP16 ? (e = cudaMalloc(&v->density_h, n * sizeof(__half)))
+                                     : (e = cudaMalloc(&v->density, n * sizeof(float)))) != cudaSuccess ||
         (e = cudaMalloc(&v->mips, kMipFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&v->lut, kLutAlloc * sizeof(float))) != cudaSuccess ||
@@ -278,7 +283,8 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
         (e = cudaMalloc(&v->pad_pair, kPadLevelFloats * sizeof(float2))) != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
                             cudaGetErrorString(e)));
-    cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
+    if (v->density_h) cudaMemsetAsync(v->density_h, 0, n * sizeof(__half), v->stream);
+    else cudaMemsetAsync(v->density, 0, n * sizeof(float), v->stream);
     *out = v;
     return MRP_OK;
 }
@@ -286,7 +292,7 @@ mrp_status mrp_volume_create(int res, mrp_volume** out) {
 mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
-    cudaFree(v->density); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
+    cudaFree(v->density); cudaFree(v->density_h); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
     cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->mips_pad); cudaFree(v->trs_pad); cudaFree(v->mip_tr); cudaFree(v->pad_pair); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
     cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
@@ -309,8 +315,28 @@ static void invalidate(mrp_volume* v) {
 mrp_status mrp_volume_set_data(mrp_volume* v, const float* data, int res, int is_device) {
     TRY(need_init());
     if (!v || !data || res != v->res) return fail(MRP_ERR_INVALID, "set_data: resolution %d != volume %d", res, v ? v->res : -1);
-    size_t bytes = (size_t)res * res * res * sizeof(float);
-    CU(cudaMemcpyAsync(v->density, data, bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, v->stream));
+    size_t n = (size_t)res * res * res;
+    if (!v->density_h) {
+        CU(cudaMemcpyAsync(v->density, data, n * sizeof(float), is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           v->stream));
+    } else if (is_device) {
+        CU(launch_narrow(data, n, v->density_h, g.sms, v->stream));
+    } else {
+        // fp16 storage from host floats: through a device staging buffer of
+        // at most 16 Mi floats, rounded on the device
+        const size_t chunk = std::min<size_t>(n, (size_t)16 << 20);
+        float* stage = nullptr;
+        CU(cudaMalloc(&stage, chunk * sizeof(float)));
+        cudaError_t e = cudaSuccess;
+        for (size_t i = 0; i < n && e == cudaSuccess; i += chunk) {
+            const size_t m = std::min(chunk, n - i);
+            e = cudaMemcpyAsync(stage, data + i, m * sizeof(float), cudaMemcpyHostToDevice, v->stream);
+            if (e == cudaSuccess) e = launch_narrow(stage, m, v->density_h + i, g.sms, v->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
+        cudaFree(stage);
+        CU(e);
+    }
     CU(cudaStreamSynchronize(v->stream));
     v->has_data = true;
     invalidate(v);
@@ -340,7 +366,8 @@ mrp_status mrp_volume_fill(mrp_volume* v, mrp_fill_fn fn, void* user) {
 mrp_status mrp_volume_generate_fbm(mrp_volume* v, uint32_t seed, float base_freq, int octaves, float gain) {
     TRY(need_init());
     if (!v || octaves < 1 || octaves > 16) return fail(MRP_ERR_INVALID, "fbm: bad arguments");
-    CU(launch_fbm(v->density, v->res, seed, base_freq, octaves, gain, g.sms, v->stream));
+    if (v->density_h) CU(launch_fbm(v->density_h, v->res, seed, base_freq, octaves, gain, g.sms, v->stream));
+    else CU(launch_fbm(v->density, v->res, seed, base_freq, octaves, gain, g.sms, v->stream));
     CU(cudaStreamSynchronize(v->stream));
     v->has_data = true;
     invalidate(v);
@@ -365,17 +392,20 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         int init;
         { float f0 = 0.00001f; std::memcpy(&init, &f0, sizeof init); }
         CU(cudaMemcpyAsync(v->d_maxbits, &init, sizeof(int), cudaMemcpyHostToDevice, v->stream));
-        CU(launch_max_density(v->density, n, v->d_maxbits, g.sms, v->stream));
+        if (v->density_h) CU(launch_max_density(v->density_h, n, v->d_maxbits, g.sms, v->stream));
+        else CU(launch_max_density(v->density, n, v->d_maxbits, g.sms, v->stream));
         int bits = 0;
         CU(cudaMemcpyAsync(&bits, v->d_maxbits, sizeof(int), cudaMemcpyDeviceToHost, v->stream));
         CU(cudaStreamSynchronize(v->stream));
         std::memcpy(&v->max_density, &bits, sizeof(float));
     }
-    CU(launch_occupancy(v->density, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
+    if (v->density_h) CU(launch_occupancy(v->density_h, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
+    else CU(launch_occupancy(v->density, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
     {
         const int init[6] = {R, R, R, -1, -1, -1};
         CU(cudaMemcpyAsync(v->d_bounds, init, sizeof init, cudaMemcpyHostToDevice, v->stream));
-        CU(launch_nonzero_bounds(v->density, R, v->d_bounds, g.sms, v->stream));
+        if (v->density_h) CU(launch_nonzero_bounds(v->density_h, R, v->d_bounds, g.sms, v->stream));
+        else CU(launch_nonzero_bounds(v->density, R, v->d_bounds, g.sms, v->stream));
         CU(cudaMemcpyAsync(v->nz_bounds, v->d_bounds, sizeof v->nz_bounds, cudaMemcpyDeviceToHost, v->stream));
         CU(cudaStreamSynchronize(v->stream));
         v->has_bounds = true;
@@ -385,14 +415,20 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         // below the input, then 9 levels 256 >> m, each from the previous one.
         int res = 256;
         while (res * 2 < R) res <<= 1;
+        // (the first level reads the density grid in its storage type; every
+        // level after it is fp32)
         const float* src = v->density;
         int src_res = R;
         float* tmp[2] = {nullptr, nullptr};
         int which = 0;
+        auto resample = [&](float* dst, int r) {
+            return src == nullptr && v->density_h ? launch_resample(dst, r, v->density_h, src_res, g.sms, v->stream)
+                                                  : launch_resample(dst, r, src, src_res, g.sms, v->stream);
+        };
         for (; res > 256; res >>= 1) {
             float*& t = tmp[which];
             if (!t) CU(cudaMalloc(&t, (size_t)res * res * res * sizeof(float)));
-            CU(launch_resample(t, res, src, src_res, g.sms, v->stream));
+            CU(resample(t, res));
             src = t;
             src_res = res;
             which ^= 1;
@@ -400,7 +436,7 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         for (int m = 0; m < 9; ++m) {
             int r = 256 >> m;
             float* dst = v->mips + mip_offset(m);
-            CU(launch_resample(dst, r, src, src_res, g.sms, v->stream));
+            CU(resample(dst, r));
             src = dst;
             src_res = r;
         }
@@ -433,7 +469,7 @@ mrp_status mrp_volume_get_info(const mrp_volume* v, mrp_volume_info* info) {
     info->tr_alpha = v->tr_alpha;
     for (int i = 0; i < 3; ++i) info->tr_light[i] = v->tr_light[i];
     size_t R = v->res;
-    info->device_bytes = R * R * R * 4 + kMipFloats * 4 + kTrFloats * 4 + kLut * kLut * 4 +
+    info->device_bytes = R * R * R * (v->density_h ? 2 : 4) + kMipFloats * 4 + kTrFloats * 4 + kLut * kLut * 4 +
                          (size_t)v->baked_alloc_res * v->baked_alloc_res * v->baked_alloc_res * 4;
     return MRP_OK;
 }
@@ -463,7 +499,7 @@ mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* 
     const void* src = nullptr;
     size_t n = 0, esize = sizeof(float);
     switch (which) {
-        case MRP_RES_DENSITY: src = v->density; n = (size_t)v->res * v->res * v->res; break;
+        case MRP_RES_DENSITY: src = v->density; n = (size_t)v->res * v->res * v->res; break;   // fp16: below
         case MRP_RES_MIP:
             if (level < 0 || level > 8) return fail(MRP_ERR_INVALID, "mip level %d", level);
             src = v->mips + mip_offset(level); n = (size_t)(256 >> level) * (256 >> level) * (256 >> level); break;
@@ -479,6 +515,27 @@ mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* 
     }
     if (count) *count = n;
     if (!dst) return MRP_OK;
+    if (which == MRP_RES_DENSITY && v->density_h) {   // fp16 storage, widened to the caller's floats
+        if (dst_is_device) {
+            CU(launch_widen(v->density_h, n, dst, g.sms, v->stream));
+        } else {
+            const size_t chunk = std::min<size_t>(n, (size_t)16 << 20);
+            float* stage = nullptr;
+            CU(cudaMalloc(&stage, chunk * sizeof(float)));
+            cudaError_t e = cudaSuccess;
+            for (size_t i = 0; i < n && e == cudaSuccess; i += chunk) {
+                const size_t m = std::min(chunk, n - i);
+                e = launch_widen(v->density_h + i, m, stage, g.sms, v->stream);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(dst + i, stage, m * sizeof(float), cudaMemcpyDeviceToHost, v->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
+            }
+            cudaFree(stage);
+            CU(e);
+        }
+        CU(cudaStreamSynchronize(v->stream));
+        return MRP_OK;
+    }
     CU(cudaMemcpyAsync(dst, src, n * esize, dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, v->stream));
     CU(cudaStreamSynchronize(v->stream));
     return MRP_OK;

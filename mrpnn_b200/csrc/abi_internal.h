@@ -99,7 +99,8 @@ struct mrp_volume {
     float last_ms = 0.0f;
     float stage_ms[3] = {0, 0, 0};
     bool stages_valid = false;
-    float* density = nullptr;
+    float* density = nullptr;       // fp32 storage, or
+    __half* density_h = nullptr;    // fp16 storage (MRP_STORAGE_FP16)
     float* mips = nullptr;
     float* trs = nullptr;
     float* lut = nullptr;
@@ -147,6 +148,7 @@ struct mrp_volume {
     VolumeDev dev() const {
         VolumeDev d{};
         d.density = density;
+        d.density_h = density_h;
         d.res = res;
         d.max_density = max_density;
         d.mips = mips;

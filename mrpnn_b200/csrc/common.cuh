@@ -10,6 +10,8 @@
 // last bit, which the parity tests allow for.
 #pragma once
 #include <cstdint>
+#include <type_traits>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #define MRP_HD __host__ __device__ __forceinline__
@@ -148,6 +150,11 @@ struct Stream {
 // for tex3D/tex2D (see the oracle for the exact definition): texel coordinate
 // u*N - 0.5, fastest axis interpolated first, weights in fp32.
 // ---------------------------------------------------------------------------
+// Loads of a grid texel as float: fp32 storage, or fp16 storage widened
+// (exact: every fp16 value is a float, so a grid stored in fp16 yields the
+// same floats as an fp32 grid holding those values).
+MRP_D float ldg_f(const float* p) { return __ldg(p); }
+MRP_D float ldg_f(const __half* p) { return __half2float(__ldg(p)); }
 MRP_D float fetch_border(const float* __restrict__ g, int n, int x, int y, int z) {
     if ((unsigned)x >= (unsigned)n || (unsigned)y >= (unsigned)n || (unsigned)z >= (unsigned)n) return 0.0f;
     return __ldg(g + ((size_t)x * n + y) * n + z);
@@ -162,8 +169,8 @@ MRP_D float lerp_w(float a, float b, float v, float omv) { return fa(fm(a, omv),
 // (so every load is in bounds); border mode then zeroes the texels whose
 // unclamped coordinate lies outside [0, n).  Values and the order of the
 // seven lerps are those of fetch_border / fetch_clamp above.
-template <bool Clamp>
-MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
+template <bool Clamp, class T = float>
+MRP_D float tex3(const T* __restrict__ g, int n, f3 pos) {
     f3 uv = adds(pos, 0.5f);
     float nf = (float)n;
     float px = fs(fm(uv.x, nf), 0.5f), py = fs(fm(uv.y, nf), 0.5f), pz = fs(fm(uv.z, nf), 0.5f);
@@ -175,17 +182,17 @@ MRP_D float tex3(const float* __restrict__ g, int n, f3 pos) {
     float t000, t001, t010, t011, t100, t101, t110, t111;
     if ((unsigned)x < (unsigned)(n - 1) && (unsigned)y < (unsigned)(n - 1) && (unsigned)z < (unsigned)(n - 1)) {
         // footprint inside the grid: the clamps and border selects are no-ops
-        const float* b = g + ((size_t)x * n + y) * n + z;
-        t000 = __ldg(b); t001 = __ldg(b + 1); t010 = __ldg(b + n); t011 = __ldg(b + n + 1);
-        t100 = __ldg(b + nn); t101 = __ldg(b + nn + 1); t110 = __ldg(b + nn + n); t111 = __ldg(b + nn + n + 1);
+        const T* b = g + ((size_t)x * n + y) * n + z;
+        t000 = ldg_f(b); t001 = ldg_f(b + 1); t010 = ldg_f(b + n); t011 = ldg_f(b + n + 1);
+        t100 = ldg_f(b + nn); t101 = ldg_f(b + nn + 1); t110 = ldg_f(b + nn + n); t111 = ldg_f(b + nn + n + 1);
     } else {
         int x0 = min(max(x, 0), n - 1), x1 = min(max(x + 1, 0), n - 1);
         int y0 = min(max(y, 0), n - 1) * n, y1 = min(max(y + 1, 0), n - 1) * n;
         int z0 = min(max(z, 0), n - 1), z1 = min(max(z + 1, 0), n - 1);
-        const float* p0 = g + (size_t)x0 * nn;
-        const float* p1 = g + (size_t)x1 * nn;
-        t000 = __ldg(p0 + y0 + z0); t001 = __ldg(p0 + y0 + z1); t010 = __ldg(p0 + y1 + z0); t011 = __ldg(p0 + y1 + z1);
-        t100 = __ldg(p1 + y0 + z0); t101 = __ldg(p1 + y0 + z1); t110 = __ldg(p1 + y1 + z0); t111 = __ldg(p1 + y1 + z1);
+        const T* p0 = g + (size_t)x0 * nn;
+        const T* p1 = g + (size_t)x1 * nn;
+        t000 = ldg_f(p0 + y0 + z0); t001 = ldg_f(p0 + y0 + z1); t010 = ldg_f(p0 + y1 + z0); t011 = ldg_f(p0 + y1 + z1);
+        t100 = ldg_f(p1 + y0 + z0); t101 = ldg_f(p1 + y0 + z1); t110 = ldg_f(p1 + y1 + z0); t111 = ldg_f(p1 + y1 + z1);
         if (!Clamp) {
             bool vx0 = (unsigned)x < (unsigned)n, vx1 = (unsigned)(x + 1) < (unsigned)n;
             bool vy0 = (unsigned)y < (unsigned)n, vy1 = (unsigned)(y + 1) < (unsigned)n;
@@ -377,7 +384,8 @@ MRP_D float tex_lut_fast(const float* __restrict__ lut, float u, float v) {
 // Device view of one volume's resources (passed by value to kernels).
 // ---------------------------------------------------------------------------
 struct VolumeDev {
-    const float* density;   // res^3, z fastest
+    const float* density;   // res^3, z fastest (fp32 storage), or null
+    const __half* density_h;   // the same grid in fp16 storage, or null
     int res;
     float max_density;
     const float* mips;      // 9 levels (256>>m)^3, concatenated (offsets: mip_offset)
@@ -437,7 +445,8 @@ constexpr int kMipOccBytes = 32 * 32 * 32 + 16 * 16 * 16 + 8 * 8 * 8 + 4 * 4 * 4
 
 // tex3<false> of an n^3 grid with brick flags occ (nb = ceil(n / 8) per
 // axis, shift 3); returns 0 without touching the grid for empty bricks.
-MRP_D float tex3_occ(const float* __restrict__ g, int n, const uint8_t* __restrict__ occ, int nb, f3 pos) {
+template <class T>
+MRP_D float tex3_occ(const T* __restrict__ g, int n, const uint8_t* __restrict__ occ, int nb, f3 pos) {
     f3 uv = adds(pos, 0.5f);
     float nf = (float)n;
     int x = (int)floorf(fs(fm(uv.x, nf), 0.5f)), y = (int)floorf(fs(fm(uv.y, nf), 0.5f)),
@@ -447,9 +456,27 @@ MRP_D float tex3_occ(const float* __restrict__ g, int n, const uint8_t* __restri
     if (__ldg(occ + b) == 0) return 0.0f;
     return tex3<false>(g, n, pos);
 }
-// Density() of the full-resolution grid with its bricks.
+// Density() of the full-resolution grid (fp32 or fp16 storage).
+MRP_D float density_tex(const VolumeDev& v, f3 p) {
+    return v.density_h ? tex3<false>(v.density_h, v.res, p) : tex3<false>(v.density, v.res, p);
+}
+// The same with the storage type fixed at compile time (DT float: fp32,
+// __half: fp16), for the kernels that instantiate one copy per type and so
+// keep the test off their inner loops; DT void chooses per call.
+template <class DT>
+MRP_D float density_as(const VolumeDev& v, f3 p) {
+    if constexpr (std::is_same<DT, float>::value) return tex3<false>(v.density, v.res, p);
+    else if constexpr (std::is_same<DT, __half>::value) return tex3<false>(v.density_h, v.res, p);
+    else return density_tex(v, p);
+}
+// Density() of the full-resolution grid with its bricks (DT as density_as).
+template <class DT = void>
 MRP_D float density_occ(const VolumeDev& v, f3 p) {
-    return v.occ ? tex3_occ(v.density, v.res, v.occ, v.occ_res, p) : tex3<false>(v.density, v.res, p);
+    if constexpr (std::is_same<DT, float>::value)
+        return v.occ ? tex3_occ(v.density, v.res, v.occ, v.occ_res, p) : tex3<false>(v.density, v.res, p);
+    else if constexpr (std::is_same<DT, __half>::value)
+        return v.occ ? tex3_occ(v.density_h, v.res, v.occ, v.occ_res, p) : tex3<false>(v.density_h, v.res, p);
+    else return v.density_h ? density_occ<__half>(v, p) : density_occ<float>(v, p);
 }
 // Mip level m of the pyramid (256 >> m) at p, with bricks for m < kOccMips.
 MRP_D float mip_density(const VolumeDev& v, int m, f3 p) {
@@ -464,6 +491,7 @@ MRP_D float mip_density(const VolumeDev& v, int m, f3 p) {
 // tracking with termination until tr <= 0.001, through the full-resolution
 // density.  Both loops share the reference's 10000-iteration bound.
 // ---------------------------------------------------------------------------
+template <class DT = void>
 MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float dis, float alpha) {
     float smax = fm(v.max_density, alpha);
     float tr = 1.0f, t = 0.0f;
@@ -472,7 +500,7 @@ MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float 
         float rk = st.next();
         t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
         if (t > dis) break;
-        float d = density_occ(v, add(pos, mul(dir, t)));
+        float d = density_occ<DT>(v, add(pos, mul(dir, t)));
         float S = fm(d, alpha);
         tr = fm(tr, fs(1.0f, fmaxf(0.0f, fd(S, smax))));
         if (d < 0) t = fs(t, d);
@@ -481,7 +509,7 @@ MRP_D float transmittance(const VolumeDev& v, Stream& st, f3 pos, f3 dir, float 
         float rk = st.next();
         t = fs(t, fm(fd(logf(fs(1.0f, rk)), smax), v.tr_scale));
         if (t > dis) break;
-        float d = density_occ(v, add(pos, mul(dir, t)));
+        float d = density_occ<DT>(v, add(pos, mul(dir, t)));
         float S = fm(d, alpha);
         if (st.next() < fmaxf(0.0f, fd(S, smax))) { tr = 0.0f; break; }
         if (d < 0) t = fs(t, d);

@@ -5,11 +5,20 @@
 namespace mrp {
 
 // volume_kernels.cu
+// The density grid's builders take fp32 or fp16 storage (VolumeDev::density
+// or density_h); everything derived from it (pyramid, TR, LUT) is fp32.
 cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
                        cudaStream_t s);
+cudaError_t launch_fbm(__half* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
+                       cudaStream_t s);
+cudaError_t launch_narrow(const float* in, size_t n, __half* out, int sms, cudaStream_t s);
+cudaError_t launch_widen(const __half* in, size_t n, float* out, int sms, cudaStream_t s);
 cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s);
+cudaError_t launch_resample(float* out, int res, const __half* src, int src_res, int sms, cudaStream_t s);
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s);
+cudaError_t launch_max_density(const __half* d, size_t n, int* out_bits, int sms, cudaStream_t s);
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
+cudaError_t launch_occupancy(const __half* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
 // VolumeDev::pad_pair from the padded mips and TR levels (kPadLevelFloats pairs).
 cudaError_t launch_pair_padded(const float* mips_pad, const float* trs_pad, float2* out, cudaStream_t s);
 // VolumeDev::mip_tr from the pyramid and the TR levels (mip_tr_offset(5) pairs).
@@ -21,6 +30,7 @@ cudaError_t launch_pad_levels(const float* l8, const float* l4, const float* l2,
 // Index bounds of the nonzero voxels: out6 = {min x, min y, min z, max x,
 // max y, max z}, which must start at {R, R, R, -1, -1, -1}.
 cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s);
+cudaError_t launch_nonzero_bounds(const __half* d, int R, int* out6, int sms, cudaStream_t s);
 cudaError_t launch_tr_level(float* out, int res, const float* src, const uint8_t* src_occ, float alpha, const float L[3], int sms,
                             cudaStream_t s);
 cudaError_t set_halton_permutations(const uint32_t perm[28]);

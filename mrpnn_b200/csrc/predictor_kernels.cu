@@ -75,7 +75,7 @@ cudaError_t set_stencil_tables(const StencilTables& t) {
     return cudaMemcpyToSymbol(c_dirs, t.dirs, sizeof t.dirs);
 }
 
-MRP_D float density(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
+MRP_D float density(const VolumeDev& v, f3 p) { return density_tex(v, p); }
 MRP_D const float* mip_level(const VolumeDev& v, int m) { return v.mips + mip_offset(m); }
 MRP_D const float* tr_level(const VolumeDev& v, int m) { return v.trs + tr_offset(m); }
 
@@ -121,6 +121,7 @@ MRP_D float brick_exit(float c, float sR, float isR, int b, int sh) {
 // *t_brick: when the brick proves the value 0 and the base voxel lies inside
 // the grid, the t up to which the ray stays in that brick (the march's next
 // steps there read 0 as well); else -1.
+template <class DT>
 MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* tl, float* t_brick) {
     const int R1 = v.res - 1, sh = v.occ_shift, nb = v.occ_res;
     const int xi = __float2int_rd(fmaf(m.sR.x, t, m.c.x));
@@ -135,11 +136,13 @@ MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* 
         return 0.0f;
     }
     if (tl) tl->fetches++;
-    return tex3<false>(v.density, v.res, add(m.pos, mul(m.dir, t)));
+    return density_as<DT>(v, add(m.pos, mul(m.dir, t)));
 }
 
 // DeterminateEstimatedHit(float& alpha, ...) (core/render.cuh:105-197).
-// pass_rate = exp(-t_step * SMax) is computed once on the host.
+// pass_rate = exp(-t_step * SMax) is computed once on the host.  DT: the
+// density grid's storage type (void: read from the volume per fetch).
+template <class DT = void>
 MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 pos, f3 dir, float dis, f3* next,
                          Tally* tl = nullptr) {
     float smax = fm(v.max_density, alpha);
@@ -199,9 +202,9 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
         if (tl) tl->steps++;
         float d, t_brick = -1.0f;
         if (v.occ) {
-            d = density_skip(v, mr, t, tl, &t_brick);
+            d = density_skip<DT>(v, mr, t, tl, &t_brick);
         } else {
-            d = density(v, add(pos, mul(dir, t)));
+            d = density_as<DT>(v, add(pos, mul(dir, t)));
             if (tl) tl->fetches++;
         }
         if (d > 0) {
@@ -248,6 +251,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
 }
 
 // GetSamplePoint (core/render.cuh:436-462)
+template <class DT = void>
 MRP_D bool first_hit(const VolumeDev& v, f3 ori, f3 dir, float alpha, float pass_rate, f3* hit, Tally* tl = nullptr) {
     dir = normalize(dir);
     *hit = mk3(0, 0, 0);
@@ -256,7 +260,7 @@ MRP_D bool first_hit(const VolumeDev& v, f3 ori, f3 dir, float alpha, float pass
     f3 sp = add(ori, mul(dir, dis));
     float md = ray_box_distance(sp, dir);
     f3 p;
-    bool in = estimated_hit(v, alpha, pass_rate, sp, dir, md, &p, tl);
+    bool in = estimated_hit<DT>(v, alpha, pass_rate, sp, dir, md, &p, tl);
     if (in) *hit = p;
     return in;
 }
@@ -788,7 +792,7 @@ MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
 // 128-thread blocks, ten resident per SM (48 registers): a block retires as
 // soon as its slowest ray ends, and march lengths vary from 0 to ~1000 steps.
 constexpr int kHitThreads = 128;
-template <bool COUNT>
+template <bool COUNT, class DT>
 __global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
     Tally tally;
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -807,7 +811,7 @@ __global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w,
         }
         f3 L = normalize(w.light_dir);
         Stream st(kPixelStream, (uint32_t)pix, 0, (uint32_t)w.frame, w.seed);   // InitRand again
-        active = first_hit(v, ori, dir, w.alpha, w.pass_rate, &hit, COUNT ? &tally : nullptr);
+        active = first_hit<DT>(v, ori, dir, w.alpha, w.pass_rate, &hit, COUNT ? &tally : nullptr);
         if (COUNT) {
             tally.events += active ? 1 : 0;
             tally.lookups += active ? 192 : 0;
@@ -925,8 +929,14 @@ cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, 
     cudaError_t e = cudaMemsetAsync(rec.count, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
     const int blocks = (n + kHitThreads - 1) / kHitThreads;
-    if (view.counters) k_hit<true><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
-    else k_hit<false><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+    // one copy of the march per counting mode and density storage type
+    if (v.density_h) {
+        if (view.counters) k_hit<true, __half><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+        else k_hit<false, __half><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+    } else {
+        if (view.counters) k_hit<true, float><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+        else k_hit<false, float><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+    }
     return cudaGetLastError();
 }
 // ---------------------------------------------------------------------------

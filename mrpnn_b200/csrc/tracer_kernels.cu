@@ -42,11 +42,12 @@ struct LaneStream {
 
 // nee_mode 1: one unbiased Tr() estimate from the sample's NEE stream,
 // positioned at draw *n.
+template <class DT>
 __device__ __forceinline__ float nee_tr(const VolumeDev& v, const ViewDev& w, int pix, int k, uint32_t* n, f3 p, f3 L) {
     Stream s(kNeeStream, (uint32_t)pix, (uint32_t)k, (uint32_t)w.frame, w.seed);
     s.n = *n;
     if (s.n & 3) philox(s.n >> 2, s.sub, s.frame, s.kind, s.k0, s.k1, s.blk);
-    float tr = transmittance(v, s, p, L, ray_box_distance(p, L), w.alpha);
+    float tr = transmittance<DT>(v, s, p, L, ray_box_distance(p, L), w.alpha);
     *n = s.n;
     return tr;
 }
@@ -65,7 +66,7 @@ MRP_D void deposit(double* __restrict__ sum3, double* __restrict__ sumsq3, int* 
 }
 }  // namespace
 
-template <bool COUNT>
+template <bool COUNT, class DT>
 __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ VolumeDev v,
                                                const __grid_constant__ ViewDev w, double* __restrict__ sum3,
                                                double* __restrict__ sumsq3, int* __restrict__ first_pos,
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
                 continue;
             }
             rk = st.next(pix, k, frame, seed);
-            float d = density_t(v, add(p, mul(rd, t)));
+            float d = density_t<DT>(v, add(p, mul(rd, t)));
             if (COUNT) tally.fetches++;
             float S = fm(d, w.alpha);
             hit = fd(S, smax) > rk;
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
         p = add(mul(rd, t), p);
         csr = mul(csr, v.scatter_rate);
         float ph = hg(dot(rd, L), w.g);
-        float tr = v.nee_mode ? nee_tr(v, w, pix, k, &nee_n, p, L) : tex3<true>(v.baked, v.baked_res, p);
+        float tr = v.nee_mode ? nee_tr<DT>(v, w, pix, k, &nee_n, p, L) : tex3<true>(v.baked, v.baked_res, p);
         if (COUNT) tally.lookups++;
         res = add(res, mul(mul(w.light_color, csr), fm(tr, ph)));
         rd = nd;
@@ -286,8 +287,14 @@ cudaError_t launch_fill_int(int* p, int n, int value, cudaStream_t s) {
 
 cudaError_t launch_trace(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
                          unsigned long long* counter, int sms, cudaStream_t s) {
-    if (view.counters) k_trace<true><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
-    else k_trace<false><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    // one copy of the event loop per counting mode and density storage type
+    if (v.density_h) {
+        if (view.counters) k_trace<true, __half><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+        else k_trace<false, __half><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    } else {
+        if (view.counters) k_trace<true, float><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+        else k_trace<false, float><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_get_samples(const VolumeDev& v, const float* alpha, const float* ori, const float* dir,

@@ -8,7 +8,9 @@ namespace mrp {
 
 // Free-flight lookups stay plain: delta tracking takes few steps in empty
 // bricks, so the brick test cost more than it saved (measured).
-MRP_D float density_t(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
+// DT: the density grid's storage type, or void (read from the volume per fetch).
+template <class DT = void>
+MRP_D float density_t(const VolumeDev& v, f3 p) { return density_as<DT>(v, p); }
 
 // DeterminateNextVertex.  SampleHenyeyGreenstein(Rand, Rand, ...) takes the
 // first draw as e1 and the second as e0 (x86-64 g++ argument order).

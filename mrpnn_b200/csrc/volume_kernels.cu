@@ -54,12 +54,25 @@ MRP_D float fbm_voxel(int R, int x, int y, int z, uint32_t seed, float base_freq
     float fall = fm(fm(t, t), fs(3.0f, fm(2.0f, t)));
     return fminf(fmaxf(fm(n, fall), 0.0f), 1.0f);
 }
-__global__ void k_fbm(float* __restrict__ out, int R, uint32_t seed, float base_freq, int octaves, float gain) {
+// Stores of a grid texel: fp32, or fp16 storage (round to nearest even).
+MRP_D void st_f(float* p, float v) { *p = v; }
+MRP_D void st_f(__half* p, float v) { *p = __float2half_rn(v); }
+template <class T>
+__global__ void k_fbm(T* __restrict__ out, int R, uint32_t seed, float base_freq, int octaves, float gain) {
     size_t n = (size_t)R * R * R;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         int z = (int)(i % R), y = (int)((i / R) % R), x = (int)(i / ((size_t)R * R));
-        out[i] = fbm_voxel(R, x, y, z, seed, base_freq, octaves, gain);
+        st_f(out + i, fbm_voxel(R, x, y, z, seed, base_freq, octaves, gain));
     }
+}
+// fp32 <-> fp16 storage of a grid (set_data into an fp16 volume, readback).
+__global__ void k_narrow(const float* __restrict__ in, size_t n, __half* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __float2half_rn(in[i]);
+}
+__global__ void k_widen(const __half* __restrict__ in, size_t n, float* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __half2float(in[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -67,11 +80,13 @@ __global__ void k_fbm(float* __restrict__ out, int R, uint32_t seed, float base_
 // (border 0, negative values clamped, core/volume.cu:835-863) at texel
 // centres u = (i + 0.5) / res (ParallelFill, core/omp.cpp:11-13).
 // ---------------------------------------------------------------------------
-MRP_D float cpu_fetch(const float* __restrict__ d, int res, int x, int y, int z) {
+template <class T>
+MRP_D float cpu_fetch(const T* __restrict__ d, int res, int x, int y, int z) {
     if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res) return 0.0f;
-    return fmaxf(0.0f, __ldg(d + ((size_t)x * res + y) * res + z));
+    return fmaxf(0.0f, ldg_f(d + ((size_t)x * res + y) * res + z));
 }
-__global__ void k_resample(float* __restrict__ out, int res, const float* __restrict__ src, int src_res) {
+template <class T>
+__global__ void k_resample(float* __restrict__ out, int res, const T* __restrict__ src, int src_res) {
     size_t n = (size_t)res * res * res;
     float sr = (float)src_res;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -94,10 +109,11 @@ __global__ void k_resample(float* __restrict__ out, int res, const float* __rest
 // default 1e-5 (core/volume.hpp:104).  Densities are compared as int bits,
 // which orders non-negative floats; negative (SDF) values never win.
 // ---------------------------------------------------------------------------
-__global__ void k_max_density(const float* __restrict__ d, size_t n, int* __restrict__ out_bits) {
+template <class T>
+__global__ void k_max_density(const T* __restrict__ d, size_t n, int* __restrict__ out_bits) {
     float m = 0.00001f;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        m = fmaxf(m, __ldg(d + i));
+        m = fmaxf(m, ldg_f(d + i));
     for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_int(m));
 }
@@ -145,16 +161,17 @@ __global__ void k_pad_levels(const float* __restrict__ l8, const float* __restri
 
 // One warp per grid row (x, y): the lanes scan z, the warp keeps the bounds
 // of the nonzero voxels it saw and adds them with six atomics at the end.
-__global__ void k_nonzero_bounds(const float* __restrict__ d, int R, int* __restrict__ out6) {
+template <class T>
+__global__ void k_nonzero_bounds(const T* __restrict__ d, int R, int* __restrict__ out6) {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x / 32);
     int lo[3] = {R, R, R}, hi[3] = {-1, -1, -1};
     for (long long row = blockIdx.x * (long long)(blockDim.x / 32) + threadIdx.x / 32; row < (long long)R * R;
          row += warps) {
-        const float* p = d + row * R;
+        const T* p = d + row * R;
         int zlo = R, zhi = -1;
         for (int z = lane; z < R; z += 32)
-            if (__ldg(p + z) != 0.0f) { zlo = min(zlo, z); zhi = max(zhi, z); }
+            if (ldg_f(p + z) != 0.0f) { zlo = min(zlo, z); zhi = max(zhi, z); }
         zlo = __reduce_min_sync(0xffffffffu, zlo);
         zhi = __reduce_max_sync(0xffffffffu, zhi);
         if (zhi >= 0) {
@@ -184,7 +201,8 @@ __global__ void k_nonzero_bounds(const float* __restrict__ d, int R, int* __rest
 // 0 exactly for every sample whose base voxel is in it or within one voxel
 // of it (border texels are 0 by addressing).
 // ---------------------------------------------------------------------------
-__global__ void k_occupancy(const float* __restrict__ d, int R, int shift, int nb, uint8_t* __restrict__ occ) {
+template <class T>
+__global__ void k_occupancy(const T* __restrict__ d, int R, int shift, int nb, uint8_t* __restrict__ occ) {
     int total = nb * nb * nb;
     for (int b = blockIdx.x; b < total; b += gridDim.x) {
         int bz = b % nb, by = (b / nb) % nb, bx = b / (nb * nb);
@@ -195,7 +213,7 @@ __global__ void k_occupancy(const float* __restrict__ d, int R, int shift, int n
         for (int t = threadIdx.x; t < span * span * span && !any; t += blockDim.x) {
             int z = z0 + t % span, y = y0 + (t / span) % span, x = x0 + t / (span * span);
             if ((unsigned)x < (unsigned)R && (unsigned)y < (unsigned)R && (unsigned)z < (unsigned)R)
-                any |= __ldg(d + ((size_t)x * R + y) * R + z) != 0.0f;
+                any |= ldg_f(d + ((size_t)x * R + y) * R + z) != 0.0f;
         }
         any = __syncthreads_or(any);
         if (threadIdx.x == 0) occ[b] = any ? 1 : 0;
@@ -315,7 +333,7 @@ __global__ void k_hg_lut(float* __restrict__ lut, float g, uint32_t seed) {
     lut[j * kLut + i] = fd(h, 1024.0f);
 }
 
-MRP_D float density(const VolumeDev& v, f3 p) { return tex3<false>(v.density, v.res, p); }
+MRP_D float density(const VolumeDev& v, f3 p) { return density_tex(v, p); }
 
 // Fill_BakeTR (core/volume.cu:1562-1587) over voxels [first, first+count).
 // replicate != 0 restarts the voxel's stream for every estimate, as InitRand
@@ -349,17 +367,44 @@ static int grid_for(size_t n, int block, int sms) {
     return (int)(g < cap ? (g ? g : 1) : cap);
 }
 
+template <class T>
+static cudaError_t fbm_t(T* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
+                         cudaStream_t s) {
+    k_fbm<T><<<grid_for((size_t)R * R * R, 256, sms), 256, 0, s>>>(out, R, seed, base_freq, octaves, gain);
+    return cudaGetLastError();
+}
 cudaError_t launch_fbm(float* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
                        cudaStream_t s) {
-    k_fbm<<<grid_for((size_t)R * R * R, 256, sms), 256, 0, s>>>(out, R, seed, base_freq, octaves, gain);
+    return fbm_t(out, R, seed, base_freq, octaves, gain, sms, s);
+}
+cudaError_t launch_fbm(__half* out, int R, uint32_t seed, float base_freq, int octaves, float gain, int sms,
+                       cudaStream_t s) {
+    return fbm_t(out, R, seed, base_freq, octaves, gain, sms, s);
+}
+cudaError_t launch_narrow(const float* in, size_t n, __half* out, int sms, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_narrow<<<grid_for(n, 256, sms), 256, 0, s>>>(in, n, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_widen(const __half* in, size_t n, float* out, int sms, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_widen<<<grid_for(n, 256, sms), 256, 0, s>>>(in, n, out);
     return cudaGetLastError();
 }
 cudaError_t launch_resample(float* out, int res, const float* src, int src_res, int sms, cudaStream_t s) {
-    k_resample<<<grid_for((size_t)res * res * res, 256, sms), 256, 0, s>>>(out, res, src, src_res);
+    k_resample<float><<<grid_for((size_t)res * res * res, 256, sms), 256, 0, s>>>(out, res, src, src_res);
+    return cudaGetLastError();
+}
+cudaError_t launch_resample(float* out, int res, const __half* src, int src_res, int sms, cudaStream_t s) {
+    k_resample<__half><<<grid_for((size_t)res * res * res, 256, sms), 256, 0, s>>>(out, res, src, src_res);
     return cudaGetLastError();
 }
 cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms, cudaStream_t s) {
-    k_max_density<<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
+    k_max_density<float><<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
+    return cudaGetLastError();
+}
+cudaError_t launch_max_density(const __half* d, size_t n, int* out_bits, int sms, cudaStream_t s) {
+    k_max_density<__half><<<grid_for(n, 256, sms), 256, 0, s>>>(d, n, out_bits);
     return cudaGetLastError();
 }
 cudaError_t launch_interleave_mip_tr(const float* mips, const float* trs, float2* out, int sms, cudaStream_t s) {
@@ -375,16 +420,30 @@ cudaError_t launch_pad_levels(const float* l8, const float* l4, const float* l2,
     k_pad_levels<<<dim3(1, 3), 256, 0, s>>>(l8, l4, l2, clamp ? 1 : 0, out);
     return cudaGetLastError();
 }
-cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s) {
+template <class T>
+static cudaError_t nonzero_bounds_t(const T* d, int R, int* out6, int sms, cudaStream_t s) {
     long long rows = (long long)R * R;
     int blocks = (int)((rows + 7) / 8 < sms * 16 ? (rows + 7) / 8 : sms * 16);
-    k_nonzero_bounds<<<blocks, 256, 0, s>>>(d, R, out6);
+    k_nonzero_bounds<T><<<blocks, 256, 0, s>>>(d, R, out6);
+    return cudaGetLastError();
+}
+cudaError_t launch_nonzero_bounds(const float* d, int R, int* out6, int sms, cudaStream_t s) {
+    return nonzero_bounds_t(d, R, out6, sms, s);
+}
+cudaError_t launch_nonzero_bounds(const __half* d, int R, int* out6, int sms, cudaStream_t s) {
+    return nonzero_bounds_t(d, R, out6, sms, s);
+}
+template <class T>
+static cudaError_t occupancy_t(const T* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s) {
+    int total = nb * nb * nb;
+    k_occupancy<T><<<total < sms * 16 ? total : sms * 16, 256, 0, s>>>(d, R, shift, nb, occ);
     return cudaGetLastError();
 }
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s) {
-    int total = nb * nb * nb;
-    k_occupancy<<<total < sms * 16 ? total : sms * 16, 256, 0, s>>>(d, R, shift, nb, occ);
-    return cudaGetLastError();
+    return occupancy_t(d, R, shift, nb, occ, sms, s);
+}
+cudaError_t launch_occupancy(const __half* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s) {
+    return occupancy_t(d, R, shift, nb, occ, sms, s);
 }
 cudaError_t launch_tr_level(float* out, int res, const float* src, const uint8_t* src_occ, float alpha,
                             const float L[3], int sms, cudaStream_t s) {

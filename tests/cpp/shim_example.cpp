@@ -2,7 +2,8 @@
 // 0.25 at the centre, Update, Render / Camera::RenderToFile) compiled against
 // include/mrpnn_volume_render.hpp and run on libmrpnn_b200.so.
 //
-// usage: shim_example <out_prefix>   -> <out_prefix>.f32 (raw float4 frame), <out_prefix>.png
+// usage: shim_example <out_prefix>   -> <out_prefix>.f32 (raw float4 frame), <out_prefix>.png,
+//                                       <out_prefix>.fp16.f32 (the frame of an fp16-stored grid)
 #include <cstdio>
 #include <fstream>
 
@@ -35,6 +36,17 @@ int main(int argc, char** argv) {
         auto img = v.Render(int2{64, 64}, ori, u, r, L, VolumeRender::MRPNN, 0.857f, 8.0f, float3{1, 1, 1}, 1, 2);
         std::ofstream(out + ".f32", std::ios::binary).write(reinterpret_cast<const char*>(img.data()),
                                                            img.size() * sizeof(float4));
+        // the same volume with its device grid in fp16 (0 and 1 are exact)
+        VolumeRender v16(64, MRP_STORAGE_FP16);
+        v16.SetDatas([](int, int, int, float u, float w, float z) {
+            float dx = u - 0.5f, dy = w - 0.5f, dz = z - 0.5f;
+            return std::sqrt(dx * dx + dy * dy + dz * dz) < 0.25f ? 1.0f : 0.0f;
+        });
+        v16.Update();
+        v16.SetScatterRate(0.99f);
+        auto img16 = v16.Render(int2{64, 64}, ori, u, r, L, VolumeRender::MRPNN, 0.857f, 8.0f, float3{1, 1, 1}, 1, 2);
+        std::ofstream(out + ".fp16.f32", std::ios::binary)
+            .write(reinterpret_cast<const char*>(img16.data()), img16.size() * sizeof(float4));
         double s = 0;
         int hits = 0;
         for (auto& p : img) { s += p.x + p.y + p.z; hits += p.w > 0; }

@@ -44,3 +44,5 @@ def test_shim_renders_like_python_api(tmp_path):
     ref = v.Render((64, 64), ori, up, right, L, M.VolumeRender.MRPNN, 0.857, 8.0, (1, 1, 1), 1, 2)
     assert (img[..., 3] > 0).sum() > 100
     np.testing.assert_allclose(img, ref, rtol=1e-5, atol=1e-6)
+    img16 = np.fromfile(prefix + ".fp16.f32", np.float32).reshape(64, 64, 4)
+    np.testing.assert_array_equal(img16.view(np.uint32), img.view(np.uint32))
