@@ -181,6 +181,24 @@ mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float al
  * width*height float4 (RGB, A = coverage for PT / hit distance for MRPNN). */
 mrp_status mrp_render(mrp_volume* v, const mrp_view* view, mrp_render_type type, int sample_num, float* out_rgba,
                       int out_is_device);
+/* mrp_render that returns once the render is queued (no counterpart in the
+ * reference, whose Render synchronises per launch, core/volume.cu:536): the
+ * result is copied to out_rgba on a second stream while the next started
+ * render computes, so a frame loop's copies back to the host overlap the
+ * device work.  Two results alternate between two device buffers; a third
+ * start waits on the device for the first one's copy.  out_rgba must stay
+ * valid and untouched until mrp_render_wait returns; host buffers must be
+ * pinned for the copy to overlap (pageable ones make the start synchronous).
+ * Any other call on the volume that uses the result buffers (mrp_render,
+ * the interactive frame, a render that needs larger buffers) first waits. */
+mrp_status mrp_render_start(mrp_volume* v, const mrp_view* view, mrp_render_type type, int sample_num, float* out_rgba,
+                            int out_is_device);
+/* keep = 0: blocks until every started render of v is in its output buffer,
+ * and reports a tensor-core wait that timed out in any of them
+ * (MRP_ERR_TIMEOUT).  keep = 1: until every one but the newest is -- a frame
+ * loop starts frame k, waits with keep = 1 and reads frame k - 1 while frame
+ * k computes. */
+mrp_status mrp_render_wait(mrp_volume* v, int keep);
 /* One launch of mrp_render (output discarded) that also counts its work:
  * MRPNN: [0] march steps, [1] density fetches (steps not skipped by the
  * occupancy bricks), [2] stencil points gathered, [3] hit pixels;

@@ -79,6 +79,8 @@ _SIGS = {
     "mrp_default_params": ([C.POINTER(Params)], None),
     "mrp_volume_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "mrp_volume_create_ex": ([C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "mrp_render_start": ([C.c_void_p, C.POINTER(View), C.c_int, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "mrp_render_wait": ([C.c_void_p, C.c_int], C.c_int),
     "mrp_volume_destroy": ([C.c_void_p], C.c_int),
     "mrp_volume_set_data": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "mrp_volume_fill": ([C.c_void_p, FILL_FN, C.c_void_p], C.c_int),
@@ -285,6 +287,7 @@ class VolumeRender:
             self.resolution = int(resolution)
         self._params = default_params()
         self._view_seed = 0
+        self._inflight = []
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -426,6 +429,22 @@ class VolumeRender:
         p, dev = _ptr(out)
         _check(lib().mrp_render(self._h, C.byref(view), int(rt), int(sample_num), p, dev))
         return out
+
+    def render_view_start(self, view, rt, sample_num, out):
+        """mrp_render_start: queues the render; `out` (pinned numpy or CUDA
+        tensor) holds the result after render_wait()."""
+        p, dev = _ptr(out)
+        self._inflight.append(out)   # kept alive until the copy into it is done
+        _check(lib().mrp_render_start(self._h, C.byref(view), int(rt), int(sample_num), p, dev))
+        return out
+
+    def render_wait(self, keep=0):
+        """mrp_render_wait: every started render done (keep=0), or every one
+        but the newest (keep=1)."""
+        try:
+            _check(lib().mrp_render_wait(self._h, int(keep)))
+        finally:
+            del self._inflight[:len(self._inflight) - keep if keep else None]
 
     # -- batch ray APIs (core/volume.cu:405-479, 710-834) ---------------------
     def GetRadiances(self, ori, dir, lightDir, lightColor=(1, 1, 1), alpha=1.0, multiScatter=1, g=0.0, sampleNum=1,

@@ -264,8 +264,13 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&v->ev0)) != cudaSuccess || (e = cudaEventCreate(&v->ev1)) != cudaSuccess ||
-        (e = cudaEventCreate(&v->ev_stage[0])) != cudaSuccess || (e = cudaEventCreate(&v->ev_stage[1])) != cudaSuccess)
+        (e = cudaEventCreate(&v->ev_stage[0])) != cudaSuccess || (e = cudaEventCreate(&v->ev_stage[1])) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&v->stream_copy, cudaStreamNonBlocking)) != cudaSuccess)
         return cleanup(fail(MRP_ERR_CUDA, "stream/event: %s", cudaGetErrorString(e)));
+    for (int s = 0; s < 2; ++s)
+        if ((e = cudaEventCreateWithFlags(&v->ev_done[s], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&v->ev_copied[s], cudaEventDisableTiming)) != cudaSuccess)
+            return cleanup(fail(MRP_ERR_CUDA, "event: %s", cudaGetErrorString(e)));
     size_t n = (size_t)res * res * res;
     v->occ_res = (res + (1 << v->occ_shift) - 1) >> v->occ_shift;
     size_t nocc = (size_t)v->occ_res * v->occ_res * v->occ_res;
@@ -292,6 +297,8 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
 mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
+    if (v->stream_copy) cudaStreamSynchronize(v->stream_copy);
+    cudaFree(v->accum_alt);
     cudaFree(v->density); cudaFree(v->density_h); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
     cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->mips_pad); cudaFree(v->trs_pad); cudaFree(v->mip_tr); cudaFree(v->pad_pair); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
     cudaFree(v->counter);
@@ -301,6 +308,11 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (v->ev0) cudaEventDestroy(v->ev0);
     if (v->ev1) cudaEventDestroy(v->ev1);
     for (auto& ev : v->ev_stage) if (ev) cudaEventDestroy(ev);
+    for (int s = 0; s < 2; ++s) {
+        if (v->ev_done[s]) cudaEventDestroy(v->ev_done[s]);
+        if (v->ev_copied[s]) cudaEventDestroy(v->ev_copied[s]);
+    }
+    if (v->stream_copy) cudaStreamDestroy(v->stream_copy);
     if (v->stream) cudaStreamDestroy(v->stream);
     delete v;
     return MRP_OK;
@@ -689,10 +701,38 @@ ViewDev make_view(const mrp_volume* v, const mrp_view* w, int frame, int mean_k)
 extern "C" {
 
 static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out,
-                              int out_is_device, unsigned long long* counters);
+                              int out_is_device, unsigned long long* counters, bool async = false);
 
 mrp_status mrp_render(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out, int out_is_device) {
     return render_impl(v, w, type, sample_num, out, out_is_device, nullptr);
+}
+
+mrp_status mrp_render_start(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out,
+                            int out_is_device) {
+    return render_impl(v, w, type, sample_num, out, out_is_device, nullptr, true);
+}
+
+mrp_status mrp_render_wait(mrp_volume* v, int keep) {
+    TRY(need_init());
+    if (!v) return fail(MRP_ERR_INVALID, "null volume");
+    if (keep != 0 && keep != 1) return fail(MRP_ERR_INVALID, "keep must be 0 or 1");
+    if (keep == 1) {
+        // every result but the newest: the second newest start used the slot
+        // the next start will take, and its copy event has not been re-recorded
+        if (v->async_inflight >= 2) CU(cudaEventSynchronize(v->ev_copied[v->async_slot]));
+        if (v->async_inflight > 1) v->async_inflight = 1;
+        return MRP_OK;
+    }
+    CU(cudaStreamSynchronize(v->stream));
+    CU(cudaStreamSynchronize(v->stream_copy));
+    v->async_inflight = 0;
+    if (v->async_tc) {   // the error flag gathers every tensor-core launch since the last wait
+        v->async_tc = false;
+        int herr = 0;
+        CU(cudaMemcpy(&herr, v->tc.d + 1, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) return fail(MRP_ERR_TIMEOUT, "tensor-core MLP: MMA completion wait timed out");
+    }
+    return MRP_OK;
 }
 
 mrp_status mrp_render_counters(mrp_volume* v, const mrp_view* w, mrp_render_type type, unsigned long long counters[4]) {
@@ -713,8 +753,10 @@ mrp_status mrp_render_counters(mrp_volume* v, const mrp_view* w, mrp_render_type
 }
 
 static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type type, int sample_num, float* out,
-                              int out_is_device, unsigned long long* counters) {
+                              int out_is_device, unsigned long long* counters, bool async) {
     TRY(need_init());
+    // a synchronous render (or counter run) first lets started ones finish
+    if (v && !async && v->async_inflight) TRY(mrp_render_wait(v, 0));
     if (!v || !w || !out) return fail(MRP_ERR_INVALID, "null argument");
     if (w->width <= 0 || w->height <= 0 || (long long)w->width * w->height > (1ll << 28))
         return fail(MRP_ERR_INVALID, "image size %dx%d", w->width, w->height);
@@ -725,6 +767,10 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     if (type == MRP_MRPNN && !v->has_pyramid) return fail(MRP_ERR_NOT_READY, "MRPNN needs the pyramid (mrp_volume_update)");
     if (type == MRP_PT && (w->spp < 1 || w->multi_scatter < 1)) return fail(MRP_ERR_INVALID, "PT needs spp, multi_scatter >= 1");
     size_t npix = (size_t)w->width * w->height;
+    // buffers that must grow are freed and reallocated: not under copies in flight
+    if (v->async_inflight && (v->accum_pix < npix || v->accum_alt_pix < npix || (type == MRP_PT && v->trace_pix < npix) ||
+                              (type == MRP_MRPNN && v->rec_cap < npix)))
+        TRY(mrp_render_wait(v, 0));
     TRY(ensure_accum(v, npix));
     if (type == MRP_PT && v->trace_pix < npix) {
         cudaFree(v->sum3); cudaFree(v->first_pos); cudaFree(v->counter);
@@ -743,8 +789,21 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
         TRY(update_baked_async(v, w->light_dir, w->alpha));
     }
     if (type == MRP_MRPNN) TRY(ensure_predictor_buffers(v, npix));
+    // result buffer: accum, or for a started render the slot's own buffer,
+    // reused only after the copy out of its previous result is done
+    const int slot = async ? v->async_slot : 0;
+    if (slot == 1 && v->accum_alt_pix < npix) {
+        cudaFree(v->accum_alt);
+        v->accum_alt = nullptr;
+        v->accum_alt_pix = 0;
+        CU(cudaMalloc(&v->accum_alt, npix * sizeof(float4)));
+        v->accum_alt_pix = npix;
+    }
+    float4* const acc = slot == 1 ? v->accum_alt : v->accum;
+    if (async) CU(cudaStreamWaitEvent(v->stream, v->ev_copied[slot], 0));
     VolumeDev d = v->dev();
-    if (type == MRP_MRPNN && v->params.precision != MRP_FP32) CU(cudaMemsetAsync(v->tc.d + 1, 0, sizeof(int), v->stream));
+    const bool tc_net = type == MRP_MRPNN && v->params.precision != MRP_FP32;
+    if (tc_net && !(async && v->async_tc)) CU(cudaMemsetAsync(v->tc.d + 1, 0, sizeof(int), v->stream));
     CU(cudaEventRecord(v->ev0, v->stream));
     for (int i = 0; i < sample_num; ++i) {
         ViewDev vd = make_view(v, w, w->frame_offset + i, i);
@@ -753,14 +812,14 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
         if (type == MRP_MRPNN) {
             HitRecords rec = v->records();
             if (last) CU(cudaEventRecord(v->ev0, v->stream));
-            CU(launch_hit(d, vd, rec, v->accum, v->stream));
+            CU(launch_hit(d, vd, rec, acc, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));
             CU(launch_gather_rec(d, vd, rec, v->feat, v->params.precision != MRP_FP32, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[1], v->stream));
             if (v->params.precision == MRP_FP32) {
-                CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, v->accum, v->stream));
+                CU(launch_mlp_rec_fp32(d, vd, rec, v->feat, g.d_weights, acc, v->stream));
             } else {
-                CU(tc_launch_mlp_rec(g.tc, v->params.precision == MRP_FP8, d, vd, rec, v->feat, v->accum, v->tc, g.sms,
+                CU(tc_launch_mlp_rec(g.tc, v->params.precision == MRP_FP8, d, vd, rec, v->feat, acc, v->tc, g.sms,
                                      v->stream));
             }
         } else {
@@ -770,12 +829,25 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
             if (last) CU(cudaEventRecord(v->ev0, v->stream));
             CU(launch_trace(d, vd, v->sum3, nullptr, v->first_pos, v->counter, g.sms, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));
-            CU(launch_trace_resolve(v->sum3, v->first_pos, (int)npix, w->spp, i, v->accum, v->stream));
+            CU(launch_trace_resolve(v->sum3, v->first_pos, (int)npix, w->spp, i, acc, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[1], v->stream));
         }
     }
     CU(cudaEventRecord(v->ev1, v->stream));
-    CU(cudaMemcpyAsync(out, v->accum, npix * sizeof(float4), out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+    if (async) {
+        // the copy out runs on stream_copy beside the next render's kernels
+        CU(cudaEventRecord(v->ev_done[slot], v->stream));
+        CU(cudaStreamWaitEvent(v->stream_copy, v->ev_done[slot], 0));
+        CU(cudaMemcpyAsync(out, acc, npix * sizeof(float4), out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           v->stream_copy));
+        CU(cudaEventRecord(v->ev_copied[slot], v->stream_copy));
+        v->async_slot ^= 1;
+        v->async_inflight++;
+        v->async_tc = v->async_tc || tc_net;
+        v->stages_valid = false;
+        return MRP_OK;
+    }
+    CU(cudaMemcpyAsync(out, acc, npix * sizeof(float4), out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                        v->stream));
     CU(cudaStreamSynchronize(v->stream));
     if (sample_num == 1) CU(cudaEventElapsedTime(&v->last_ms, v->ev0, v->ev1));

@@ -128,6 +128,16 @@ struct mrp_volume {
     // render buffers
     float4* accum = nullptr;
     size_t accum_pix = 0;
+    // mrp_render_start: results alternate between accum and accum_alt, and
+    // are copied out on stream_copy while the next render computes
+    cudaStream_t stream_copy = nullptr;
+    float4* accum_alt = nullptr;
+    size_t accum_alt_pix = 0;
+    cudaEvent_t ev_done[2] = {nullptr, nullptr};     // compute into slot s finished
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr};   // copy out of slot s finished
+    int async_slot = 0;
+    int async_inflight = 0;
+    bool async_tc = false;   // a tensor-core network ran since the last wait
     double* sum3 = nullptr;
     int* first_pos = nullptr;
     unsigned long long* counter = nullptr;

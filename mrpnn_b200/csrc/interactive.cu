@@ -195,6 +195,7 @@ mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_rende
         return fail(MRP_ERR_INVALID, "image size %dx%d", view->width, view->height);
     if (!v->has_data) return fail(MRP_ERR_NOT_READY, "no volume data");
     if (type == MRP_MRPNN && !v->has_pyramid) return fail(MRP_ERR_NOT_READY, "MRPNN needs the pyramid");
+    if (v->async_inflight) TRY(mrp_render_wait(v, 0));   // started renders may still read accum
     const int W = view->width, H = view->height, npix = W * H;
     const int fnum = checkerboard ? frame_num / 2 : frame_num;
     ViewDev vd = make_view(v, view, view->frame_offset, 0);
