@@ -529,7 +529,7 @@ def run_mine(args, rank, world, local):
     import mrpnn_b200 as M
     M.init(local)
     precs = {"fp32": M.FP32, "bf16": M.BF16, "fp8": M.FP8}
-    vol = M.VolumeRender(RES)
+    vol = M.VolumeRender(RES, storage=args.storage)
     vol.generate_fbm(SCENE["seed"], SCENE["freq"], SCENE["octaves"], SCENE["gain"])
     vol.Update()
     vol.SetScatterRate(SCENE["albedo"])
@@ -649,7 +649,7 @@ def run_mine(args, rank, world, local):
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp32": "f32", "bf16": "bf16", "fp8": "fp8-e4m3"}[args.precision], "data": "synthetic",
             "config": {"workload": f"MRPNN predictor frame {W}x{H}, {RES}^3 fBm cloud (seed 1, freq 6), 9-level pyramid",
-                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "precision": args.precision, "grid_storage": args.storage, "parallelism": f"replicas x{world}",
                        "l2": "flushed (256 MiB write) between timed steps", "hit_pixels": active,
                        "precision_forms": forms},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 96, "d2h_bytes_per_step": W * H * 16,
@@ -680,6 +680,8 @@ def main():
     ap.add_argument("--ref-pixels", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=1024, help="frame edge (the headline workload is 1024)")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
+                    help="density grid storage of the headline volume (fp32: the reference's float grid)")
     ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving workload (0: skip)")
     ap.add_argument("--rmse-spp", type=int, default=4096, help="spp of the PT reference image (0: skip)")
