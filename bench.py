@@ -313,7 +313,7 @@ def run_serving(args, local):
                            SCENE["g"], alpha, seed=i)
         reqs.append((vi, view))
     pool = [torch.empty(1920 * 1080 * 4, dtype=torch.float32, device=f"cuda:{local}") for _ in range(64)]
-    srv = M.Server(memory_budget=SERVE["budget"], max_slots=SERVE["slots"], precision=M.BF16,
+    srv = M.Server(memory_budget=SERVE["budget"], max_slots=args.serve_slots, precision=M.BF16,
                    slot_pixels=1920 * 1080)
     try:
         # warm-up: one request of each image size (LUT, slot buffers)
@@ -359,7 +359,8 @@ def run_serving(args, local):
     pm = np.median(np.asarray(parts), axis=0)
     return {"workload": "16 resident fp16 fBm volumes (128/256/512^3, seeds 10-25, alpha 16-256), Poisson "
                         f"{SERVE['rate']:.0f} req/s, images 256^2/512^2/1024^2/1920x1080, orbit cameras, random "
-                        "lights, BF16 network, 120 GB budget, 16 slots sized for 1920x1080 at open, results in device buffers",
+                        f"lights, BF16 network, 120 GB budget, {args.serve_slots} slots sized for 1920x1080 at open, "
+                        "results in device buffers",
             "requests": n_req, "offered_req_s": SERVE["rate"], "achieved_req_s": n_req / span_s,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
@@ -684,6 +685,7 @@ def main():
                     help="density grid storage of the headline volume (fp32: the reference's float grid)")
     ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving workload (0: skip)")
+    ap.add_argument("--serve-slots", type=int, default=SERVE["slots"], help="request slots of the server")
     ap.add_argument("--rmse-spp", type=int, default=4096, help="spp of the PT reference image (0: skip)")
     ap.add_argument("--large", type=int, default=1, help="run the 1024^3 / 64-view workload (0: skip)")
     ap.add_argument("--large-judge", type=int, default=1, help="judge 4 large views against the tracer (0: skip)")
