@@ -52,6 +52,20 @@ def test_fails_loudly_without_gpu():
     assert e.value.status == api.ERR_NO_DEVICE
     with pytest.raises(mrpnn_b200.MrpError):
         mrpnn_b200.predict_features(np.zeros((1, 576), np.float32), np.zeros(1, np.float32), 0.5, (1, 1, 1))
+    import ctypes as C
+    h = C.c_void_p()
+    assert api.lib().mrp_volume_create_ex(64, 1, C.byref(h)) == api.ERR_NOT_READY   # fp16 grid
+    assert api.lib().mrp_render_wait(None, 0) == api.ERR_NOT_READY
+    with pytest.raises(mrpnn_b200.MrpError):
+        mrpnn_b200.VolumeRender(64, storage="fp16")
+
+
+def test_grid_storage_names():
+    import mrpnn_b200
+    from mrpnn_b200 import api
+    assert api.STORAGE == {"fp32": 0, "fp16": 1}
+    with pytest.raises(ValueError):
+        mrpnn_b200.VolumeRender(64, storage="bf16")   # rejected before any device call
 
 
 def test_default_params():
