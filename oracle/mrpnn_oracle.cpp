@@ -765,7 +765,8 @@ void orc_tr_mip_level(const float* mips, int level, float alpha, const float lig
 // Scrambled radical inverse (core/volume.cu:1186-1319 restates PBRT's
 // ScrambledRadicalInverse).  The digit permutations are drawn here from a
 // seeded Fisher-Yates shuffle rather than copied; bn is a per-texel hash
-// instead of a curand draw (SURVEY hazard 4).
+// instead of a curand draw (the reference's draw depends on curand's XORWOW
+// state, which no other generator reproduces).
 namespace {
 const uint32_t kPrimes[5] = {2, 3, 5, 7, 11};
 const uint32_t kPrimeSums[5] = {0, 2, 5, 10, 17};
