@@ -60,7 +60,9 @@ typedef struct orc_view {
 
 /* ---- RNG: Philox-4x32-10 (Salmon et al., SC'11) ------------------------- */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
-/* n-th uniform of stream (kind, id, sub, frame, seed); see DESIGN.md RNG. */
+/* n-th uniform of stream (kind, id, sub, frame, seed): word n % 4 of
+ * Philox(counter = (n / 4, sub, frame, kind), key = (id, seed ^ kind * 0x9E3779B9)),
+ * mapped to (0, 1) as the device streams do. */
 float orc_stream_uniform(uint32_t kind, uint32_t id, uint32_t sub, uint32_t frame,
                          uint32_t seed, uint32_t n);
 
