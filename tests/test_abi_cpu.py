@@ -107,3 +107,30 @@ def test_model_file_layout():
             total += c if names[-1] != "STENCIL_DIRS" else 0
     assert n == 147 and "STENCIL_DIRS" in names
     assert total == 49673
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/mrpnn.h is a C99 header (the FFI boundary): a C program that
+    calls entry points links against the library."""
+    import shutil
+    import subprocess
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else shutil.which("gcc")
+    if not cc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi.c"
+    src.write_text('#include "mrpnn.h"\n'
+                   "int main(void) {\n"
+                   "    mrp_volume* v = 0;\n"
+                   "    mrp_params p;\n"
+                   "    mrp_default_params(&p);\n"
+                   "    if (mrp_volume_create_ex(8, MRP_STORAGE_FP16, &v) == MRP_OK) return 1;  /* no device here */\n"
+                   "    return mrp_render_wait(v, 0) == MRP_OK;\n"
+                   "}\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = os.path.join(root, "mrpnn_b200")
+    exe = tmp_path / "abi"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I" + os.path.join(root, "include"),
+                    "-I/usr/local/cuda/include", str(src), "-o", str(exe), "-L" + lib, "-lmrpnn_b200",
+                    "-Wl,-rpath," + lib], check=True)
+    if not _has_gpu():
+        assert subprocess.run([str(exe)]).returncode == 0
