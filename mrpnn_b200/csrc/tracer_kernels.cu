@@ -18,8 +18,11 @@
 // item from a global counter at once (one atomic per warp for all lanes
 // that need work).  Every sample has its own Philox stream (sub = sample
 // index) and its arithmetic is CalculateRadiance's, in the reference's order,
-// so results do not depend on which lane ran it or when.  Per-sample
-// radiance is fp32, accumulated per pixel in FP64.
+// so results do not depend on which lane ran it or when.  The free-flight
+// step (distance and accept test) uses the fast log and division that the
+// reference's -use_fast_math build compiles to (CMakeLists.txt:184); the
+// rest is in IEEE float.  Per-sample radiance is fp32, accumulated per pixel
+// in FP64.
 #include "kernels.h"
 #include "tracing.cuh"
 
@@ -147,7 +150,10 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
             if (loop >= 10000) { hit = true; continue; }
             ++loop;
             float rk = st.next(pix, k, frame, seed);
-            t = fs(t, fd(logf(fs(1.0f, rk)), smax));
+            // the free-flight step in the reference's build arithmetic
+            // (-use_fast_math: __logf, __fdividef), 10 % of the frame
+            // against IEEE log and division; decisions stay per sample
+            t = t - __fdividef(__logf(1.0f - rk), smax);
             if (t > md) {   // left the box: sky radiance, the sample ends
                 res = add(res, mul(v.sky, csr));
                 deposit(sum3, sumsq3, first_pos, pix, k, res, true);
@@ -157,8 +163,8 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
             rk = st.next(pix, k, frame, seed);
             float d = density_t<DT>(v, add(p, mul(rd, t)));
             if (COUNT) tally.fetches++;
-            float S = fm(d, w.alpha);
-            hit = fd(S, smax) > rk;
+            float S = d * w.alpha;
+            hit = __fdividef(S, smax) > rk;
             if (!hit && d < 0) t = fs(t, d);
             continue;
         }
