@@ -108,6 +108,12 @@ typedef enum mrp_resource {
 mrp_status mrp_init(int device, const char* model_path);
 const char* mrp_last_error(void);
 const char* mrp_version(void);
+/* Number of CUDA allocation and free calls (device, stream-ordered and
+ * pinned host) the library has made since it was loaded.  No counterpart in
+ * the reference; a diagnostic that lets a caller check that an entry point
+ * which promises not to allocate (mrp_predict_features_noalloc) made no such
+ * call.  Needs no device. */
+unsigned long long mrp_debug_alloc_calls(void);
 /* Replaces the network weights from a model file (format: mrpnn_b200/data/
  * make_model.py).  The reference bakes them into __constant__ arrays
  * (core/NNWeight.cuh, core/radiancePredict.cu:299). */

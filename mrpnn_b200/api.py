@@ -75,6 +75,7 @@ _SIGS = {
     "mrp_init": ([C.c_int, C.c_char_p], C.c_int),
     "mrp_last_error": ([], C.c_char_p),
     "mrp_version": ([], C.c_char_p),
+    "mrp_debug_alloc_calls": ([], C.c_ulonglong),
     "mrp_load_model": ([C.c_char_p], C.c_int),
     "mrp_default_params": ([C.POINTER(Params)], None),
     "mrp_volume_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
@@ -183,6 +184,22 @@ def _host_f32(a, shape=None):
     return a
 
 
+FEATURES_PER_SET = 576   # X_Val, X_Val_Sub, X_Val_Hg: 3 x 192 stencil points
+
+
+def _feature_sets(feat, gamma):
+    """Host feature sets as contiguous float32 ([n, 576], [n], n), or
+    ValueError when the shapes disagree: the C ABI reads n * 576 and n floats
+    from these pointers, so a malformed array must never reach it."""
+    feat = np.ascontiguousarray(feat, dtype=np.float32)
+    gamma = np.ascontiguousarray(gamma, dtype=np.float32)
+    if feat.ndim != 2 or feat.shape[1] != FEATURES_PER_SET:
+        raise ValueError(f"feat must be [n, {FEATURES_PER_SET}]; got {feat.shape}")
+    if gamma.ndim != 1 or gamma.shape[0] != feat.shape[0]:
+        raise ValueError(f"gamma must be [n] with n = {feat.shape[0]}; got {gamma.shape}")
+    return feat, gamma, feat.shape[0]
+
+
 def default_params():
     p = Params()
     lib().mrp_default_params(C.byref(p))
@@ -192,19 +209,33 @@ def default_params():
 def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
     """RadiancePredictInternal on n feature sets (feat [n, 576] = X_Val, X_Val_Sub,
     X_Val_Hg; gamma [n]) -> [n, 3].  Accepts numpy arrays (host) or CUDA tensors."""
-    _ensure_init()
     if isinstance(feat, np.ndarray):
-        feat = _host_f32(feat)
-        gamma = _host_f32(gamma)
-        n = feat.shape[0]
-        out = np.empty((n, 3), np.float32) if out is None else out
+        feat, gamma, n = _feature_sets(feat, gamma)
+        if out is None:
+            out = np.empty((n, 3), np.float32)
+        elif not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.shape == (n, 3)
+                  and out.flags.c_contiguous):
+            raise ValueError(f"out must be a C-contiguous float32 array of shape ({n}, 3)")
+        _ensure_init()
         _check(lib().mrp_predict_features(feat.ctypes.data, gamma.ctypes.data, float(g), _f3(scatter_rate), n,
                                           out.ctypes.data, int(precision), 0))
         return out
+    import torch
+    if not (isinstance(feat, torch.Tensor) and isinstance(gamma, torch.Tensor) and feat.is_cuda and gamma.is_cuda):
+        raise TypeError("feat and gamma must both be numpy arrays or both CUDA tensors")
+    if feat.dtype != torch.float32 or gamma.dtype != torch.float32 or not feat.is_contiguous() \
+            or not gamma.is_contiguous():
+        raise ValueError("feat and gamma must be contiguous float32 tensors")
+    if feat.dim() != 2 or feat.shape[1] != FEATURES_PER_SET or gamma.numel() != feat.shape[0]:
+        raise ValueError(f"feat must be [n, {FEATURES_PER_SET}] and gamma [n]; got {tuple(feat.shape)} "
+                         f"and {tuple(gamma.shape)}")
     n = feat.shape[0]
     if out is None:
-        import torch
         out = torch.empty((n, 3), dtype=torch.float32, device=feat.device)
+    elif not (isinstance(out, torch.Tensor) and out.is_cuda and out.dtype == torch.float32
+              and tuple(out.shape) == (n, 3) and out.is_contiguous()):
+        raise ValueError(f"out must be a contiguous float32 CUDA tensor of shape ({n}, 3)")
+    _ensure_init()
     _check(lib().mrp_predict_features(feat.data_ptr(), gamma.data_ptr(), float(g), _f3(scatter_rate), n,
                                       out.data_ptr(), int(precision), 1))
     return out
@@ -228,6 +259,12 @@ def write_volume_bin(path, data):
     _check(lib().mrp_volume_file_write_bin(path.encode(), data.ctypes.data, R))
 
 
+def debug_alloc_calls():
+    """mrp_debug_alloc_calls: CUDA allocation and free calls the library has
+    made so far (device, stream-ordered and pinned host)."""
+    return int(lib().mrp_debug_alloc_calls())
+
+
 NOALLOC_MAX_POINTS = 2048   # MRP_NOALLOC_MAX_POINTS in include/mrpnn.h
 
 
@@ -237,10 +274,8 @@ def predict_features_noalloc(feat, gamma, g, scatter_rate, precision=FP32):
     copies, the output and the tensor-core network's counters sit in the
     library's fixed device array.  At most NOALLOC_MAX_POINTS feature sets
     per call."""
+    feat, gamma, n = _feature_sets(feat, gamma)
     _ensure_init()
-    feat = _host_f32(feat)
-    gamma = _host_f32(gamma)
-    n = feat.shape[0]
     out = np.empty((n, 3), np.float32)
     _check(lib().mrp_predict_features_noalloc(feat.ctypes.data, gamma.ctypes.data, float(g), _f3(scatter_rate), n,
                                               out.ctypes.data, int(precision)))

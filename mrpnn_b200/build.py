@@ -70,7 +70,7 @@ def build(verbose=False, ptxas_info=False):
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed on {src}")
     if _newer(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", host_compiler(), "-o", LIB] + objs + ["-ldl"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", host_compiler(), "-o", LIB] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

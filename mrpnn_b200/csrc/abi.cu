@@ -171,20 +171,25 @@ mrp_status pack_weights(const std::map<std::string, std::vector<float>>& m, std:
 
 mrp_status ensure_scratch(size_t bytes) {
     if (g.scratch_bytes >= bytes) return MRP_OK;
-    if (g.scratch) cudaFree(g.scratch);
+    if (g.scratch) mrp::dev_free(g.scratch);
     g.scratch = nullptr;
     g.scratch_bytes = 0;
-    CU(cudaMalloc(&g.scratch, bytes));
+    CU(mrp::dev_malloc(&g.scratch, bytes));
     g.scratch_bytes = bytes;
     return MRP_OK;
 }
 
 }  // namespace
 
+namespace mrp {
+std::atomic<unsigned long long> g_alloc_calls{0};
+}
+
 extern "C" {
 
 const char* mrp_last_error(void) { return t_err.c_str(); }
 const char* mrp_version(void) { return "mrpnn_b200 0.1 (sm_100a)"; }
+unsigned long long mrp_debug_alloc_calls(void) { return mrp::g_alloc_calls.load(); }
 
 void mrp_default_params(mrp_params* p) {
     if (!p) return;
@@ -210,7 +215,7 @@ mrp_status mrp_load_model(const char* path) {
     StencilTables st;
     stencil_tables(st, it->second);
     CU(set_stencil_tables(st));
-    if (!g.d_weights) CU(cudaMalloc(&g.d_weights, sizeof(float) * kWeightCount));
+    if (!g.d_weights) CU(mrp::dev_malloc(&g.d_weights, sizeof(float) * kWeightCount));
     CU(cudaMemcpy(g.d_weights, w.data(), sizeof(float) * kWeightCount, cudaMemcpyHostToDevice));
     CU(tc_prepare_weights(w.data(), g.tc));
     g.tc.d_fp32 = g.d_weights;
@@ -274,18 +279,18 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
     size_t n = (size_t)res * res * res;
     v->occ_res = (res + (1 << v->occ_shift) - 1) >> v->occ_shift;
     size_t nocc = (size_t)v->occ_res * v->occ_res * v->occ_res;
-    if ((storage == MRP_STORAGE_FP16 ? (e = cudaMalloc(&v->density_h, n * sizeof(__half)))
-                                     : (e = cudaMalloc(&v->density, n * sizeof(float)))) != cudaSuccess ||
-        (e = cudaMalloc(&v->mips, kMipFloats * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->lut, kLutAlloc * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->occ, nocc)) != cudaSuccess || (e = cudaMalloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
-        (e = cudaMalloc(&v->d_maxbits, sizeof(int))) != cudaSuccess ||
-        (e = cudaMalloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess ||
-        (e = cudaMalloc(&v->mips_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->trs_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&v->mip_tr, mip_tr_offset(5) * sizeof(float2))) != cudaSuccess ||
-        (e = cudaMalloc(&v->pad_pair, kPadLevelFloats * sizeof(float2))) != cudaSuccess)
+    if ((storage == MRP_STORAGE_FP16 ? (e = mrp::dev_malloc(&v->density_h, n * sizeof(__half)))
+                                     : (e = mrp::dev_malloc(&v->density, n * sizeof(float)))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->mips, kMipFloats * sizeof(float))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->lut, kLutAlloc * sizeof(float))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->occ, nocc)) != cudaSuccess || (e = mrp::dev_malloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->d_maxbits, sizeof(int))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->mips_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->trs_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->mip_tr, mip_tr_offset(5) * sizeof(float2))) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->pad_pair, kPadLevelFloats * sizeof(float2))) != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? MRP_ERR_OOM : MRP_ERR_CUDA, "volume allocation: %s",
                             cudaGetErrorString(e)));
     if (v->density_h) cudaMemsetAsync(v->density_h, 0, n * sizeof(__half), v->stream);
@@ -298,11 +303,11 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
     if (v->stream_copy) cudaStreamSynchronize(v->stream_copy);
-    cudaFree(v->accum_alt);
-    cudaFree(v->density); cudaFree(v->density_h); cudaFree(v->mips); cudaFree(v->trs); cudaFree(v->lut); cudaFree(v->baked);
-    cudaFree(v->occ); cudaFree(v->mip_occ); cudaFree(v->d_maxbits); cudaFree(v->d_bounds); cudaFree(v->mips_pad); cudaFree(v->trs_pad); cudaFree(v->mip_tr); cudaFree(v->pad_pair); cudaFree(v->accum); cudaFree(v->sum3); cudaFree(v->first_pos);
-    cudaFree(v->counter);
-    cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
+    mrp::dev_free(v->accum_alt);
+    mrp::dev_free(v->density); mrp::dev_free(v->density_h); mrp::dev_free(v->mips); mrp::dev_free(v->trs); mrp::dev_free(v->lut); mrp::dev_free(v->baked);
+    mrp::dev_free(v->occ); mrp::dev_free(v->mip_occ); mrp::dev_free(v->d_maxbits); mrp::dev_free(v->d_bounds); mrp::dev_free(v->mips_pad); mrp::dev_free(v->trs_pad); mrp::dev_free(v->mip_tr); mrp::dev_free(v->pad_pair); mrp::dev_free(v->accum); mrp::dev_free(v->sum3); mrp::dev_free(v->first_pos);
+    mrp::dev_free(v->counter);
+    mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     tc_free_scratch(v->tc);
     free_multiview(v);
     if (v->ev0) cudaEventDestroy(v->ev0);
@@ -338,7 +343,7 @@ mrp_status mrp_volume_set_data(mrp_volume* v, const float* data, int res, int is
         // at most 16 Mi floats, rounded on the device
         const size_t chunk = std::min<size_t>(n, (size_t)16 << 20);
         float* stage = nullptr;
-        CU(cudaMalloc(&stage, chunk * sizeof(float)));
+        CU(mrp::dev_malloc(&stage, chunk * sizeof(float)));
         cudaError_t e = cudaSuccess;
         for (size_t i = 0; i < n && e == cudaSuccess; i += chunk) {
             const size_t m = std::min(chunk, n - i);
@@ -346,7 +351,7 @@ mrp_status mrp_volume_set_data(mrp_volume* v, const float* data, int res, int is
             if (e == cudaSuccess) e = launch_narrow(stage, m, v->density_h + i, g.sms, v->stream);
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
-        cudaFree(stage);
+        mrp::dev_free(stage);
         CU(e);
     }
     CU(cudaStreamSynchronize(v->stream));
@@ -439,7 +444,7 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         };
         for (; res > 256; res >>= 1) {
             float*& t = tmp[which];
-            if (!t) CU(cudaMalloc(&t, (size_t)res * res * res * sizeof(float)));
+            if (!t) CU(mrp::dev_malloc(&t, (size_t)res * res * res * sizeof(float)));
             CU(resample(t, res));
             src = t;
             src_res = res;
@@ -458,8 +463,8 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         CU(launch_pad_levels(v->mips + mip_offset(5), v->mips + mip_offset(6), v->mips + mip_offset(7), false,
                              v->mips_pad, v->stream));
         CU(cudaStreamSynchronize(v->stream));
-        cudaFree(tmp[0]);
-        cudaFree(tmp[1]);
+        mrp::dev_free(tmp[0]);
+        mrp::dev_free(tmp[1]);
         v->has_pyramid = true;
     }
     CU(cudaStreamSynchronize(v->stream));
@@ -533,7 +538,7 @@ mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* 
         } else {
             const size_t chunk = std::min<size_t>(n, (size_t)16 << 20);
             float* stage = nullptr;
-            CU(cudaMalloc(&stage, chunk * sizeof(float)));
+            CU(mrp::dev_malloc(&stage, chunk * sizeof(float)));
             cudaError_t e = cudaSuccess;
             for (size_t i = 0; i < n && e == cudaSuccess; i += chunk) {
                 const size_t m = std::min(chunk, n - i);
@@ -542,7 +547,7 @@ mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* 
                     e = cudaMemcpyAsync(dst + i, stage, m * sizeof(float), cudaMemcpyDeviceToHost, v->stream);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
             }
-            cudaFree(stage);
+            mrp::dev_free(stage);
             CU(e);
         }
         CU(cudaStreamSynchronize(v->stream));
@@ -605,10 +610,10 @@ mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha) {
         v->bk_light[0] == L[0] && v->bk_light[1] == L[1] && v->bk_light[2] == L[2])
         return MRP_OK;
     if (v->baked_alloc_res != B) {
-        cudaFree(v->baked);
+        mrp::dev_free(v->baked);
         v->baked = nullptr;
         v->baked_alloc_res = 0;
-        CU(cudaMalloc(&v->baked, (size_t)B * B * B * sizeof(float)));
+        CU(mrp::dev_malloc(&v->baked, (size_t)B * B * B * sizeof(float)));
         v->baked_alloc_res = B;
     }
     v->bk_res = B;
@@ -652,22 +657,22 @@ mrp_status mrp_update_baked_tr(mrp_volume* v, const float light_dir[3], float al
 namespace mrpi {
 mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
     if (v->rec_cap >= npix) return MRP_OK;
-    cudaFree(v->rec_count); cudaFree(v->rec_pix); cudaFree(v->rec_f); cudaFree(v->feat);
+    mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     v->rec_count = nullptr; v->rec_pix = nullptr; v->rec_f = nullptr; v->feat = nullptr; v->rec_cap = 0;
-    CU(cudaMalloc(&v->rec_count, sizeof(int)));
-    CU(cudaMalloc(&v->rec_pix, npix * sizeof(int)));
-    CU(cudaMalloc(&v->rec_f, npix * 16 * sizeof(float)));
-    CU(cudaMalloc(&v->feat, tiled_feature_floats(npix) * sizeof(float)));
+    CU(mrp::dev_malloc(&v->rec_count, sizeof(int)));
+    CU(mrp::dev_malloc(&v->rec_pix, npix * sizeof(int)));
+    CU(mrp::dev_malloc(&v->rec_f, npix * 16 * sizeof(float)));
+    CU(mrp::dev_malloc(&v->feat, tiled_feature_floats(npix) * sizeof(float)));
     CU(tc_ensure_scratch(v->tc));
     v->rec_cap = npix;
     return MRP_OK;
 }
 mrp_status ensure_accum(mrp_volume* v, size_t npix) {
     if (v->accum_pix >= npix) return MRP_OK;
-    cudaFree(v->accum);
+    mrp::dev_free(v->accum);
     v->accum = nullptr;
     v->accum_pix = 0;
-    CU(cudaMalloc(&v->accum, npix * sizeof(float4)));
+    CU(mrp::dev_malloc(&v->accum, npix * sizeof(float4)));
     v->accum_pix = npix;
     return MRP_OK;
 }
@@ -739,16 +744,16 @@ mrp_status mrp_render_counters(mrp_volume* v, const mrp_view* w, mrp_render_type
     TRY(need_init());
     if (!counters) return fail(MRP_ERR_INVALID, "null argument");
     unsigned long long* d = nullptr;
-    CU(cudaMalloc(&d, 4 * sizeof(unsigned long long)));
+    CU(mrp::dev_malloc(&d, 4 * sizeof(unsigned long long)));
     cudaMemset(d, 0, 4 * sizeof(unsigned long long));
     float* out = nullptr;
     size_t npix = (size_t)std::max(w ? w->width : 0, 0) * std::max(w ? w->height : 0, 0);
-    if (cudaMalloc(&out, std::max<size_t>(npix, 1) * 16) != cudaSuccess) { cudaFree(d); return fail(MRP_ERR_OOM, "counters"); }
+    if (mrp::dev_malloc(&out, std::max<size_t>(npix, 1) * 16) != cudaSuccess) { mrp::dev_free(d); return fail(MRP_ERR_OOM, "counters"); }
     mrp_status st = render_impl(v, w, type, 1, out, 1, d);
     if (st == MRP_OK && cudaMemcpy(counters, d, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
         st = fail(MRP_ERR_CUDA, "counters readback");
-    cudaFree(d);
-    cudaFree(out);
+    mrp::dev_free(d);
+    mrp::dev_free(out);
     return st;
 }
 
@@ -773,11 +778,11 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
         TRY(mrp_render_wait(v, 0));
     TRY(ensure_accum(v, npix));
     if (type == MRP_PT && v->trace_pix < npix) {
-        cudaFree(v->sum3); cudaFree(v->first_pos); cudaFree(v->counter);
+        mrp::dev_free(v->sum3); mrp::dev_free(v->first_pos); mrp::dev_free(v->counter);
         v->sum3 = nullptr; v->first_pos = nullptr; v->counter = nullptr; v->trace_pix = 0;
-        CU(cudaMalloc(&v->sum3, npix * 3 * sizeof(double)));
-        CU(cudaMalloc(&v->first_pos, npix * sizeof(int)));
-        CU(cudaMalloc(&v->counter, sizeof(unsigned long long)));
+        CU(mrp::dev_malloc(&v->sum3, npix * 3 * sizeof(double)));
+        CU(mrp::dev_malloc(&v->first_pos, npix * sizeof(int)));
+        CU(mrp::dev_malloc(&v->counter, sizeof(unsigned long long)));
         v->trace_pix = npix;
     }
     // caches first (the reference updates them inside its launch loop,
@@ -793,10 +798,10 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     // reused only after the copy out of its previous result is done
     const int slot = async ? v->async_slot : 0;
     if (slot == 1 && v->accum_alt_pix < npix) {
-        cudaFree(v->accum_alt);
+        mrp::dev_free(v->accum_alt);
         v->accum_alt = nullptr;
         v->accum_alt_pix = 0;
-        CU(cudaMalloc(&v->accum_alt, npix * sizeof(float4)));
+        CU(mrp::dev_malloc(&v->accum_alt, npix * sizeof(float4)));
         v->accum_alt_pix = npix;
     }
     float4* const acc = slot == 1 ? v->accum_alt : v->accum;
@@ -884,8 +889,8 @@ mrp_status mrp_render_predict_debug(mrp_volume* v, const mrp_view* w, float* rgb
     float4* acc = nullptr;
     float *da = aux, *df = feat;
     std::vector<void*> allocs;
-    auto alloc = [&](size_t b) { void* p = nullptr; if (cudaMalloc(&p, b) == cudaSuccess) allocs.push_back(p); return p; };
-    auto release = [&]() { for (void* p : allocs) cudaFree(p); };
+    auto alloc = [&](size_t b) { void* p = nullptr; if (mrp::dev_malloc(&p, b) == cudaSuccess) allocs.push_back(p); return p; };
+    auto release = [&]() { for (void* p : allocs) mrp::dev_free(p); };
     acc = (float4*)alloc(npix * sizeof(float4));
     if (!is_device) { da = (float*)alloc(npix * 20 * 4); df = (float*)alloc(npix * 576 * 4); }
     if (!acc || !da || !df) { release(); return fail(MRP_ERR_OOM, "debug render buffers"); }
@@ -1084,8 +1089,8 @@ mrp_status mrp_gather_features(mrp_volume* v, const float* pos, const float* bas
     float* dl = nullptr;
     float *dp = (float*)pos, *db = (float*)bases, *dfeat = feat, *dgam = gamma;
     std::vector<void*> allocs;
-    auto alloc = [&](size_t bytes) -> float* { void* p = nullptr; if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr; allocs.push_back(p); return (float*)p; };
-    auto release = [&]() { for (void* p : allocs) cudaFree(p); };
+    auto alloc = [&](size_t bytes) -> float* { void* p = nullptr; if (mrp::dev_malloc(&p, bytes) != cudaSuccess) return nullptr; allocs.push_back(p); return (float*)p; };
+    auto release = [&]() { for (void* p : allocs) mrp::dev_free(p); };
     dl = alloc(3 * sizeof(float));
     if (!dl) { release(); return fail(MRP_ERR_OOM, "gather scratch"); }
     cudaMemcpyAsync(dl, L, 3 * sizeof(float), cudaMemcpyHostToDevice, v->stream);
@@ -1117,7 +1122,7 @@ mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, floa
     float* dhit = hit4;
     float* tmp = nullptr;
     if (!is_device) {
-        CU(cudaMalloc(&tmp, (size_t)n * 10 * sizeof(float)));
+        CU(mrp::dev_malloc(&tmp, (size_t)n * 10 * sizeof(float)));
         float* o = tmp; float* d = tmp + 3 * (size_t)n; dhit = tmp + 6 * (size_t)n;
         cudaMemcpyAsync(o, ori, (size_t)n * 12, cudaMemcpyHostToDevice, v->stream);
         cudaMemcpyAsync(d, dir, (size_t)n * 12, cudaMemcpyHostToDevice, v->stream);
@@ -1126,7 +1131,7 @@ mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, floa
     cudaError_t e = launch_first_hit(v->dev(), dori, ddir, alpha, pass_rate, n, dhit, v->stream);
     if (e == cudaSuccess && !is_device) cudaMemcpyAsync(hit4, dhit, (size_t)n * 16, cudaMemcpyDeviceToHost, v->stream);
     cudaError_t e2 = cudaStreamSynchronize(v->stream);
-    if (tmp) cudaFree(tmp);
+    if (tmp) mrp::dev_free(tmp);
     if (e != cudaSuccess || e2 != cudaSuccess) return fail(MRP_ERR_CUDA, "first_hit: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
     return MRP_OK;
 }

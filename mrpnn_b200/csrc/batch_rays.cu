@@ -27,20 +27,20 @@ __global__ void k_rgba_to_rgb(const float4* __restrict__ in, int n, float* __res
 struct Staging {
     std::vector<void*> bufs;
     ~Staging() {
-        for (void* p : bufs) cudaFree(p);
+        for (void* p : bufs) mrp::dev_free(p);
     }
     // returns a device pointer to `bytes` of src (host or device)
     cudaError_t in(const void* src, size_t bytes, int is_device, cudaStream_t s, const float** out) {
         if (is_device) { *out = (const float*)src; return cudaSuccess; }
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, bytes);
+        cudaError_t e = mrp::dev_malloc(&p, bytes);
         if (e != cudaSuccess) return e;
         bufs.push_back(p);
         *out = (const float*)p;
         return cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, s);
     }
     cudaError_t scratch(size_t bytes, void** out) {
-        cudaError_t e = cudaMalloc(out, bytes);
+        cudaError_t e = mrp::dev_malloc(out, bytes);
         if (e == cudaSuccess) bufs.push_back(*out);
         return e;
     }

@@ -206,7 +206,7 @@ mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_rende
     uint32_t* out = rgba8;
     uint32_t* tmp = nullptr;
     if (!rgba8_is_device) {
-        CU(cudaMallocAsync(&tmp, (size_t)npix * 4, v->stream));
+        CU(mrp::dev_malloc_async(&tmp, (size_t)npix * 4, v->stream));
         out = tmp;
     }
     mrp_status st = MRP_OK;
@@ -243,7 +243,7 @@ mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_rende
         return MRP_OK;
     };
     st = run();
-    if (tmp) cudaFreeAsync(tmp, v->stream);
+    if (tmp) mrp::dev_free_async(tmp, v->stream);
     if (st != MRP_OK) return st;
     if (predict && v->params.precision != MRP_FP32) {
         int herr = 0;

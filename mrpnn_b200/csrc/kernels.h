@@ -1,6 +1,7 @@
 // kernels.h -- launch entry points of the MRPNN B200 kernels (host side).
 #pragma once
 #include "common.cuh"
+#include "dev_alloc.h"
 
 namespace mrp {
 

@@ -161,14 +161,14 @@ cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
     std::memcpy(&aux[kAuxLX12W], w32 + kLX12W, 16 * sizeof(float));
     aux[kAuxLX12B] = w32[kLX12B];
     cudaError_t e;
-    if (!w.d_aux && (e = cudaMalloc(&w.d_aux, kAuxCount * sizeof(float))) != cudaSuccess) return e;
+    if (!w.d_aux && (e = mrp::dev_malloc(&w.d_aux, kAuxCount * sizeof(float))) != cudaSuccess) return e;
     if ((e = cudaMemcpy(w.d_aux, aux.data(), kAuxCount * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
         return e;
-    if (!w.d_bf16 && (e = cudaMalloc(&w.d_bf16, img16.size())) != cudaSuccess) return e;
-    if (!w.d_fp8 && (e = cudaMalloc(&w.d_fp8, img8.size())) != cudaSuccess) return e;
-    if (!w.d_scales && (e = cudaMalloc(&w.d_scales, kScaleCount * sizeof(float))) != cudaSuccess) return e;
-    if (!w.d_err && (e = cudaMalloc(&w.d_err, sizeof(int))) != cudaSuccess) return e;
-    if (!w.d_counter && (e = cudaMalloc(&w.d_counter, sizeof(int))) != cudaSuccess) return e;
+    if (!w.d_bf16 && (e = mrp::dev_malloc(&w.d_bf16, img16.size())) != cudaSuccess) return e;
+    if (!w.d_fp8 && (e = mrp::dev_malloc(&w.d_fp8, img8.size())) != cudaSuccess) return e;
+    if (!w.d_scales && (e = mrp::dev_malloc(&w.d_scales, kScaleCount * sizeof(float))) != cudaSuccess) return e;
+    if (!w.d_err && (e = mrp::dev_malloc(&w.d_err, sizeof(int))) != cudaSuccess) return e;
+    if (!w.d_counter && (e = mrp::dev_malloc(&w.d_counter, sizeof(int))) != cudaSuccess) return e;
     if ((e = cudaMemcpy(w.d_bf16, img16.data(), img16.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     if ((e = cudaMemcpy(w.d_fp8, img8.data(), img8.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     if ((e = cudaMemcpy(w.d_scales, scales.data(), kScaleCount * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -180,12 +180,12 @@ cudaError_t tc_prepare_weights(const float* w32, TcWeights& w) {
 }
 cudaError_t tc_ensure_scratch(TcScratch& s) {
     if (s.d) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&s.d, 2 * sizeof(int));
+    cudaError_t e = mrp::dev_malloc(&s.d, 2 * sizeof(int));
     if (e != cudaSuccess) { s.d = nullptr; return e; }
     return cudaMemset(s.d, 0, 2 * sizeof(int));
 }
 void tc_free_scratch(TcScratch& s) {
-    if (s.d) cudaFree(s.d);
+    if (s.d) mrp::dev_free(s.d);
     s.d = nullptr;
 }
 

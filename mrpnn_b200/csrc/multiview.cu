@@ -42,23 +42,23 @@ mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* 
     // buffers (kept on the volume between calls)
     MultiViewBuffers& B = v->mv;
     if (B.cap_views < kTcMaxSegments) {
-        CU(cudaMalloc(&B.rec_count, kTcMaxSegments * sizeof(int)));
-        CU(cudaMalloc(&B.d_segs, kTcMaxSegments * sizeof(TcSegment)));
+        CU(mrp::dev_malloc(&B.rec_count, kTcMaxSegments * sizeof(int)));
+        CU(mrp::dev_malloc(&B.d_segs, kTcMaxSegments * sizeof(TcSegment)));
         B.cap_views = kTcMaxSegments;
     }
     if (B.cap_pix < total) {
-        cudaFree(B.rec_pix); cudaFree(B.rec_f); cudaFree(B.accum);
+        mrp::dev_free(B.rec_pix); mrp::dev_free(B.rec_f); mrp::dev_free(B.accum);
         B.rec_pix = nullptr; B.rec_f = nullptr; B.accum = nullptr; B.cap_pix = 0;
-        CU(cudaMalloc(&B.rec_pix, total * sizeof(int)));
-        CU(cudaMalloc(&B.rec_f, total * 16 * sizeof(float)));
-        CU(cudaMalloc(&B.accum, total * sizeof(float4)));
+        CU(mrp::dev_malloc(&B.rec_pix, total * sizeof(int)));
+        CU(mrp::dev_malloc(&B.rec_f, total * 16 * sizeof(float)));
+        CU(mrp::dev_malloc(&B.accum, total * sizeof(float4)));
         B.cap_pix = total;
     }
     if (B.cap_feat < feat_floats) {
-        cudaFree(B.feat);
+        mrp::dev_free(B.feat);
         B.feat = nullptr;
         B.cap_feat = 0;
-        CU(cudaMalloc(&B.feat, feat_floats * sizeof(float)));
+        CU(mrp::dev_malloc(&B.feat, feat_floats * sizeof(float)));
         B.cap_feat = feat_floats;
     }
     CU(tc_ensure_scratch(v->tc));
@@ -111,8 +111,8 @@ mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* 
 namespace mrpi {
 void free_multiview(mrp_volume* v) {
     MultiViewBuffers& B = v->mv;
-    cudaFree(B.rec_count); cudaFree(B.rec_pix); cudaFree(B.rec_f); cudaFree(B.feat); cudaFree(B.accum);
-    cudaFree(B.d_segs);
+    mrp::dev_free(B.rec_count); mrp::dev_free(B.rec_pix); mrp::dev_free(B.rec_f); mrp::dev_free(B.feat); mrp::dev_free(B.accum);
+    mrp::dev_free(B.d_segs);
     B = MultiViewBuffers{};
 }
 }  // namespace mrpi

@@ -129,7 +129,7 @@ struct mrp_server {
     void free_buffers(Slot& s) {
         for (void* p : {(void*)s.trs, (void*)s.rec_count, (void*)s.rec_pix, (void*)s.rec_f, (void*)s.feat,
                         (void*)s.accum})
-            if (p) cudaFreeAsync(p, s.stream);
+            if (p) mrp::dev_free_async(p, s.stream);
         s.trs = nullptr; s.rec_count = nullptr; s.rec_pix = nullptr; s.rec_f = nullptr; s.feat = nullptr;
         s.accum = nullptr;
         used -= s.bytes;
@@ -139,12 +139,12 @@ struct mrp_server {
     cudaError_t grow(Slot& s, size_t npix) {
         free_buffers(s);
         cudaError_t e;
-        if ((e = cudaMallocAsync(&s.trs, kTrFloats * sizeof(float), s.stream)) != cudaSuccess ||
-            (e = cudaMallocAsync(&s.rec_count, sizeof(int), s.stream)) != cudaSuccess ||
-            (e = cudaMallocAsync(&s.rec_pix, npix * sizeof(int), s.stream)) != cudaSuccess ||
-            (e = cudaMallocAsync(&s.rec_f, npix * 16 * sizeof(float), s.stream)) != cudaSuccess ||
-            (e = cudaMallocAsync(&s.feat, tiled_feature_floats(npix) * sizeof(float), s.stream)) != cudaSuccess ||
-            (e = cudaMallocAsync(&s.accum, npix * sizeof(float4), s.stream)) != cudaSuccess) {
+        if ((e = mrp::dev_malloc_async(&s.trs, kTrFloats * sizeof(float), s.stream)) != cudaSuccess ||
+            (e = mrp::dev_malloc_async(&s.rec_count, sizeof(int), s.stream)) != cudaSuccess ||
+            (e = mrp::dev_malloc_async(&s.rec_pix, npix * sizeof(int), s.stream)) != cudaSuccess ||
+            (e = mrp::dev_malloc_async(&s.rec_f, npix * 16 * sizeof(float), s.stream)) != cudaSuccess ||
+            (e = mrp::dev_malloc_async(&s.feat, tiled_feature_floats(npix) * sizeof(float), s.stream)) != cudaSuccess ||
+            (e = mrp::dev_malloc_async(&s.accum, npix * sizeof(float4), s.stream)) != cudaSuccess) {
             free_buffers(s);
             return e;
         }
@@ -173,11 +173,11 @@ const Lut* mrp_server::lut_for(float g_, uint32_t seed, cudaStream_t s, std::str
         }
     Lut l{g_, seed, nullptr, nullptr};
     cudaError_t e;
-    if ((e = cudaMalloc(&l.d, kLutBytes)) != cudaSuccess) { *err = cuda_msg("LUT", e); return nullptr; }
+    if ((e = mrp::dev_malloc(&l.d, kLutBytes)) != cudaSuccess) { *err = cuda_msg("LUT", e); return nullptr; }
     if ((e = cudaEventCreateWithFlags(&l.ready, cudaEventDisableTiming)) != cudaSuccess ||
         (e = launch_hg_lut(l.d, g_, seed, s)) != cudaSuccess ||
         (e = launch_lut_dirs(l.d, l.d + kLut * kLut, s)) != cudaSuccess || (e = cudaEventRecord(l.ready, s)) != cudaSuccess) {
-        cudaFree(l.d);
+        mrp::dev_free(l.d);
         if (l.ready) cudaEventDestroy(l.ready);
         *err = cuda_msg("LUT", e);
         return nullptr;
@@ -349,10 +349,10 @@ void mrp_server::enqueue_output(Slot& s, bool after_net) {
                 e = cudaMemcpyAsync(out, s.accum, bytes, cudaMemcpyDeviceToHost, s.stream);
             } else {
                 if (s.staging_cap < bytes) {
-                    if (s.staging) cudaFreeHost(s.staging);
+                    if (s.staging) mrp::host_free_pinned(s.staging);
                     s.staging = nullptr;
                     s.staging_cap = 0;
-                    e = cudaMallocHost(&s.staging, bytes);
+                    e = mrp::host_malloc_pinned(&s.staging, bytes);
                     if (e == cudaSuccess) s.staging_cap = bytes;
                 }
                 if (e == cudaSuccess) e = cudaMemcpyAsync(s.staging, s.accum, bytes, cudaMemcpyDeviceToHost, s.stream);
@@ -448,9 +448,9 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
         if (p->net) cudaStreamDestroy(p->net);
         if (p->ev_net) cudaEventDestroy(p->ev_net);
         tc_free_scratch(p->sc);
-        cudaFree(p->d_segs);
-        if (p->h_segs) cudaFreeHost(p->h_segs);
-        if (p->h_err) cudaFreeHost(p->h_err);
+        mrp::dev_free(p->d_segs);
+        if (p->h_segs) mrp::host_free_pinned(p->h_segs);
+        if (p->h_err) mrp::host_free_pinned(p->h_err);
         delete p;
         return st;
     };
@@ -464,9 +464,9 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
     if ((e = cudaStreamCreateWithFlags(&S->net, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&S->ev_net, cudaEventDisableTiming)) != cudaSuccess ||
         (e = tc_ensure_scratch(S->sc)) != cudaSuccess ||
-        (e = cudaMalloc(&S->d_segs, kTcMaxSegments * sizeof(TcSegment))) != cudaSuccess ||
-        (e = cudaMallocHost(&S->h_segs, kTcMaxSegments * sizeof(TcSegment))) != cudaSuccess ||
-        (e = cudaMallocHost(&S->h_err, sizeof(int))) != cudaSuccess)
+        (e = mrp::dev_malloc(&S->d_segs, kTcMaxSegments * sizeof(TcSegment))) != cudaSuccess ||
+        (e = mrp::host_malloc_pinned(&S->h_segs, kTcMaxSegments * sizeof(TcSegment))) != cudaSuccess ||
+        (e = mrp::host_malloc_pinned(&S->h_err, sizeof(int))) != cudaSuccess)
         return cleanup(fail(MRP_ERR_CUDA, "server set-up: %s", cudaGetErrorString(e)));
     *S->h_err = 0;
     {   // keep freed slot memory in the device pool instead of returning it
@@ -552,21 +552,21 @@ mrp_status mrp_serve_close(mrp_server* S) {
     for (Slot& s : S->slots) {
         S->free_buffers(s);
         cudaStreamSynchronize(s.stream);
-        if (s.staging) cudaFreeHost(s.staging);
+        if (s.staging) mrp::host_free_pinned(s.staging);
         cudaStreamDestroy(s.stream);
         cudaEventDestroy(s.ev_feat);
         cudaEventDestroy(s.ev_done);
     }
     for (Lut& l : S->luts) {
-        cudaFree(l.d);
+        mrp::dev_free(l.d);
         cudaEventDestroy(l.ready);
     }
     cudaStreamDestroy(S->net);
     cudaEventDestroy(S->ev_net);
     tc_free_scratch(S->sc);
-    cudaFree(S->d_segs);
-    cudaFreeHost(S->h_segs);
-    cudaFreeHost(S->h_err);
+    mrp::dev_free(S->d_segs);
+    mrp::host_free_pinned(S->h_segs);
+    mrp::host_free_pinned(S->h_err);
     cudaMemPool_t pool;   // give the slots' memory back to the device
     if (cudaDeviceGetDefaultMemPool(&pool, g.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     delete S;

@@ -14,7 +14,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libmrpnn_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmrpnn_ref.so")
-REF_TREE = os.environ.get("MRPNN_REFERENCE", "/root/reference")
+# The reference tree is located by oracle/Makefile (its REF variable, which
+# MRPNN_REFERENCE overrides); this module never names a path of its own.
+REF_TREE_ENV = "MRPNN_REFERENCE"
 MODEL = os.path.join(os.path.dirname(HERE), "mrpnn_b200", "data", "mrpnn_model.bin")
 
 f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -112,8 +114,23 @@ def lib():
     return _lib
 
 
+def _make_ref_args():
+    tree = os.environ.get(REF_TREE_ENV)
+    return [f"REF={tree}"] if tree else []
+
+
+def ref_tree():
+    """The reference tree the Makefile's `ref` target compiles from."""
+    make = shutil.which("make") or "make"
+    r = subprocess.run([make, "-s", "-C", HERE, "ref-tree"] + _make_ref_args(), capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
 def ref_available():
-    return os.path.exists(REF_SO) or os.path.isdir(os.path.join(REF_TREE, "core"))
+    if os.path.exists(REF_SO):
+        return True
+    tree = ref_tree()
+    return bool(tree) and os.path.isdir(os.path.join(tree, "core"))
 
 
 def ref():
@@ -121,9 +138,9 @@ def ref():
     global _ref
     if _ref is None:
         if not os.path.exists(REF_SO):
-            if not os.path.isdir(os.path.join(REF_TREE, "core")):
+            if not ref_available():
                 raise RuntimeError("reference checker not built and reference tree absent")
-            subprocess.run([shutil.which("make") or "make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+            subprocess.run([shutil.which("make") or "make", "-s", "-C", HERE, "ref"] + _make_ref_args(), check=True)
         R = C.CDLL(REF_SO)
         vp = C.c_void_p
         R.ref_bind_scene.argtypes = [vp, C.c_int, C.c_float, vp, vp, vp, vp, C.c_int, f32p, C.c_float, f32p]

@@ -11,7 +11,8 @@ Scene-based cases use a small synthetic scene rebuilt identically by the test
 (fBm 32^3, pyramid, TR mips, the HG-LUT rows the gather reads); checksums of
 those scene arrays are stored too.
 
-Usage: python tests/golden/make_golden.py   (needs /root/reference)
+Usage: python tests/golden/make_golden.py   (needs the reference tree that
+oracle/Makefile reads: its REF default, or MRPNN_REFERENCE)
 """
 import ctypes as C
 import hashlib

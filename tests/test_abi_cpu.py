@@ -134,3 +134,25 @@ def test_header_is_plain_c(tmp_path):
                     "-Wl,-rpath," + lib], check=True)
     if not _has_gpu():
         assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_feature_sets_are_validated_before_the_c_abi():
+    """The predictor entry points read n * 576 and n floats from the caller's
+    pointers; malformed arrays are refused in the host mirror with a clear
+    error, before any device or C ABI call."""
+    import mrpnn_b200
+    good_f, good_g = np.zeros((3, 576), np.float32), np.zeros(3, np.float32)
+    for fn in (mrpnn_b200.predict_features, mrpnn_b200.predict_features_noalloc):
+        with pytest.raises(ValueError, match="576"):
+            fn(np.zeros((3, 575), np.float32), good_g, 0.5, (1, 1, 1))
+        with pytest.raises(ValueError, match="576"):
+            fn(np.zeros(576, np.float32), np.zeros(1, np.float32), 0.5, (1, 1, 1))
+        with pytest.raises(ValueError, match="gamma"):
+            fn(good_f, np.zeros(4, np.float32), 0.5, (1, 1, 1))
+    with pytest.raises(ValueError, match="out"):
+        mrpnn_b200.predict_features(good_f, good_g, 0.5, (1, 1, 1), out=np.zeros((3, 4), np.float32))
+
+
+def test_allocation_counter_needs_no_device():
+    import mrpnn_b200
+    assert isinstance(mrpnn_b200.debug_alloc_calls(), int)

@@ -12,6 +12,7 @@ import os
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from tests.golden.make_golden import SCENE, build_scene, camera, light_dir
 
 
@@ -149,9 +150,7 @@ def test_philox_known_answers(oracle):
         assert list(out) == want
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
-                                                    "oracle", "_ref", "libmrpnn_ref.so"))
-                    and not os.path.isdir("/root/reference/core"), reason="reference checker not available")
+@pytest.mark.skipif(not O.ref_available(), reason="reference checker not available")
 def test_live_reference_mlp_small(oracle):
     """Re-run the reference MLP (live build) on fresh random features."""
     rng = np.random.default_rng(7)

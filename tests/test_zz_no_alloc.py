@@ -7,8 +7,9 @@ synchronisation of cudaFree, or a process whose memory pool already holds
 the HBM).  It runs the same network kernels as mrp_predict_features, with
 its staging, output, tile counter and error flag in the library's fixed
 device array.  So two calls in a row must each match the allocating call
-within the predictor's test tolerance, and the device memory in use must
-not change across calls.  The file is named to be collected last."""
+within the predictor's test tolerance, and the library's count of
+allocation calls (and the device memory in use) must not change across
+calls.  The file is named to be collected last."""
 import numpy as np
 import pytest
 
@@ -52,15 +53,23 @@ def test_noalloc_full_capacity_and_rejects_more():
         M.predict_features_noalloc(feat, gam, 0.5, (1, 1, 1))
 
 
-def test_noalloc_leaves_device_memory_unchanged():
+def test_noalloc_makes_no_allocation_call():
+    """The library counts every cudaMalloc / cudaMallocAsync / cudaMallocHost
+    and free it makes; the no-allocation entry point must add none, not even
+    one freed again before it returns.  Device-wide free memory is checked as
+    well, as a second witness."""
     import torch
     import mrpnn_b200 as M
     M.init()
     feat, gam = _features(1024, 34)
     M.predict_features_noalloc(feat, gam, 0.857, (1, 1, 1), precision=M.BF16)   # first call: address lookup
     torch.cuda.synchronize()
+    calls = M.debug_alloc_calls()
     before = torch.cuda.mem_get_info()[0]
     for prec in (M.FP32, M.BF16, M.FP8, M.BF16):
         M.predict_features_noalloc(feat, gam, 0.857, (1, 1, 1), precision=prec)
-    after = torch.cuda.mem_get_info()[0]
-    assert after == before
+    assert M.debug_alloc_calls() == calls
+    assert torch.cuda.mem_get_info()[0] == before
+    v = M.VolumeRender(16)                      # a volume handle allocates: the counter sees it
+    assert M.debug_alloc_calls() > calls
+    del v
