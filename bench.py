@@ -170,8 +170,9 @@ def view_vectors():
     return ori, (up * s).astype(np.float32), (right * s).astype(np.float32)
 
 
-def time_cpu_predict(sc, n_pix, seed=0, reps=1):
-    """Oracle predictor on a random sample of the 1024^2 frame -> pixels/s."""
+def time_cpu_predict(sc, n_pix, seed=0, reps=1, want=False):
+    """Oracle predictor on a random sample of the 1024^2 frame -> pixels/s
+    (and, with want, the sampled pixel indices and their RGBA)."""
     from oracle import oracle as O
     ori, up, right = view_vectors()
     view = O.make_view(W, H, ori, up, right, light(), alpha=SCENE["alpha"], g=SCENE["g"], seed=seed, frame=0)
@@ -179,9 +180,39 @@ def time_cpu_predict(sc, n_pix, seed=0, reps=1):
     px = rng.choice(W * H, n_pix, replace=False).astype(np.int32)
     t0 = time.perf_counter()
     for _ in range(reps):
-        O.predict_pixels(sc, view, px)
+        rgba = O.predict_pixels(sc, view, px)
     dt = time.perf_counter() - t0
+    if want:
+        return n_pix * reps / dt, dt, px, rgba
     return n_pix * reps / dt, dt
+
+
+def frame_parity(vol, px, ref, local):
+    """The GPU's FP32 frame of the CPU baseline's view (seed 0, frame 0)
+    against the oracle's pixels px (RGBA ref): the FP32 predictor's 1e-4
+    relative contract, checked at the benchmarked size."""
+    import torch
+
+    import mrpnn_b200 as M
+    ori, up, right = view_vectors()
+    prec = vol.GetPrecision()
+    vol.SetPrecision(M.FP32)
+    try:
+        view = vol.make_view((W, H), ori, up, right, light(), SCENE["g"], SCENE["alpha"], seed=0, frame_offset=0)
+        out = torch.empty((H, W, 4), dtype=torch.float32, device=f"cuda:{local}")
+        vol.render_view(view, M.VolumeRender.MRPNN, 1, out)
+        got = out.reshape(-1, 4).cpu().numpy()[px]
+    finally:
+        vol.SetPrecision(prec)
+    ok = np.isclose(got, ref, rtol=1e-4, atol=1e-6).all(axis=1)
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-6)
+    hit_g, hit_r = got[:, 3] > 0, ref[:, 3] > 0
+    return {"form": "fp32", "pixels": int(px.size), "hit_pixels": int(hit_r.sum()),
+            "hit_mismatch": int((hit_g != hit_r).sum()), "frac_within_1e-4_rel": float(ok.mean()),
+            "max_rel": float(rel[:, :3].max()),
+            "median_rel_hit": float(np.median(rel[hit_r, :3])) if hit_r.any() else 0.0,
+            "tolerance": "rtol 1e-4 + atol 1e-6 per RGBA component (the FP32 predictor contract)",
+            "oracle": "OpenMP CPU oracle, pinned bit for bit to the reference's own NNPredict compiled on the CPU"}
 
 
 def omp_threads():
@@ -198,19 +229,22 @@ def run_reference(args, rank, world):
     n_pix = args.ref_pixels
     for _ in range(args.warmup):
         time_cpu_predict(sc, max(256, n_pix // 8))
-    rates = []
+    secs = []
     for k in range(args.steps):
-        r, _ = time_cpu_predict(sc, n_pix, seed=k + 1)
-        rates.append(r)
-    pix_s = float(np.mean(rates))
+        _, dt = time_cpu_predict(sc, n_pix, seed=k + 1)
+        secs.append(dt)
+    pix_s = n_pix * len(secs) / float(np.sum(secs))
     fps = pix_s / (W * H)
     cores = omp_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000.0 / fps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.mean(secs)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"MRPNN predictor, {W}x{H} frame, {RES}^3 fBm (seed 1, freq 6), FP32 MLP",
-                   "sample": f"{n_pix} random pixels per step"},
+                   "sample": f"{n_pix} random pixels per step",
+                   "step": "one step = the sampled pixels of one frame; ms_per_step is the measured time of that "
+                           "sample; value = sampled pixels/s over all steps / pixels per frame",
+                   "ms_per_full_frame": 1000.0 / fps},
         "cpu_baseline": {"value": fps, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{n_pix} random pixels of the {W}x{H} frame per step, scene setup {setup_s:.1f}s"},
         "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -245,27 +279,57 @@ def run_tracer(args, local):
                          spp=TRACER["spp"], seed=7)
     out = torch.empty((n, n, 4), dtype=torch.float32, device=f"cuda:{local}")
     vol.render_view(view, M.VolumeRender.PT, 1, out)
-    ms = []
+    ms, trace_ms = [], []
     for k in range(args.tracer_steps):
         view.frame_offset = 10 + k
         vol.render_view(view, M.VolumeRender.PT, 1, out)
         ms.append(vol.last_render_ms())
-    view.frame_offset = 10   # the counters of the first timed frame, whatever --tracer-steps is
+        trace_ms.append(vol.last_render_stages()[0])   # the trace kernel of this timed frame
+    trace_ms = float(np.mean(trace_ms))
+    # work counters of the first timed frame (same streams; a separate,
+    # instrumented launch that is not timed)
+    view.frame_offset = 10
     cnt = vol.render_counters(view, M.VolumeRender.PT)   # bounces, fetches, NEE lookups, samples
     t = float(np.mean(ms))
-    trace_ms = vol.last_render_stages()[0]
     hbm, _, peak_kind = peaks()
     alg = (cnt[1] + cnt[2]) * 32 + n * n * 16
     ach = alg / (trace_ms / 1000.0) / 1e9
-    return {"workload": f"PT {n}x{n}, {TRACER['spp']} spp, <= {TRACER['bounces']} bounces, "
-                        f"{TRACER['res']}^3 fBm (seed 0, freq 4), NEE via {TRACER['bake_res']}^3 baked TR",
-            "ms_per_frame": t, "samples_per_s": n * n * TRACER["spp"] / (t / 1000.0),
-            "density_lookups_per_s": (cnt[1] + cnt[2]) / (trace_ms / 1000.0),
-            "counters": {"bounces": cnt[0], "free_flight_fetches": cnt[1], "nee_lookups": cnt[2], "samples": cnt[3]},
-            "bake_s": bake_s,
-            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "note": f"trace kernel; algorithmic bytes = (fetches + NEE lookups) x 32 B (8 fp32 texels) "
-                                 f"+ 16 B/pixel; peak {peak_kind}; the 8 MiB volume is L2-resident"}}
+    res = {"workload": f"PT {n}x{n}, {TRACER['spp']} spp, <= {TRACER['bounces']} bounces, "
+                       f"{TRACER['res']}^3 fBm (seed 0, freq 4), NEE via {TRACER['bake_res']}^3 baked TR",
+           "ms_per_frame": t, "trace_kernel_ms": trace_ms, "samples_per_s": n * n * TRACER["spp"] / (t / 1000.0),
+           "density_lookups_per_s": (cnt[1] + cnt[2]) / (trace_ms / 1000.0),
+           "counters": {"bounces": cnt[0], "free_flight_fetches": cnt[1], "nee_lookups": cnt[2], "samples": cnt[3]},
+           "bake_s": bake_s,
+           "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                        "note": f"trace kernel of the timed frames; algorithmic bytes = (fetches + NEE lookups) x 32 B "
+                                f"(8 fp32 texels) + 16 B/pixel; peak {peak_kind}; the 8 MiB volume is L2-resident"}}
+    if args.tracer_cpu_pixels > 0:
+        res["cpu_baseline"] = time_cpu_tracer(vol, min(args.tracer_cpu_pixels, n * n))
+    return res
+
+
+def time_cpu_tracer(vol, n_pix):
+    """The oracle's CalculateRadiance (OpenMP) on the tracer workload: the
+    same scene (the GPU's grid and baked NEE grid), the same spp and bounce
+    limit, over a seeded sample of the frame's pixels -> samples/s."""
+    import mrpnn_b200 as M
+    from oracle import oracle as O
+    R = TRACER["res"]
+    sc = O.SceneBuf(vol.read(M.api.RES_DENSITY), R, vol.max_density, baked=vol.read(M.api.RES_BAKED_TR),
+                    baked_res=TRACER["bake_res"], scatter_rate=(SCENE["albedo"],) * 3, sky=(SCENE["sky"],) * 3)
+    n = TRACER["size"]
+    ori, up, right = view_vectors()
+    ov = O.make_view(n, n, ori, up, right, light(), alpha=SCENE["alpha"], g=SCENE["g"],
+                     multi_scatter=TRACER["bounces"], spp=TRACER["spp"], seed=7, frame=10)
+    px = np.random.default_rng(11).choice(n * n, n_pix, replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    O.trace_pixels(sc, ov, px)
+    dt = time.perf_counter() - t0
+    sps = n_pix * TRACER["spp"] / dt
+    return {"value": sps, "unit": "samples/s", "cores": omp_threads(), "kind": "port",
+            "ms_per_frame": n * n * TRACER["spp"] / sps * 1000.0,
+            "sample": f"{n_pix} of the {n}x{n} pixels x {TRACER['spp']} spp ({dt:.1f} s), OpenMP oracle "
+                      "CalculateRadiance with the baked NEE grid"}
 
 
 SERVE = dict(volumes=16, sizes=(128, 256, 512), seeds=range(10, 26), alpha=(16.0, 256.0), freq=4.0, rate=200.0,
@@ -524,6 +588,34 @@ def time_frames(vol, view, steps, flush, dev_out, frame0):
     return ms, np.mean(np.asarray(stages), axis=0)
 
 
+def e2e_loops(vol, view, n, host_out, world):
+    """Frames/s end to end through the public API, every frame copied to a
+    pinned host buffer: mrp_render (each call returns with its frame on the
+    host), then the frame loop of mrp_render_start / mrp_render_wait(keep=1),
+    in which frame k - 1's copy back overlaps frame k's kernels (two host
+    buffers alternate).  Both after three warm-up frames of each API."""
+    import mrpnn_b200 as M
+    for k in range(3):
+        vol.render_view(view, M.VolumeRender.MRPNN, 1, host_out[0])
+        vol.render_view_start(view, M.VolumeRender.MRPNN, 1, host_out[k % 2])
+    vol.render_wait()
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(n):
+        view.frame_offset = 2000 + k
+        vol.render_view(view, M.VolumeRender.MRPNN, 1, host_out[0])
+    sync = n * world / max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(n):
+        view.frame_offset = 3000 + k
+        vol.render_view_start(view, M.VolumeRender.MRPNN, 1, host_out[k % 2])
+        if k:
+            vol.render_wait(keep=1)   # frame k - 1 is in host_out[(k - 1) % 2]
+    vol.render_wait()
+    return sync, n * world / max_over_ranks(time.perf_counter() - t0, world)
+
+
 def run_mine(args, rank, world, local):
     import torch
 
@@ -564,7 +656,6 @@ def run_mine(args, rank, world, local):
                     "stage_ms": dict(zip(STAGES, [round(float(x), 4) for x in stage_ms]))}
     head = forms[args.precision]
     total_ms = head["ms_per_frame"] * args.steps
-    frames = args.steps * world
     value = head["value"]
     img = dev_out.cpu().numpy()
     active = int((img[..., 3] > 0).sum())
@@ -575,21 +666,15 @@ def run_mine(args, rank, world, local):
     # frame k - 1 is on the host while frame k computes (its copy back
     # overlapped frame k's kernels); two host buffers alternate
     host_out = [torch.empty((H, W, 4), dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
-    barrier(world)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        view.frame_offset = 2000 + k
-        vol.render_view(view, M.VolumeRender.MRPNN, 1, host_out[0])
-    e2e_sync = frames / max_over_ranks(time.perf_counter() - t0, world)
-    barrier(world)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        view.frame_offset = 3000 + k
-        vol.render_view_start(view, M.VolumeRender.MRPNN, 1, host_out[k % 2])
-        if k:
-            vol.render_wait(keep=1)   # frame k - 1 is in host_out[(k - 1) % 2]
-    vol.render_wait()
-    e2e = frames / max_over_ranks(time.perf_counter() - t0, world)
+    n_e2e = max(args.e2e_frames, args.steps)
+    e2e_sync, e2e = e2e_loops(vol, view, n_e2e, host_out, world)
+    # the FP32 drop-in through the same public API (like-for-like with the
+    # reference arm, whose MLP is FP32)
+    n_fp32 = max(50, n_e2e // 4)
+    vol.SetPrecision(M.FP32)
+    fp32_sync, fp32_async = e2e_loops(vol, view, n_fp32, host_out, world)
+    vol.SetPrecision(precs[args.precision])
+    forms["fp32"]["e2e"] = {"value": fp32_async, "sync_value": fp32_sync, "frames": n_fp32}
 
     hbm, bf16, peak_kind = peaks()
     st = list(head["stage_ms"].values())
@@ -635,13 +720,15 @@ def run_mine(args, rank, world, local):
     large = run_large(args, local) if (rank == 0 and args.large) else None
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sc = cpu_scene_from_gpu(vol)
         n_cpu = min(args.cpu_pixels, W * H)
-        pix_s, dt = time_cpu_predict(sc, n_cpu, reps=args.cpu_reps)
+        pix_s, dt, px, ref = time_cpu_predict(sc, n_cpu, reps=args.cpu_reps, want=True)
         cpu = {"value": pix_s / (W * H), "unit": UNIT, "cores": omp_threads(), "kind": "port",
                "sample": f"{args.cpu_reps} passes over {n_cpu} pixels of the {W}x{H} frame ({dt:.1f} s), "
                          f"OpenMP oracle (first hit, gather, FP32 MLP)"}
+        parity = frame_parity(vol, px, ref, local)
 
     if rank == 0:
         line = {
@@ -654,11 +741,13 @@ def run_mine(args, rank, world, local):
                        "l2": "flushed (256 MiB write) between timed steps", "hit_pixels": active,
                        "precision_forms": forms},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 96, "d2h_bytes_per_step": W * H * 16,
+                    "frames": n_e2e,
                     "api": "mrp_render_start + mrp_render_wait(keep=1) frame loop, pinned host buffers",
                     "sync_value": e2e_sync, "sync_api": "mrp_render per frame, pinned host buffer"},
             "gpu_launches": args.steps * 3,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clocks.summary(),
             "tracer": tracer,
             "serving": serving,
@@ -684,6 +773,9 @@ def main():
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="density grid storage of the headline volume (fp32: the reference's float grid)")
     ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
+    ap.add_argument("--tracer-cpu-pixels", type=int, default=16384,
+                    help="pixels of the tracer's CPU-baseline sample (0: skip)")
+    ap.add_argument("--e2e-frames", type=int, default=200, help="frames of each end-to-end loop (at least --steps)")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving workload (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=SERVE["slots"], help="request slots of the server")
     ap.add_argument("--rmse-spp", type=int, default=4096, help="spp of the PT reference image (0: skip)")

@@ -416,6 +416,9 @@ class VolumeRender:
         self._params.precision = int(precision)
         self._push()
 
+    def GetPrecision(self):
+        return int(self._params.precision)
+
     def SetBakeResolution(self, res, replicate_reference_seeding=True):
         self._params.bake_res = int(res)
         self._params.bake_replicate_seeding = 1 if replicate_reference_seeding else 0
