@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libmrpnn_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmrpnn_ref.so")
+REF_VOLUME_SO = os.path.join(HERE, "_ref", "libmrpnn_ref_volume.so")
 # The reference tree is located by oracle/Makefile (its REF variable, which
 # MRPNN_REFERENCE overrides); this module never names a path of its own.
 REF_TREE_ENV = "MRPNN_REFERENCE"
@@ -48,6 +49,7 @@ def _build(target):
 
 _lib = None
 _ref = None
+_ref_vol = None
 
 
 def lib():
@@ -171,6 +173,79 @@ def ref():
                                       C.c_int, C.c_int, C.c_int, C.c_int, f32p]
         _ref = R
     return _ref
+
+
+def ref_volume():
+    """The reference's core/volume.cu volume builders compiled on the CPU
+    (built on demand with the `ref` target)."""
+    global _ref_vol
+    if _ref_vol is None:
+        if not os.path.exists(REF_VOLUME_SO):
+            if not ref_available():
+                raise RuntimeError("reference checker not built and reference tree absent")
+            subprocess.run([shutil.which("make") or "make", "-s", "-C", HERE, "ref"] + _make_ref_args(), check=True)
+        R = C.CDLL(REF_VOLUME_SO)
+        R.ref_vol_pyramid.argtypes = [f32p, C.c_int, f32p]
+        R.ref_vol_tr.argtypes = [f32p, C.c_int, C.c_float, f32p, C.c_int, f32p]
+        R.ref_vol_hg_texels.argtypes = [C.c_float, C.c_uint32, i32p, C.c_int, f32p]
+        R.ref_vol_get_hg_lut.argtypes = [f32p, C.c_float, C.c_float]
+        R.ref_vol_get_hg_lut.restype = C.c_float
+        R.ref_vol_bake_voxels.argtypes = [f32p, C.c_int, C.c_float, C.c_float, f32p, C.c_int, C.c_uint32, i64p,
+                                          C.c_int, f32p]
+        R.ref_vol_load_hdr.argtypes = [C.c_char_p, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p, C.c_size_t]
+        _ref_vol = R
+    return _ref_vol
+
+
+def ref_pyramid(data, R):
+    out = np.empty(sum(r ** 3 for r in mip_sizes()), np.float32)
+    ref_volume().ref_vol_pyramid(np.ascontiguousarray(data, np.float32).ravel(), R, out)
+    return out
+
+
+def ref_tr(data, R, alpha, light_dir, cpu=False):
+    out = np.empty(sum(r ** 3 for r in tr_sizes()), np.float32)
+    ref_volume().ref_vol_tr(np.ascontiguousarray(data, np.float32).ravel(), R, alpha,
+                            np.asarray(light_dir, np.float32), 1 if cpu else 0, out)
+    return out
+
+
+def ref_hg_texels(g, seed, texels):
+    t = np.ascontiguousarray(texels, np.int32)
+    out = np.empty(t.size, np.float32)
+    ref_volume().ref_vol_hg_texels(g, seed, t, t.size, out)
+    return out
+
+
+def ref_get_hg_lut(lut, cosv, angle):
+    return ref_volume().ref_vol_get_hg_lut(np.ascontiguousarray(lut, np.float32).ravel(), cosv, angle)
+
+
+def ref_bake_voxels(data, R, max_density, alpha, light_dir, bake_res, seed, voxels):
+    v = np.ascontiguousarray(voxels, np.int64)
+    out = np.empty(v.size, np.float32)
+    ref_volume().ref_vol_bake_voxels(np.ascontiguousarray(data, np.float32).ravel(), R, max_density, alpha,
+                                     np.asarray(light_dir, np.float32), bake_res, seed, v, v.size, out)
+    return out
+
+
+def ref_load_hdr(path):
+    """The reference's RGBE loader: float32 [ry, rx, 4], or None if it fails."""
+    rx, ry = C.c_uint(), C.c_uint()
+    if ref_volume().ref_vol_load_hdr(path.encode(), C.byref(rx), C.byref(ry), None, 0) != 0:
+        return None
+    out = np.empty((ry.value, rx.value, 4), np.float32)
+    ref_volume().ref_vol_load_hdr(path.encode(), C.byref(rx), C.byref(ry), out.ctypes.data, out.size)
+    return out
+
+
+def baked_tr_voxels(scene, alpha, light_dir, bake_res, seed, voxels, replicate=True):
+    """The oracle's Fill_BakeTR at voxels (index (x * B + y) * B + z)."""
+    v = np.ascontiguousarray(voxels, np.int64)
+    out = np.empty(v.size, np.float32)
+    lib().orc_baked_tr(C.byref(scene.c), alpha, np.asarray(light_dir, np.float32), bake_res, seed,
+                       1 if replicate else 0, v, v.size, out)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -131,6 +131,22 @@ T tex2D(const texture<T, D, M>& t, float x, float y) {
         float r0 = ref_shim_lerp(F(ix, iy), F(ix, iy + 1), wy);
         float r1 = ref_shim_lerp(F(ix + 1, iy), F(ix + 1, iy + 1), wy);
         return ref_shim_lerp(r0, r1, wx);
+    } else if constexpr (std::is_same<T, float4>::value) {
+        // environment map: wrap addressing, bilinear in software with fp32
+        // weights, u (x) interpolated first -- the order of the reference's
+        // own CPU sampler Image_host::Sample (core/volume.hpp:35-42); with no
+        // map bound, the constant environment
+        if (!t.data) return t.constant;
+        float px = x * (float)t.nx - 0.5f, py = y * (float)t.ny - 0.5f;
+        int ix = (int)floorf(px), iy = (int)floorf(py);
+        float wx = px - (float)ix, wy = py - (float)iy;
+        auto W = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
+        auto F = [&](int a, int b) { return t.data[(size_t)W(b, t.ny) * t.nx + W(a, t.nx)]; };
+        auto L = [&](float4 a, float4 b, float w) {
+            return float4{ref_shim_lerp(a.x, b.x, w), ref_shim_lerp(a.y, b.y, w), ref_shim_lerp(a.z, b.z, w),
+                          ref_shim_lerp(a.w, b.w, w)};
+        };
+        return L(L(F(ix, iy), F(ix + 1, iy), wx), L(F(ix, iy + 1), F(ix + 1, iy + 1), wx), wy);
     } else {
         return t.constant;
     }
