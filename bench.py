@@ -303,15 +303,15 @@ def run_tracer(args, local):
            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                         "note": f"trace kernel of the timed frames; algorithmic bytes = (fetches + NEE lookups) x 32 B "
                                 f"(8 fp32 texels) + 16 B/pixel; peak {peak_kind}; the 8 MiB volume is L2-resident"}}
-    if args.tracer_cpu_pixels > 0:
-        res["cpu_baseline"] = time_cpu_tracer(vol, min(args.tracer_cpu_pixels, n * n))
+    if args.tracer_cpu_frames > 0:
+        res["cpu_baseline"] = time_cpu_tracer(vol, args.tracer_cpu_frames)
     return res
 
 
-def time_cpu_tracer(vol, n_pix):
+def time_cpu_tracer(vol, frames):
     """The oracle's CalculateRadiance (OpenMP) on the tracer workload: the
     same scene (the GPU's grid and baked NEE grid), the same spp and bounce
-    limit, over a seeded sample of the frame's pixels -> samples/s."""
+    limit, whole frames -> samples/s."""
     import mrpnn_b200 as M
     from oracle import oracle as O
     R = TRACER["res"]
@@ -319,16 +319,17 @@ def time_cpu_tracer(vol, n_pix):
                     baked_res=TRACER["bake_res"], scatter_rate=(SCENE["albedo"],) * 3, sky=(SCENE["sky"],) * 3)
     n = TRACER["size"]
     ori, up, right = view_vectors()
-    ov = O.make_view(n, n, ori, up, right, light(), alpha=SCENE["alpha"], g=SCENE["g"],
-                     multi_scatter=TRACER["bounces"], spp=TRACER["spp"], seed=7, frame=10)
-    px = np.random.default_rng(11).choice(n * n, n_pix, replace=False).astype(np.int32)
+    px = np.arange(n * n, dtype=np.int32)
     t0 = time.perf_counter()
-    O.trace_pixels(sc, ov, px)
+    for f in range(frames):
+        ov = O.make_view(n, n, ori, up, right, light(), alpha=SCENE["alpha"], g=SCENE["g"],
+                         multi_scatter=TRACER["bounces"], spp=TRACER["spp"], seed=7, frame=10 + f)
+        O.trace_pixels(sc, ov, px)
     dt = time.perf_counter() - t0
-    sps = n_pix * TRACER["spp"] / dt
+    sps = frames * n * n * TRACER["spp"] / dt
     return {"value": sps, "unit": "samples/s", "cores": omp_threads(), "kind": "port",
-            "ms_per_frame": n * n * TRACER["spp"] / sps * 1000.0,
-            "sample": f"{n_pix} of the {n}x{n} pixels x {TRACER['spp']} spp ({dt:.1f} s), OpenMP oracle "
+            "ms_per_frame": dt / frames * 1000.0,
+            "sample": f"{frames} whole {n}x{n} frames x {TRACER['spp']} spp ({dt:.1f} s), OpenMP oracle "
                       "CalculateRadiance with the baked NEE grid"}
 
 
@@ -773,8 +774,8 @@ def main():
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="density grid storage of the headline volume (fp32: the reference's float grid)")
     ap.add_argument("--tracer-steps", type=int, default=3, help="timed PT frames of the tracer workload (0: skip)")
-    ap.add_argument("--tracer-cpu-pixels", type=int, default=16384,
-                    help="pixels of the tracer's CPU-baseline sample (0: skip)")
+    ap.add_argument("--tracer-cpu-frames", type=int, default=20,
+                    help="whole frames of the tracer's CPU baseline (0: skip)")
     ap.add_argument("--e2e-frames", type=int, default=200, help="frames of each end-to-end loop (at least --steps)")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving workload (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=SERVE["slots"], help="request slots of the server")

@@ -156,6 +156,14 @@ mrp_status mrp_get_params(const mrp_volume* v, mrp_params* p);
  * in *count when dst is NULL. */
 mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* dst, size_t* count, int dst_is_device);
 
+/* VolumeRender::GetHGLut(cos, angle) (core/volume.cu:1424-1442): the HG
+ * lookup table (512 x 512, row = cone angle, column = cos theta, as
+ * mrp_volume_read(MRP_RES_LUT) returns it) read at (cos, angle) with the
+ * reference's host arithmetic, quirks included (the two texels of a row are
+ * blended with the row fraction, the two rows with the column fraction).
+ * Host only (no device needed). */
+mrp_status mrp_hg_lut_lookup(const float* lut, float cos_theta, float angle, float* out);
+
 /* -- volume files: VolumeRender(string path, bool cacheTR) / LoadData
  * (core/volume.cu:970-1149) --------------------------------------------------------- */
 /* .bin (int32 R, R^3 float32, z fastest), .txt (R then R^3 floats) or .vox

@@ -127,6 +127,23 @@ class VolumeRender {
         mrpnn::check(mrp_update_tr(h, L, alpha), "Update_TR");
     }
     void UpdateHGLut(float g) { mrpnn::check(mrp_update_hg_lut(h, g), "UpdateHGLut"); }
+    // core/volume.cu:1424-1442, on a host copy of the current table (read
+    // back once per table)
+    float GetHGLut(float cos, float angle) {
+        mrp_volume_info info;
+        mrpnn::check(mrp_volume_get_info(h, &info), "GetHGLut");
+        if (!info.has_lut) throw std::runtime_error("GetHGLut: no HG table yet (UpdateHGLut)");
+        if (lut_host.empty() || lut_host_g != info.lut_g) {
+            size_t n = 0;
+            mrpnn::check(mrp_volume_read(h, MRP_RES_LUT, 0, nullptr, &n, 0), "GetHGLut");
+            lut_host.assign(n, 0.0f);
+            mrpnn::check(mrp_volume_read(h, MRP_RES_LUT, 0, lut_host.data(), &n, 0), "GetHGLut");
+            lut_host_g = info.lut_g;
+        }
+        float r = 0.0f;
+        mrpnn::check(mrp_hg_lut_lookup(lut_host.data(), cos, angle, &r), "GetHGLut");
+        return r;
+    }
 
     void SetScatterRate(float rate) { SetScatterRate(float3{rate, rate, rate}); }
     void SetScatterRate(float3 rate) {
@@ -192,6 +209,8 @@ class VolumeRender {
     bool dirty = true;
     bool checkboard = true;
     float exposure = 1.0f, ior = -1.0f;
+    std::vector<float> lut_host;
+    float lut_host_g = 0.0f;
 };
 
 typedef std::function<float3(float3 radiance)> ToneMapFunction;

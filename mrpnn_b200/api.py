@@ -106,6 +106,7 @@ _SIGS = {
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "mrp_hg_lut_lookup": ([C.c_void_p, C.c_float, C.c_float, C.POINTER(C.c_float)], C.c_int),
     "mrp_volume_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
     "mrp_volume_file_write_bin": ([C.c_char_p, C.c_void_p, C.c_int], C.c_int),
     "mrp_volume_load": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
@@ -239,6 +240,17 @@ def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
     _check(lib().mrp_predict_features(feat.data_ptr(), gamma.data_ptr(), float(g), _f3(scatter_rate), n,
                                       out.data_ptr(), int(precision), 1))
     return out
+
+
+def hg_lut_lookup(lut, cos_theta, angle):
+    """mrp_hg_lut_lookup: VolumeRender::GetHGLut's read of a 512 x 512 HG
+    table (host only)."""
+    lut = _host_f32(lut).ravel()
+    if lut.size != 512 * 512:
+        raise ValueError("the HG table has 512 x 512 entries")
+    out = C.c_float()
+    _check(lib().mrp_hg_lut_lookup(lut.ctypes.data, float(cos_theta), float(angle), C.byref(out)))
+    return out.value
 
 
 def read_volume_file(path):
@@ -438,6 +450,15 @@ class VolumeRender:
     # -- caches -------------------------------------------------------------------
     def UpdateHGLut(self, g):
         _check(lib().mrp_update_hg_lut(self._h, float(g)))
+
+    def GetHGLut(self, cos, angle):
+        """VolumeRender::GetHGLut (core/volume.cu:1424-1442) on the volume's
+        current HG table (read back from the device once per table)."""
+        key = float(self.info().lut_g)
+        if getattr(self, "_lut_host_g", None) != key:
+            self._lut_host = self.read(RES_LUT)[:512 * 512].copy()
+            self._lut_host_g = key
+        return hg_lut_lookup(self._lut_host, cos, angle)
 
     def Update_TR(self, lightDir, alpha=64.0, CPU=False):
         _check(lib().mrp_update_tr(self._h, _f3(lightDir), float(alpha)))

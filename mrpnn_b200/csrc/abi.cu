@@ -51,26 +51,26 @@ std::string default_model_path() {
     return "mrpnn_model.bin";
 }
 
-uint32_t pcg_host(uint32_t v) {
-    uint32_t s = v * 747796405u + 2891336453u;
-    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
-    return (w >> 22u) ^ w;
-}
-
-// Digit permutations of the scrambled radical inverse for bases 2,3,5,7,11
-// (seeded Fisher-Yates; the reference ships a fixed random table,
-// core/volume.cu:1196).
-void halton_perms(uint32_t perm[28]) {
+// Digit permutations of the scrambled radical inverse for bases 2, 3, 5, 7,
+// 11: the reference's table (RadicalInversePermutations_, core/volume.cu:1195),
+// carried by the model file as HALTON_PERMS; each base's block must be a
+// permutation of its digits.
+mrp_status halton_perms(const std::map<std::string, std::vector<float>>& m, uint32_t perm[28]) {
+    auto it = m.find("HALTON_PERMS");
+    if (it == m.end() || it->second.size() != 28) return fail(MRP_ERR_IO, "model file: missing HALTON_PERMS");
     const uint32_t primes[5] = {2, 3, 5, 7, 11}, sums[5] = {0, 2, 5, 10, 17};
     for (int b = 0; b < 5; ++b) {
-        for (uint32_t i = 0; i < primes[b]; ++i) perm[sums[b] + i] = i;
-        uint32_t h = 0x4D525031u + (uint32_t)b;
-        for (uint32_t i = primes[b] - 1; i > 0; --i) {
-            h = pcg_host(h);
-            uint32_t j = h % (i + 1);
-            std::swap(perm[sums[b] + i], perm[sums[b] + j]);
+        uint32_t seen = 0;
+        for (uint32_t i = 0; i < primes[b]; ++i) {
+            float v = it->second[sums[b] + i];
+            if (!(v >= 0.0f && v < (float)primes[b]) || v != (float)(uint32_t)v)
+                return fail(MRP_ERR_IO, "model file: HALTON_PERMS is not a digit permutation");
+            perm[sums[b] + i] = (uint32_t)v;
+            seen |= 1u << perm[sums[b] + i];
         }
+        if (seen != (1u << primes[b]) - 1) return fail(MRP_ERR_IO, "model file: HALTON_PERMS is not a digit permutation");
     }
+    return MRP_OK;
 }
 
 float lerp_h(float a, float b, float v) { return a * (1.0f - v) + b * v; }
@@ -214,7 +214,10 @@ mrp_status mrp_load_model(const char* path) {
     if (it == m.end() || it->second.size() != 480) return fail(MRP_ERR_IO, "%s: missing STENCIL_DIRS", path);
     StencilTables st;
     stencil_tables(st, it->second);
+    uint32_t perm[28];
+    if (halton_perms(m, perm) != MRP_OK) return fail(MRP_ERR_IO, "%s: %s", path, t_err.c_str());
     CU(set_stencil_tables(st));
+    CU(set_halton_permutations(perm));
     if (!g.d_weights) CU(mrp::dev_malloc(&g.d_weights, sizeof(float) * kWeightCount));
     CU(cudaMemcpy(g.d_weights, w.data(), sizeof(float) * kWeightCount, cudaMemcpyHostToDevice));
     CU(tc_prepare_weights(w.data(), g.tc));
@@ -242,9 +245,6 @@ mrp_status mrp_init(int device, const char* model_path) {
             g.device = device;
             g.sms = prop.multiProcessorCount;
             CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
-            uint32_t perm[28];
-            halton_perms(perm);
-            CU(set_halton_permutations(perm));
             g.ready = true;
         } else {
             CU(cudaSetDevice(g.device));
@@ -508,6 +508,26 @@ mrp_status mrp_set_params(mrp_volume* v, const mrp_params* p) {
 mrp_status mrp_get_params(const mrp_volume* v, mrp_params* p) {
     if (!v || !p) return fail(MRP_ERR_INVALID, "null argument");
     *p = v->params;
+    return MRP_OK;
+}
+
+mrp_status mrp_hg_lut_lookup(const float* lut, float cos_theta, float angle, float* out) {
+    if (!lut || !out) return fail(MRP_ERR_INVALID, "null argument");
+    // GetHGLut's own arithmetic: u, v from double expressions, texels clamped
+    // to the table, then lerp(a00, a10, frac(v*N)), lerp(a01, a11, frac(v*N))
+    // and a lerp of the two by frac(u*N) (core/volume.cu:1424-1442)
+    const int N = 512;
+    auto lerp = [](float a, float b, float w) { return a * (1.0f - w) + b * w; };
+    auto frac = [](float f) { return f - (float)(long)f; };
+    auto clampi = [N](int i) { return std::max(std::min(i, N - 1), 0); };
+    float u = (float)((double)cos_theta * 0.5 + 0.5);
+    float v = (float)((double)angle / (3.1415926535 * 60.0 / 180.0));
+    float uN = u * (float)N, vN = v * (float)N;
+    int u0 = clampi((int)uN), v0 = clampi((int)vN), u1 = clampi((int)uN + 1), v1 = clampi((int)vN + 1);
+    float a00 = lut[u0 + v0 * N], a10 = lut[u1 + v0 * N], a01 = lut[u0 + v1 * N], a11 = lut[u1 + v1 * N];
+    float ax0 = lerp(a00, a10, frac(vN));
+    float ax1 = lerp(a01, a11, frac(vN));
+    *out = lerp(ax0, ax1, frac(uN));
     return MRP_OK;
 }
 

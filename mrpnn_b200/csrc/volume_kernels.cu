@@ -249,8 +249,9 @@ __global__ void k_tr_level(float* __restrict__ out, int res, const float* __rest
 // ---------------------------------------------------------------------------
 // Fill_Hg (core/volume.cu:1322-1400): 512x512 LUT of the HG phase averaged
 // over a cone, 1024 scrambled-Halton samples per texel.  The digit
-// permutations come from the host (seeded Fisher-Yates), the per-texel shift
-// bn from the texel's LUT stream instead of a curand draw.
+// permutations are the reference's (core/volume.cu:1195, from the model
+// file), the per-texel shift bn comes from the texel's LUT stream instead of
+// a curand draw.
 // ---------------------------------------------------------------------------
 __constant__ uint32_t c_perm[28];
 __constant__ uint32_t c_primes[5] = {2, 3, 5, 7, 11};

@@ -11,8 +11,12 @@ script packs both into one little-endian file::
     n_tensors x { u16 name_len, name (ascii), u32 count, f32[count] }
 
 with the stencil directions stored as tensor ``STENCIL_DIRS`` (160 x 3, index
-order of ``SphereRandom3``).  It cross-checks every weight array against the
-``.cuh`` copy before writing.
+order of ``SphereRandom3``) and the digit permutations of the scrambled radical
+inverse that the HG lookup table integrates with (``RadicalInversePermutations_``
+in ``core/volume.cu:1195``, the 2 + 3 + 5 + 7 + 11 = 28 entries of bases 2-11,
+the only bases Fill_Hg uses) as tensor ``HALTON_PERMS`` (28 values).  The LUT
+the network was trained with was built from that table, so it is model data.
+It cross-checks every weight array against the ``.cuh`` copy before writing.
 
 Usage: python make_model.py /path/to/reference [out.bin]
 """
@@ -52,6 +56,23 @@ def parse_stencil(text):
     return np.asarray(dirs, dtype=np.float32)
 
 
+HALTON_BASES = (2, 3, 5, 7, 11)
+
+
+def parse_halton_perms(text):
+    m = re.search(r"RadicalInversePermutations_\[\]\s*=\s*\{([^}]*)\}", text)
+    if not m:
+        raise ValueError("RadicalInversePermutations_ not found")
+    vals = [int(v) for v in m.group(1).replace("\n", "").split(",") if v.strip()]
+    perms = np.asarray(vals[:sum(HALTON_BASES)], dtype=np.float32)
+    off = 0
+    for b in HALTON_BASES:   # each base's block is a permutation of its digits
+        if sorted(perms[off:off + b].astype(int)) != list(range(b)):
+            raise ValueError(f"base {b}: not a permutation")
+        off += b
+    return perms
+
+
 def build(ref_root, out_path):
     weights = np.load(os.path.join(ref_root, "training_pipeline", "NNWeight.npy"),
                       allow_pickle=True).item()
@@ -66,6 +87,8 @@ def build(ref_root, out_path):
         dirs = parse_stencil(f.read())
     tensors = [(k, np.asarray(weights[k], dtype=np.float32).ravel()) for k in sorted(weights)]
     tensors.append(("STENCIL_DIRS", dirs.ravel()))
+    with open(os.path.join(ref_root, "core", "volume.cu")) as f:
+        tensors.append(("HALTON_PERMS", parse_halton_perms(f.read())))
     with open(out_path, "wb") as f:
         f.write(b"MRPNNMD1")
         f.write(struct.pack("<I", len(tensors)))

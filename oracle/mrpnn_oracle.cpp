@@ -763,28 +763,18 @@ void orc_tr_mip_level(const float* mips, int level, float alpha, const float lig
 }
 
 // Scrambled radical inverse (core/volume.cu:1186-1319 restates PBRT's
-// ScrambledRadicalInverse).  The digit permutations are drawn here from a
-// seeded Fisher-Yates shuffle rather than copied; bn is a per-texel hash
-// instead of a curand draw (the reference's draw depends on curand's XORWOW
-// state, which no other generator reproduces).
+// ScrambledRadicalInverse) with the reference's digit permutations for bases
+// 2-11 (RadicalInversePermutations_, core/volume.cu:1195), which the model
+// file carries as HALTON_PERMS; bn is a per-texel Philox draw instead of a
+// curand draw (the reference's draw depends on curand's XORWOW state, which
+// no other generator reproduces).
 namespace {
 const uint32_t kPrimes[5] = {2, 3, 5, 7, 11};
 const uint32_t kPrimeSums[5] = {0, 2, 5, 10, 17};
 uint32_t g_perm[28];
-bool g_perm_ready = false;
-void make_perms() {
-    if (g_perm_ready) return;
-    for (int b = 0; b < 5; ++b) {
-        uint32_t base = kPrimes[b], off = kPrimeSums[b];
-        for (uint32_t i = 0; i < base; ++i) g_perm[off + i] = i;
-        uint32_t h = 0x4D525031u + (uint32_t)b;
-        for (uint32_t i = base - 1; i > 0; --i) {
-            h = pcg(h);
-            uint32_t j = h % (i + 1);
-            std::swap(g_perm[off + i], g_perm[off + j]);
-        }
-    }
-    g_perm_ready = true;
+void make_perms() {   // from the loaded model, before each table build
+    const float* p = T("HALTON_PERMS");
+    for (int i = 0; i < 28; ++i) g_perm[i] = (uint32_t)p[i];
 }
 float scrambled_radical_inverse(uint32_t bi, uint32_t a) {
     const uint32_t base = kPrimes[bi], off = kPrimeSums[bi];

@@ -12,11 +12,10 @@
  * GetMatrixFromNormal, DeterminateNextVertex, CalculateRadiance and Tr) are
  * checked against the reference's own sources compiled on the CPU by the
  * recipe in oracle/ref/ (outputs into oracle/_ref/), and against golden
- * vectors generated from that build (tests/golden/).  The volume pyramid,
- * Fill_TR, Fill_Hg and Fill_BakeTR live in the reference's volume.cu, which
- * does not compile with CUDA 12 (legacy texture references); they are
- * restated here from core/volume.cu line by line and are unpinned beyond
- * the closed-form self-tests in tests/.
+ * vectors generated from that build (tests/golden/).  The volume builders --
+ * the pyramid of Update, Fill_TR, Fill_Hg, GetHGLut and Fill_BakeTR -- are
+ * pinned the same way to core/volume.cu compiled on the CPU by that recipe
+ * (kernel launches rewritten to a host launcher, CUDA arrays as host memory).
  *
  * All float arithmetic is compiled with -ffp-contract=off so that the order
  * of roundings is the one written here; the CUDA kernels use the same order

@@ -67,6 +67,54 @@ def camera(W):
     return ori, (up * t).astype(np.float32), (right * t).astype(np.float32)
 
 
+def smooth_lut():
+    """A smooth 512 x 512 table (rows: cone angle, columns: cos theta) for the
+    GetHGLut pins, rebuilt identically by the tests."""
+    j, i = np.mgrid[0:512, 0:512].astype(np.float32)
+    return (np.float32(1.5) + np.sin(i * np.float32(0.021)) * np.cos(j * np.float32(0.013))).astype(np.float32)
+
+
+def lut_queries(rng, n=256):
+    """(cos, angle) queries for GetHGLut, the table's edges included."""
+    c = rng.uniform(-1.05, 1.05, n).astype(np.float32)
+    a = rng.uniform(-0.05, 1.1, n).astype(np.float32)
+    c[:6] = [-1.0, 1.0, 0.0, -1.0, 1.0, 0.5]
+    a[:6] = [0.0, 0.0, 0.0, 1.0471975, 1.0471975, 0.5]
+    return np.stack([c, a], 1)
+
+
+BAKE_RES = 48
+
+
+def volume_pins(out, rng):
+    """VolumeRender::Update's pyramid, Update_TR (device and host branches),
+    Fill_Hg texels, GetHGLut and Fill_BakeTR voxels from the reference's
+    core/volume.cu compiled on the CPU (oracle/_ref/libmrpnn_ref_volume.so)."""
+    R = SCENE["R"]
+    vol = O.fbm_volume(R, SCENE["seed"], SCENE["freq"])
+    L = light_dir()
+    out["vol_pyramid_digest"] = np.array(digest(O.ref_pyramid(vol, R)))
+    v300 = O.fbm_volume(300, 3, 5.0)
+    out["vol_pyramid300_digest"] = np.array(digest(O.ref_pyramid(v300, 300)))
+    out["vol_tr_digest"] = np.array(digest(O.ref_tr(vol, R, SCENE["alpha"], L, cpu=False)))
+    out["vol_tr_cpu_digest"] = np.array(digest(O.ref_tr(vol, R, SCENE["alpha"], L, cpu=True)))
+    tex = np.sort(rng.choice(512 * 512, 256, replace=False)).astype(np.int32)
+    out["vol_lut_texels"] = tex
+    for tag, g in LUT_GS:
+        out[f"vol_lut_{tag}"] = O.ref_hg_texels(g, SCENE["lut_seed"], tex)
+    q = lut_queries(rng)
+    lut = smooth_lut()
+    out["vol_getlut_q"] = q
+    out["vol_getlut_out"] = np.array([O.ref_get_hg_lut(lut, c, a) for c, a in q], np.float32)
+    md = O.lib().orc_max_density(vol, vol.size)
+    vox = np.sort(rng.choice(BAKE_RES ** 3, 512, replace=False)).astype(np.int64)
+    out["vol_bake_vox"] = vox
+    out["vol_bake_out"] = O.ref_bake_voxels(vol, R, md, SCENE["alpha"], L, BAKE_RES, SCENE["lut_seed"], vox)
+
+
+LUT_GS = (("g0857", 0.857), ("gm05", -0.5), ("g065", 0.65))
+
+
 def main():
     R = O.ref()
     rng = np.random.default_rng(20261203)
@@ -195,6 +243,9 @@ def main():
         R.ref_gather_tile(TW, TW, tori, tup, tright, L, SCENE["alpha"], SCENE["g"], 5, 2, 3, 5, idx, o)
         tiles[idx] = o
     out["tile_out"] = tiles
+
+    # -- volume builders: core/volume.cu's own code on the CPU --------------------
+    volume_pins(out, rng)
 
     np.savez_compressed(OUT, **out)
     print(OUT, os.path.getsize(OUT), "bytes")

@@ -104,8 +104,8 @@ def test_model_file_layout():
             names.append(f.read(ln).decode())
             c = struct.unpack("<I", f.read(4))[0]
             f.seek(4 * c, 1)
-            total += c if names[-1] != "STENCIL_DIRS" else 0
-    assert n == 147 and "STENCIL_DIRS" in names
+            total += c if names[-1] not in ("STENCIL_DIRS", "HALTON_PERMS") else 0
+    assert n == 148 and "STENCIL_DIRS" in names and "HALTON_PERMS" in names
     assert total == 49673
 
 

@@ -170,3 +170,90 @@ def test_gather_tiles(oracle, scene, golden):
     ref = golden["tile_out"]
     np.testing.assert_array_equal(got, ref)
     assert (ref[:, 0] != -1000).sum() > 20     # most tiles see the cloud
+
+
+# ---------------------------------------------------------------------------
+# volume builders, pinned to core/volume.cu compiled on the CPU
+# ---------------------------------------------------------------------------
+from tests.golden.make_golden import BAKE_RES, LUT_GS, digest, lut_queries, smooth_lut  # noqa: E402
+
+
+def test_pyramid_matches_reference(oracle, golden):
+    """VolumeRender::Update's CPU pyramid (core/volume.cu:835-882, 1474-1515),
+    the 32^3 scene and a 300^3 grid (non power of two)."""
+    R = SCENE["R"]
+    vol = oracle.fbm_volume(R, SCENE["seed"], SCENE["freq"])
+    assert digest(oracle.build_pyramid(vol, R)) == str(golden["vol_pyramid_digest"])
+    v300 = oracle.fbm_volume(300, 3, 5.0)
+    assert digest(oracle.build_pyramid(v300, 300)) == str(golden["vol_pyramid300_digest"])
+
+
+def test_tr_levels_match_reference(oracle, golden):
+    """Update_TR: Fill_TR over the mip textures (the device branch) and
+    Sample_TR (the host branch) give the same levels, and the oracle's."""
+    R = SCENE["R"]
+    vol = oracle.fbm_volume(R, SCENE["seed"], SCENE["freq"])
+    tr = oracle.tr_mips(oracle.build_pyramid(vol, R), SCENE["alpha"], light_dir())
+    assert digest(tr) == str(golden["vol_tr_digest"])
+    assert str(golden["vol_tr_cpu_digest"]) == str(golden["vol_tr_digest"])
+
+
+def test_hg_lut_texels_match_reference(oracle, golden):
+    """Fill_Hg (core/volume.cu:1322-1400) with the reference's digit
+    permutations at the same per-texel shift bn: bit for bit."""
+    tex = golden["vol_lut_texels"]
+    for tag, g in LUT_GS:
+        np.testing.assert_array_equal(oracle.hg_lut_texels(g, SCENE["lut_seed"], tex), golden[f"vol_lut_{tag}"])
+
+
+def test_get_hg_lut_matches_reference(golden):
+    """VolumeRender::GetHGLut (core/volume.cu:1424-1442) through the
+    library's host-only mrp_hg_lut_lookup."""
+    import mrpnn_b200 as M
+    lut = smooth_lut()
+    got = np.array([M.hg_lut_lookup(lut, c, a) for c, a in golden["vol_getlut_q"]], np.float32)
+    np.testing.assert_array_equal(got, golden["vol_getlut_out"])
+
+
+def test_baked_tr_matches_reference(oracle, golden):
+    """Fill_BakeTR (core/volume.cu:1562-1587) per voxel, the estimates'
+    streams restarted as the kernel's InitRand does."""
+    R = SCENE["R"]
+    vol = oracle.fbm_volume(R, SCENE["seed"], SCENE["freq"])
+    md = oracle.lib().orc_max_density(vol, vol.size)
+    sc = oracle.SceneBuf(vol, R, md)
+    got = oracle.baked_tr_voxels(sc, SCENE["alpha"], light_dir(), BAKE_RES, SCENE["lut_seed"], golden["vol_bake_vox"])
+    np.testing.assert_array_equal(got, golden["vol_bake_out"])
+
+
+def test_halton_permutations_are_the_references():
+    """The model file carries the first 28 entries of the reference's
+    RadicalInversePermutations_ (bases 2, 3, 5, 7, 11)."""
+    from oracle import oracle as O
+    O.lib()
+    data = C.POINTER(C.c_float)()
+    cnt = C.c_int()
+    assert O.lib().orc_model_tensor(b"HALTON_PERMS", C.byref(data), C.byref(cnt)) == 0
+    perms = np.ctypeslib.as_array(data, (cnt.value,)).astype(int)
+    assert list(perms[:2]) == [0, 1] and sorted(perms[17:28]) == list(range(11))
+    assert list(perms) == [0, 1, 2, 1, 0, 4, 1, 2, 3, 0, 6, 2, 4, 1, 0, 5, 3, 8, 3, 5, 4, 7, 2, 6, 9, 1, 10, 0]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference checker not available")
+def test_live_reference_volume_builders(oracle):
+    """The volume builders re-run live on inputs the golden file does not
+    hold: a 40^3 grid, another light, another g and bake resolution."""
+    R = 40
+    vol = oracle.fbm_volume(R, 9, 3.0)
+    mips = oracle.build_pyramid(vol, R)
+    np.testing.assert_array_equal(mips, oracle.ref_pyramid(vol, R))
+    L = np.array([-0.6, 0.7, 0.38], np.float32)
+    L /= np.float32(np.sqrt(np.float32(np.dot(L, L))))
+    np.testing.assert_array_equal(oracle.tr_mips(mips, 23.0, L), oracle.ref_tr(vol, R, 23.0, L))
+    tex = np.random.default_rng(4).choice(512 * 512, 64, replace=False).astype(np.int32)
+    np.testing.assert_array_equal(oracle.hg_lut_texels(0.3, 11, tex), oracle.ref_hg_texels(0.3, 11, tex))
+    md = oracle.lib().orc_max_density(vol, vol.size)
+    vox = np.random.default_rng(5).choice(32 ** 3, 200, replace=False).astype(np.int64)
+    sc = oracle.SceneBuf(vol, R, md)
+    np.testing.assert_array_equal(oracle.baked_tr_voxels(sc, 23.0, L, 32, 3, vox),
+                                  oracle.ref_bake_voxels(vol, R, md, 23.0, L, 32, 3, vox))
