@@ -410,9 +410,28 @@ void mlp_one(const float* feat, float gamma_f, float g_f, const float sr[3], R o
     }
 }
 
-// SkyBox stand-in: constant environment radiance (core/render.cuh:24-32
-// returns the HDRI texel times enviroment_exp; with no HDRI bound it is 0).
-inline f3 sky(const orc_scene* s) { return load3(s->sky); }
+// SkyBox, core/render.cuh:24-27: the equirect environment map at
+// u = atan2(-z, x) / 2pi + 1/2, v = acos(y) / pi, filtered bilinearly with
+// wrap addressing (u interpolated first, as the reference's own host sampler
+// Image_host::Sample, core/volume.hpp:35-42), times enviroment_exp; with no
+// map bound, the constant environment radiance.
+inline f3 sky(const orc_scene* s, f3 dir) {
+    if (!s->hdri) return load3(s->sky);
+    float u = atan2f(-dir.z, dir.x) * (float)(0.5 / 3.1415926) + 0.5f;
+    float v = acosf(fmaxf(fminf(dir.y, 1.0f), -1.0f)) * (float)(1.0 / 3.1415926);
+    const int W = s->hdri_w, H = s->hdri_h;
+    float px = u * (float)W - 0.5f, py = v * (float)H - 0.5f;
+    int ix = (int)std::floor(px), iy = (int)std::floor(py);
+    float wx = px - (float)ix, wy = py - (float)iy;
+    auto wrap = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
+    auto F = [&](int a, int b) {
+        const float* t = s->hdri + 4 * ((size_t)wrap(b, H) * W + wrap(a, W));
+        return f3{t[0], t[1], t[2]};
+    };
+    auto L = [](f3 a, f3 b, float w) { return f3{lerpf(a.x, b.x, w), lerpf(a.y, b.y, w), lerpf(a.z, b.z, w)}; };
+    f3 c = L(L(F(ix, iy), F(ix + 1, iy), wx), L(F(ix, iy + 1), F(ix + 1, iy + 1), wx), wy);
+    return c * s->env_exp;
+}
 
 // ---------------------------------------------------------------------------
 // DeterminateEstimatedHit(float& alpha, ...), core/render.cuh:105-197
@@ -1004,7 +1023,7 @@ void orc_predict_pixels(const orc_scene* s, const orc_view* v, const int* pixels
             o[0] = res.x; o[1] = res.y; o[2] = res.z;
             o[3] = length(ori - load3(hit));
         } else {
-            f3 sk = sky(s);
+            f3 sk = sky(s, dir);
             o[0] = sk.x; o[1] = sk.y; o[2] = sk.z; o[3] = -1;
         }
         for (int c = 0; c < 4; ++c) rgba_out[4 * q + c] = fmax_(0.0f, o[c]);
@@ -1027,7 +1046,7 @@ static f3 trace_sample(const orc_scene* s, const orc_view* v, f3 ori, f3 dir, fl
         f3 np, nd;
         float md = ray_box_distance(p, rd);
         if (!next_vertex(s, st, v->alpha, v->g, p, rd, md, &np, &nd)) {
-            res = res + sky(s) * csr;
+            res = res + sky(s, rd) * csr;
             break;
         }
         p = np;
@@ -1059,7 +1078,7 @@ void orc_trace_pixels(const orc_scene* s, const orc_view* v, const int* pixels, 
         double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
         float out[4];
         if (dis < 0) {
-            f3 sk = sky(s);
+            f3 sk = sky(s, dir);
             for (int c = 0; c < 3; ++c) { float x = (&sk.x)[c]; acc[c] = (double)x * v->spp; acc2[c] = (double)x * x * v->spp; }
             out[0] = sk.x; out[1] = sk.y; out[2] = sk.z; out[3] = -1;
         } else {
@@ -1097,7 +1116,7 @@ void orc_trace_rays(const orc_scene* s, const orc_view* v, const float* ori_, co
         float dis = ray_box_offset(ori, dir);
         double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
         for (int k = 0; k < v->spp; ++k) {
-            f3 res = sky(s);
+            f3 res = sky(s, dir);
             if (dis >= 0) {
                 Stream st(0, (uint32_t)q, (uint32_t)k, (uint32_t)v->frame, v->seed);
                 Stream nst(3, (uint32_t)q, (uint32_t)k, (uint32_t)v->frame, v->seed);
@@ -1134,7 +1153,7 @@ void orc_get_samples(const orc_scene* s, const float* alpha, const float* ori, c
                 f3 np, nd;
                 float dis = ray_box_distance(pos, rd);
                 if (!next_vertex(s, st, a, gq, pos, rd, dis, &np, &nd)) {
-                    res = res + sky(s) * csr;
+                    res = res + sky(s, rd) * csr;
                     break;
                 }
                 pos = np;
@@ -1250,7 +1269,7 @@ void orc_frame_pt(const orc_scene* s, const orc_view* v, int fnum, int checker, 
         f3 dir = normalize(fwd + (load3(v->right) * (u * 2 - 1)) + (load3(v->up) * (w * 2 - 1)));
         f3 L = normalize(load3(v->light_dir));
         float dis = ray_box_offset(ori, dir);
-        f3 res = sky(s);
+        f3 res = sky(s, dir);
         if (dis >= 0) {
             Stream s0(0, (uint32_t)idx, 0, (uint32_t)v->frame, v->seed);
             Stream nst(3, (uint32_t)idx, 0, (uint32_t)v->frame, v->seed);

@@ -42,7 +42,11 @@ typedef struct orc_scene {
     int baked_res;
     float scatter_rate[3];  /* "scatter_rate" (core/render.cuh:17)              */
     float tr_scale;         /* "tr_scale" (core/render.cuh:16)                  */
-    float sky[3];           /* constant environment radiance (SkyBox stand-in)  */
+    float sky[3];           /* constant environment radiance, used when no map  */
+    const float* hdri;      /* equirect environment map, RGBA float rows of
+                               hdri_w texels (SetHDRI); NULL: constant sky      */
+    int hdri_w, hdri_h;
+    float env_exp;          /* "enviroment_exp" (core/render.cuh:15), scales the map */
 } orc_scene;
 
 /* One camera launch.  Mirrors RenderCamera's arguments (core/volume.cu:199). */

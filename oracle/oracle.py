@@ -31,7 +31,8 @@ class Scene(C.Structure):
     _fields_ = [("density", C.c_void_p), ("res", C.c_int), ("max_density", C.c_float),
                 ("mips", C.c_void_p), ("tr_mips", C.c_void_p), ("hg_lut", C.c_void_p),
                 ("baked_tr", C.c_void_p), ("baked_res", C.c_int),
-                ("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3)]
+                ("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3),
+                ("hdri", C.c_void_p), ("hdri_w", C.c_int), ("hdri_h", C.c_int), ("env_exp", C.c_float)]
 
 
 class View(C.Structure):
@@ -145,7 +146,8 @@ def ref():
             subprocess.run([shutil.which("make") or "make", "-s", "-C", HERE, "ref"] + _make_ref_args(), check=True)
         R = C.CDLL(REF_SO)
         vp = C.c_void_p
-        R.ref_bind_scene.argtypes = [vp, C.c_int, C.c_float, vp, vp, vp, vp, C.c_int, f32p, C.c_float, f32p]
+        R.ref_bind_scene.argtypes = [vp, C.c_int, C.c_float, vp, vp, vp, vp, C.c_int, f32p, C.c_float, f32p,
+                                     vp, C.c_int, C.c_int, C.c_float]
         R.ref_hg.argtypes = [C.c_float, C.c_float]
         R.ref_hg.restype = C.c_float
         R.ref_sample_hg.argtypes = [C.c_float, C.c_float, f32p, C.c_float, f32p]
@@ -323,21 +325,27 @@ class SceneBuf:
     """Host arrays for one scene plus the ctypes struct pointing at them."""
 
     def __init__(self, density, res, max_density, mips=None, tr=None, lut=None, baked=None, baked_res=0,
-                 scatter_rate=(1.001, 1.001, 1.001), tr_scale=1.0, sky=(0.0, 0.0, 0.0)):
+                 scatter_rate=(1.001, 1.001, 1.001), tr_scale=1.0, sky=(0.0, 0.0, 0.0), hdri=None, env_exp=1.0):
+        """hdri: an equirect environment map, float32 [h, w, 4] (RGBA rows),
+        or None for the constant sky."""
         keep = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).ravel()
         self.density, self.mips, self.tr, self.lut, self.baked = map(keep, (density, mips, tr, lut, baked))
         self.res, self.max_density, self.baked_res = res, float(max_density), baked_res
         self.scatter_rate = np.asarray(scatter_rate, np.float32)
         self.tr_scale = float(tr_scale)
         self.sky = np.asarray(sky, np.float32)
+        self.hdri = None if hdri is None else np.ascontiguousarray(hdri, np.float32)
+        hh, hw = (0, 0) if hdri is None else self.hdri.shape[:2]
+        self.env_exp = float(env_exp)
         ptr = lambda a: None if a is None else a.ctypes.data
         self.c = Scene(ptr(self.density), res, self.max_density, ptr(self.mips), ptr(self.tr), ptr(self.lut),
-                       ptr(self.baked), baked_res, F3(*self.scatter_rate), self.tr_scale, F3(*self.sky))
+                       ptr(self.baked), baked_res, F3(*self.scatter_rate), self.tr_scale, F3(*self.sky),
+                       ptr(self.hdri), hw, hh, self.env_exp)
 
     def bind_ref(self):
         ref().ref_bind_scene(self.c.density, self.res, self.max_density, self.c.mips, self.c.tr_mips,
                              self.c.hg_lut, self.c.baked_tr, self.baked_res, self.scatter_rate, self.tr_scale,
-                             self.sky)
+                             self.sky, self.c.hdri, self.c.hdri_w, self.c.hdri_h, self.env_exp)
 
 
 def make_view(width, height, ori, up, right, light_dir, light_color=(1, 1, 1), alpha=64.0, g=0.857,

@@ -37,13 +37,12 @@ extern "C" {
 // 1687-1693).  If baked_tr is given it takes _TR_Mips0, as in PT mode.
 void ref_bind_scene(const float* density, int res, float max_density, const float* mips, const float* tr_mips,
                     const float* lut, const float* baked_tr, int baked_res, const float sr[3], float trs,
-                    const float sky[3]) {
+                    const float sky[3], const float* hdri, int hdri_w, int hdri_h, float env_exp) {
     bind3(_DensityVolume, density, res, false);
     Resolution = res;
     maxDensity = max_density;
     scatter_rate = ld3(sr);
     tr_scale = trs;
-    enviroment_exp = 1.0f;
     texture<float, cudaTextureType3D, cudaReadModeElementType>* m[9] = {&_Mips0, &_Mips1, &_Mips2, &_Mips3, &_Mips4,
                                                                          &_Mips5, &_Mips6, &_Mips7, &_Mips8};
     size_t off = 0;
@@ -62,8 +61,14 @@ void ref_bind_scene(const float* density, int res, float max_density, const floa
     }
     if (baked_tr) bind3(_TR_Mips0, baked_tr, baked_res, true);
     _HGLut.data = lut; _HGLut.nx = 512; _HGLut.ny = 512;
+    // SetHDRI (core/volume.cu:1696-1728) binds the map with wrap addressing
+    // and SetEnvExp sets enviroment_exp; without a map the constant sky
+    // stands in for the (otherwise unbound, zero) environment
     _HDRI.constant = float4{sky[0], sky[1], sky[2], 1.0f};
-    _HDRI.data = nullptr;
+    _HDRI.data = reinterpret_cast<const float4*>(hdri);
+    _HDRI.nx = hdri ? hdri_w : 0;
+    _HDRI.ny = hdri ? hdri_h : 0;
+    enviroment_exp = hdri ? env_exp : 1.0f;
 }
 
 float ref_hg(float c, float g) { return HenyeyGreenstein(c, g); }

@@ -84,6 +84,47 @@ def lut_queries(rng, n=256):
 
 
 BAKE_RES = 48
+HDRI_ENV_EXP = 1.7
+
+
+def smooth_hdri(w=48, h=24):
+    """A smooth synthetic equirect map, float32 [h, w, 4], rebuilt
+    identically by the tests (bright band near the horizon, warm to cold)."""
+    j, i = np.mgrid[0:h, 0:w].astype(np.float32)
+    band = np.exp(-((j - np.float32(h * 0.45)) / np.float32(h * 0.2)) ** 2).astype(np.float32)
+    r = np.float32(0.2) + band * (np.float32(1.0) + np.float32(0.5) * np.sin(i * np.float32(0.26)))
+    g = np.float32(0.3) + np.float32(0.6) * band
+    b = np.float32(0.9) - np.float32(0.5) * band + np.float32(0.05) * np.cos(j * np.float32(0.7))
+    return np.stack([r, g, b, np.ones_like(r)], -1).astype(np.float32)
+
+
+def hdri_pins(out, rng):
+    """NNPredict and CalculateRadiance with an environment map bound
+    (SkyBox, core/render.cuh:24-27): missed pixels and escaping paths."""
+    R = O.ref()
+    sc = build_scene()
+    sc2 = O.SceneBuf(sc.density, sc.res, sc.max_density, sc.mips, sc.tr, sc.lut, baked=sc.baked,
+                     baked_res=sc.baked_res, scatter_rate=SCENE["sr"], sky=SCENE["sky"], hdri=smooth_hdri(),
+                     env_exp=HDRI_ENV_EXP)
+    sc2.bind_ref()
+    L = light_dir()
+    W = 16
+    ori, up, right = camera(W)
+    up, right = (up * np.float32(2.5)).astype(np.float32), (right * np.float32(2.5)).astype(np.float32)
+    px = np.arange(W * W, dtype=np.int32)
+    rgba = np.zeros((W * W, 4), np.float32)
+    R.ref_predict_pixels(W, W, ori, up, right, L, np.ones(3, np.float32), SCENE["alpha"], SCENE["g"], 5, 2, px,
+                         W * W, rgba)
+    out["hdri_pp_rgba"] = rgba
+    cases = [(int(p_), int(k_)) for p_, k_ in zip(rng.integers(0, W * W, 48), rng.integers(0, 8, 48))]
+    tr_out = np.zeros((len(cases), 4), np.float32)
+    for i, (p_, k_) in enumerate(cases):
+        o4 = np.zeros(4, np.float32)
+        R.ref_trace_sample(W, W, ori, up, right, L, np.ones(3, np.float32), SCENE["alpha"], SCENE["g"], 64, 5, 2,
+                           p_, k_, o4)
+        tr_out[i] = o4
+    out["hdri_ts_cases"], out["hdri_ts_out"] = np.asarray(cases, np.int32), tr_out
+    sc.bind_ref()
 
 
 def volume_pins(out, rng):
@@ -243,6 +284,9 @@ def main():
         R.ref_gather_tile(TW, TW, tori, tup, tright, L, SCENE["alpha"], SCENE["g"], 5, 2, 3, 5, idx, o)
         tiles[idx] = o
     out["tile_out"] = tiles
+
+    # -- environment map (SetHDRI / SkyBox) ----------------------------------------
+    hdri_pins(out, rng)
 
     # -- volume builders: core/volume.cu's own code on the CPU --------------------
     volume_pins(out, rng)

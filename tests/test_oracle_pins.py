@@ -257,3 +257,48 @@ def test_live_reference_volume_builders(oracle):
     sc = oracle.SceneBuf(vol, R, md)
     np.testing.assert_array_equal(oracle.baked_tr_voxels(sc, 23.0, L, 32, 3, vox),
                                   oracle.ref_bake_voxels(vol, R, md, 23.0, L, 32, 3, vox))
+
+
+# ---------------------------------------------------------------------------
+# environment map: SetHDRI's equirect texture sampled by SkyBox
+# ---------------------------------------------------------------------------
+from tests.golden.make_golden import HDRI_ENV_EXP, smooth_hdri  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def hdri_scene(oracle, scene):
+    return oracle.SceneBuf(scene.density, scene.res, scene.max_density, scene.mips, scene.tr, scene.lut,
+                           baked=scene.baked, baked_res=scene.baked_res, scatter_rate=SCENE["sr"], sky=SCENE["sky"],
+                           hdri=smooth_hdri(), env_exp=HDRI_ENV_EXP)
+
+
+def _wide_camera(W):
+    ori, up, right = camera(W)
+    return ori, (up * np.float32(2.5)).astype(np.float32), (right * np.float32(2.5)).astype(np.float32)
+
+
+def test_hdri_predict_pixels(oracle, hdri_scene, golden):
+    """NNPredict<MRPNN> returns SkyBox(dir) for the rays that miss the cloud."""
+    W = 16
+    ori, up, right = _wide_camera(W)
+    view = oracle.make_view(W, W, ori, up, right, light_dir(), alpha=SCENE["alpha"], g=SCENE["g"], seed=5, frame=2)
+    rgba = oracle.predict_pixels(hdri_scene, view, np.arange(W * W, dtype=np.int32))
+    np.testing.assert_array_equal(rgba, golden["hdri_pp_rgba"])
+    miss = rgba[:, 3] == 0
+    assert miss.sum() > 100 and (~miss).sum() > 10
+    assert np.ptp(rgba[miss, 0]) > 0.3          # the map varies across the missed pixels
+
+
+def test_hdri_trace_samples(oracle, hdri_scene, golden):
+    """CalculateRadiance: escaping paths add SkyBox(direction) x throughput."""
+    W = 16
+    ori, up, right = _wide_camera(W)
+    for (pix, k), ref in zip(golden["hdri_ts_cases"], golden["hdri_ts_out"]):
+        view = oracle.make_view(W, W, ori, up, right, light_dir(), alpha=SCENE["alpha"], g=SCENE["g"],
+                                multi_scatter=64, spp=int(k) + 1, seed=5, frame=2)
+        _, s, _ = oracle.trace_pixels(hdri_scene, view, np.array([pix], np.int32))
+        if k > 0:
+            view.spp = int(k)
+            _, s0, _ = oracle.trace_pixels(hdri_scene, view, np.array([pix], np.int32))
+            s = s - s0
+        np.testing.assert_array_equal(s[0].astype(np.float32), ref[:3])
