@@ -156,6 +156,28 @@ mrp_status mrp_get_params(const mrp_volume* v, mrp_params* p);
  * in *count when dst is NULL. */
 mrp_status mrp_volume_read(mrp_volume* v, mrp_resource which, int level, float* dst, size_t* count, int dst_is_device);
 
+/* -- environment map: VolumeRender::SetHDRI(path) (core/volume.cu:1696-1728) -- */
+/* Reads a Radiance RGBE .hdr file as the reference's loader does
+ * (core/hdr_loader.h): width x height RGBA floats, rows top to bottom,
+ * (m + 0.5) 2^(e - 136) per channel, alpha 0.  Host only.  rgba == NULL:
+ * only the size is returned. */
+mrp_status mrp_hdri_file_read(const char* path, int* width, int* height, float* rgba, size_t rgba_floats);
+/* Sets the volume's equirect environment map (host RGBA floats, width x
+ * height; NULL clears it: the constant sky of mrp_params.sky returns).
+ * SkyBox then samples it (bilinear, wrap addressing) times env_exp for every
+ * ray that leaves the volume, in the tracer, the predictor's missed pixels,
+ * the batch-ray APIs and the viewer frame; and each predictor launch of
+ * mrp_render / mrp_render_start, each viewer frame and each served request
+ * is lit either by the map (from its Roberts2 direction, with probability
+ * 4 env_exp / (4 env_exp + max light colour)) or by the sun with its colour
+ * divided by 1 - that probability, as the reference's Render does
+ * (core/volume.cu:494-509); the coin is Philox stream (6, 0, 0, frame, seed)
+ * instead of rand().  mrp_render_views keeps the views' own light.  Not
+ * while requests on this volume are in flight in a server. */
+mrp_status mrp_volume_set_hdri(mrp_volume* v, const float* rgba, int width, int height);
+/* mrp_hdri_file_read + mrp_volume_set_hdri. */
+mrp_status mrp_volume_load_hdri(mrp_volume* v, const char* path);
+
 /* VolumeRender::GetHGLut(cos, angle) (core/volume.cu:1424-1442): the HG
  * lookup table (512 x 512, row = cone angle, column = cos theta, as
  * mrp_volume_read(MRP_RES_LUT) returns it) read at (cos, angle) with the

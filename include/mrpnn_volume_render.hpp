@@ -155,7 +155,9 @@ class VolumeRender {
     void SetExposure(float exp) { exposure = exp; }          // interactive tone mapping only
     void SetCheckboard(bool checkboard) { this->checkboard = checkboard; }
     void SetSurfaceIOR(float ior) { this->ior = ior; }       // marching mode only
-    // Constant environment radiance standing in for SetHDRI's map.
+    // core/volume.cu:1696-1728: a Radiance .hdr file as the environment map
+    void SetHDRI(const std::string& path) { mrpnn::check(mrp_volume_load_hdri(h, path.c_str()), "SetHDRI"); }
+    // Constant environment radiance, used while no map is set.
     void SetSky(float3 radiance) {
         params.sky[0] = radiance.x; params.sky[1] = radiance.y; params.sky[2] = radiance.z;
         push();

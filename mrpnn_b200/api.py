@@ -106,6 +106,9 @@ _SIGS = {
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "mrp_hdri_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
+    "mrp_volume_set_hdri": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "mrp_volume_load_hdri": ([C.c_void_p, C.c_char_p], C.c_int),
     "mrp_hg_lut_lookup": ([C.c_void_p, C.c_float, C.c_float, C.POINTER(C.c_float)], C.c_int),
     "mrp_volume_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
     "mrp_volume_file_write_bin": ([C.c_char_p, C.c_void_p, C.c_int], C.c_int),
@@ -239,6 +242,16 @@ def predict_features(feat, gamma, g, scatter_rate, precision=FP32, out=None):
     _ensure_init()
     _check(lib().mrp_predict_features(feat.data_ptr(), gamma.data_ptr(), float(g), _f3(scatter_rate), n,
                                       out.data_ptr(), int(precision), 1))
+    return out
+
+
+def read_hdri(path):
+    """mrp_hdri_file_read: a Radiance .hdr file as float32 [height, width, 4]
+    (RGBA rows top to bottom, alpha 0), as the reference's loader reads it."""
+    w, h = C.c_int(), C.c_int()
+    _check(lib().mrp_hdri_file_read(path.encode(), C.byref(w), C.byref(h), None, 0))
+    out = np.empty((h.value, w.value, 4), np.float32)
+    _check(lib().mrp_hdri_file_read(path.encode(), C.byref(w), C.byref(h), out.ctypes.data, out.size))
     return out
 
 
@@ -450,6 +463,19 @@ class VolumeRender:
     # -- caches -------------------------------------------------------------------
     def UpdateHGLut(self, g):
         _check(lib().mrp_update_hg_lut(self._h, float(g)))
+
+    def SetHDRI(self, path_or_map):
+        """VolumeRender::SetHDRI (core/volume.cu:1696-1728): a .hdr file path,
+        or an equirect map float32 [h, w, 4]; None clears it."""
+        if path_or_map is None:
+            _check(lib().mrp_volume_set_hdri(self._h, None, 0, 0))
+        elif isinstance(path_or_map, str):
+            _check(lib().mrp_volume_load_hdri(self._h, path_or_map.encode()))
+        else:
+            m = _host_f32(path_or_map)
+            if m.ndim != 3 or m.shape[2] != 4:
+                raise ValueError("the environment map is float32 [height, width, 4]")
+            _check(lib().mrp_volume_set_hdri(self._h, m.ctypes.data, m.shape[1], m.shape[0]))
 
     def GetHGLut(self, cos, angle):
         """VolumeRender::GetHGLut (core/volume.cu:1424-1442) on the volume's

@@ -307,6 +307,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     mrp::dev_free(v->density); mrp::dev_free(v->density_h); mrp::dev_free(v->mips); mrp::dev_free(v->trs); mrp::dev_free(v->lut); mrp::dev_free(v->baked);
     mrp::dev_free(v->occ); mrp::dev_free(v->mip_occ); mrp::dev_free(v->d_maxbits); mrp::dev_free(v->d_bounds); mrp::dev_free(v->mips_pad); mrp::dev_free(v->trs_pad); mrp::dev_free(v->mip_tr); mrp::dev_free(v->pad_pair); mrp::dev_free(v->accum); mrp::dev_free(v->sum3); mrp::dev_free(v->first_pos);
     mrp::dev_free(v->counter);
+    mrp::dev_free(v->hdri);
     mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     tc_free_scratch(v->tc);
     free_multiview(v);
@@ -807,9 +808,12 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     }
     // caches first (the reference updates them inside its launch loop,
     // core/volume.cu:511-518; they do not change between its launches)
+    // with an environment map each predictor launch picks its light from the
+    // map or the sun (core/volume.cu:494-509) and updates the TR levels for it
+    const bool env_light = type == MRP_MRPNN && v->hdri;
     if (type == MRP_MRPNN) {
         TRY(update_lut_async(v, w->g));
-        TRY(update_tr_async(v, w->light_dir, w->alpha));
+        if (!env_light) TRY(update_tr_async(v, w->light_dir, w->alpha));
     } else if (v->params.nee_mode == 0) {
         TRY(update_baked_async(v, w->light_dir, w->alpha));
     }
@@ -831,7 +835,12 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
     if (tc_net && !(async && v->async_tc)) CU(cudaMemsetAsync(v->tc.d + 1, 0, sizeof(int), v->stream));
     CU(cudaEventRecord(v->ev0, v->stream));
     for (int i = 0; i < sample_num; ++i) {
-        ViewDev vd = make_view(v, w, w->frame_offset + i, i);
+        mrp_view wi = *w;
+        if (env_light) {
+            env_light_for_launch(v, (uint32_t)(w->frame_offset + i), w->seed, wi.light_dir, wi.light_color);
+            TRY(update_tr_async(v, wi.light_dir, wi.alpha));
+        }
+        ViewDev vd = make_view(v, &wi, w->frame_offset + i, i);
         vd.counters = counters;
         bool last = i == sample_num - 1;
         if (type == MRP_MRPNN) {

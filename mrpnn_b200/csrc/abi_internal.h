@@ -148,6 +148,11 @@ struct mrp_volume {
     float* rec_f = nullptr;
     float* feat = nullptr;
     size_t rec_cap = 0;
+    // environment map of SetHDRI (RGBA float rows), device and host copies
+    float4* hdri = nullptr;
+    int hdri_w = 0, hdri_h = 0;
+    std::vector<float> hdri_host;
+    int hdri_light_n = 0;   // Roberts2 index of the map's light direction (the reference's rand_cpu)
     // tensor-core predictor scratch
     TcScratch tc;
     // mrp_render_views
@@ -179,6 +184,10 @@ struct mrp_volume {
         d.mip_tr = has_tr ? mip_tr : nullptr;
         d.pad_pair = has_tr && has_pyramid ? pad_pair : nullptr;
         d.lut_dirs = has_lut ? lut + mrp::kLut * mrp::kLut : nullptr;
+        d.hdri = hdri;
+        d.hdri_w = hdri_w;
+        d.hdri_h = hdri_h;
+        d.env_exp = params.env_exp;
         d.has_bounds = has_bounds ? 1 : 0;
         if (has_bounds) {
             // Density() at p reads base voxel floor((p + 0.5) R - 0.5) and the
@@ -194,3 +203,15 @@ struct mrp_volume {
     }
 };
 
+namespace mrpi {
+// The light of predictor launch `frame` when the volume has an environment
+// map (core/volume.cu:494-509): L and C (light direction and colour) are
+// replaced in place.  The launch's coin is the first uniform of Philox
+// stream (kEnvLightStream, 0, 0, frame, seed) -- the reference calls rand().
+void hdri_light(const mrp_volume* v, float coin, int n, float L[3], float C[3]);
+inline void env_light_for_launch(const mrp_volume* v, uint32_t frame, uint32_t seed, float L[3], float C[3]) {
+    uint32_t blk[4];
+    mrp::philox(0, 0, frame, mrp::kEnvLightStream, 0u, seed ^ (mrp::kEnvLightStream * 0x9E3779B9u), blk);
+    hdri_light(v, mrp::u01(blk[0]), v->hdri_light_n, L, C);
+}
+}  // namespace mrpi

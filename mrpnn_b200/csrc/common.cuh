@@ -127,7 +127,7 @@ MRP_HD void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t 
 MRP_HD float u01(uint32_t x) { return (float)(((x >> 9) << 1) | 1u) * 5.9604644775390625e-8f; }
 
 enum StreamKind : uint32_t { kPixelStream = 0, kLutStream = 1, kBakeStream = 2, kNeeStream = 3, kSampleStream = 4,
-                             kTrStream = 5 };
+                             kTrStream = 5, kEnvLightStream = 6 };
 
 struct Stream {
     uint32_t k0, k1, sub, frame, kind, n;
@@ -421,7 +421,37 @@ struct VolumeDev {
     // first LUT factor of X_Hg, which depends only on the point and g), or
     // null; stored right after the LUT (kLutAlloc floats per LUT buffer).
     const float* lut_dirs;
+    // Equirect environment map of SetHDRI (RGBA rows of hdri_w texels), or
+    // null for the constant sky; env_exp scales it (enviroment_exp).
+    const float4* hdri;
+    int hdri_w, hdri_h;
+    float env_exp;
 };
+
+// SkyBox (core/render.cuh:24-27): the environment map at u = atan2(-z, x) /
+// 2pi + 1/2, v = acos(y) / pi, bilinear with wrap addressing (u interpolated
+// first, the order of the reference's host sampler Image_host::Sample,
+// core/volume.hpp:35-42), times enviroment_exp; the constant sky when no
+// map is set.  Software filtering with fp32 weights (the reference's texture
+// unit quantises the weights to 1/256).
+MRP_D f3 sky_radiance(const VolumeDev& v, f3 dir) {
+    if (!v.hdri) return v.sky;
+    const float u = fa(fm(atan2f(-dir.z, dir.x), (float)(0.5 / 3.1415926)), 0.5f);
+    const float t = fm(acosf(fmaxf(fminf(dir.y, 1.0f), -1.0f)), (float)(1.0 / 3.1415926));
+    const int W = v.hdri_w, H = v.hdri_h;
+    const float px = fs(fm(u, (float)W), 0.5f), py = fs(fm(t, (float)H), 0.5f);
+    const float fx = floorf(px), fy = floorf(py);
+    const float wx = fs(px, fx), wy = fs(py, fy);
+    int x0 = (int)fx % W, y0 = (int)fy % H;
+    x0 += x0 < 0 ? W : 0;
+    y0 += y0 < 0 ? H : 0;
+    const int x1 = x0 + 1 == W ? 0 : x0 + 1, y1 = y0 + 1 == H ? 0 : y0 + 1;
+    const float4 a = __ldg(v.hdri + (size_t)y0 * W + x0), b = __ldg(v.hdri + (size_t)y0 * W + x1);
+    const float4 c = __ldg(v.hdri + (size_t)y1 * W + x0), d = __ldg(v.hdri + (size_t)y1 * W + x1);
+    const f3 r = mk3(lerp(lerp(a.x, b.x, wx), lerp(c.x, d.x, wx), wy), lerp(lerp(a.y, b.y, wx), lerp(c.y, d.y, wx), wy),
+                     lerp(lerp(a.z, b.z, wx), lerp(c.z, d.z, wx), wy));
+    return mk3(fm(r.x, v.env_exp), fm(r.y, v.env_exp), fm(r.z, v.env_exp));
+}
 // A level of edge n (n <= 8) stored with one texel of margin below and two
 // above per axis, (n + 3)^3 floats, texel (x, y, z) at ((x + 1) P + y + 1) P
 // + z + 1 (P = n + 3).  The margin holds what the fetch reads outside the

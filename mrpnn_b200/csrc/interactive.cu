@@ -105,7 +105,7 @@ __global__ void k_frame_pt(VolumeDev v, ViewDev w, int fnum, float* __restrict__
     f3 dir = camera_ray_dir(w, row, col);
     f3 L = normalize(w.light_dir);
     float dis = ray_box_offset(w.ori, dir);
-    f3 res = dis < 0 ? v.sky : trace_sample(v, w, idx, 0, w.ori, dir, dis, L, nullptr);
+    f3 res = dis < 0 ? sky_radiance(v, dir) : trace_sample(v, w, idx, 0, w.ori, dir, dis, L, nullptr);
     res = mk3(fmaxf(0.0f, res.x), fmaxf(0.0f, res.y), fmaxf(0.0f, res.z));
     mrp_histogram h = histo[idx];
     if (fnum == 0) h = mrp_histogram{};
@@ -198,6 +198,13 @@ mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_rende
     if (v->async_inflight) TRY(mrp_render_wait(v, 0));   // started renders may still read accum
     const int W = view->width, H = view->height, npix = W * H;
     const int fnum = checkerboard ? frame_num / 2 : frame_num;
+    // the viewer's predictor frame with an environment map lights it from the
+    // map or the sun (core/volume.cu:552-567); the map's direction index
+    // advances every frame (rand_cpu++, core/volume.cu:579)
+    mrp_view vw = *view;
+    if (type == MRP_MRPNN && v->hdri)
+        env_light_for_launch(v, (uint32_t)view->frame_offset, view->seed, vw.light_dir, vw.light_color);
+    view = &vw;
     ViewDev vd = make_view(v, view, view->frame_offset, 0);
     vd.cam_mode = 1;
     vd.checker = checkerboard ? 1 : 0;
@@ -243,6 +250,7 @@ mrp_status mrp_render_interactive(mrp_volume* v, const mrp_view* view, mrp_rende
         return MRP_OK;
     };
     st = run();
+    ++v->hdri_light_n;
     if (tmp) mrp::dev_free_async(tmp, v->stream);
     if (st != MRP_OK) return st;
     if (predict && v->params.precision != MRP_FP32) {

@@ -820,7 +820,10 @@ __global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w,
         f3 LY, LZ;
         basis(dir, 0.1f, st, &X, &Y, &Z);
         basis(L, 0.1f, st, &LX, &LY, &LZ);
-        if (!active) running_mean(accum, pix, w.mean_k, make_float4(v.sky.x, v.sky.y, v.sky.z, -1.0f));
+        if (!active) {   // NNPredict returns SkyBox(dir) for a ray that finds no hit
+            const f3 sk = sky_radiance(v, dir);
+            running_mean(accum, pix, w.mean_k, make_float4(sk.x, sk.y, sk.z, -1.0f));
+        }
     }
     // warp-aggregated append of the hit pixels
     unsigned lane = threadIdx.x & 31;

@@ -209,7 +209,10 @@ bool mrp_server::admit() {
         if (pick < 0) break;
         Slot& s = slots[pick];
         mrp_volume* v = T->req.volume;
-        const mrp_view& w = T->req.view;
+        // with an environment map the request's light is the map's or the
+        // sun's, picked as mrp_render picks it for its launch
+        mrp_view w = T->req.view;
+        if (v->hdri) env_light_for_launch(v, (uint32_t)w.frame_offset, w.seed, w.light_dir, w.light_color);
         bool need_lut = true;
         for (const Lut& l : luts)
             if (l.g == w.g && l.seed == v->params.seed) need_lut = false;

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
                     }
                     float dis = ray_box_offset(ori, dir);
                     if (dis < 0) {
-                        deposit(sum3, sumsq3, first_pos, pix, k, v.sky, false);   // SkyBox(dir), coverage stays 0
+                        deposit(sum3, sumsq3, first_pos, pix, k, sky_radiance(v, dir), false);   // SkyBox(dir), coverage stays 0
                     } else {
                         if (COUNT) tally.events++;
                         if (w.multi_scatter < 1) {
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
             // against IEEE log and division; decisions stay per sample
             t = t - __fdividef(__logf(1.0f - rk), smax);
             if (t > md) {   // left the box: sky radiance, the sample ends
-                res = add(res, mul(v.sky, csr));
+                res = add(res, mul(sky_radiance(v, rd), csr));
                 deposit(sum3, sumsq3, first_pos, pix, k, res, true);
                 live = false;
                 continue;
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(128) k_get_samples(VolumeDev v, SampleTasks T,
             f3 np, nd;
             float dis = ray_box_distance(pos, rd);
             if (!next_vertex(v, st, a, gq, pos, rd, dis, &np, &nd, nullptr)) {
-                res = add(res, mul(v.sky, csr));
+                res = add(res, mul(sky_radiance(v, rd), csr));
                 break;
             }
             pos = np;

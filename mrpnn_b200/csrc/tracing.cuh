@@ -50,7 +50,7 @@ MRP_D f3 trace_sample(const VolumeDev& v, const ViewDev& w, int pix, int k, f3 o
         float md = ray_box_distance(p, rd);
         if (tl) tl->steps++;
         if (!next_vertex(v, st, w.alpha, w.g, p, rd, md, &np, &nd, tl)) {
-            res = add(res, mul(v.sky, csr));
+            res = add(res, mul(sky_radiance(v, rd), csr));
             break;
         }
         p = np;

@@ -1577,4 +1577,53 @@ void orc_gather_tiles(const orc_scene* s, const orc_view* v, int px, int py, flo
         if (idx == 0) ob[0] *= 1.00001f;
     }
 }
+
+// Roberts2, core/vector.cu:179-183: frac(a * n + 0.5) with a = (1/g, 1/g^2, 0)
+void orc_roberts2(int n, float out[3]) {
+    const float g = 1.32471795724474602596f;
+    const float a[3] = {1.0f / g, 1.0f / (g * g), 0.0f};
+    for (int c = 0; c < 3; ++c) out[c] = fracf(a[c] * (float)n + 0.5f);
+}
+// UniformSampleSphere, core/vector.cu:195-205
+void orc_uniform_sample_sphere(float ex, float ey, float out[3]) {
+    float phi = 2 * 3.14159265359f * ex;
+    float ct = 1 - 2 * ey;
+    float st = std::sqrt(1 - ct * ct);
+    out[0] = st * std::cos(phi);
+    out[1] = st * std::sin(phi);
+    out[2] = ct;
+}
+// Image_host::Sample, core/volume.hpp:24-42: bilinear, x first, clamped texels
+void orc_image_sample(const float* rgba, int sx, int sy, float u, float v, float out[3]) {
+    float px = u * (float)sx - 0.5f, py = v * (float)sy - 0.5f;
+    int x = (int)std::floor(px), y = (int)std::floor(py);
+    float wx = px - (float)x, wy = py - (float)y;
+    auto S = [&](int a, int b, int c) {
+        a = a < 0 ? 0 : (a > sx - 1 ? sx - 1 : a);
+        b = b < 0 ? 0 : (b > sy - 1 ? sy - 1 : b);
+        return rgba[4 * ((size_t)b * sx + a) + c];
+    };
+    for (int c = 0; c < 3; ++c)
+        out[c] = lerpf(lerpf(S(x, y, c), S(x + 1, y, c), wx), lerpf(S(x, y + 1, c), S(x + 1, y + 1, c), wx), wy);
+}
+// VolumeRender::Render's light choice with an environment map,
+// core/volume.cu:494-509 (the coin replaces rand() / RAND_MAX)
+void orc_env_light(const orc_scene* s, float coin, int n, float L[3], float C[3]) {
+    const float e = s->env_exp;
+    const float rate = e * 4 / (e * 4 + fmax_(C[0], fmax_(C[1], C[2])));
+    if (!(coin < rate)) {
+        for (int c = 0; c < 3; ++c) C[c] = C[c] / (1 - rate);
+        return;
+    }
+    float r[3], d[3], col[3];
+    orc_roberts2(n, r);
+    orc_uniform_sample_sphere(r[0], r[1], d);
+    float u = atan2f(-d[2], d[0]) * (float)(0.5 / 3.1415926) + 0.5f;
+    float v = acosf(fmaxf(fminf(d[1], 1.0f), -1.0f)) * (float)(1.0 / 3.1415926);
+    orc_image_sample(s->hdri, s->hdri_w, s->hdri_h, u, v, col);
+    for (int c = 0; c < 3; ++c) {
+        L[c] = d[c];
+        C[c] = col[c] * e * 4 / rate;
+    }
+}
 }  // extern "C"

@@ -151,6 +151,15 @@ void orc_gather_tiles(const orc_scene* s, const orc_view* v, int px, int py, flo
 /* GetTrs: ShadowTerm_TRs per task; out [n][3]. */
 void orc_get_trs(const orc_scene* s, float alpha, const float* ori, const float* dir, int n, const float L[3],
                  const float lc[3], float g, int spp, uint32_t seed, float* out3);
+/* The light of one predictor launch with an environment map
+ * (core/volume.cu:494-509): L, C replaced in place; coin in [0, 1) stands in
+ * for rand() / RAND_MAX, n is the Roberts2 index (rand_cpu).  The pieces
+ * Roberts2 (core/vector.cu:179-183), UniformSampleSphere (:195-205) and
+ * Image_host::Sample (core/volume.hpp:24-42) are exported for the pins. */
+void orc_env_light(const orc_scene* s, float coin, int n, float L[3], float C[3]);
+void orc_roberts2(int n, float out[3]);
+void orc_uniform_sample_sphere(float ex, float ey, float out[3]);
+void orc_image_sample(const float* rgba, int sx, int sy, float u, float v, float out[3]);
 
 #ifdef __cplusplus
 }

@@ -110,6 +110,10 @@ def lib():
                                                                                C.c_uint32, C.c_void_p]
         L.orc_get_trs.argtypes = [C.POINTER(Scene), C.c_float, C.c_void_p, C.c_void_p, C.c_int, F3, F3, C.c_float,
                                   C.c_int, C.c_uint32, C.c_void_p]
+        L.orc_env_light.argtypes = [C.POINTER(Scene), C.c_float, C.c_int, f32p, f32p]
+        L.orc_roberts2.argtypes = [C.c_int, f32p]
+        L.orc_uniform_sample_sphere.argtypes = [C.c_float, C.c_float, f32p]
+        L.orc_image_sample.argtypes = [f32p, C.c_int, C.c_int, C.c_float, C.c_float, f32p]
         rc = L.orc_load_model(MODEL.encode())
         if rc != 0:
             raise RuntimeError(f"oracle: cannot load model file {MODEL} (rc={rc})")
@@ -195,6 +199,9 @@ def ref_volume():
         R.ref_vol_bake_voxels.argtypes = [f32p, C.c_int, C.c_float, C.c_float, f32p, C.c_int, C.c_uint32, i64p,
                                           C.c_int, f32p]
         R.ref_vol_load_hdr.argtypes = [C.c_char_p, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p, C.c_size_t]
+        R.ref_vol_roberts2.argtypes = [C.c_int, f32p]
+        R.ref_vol_uniform_sample_sphere.argtypes = [C.c_float, C.c_float, f32p]
+        R.ref_vol_image_sample.argtypes = [f32p, C.c_int, C.c_int, C.c_float, C.c_float, f32p]
         _ref_vol = R
     return _ref_vol
 
@@ -239,6 +246,17 @@ def ref_load_hdr(path):
     out = np.empty((ry.value, rx.value, 4), np.float32)
     ref_volume().ref_vol_load_hdr(path.encode(), C.byref(rx), C.byref(ry), out.ctypes.data, out.size)
     return out
+
+
+def env_light(scene, frame, seed, light_dir, light_color, n=0):
+    """The light of predictor launch `frame` with the scene's environment
+    map: the coin is the first uniform of Philox stream (6, 0, 0, frame,
+    seed), as the library draws it.  Returns (L, C)."""
+    L = np.array(light_dir, np.float32)
+    Cc = np.array(light_color, np.float32)
+    coin = lib().orc_stream_uniform(6, 0, 0, frame, seed, 0)
+    lib().orc_env_light(C.byref(scene.c), coin, n, L, Cc)
+    return L, Cc
 
 
 def baked_tr_voxels(scene, alpha, light_dir, bake_res, seed, voxels, replicate=True):

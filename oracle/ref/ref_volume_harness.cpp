@@ -242,4 +242,25 @@ int ref_vol_load_hdr(const char* path, unsigned* rx, unsigned* ry, float* out, s
     return 0;
 }
 
+// The pieces of Render's light choice with an environment map
+// (core/volume.cu:494-509): Roberts2, UniformSampleSphere and
+// Image_host::Sample.
+void ref_vol_roberts2(int n, float out[3]) {
+    float3 r = Roberts2(n);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+void ref_vol_uniform_sample_sphere(float ex, float ey, float out[3]) {
+    float3 d = UniformSampleSphere(float2{ex, ey});
+    out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+void ref_vol_image_sample(const float* rgba, int sx, int sy, float u, float v, float out[3]) {
+    Image_host img;
+    img.data = reinterpret_cast<float4*>(const_cast<float*>(rgba));
+    img.sx = sx;
+    img.sy = sy;
+    float3 c = img.Sample(float2{u, v});
+    img.data = nullptr;
+    out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+
 }  // extern "C"

@@ -302,3 +302,26 @@ def test_hdri_trace_samples(oracle, hdri_scene, golden):
             _, s0, _ = oracle.trace_pixels(hdri_scene, view, np.array([pix], np.int32))
             s = s - s0
         np.testing.assert_array_equal(s[0].astype(np.float32), ref[:3])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference checker not available")
+def test_env_light_pieces_match_reference(oracle):
+    """Render's light choice with a map (core/volume.cu:494-509) is built from
+    Roberts2, UniformSampleSphere and Image_host::Sample: each bit for bit."""
+    L = oracle.lib()
+    a, b = np.zeros(3, np.float32), np.zeros(3, np.float32)
+    for n in (0, 1, 2, 7, 100, 12345):
+        L.orc_roberts2(n, a)
+        oracle.ref_volume().ref_vol_roberts2(n, b)
+        np.testing.assert_array_equal(a, b)
+    rng = np.random.default_rng(8)
+    for ex, ey in rng.uniform(0, 1, (64, 2)).astype(np.float32):
+        L.orc_uniform_sample_sphere(ex, ey, a)
+        oracle.ref_volume().ref_vol_uniform_sample_sphere(ex, ey, b)
+        np.testing.assert_array_equal(a, b)
+    m = smooth_hdri()
+    flat = np.ascontiguousarray(m).ravel()
+    for u, v in rng.uniform(-0.05, 1.05, (64, 2)).astype(np.float32):
+        L.orc_image_sample(flat, m.shape[1], m.shape[0], u, v, a)
+        oracle.ref_volume().ref_vol_image_sample(flat, m.shape[1], m.shape[0], u, v, b)
+        np.testing.assert_array_equal(a, b)
