@@ -417,6 +417,17 @@ def run_serving(args, local):
             pix += reqs[i][1].width * reqs[i][1].height
         th.join()
         st = srv.stats()
+        # a burst: 64 requests submitted at once (the same views), to show the
+        # batched network at load; the Poisson stream above rarely has two
+        # requests' features ready while the network is idle
+        b0 = srv.stats()
+        tb = time.perf_counter()
+        burst = [srv.submit(vols[vi][0], view, pool[i % len(pool)][:view.width * view.height * 4])
+                 for i, (vi, view) in enumerate(reqs[:len(pool)])]
+        bpix = sum(view.width * view.height for _, view in reqs[:len(pool)])
+        blat = [srv.wait(t)[1] for t in burst]
+        burst_s = time.perf_counter() - tb
+        b1 = srv.stats()
     finally:
         srv.close()
     span_s = (last_done - first_submit) / 1000.0
@@ -433,7 +444,13 @@ def run_serving(args, local):
             "median_split_ms": {"queue": float(pm[0]), "tr+hit+gather": float(pm[1]), "network": float(pm[2]),
                                 "result copy": float(pm[3])},
             "batches": st["batches"], "mean_batch": st["batched_requests"] / max(1, st["batches"]),
-            "max_batch": st["max_batch"], "peak_bytes": st["peak_bytes"]}
+            "max_batch": st["max_batch"], "peak_bytes": st["peak_bytes"],
+            "burst": {"requests": len(burst), "seconds": burst_s, "req_s": len(burst) / burst_s,
+                      "frames_per_s_1024eq": bpix / (1024 * 1024) / burst_s,
+                      "p50_ms": float(np.percentile([t["done_ms"] - t["submit_ms"] for t in blat], 50)),
+                      "batches": b1["batches"] - b0["batches"],
+                      "mean_batch": (b1["batched_requests"] - b0["batched_requests"]) /
+                                    max(1, b1["batches"] - b0["batches"])}}
 
 
 def lum_rmse_x100(a, b):

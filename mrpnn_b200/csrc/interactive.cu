@@ -102,7 +102,7 @@ __global__ void k_frame_pt(VolumeDev v, ViewDev w, int fnum, float* __restrict__
     if (idx >= w.width * w.height) return;
     int row = idx / w.width, col = idx % w.width;
     if (!pixel_selected(w, row, col)) return;
-    f3 dir = camera_ray_dir(w, row, col);
+    f3 dir = normalize(camera_ray_dir(w, row, col));   // CalculateRadiance normalizes again (core/render.cuh:540)
     f3 L = normalize(w.light_dir);
     float dis = ray_box_offset(w.ori, dir);
     f3 res = dis < 0 ? sky_radiance(v, dir) : trace_sample(v, w, idx, 0, w.ori, dir, dis, L, nullptr);

@@ -1267,6 +1267,7 @@ void orc_frame_pt(const orc_scene* s, const orc_view* v, int fnum, int checker, 
         f3 ori = load3(v->ori);
         f3 fwd = normalize(neg(ori));
         f3 dir = normalize(fwd + (load3(v->right) * (u * 2 - 1)) + (load3(v->up) * (w * 2 - 1)));
+        dir = normalize(dir);   // CalculateRadiance normalizes its direction again (core/render.cuh:540)
         f3 L = normalize(load3(v->light_dir));
         float dis = ray_box_offset(ori, dir);
         f3 res = sky(s, dir);

@@ -199,6 +199,10 @@ def ref_volume():
         R.ref_vol_bake_voxels.argtypes = [f32p, C.c_int, C.c_float, C.c_float, f32p, C.c_int, C.c_uint32, i64p,
                                           C.c_int, f32p]
         R.ref_vol_load_hdr.argtypes = [C.c_char_p, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p, C.c_size_t]
+        R.ref_vol_frame_pt.argtypes = [f32p, C.c_int, C.c_float, f32p, C.c_int, f32p, f32p, C.c_int, C.c_int] + \
+            [f32p] * 5 + [C.c_float, C.c_float, C.c_int, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, f32p, f32p]
+        R.ref_vol_frame_finish.argtypes = [f32p, f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_float, C.c_int, np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")]
         R.ref_vol_roberts2.argtypes = [C.c_int, f32p]
         R.ref_vol_uniform_sample_sphere.argtypes = [C.c_float, C.c_float, f32p]
         R.ref_vol_image_sample.argtypes = [f32p, C.c_int, C.c_int, C.c_float, C.c_float, f32p]

@@ -242,6 +242,78 @@ int ref_vol_load_hdr(const char* path, unsigned* rx, unsigned* ry, float* out, s
     return 0;
 }
 
+// The viewer's PT frame (RenderCamera<false> with the histogram buffer,
+// core/volume.cu:57-150) over a scene bound as Update / Update_CachedTR bind
+// it: density (border), the baked NEE grid as _TR_Mips0 (clamp), majorant,
+// albedo, constant sky.  Pixel (row i, column j) runs as the kernel's thread
+// (i, column slot) with its random numbers from Philox stream (0, i W + j, 0,
+// frame, seed); frame_num is the kernel's frameNum (its running-mean count).
+void ref_vol_frame_pt(const float* density, int R, float max_density, const float* baked, int baked_res,
+                      const float sr[3], const float sky[3], int W, int H, const float ori[3], const float up[3],
+                      const float right[3], const float L[3], const float lc[3], float alpha, float g, int multi,
+                      uint32_t seed, int frame, int frame_num, int checker, int flip_, float* target, float* histo) {
+    _DensityVolume.data = density;
+    _DensityVolume.nx = _DensityVolume.ny = _DensityVolume.nz = R;
+    _DensityVolume.addressMode[0] = _DensityVolume.addressMode[1] = _DensityVolume.addressMode[2] =
+        cudaAddressModeBorder;
+    _TR_Mips0.data = baked;
+    _TR_Mips0.nx = _TR_Mips0.ny = _TR_Mips0.nz = baked_res;
+    _TR_Mips0.addressMode[0] = _TR_Mips0.addressMode[1] = _TR_Mips0.addressMode[2] = cudaAddressModeClamp;
+    Resolution = R;
+    maxDensity = max_density;
+    scatter_rate = float3{sr[0], sr[1], sr[2]};
+    tr_scale = 1.0f;
+    enviroment_exp = 1.0f;
+    _HDRI.data = nullptr;
+    _HDRI.constant = float4{sky[0], sky[1], sky[2], 1.0f};
+    dev_checkboard = checker;
+    flip = flip_;
+    frameNum = frame_num;
+    const int cols = checker ? (W + 1) / 2 : W;
+    std::vector<std::thread> pool;
+    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+    for (unsigned t = 0; t < nt; ++t) {
+        pool.emplace_back([&, t] {
+            blockDim = dim3(1, 1, 1);
+            threadIdx = uint3{0, 0, 0};
+            for (int q = (int)t; q < H * cols; q += (int)nt) {
+                int i = q / cols, jj = q % cols;
+                int j = checker ? jj * 2 + ((i + flip_) % 2) : jj;
+                if (j >= W) continue;
+                blockIdx = uint3{(unsigned)i, (unsigned)jj, 0};
+                ref_set_stream(0, (uint32_t)(i * W + j), 0, (uint32_t)frame, seed);
+                RenderCamera<false>(reinterpret_cast<float3*>(target), reinterpret_cast<Histogram*>(histo),
+                                    int2{W, H}, float3{ori[0], ori[1], ori[2]}, float3{up[0], up[1], up[2]},
+                                    float3{right[0], right[1], right[2]}, float3{L[0], L[1], L[2]},
+                                    float3{lc[0], lc[1], lc[2]}, alpha, multi, g);
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+    _DensityVolume.data = nullptr;
+    _TR_Mips0.data = nullptr;
+}
+
+// The viewer's finishing pass: Denoise<denoise> for a PT frame or
+// ReprojectionDenoise for a predictor frame (core/volume.cu:285-372, the
+// tone maps of core/ACES.cuh), RGBA8 into rgba8.
+void ref_vol_frame_finish(float* target, float* histo, int W, int H, int frame_num, int flip_, int predict, int denoise,
+                          float exposure_, int tone, uint32_t* rgba8) {
+    frameNum = frame_num;
+    flip = flip_;
+    exposure = exposure_;
+    blockDim = dim3(1, 1, 1);
+    threadIdx = uint3{0, 0, 0};
+    for (int id = 0; id < W * H; ++id) {
+        blockIdx = uint3{(unsigned)id, 0, 0};
+        float3* T = reinterpret_cast<float3*>(target);
+        Histogram* Hs = reinterpret_cast<Histogram*>(histo);
+        if (predict) ReprojectionDenoise(T, Hs, rgba8, int2{W, H}, tone);
+        else if (denoise) Denoise<true>(T, Hs, rgba8, int2{W, H}, tone);
+        else Denoise<false>(T, Hs, rgba8, int2{W, H}, tone);
+    }
+}
+
 // The pieces of Render's light choice with an environment map
 // (core/volume.cu:494-509): Roberts2, UniformSampleSphere and
 // Image_host::Sample.

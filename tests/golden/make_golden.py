@@ -155,6 +155,37 @@ def volume_pins(out, rng):
 
 LUT_GS = (("g0857", 0.857), ("gm05", -0.5), ("g065", 0.65))
 
+VIEWER = dict(W=24, H=24, multi=32, seed=5, frame=2, exposure=1.3)
+FINISH_MODES = ((0, 0, 2), (0, 1, 1), (1, 0, 2), (0, 1, 0))   # (predict, denoise, tone)
+
+
+def viewer_pins(out, rng):
+    """The viewer frame: RenderCamera<false> with the histogram buffer over
+    two frames (checkerboard, flip 1; square: the reference bounds pixels by
+    the opposite edges, core/volume.cu:102), then the finishing pass in each mode
+    (Denoise / ReprojectionDenoise, Gamma / ACES / none, RGBA8), from
+    core/volume.cu compiled on the CPU."""
+    sc = build_scene()
+    V = VIEWER
+    W, H = V["W"], V["H"]
+    ori, up, right = camera(W)
+    L = light_dir()
+    tgt = rng.uniform(0, 1, W * H * 3).astype(np.float32)
+    his = rng.uniform(0, 2, W * H * 33).astype(np.float32)
+    out["vw_target0"], out["vw_histo0"] = tgt.copy(), his.copy()
+    for fnum in (0, 1):
+        O.ref_volume().ref_vol_frame_pt(sc.density, sc.res, sc.max_density, sc.baked, sc.baked_res, sc.scatter_rate,
+                                        sc.sky, W, H, ori, up, right, L, np.ones(3, np.float32), SCENE["alpha"],
+                                        SCENE["g"], V["multi"], V["seed"], V["frame"] + fnum, 2 * fnum, 1, 1, tgt, his)
+    out["vw_target"], out["vw_histo"] = tgt, his
+    for k, (pred, den, tone) in enumerate(FINISH_MODES):
+        for fn in (0, 5):
+            o8 = np.zeros(W * H, np.uint32)
+            h = his.copy()
+            O.ref_volume().ref_vol_frame_finish(tgt.copy(), h, W, H, fn, 1, pred, den, V["exposure"], tone, o8)
+            out[f"vw_rgba8_{k}_{fn}"] = o8
+            out[f"vw_histo_{k}_{fn}"] = h
+
 
 def main():
     R = O.ref()
@@ -290,6 +321,7 @@ def main():
 
     # -- volume builders: core/volume.cu's own code on the CPU --------------------
     volume_pins(out, rng)
+    viewer_pins(out, rng)
 
     np.savez_compressed(OUT, **out)
     print(OUT, os.path.getsize(OUT), "bytes")

@@ -325,3 +325,30 @@ def test_env_light_pieces_match_reference(oracle):
         L.orc_image_sample(flat, m.shape[1], m.shape[0], u, v, a)
         oracle.ref_volume().ref_vol_image_sample(flat, m.shape[1], m.shape[0], u, v, b)
         np.testing.assert_array_equal(a, b)
+
+
+# ---------------------------------------------------------------------------
+# the viewer frame (core/volume.cu:57-150, 285-372; core/ACES.cuh)
+# ---------------------------------------------------------------------------
+from tests.golden.make_golden import FINISH_MODES, VIEWER  # noqa: E402
+
+
+def test_viewer_frame_matches_reference(oracle, scene, golden):
+    """Two checkerboard PT frames with the running mean and the radiance
+    histograms, then the finishing pass in every mode: bit for bit."""
+    V = VIEWER
+    W, H = V["W"], V["H"]
+    ori, up, right = camera(W)
+    tgt = golden["vw_target0"].reshape(H, W, 3)
+    his = golden["vw_histo0"].reshape(H, W, 33)
+    for fnum in (0, 1):
+        view = oracle.make_view(W, H, ori, up, right, light_dir(), alpha=SCENE["alpha"], g=SCENE["g"],
+                                multi_scatter=V["multi"], seed=V["seed"], frame=V["frame"] + fnum)
+        tgt, his = oracle.frame_pt(scene, view, fnum, 1, 1, tgt, his)
+    np.testing.assert_array_equal(tgt.ravel(), golden["vw_target"])
+    np.testing.assert_array_equal(his.ravel(), golden["vw_histo"])
+    for k, (pred, den, tone) in enumerate(FINISH_MODES):
+        for fn in (0, 5):
+            o8, h = oracle.frame_finish(tgt, his, fn, 1, pred, den, V["exposure"], tone)
+            np.testing.assert_array_equal(o8.ravel(), golden[f"vw_rgba8_{k}_{fn}"])
+            np.testing.assert_array_equal(h.ravel(), golden[f"vw_histo_{k}_{fn}"])
