@@ -187,6 +187,38 @@ def time_cpu_predict(sc, n_pix, seed=0, reps=1, want=False):
     return n_pix * reps / dt, dt
 
 
+def time_torch_network(sc, hits_per_frame, n_pix=16384, min_s=3.0):
+    """The network alone as a batched PyTorch CPU model (oracle/torch_mlp.py)
+    on the stencil features of n_pix sampled hit pixels of the frame ->
+    network pixels/s and the frames/s that rate gives at the frame's hit
+    count; torch's own thread count."""
+    import torch
+
+    from oracle import oracle as O
+    from oracle.torch_mlp import RadiancePredictor
+    ori, up, right = view_vectors()
+    view = O.make_view(W, H, ori, up, right, light(), alpha=SCENE["alpha"], g=SCENE["g"], seed=0, frame=0)
+    px = np.random.default_rng(5).choice(W * H, 4 * n_pix, replace=False).astype(np.int32)
+    rgba, feat, gam, hit = O.predict_pixels(sc, view, px, want_features=True)
+    sel = np.flatnonzero(hit[:, 3] > 0)[:n_pix]
+    feat, gam = feat[sel], gam[sel]
+    model = RadiancePredictor()
+    sr = (SCENE["albedo"] / 1.001,) * 3
+    model(feat[:256], gam[:256], SCENE["g"], sr)   # warm-up
+    t0, reps = time.perf_counter(), 0
+    while True:
+        model(feat, gam, SCENE["g"], sr)
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt >= min_s:
+            break
+    pps = reps * len(sel) / dt
+    return {"value": pps, "unit": "network pixels/s", "cores": torch.get_num_threads(), "kind": "port",
+            "frames_per_s_network_only": pps / max(1, hits_per_frame),
+            "sample": f"{reps} passes over the features of {len(sel)} hit pixels ({dt:.1f} s), batched PyTorch "
+                      f"float32 CPU port of RadiancePredictInternal"}
+
+
 def frame_parity(vol, px, ref, local):
     """The GPU's FP32 frame of the CPU baseline's view (seed 0, frame 0)
     against the oracle's pixels px (RGBA ref): the FP32 predictor's 1e-4
@@ -747,6 +779,7 @@ def run_mine(args, rank, world, local):
                "sample": f"{args.cpu_reps} passes over {n_cpu} pixels of the {W}x{H} frame ({dt:.1f} s), "
                          f"OpenMP oracle (first hit, gather, FP32 MLP)"}
         parity = frame_parity(vol, px, ref, local)
+        cpu["torch_network"] = time_torch_network(sc, active)
 
     if rank == 0:
         line = {

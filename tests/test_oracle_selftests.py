@@ -174,3 +174,19 @@ def test_tracer_single_scatter_homogeneous_box():
         mean = s[q, 0] / spp
         se = np.sqrt(max(s2[q, 0] / spp - mean ** 2, 0) / spp)
         assert abs(mean - expect) < 4 * se + 0.015 * expect, (p, mean, expect, se)
+
+
+def test_torch_cpu_port_of_the_network(oracle):
+    """The batched PyTorch port of RadiancePredictInternal (the network's CPU
+    baseline) agrees with the oracle's network to 1e-4 relative."""
+    from oracle.torch_mlp import RadiancePredictor
+    rng = np.random.default_rng(21)
+    n = 500
+    feat = np.concatenate([rng.uniform(0, 1.5, (n, 192)), rng.uniform(0, 1, (n, 192)),
+                           rng.uniform(0, 3, (n, 192))], 1).astype(np.float32)
+    gam = rng.uniform(0, np.pi, n).astype(np.float32)
+    model = RadiancePredictor()
+    for sr in ((1.0, 1.0, 1.0), (0.99, 0.9, 0.8), (0.9, 0.9, 0.7)):
+        got = model(feat, gam, 0.857, sr)
+        ref = oracle.mlp_f32(feat, gam, 0.857, sr)
+        np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-6)
