@@ -360,6 +360,12 @@ mrp_status mrp_first_hit(mrp_volume* v, const float* ori, const float* dir, floa
  * (32 for E4M3) up to 128. */
 mrp_status mrp_tc_gemm_check(int fp8, const float* A, const float* B, int n, int k, float* D);
 
+/* Measured rate (GB/s) at which the SMs return cached 8-byte read-only loads
+ * (every CTA reads its own 16 KiB window, eight loads in flight per thread):
+ * the ceiling of the stencil gather's texel reads, which hit L1.  No
+ * counterpart in the reference (a measurement of this GPU). */
+mrp_status mrp_measure_l1_rate(float* gbs);
+
 /* One MRPNN launch of mrp_render (launch index view->frame_offset, no
  * running mean) that also returns the intermediates of NNPredict per pixel:
  * aux [w*h][20] = hit x, y, z, hit flag, gamma, XMain, YMain, ZMain, LXMain

@@ -105,6 +105,7 @@ _SIGS = {
                              C.c_void_p, C.c_int], C.c_int),
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "mrp_measure_l1_rate": ([C.POINTER(C.c_float)], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "mrp_hdri_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
     "mrp_volume_set_hdri": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
@@ -305,6 +306,14 @@ def predict_features_noalloc(feat, gamma, g, scatter_rate, precision=FP32):
     _check(lib().mrp_predict_features_noalloc(feat.ctypes.data, gamma.ctypes.data, float(g), _f3(scatter_rate), n,
                                               out.ctypes.data, int(precision)))
     return out
+
+
+def measure_l1_rate():
+    """mrp_measure_l1_rate: GB/s of cached 8-byte loads on this GPU."""
+    _ensure_init()
+    r = C.c_float()
+    _check(lib().mrp_measure_l1_rate(C.byref(r)))
+    return r.value
 
 
 def tc_gemm_check(A, B, fp8=False):
