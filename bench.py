@@ -335,6 +335,26 @@ def run_tracer(args, local):
            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                         "note": f"trace kernel of the timed frames; algorithmic bytes = (fetches + NEE lookups) x 32 B "
                                 f"(8 fp32 texels) + 16 B/pixel; peak {peak_kind}; the 8 MiB volume is L2-resident"}}
+    # the same frames with the texture unit's trilinear filter in the free
+    # flight (tracer_filter 1, the reference's own tex3D filtering)
+    vol.SetTracerFilter(True)
+    view.frame_offset = 9
+    vol.render_view(view, M.VolumeRender.PT, 1, out)   # builds the density texture
+    ms_hw, tr_hw = [], []
+    for k in range(args.tracer_steps):
+        view.frame_offset = 10 + k
+        vol.render_view(view, M.VolumeRender.PT, 1, out)
+        ms_hw.append(vol.last_render_ms())
+        tr_hw.append(vol.last_render_stages()[0])
+    vol.SetTracerFilter(False)
+    t_hw = float(np.mean(tr_hw))
+    ach_hw = alg / (t_hw / 1000.0) / 1e9
+    res["hw_filter"] = {"ms_per_frame": float(np.mean(ms_hw)), "trace_kernel_ms": t_hw,
+                        "samples_per_s": n * n * TRACER["spp"] / (float(np.mean(ms_hw)) / 1000.0),
+                        "roofline": {"bound": "hbm", "achieved": ach_hw, "peak": hbm, "unit": "GB/s",
+                                     "frac": ach_hw / hbm,
+                                     "note": "same algorithmic bytes (the software path's counters); free-flight "
+                                             "fetches through the texture unit"}}
     if args.tracer_cpu_frames > 0:
         res["cpu_baseline"] = time_cpu_tracer(vol, args.tracer_cpu_frames)
     return res

@@ -72,6 +72,11 @@ typedef struct mrp_params {
     int nee_mode;            /* PT next-event estimation: 0 (default) the baked
                                 TR grid, as the reference; 1 one ratio-tracking
                                 Tr() estimate per vertex (unbiased, no bake) */
+    int tracer_filter;       /* the frame tracer's free-flight density fetch:
+                                0 (default) software trilinear, fp32 weights in
+                                the reference's float order; 1 the texture
+                                unit's trilinear filter, as the reference's
+                                tex3D (weights quantised to 1/256) */
 } mrp_params;
 
 /* One camera: VolumeRender::Render(int2 size, ori, up, right, lightDir, rt,

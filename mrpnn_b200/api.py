@@ -34,7 +34,7 @@ class MrpError(RuntimeError):
 class Params(C.Structure):
     _fields_ = [("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3), ("env_exp", C.c_float),
                 ("bake_res", C.c_int), ("bake_replicate_seeding", C.c_int), ("precision", C.c_int),
-                ("seed", C.c_uint32), ("nee_mode", C.c_int)]
+                ("seed", C.c_uint32), ("nee_mode", C.c_int), ("tracer_filter", C.c_int)]
 
 
 class View(C.Structure):
@@ -460,6 +460,13 @@ class VolumeRender:
 
     def SetSeed(self, seed):
         self._params.seed = int(seed)
+        self._push()
+
+    def SetTracerFilter(self, hardware):
+        """The frame tracer's free-flight density fetch: False (default)
+        software trilinear in the reference's float order; True the texture
+        unit's trilinear filter, as the reference's own tex3D."""
+        self._params.tracer_filter = 1 if hardware else 0
         self._push()
 
     def SetNeeMode(self, unbiased):

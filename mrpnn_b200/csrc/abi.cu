@@ -299,6 +299,8 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
     return MRP_OK;
 }
 
+static void drop_density_texture(mrp_volume* v);
+
 mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
     if (v->stream) cudaStreamSynchronize(v->stream);
@@ -308,6 +310,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     mrp::dev_free(v->occ); mrp::dev_free(v->mip_occ); mrp::dev_free(v->d_maxbits); mrp::dev_free(v->d_bounds); mrp::dev_free(v->mips_pad); mrp::dev_free(v->trs_pad); mrp::dev_free(v->mip_tr); mrp::dev_free(v->pad_pair); mrp::dev_free(v->accum); mrp::dev_free(v->sum3); mrp::dev_free(v->first_pos);
     mrp::dev_free(v->counter);
     mrp::dev_free(v->hdri);
+    drop_density_texture(v);
     mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     tc_free_scratch(v->tc);
     free_multiview(v);
@@ -324,7 +327,48 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     return MRP_OK;
 }
 
+static void drop_density_texture(mrp_volume* v) {
+    if (v->dens_tex) cudaDestroyTextureObject(v->dens_tex);
+    if (v->dens_arr) mrp::dev_free_array(v->dens_arr);
+    v->dens_tex = 0;
+    v->dens_arr = nullptr;
+}
+
+// The density grid copied into a 3D array (width = z, the fastest axis, as
+// the reference's texture coordinate x = z) behind a trilinear texture with
+// border addressing and normalized coordinates, as Update binds
+// _DensityVolume (core/volume.cu:1458-1465).
+static mrp_status ensure_density_texture(mrp_volume* v) {
+    if (v->dens_tex) return MRP_OK;
+    const int R = v->res;
+    cudaChannelFormatDesc desc = v->density_h ? cudaCreateChannelDescHalf() : cudaCreateChannelDesc<float>();
+    const cudaExtent ext = make_cudaExtent(R, R, R);
+    CU(mrp::dev_malloc_3d_array(&v->dens_arr, &desc, ext));
+    cudaMemcpy3DParms cp = {};
+    const size_t elem = v->density_h ? sizeof(__half) : sizeof(float);
+    cp.srcPtr = make_cudaPitchedPtr(v->density_h ? (void*)v->density_h : (void*)v->density, R * elem, R, R);
+    cp.dstArray = v->dens_arr;
+    cp.extent = ext;
+    cp.kind = cudaMemcpyDeviceToDevice;
+    cudaError_t e = cudaMemcpy3DAsync(&cp, v->stream);
+    cudaResourceDesc res = {};
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = v->dens_arr;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    if (e == cudaSuccess) e = cudaCreateTextureObject(&v->dens_tex, &res, &td, nullptr);
+    if (e != cudaSuccess) {
+        drop_density_texture(v);
+        CU(e);
+    }
+    return MRP_OK;
+}
+
 static void invalidate(mrp_volume* v) {
+    drop_density_texture(v);
     v->has_pyramid = v->has_tr = v->has_baked = false;
     v->has_bounds = false;
     v->tr_alpha = NAN; v->bk_alpha = NAN;
@@ -861,7 +905,12 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
             CU(launch_fill_int(v->first_pos, (int)npix, w->spp, v->stream));
             CU(cudaMemsetAsync(v->counter, 0, sizeof(unsigned long long), v->stream));
             if (last) CU(cudaEventRecord(v->ev0, v->stream));
-            CU(launch_trace(d, vd, v->sum3, nullptr, v->first_pos, v->counter, g.sms, v->stream));
+            VolumeDev dt = d;
+            if (v->params.tracer_filter) {
+                TRY(ensure_density_texture(v));
+                dt.dens_tex = v->dens_tex;
+            }
+            CU(launch_trace(dt, vd, v->sum3, nullptr, v->first_pos, v->counter, g.sms, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));
             CU(launch_trace_resolve(v->sum3, v->first_pos, (int)npix, w->spp, i, acc, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[1], v->stream));

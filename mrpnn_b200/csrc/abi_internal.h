@@ -153,6 +153,10 @@ struct mrp_volume {
     int hdri_w = 0, hdri_h = 0;
     std::vector<float> hdri_host;
     int hdri_light_n = 0;   // Roberts2 index of the map's light direction (the reference's rand_cpu)
+    // the density grid as a texture for the tracer's hardware filter (built
+    // on first use, dropped when the grid changes)
+    cudaArray_t dens_arr = nullptr;
+    cudaTextureObject_t dens_tex = 0;
     // tensor-core predictor scratch
     TcScratch tc;
     // mrp_render_views

@@ -426,6 +426,10 @@ struct VolumeDev {
     const float4* hdri;
     int hdri_w, hdri_h;
     float env_exp;
+    // The density grid as a 3D texture (trilinear, border addressing,
+    // normalized coordinates) for the frame tracer's free flight, or 0 for
+    // the software fetch (mrp_params.tracer_filter).
+    cudaTextureObject_t dens_tex;
 };
 
 // SkyBox (core/render.cuh:24-27): the environment map at u = atan2(-z, x) /

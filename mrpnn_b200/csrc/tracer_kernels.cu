@@ -161,7 +161,10 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
                 continue;
             }
             rk = st.next(pix, k, frame, seed);
-            float d = density_t<DT>(v, add(p, mul(rd, t)));
+            const f3 q = add(p, mul(rd, t));
+            // the texture unit's filter (tracer_filter 1), as the reference's
+            // Density(): tex3D(uv.z, uv.y, uv.x) with uv = pos + 0.5
+            float d = v.dens_tex ? tex3D<float>(v.dens_tex, q.z + 0.5f, q.y + 0.5f, q.x + 0.5f) : density_t<DT>(v, q);
             if (COUNT) tally.fetches++;
             float S = d * w.alpha;
             hit = __fdividef(S, smax) > rk;

@@ -71,3 +71,31 @@ def test_tracer_unbiased_nee_zscore():
     assert np.mean(np.abs(zf) < 4) >= 0.999
     assert abs(zf.mean()) < 0.1
     assert np.mean(np.isclose(got[:, :3], rgba[:, :3], rtol=1e-5, atol=1e-7).all(axis=1)) > 0.5
+
+
+def test_tracer_hardware_filter_zscore(scene):
+    """tracer_filter 1: the free flight reads the density through the texture
+    unit's trilinear filter, as the reference's tex3D does (weights quantised
+    to 1/256).  The paths then differ from the oracle's exact-weight fetches,
+    so the bar is the statistical one alone: per-pixel z-scores against the
+    oracle at equal spp."""
+    import mrpnn_b200 as M
+    W, spp = 48, 64
+    ori, up, right = view_frame()
+    scene.vol.SetTracerFilter(True)
+    try:
+        got = scene.vol.Render((W, W), ori, up, right, LIGHT, M.VolumeRender.PT, scene.g, scene.alpha,
+                               multiScatter=64, sampleNum=1, spp=spp, seed=21).reshape(-1, 4)
+    finally:
+        scene.vol.SetTracerFilter(False)
+    view = O.make_view(W, W, ori, up, right, LIGHT, alpha=scene.alpha, g=scene.g, multi_scatter=64, spp=spp,
+                       seed=21, frame=0)
+    rgba, s, s2 = O.trace_pixels(scene.orc, view, np.arange(W * W, dtype=np.int32))
+    mean = s / spp
+    var = np.maximum(s2 / spp - mean ** 2, 0) * spp / (spp - 1)
+    se = np.sqrt(2 * var / spp) + 1e-7
+    hit = rgba[:, 3] >= 0
+    z = ((got[:, :3] - mean) / se)[hit]
+    zf = z[np.isfinite(z)]
+    assert np.mean(np.abs(zf) < 4) >= 0.999
+    assert abs(zf.mean()) < 0.1
