@@ -774,7 +774,7 @@ def run_mine(args, rank, world, local):
         alg = active * stage_bytes_per_hit(args.precision)[dom]
         achieved = alg / (st[dom] / 1000.0) / 1e9
         dram = traffic / (st[dom] / 1000.0) / 1e9 if traffic else None
-        l1 = M.measure_l1_rate()
+        l1 = M.api.measure_l1_rate()
         roof = {"bound": "l1", "achieved": achieved, "peak": l1, "unit": "GB/s", "frac": achieved / l1,
                 "traffic": traffic, "kernel": STAGES[dom],
                 "hbm": {"peak": hbm, "peak_kind": peak_kind, "algorithmic_frac": achieved / hbm,

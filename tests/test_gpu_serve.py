@@ -68,10 +68,10 @@ def test_serve_mix_equals_alone(precision):
         st = srv.stats()
         assert st["completed"] == len(reqs) and st["failed"] == 0
         # continuous batching, not a queue: requests were on the device at the
-        # same time (their TR + first-hit + gather intervals overlap) ...
+        # same time (their intervals from admission to result overlap) ...
         overlaps = sum(1 for i in range(len(times)) for j in range(i + 1, len(times))
-                       if times[i]["admit_ms"] < times[j]["features_ms"] and
-                       times[j]["admit_ms"] < times[i]["features_ms"])
+                       if times[i]["admit_ms"] < times[j]["done_ms"] and
+                       times[j]["admit_ms"] < times[i]["done_ms"])
         assert overlaps >= 3, overlaps
         if prec != M.FP32:
             # ... and network launches carried several requests each
