@@ -482,96 +482,6 @@ __constant__ BlockDesc c_blocks[12] = {
     {8, 176, 0, 1, 33, 128, kAuxSE + 88 * 10, 30, kColPrevDi, 8}, {8, 184, 0, 1, 36, 128, kAuxSE + 88 * 11, 33, kColPrevDi, 8},
 };
 
-// SE gates of the twelve blocks, two blocks per 8-column TMEM slot ([gates
-// of block 2k, 0, gates of block 2k + 1, 0]): the main blocks' at columns
-// 128..159 and the direct-illumination blocks' at 112..127, both unused
-// while the blocks run (the DI blocks' accumulators overwrite the main
-// gates only after the main blocks have read them).
-MRP_D int gate_col(int b) { return b < 8 ? 128 + 8 * (b >> 1) : 112 + 8 * ((b - 8) >> 1); }
-
-// Pools, LSEFin1 contribution and SE gate of block b (core/radiancePredict.cu:
-// 240-247): avg and max of the three channels' slices, with g and gamma,
-// through 8 -> 8 (ReLU) -> 3 (sigmoid); hf accumulates LSEFin1 over the
-// pools in the same order as the reference's 75-input layer.
-template <int W, class Src>
-MRP_D void block_gate(const Src& src, const float* aux, int b, float g, float gamma, float* hf, float* gate) {
-    const BlockDesc bd = c_blocks[b];
-    float p8[8];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        float xs[W];
-        src.template load<W>(c, bd.from, xs);
-        float s = 0.0f, m = -10000.0f;
-#pragma unroll
-        for (int i = 0; i < W; ++i) { s += xs[i]; m = fmaxf(m, xs[i]); }
-        p8[c] = s / (float)W;
-        p8[3 + c] = m;
-    }
-    p8[6] = g;
-    p8[7] = gamma;
-    // (LSEFin1 is stored input-major: the 16 weights of input j at
-    // kAuxLSE1 + 16 j; per output the same sequence of FMAs as o-major)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        float wa[16], wm[16];
-        aux_row<16>(aux, kAuxLSE1 + 16 * (bd.pid + c), wa);
-        aux_row<16>(aux, kAuxLSE1 + 16 * (36 + bd.pid + c), wm);
-#pragma unroll
-        for (int o = 0; o < 16; ++o) {
-            hf[o] = fmaf(wa[o], p8[c], hf[o]);
-            hf[o] = fmaf(wm[o], p8[3 + c], hf[o]);
-        }
-    }
-    float h[8];
-#pragma unroll
-    for (int o = 0; o < 8; ++o) {
-        float w[8];
-        aux_row<8>(aux, bd.se_off + o * 8, w);
-        float a = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], w[j], a);
-        h[o] = fmaxf(a, 0.0f);
-    }
-#pragma unroll
-    for (int o = 0; o < 3; ++o) {
-        float w[8];
-        aux_row<8>(aux, bd.se_off + 64 + o * 8, w);
-        float a = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) a = fmaf(h[j], w[j], a);
-        gate[o] = sigmoid_d(a);
-    }
-}
-template <class Src>
-MRP_D void block_gate_w(const Src& src, const float* aux, int b, float g, float gamma, float* hf, float* gate) {
-    const int w = c_blocks[b].w;
-    if (w == 8) block_gate<8>(src, aux, b, g, gamma, hf, gate);
-    else if (w == 16) block_gate<16>(src, aux, b, g, gamma, hf, gate);
-    else block_gate<32>(src, aux, b, g, gamma, hf, gate);
-}
-
-// The SE gates and the LSEFin1 sums of a tile, ahead of the block chain.
-// They depend only on the feature slices (and g, gamma), not on earlier
-// blocks' outputs, so they need not sit between the dependent MMA rounds;
-// the arithmetic and its order are those of the chained form.
-template <class Src>
-__device__ __noinline__ void tc_gates(const Group G, const Src src, const float* aux, float g, float gamma) {
-    float hf[16];
-#pragma unroll
-    for (int o = 0; o < 16; ++o) hf[o] = 0.0f;
-#pragma unroll 1
-    for (int k = 0; k < 6; ++k) {
-        float slot[8];
-        block_gate_w(src, aux, 2 * k, g, gamma, hf, slot);
-        block_gate_w(src, aux, 2 * k + 1, g, gamma, hf, slot + 4);
-        slot[3] = 0.0f;
-        slot[7] = 0.0f;
-        tmem_put<8>(G, gate_col(2 * k), slot);
-    }
-    tmem_put<16>(G, kColHf, hf);
-    tc::tmem_wait_st();
-}
-
 // One SE block over the three channels (SE / SERES + ADD3 / REP3,
 // core/radiancePredict.cu:240-294): gate from the slice pools, branch layers
 // l0..l0+2 on the tensor cores (D at dcol, dcol+stride, dcol+2*stride), then
@@ -581,21 +491,61 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
                                      float gamma) {
     const BlockDesc bd = c_blocks[b];
     const int from = bd.from, widen = bd.widen, has_prev = bd.has_prev, l0 = bd.l0, dcol = bd.dcol,
-              pcol = bd.pcol, pstride = bd.pstride;
+              se_off = bd.se_off, pid = bd.pid, pcol = bd.pcol, pstride = bd.pstride;
     constexpr int KP = pad_to(W, EB == 2 ? 16 : 32);
     constexpr int SUB = 128 * KP * EB;   // bytes of one branch's A sub-tile
     constexpr int DSTR = W <= 16 ? 16 : 32;
     float xs[3][W];                      // the block's feature slice, loaded once
+    float p8[8];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) src.template load<W>(c, from, xs[c]);
-    // this block's SE gate, computed ahead by tc_gates
-    float gate[3];
+    for (int c = 0; c < 3; ++c) {
+        src.template load<W>(c, from, xs[c]);
+        float s = 0.0f, m = -10000.0f;
+#pragma unroll
+        for (int i = 0; i < W; ++i) { s += xs[c][i]; m = fmaxf(m, xs[c][i]); }
+        p8[c] = s / (float)W;
+        p8[3 + c] = m;
+    }
+    p8[6] = g;
+    p8[7] = gamma;
+    // LSEFin1 (75 -> 16) accumulated block by block in TMEM: pool[pid + c] =
+    // avg, pool[36 + pid + c] = max
     {
-        float gs[8];
-        tmem_get<8>(G, gate_col(b), gs);
-        const bool odd = b & 1;
+        float hf[16];
+        tmem_get<16>(G, kColHf, hf);
+        // (LSEFin1 is stored input-major: the 16 weights of input j at
+        // kAuxLSE1 + 16 j; per output the same sequence of FMAs as o-major)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) gate[c] = odd ? gs[4 + c] : gs[c];
+        for (int c = 0; c < 3; ++c) {
+            float wa[16], wm[16];
+            aux_row<16>(aux, kAuxLSE1 + 16 * (pid + c), wa);
+            aux_row<16>(aux, kAuxLSE1 + 16 * (36 + pid + c), wm);
+#pragma unroll
+            for (int o = 0; o < 16; ++o) {
+                hf[o] = fmaf(wa[o], p8[c], hf[o]);
+                hf[o] = fmaf(wm[o], p8[3 + c], hf[o]);
+            }
+        }
+        tmem_put<16>(G, kColHf, hf);
+    }
+    float h[8], gate[3];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        float w[8];
+        aux_row<8>(aux, se_off + o * 8, w);
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = fmaf(p8[j], w[j], a);
+        h[o] = fmaxf(a, 0.0f);
+    }
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        float w[8];
+        aux_row<8>(aux, se_off + 64 + o * 8, w);
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = fmaf(h[j], w[j], a);
+        gate[o] = sigmoid_d(a);
     }
     float rs[3];
 #pragma unroll
@@ -748,7 +698,13 @@ MRP_D int run_block(const Group& G, int st, const Src& src, const float* aux, in
 template <int EB, class Src>
 MRP_D int tc_network(const Group& G, int st, const Src& src, const float* aux,
                       float gamma, float g, f3 sr, float out[3]) {
-    tc_gates(G, src, aux, g, gamma);
+    {
+        float z[16];
+#pragma unroll
+        for (int o = 0; o < 16; ++o) z[o] = 0.0f;
+        tmem_put<16>(G, kColHf, z);
+        tc::tmem_wait_st();
+    }
     // main branch, X[0:160]; the three 32x32 finals leave comb[0:96) in TMEM columns 0..95
 #pragma unroll 1
     for (int b = 0; b < 8; ++b) st = run_block<EB>(G, st, src, aux, b, g, gamma);
