@@ -437,12 +437,12 @@ struct VolumeDev {
 // first, the order of the reference's host sampler Image_host::Sample,
 // core/volume.hpp:35-42), times enviroment_exp; the constant sky when no
 // map is set.  Software filtering with fp32 weights (the reference's texture
-// unit quantises the weights to 1/256).
-MRP_D f3 sky_radiance(const VolumeDev& v, f3 dir) {
-    if (!v.hdri) return v.sky;
+// unit quantises the weights to 1/256).  The map lookup is an out-of-line
+// call: it runs only where a ray leaves the volume, and inlined its
+// transcendentals would weigh on the register allocation of the hot loops.
+__device__ __noinline__ f3 sky_map(const float4* __restrict__ hdri, int W, int H, float env_exp, f3 dir) {
     const float u = fa(fm(atan2f(-dir.z, dir.x), (float)(0.5 / 3.1415926)), 0.5f);
     const float t = fm(acosf(fmaxf(fminf(dir.y, 1.0f), -1.0f)), (float)(1.0 / 3.1415926));
-    const int W = v.hdri_w, H = v.hdri_h;
     const float px = fs(fm(u, (float)W), 0.5f), py = fs(fm(t, (float)H), 0.5f);
     const float fx = floorf(px), fy = floorf(py);
     const float wx = fs(px, fx), wy = fs(py, fy);
@@ -450,11 +450,14 @@ MRP_D f3 sky_radiance(const VolumeDev& v, f3 dir) {
     x0 += x0 < 0 ? W : 0;
     y0 += y0 < 0 ? H : 0;
     const int x1 = x0 + 1 == W ? 0 : x0 + 1, y1 = y0 + 1 == H ? 0 : y0 + 1;
-    const float4 a = __ldg(v.hdri + (size_t)y0 * W + x0), b = __ldg(v.hdri + (size_t)y0 * W + x1);
-    const float4 c = __ldg(v.hdri + (size_t)y1 * W + x0), d = __ldg(v.hdri + (size_t)y1 * W + x1);
+    const float4 a = __ldg(hdri + (size_t)y0 * W + x0), b = __ldg(hdri + (size_t)y0 * W + x1);
+    const float4 c = __ldg(hdri + (size_t)y1 * W + x0), d = __ldg(hdri + (size_t)y1 * W + x1);
     const f3 r = mk3(lerp(lerp(a.x, b.x, wx), lerp(c.x, d.x, wx), wy), lerp(lerp(a.y, b.y, wx), lerp(c.y, d.y, wx), wy),
                      lerp(lerp(a.z, b.z, wx), lerp(c.z, d.z, wx), wy));
-    return mk3(fm(r.x, v.env_exp), fm(r.y, v.env_exp), fm(r.z, v.env_exp));
+    return mk3(fm(r.x, env_exp), fm(r.y, env_exp), fm(r.z, env_exp));
+}
+MRP_D f3 sky_radiance(const VolumeDev& v, f3 dir) {
+    return v.hdri ? sky_map(v.hdri, v.hdri_w, v.hdri_h, v.env_exp, dir) : v.sky;
 }
 // A level of edge n (n <= 8) stored with one texel of margin below and two
 // above per axis, (n + 3)^3 floats, texel (x, y, z) at ((x + 1) P + y + 1) P

@@ -792,7 +792,7 @@ MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
 // 128-thread blocks, ten resident per SM (48 registers): a block retires as
 // soon as its slowest ray ends, and march lengths vary from 0 to ~1000 steps.
 constexpr int kHitThreads = 128;
-template <bool COUNT, class DT>
+template <bool COUNT, class DT, bool ENV = false>
 __global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
     Tally tally;
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -817,11 +817,14 @@ __global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w,
             tally.lookups += active ? 192 : 0;
             flush_tally(w.counters, tally);
         }
-        f3 LY, LZ;
-        basis(dir, 0.1f, st, &X, &Y, &Z);
-        basis(L, 0.1f, st, &LX, &LY, &LZ);
-        if (!active) {   // NNPredict returns SkyBox(dir) for a ray that finds no hit
-            const f3 sk = sky_radiance(v, dir);
+        if (active) {   // the bases only matter for a hit (they draw after the march)
+            f3 LY, LZ;
+            basis(dir, 0.1f, st, &X, &Y, &Z);
+            basis(L, 0.1f, st, &LX, &LY, &LZ);
+        } else {        // NNPredict returns SkyBox(dir) for a ray that finds no hit
+            // (the map lookup only in the copy compiled for volumes with an
+            // environment map: its call would cost the march registers)
+            const f3 sk = ENV ? sky_map(v.hdri, v.hdri_w, v.hdri_h, v.env_exp, dir) : v.sky;
             running_mean(accum, pix, w.mean_k, make_float4(sk.x, sk.y, sk.z, -1.0f));
         }
     }
@@ -932,8 +935,12 @@ cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, 
     cudaError_t e = cudaMemsetAsync(rec.count, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
     const int blocks = (n + kHitThreads - 1) / kHitThreads;
-    // one copy of the march per counting mode and density storage type
-    if (v.density_h) {
+    // one copy of the march per counting mode and density storage type, and
+    // for volumes with an environment map
+    if (v.hdri) {
+        if (v.density_h) k_hit<false, __half, true><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+        else k_hit<false, float, true><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
+    } else if (v.density_h) {
         if (view.counters) k_hit<true, __half><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
         else k_hit<false, __half><<<blocks, kHitThreads, 0, s>>>(v, view, rec, accum);
     } else {

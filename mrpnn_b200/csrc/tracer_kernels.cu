@@ -69,7 +69,7 @@ MRP_D void deposit(double* __restrict__ sum3, double* __restrict__ sumsq3, int* 
 }
 }  // namespace
 
-template <bool COUNT, class DT>
+template <bool COUNT, class DT, bool TEX = false, bool ENV = false>
 __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ VolumeDev v,
                                                const __grid_constant__ ViewDev w, double* __restrict__ sum3,
                                                double* __restrict__ sumsq3, int* __restrict__ first_pos,
@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
                     }
                     float dis = ray_box_offset(ori, dir);
                     if (dis < 0) {
-                        deposit(sum3, sumsq3, first_pos, pix, k, sky_radiance(v, dir), false);   // SkyBox(dir), coverage stays 0
+                        deposit(sum3, sumsq3, first_pos, pix, k, ENV ? sky_map(v.hdri, v.hdri_w, v.hdri_h, v.env_exp, dir) : v.sky,
+                                false);   // SkyBox(dir), coverage stays 0
                     } else {
                         if (COUNT) tally.events++;
                         if (w.multi_scatter < 1) {
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
             // against IEEE log and division; decisions stay per sample
             t = t - __fdividef(__logf(1.0f - rk), smax);
             if (t > md) {   // left the box: sky radiance, the sample ends
-                res = add(res, mul(sky_radiance(v, rd), csr));
+                res = add(res, mul(ENV ? sky_map(v.hdri, v.hdri_w, v.hdri_h, v.env_exp, rd) : v.sky, csr));
                 deposit(sum3, sumsq3, first_pos, pix, k, res, true);
                 live = false;
                 continue;
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
             const f3 q = add(p, mul(rd, t));
             // the texture unit's filter (tracer_filter 1), as the reference's
             // Density(): tex3D(uv.z, uv.y, uv.x) with uv = pos + 0.5
-            float d = v.dens_tex ? tex3D<float>(v.dens_tex, q.z + 0.5f, q.y + 0.5f, q.x + 0.5f) : density_t<DT>(v, q);
+            float d = TEX ? tex3D<float>(v.dens_tex, q.z + 0.5f, q.y + 0.5f, q.x + 0.5f) : density_t<DT>(v, q);
             if (COUNT) tally.fetches++;
             float S = d * w.alpha;
             hit = __fdividef(S, smax) > rk;
@@ -294,16 +295,25 @@ cudaError_t launch_fill_int(int* p, int n, int value, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// One copy of the event loop per density storage type and: counting mode,
+// the free flight through the density texture (tracer_filter), an
+// environment map (its lookup is a call, which costs the loop registers
+// where it is compiled in).  The counting copy ignores the map: the work it
+// counts does not depend on the sky, and its image is not kept.
+template <class DT>
+static void launch_trace_dt(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
+                            unsigned long long* counter, int sms, cudaStream_t s) {
+    const dim3 grid(sms * 8), block(128);
+    if (view.counters) k_trace<true, DT><<<grid, block, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    else if (v.dens_tex && v.hdri) k_trace<false, DT, true, true><<<grid, block, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    else if (v.dens_tex) k_trace<false, DT, true, false><<<grid, block, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    else if (v.hdri) k_trace<false, DT, false, true><<<grid, block, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+    else k_trace<false, DT><<<grid, block, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
+}
 cudaError_t launch_trace(const VolumeDev& v, const ViewDev& view, double* sum3, double* sumsq3, int* first_pos,
                          unsigned long long* counter, int sms, cudaStream_t s) {
-    // one copy of the event loop per counting mode and density storage type
-    if (v.density_h) {
-        if (view.counters) k_trace<true, __half><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
-        else k_trace<false, __half><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
-    } else {
-        if (view.counters) k_trace<true, float><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
-        else k_trace<false, float><<<sms * 8, 128, 0, s>>>(v, view, sum3, sumsq3, first_pos, counter);
-    }
+    if (v.density_h) launch_trace_dt<__half>(v, view, sum3, sumsq3, first_pos, counter, sms, s);
+    else launch_trace_dt<float>(v, view, sum3, sumsq3, first_pos, counter, sms, s);
     return cudaGetLastError();
 }
 cudaError_t launch_get_samples(const VolumeDev& v, const float* alpha, const float* ori, const float* dir,
