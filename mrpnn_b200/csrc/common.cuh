@@ -440,7 +440,7 @@ struct VolumeDev {
 // unit quantises the weights to 1/256).  The map lookup is an out-of-line
 // call: it runs only where a ray leaves the volume, and inlined its
 // transcendentals would weigh on the register allocation of the hot loops.
-__device__ __noinline__ f3 sky_map(const float4* __restrict__ hdri, int W, int H, float env_exp, f3 dir) {
+static __device__ __noinline__ f3 sky_map(const float4* __restrict__ hdri, int W, int H, float env_exp, f3 dir) {
     const float u = fa(fm(atan2f(-dir.z, dir.x), (float)(0.5 / 3.1415926)), 0.5f);
     const float t = fm(acosf(fmaxf(fminf(dir.y, 1.0f), -1.0f)), (float)(1.0 / 3.1415926));
     const float px = fs(fm(u, (float)W), 0.5f), py = fs(fm(t, (float)H), 0.5f);
