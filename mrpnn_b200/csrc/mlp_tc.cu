@@ -392,7 +392,6 @@ MRP_D void aux_row(const float* aux, int off, float* out) {
 struct RowFeatures {           // [n][576] row-major
     const float* x;
     bool valid;
-    MRP_D void prefetch_slice(int, int) const {}
     template <int W>
     MRP_D void load(int c, int from, float* xs) const {
 #pragma unroll
@@ -402,20 +401,6 @@ struct RowFeatures {           // [n][576] row-major
 struct TileFeatures {          // FP16 pairs of the staged predictor's tiled layout
     const __half2* x;          // already offset to (r / 32) * 288 * 32 + r % 32
     bool valid;
-    // Pulls the slice [from, from + w) of the warp's 32 rows into L1: each
-    // (channel, pair) is one 128-byte line of the warp, lane l fetches line l.
-    // Only for a 32-row group that holds records (lane 0's row is the
-    // group's first): the feature buffer is allocated in whole groups up to
-    // its record capacity.  Every lane of the warp calls this.
-    MRP_D void prefetch_slice(int from, int w) const {
-        const int lane = threadIdx.x & 31, half = w >> 1;
-        const bool group_ok = __shfl_sync(0xffffffffu, valid, 0);
-        if (group_ok && lane < 3 * half) {
-            const int c = lane / half, k = lane - c * half;
-            const __half2* line = x - lane + (size_t)(c * 96 + (from >> 1) + k) * 32;
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(line));
-        }
-    }
     template <int W>
     MRP_D void load(int c, int from, float* xs) const {
 #pragma unroll
@@ -562,9 +547,6 @@ __device__ __noinline__ int tc_block(const Group G, int st, const Src src, const
         }
         rs[c] = write_row<EB, W, KP>(G.a_s, c * SUB, G.t, in);
     }
-    // the next block's slice into L1 while this block's MMAs run (the gate
-    // pass left it in L2)
-    if (b < 11) src.prefetch_slice(c_blocks[b + 1].from, c_blocks[b + 1].w);
     st = mma_round<EB>(G, st, 3, l0, SUB, dcol, DSTR);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
