@@ -7,7 +7,8 @@
   oracle (pinned to the reference's own NNPredict, core/render.cuh:808-875)
   evaluates 4,096 sampled pixels of it (2,048 of them among the hit pixels).
   Bar: the same pixels hit, and 99.9 % of the sampled pixels within 1e-4
-  relative (+1e-6 absolute), the FP32 predictor's contract.
+  relative (+1e-6 absolute), the FP32 predictor's contract.  The same for the
+  1920x1080 view of the precision form (2,048 sampled pixels).
 * Tracer: the tracer workload -- 128^3 fBm (seed 0, base frequency 4),
   256x256, 16 spp, <= 256 bounces, NEE through the 768^3 baked transmittance
   grid, against the oracle's CalculateRadiance (core/render.cuh:535-597) over
@@ -46,6 +47,22 @@ def test_headline_frame_fp32_matches_oracle():
     assert ok.mean() >= 0.999, (ok.mean(), px[~ok][:5])
     rel = np.abs(got[:, :3] - ref[:, :3]) / np.maximum(np.abs(ref[:, :3]), 1e-6)
     assert np.median(rel) < 1e-5
+
+    # the precision form's second view: 1920x1080, the same 45 degree vertical
+    # field of view (right scaled by 16/9), non-square rows and columns
+    Wd, Hd = 1920, 1080
+    right_w = (right * np.float32(16.0 / 9.0)).astype(np.float32)
+    img = sc.vol.Render((Wd, Hd), ori, up, right_w, LIGHT, M.VolumeRender.MRPNN, sc.g, sc.alpha, sampleNum=1,
+                        seed=4).reshape(-1, 4)
+    hit = np.flatnonzero(img[:, 3] > 0)
+    px = np.unique(np.concatenate([rng.choice(hit, 1024, replace=False),
+                                   rng.choice(Wd * Hd, 1024, replace=False)])).astype(np.int32)
+    view = O.make_view(Wd, Hd, ori, up, right_w, LIGHT, alpha=sc.alpha, g=sc.g, seed=4, frame=0)
+    ref = O.predict_pixels(sc.orc, view, px)
+    got = img[px]
+    np.testing.assert_array_equal(got[:, 3] > 0, ref[:, 3] > 0)
+    ok = np.isclose(got, ref, rtol=MLP_RTOL, atol=MLP_ATOL).all(axis=1)
+    assert ok.mean() >= 0.999, (ok.mean(), px[~ok][:5])
 
 
 def test_tracer_workload_zscore():
