@@ -77,6 +77,15 @@ typedef struct mrp_params {
                                 the reference's float order; 1 the texture
                                 unit's trilinear filter, as the reference's
                                 tex3D (weights quantised to 1/256) */
+    int gather_filter;       /* the stencil gather of the BF16 / FP8 forms
+                                (fp16 features): 1 (default) the texture
+                                unit's trilinear and bilinear filters on the
+                                mip, TR and HG-LUT levels, as the reference's
+                                own tex3D / tex2D sampling in SetupInputData
+                                (weights quantised to 1/256); 0 software
+                                filters with fp32 weights.  The FP32 form
+                                always filters in software (the oracle's
+                                features to ~1e-6). */
 } mrp_params;
 
 /* One camera: VolumeRender::Render(int2 size, ori, up, right, lightDir, rt,

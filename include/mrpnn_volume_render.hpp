@@ -163,6 +163,10 @@ class VolumeRender {
         push();
     }
     void SetPrecision(mrp_precision p) { params.precision = p; push(); }
+    // texture-unit filtering (the reference's tex3D / tex2D) for the tracer's
+    // free flight and for the BF16 / FP8 stencil gather (mrp_params)
+    void SetTracerFilter(bool hardware) { params.tracer_filter = hardware ? 1 : 0; push(); }
+    void SetGatherFilter(bool hardware) { params.gather_filter = hardware ? 1 : 0; push(); }
     void SetMaxDensity(float md) {
         mrpnn::check(mrp_volume_set_max_density(h, md), "SetMaxDensity");
         max_density = md;

@@ -34,7 +34,8 @@ class MrpError(RuntimeError):
 class Params(C.Structure):
     _fields_ = [("scatter_rate", F3), ("tr_scale", C.c_float), ("sky", F3), ("env_exp", C.c_float),
                 ("bake_res", C.c_int), ("bake_replicate_seeding", C.c_int), ("precision", C.c_int),
-                ("seed", C.c_uint32), ("nee_mode", C.c_int), ("tracer_filter", C.c_int)]
+                ("seed", C.c_uint32), ("nee_mode", C.c_int), ("tracer_filter", C.c_int),
+                ("gather_filter", C.c_int)]
 
 
 class View(C.Structure):
@@ -469,6 +470,14 @@ class VolumeRender:
         self._params.tracer_filter = 1 if hardware else 0
         self._push()
 
+    def SetGatherFilter(self, hardware):
+        """The stencil gather of the BF16 / FP8 forms: True (default) the
+        texture unit's trilinear / bilinear filters, as the reference's own
+        tex3D / tex2D sampling; False software filters with fp32 weights.  The
+        FP32 form always filters in software."""
+        self._params.gather_filter = 1 if hardware else 0
+        self._push()
+
     def SetNeeMode(self, unbiased):
         """PT next-event estimation: False (default) samples the baked TR grid
         like the reference; True takes one ratio-tracking Tr() estimate per
@@ -757,9 +766,13 @@ class Server:
         _check(st)
         return False, None, None
 
-    def wait(self, ticket):
-        """Blocks until done; returns (output, timing)."""
-        done, tm, out = self.poll(ticket, -1)
+    def wait(self, ticket, timeout_s=300.0):
+        """Blocks until done (at most timeout_s; None waits without a bound);
+        returns (output, timing).  MrpError(ERR_TIMEOUT) when the bound ends
+        first -- the request stays queued."""
+        done, tm, out = self.poll(ticket, -1 if timeout_s is None else max(0, int(timeout_s * 1000)))
+        if not done:
+            raise MrpError(ERR_TIMEOUT, f"request {ticket} not done after {timeout_s} s")
         return out, tm
 
     def stats(self):

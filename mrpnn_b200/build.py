@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmrpnn_b200.so")
 
-SOURCES = ["abi.cu", "serve.cu", "multiview.cu", "batch_rays.cu", "interactive.cu", "volume_io.cu", "hdri.cu", "probe.cu", "volume_kernels.cu", "predictor_kernels.cu", "tracer_kernels.cu", "mlp_tc.cu",
+SOURCES = ["abi.cu", "serve.cu", "multiview.cu", "batch_rays.cu", "interactive.cu", "volume_io.cu", "hdri.cu", "probe.cu", "gather_tex.cu", "volume_kernels.cu", "predictor_kernels.cu", "tracer_kernels.cu", "mlp_tc.cu",
            ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

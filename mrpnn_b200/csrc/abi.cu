@@ -1,6 +1,7 @@
 // abi.cu -- host side of the C ABI (include/mrpnn.h): library state, volume
 // handles, resource caches and the render loop of VolumeRender::Render.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -201,6 +202,7 @@ void mrp_default_params(mrp_params* p) {
     p->bake_replicate_seeding = 1;
     p->precision = MRP_FP32;
     p->seed = 0;
+    p->gather_filter = 1;
 }
 
 mrp_status mrp_load_model(const char* path) {
@@ -263,6 +265,8 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
     if (storage != MRP_STORAGE_FP32 && storage != MRP_STORAGE_FP16)
         return fail(MRP_ERR_INVALID, "unknown density storage %d", (int)storage);
     mrp_volume* v = new mrp_volume();
+    static std::atomic<uint64_t> next_uid{1};
+    v->uid = next_uid.fetch_add(1);
     v->res = res;
     mrp_default_params(&v->params);
     auto cleanup = [&](mrp_status s) { mrp_volume_destroy(v); return s; };
@@ -300,6 +304,7 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
 }
 
 static void drop_density_texture(mrp_volume* v);
+static void drop_gather_textures(mrp_volume* v);
 
 mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (!v) return MRP_OK;
@@ -311,6 +316,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     mrp::dev_free(v->counter);
     mrp::dev_free(v->hdri);
     drop_density_texture(v);
+    drop_gather_textures(v);
     mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     tc_free_scratch(v->tc);
     free_multiview(v);
@@ -364,6 +370,46 @@ static mrp_status ensure_density_texture(mrp_volume* v) {
         drop_density_texture(v);
         CU(e);
     }
+    return MRP_OK;
+}
+
+static void drop_gather_textures(mrp_volume* v) {
+    for (auto& L : v->gmip) gtex_free(&L);
+    for (auto& L : v->gtr) gtex_free(&L);
+    gtex_free(&v->glut);
+    v->gtex_alloc = false;
+    v->gtex_dirty = 7;
+}
+
+// The gather's textures, bound as the reference binds Mip(i), TR_Mip(i) and
+// _HGLut (gather_tex.cu): allocated the first time a BF16 / FP8 gather with
+// gather_filter asks for them, then refreshed on the volume's stream from
+// the linear copies that the builders rewrote.  Called after the LUT and TR
+// levels are current.
+static mrp_status sync_gather_textures(mrp_volume* v) {
+    if (!v->gather_tex_wanted() || !v->has_pyramid || !v->has_tr || !v->has_lut) return MRP_OK;
+    if (!v->gtex_alloc) {
+        cudaError_t e = cudaSuccess;
+        for (int m = 0; m < 9 && e == cudaSuccess; ++m) e = gtex_alloc_level(256 >> m, false, &v->gmip[m]);
+        for (int l = 0; l < 8 && e == cudaSuccess; ++l) e = gtex_alloc_level(128 >> l, true, &v->gtr[l]);
+        if (e == cudaSuccess) e = gtex_alloc_lut(&v->glut);
+        if (e != cudaSuccess) {
+            drop_gather_textures(v);
+            CU(e);
+        }
+        v->gtex_alloc = true;
+        v->gtex_dirty = 7;
+    }
+    const GtexLevel* lv[18];
+    const float* src[18];
+    int k = 0;
+    if (v->gtex_dirty & 1)
+        for (int m = 0; m < 9; ++m, ++k) { lv[k] = &v->gmip[m]; src[k] = v->mips + mip_offset(m); }
+    if (v->gtex_dirty & 2)
+        for (int l = 0; l < 8; ++l, ++k) { lv[k] = &v->gtr[l]; src[k] = v->trs + tr_offset(l); }
+    if (v->gtex_dirty & 4) { lv[k] = &v->glut; src[k] = v->lut; ++k; }
+    if (k) CU(gtex_fill(lv, src, k, g.sms, v->stream));
+    v->gtex_dirty = 0;
     return MRP_OK;
 }
 
@@ -511,6 +557,8 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
         mrp::dev_free(tmp[0]);
         mrp::dev_free(tmp[1]);
         v->has_pyramid = true;
+        v->gtex_dirty |= 1;
+        ++v->pyramid_version;
     }
     CU(cudaStreamSynchronize(v->stream));
     v->has_tr = false; v->tr_alpha = NAN;
@@ -542,6 +590,8 @@ mrp_status mrp_set_params(mrp_volume* v, const mrp_params* p) {
     if (p->precision != MRP_FP32 && p->precision != MRP_BF16 && p->precision != MRP_FP8)
         return fail(MRP_ERR_INVALID, "unknown precision %d", (int)p->precision);
     if (p->nee_mode != 0 && p->nee_mode != 1) return fail(MRP_ERR_INVALID, "nee_mode %d (0 or 1)", p->nee_mode);
+    if (p->gather_filter != 0 && p->gather_filter != 1)
+        return fail(MRP_ERR_INVALID, "gather_filter %d (0 or 1)", p->gather_filter);
     bool bake_changed = p->bake_res != v->params.bake_res || p->tr_scale != v->params.tr_scale ||
                         p->bake_replicate_seeding != v->params.bake_replicate_seeding || p->seed != v->params.seed;
     bool lut_changed = p->seed != v->params.seed;
@@ -646,6 +696,7 @@ mrp_status update_lut_async(mrp_volume* v, float g_) {
     if (v->has_lut && v->lut_g == g_ && v->lut_seed == v->params.seed) return MRP_OK;
     CU(launch_hg_lut(v->lut, g_, v->params.seed, v->stream));
     CU(launch_lut_dirs(v->lut, v->lut + kLut * kLut, v->stream));
+    v->gtex_dirty |= 4;
     v->has_lut = true;
     v->lut_g = g_;
     v->lut_seed = v->params.seed;
@@ -654,7 +705,7 @@ mrp_status update_lut_async(mrp_volume* v, float g_) {
 mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
     if (!v->has_pyramid) return fail(MRP_ERR_NOT_READY, "TR mips need the pyramid (call mrp_volume_update)");
     if (v->has_tr && v->tr_alpha == alpha && v->tr_light[0] == L[0] && v->tr_light[1] == L[1] && v->tr_light[2] == L[2])
-        return MRP_OK;
+        return sync_gather_textures(v);
     CU(build_tr_levels(v->trs, v->mips, v->mip_occ, L, alpha, v->stream));
     CU(launch_pad_levels(v->trs + tr_offset(4), v->trs + tr_offset(5), v->trs + tr_offset(6), true, v->trs_pad,
                          v->stream));
@@ -663,7 +714,8 @@ mrp_status update_tr_async(mrp_volume* v, const float L[3], float alpha) {
     v->has_tr = true;
     v->tr_alpha = alpha;
     std::memcpy(v->tr_light, L, sizeof v->tr_light);
-    return MRP_OK;
+    v->gtex_dirty |= 2;
+    return sync_gather_textures(v);
 }
 }  // namespace mrpi
 extern "C" {

@@ -157,6 +157,15 @@ struct mrp_volume {
     // on first use, dropped when the grid changes)
     cudaArray_t dens_arr = nullptr;
     cudaTextureObject_t dens_tex = 0;
+    // the pyramid, TR levels and LUT as textures for the fp16-feature gather
+    // (gather_filter): allocated on first use, refreshed in place whenever a
+    // builder rewrites the linear copy (gtex_dirty: 1 mips, 2 TR, 4 LUT)
+    mrp::GtexLevel gmip[9], gtr[8], glut;
+    bool gtex_alloc = false;
+    int gtex_dirty = 7;
+    uint64_t uid = 0;                // unique per volume of the process (a server's texture cache key)
+    unsigned pyramid_version = 0;    // counts pyramid builds
+    bool gather_tex_wanted() const { return params.gather_filter != 0 && params.precision != MRP_FP32; }
     // tensor-core predictor scratch
     TcScratch tc;
     // mrp_render_views
@@ -193,6 +202,11 @@ struct mrp_volume {
         d.hdri_h = hdri_h;
         d.env_exp = params.env_exp;
         d.has_bounds = has_bounds ? 1 : 0;
+        if (gtex_alloc && gtex_dirty == 0 && gather_tex_wanted() && has_pyramid && has_tr && has_lut) {
+            for (int m = 0; m < 9; ++m) d.gmip_tex[m] = gmip[m].tex;
+            for (int l = 0; l < 8; ++l) d.gtr_tex[l] = gtr[l].tex;
+            d.glut_tex = glut.tex;
+        }
         if (has_bounds) {
             // Density() at p reads base voxel floor((p + 0.5) R - 0.5) and the
             // next one: nonzero only for base voxels in [min - 1, max]; one

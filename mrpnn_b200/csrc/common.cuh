@@ -430,6 +430,12 @@ struct VolumeDev {
     // normalized coordinates) for the frame tracer's free flight, or 0 for
     // the software fetch (mrp_params.tracer_filter).
     cudaTextureObject_t dens_tex;
+    // The fp16-feature gather through the texture unit's filters
+    // (mrp_params.gather_filter), as the reference samples Mip(i), TR_Mip(i)
+    // and _HGLut: mip levels 0..8 (trilinear, border), TR levels 0..7
+    // (trilinear, clamp), the HG LUT (bilinear, clamp), all with normalized
+    // coordinates.  glut_tex 0: the gather filters in software.
+    cudaTextureObject_t gmip_tex[9], gtr_tex[8], glut_tex;
 };
 
 // SkyBox (core/render.cuh:24-27): the environment map at u = atan2(-z, x) /

@@ -39,9 +39,10 @@ inline cudaError_t dev_free_async(void* p, cudaStream_t s) {
     g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
     return cudaFreeAsync(p, s);
 }
-inline cudaError_t dev_malloc_3d_array(cudaArray_t* a, const cudaChannelFormatDesc* desc, cudaExtent e) {
+inline cudaError_t dev_malloc_3d_array(cudaArray_t* a, const cudaChannelFormatDesc* desc, cudaExtent e,
+                                       unsigned flags = 0) {
     g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
-    return cudaMalloc3DArray(a, desc, e);
+    return cudaMalloc3DArray(a, desc, e, flags);
 }
 inline cudaError_t dev_free_array(cudaArray_t a) {
     g_alloc_calls.fetch_add(1, std::memory_order_relaxed);

@@ -85,6 +85,25 @@ cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, bool fp16, i
 // Tiled feature buffer size for n records (floats).
 inline size_t tiled_feature_floats(size_t n) { return ((n + 31) / 32) * 32 * 576; }
 
+// gather_tex.cu: fp16 array copies of linear fp32 levels behind
+// hardware-filtered textures (trilinear, normalized coordinates, border or
+// clamp addressing) for the texture-unit gather, and of the HG LUT
+// (bilinear, clamp).
+struct GtexLevel {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    cudaSurfaceObject_t surf = 0;   // the fill kernel's view of arr
+    int n = 0;                      // edge: n^3 texels, or n x n for a flat level
+    bool flat = false;
+};
+cudaError_t gtex_alloc_level(int n, bool clamp, GtexLevel* L);
+cudaError_t gtex_alloc_lut(GtexLevel* L);
+void gtex_free(GtexLevel* L);
+// levels[i] <- src[i] (n^3 fp32, z fastest; a flat level 512 x 512, u
+// fastest), rounded to fp16, in one launch per nine levels
+cudaError_t gtex_fill(const GtexLevel* const* levels, const float* const* src, int count, int sms, cudaStream_t s);
+size_t gtex_level_bytes(int n);
+
 // tracer_kernels.cu: one launch of RenderCamera<false> (spp samples per
 // pixel); FP64 sums of per-sample radiance and of its square per pixel.
 // first_pos[pix] must start at spp and counter at 0.

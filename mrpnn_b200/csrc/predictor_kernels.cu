@@ -489,6 +489,78 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
         }
     }
 }
+// The fp16-feature gather through the texture unit (gather_filter): the
+// reference's own sampling in SetupInputData (core/radiancePredict.cu:
+// 433-471) -- tex3D on Mip(layer) (border) and TR_Mip(layer - 1) (clamp),
+// tex2D on _HGLut (clamp), weights quantised by the filter to 1/256 -- in
+// place of the software trilinear of gather_point_fast.  Everything around
+// the fetches is gather_point_fast's: stencil positions, X_Hg's per-record
+// constants, ShadowTerm_TRTex's box entry for points outside the volume.
+MRP_D float tex_at(cudaTextureObject_t t, f3 p) { return tex3D<float>(t, p.z + 0.5f, p.y + 0.5f, p.x + 0.5f); }
+MRP_D void gather_point_tex(const VolumeDev& v, const PixelFrame& f, cudaTextureObject_t mt, cudaTextureObject_t tt,
+                            bool light, const HgFast& H, f3 iLX, int i, float* fd_, float* fs_, float* fh_) {
+    const float4 p0 = c_pt0[i], p1 = c_pt1[i];
+    const float off = p0.w;
+    f3 d;
+    if (!light) {
+        const float px = p0.x, py = p0.y, pz = p0.z;
+        d = mk3(fmaf(f.Z.x, pz, fmaf(f.Y.x, py, f.X.x * px)) * off, fmaf(f.Z.y, pz, fmaf(f.Y.y, py, f.X.y * px)) * off,
+                fmaf(f.Z.z, pz, fmaf(f.Y.z, py, f.X.z * px)) * off);
+    } else {
+        d = mk3(f.L.x * off, f.L.y * off, f.L.z * off);
+    }
+    const f3 cur = mk3(f.pos.x + d.x, f.pos.y + d.y, f.pos.z + d.z);
+    *fd_ = __logf(fmaf(f.alpha * tex_at(mt, cur), 0.015625f, 1.0f));
+    if (i == 0) {
+        *fh_ = __logf(hg(dot(f.X, f.L), f.g) + 1.0f);
+    } else {
+        const float lv = p1.w;
+        float a, b;
+        if (!light) {
+            const float c2 = fmaf(H.q.z, p1.z, fmaf(H.q.y, p1.y, H.q.x * p1.x));
+            a = __ldg(H.lut_dirs + i);
+            b = tex2D<float>(v.glut_tex, fmaf(c2, 0.5f, 0.5f), lv);
+        } else {
+            a = tex2D<float>(v.glut_tex, H.u1L, lv);
+            b = tex2D<float>(v.glut_tex, H.u2L, lv);
+        }
+        *fh_ = __logf(fmaf(a, b, 1.0f));
+    }
+    const bool outside = cur.x < -0.5f || cur.y < -0.5f || cur.z < -0.5f || cur.x > 0.5f || cur.y > 0.5f || cur.z > 0.5f;
+    float tr = 1.0f;
+    if (!outside) {
+        tr = tex_at(tt, cur);
+    } else {
+        const float o = ray_box_offset_inv(cur, iLX);
+        if (o >= 0) tr = tex_at(tt, mk3(fmaf(f.LX.x, o, cur.x), fmaf(f.LX.y, o, cur.y), fmaf(f.LX.z, o, cur.z)));
+    }
+    *fs_ = tr;
+}
+MRP_D void gather_all_tex(const VolumeDev& v, const PixelFrame& f, float* feat, int r) {
+    __half2* out2 = reinterpret_cast<__half2*>(feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31);
+    float pa = 0.0f, pb = 0.0f, pc = 0.0f;   // the even sample of a pair
+    const HgFast H = hg_fast(v, f);
+    const f3 iLX = inv(f.LX);
+#pragma unroll 1
+    for (int run = 0; run < 12; ++run) {
+        const int layer = c_stencil_runs[run][0], from = c_stencil_runs[run][1], to = c_stencil_runs[run][2];
+        const cudaTextureObject_t mt = v.gmip_tex[layer], tt = v.gtr_tex[layer > 1 ? layer - 1 : 0];
+        const bool light = from >= 160;
+#pragma unroll 1
+        for (int i = from; i < to; ++i) {
+            float a, b, c;
+            gather_point_tex(v, f, mt, tt, light, H, iLX, i, &a, &b, &c);
+            if (i & 1) {   // runs start on even samples
+                const int k = i >> 1;
+                out2[k * 32] = __floats2half2_rn(pa, a);
+                out2[(96 + k) * 32] = __floats2half2_rn(pb, b);
+                out2[(192 + k) * 32] = __floats2half2_rn(pc, c);
+            } else {
+                pa = a; pb = b; pc = c;
+            }
+        }
+    }
+}
 MRP_D float gamma_of(const PixelFrame& f) { return acosf(fminf(1.0f, fmaxf(-1.0f, dot(f.X, f.LX)))); }
 
 // All 192 points; feature i of channel c to out[c * stride + i].
@@ -861,12 +933,13 @@ MRP_D PixelFrame record_frame(const HitRecords& rec, int r, f3 L, float g, float
     return pf;
 }
 
-template <bool FP16>
+template <bool FP16, bool TEX = false>
 __global__ void __launch_bounds__(128) k_gather_rec(VolumeDev v, ViewDev w, HitRecords rec, float* __restrict__ feat) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *rec.count) return;
     PixelFrame pf = record_frame(rec, r, normalize(w.light_dir), w.g, w.alpha);
-    gather_all_fast<FP16>(v, pf, feat, r);
+    if (TEX) gather_all_tex(v, pf, feat, r);
+    else gather_all_fast<FP16>(v, pf, feat, r);
 }
 
 __global__ void __launch_bounds__(128) k_mlp_rec(VolumeDev v, ViewDev w, HitRecords rec, const float* __restrict__ feat,
@@ -1188,7 +1261,8 @@ cudaError_t launch_gather_rec(const VolumeDev& v, const ViewDev& view, HitRecord
                               cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;
-    if (fp16) k_gather_rec<true><<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
+    if (fp16 && v.glut_tex) k_gather_rec<true, true><<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
+    else if (fp16) k_gather_rec<true><<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
     else k_gather_rec<false><<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat);
     return cudaGetLastError();
 }

@@ -53,6 +53,7 @@ struct Slot {
     float* rec_f = nullptr;
     float* feat = nullptr;
     float4* accum = nullptr;
+    GtexLevel gtr[8];              // texture copies of trs (tensor-core servers; gtr[0].arr null until used)
     float* staging = nullptr;      // pinned host copy for pageable outputs
     size_t staging_cap = 0;
     bool staged_out = false;
@@ -74,7 +75,30 @@ struct Lut {
     uint32_t seed;
     float* d;
     cudaEvent_t ready;
+    GtexLevel tex;   // its texture copy (tensor-core servers)
 };
+
+// Texture copies of one volume's mip pyramid for the texture-unit gather,
+// shared by every request on that volume; rebuilt when the volume's pyramid
+// is (version), given back under budget pressure when no slot uses them.
+struct VolTex {
+    uint64_t uid = 0;
+    unsigned version = 0;
+    GtexLevel mip[9];
+    cudaEvent_t ready = nullptr;
+    int users = 0;
+};
+size_t tr_tex_bytes() {
+    size_t b = 0;
+    for (int l = 0; l < 8; ++l) b += gtex_level_bytes(128 >> l);
+    return b;
+}
+size_t mip_tex_bytes() {
+    size_t b = 0;
+    for (int m = 0; m < 9; ++m) b += gtex_level_bytes(256 >> m);
+    return b;
+}
+const size_t kLutTexBytes = (size_t)kLut * kLut * 2;
 
 double ms_since(Clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
@@ -97,6 +121,9 @@ struct mrp_server {
     std::deque<std::shared_ptr<Ticket>> pending;
     std::vector<Slot> slots;
     std::vector<Lut> luts;
+    std::vector<std::unique_ptr<VolTex>> vtex;
+    std::vector<VolTex*> slot_vtex;   // per slot: the pyramid textures its request holds, or null
+    bool tex_mode = false;            // tensor-core network: the gather may sample textures
     size_t used = 0;
     cudaStream_t net = nullptr;
     cudaEvent_t ev_net = nullptr;
@@ -119,6 +146,9 @@ struct mrp_server {
         cv_done.notify_all();
     }
     void release(Slot& s) {
+        VolTex*& vt = slot_vtex[&s - slots.data()];
+        if (vt) vt->users--;
+        vt = nullptr;
         s.state = kFree;
         s.t.reset();
         s.staged_out = false;
@@ -135,7 +165,37 @@ struct mrp_server {
         used -= s.bytes;
         s.bytes = 0;
         s.cap = 0;
+        if (s.gtr[0].arr) {   // arrays are not stream-ordered: the slot's work ends first
+            cudaStreamSynchronize(s.stream);
+            for (GtexLevel& L : s.gtr) gtex_free(&L);
+            used -= tr_tex_bytes();
+        }
     }
+    cudaError_t ensure_tr_textures(Slot& s) {
+        if (s.gtr[0].arr) return cudaSuccess;
+        cudaError_t e = cudaSuccess;
+        for (int l = 0; l < 8 && e == cudaSuccess; ++l) e = gtex_alloc_level(128 >> l, true, &s.gtr[l]);
+        if (e != cudaSuccess) {
+            for (GtexLevel& L : s.gtr) gtex_free(&L);
+            return e;
+        }
+        used += tr_tex_bytes();
+        return cudaSuccess;
+    }
+    VolTex* find_vtex(const mrp_volume* v) {
+        for (auto& p : vtex)
+            if (p->uid == v->uid) return p.get();
+        return nullptr;
+    }
+    void drop_vtex(size_t i) {
+        VolTex* p = vtex[i].get();
+        if (p->ready) cudaEventSynchronize(p->ready);
+        for (GtexLevel& L : p->mip) gtex_free(&L);
+        if (p->ready) cudaEventDestroy(p->ready);
+        used -= mip_tex_bytes();
+        vtex.erase(vtex.begin() + (long)i);
+    }
+    VolTex* vtex_for(const mrp_volume* v, cudaStream_t st, std::string* err);
     cudaError_t grow(Slot& s, size_t npix) {
         free_buffers(s);
         cudaError_t e;
@@ -171,20 +231,65 @@ const Lut* mrp_server::lut_for(float g_, uint32_t seed, cudaStream_t s, std::str
             cudaStreamWaitEvent(s, l.ready, 0);
             return &l;
         }
-    Lut l{g_, seed, nullptr, nullptr};
+    Lut l{g_, seed, nullptr, nullptr, GtexLevel{}};
     cudaError_t e;
     if ((e = mrp::dev_malloc(&l.d, kLutBytes)) != cudaSuccess) { *err = cuda_msg("LUT", e); return nullptr; }
+    const GtexLevel* lv = &l.tex;
+    const float* src = l.d;
     if ((e = cudaEventCreateWithFlags(&l.ready, cudaEventDisableTiming)) != cudaSuccess ||
         (e = launch_hg_lut(l.d, g_, seed, s)) != cudaSuccess ||
-        (e = launch_lut_dirs(l.d, l.d + kLut * kLut, s)) != cudaSuccess || (e = cudaEventRecord(l.ready, s)) != cudaSuccess) {
+        (e = launch_lut_dirs(l.d, l.d + kLut * kLut, s)) != cudaSuccess ||
+        (tex_mode && ((e = gtex_alloc_lut(&l.tex)) != cudaSuccess || (e = gtex_fill(&lv, &src, 1, g.sms, s)) != cudaSuccess)) ||
+        (e = cudaEventRecord(l.ready, s)) != cudaSuccess) {
+        if (l.tex.arr) {
+            cudaStreamSynchronize(s);
+            gtex_free(&l.tex);
+        }
         mrp::dev_free(l.d);
         if (l.ready) cudaEventDestroy(l.ready);
         *err = cuda_msg("LUT", e);
         return nullptr;
     }
-    used += kLutBytes;
+    used += kLutBytes + (tex_mode ? kLutTexBytes : 0);
     luts.push_back(l);
     return &luts.back();
+}
+
+// The pyramid textures of volume v, built on the stream of the first request
+// that asks for them (or after the volume's pyramid changed), which later
+// requests wait for.  The caller counts the request as a user.
+VolTex* mrp_server::vtex_for(const mrp_volume* v, cudaStream_t st, std::string* err) {
+    VolTex* p = find_vtex(v);
+    if (p && p->version == v->pyramid_version) {
+        cudaStreamWaitEvent(st, p->ready, 0);
+        return p;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!p) {
+        auto q = std::make_unique<VolTex>();
+        q->uid = v->uid;
+        for (int m = 0; m < 9 && e == cudaSuccess; ++m) e = gtex_alloc_level(256 >> m, false, &q->mip[m]);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q->ready, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            for (GtexLevel& L : q->mip) gtex_free(&L);
+            *err = cuda_msg("pyramid textures", e);
+            return nullptr;
+        }
+        used += mip_tex_bytes();
+        vtex.push_back(std::move(q));
+        p = vtex.back().get();
+    } else {
+        cudaStreamWaitEvent(st, p->ready, 0);   // a previous fill of the old pyramid
+    }
+    const GtexLevel* lv[9];
+    const float* src[9];
+    for (int m = 0; m < 9; ++m) { lv[m] = &p->mip[m]; src[m] = v->mips + mip_offset(m); }
+    if ((e = gtex_fill(lv, src, 9, g.sms, st)) != cudaSuccess || (e = cudaEventRecord(p->ready, st)) != cudaSuccess) {
+        *err = cuda_msg("pyramid textures", e);
+        return nullptr;
+    }
+    p->version = v->pyramid_version;
+    return p;
 }
 
 // Admission, first come first served: the head request enters when a slot
@@ -216,10 +321,26 @@ bool mrp_server::admit() {
         bool need_lut = true;
         for (const Lut& l : luts)
             if (l.g == w.g && l.seed == v->params.seed) need_lut = false;
-        size_t need = (s.cap >= T->npix ? 0 : slot_bytes(T->npix) - s.bytes) + (need_lut ? kLutBytes : 0);
+        // the texture-unit gather (the volume's gather_filter) adds the
+        // slot's TR textures, the volume's pyramid textures and the LUT's
+        const bool use_tex = tex_mode && v->params.gather_filter;
+        size_t need = (s.cap >= T->npix ? 0 : slot_bytes(T->npix) - s.bytes) +
+                      (need_lut ? kLutBytes + (tex_mode ? kLutTexBytes : 0) : 0) +
+                      (use_tex && !s.gtr[0].arr ? tr_tex_bytes() : 0) + (use_tex && !find_vtex(v) ? mip_tex_bytes() : 0);
         if (used + need > cfg.memory_budget) {
             for (Slot& o : slots)   // idle slots give their buffers back
-                if (&o != &s && o.state == kFree && o.bytes && used + need > cfg.memory_budget) free_buffers(o);
+                if (&o != &s && o.state == kFree && (o.bytes || o.gtr[0].arr) && used + need > cfg.memory_budget)
+                    free_buffers(o);
+            for (size_t i = vtex.size(); i-- > 0 && used + need > cfg.memory_budget;)   // and unused pyramid textures
+                if (vtex[i]->users == 0 && vtex[i]->uid != v->uid) drop_vtex(i);
+            bool busy = false;
+            for (const Slot& o : slots) busy = busy || o.state != kFree;
+            if (used + need > cfg.memory_budget && !busy) {   // nothing left to wait for
+                pending.pop_front();
+                moved = true;
+                complete(T, MRP_ERR_BUDGET, "request does not fit the budget beside the server's caches");
+                continue;
+            }
             if (used + need > cfg.memory_budget) break;   // wait for running requests to finish
         }
         pending.pop_front();
@@ -241,9 +362,30 @@ bool mrp_server::admit() {
         s.vd.pad_pair = nullptr;
         s.vd.lut = lut->d;
         s.vd.lut_dirs = lut->d + kLut * kLut;
+        for (auto& t : s.vd.gmip_tex) t = 0;   // textures: the server's own, below
+        for (auto& t : s.vd.gtr_tex) t = 0;
+        s.vd.glut_tex = 0;
+        if (use_tex) {
+            if ((e = ensure_tr_textures(s)) != cudaSuccess) {
+                complete(T, MRP_ERR_OOM, cuda_msg("slot textures", e));
+                release(s);
+                continue;
+            }
+            VolTex* vt = vtex_for(v, s.stream, &err);
+            if (!vt) { complete(T, MRP_ERR_CUDA, err); release(s); continue; }
+            vt->users++;
+            slot_vtex[pick] = vt;
+            for (int m = 0; m < 9; ++m) s.vd.gmip_tex[m] = vt->mip[m].tex;
+            for (int l = 0; l < 8; ++l) s.vd.gtr_tex[l] = s.gtr[l].tex;
+            s.vd.glut_tex = lut->tex.tex;
+        }
         s.view = make_view(v, &w, w.frame_offset, 0);
         HitRecords rec = s.records();
+        const GtexLevel* trl[8];
+        const float* trsrc[8];
+        for (int l = 0; l < 8; ++l) { trl[l] = &s.gtr[l]; trsrc[l] = s.trs + tr_offset(l); }
         if ((e = build_tr_levels(s.trs, v->mips, v->mip_occ, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
+            (use_tex && (e = gtex_fill(trl, trsrc, 8, g.sms, s.stream)) != cudaSuccess) ||
             (e = launch_hit(s.vd, s.view, rec, s.accum, s.stream)) != cudaSuccess ||
             (e = launch_gather_rec(s.vd, s.view, rec, s.feat, cfg.precision != MRP_FP32, s.stream)) != cudaSuccess) {
             complete(T, MRP_ERR_CUDA, cuda_msg("request launch", e));
@@ -459,6 +601,8 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
     };
     cudaError_t e;
     S->slots.resize(cfg.max_slots);
+    S->slot_vtex.assign(cfg.max_slots, nullptr);
+    S->tex_mode = cfg.precision != MRP_FP32;
     for (Slot& s : S->slots)
         if ((e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&s.ev_feat, cudaEventDisableTiming)) != cudaSuccess ||
@@ -505,6 +649,7 @@ mrp_status mrp_serve_submit(mrp_server* S, const mrp_request* r, uint64_t* ticke
     T->req = *r;
     T->npix = (size_t)w.width * w.height;
     size_t need = slot_bytes(T->npix) + kLutBytes;
+    if (S->tex_mode && r->volume->params.gather_filter) need += tr_tex_bytes() + mip_tex_bytes() + kLutTexBytes;
     if (need > S->cfg.memory_budget)
         return fail(MRP_ERR_BUDGET, "request needs %zu bytes, budget is %zu", need, S->cfg.memory_budget);
     std::lock_guard<std::mutex> lk(S->mu);
@@ -561,9 +706,11 @@ mrp_status mrp_serve_close(mrp_server* S) {
         cudaEventDestroy(s.ev_done);
     }
     for (Lut& l : S->luts) {
+        gtex_free(&l.tex);
         mrp::dev_free(l.d);
         cudaEventDestroy(l.ready);
     }
+    while (!S->vtex.empty()) S->drop_vtex(S->vtex.size() - 1);
     cudaStreamDestroy(S->net);
     cudaEventDestroy(S->ev_net);
     tc_free_scratch(S->sc);

@@ -13,6 +13,20 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: long-running CPU case")
 
 
+GPU_TEST_TIMEOUT_S = 600
+
+
+def pytest_collection_modifyitems(config, items):
+    """Every GPU test ends within GPU_TEST_TIMEOUT_S: a test stuck in a
+    blocking library call is ended with the whole process (pytest-timeout's
+    thread method) instead of holding the GPU."""
+    if not config.pluginmanager.hasplugin("timeout"):
+        return
+    for item in items:
+        if item.get_closest_marker("gpu") and not item.get_closest_marker("timeout"):
+            item.add_marker(pytest.mark.timeout(GPU_TEST_TIMEOUT_S, method="thread"))
+
+
 @pytest.fixture(scope="session")
 def golden():
     import numpy as np

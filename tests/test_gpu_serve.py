@@ -89,7 +89,7 @@ def test_serve_device_output_and_budget():
     rng = np.random.default_rng(8)
     (v, view), = _requests(M, vols[:1], 1, rng)
     alone = v.render_view(view, M.VolumeRender.MRPNN, 1, np.empty((view.height, view.width, 4), np.float32))
-    srv = M.Server(max_slots=2, precision=M.BF16, memory_budget=64 << 20)
+    srv = M.Server(max_slots=2, precision=M.BF16, memory_budget=128 << 20)
     try:
         out = torch.empty((view.height, view.width, 4), dtype=torch.float32, device="cuda")
         got, _ = srv.wait(srv.submit(v, view, out))
@@ -98,6 +98,6 @@ def test_serve_device_output_and_budget():
         with pytest.raises(M.MrpError) as e:
             srv.submit(v, big)
         assert e.value.status == M.api.ERR_BUDGET
-        assert srv.stats()["peak_bytes"] <= 64 << 20
+        assert srv.stats()["peak_bytes"] <= 128 << 20
     finally:
         srv.close()
