@@ -374,8 +374,9 @@ static mrp_status ensure_density_texture(mrp_volume* v) {
 }
 
 static void drop_gather_textures(mrp_volume* v) {
-    for (auto& L : v->gmip) gtex_free(&L);
-    for (auto& L : v->gtr) gtex_free(&L);
+    gtex_free(&v->gmip0);
+    gtex_free(&v->gtr0);
+    for (auto& L : v->gpair) gtex_free(&L);
     gtex_free(&v->glut);
     v->gtex_alloc = false;
     v->gtex_dirty = 7;
@@ -390,8 +391,9 @@ static mrp_status sync_gather_textures(mrp_volume* v) {
     if (!v->gather_tex_wanted() || !v->has_pyramid || !v->has_tr || !v->has_lut) return MRP_OK;
     if (!v->gtex_alloc) {
         cudaError_t e = cudaSuccess;
-        for (int m = 0; m < 9 && e == cudaSuccess; ++m) e = gtex_alloc_level(256 >> m, false, &v->gmip[m]);
-        for (int l = 0; l < 8 && e == cudaSuccess; ++l) e = gtex_alloc_level(128 >> l, true, &v->gtr[l]);
+        e = gtex_alloc_level(256, false, &v->gmip0);
+        if (e == cudaSuccess) e = gtex_alloc_level(128, true, &v->gtr0);
+        for (int l = 1; l < kGtexPairs && e == cudaSuccess; ++l) e = gtex_alloc_pair(256 >> l, &v->gpair[l]);
         if (e == cudaSuccess) e = gtex_alloc_lut(&v->glut);
         if (e != cudaSuccess) {
             drop_gather_textures(v);
@@ -400,15 +402,14 @@ static mrp_status sync_gather_textures(mrp_volume* v) {
         v->gtex_alloc = true;
         v->gtex_dirty = 7;
     }
-    const GtexLevel* lv[18];
-    const float* src[18];
+    const GtexLevel* lv[3];
+    const float* src[3];
     int k = 0;
-    if (v->gtex_dirty & 1)
-        for (int m = 0; m < 9; ++m, ++k) { lv[k] = &v->gmip[m]; src[k] = v->mips + mip_offset(m); }
-    if (v->gtex_dirty & 2)
-        for (int l = 0; l < 8; ++l, ++k) { lv[k] = &v->gtr[l]; src[k] = v->trs + tr_offset(l); }
+    if (v->gtex_dirty & 1) { lv[k] = &v->gmip0; src[k] = v->mips; ++k; }
+    if (v->gtex_dirty & 2) { lv[k] = &v->gtr0; src[k] = v->trs; ++k; }
     if (v->gtex_dirty & 4) { lv[k] = &v->glut; src[k] = v->lut; ++k; }
     if (k) CU(gtex_fill(lv, src, k, g.sms, v->stream));
+    if (v->gtex_dirty & 3) CU(gtex_fill_pairs(v->gpair, v->mips, v->trs, g.sms, v->stream));
     v->gtex_dirty = 0;
     return MRP_OK;
 }

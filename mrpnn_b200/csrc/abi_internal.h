@@ -160,7 +160,7 @@ struct mrp_volume {
     // the pyramid, TR levels and LUT as textures for the fp16-feature gather
     // (gather_filter): allocated on first use, refreshed in place whenever a
     // builder rewrites the linear copy (gtex_dirty: 1 mips, 2 TR, 4 LUT)
-    mrp::GtexLevel gmip[9], gtr[8], glut;
+    mrp::GtexLevel gmip0, gtr0, gpair[mrp::kGtexPairs], glut;
     bool gtex_alloc = false;
     int gtex_dirty = 7;
     uint64_t uid = 0;                // unique per volume of the process (a server's texture cache key)
@@ -203,8 +203,9 @@ struct mrp_volume {
         d.env_exp = params.env_exp;
         d.has_bounds = has_bounds ? 1 : 0;
         if (gtex_alloc && gtex_dirty == 0 && gather_tex_wanted() && has_pyramid && has_tr && has_lut) {
-            for (int m = 0; m < 9; ++m) d.gmip_tex[m] = gmip[m].tex;
-            for (int l = 0; l < 8; ++l) d.gtr_tex[l] = gtr[l].tex;
+            d.gmip0_tex = gmip0.tex;
+            d.gtr0_tex = gtr0.tex;
+            for (int l = 1; l < mrp::kGtexPairs; ++l) d.gpair_tex[l] = gpair[l].tex;
             d.glut_tex = glut.tex;
         }
         if (has_bounds) {

@@ -344,6 +344,7 @@ MRP_D float tex3_fast(const float* __restrict__ g, int n, f3 pos) {
 }
 
 constexpr int kLut = 512;
+constexpr int kGtexPairs = 8;   // pair textures of stencil layers 1..7 (index 0 unused)
 constexpr int kLutAlloc = kLut * kLut + 160;   // the LUT and its lut_dirs table
 MRP_D float tex_lut(const float* __restrict__ lut, float u, float v) {
     float px = fs(fm(u, (float)kLut), 0.5f), py = fs(fm(v, (float)kLut), 0.5f);
@@ -432,10 +433,12 @@ struct VolumeDev {
     cudaTextureObject_t dens_tex;
     // The fp16-feature gather through the texture unit's filters
     // (mrp_params.gather_filter), as the reference samples Mip(i), TR_Mip(i)
-    // and _HGLut: mip levels 0..8 (trilinear, border), TR levels 0..7
-    // (trilinear, clamp), the HG LUT (bilinear, clamp), all with normalized
-    // coordinates.  glut_tex 0: the gather filters in software.
-    cudaTextureObject_t gmip_tex[9], gtr_tex[8], glut_tex;
+    // and _HGLut: mip level 0 (trilinear, border) and TR level 0 (trilinear,
+    // clamp) for the stencil's layer 0, the (mip L, TR L - 1) pairs of layers
+    // 1..7 in one half2 texture each (gtex_alloc_pair: padded, clamp,
+    // unnormalized), the HG LUT (bilinear, clamp).  glut_tex 0: the gather
+    // filters in software.
+    cudaTextureObject_t gmip0_tex, gtr0_tex, gpair_tex[kGtexPairs], glut_tex;
 };
 
 // SkyBox (core/render.cuh:24-27): the environment map at u = atan2(-z, x) /

@@ -69,7 +69,74 @@ __global__ void __launch_bounds__(256) k_fill_half(const __grid_constant__ FillT
         else surf3Dwrite(h, t.surf[L], z * (int)sizeof(h), y, x);
     }
 }
+// The (mip L, TR L - 1) pair levels, L = 1..7 (edge n = 256 >> L for both):
+// half2 texels on a grid padded by one texel per side, read with clamp
+// addressing and unnormalized coordinates.  The padding holds density 0
+// (the mip's border value) and the TR level's edge texel (its clamp value),
+// so one trilinear fetch of the pair returns what the mip's border-mode and
+// the TR level's clamp-mode fetches return at the same point, anywhere.
+struct PairTable {
+    const float* mip[kGtexPairs];
+    const float* tr[kGtexPairs];
+    cudaSurfaceObject_t surf[kGtexPairs];
+    int n[kGtexPairs];
+};
+__global__ void __launch_bounds__(256) k_fill_pairs(const __grid_constant__ PairTable t) {
+    const int L = blockIdx.y, n = t.n[L], P = n + 2;
+    if (n == 0) return;
+    const size_t total = (size_t)P * P * P;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int zp = (int)(i % P), yp = (int)((i / P) % P), xp = (int)(i / ((size_t)P * P));
+        const int x = xp - 1, y = yp - 1, z = zp - 1;
+        const bool in = (unsigned)x < (unsigned)n && (unsigned)y < (unsigned)n && (unsigned)z < (unsigned)n;
+        const int cx = min(max(x, 0), n - 1), cy = min(max(y, 0), n - 1), cz = min(max(z, 0), n - 1);
+        const size_t c = ((size_t)cx * n + cy) * n + cz;
+        const float d = in ? __ldg(t.mip[L] + c) : 0.0f;
+        const __half2 h = __floats2half2_rn(d, __ldg(t.tr[L] + c));
+        surf3Dwrite(*reinterpret_cast<const unsigned*>(&h), t.surf[L], zp * 4, yp, xp);
+    }
+}
 }  // namespace
+
+cudaError_t gtex_alloc_pair(int n, GtexLevel* L) {
+    *L = GtexLevel{};
+    const int P = n + 2;
+    cudaChannelFormatDesc desc = cudaCreateChannelDescHalf2();
+    cudaError_t e = dev_malloc_3d_array(&L->arr, &desc, make_cudaExtent(P, P, P), cudaArraySurfaceLoadStore);
+    if (e == cudaSuccess) {
+        cudaResourceDesc res = {};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = L->arr;
+        cudaTextureDesc td = {};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        e = cudaCreateTextureObject(&L->tex, &res, &td, nullptr);
+    }
+    if (e == cudaSuccess) e = make_surface(L->arr, &L->surf);
+    if (e != cudaSuccess) gtex_free(L);
+    else L->n = n;
+    return e;
+}
+
+cudaError_t gtex_fill_pairs(const GtexLevel* pairs, const float* mips, const float* trs, int sms, cudaStream_t s) {
+    PairTable t{};
+    for (int L = 1; L < kGtexPairs; ++L) {
+        if (!pairs[L].surf || pairs[L].n != (256 >> L)) return cudaErrorInvalidValue;
+        t.mip[L] = mips + mip_offset(L);
+        t.tr[L] = trs + tr_offset(L - 1);
+        t.surf[L] = pairs[L].surf;
+        t.n[L] = pairs[L].n;
+    }
+    const size_t most = (size_t)130 * 130 * 130;
+    const size_t want = (most + 255) / 256;
+    const unsigned bx = (unsigned)(want < (size_t)sms * 8 ? want : (size_t)sms * 8);
+    k_fill_pairs<<<dim3(bx, kGtexPairs), 256, 0, s>>>(t);   // row 0 (n = 0) returns at once
+    return cudaGetLastError();
+}
+
+size_t gtex_pair_bytes(int n) { return (size_t)(n + 2) * (n + 2) * (n + 2) * sizeof(__half2); }
 
 cudaError_t gtex_alloc_level(int n, bool clamp, GtexLevel* L) {
     return alloc(n, n, clamp ? cudaAddressModeClamp : cudaAddressModeBorder, L);

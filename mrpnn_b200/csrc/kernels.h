@@ -103,6 +103,13 @@ void gtex_free(GtexLevel* L);
 // fastest), rounded to fp16, in one launch per nine levels
 cudaError_t gtex_fill(const GtexLevel* const* levels, const float* const* src, int count, int sms, cudaStream_t s);
 size_t gtex_level_bytes(int n);
+// The (mip L, TR L - 1) pair levels of the gather, L = 1..kGtexPairs-1
+// (index 0 unused): half2 texels on an (n+2)^3 grid padded with the mip's
+// border value and the TR level's clamp value, clamp addressing,
+// unnormalized coordinates (texel centre of voxel i at i + 1.5).
+cudaError_t gtex_alloc_pair(int n, GtexLevel* L);
+cudaError_t gtex_fill_pairs(const GtexLevel* pairs, const float* mips, const float* trs, int sms, cudaStream_t s);
+size_t gtex_pair_bytes(int n);
 
 // tracer_kernels.cu: one launch of RenderCamera<false> (spp samples per
 // pixel); FP64 sums of per-sample radiance and of its square per pixel.

@@ -493,16 +493,29 @@ MRP_D void gather_all_fast(const VolumeDev& v, const PixelFrame& f, float* feat,
 // reference's own sampling in SetupInputData (core/radiancePredict.cu:
 // 433-471) -- tex3D on Mip(layer) (border) and TR_Mip(layer - 1) (clamp),
 // tex2D on _HGLut (clamp), weights quantised by the filter to 1/256 -- in
-// place of the software trilinear of gather_point_fast.  Everything around
-// the fetches is gather_point_fast's: stencil positions, X_Hg's per-record
-// constants, ShadowTerm_TRTex's box entry for points outside the volume.
+// place of the software trilinear of gather_point_fast.  Layers 1..7 read
+// mip and TR from one pair texture (one fetch for both where the point is
+// inside the volume); layer 0 (mip 256^3, TR 128^3) from two textures.
+// Everything around the fetches is gather_point_fast's: stencil positions,
+// X_Hg's per-record constants, ShadowTerm_TRTex's box entry for points
+// outside the volume.
 MRP_D float tex_at(cudaTextureObject_t t, f3 p) { return tex3D<float>(t, p.z + 0.5f, p.y + 0.5f, p.x + 0.5f); }
-MRP_D void gather_point_tex(const VolumeDev& v, const PixelFrame& f, cudaTextureObject_t mt, cudaTextureObject_t tt,
-                            bool light, const HgFast& H, f3 iLX, int i, float* fd_, float* fs_, float* fh_) {
+// pair texel coordinate of p on a level of edge n: (p + 0.5) n + 1, the
+// padded grid's unnormalized coordinate (voxel i centred at i + 1.5)
+MRP_D float2 pair_at(cudaTextureObject_t t, float n, float c, f3 p) {
+    return tex3D<float2>(t, fmaf(p.z, n, c), fmaf(p.y, n, c), fmaf(p.x, n, c));
+}
+struct TexRun {
+    cudaTextureObject_t a, b;   // layer 0: mip, TR; else the pair (a) of the run's layer
+    float n, c;                 // the pair level's edge and coordinate offset n / 2 + 1
+    bool pair, light;
+};
+MRP_D void gather_point_tex(const VolumeDev& v, const PixelFrame& f, const TexRun& R, const HgFast& H, f3 iLX, int i,
+                            float* fd_, float* fs_, float* fh_) {
     const float4 p0 = c_pt0[i], p1 = c_pt1[i];
     const float off = p0.w;
     f3 d;
-    if (!light) {
+    if (!R.light) {
         const float px = p0.x, py = p0.y, pz = p0.z;
         d = mk3(fmaf(f.Z.x, pz, fmaf(f.Y.x, py, f.X.x * px)) * off, fmaf(f.Z.y, pz, fmaf(f.Y.y, py, f.X.y * px)) * off,
                 fmaf(f.Z.z, pz, fmaf(f.Y.z, py, f.X.z * px)) * off);
@@ -510,13 +523,30 @@ MRP_D void gather_point_tex(const VolumeDev& v, const PixelFrame& f, cudaTexture
         d = mk3(f.L.x * off, f.L.y * off, f.L.z * off);
     }
     const f3 cur = mk3(f.pos.x + d.x, f.pos.y + d.y, f.pos.z + d.z);
-    *fd_ = __logf(fmaf(f.alpha * tex_at(mt, cur), 0.015625f, 1.0f));
+    // ShadowTerm_TRTex: the TR at the point inside the volume, else where the
+    // light ray from it enters the volume (1 where it misses)
+    const bool outside = cur.x < -0.5f || cur.y < -0.5f || cur.z < -0.5f || cur.x > 0.5f || cur.y > 0.5f || cur.z > 0.5f;
+    float o = 0.0f;
+    if (outside) o = ray_box_offset_inv(cur, iLX);
+    const f3 q = mk3(fmaf(f.LX.x, o, cur.x), fmaf(f.LX.y, o, cur.y), fmaf(f.LX.z, o, cur.z));
+    float dens, tr = 1.0f;
+    if (R.pair) {
+        const float2 m = pair_at(R.a, R.n, R.c, cur);
+        dens = m.x;
+        if (!outside) tr = m.y;
+        else if (o >= 0) tr = pair_at(R.a, R.n, R.c, q).y;
+    } else {
+        dens = tex_at(R.a, cur);
+        if (!outside || o >= 0) tr = tex_at(R.b, q);
+    }
+    *fd_ = __logf(fmaf(f.alpha * dens, 0.015625f, 1.0f));
+    *fs_ = tr;
     if (i == 0) {
         *fh_ = __logf(hg(dot(f.X, f.L), f.g) + 1.0f);
     } else {
         const float lv = p1.w;
         float a, b;
-        if (!light) {
+        if (!R.light) {
             const float c2 = fmaf(H.q.z, p1.z, fmaf(H.q.y, p1.y, H.q.x * p1.x));
             a = __ldg(H.lut_dirs + i);
             b = tex2D<float>(v.glut_tex, fmaf(c2, 0.5f, 0.5f), lv);
@@ -526,15 +556,6 @@ MRP_D void gather_point_tex(const VolumeDev& v, const PixelFrame& f, cudaTexture
         }
         *fh_ = __logf(fmaf(a, b, 1.0f));
     }
-    const bool outside = cur.x < -0.5f || cur.y < -0.5f || cur.z < -0.5f || cur.x > 0.5f || cur.y > 0.5f || cur.z > 0.5f;
-    float tr = 1.0f;
-    if (!outside) {
-        tr = tex_at(tt, cur);
-    } else {
-        const float o = ray_box_offset_inv(cur, iLX);
-        if (o >= 0) tr = tex_at(tt, mk3(fmaf(f.LX.x, o, cur.x), fmaf(f.LX.y, o, cur.y), fmaf(f.LX.z, o, cur.z)));
-    }
-    *fs_ = tr;
 }
 MRP_D void gather_all_tex(const VolumeDev& v, const PixelFrame& f, float* feat, int r) {
     __half2* out2 = reinterpret_cast<__half2*>(feat) + (size_t)(r >> 5) * 288 * 32 + (r & 31);
@@ -544,12 +565,13 @@ MRP_D void gather_all_tex(const VolumeDev& v, const PixelFrame& f, float* feat, 
 #pragma unroll 1
     for (int run = 0; run < 12; ++run) {
         const int layer = c_stencil_runs[run][0], from = c_stencil_runs[run][1], to = c_stencil_runs[run][2];
-        const cudaTextureObject_t mt = v.gmip_tex[layer], tt = v.gtr_tex[layer > 1 ? layer - 1 : 0];
-        const bool light = from >= 160;
+        const float n = (float)(256 >> layer);
+        const TexRun R = layer == 0 ? TexRun{v.gmip0_tex, v.gtr0_tex, 0.0f, 0.0f, false, from >= 160}
+                                    : TexRun{v.gpair_tex[layer], 0, n, fmaf(n, 0.5f, 1.0f), true, from >= 160};
 #pragma unroll 1
         for (int i = from; i < to; ++i) {
             float a, b, c;
-            gather_point_tex(v, f, mt, tt, light, H, iLX, i, &a, &b, &c);
+            gather_point_tex(v, f, R, H, iLX, i, &a, &b, &c);
             if (i & 1) {   // runs start on even samples
                 const int k = i >> 1;
                 out2[k * 32] = __floats2half2_rn(pa, a);

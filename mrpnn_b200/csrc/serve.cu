@@ -53,7 +53,8 @@ struct Slot {
     float* rec_f = nullptr;
     float* feat = nullptr;
     float4* accum = nullptr;
-    GtexLevel gtr[8];              // texture copies of trs (tensor-core servers; gtr[0].arr null until used)
+    GtexLevel gtr0;                // texture copies of TR level 0 and of the (mip, TR) pairs of this
+    GtexLevel gpair[kGtexPairs];   // request (tensor-core servers; gtr0.arr null until used)
     float* staging = nullptr;      // pinned host copy for pageable outputs
     size_t staging_cap = 0;
     bool staged_out = false;
@@ -78,26 +79,22 @@ struct Lut {
     GtexLevel tex;   // its texture copy (tensor-core servers)
 };
 
-// Texture copies of one volume's mip pyramid for the texture-unit gather,
+// Texture copy of one volume's mip level 0 for the texture-unit gather,
 // shared by every request on that volume; rebuilt when the volume's pyramid
 // is (version), given back under budget pressure when no slot uses them.
 struct VolTex {
     uint64_t uid = 0;
     unsigned version = 0;
-    GtexLevel mip[9];
+    GtexLevel mip0;
     cudaEvent_t ready = nullptr;
     int users = 0;
 };
-size_t tr_tex_bytes() {
-    size_t b = 0;
-    for (int l = 0; l < 8; ++l) b += gtex_level_bytes(128 >> l);
+size_t tr_tex_bytes() {   // a slot's: TR level 0 and the pairs
+    size_t b = gtex_level_bytes(128);
+    for (int l = 1; l < kGtexPairs; ++l) b += gtex_pair_bytes(256 >> l);
     return b;
 }
-size_t mip_tex_bytes() {
-    size_t b = 0;
-    for (int m = 0; m < 9; ++m) b += gtex_level_bytes(256 >> m);
-    return b;
-}
+size_t mip_tex_bytes() { return gtex_level_bytes(256); }
 const size_t kLutTexBytes = (size_t)kLut * kLut * 2;
 
 double ms_since(Clock::time_point t0) {
@@ -165,18 +162,20 @@ struct mrp_server {
         used -= s.bytes;
         s.bytes = 0;
         s.cap = 0;
-        if (s.gtr[0].arr) {   // arrays are not stream-ordered: the slot's work ends first
+        if (s.gtr0.arr) {   // arrays are not stream-ordered: the slot's work ends first
             cudaStreamSynchronize(s.stream);
-            for (GtexLevel& L : s.gtr) gtex_free(&L);
+            gtex_free(&s.gtr0);
+            for (GtexLevel& L : s.gpair) gtex_free(&L);
             used -= tr_tex_bytes();
         }
     }
     cudaError_t ensure_tr_textures(Slot& s) {
-        if (s.gtr[0].arr) return cudaSuccess;
-        cudaError_t e = cudaSuccess;
-        for (int l = 0; l < 8 && e == cudaSuccess; ++l) e = gtex_alloc_level(128 >> l, true, &s.gtr[l]);
+        if (s.gtr0.arr) return cudaSuccess;
+        cudaError_t e = gtex_alloc_level(128, true, &s.gtr0);
+        for (int l = 1; l < kGtexPairs && e == cudaSuccess; ++l) e = gtex_alloc_pair(256 >> l, &s.gpair[l]);
         if (e != cudaSuccess) {
-            for (GtexLevel& L : s.gtr) gtex_free(&L);
+            gtex_free(&s.gtr0);
+            for (GtexLevel& L : s.gpair) gtex_free(&L);
             return e;
         }
         used += tr_tex_bytes();
@@ -190,7 +189,7 @@ struct mrp_server {
     void drop_vtex(size_t i) {
         VolTex* p = vtex[i].get();
         if (p->ready) cudaEventSynchronize(p->ready);
-        for (GtexLevel& L : p->mip) gtex_free(&L);
+        gtex_free(&p->mip0);
         if (p->ready) cudaEventDestroy(p->ready);
         used -= mip_tex_bytes();
         vtex.erase(vtex.begin() + (long)i);
@@ -268,10 +267,10 @@ VolTex* mrp_server::vtex_for(const mrp_volume* v, cudaStream_t st, std::string* 
     if (!p) {
         auto q = std::make_unique<VolTex>();
         q->uid = v->uid;
-        for (int m = 0; m < 9 && e == cudaSuccess; ++m) e = gtex_alloc_level(256 >> m, false, &q->mip[m]);
+        e = gtex_alloc_level(256, false, &q->mip0);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q->ready, cudaEventDisableTiming);
         if (e != cudaSuccess) {
-            for (GtexLevel& L : q->mip) gtex_free(&L);
+            gtex_free(&q->mip0);
             *err = cuda_msg("pyramid textures", e);
             return nullptr;
         }
@@ -281,10 +280,9 @@ VolTex* mrp_server::vtex_for(const mrp_volume* v, cudaStream_t st, std::string* 
     } else {
         cudaStreamWaitEvent(st, p->ready, 0);   // a previous fill of the old pyramid
     }
-    const GtexLevel* lv[9];
-    const float* src[9];
-    for (int m = 0; m < 9; ++m) { lv[m] = &p->mip[m]; src[m] = v->mips + mip_offset(m); }
-    if ((e = gtex_fill(lv, src, 9, g.sms, st)) != cudaSuccess || (e = cudaEventRecord(p->ready, st)) != cudaSuccess) {
+    const GtexLevel* lv = &p->mip0;
+    const float* src = v->mips;
+    if ((e = gtex_fill(&lv, &src, 1, g.sms, st)) != cudaSuccess || (e = cudaEventRecord(p->ready, st)) != cudaSuccess) {
         *err = cuda_msg("pyramid textures", e);
         return nullptr;
     }
@@ -326,10 +324,10 @@ bool mrp_server::admit() {
         const bool use_tex = tex_mode && v->params.gather_filter;
         size_t need = (s.cap >= T->npix ? 0 : slot_bytes(T->npix) - s.bytes) +
                       (need_lut ? kLutBytes + (tex_mode ? kLutTexBytes : 0) : 0) +
-                      (use_tex && !s.gtr[0].arr ? tr_tex_bytes() : 0) + (use_tex && !find_vtex(v) ? mip_tex_bytes() : 0);
+                      (use_tex && !s.gtr0.arr ? tr_tex_bytes() : 0) + (use_tex && !find_vtex(v) ? mip_tex_bytes() : 0);
         if (used + need > cfg.memory_budget) {
             for (Slot& o : slots)   // idle slots give their buffers back
-                if (&o != &s && o.state == kFree && (o.bytes || o.gtr[0].arr) && used + need > cfg.memory_budget)
+                if (&o != &s && o.state == kFree && (o.bytes || o.gtr0.arr) && used + need > cfg.memory_budget)
                     free_buffers(o);
             for (size_t i = vtex.size(); i-- > 0 && used + need > cfg.memory_budget;)   // and unused pyramid textures
                 if (vtex[i]->users == 0 && vtex[i]->uid != v->uid) drop_vtex(i);
@@ -362,9 +360,8 @@ bool mrp_server::admit() {
         s.vd.pad_pair = nullptr;
         s.vd.lut = lut->d;
         s.vd.lut_dirs = lut->d + kLut * kLut;
-        for (auto& t : s.vd.gmip_tex) t = 0;   // textures: the server's own, below
-        for (auto& t : s.vd.gtr_tex) t = 0;
-        s.vd.glut_tex = 0;
+        s.vd.gmip0_tex = s.vd.gtr0_tex = s.vd.glut_tex = 0;   // textures: the server's own, below
+        for (auto& t : s.vd.gpair_tex) t = 0;
         if (use_tex) {
             if ((e = ensure_tr_textures(s)) != cudaSuccess) {
                 complete(T, MRP_ERR_OOM, cuda_msg("slot textures", e));
@@ -375,17 +372,18 @@ bool mrp_server::admit() {
             if (!vt) { complete(T, MRP_ERR_CUDA, err); release(s); continue; }
             vt->users++;
             slot_vtex[pick] = vt;
-            for (int m = 0; m < 9; ++m) s.vd.gmip_tex[m] = vt->mip[m].tex;
-            for (int l = 0; l < 8; ++l) s.vd.gtr_tex[l] = s.gtr[l].tex;
+            s.vd.gmip0_tex = vt->mip0.tex;
+            s.vd.gtr0_tex = s.gtr0.tex;
+            for (int l = 1; l < kGtexPairs; ++l) s.vd.gpair_tex[l] = s.gpair[l].tex;
             s.vd.glut_tex = lut->tex.tex;
         }
         s.view = make_view(v, &w, w.frame_offset, 0);
         HitRecords rec = s.records();
-        const GtexLevel* trl[8];
-        const float* trsrc[8];
-        for (int l = 0; l < 8; ++l) { trl[l] = &s.gtr[l]; trsrc[l] = s.trs + tr_offset(l); }
+        const GtexLevel* trl = &s.gtr0;
+        const float* trsrc = s.trs;
         if ((e = build_tr_levels(s.trs, v->mips, v->mip_occ, w.light_dir, w.alpha, s.stream)) != cudaSuccess ||
-            (use_tex && (e = gtex_fill(trl, trsrc, 8, g.sms, s.stream)) != cudaSuccess) ||
+            (use_tex && ((e = gtex_fill(&trl, &trsrc, 1, g.sms, s.stream)) != cudaSuccess ||
+                         (e = gtex_fill_pairs(s.gpair, v->mips, s.trs, g.sms, s.stream)) != cudaSuccess)) ||
             (e = launch_hit(s.vd, s.view, rec, s.accum, s.stream)) != cudaSuccess ||
             (e = launch_gather_rec(s.vd, s.view, rec, s.feat, cfg.precision != MRP_FP32, s.stream)) != cudaSuccess) {
             complete(T, MRP_ERR_CUDA, cuda_msg("request launch", e));
