@@ -788,6 +788,17 @@ def run_mine(args, rank, world, local):
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": traffic,
                 "kernel": STAGES[dom], "note": "march lookups are data dependent; see profiles/"}
+    if dom == 2 and args.precision == "fp32":
+        # the FP32 drop-in network: SIMT FMAs, roofline = the CUDA cores' FP32
+        # rate (no measured figure exists for it: nominal 128 FMA lanes per SM)
+        flop = active * FLOP_PER_HIT
+        achieved = flop / (st[dom] / 1000.0) / 1e12
+        mhz = clocks.summary().get("sm_max_mhz") or 1965.0
+        fp32_peak = torch.cuda.get_device_properties(local).multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+        roof = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": traffic, "kernel": STAGES[dom],
+                "note": f"algorithmic FLOP = {FLOP_PER_HIT} x {active} hit pixels per launch; duration = CUDA events "
+                        f"around the stage; peak = nominal FP32 FMA rate of the SMs at {mhz:.0f} MHz (not measured)"}
 
     tracer = run_tracer(args, local) if (rank == 0 and args.tracer_steps > 0) else None
     serving = run_serving(args, local) if (rank == 0 and args.serve_requests > 0) else None

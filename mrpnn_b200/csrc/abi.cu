@@ -317,6 +317,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     mrp::dev_free(v->hdri);
     drop_density_texture(v);
     drop_gather_textures(v);
+    gtex_free(&v->baked_gtex);
     mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     tc_free_scratch(v->tc);
     free_multiview(v);
@@ -411,6 +412,29 @@ static mrp_status sync_gather_textures(mrp_volume* v) {
     if (k) CU(gtex_fill(lv, src, k, g.sms, v->stream));
     if (v->gtex_dirty & 3) CU(gtex_fill_pairs(v->gpair, v->mips, v->trs, g.sms, v->stream));
     v->gtex_dirty = 0;
+    return MRP_OK;
+}
+
+// The baked NEE grid copied into an fp16 3D array behind a trilinear
+// texture with clamp addressing, as Update_CachedTR binds TR_Mip(0) to the
+// baked array (core/volume.cu:1687-1693), for the tracer's NEE lookup under
+// tracer_filter; refilled after every bake.
+static mrp_status ensure_baked_texture(mrp_volume* v) {
+    if (v->baked_gtex.arr && v->baked_gtex.n != v->bk_res) {
+        CU(cudaStreamSynchronize(v->stream));   // arrays are not stream-ordered
+        gtex_free(&v->baked_gtex);
+        v->baked_gtex_ok = false;
+    }
+    if (!v->baked_gtex.arr) {
+        CU(gtex_alloc_level(v->bk_res, true, &v->baked_gtex));
+        v->baked_gtex_ok = false;
+    }
+    if (!v->baked_gtex_ok) {
+        const GtexLevel* lv = &v->baked_gtex;
+        const float* src = v->baked;
+        CU(gtex_fill(&lv, &src, 1, g.sms, v->stream));
+        v->baked_gtex_ok = true;
+    }
     return MRP_OK;
 }
 
@@ -737,6 +761,7 @@ mrp_status update_baked_async(mrp_volume* v, const float L[3], float alpha) {
     v->bk_res = B;
     VolumeDev d = v->dev();
     CU(launch_baked_tr(v->baked, d, B, alpha, L, v->params.seed, v->params.bake_replicate_seeding, g.sms, v->stream));
+    v->baked_gtex_ok = false;
     v->has_baked = true;
     v->bk_alpha = alpha;
     v->bk_seed = v->params.seed;
@@ -962,6 +987,10 @@ static mrp_status render_impl(mrp_volume* v, const mrp_view* w, mrp_render_type 
             if (v->params.tracer_filter) {
                 TRY(ensure_density_texture(v));
                 dt.dens_tex = v->dens_tex;
+                if (v->params.nee_mode == 0) {
+                    TRY(ensure_baked_texture(v));
+                    dt.baked_tex = v->baked_gtex.tex;
+                }
             }
             CU(launch_trace(dt, vd, v->sum3, nullptr, v->first_pos, v->counter, g.sms, v->stream));
             if (last) CU(cudaEventRecord(v->ev_stage[0], v->stream));

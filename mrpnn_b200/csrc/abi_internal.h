@@ -157,6 +157,8 @@ struct mrp_volume {
     // on first use, dropped when the grid changes)
     cudaArray_t dens_arr = nullptr;
     cudaTextureObject_t dens_tex = 0;
+    mrp::GtexLevel baked_gtex;   // the baked NEE grid as a texture (tracer_filter), refilled after each bake
+    bool baked_gtex_ok = false;
     // the pyramid, TR levels and LUT as textures for the fp16-feature gather
     // (gather_filter): allocated on first use, refreshed in place whenever a
     // builder rewrites the linear copy (gtex_dirty: 1 mips, 2 TR, 4 LUT)

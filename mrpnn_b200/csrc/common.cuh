@@ -431,6 +431,10 @@ struct VolumeDev {
     // normalized coordinates) for the frame tracer's free flight, or 0 for
     // the software fetch (mrp_params.tracer_filter).
     cudaTextureObject_t dens_tex;
+    // The baked NEE grid as an fp16 texture (trilinear, clamp, normalized
+    // coordinates) for the frame tracer's NEE lookup under tracer_filter, as
+    // the reference binds it to TR_Mip(0) (core/volume.cu:1687-1693), or 0.
+    cudaTextureObject_t baked_tex;
     // The fp16-feature gather through the texture unit's filters
     // (mrp_params.gather_filter), as the reference samples Mip(i), TR_Mip(i)
     // and _HGLut: mip level 0 (trilinear, border) and TR level 0 (trilinear,

@@ -139,6 +139,27 @@ MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* 
     return density_as<DT>(v, add(m.pos, mul(m.dir, t)));
 }
 
+// The march's runs of empty steps, `while (loop < lim && t <= b_le && t <
+// b_lt) { ++loop; t += e; }`, in closed form.  When e = 1 / res is a power
+// of two and t a multiple of it, every one of those additions is exact (t
+// stays a small integer times e), so the run ends at the first multiple of
+// e past the bounds, or after lim - loop steps: the same t and loop as the
+// additions one by one.  inv_e = res.  False (nothing done) when t is not a
+// multiple of e; the caller then adds step by step.
+MRP_D bool replay_empty(float& t, int& loop, float inv_e, float e, float b_le, float b_lt, int lim) {
+    const float j0 = t * inv_e;   // exact: inv_e is a power of two
+    if (j0 != floorf(j0)) return false;
+    const float cap = 16777216.0f;  // 2^24: beyond any reachable step count
+    const float j_le = floorf(fminf(b_le * inv_e, cap));
+    const float j_lt = ceilf(fminf(b_lt * inv_e, cap)) - 1.0f;
+    const float jm = fminf(j_le, j_lt);
+    int k = jm >= j0 ? (int)(jm - j0) + 1 : 0;
+    k = min(k, max(lim - loop, 0));
+    loop += k;
+    t = (j0 + (float)k) * e;        // exact: an integer below 2^24 times a power of two
+    return true;
+}
+
 // DeterminateEstimatedHit(float& alpha, ...) (core/render.cuh:105-197).
 // pass_rate = exp(-t_step * SMax) is computed once on the host.  DT: the
 // density grid's storage type (void: read from the volume per fetch).
@@ -149,6 +170,9 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
     float t = 0.0f, last_non_empty_t = 0.0f, prob = 1.0f, last_dens = 0.0f;
     float rf = (float)v.res;
     float t_step = fd(2.0f, rf), empty_step = fd(1.0f, rf);
+    // runs of empty steps replay in closed form on power-of-two grids (the
+    // counting copy adds step by step: it tallies every step)
+    const bool pow2 = !tl && (v.res & (v.res - 1)) == 0;
     const MarchRay mr = march_ray(v, pos, dir);
     int loop = 0;
     float t_exit = 3.0e38f;   // beyond it (and within dis) every step reads 0
@@ -177,6 +201,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
         }
         const float t_enter = never ? 3.0e38f : t0;
         if (!never) t_exit = t1;
+        if (pow2) replay_empty(t, loop, rf, empty_step, dis, t_enter, 10000);
         while (loop < 10000 && t <= dis && t < t_enter) {
             ++loop;
             if (tl) tl->steps++;
@@ -240,6 +265,7 @@ MRP_D bool estimated_hit(const VolumeDev& v, float alpha, float pass_rate, f3 po
         // The step read 0 from an empty brick: the following steps that
         // start inside the brick read 0 too and, last_dens being 0, only
         // advance t by empty_step -- replayed as additions alone.
+        if (pow2 && t_brick >= 0.0f) replay_empty(t, loop, rf, empty_step, fminf(t_brick, dis), 3.0e38f, 10000);
         while (t <= t_brick && t <= dis && loop < 10000) {
             ++loop;
             if (tl) tl->steps++;
@@ -883,11 +909,11 @@ MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
     accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
 }
 
-// 128-thread blocks, ten resident per SM (48 registers): a block retires as
+// 128-thread blocks, nine resident per SM (56 registers): a block retires as
 // soon as its slowest ray ends, and march lengths vary from 0 to ~1000 steps.
 constexpr int kHitThreads = 128;
 template <bool COUNT, class DT, bool ENV = false>
-__global__ void __launch_bounds__(kHitThreads, 10) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
+__global__ void __launch_bounds__(kHitThreads, 9) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
     Tally tally;
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
     int npix = w.width * w.height;

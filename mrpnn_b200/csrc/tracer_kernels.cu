@@ -180,7 +180,11 @@ __global__ void __launch_bounds__(128, 8) k_trace(const __grid_constant__ Volume
         p = add(mul(rd, t), p);
         csr = mul(csr, v.scatter_rate);
         float ph = hg(dot(rd, L), w.g);
-        float tr = v.nee_mode ? nee_tr<DT>(v, w, pix, k, &nee_n, p, L) : tex3<true>(v.baked, v.baked_res, p);
+        // NEE: MipTr(0, p) on the baked grid (core/render.cuh:589), through
+        // the texture unit under tracer_filter as the reference's tex3D
+        float tr = v.nee_mode ? nee_tr<DT>(v, w, pix, k, &nee_n, p, L)
+                 : TEX && v.baked_tex ? tex3D<float>(v.baked_tex, p.z + 0.5f, p.y + 0.5f, p.x + 0.5f)
+                                      : tex3<true>(v.baked, v.baked_res, p);
         if (COUNT) tally.lookups++;
         res = add(res, mul(mul(w.light_color, csr), fm(tr, ph)));
         rd = nd;
