@@ -282,6 +282,7 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
             return cleanup(fail(MRP_ERR_CUDA, "event: %s", cudaGetErrorString(e)));
     size_t n = (size_t)res * res * res;
     v->occ_res = (res + (1 << v->occ_shift) - 1) >> v->occ_shift;
+    v->occ2_res = (v->occ_res + 3) / 4;
     size_t nocc = (size_t)v->occ_res * v->occ_res * v->occ_res;
     if ((storage == MRP_STORAGE_FP16 ? (e = mrp::dev_malloc(&v->density_h, n * sizeof(__half)))
                                      : (e = mrp::dev_malloc(&v->density, n * sizeof(float)))) != cudaSuccess ||
@@ -289,6 +290,7 @@ mrp_status mrp_volume_create_ex(int res, mrp_storage storage, mrp_volume** out) 
         (e = mrp::dev_malloc(&v->trs, kTrFloats * sizeof(float))) != cudaSuccess ||
         (e = mrp::dev_malloc(&v->lut, kLutAlloc * sizeof(float))) != cudaSuccess ||
         (e = mrp::dev_malloc(&v->occ, nocc)) != cudaSuccess || (e = mrp::dev_malloc(&v->mip_occ, kMipOccBytes)) != cudaSuccess ||
+        (e = mrp::dev_malloc(&v->occ2, (size_t)v->occ2_res * v->occ2_res * v->occ2_res)) != cudaSuccess ||
         (e = mrp::dev_malloc(&v->d_maxbits, sizeof(int))) != cudaSuccess ||
         (e = mrp::dev_malloc(&v->d_bounds, 6 * sizeof(int))) != cudaSuccess ||
         (e = mrp::dev_malloc(&v->mips_pad, kPadLevelFloats * sizeof(float))) != cudaSuccess ||
@@ -312,7 +314,7 @@ mrp_status mrp_volume_destroy(mrp_volume* v) {
     if (v->stream_copy) cudaStreamSynchronize(v->stream_copy);
     mrp::dev_free(v->accum_alt);
     mrp::dev_free(v->density); mrp::dev_free(v->density_h); mrp::dev_free(v->mips); mrp::dev_free(v->trs); mrp::dev_free(v->lut); mrp::dev_free(v->baked);
-    mrp::dev_free(v->occ); mrp::dev_free(v->mip_occ); mrp::dev_free(v->d_maxbits); mrp::dev_free(v->d_bounds); mrp::dev_free(v->mips_pad); mrp::dev_free(v->trs_pad); mrp::dev_free(v->mip_tr); mrp::dev_free(v->pad_pair); mrp::dev_free(v->accum); mrp::dev_free(v->sum3); mrp::dev_free(v->first_pos);
+    mrp::dev_free(v->occ); mrp::dev_free(v->occ2); mrp::dev_free(v->mip_occ); mrp::dev_free(v->d_maxbits); mrp::dev_free(v->d_bounds); mrp::dev_free(v->mips_pad); mrp::dev_free(v->trs_pad); mrp::dev_free(v->mip_tr); mrp::dev_free(v->pad_pair); mrp::dev_free(v->accum); mrp::dev_free(v->sum3); mrp::dev_free(v->first_pos);
     mrp::dev_free(v->counter);
     mrp::dev_free(v->hdri);
     drop_density_texture(v);
@@ -534,6 +536,7 @@ mrp_status mrp_volume_update(mrp_volume* v, int process_mips) {
     }
     if (v->density_h) CU(launch_occupancy(v->density_h, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
     else CU(launch_occupancy(v->density, R, v->occ_shift, v->occ_res, v->occ, g.sms, v->stream));
+    CU(launch_occupancy_coarse(v->occ, v->occ_res, v->occ2, g.sms, v->stream));
     {
         const int init[6] = {R, R, R, -1, -1, -1};
         CU(cudaMemcpyAsync(v->d_bounds, init, sizeof init, cudaMemcpyHostToDevice, v->stream));

@@ -109,6 +109,8 @@ struct mrp_volume {
     uint8_t* occ = nullptr;
     uint8_t* mip_occ = nullptr;   // bricks of mip levels 0..kOccMips-1
     int occ_shift = 3, occ_res = 0;
+    uint8_t* occ2 = nullptr;      // coarse occupancy (4^3 bricks each), built with occ
+    int occ2_res = 0;
     int* d_maxbits = nullptr;
     float* mips_pad = nullptr;    // padded mips 5..7 (pad_offset layout), built with the pyramid
     float* trs_pad = nullptr;     // padded TR levels 4..6, built with the TR levels
@@ -189,6 +191,8 @@ struct mrp_volume {
         d.occ = occ;
         d.occ_shift = occ_shift;
         d.occ_res = occ_res;
+        d.occ2 = occ2;
+        d.occ2_res = occ2_res;
         d.scatter_rate = {params.scatter_rate[0], params.scatter_rate[1], params.scatter_rate[2]};
         d.tr_scale = params.tr_scale;
         d.sky = {params.sky[0] * params.env_exp, params.sky[1] * params.env_exp, params.sky[2] * params.env_exp};

@@ -396,6 +396,8 @@ struct VolumeDev {
     int baked_res;
     const uint8_t* occ;     // 1 where a brick (or its trilinear apron) holds density != 0
     int occ_shift;          // brick edge = 1 << occ_shift voxels
+    const uint8_t* occ2;    // coarse bricks of 4^3 bricks (launch_occupancy_coarse), or null
+    int occ2_res;           // coarse bricks per axis
     int occ_res;            // bricks per axis
     f3 scatter_rate;
     float tr_scale;

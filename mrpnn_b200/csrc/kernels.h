@@ -20,6 +20,8 @@ cudaError_t launch_max_density(const float* d, size_t n, int* out_bits, int sms,
 cudaError_t launch_max_density(const __half* d, size_t n, int* out_bits, int sms, cudaStream_t s);
 cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
 cudaError_t launch_occupancy(const __half* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s);
+// Coarse bricks (edge 4 bricks) of an occupancy grid of nb^3 bricks: (nb+3)/4 per axis.
+cudaError_t launch_occupancy_coarse(const uint8_t* occ, int nb, uint8_t* coarse, int sms, cudaStream_t s);
 // VolumeDev::pad_pair from the padded mips and TR levels (kPadLevelFloats pairs).
 cudaError_t launch_pair_padded(const float* mips_pad, const float* trs_pad, float2* out, cudaStream_t s);
 // VolumeDev::mip_tr from the pyramid and the TR levels (mip_tr_offset(5) pairs).

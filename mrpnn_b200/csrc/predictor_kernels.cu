@@ -119,8 +119,10 @@ MRP_D float brick_exit(float c, float sR, float isR, int b, int sh) {
     return 3.0e38f;
 }
 // *t_brick: when the brick proves the value 0 and the base voxel lies inside
-// the grid, the t up to which the ray stays in that brick (the march's next
-// steps there read 0 as well); else -1.
+// the grid, the t up to which the ray stays in that brick -- or in its
+// coarse brick of 4^3 bricks, when that one is empty as well -- (the march's
+// next steps there read 0 as well); else -1.  The coarse brick is looked up
+// only after an empty brick, so steps inside the cloud pay nothing for it.
 template <class DT>
 MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* tl, float* t_brick) {
     const int R1 = v.res - 1, sh = v.occ_shift, nb = v.occ_res;
@@ -130,9 +132,15 @@ MRP_D float density_skip(const VolumeDev& v, const MarchRay& m, float t, Tally* 
     const int x = min(max(xi, 0), R1) >> sh, y = min(max(yi, 0), R1) >> sh, z = min(max(zi, 0), R1) >> sh;
     *t_brick = -1.0f;
     if (__ldg(v.occ + (x * nb + y) * nb + z) == 0) {
-        if ((unsigned)xi <= (unsigned)R1 && (unsigned)yi <= (unsigned)R1 && (unsigned)zi <= (unsigned)R1)
-            *t_brick = fminf(brick_exit(m.c.x, m.sR.x, m.isR.x, x, sh),
-                             fminf(brick_exit(m.c.y, m.sR.y, m.isR.y, y, sh), brick_exit(m.c.z, m.sR.z, m.isR.z, z, sh)));
+        if ((unsigned)xi <= (unsigned)R1 && (unsigned)yi <= (unsigned)R1 && (unsigned)zi <= (unsigned)R1) {
+            int bx = x, by = y, bz = z, bs = sh;
+            const int nc = v.occ2_res;
+            if (v.occ2 && __ldg(v.occ2 + ((x >> 2) * nc + (y >> 2)) * nc + (z >> 2)) == 0) {
+                bx = x >> 2; by = y >> 2; bz = z >> 2; bs = sh + 2;
+            }
+            *t_brick = fminf(brick_exit(m.c.x, m.sR.x, m.isR.x, bx, bs),
+                             fminf(brick_exit(m.c.y, m.sR.y, m.isR.y, by, bs), brick_exit(m.c.z, m.sR.z, m.isR.z, bz, bs)));
+        }
         return 0.0f;
     }
     if (tl) tl->fetches++;

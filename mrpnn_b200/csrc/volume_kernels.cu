@@ -220,6 +220,23 @@ __global__ void k_occupancy(const T* __restrict__ d, int R, int shift, int nb, u
     }
 }
 
+// Coarse bricks of 4^3 occupancy bricks (edge 4B): coarse brick C is empty
+// when the 64 bricks 4C..4C+3 per axis are.  Their aprons together cover
+// voxels [4CB - 1, 4CB + 4B + 1], the coarse brick's own apron, so a zero
+// coarse brick carries the same guarantee as a zero brick, over its span.
+__global__ void k_occupancy_coarse(const uint8_t* __restrict__ occ, int nb, int nc, uint8_t* __restrict__ out) {
+    const int total = nc * nc * nc;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+        const int cz = c % nc, cy = (c / nc) % nc, cx = c / (nc * nc);
+        int any = 0;
+        for (int k = 0; k < 64 && !any; ++k) {
+            const int x = 4 * cx + k / 16, y = 4 * cy + (k / 4) % 4, z = 4 * cz + k % 4;
+            if (x < nb && y < nb && z < nb) any = occ[(x * nb + y) * nb + z];
+        }
+        out[c] = any ? 1 : 0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Fill_TR (core/volume.cu:1535-1560): transmittance of TR level `level`
 // (res 128>>level) marched 128 steps toward the light through density level
@@ -445,6 +462,11 @@ cudaError_t launch_occupancy(const float* d, int R, int shift, int nb, uint8_t* 
 }
 cudaError_t launch_occupancy(const __half* d, int R, int shift, int nb, uint8_t* occ, int sms, cudaStream_t s) {
     return occupancy_t(d, R, shift, nb, occ, sms, s);
+}
+cudaError_t launch_occupancy_coarse(const uint8_t* occ, int nb, uint8_t* coarse, int sms, cudaStream_t s) {
+    const int nc = (nb + 3) / 4, total = nc * nc * nc;
+    k_occupancy_coarse<<<grid_for((size_t)total, 128, sms), 128, 0, s>>>(occ, nb, nc, coarse);
+    return cudaGetLastError();
 }
 cudaError_t launch_tr_level(float* out, int res, const float* src, const uint8_t* src_occ, float alpha,
                             const float L[3], int sms, cudaStream_t s) {
