@@ -349,6 +349,12 @@ def run_tracer(args, local):
     vol.SetTracerFilter(False)
     t_hw = float(np.mean(tr_hw))
     ach_hw = alg / (t_hw / 1000.0) / 1e9
+    # the level the lookups are served from: the 8 MiB volume stays in L2
+    # (and mostly L1); its ceiling is the measured rate of L2 reads
+    l2 = M.api.measure_l2_rate()
+    res["roofline"]["l2"] = {"peak": l2, "unit": "GB/s", "frac": ach / l2, "frac_hw_filter": ach_hw / l2,
+                             "note": "same algorithmic bytes against the measured L2 read rate "
+                                     "(mrp_measure_l2_rate, 64 MiB L2-resident buffer, L1 bypassed)"}
     res["hw_filter"] = {"ms_per_frame": float(np.mean(ms_hw)), "trace_kernel_ms": t_hw,
                         "samples_per_s": n * n * TRACER["spp"] / (float(np.mean(ms_hw)) / 1000.0),
                         "roofline": {"bound": "hbm", "achieved": ach_hw, "peak": hbm, "unit": "GB/s",

@@ -379,6 +379,11 @@ mrp_status mrp_tc_gemm_check(int fp8, const float* A, const float* B, int n, int
  * the ceiling of the stencil gather's texel reads, which hit L1.  No
  * counterpart in the reference (a measurement of this GPU). */
 mrp_status mrp_measure_l1_rate(float* gbs);
+/* The rate (GB/s) at which this GPU's SMs read 16-byte words that bypass L1
+ * from a 64 MiB buffer resident in L2: the ceiling the bench states the
+ * tracer's L2-resident density reads against.  No counterpart in the
+ * reference; allocates and frees its buffer. */
+mrp_status mrp_measure_l2_rate(float* gbs);
 
 /* One MRPNN launch of mrp_render (launch index view->frame_offset, no
  * running mean) that also returns the intermediates of NNPredict per pixel:

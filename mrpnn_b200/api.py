@@ -107,6 +107,7 @@ _SIGS = {
     "mrp_first_hit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "mrp_tc_gemm_check": ([C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "mrp_measure_l1_rate": ([C.POINTER(C.c_float)], C.c_int),
+    "mrp_measure_l2_rate": ([C.POINTER(C.c_float)], C.c_int),
     "mrp_render_predict_debug": ([C.c_void_p, C.POINTER(View), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "mrp_hdri_file_read": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t], C.c_int),
     "mrp_volume_set_hdri": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
@@ -315,6 +316,14 @@ def measure_l1_rate():
     r = C.c_float()
     _check(lib().mrp_measure_l1_rate(C.byref(r)))
     return r.value
+
+
+def measure_l2_rate():
+    """mrp_measure_l2_rate: GB/s of 16-byte L2 reads (L1 bypassed) on this GPU."""
+    _ensure_init()
+    r = C.c_float()
+    _check(lib().mrp_measure_l2_rate(C.byref(r)))
+    return float(r.value)
 
 
 def tc_gemm_check(A, B, fp8=False):

@@ -805,7 +805,7 @@ mrp_status ensure_predictor_buffers(mrp_volume* v, size_t npix) {
     if (v->rec_cap >= npix) return MRP_OK;
     mrp::dev_free(v->rec_count); mrp::dev_free(v->rec_pix); mrp::dev_free(v->rec_f); mrp::dev_free(v->feat);
     v->rec_count = nullptr; v->rec_pix = nullptr; v->rec_f = nullptr; v->feat = nullptr; v->rec_cap = 0;
-    CU(mrp::dev_malloc(&v->rec_count, sizeof(int)));
+    CU(mrp::dev_malloc(&v->rec_count, 2 * sizeof(int)));   // records, the march's pixel chunks
     CU(mrp::dev_malloc(&v->rec_pix, npix * sizeof(int)));
     CU(mrp::dev_malloc(&v->rec_f, npix * 16 * sizeof(float)));
     CU(mrp::dev_malloc(&v->feat, tiled_feature_floats(npix) * sizeof(float)));

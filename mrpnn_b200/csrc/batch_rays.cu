@@ -105,7 +105,7 @@ mrp_status mrp_get_radiances(mrp_volume* v, const float* ori, const float* dir, 
         vd.ray_dir = d_dir;
         int *rc, *rp;
         float *rf, *feat;
-        CU(S.scratch(sizeof(int), (void**)&rc));
+        CU(S.scratch(2 * sizeof(int), (void**)&rc));   // records, the march's pixel chunks
         CU(S.scratch((size_t)n * sizeof(int), (void**)&rp));
         CU(S.scratch((size_t)n * 16 * sizeof(float), (void**)&rf));
         CU(S.scratch(tiled_feature_floats(n) * sizeof(float), (void**)&feat));

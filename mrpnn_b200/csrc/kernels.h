@@ -65,7 +65,7 @@ cudaError_t launch_first_hit(const VolumeDev& v, const float* ori, const float* 
 //   launch_gather_rec  stencil features of the hit pixels (tiled layout)
 //   launch_mlp_rec_*   network on the features, result at each pixel
 struct HitRecords {
-    int* count;     // number of records (device)
+    int* count;     // [0] number of records, [1] the march's work counter (device; launch_hit zeroes both)
     int* pix;       // [cap] pixel index of each record
     float* f;       // [16][cap]: hit xyz, X, Y, Z, LX, gamma
     size_t cap;     // >= pixels of the launch

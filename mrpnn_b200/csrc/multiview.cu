@@ -42,7 +42,7 @@ mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* 
     // buffers (kept on the volume between calls)
     MultiViewBuffers& B = v->mv;
     if (B.cap_views < kTcMaxSegments) {
-        CU(mrp::dev_malloc(&B.rec_count, kTcMaxSegments * sizeof(int)));
+        CU(mrp::dev_malloc(&B.rec_count, 2 * kTcMaxSegments * sizeof(int)));   // per view: records, pixel chunks
         CU(mrp::dev_malloc(&B.d_segs, kTcMaxSegments * sizeof(TcSegment)));
         B.cap_views = kTcMaxSegments;
     }
@@ -69,7 +69,7 @@ mrp_status mrp_render_views(mrp_volume* v, const mrp_view* views, int n, float* 
     for (int i = 0; i < n; ++i) {
         size_t np = (size_t)views[i].width * views[i].height;
         // records of view i: SoA arrays with its own capacity np
-        HitRecords rec{B.rec_count + i, B.rec_pix + pix_off[i], B.rec_f + 16 * pix_off[i], np};
+        HitRecords rec{B.rec_count + 2 * i, B.rec_pix + pix_off[i], B.rec_f + 16 * pix_off[i], np};
         ViewDev vd = make_view(v, &views[i], views[i].frame_offset, 0);
         float4* acc = B.accum + pix_off[i];
         float* ft = B.feat + feat_off[i];

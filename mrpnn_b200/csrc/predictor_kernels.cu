@@ -917,13 +917,14 @@ MRP_D void running_mean(float4* accum, int pix, int mean_k, float4 res) {
     accum[pix] = make_float4(lerp(a.x, res.x, rate), lerp(a.y, res.y, rate), lerp(a.z, res.z, rate), lerp(a.w, res.w, rate));
 }
 
-// 128-thread blocks, nine resident per SM (56 registers): a block retires as
-// soon as its slowest ray ends, and march lengths vary from 0 to ~1000 steps.
+// 128-thread blocks, eight resident per SM (64 registers), each warp taking
+// 32 pixels at a time: march lengths vary from 0 to ~1000 steps.
 constexpr int kHitThreads = 128;
-template <bool COUNT, class DT, bool ENV = false>
-__global__ void __launch_bounds__(kHitThreads, 9) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
+// One warp's 32 pixels (lane = pixel pix); every lane of the warp calls it.
+template <bool COUNT, class DT, bool ENV>
+MRP_D void hit_pixels(const VolumeDev& v, const ViewDev& w, const HitRecords& rec, float4* __restrict__ accum,
+                      int pix) {
     Tally tally;
-    int pix = blockIdx.x * blockDim.x + threadIdx.x;
     int npix = w.width * w.height;
     bool valid = pix < npix && pixel_selected(w, pix / w.width, pix % w.width);
     bool active = false;
@@ -972,6 +973,22 @@ __global__ void __launch_bounds__(kHitThreads, 9) k_hit(VolumeDev v, ViewDev w, 
                       gamma_of(PixelFrame{hit, X, Y, Z, LX, mk3(0, 0, 0), 0.0f, 0.0f})};
 #pragma unroll
     for (int k = 0; k < 16; ++k) f[k * cap] = vals[k];
+}
+// Persistent warps: each takes the next 32 consecutive pixels from a
+// counter (rec.count[1]) as soon as its previous 32 rays have ended, so a
+// long march holds one warp, not a whole block, and the SMs stay full until
+// the last pixels are handed out.
+template <bool COUNT, class DT, bool ENV = false>
+__global__ void __launch_bounds__(kHitThreads, 8) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
+    const int nchunks = (w.width * w.height + 31) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(rec.count + 1, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= nchunks) return;
+        hit_pixels<COUNT, DT, ENV>(v, w, rec, accum, (c << 5) + (int)lane);
+    }
 }
 
 MRP_D PixelFrame record_frame(const HitRecords& rec, int r, f3 L, float g, float alpha) {
@@ -1061,9 +1078,14 @@ cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float
 cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, float4* accum, cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(rec.count, 0, sizeof(int), s);
+    cudaError_t e = cudaMemsetAsync(rec.count, 0, 2 * sizeof(int), s);   // records, pixel chunks handed out
     if (e != cudaSuccess) return e;
-    const int blocks = (n + kHitThreads - 1) / kHitThreads;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    const int need = (n + kHitThreads - 1) / kHitThreads;
+    const int blocks = need < sms * 8 ? need : sms * 8;   // eight resident per SM
     // one copy of the march per counting mode and density storage type, and
     // for volumes with an environment map
     if (v.hdri) {

@@ -31,6 +31,25 @@ __global__ void __launch_bounds__(kProbeThreads) k_l1_probe(const float2* __rest
     if (ax + ay == 1234.5f) out[blockIdx.x] = ax;   // keeps the loads; never true for the zeroed buffer
 }
 
+// The L2 counterpart: every thread streams 16-byte loads that bypass L1
+// (ld.global.cg) over a buffer that fits L2, the rate at which the tracer's
+// L2-resident density volume can be read at best.
+constexpr size_t kL2ProbeBytes = 64ull << 20;
+__global__ void __launch_bounds__(kProbeThreads) k_l2_probe(const float4* __restrict__ buf, size_t n, int passes,
+                                                            float* out) {
+    float ax = 0.0f;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+#pragma unroll 1
+    for (int p = 0; p < passes; ++p) {
+#pragma unroll 4
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const float4 v = __ldcg(buf + i);
+            ax += v.x + v.y + v.z + v.w;
+        }
+    }
+    if (ax == 1234.5f) out[blockIdx.x] = ax;   // keeps the loads; never true for the zeroed buffer
+}
+
 }  // namespace
 
 extern "C" {
@@ -64,6 +83,38 @@ mrp_status mrp_measure_l1_rate(float* gbs) {
     CU(e);
     const double bytes = (double)blocks * kProbeThreads * iters * 8 * sizeof(float2);
     *gbs = (float)(bytes / (ms * 1e-3) / 1e9);
+    return MRP_OK;
+}
+
+mrp_status mrp_measure_l2_rate(float* gbs) {
+    TRY(need_init());
+    if (!gbs) return fail(MRP_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g.mu);
+    const int blocks = g.sms * 8, passes = 8;
+    const size_t n = kL2ProbeBytes / sizeof(float4);
+    float4* buf = nullptr;
+    float* out = nullptr;
+    CU(mrp::dev_malloc(&buf, kL2ProbeBytes));
+    cudaError_t e = mrp::dev_malloc(&out, blocks * sizeof(float));
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaMemsetAsync(buf, 0, kL2ProbeBytes, g.stream);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    float ms = 0.0f;
+    for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {   // the first run brings the buffer into L2
+        cudaEventRecord(a, g.stream);
+        k_l2_probe<<<blocks, kProbeThreads, 0, g.stream>>>(buf, n, passes, out);
+        e = cudaGetLastError();
+        cudaEventRecord(b, g.stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    mrp::dev_free(buf);
+    mrp::dev_free(out);
+    CU(e);
+    *gbs = (float)((double)kL2ProbeBytes * passes / (ms * 1e-3) / 1e9);
     return MRP_OK;
 }
 

@@ -66,7 +66,7 @@ struct Slot {
 };
 
 size_t slot_bytes(size_t npix) {
-    return kTrFloats * sizeof(float) + sizeof(int) + npix * (sizeof(int) + 16 * sizeof(float) + sizeof(float4)) +
+    return kTrFloats * sizeof(float) + 2 * sizeof(int) + npix * (sizeof(int) + 16 * sizeof(float) + sizeof(float4)) +
            tiled_feature_floats(npix) * sizeof(float);
 }
 constexpr size_t kLutBytes = kLutAlloc * sizeof(float);   // the LUT and its lut_dirs table
@@ -199,7 +199,7 @@ struct mrp_server {
         free_buffers(s);
         cudaError_t e;
         if ((e = mrp::dev_malloc_async(&s.trs, kTrFloats * sizeof(float), s.stream)) != cudaSuccess ||
-            (e = mrp::dev_malloc_async(&s.rec_count, sizeof(int), s.stream)) != cudaSuccess ||
+            (e = mrp::dev_malloc_async(&s.rec_count, 2 * sizeof(int), s.stream)) != cudaSuccess ||
             (e = mrp::dev_malloc_async(&s.rec_pix, npix * sizeof(int), s.stream)) != cudaSuccess ||
             (e = mrp::dev_malloc_async(&s.rec_f, npix * 16 * sizeof(float), s.stream)) != cudaSuccess ||
             (e = mrp::dev_malloc_async(&s.feat, tiled_feature_floats(npix) * sizeof(float), s.stream)) != cudaSuccess ||

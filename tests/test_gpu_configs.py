@@ -65,6 +65,43 @@ def test_headline_frame_fp32_matches_oracle():
     assert ok.mean() >= 0.999, (ok.mean(), px[~ok][:5])
 
 
+# the tensor-core forms against the FP32 drop-in on the same frame
+# (tests/test_gpu_tensor_core.py states the same bounds against FP64)
+TC_REL_RMS = {"BF16": 0.02, "FP8": 0.08}
+
+
+@pytest.mark.parametrize("prec", ["BF16", "FP8"])
+def test_headline_frame_tensor_core_forms(prec):
+    """The precision forms on the headline frame (1024x1024 over the 512^3
+    cloud): the same pixels hit at the same distances as the FP32 form (the
+    march is shared and exact), and the radiance of the hit pixels within the
+    form's relative RMS of the FP32 form's, with the fp16 features of the
+    texture-unit gather (the default) and of the software gather."""
+    import mrpnn_b200 as M
+    sc = Scene(R=512, seed=1, freq=6.0, alpha=64.0, g=0.857, sr=0.99, sky=0.05)
+    W = 1024
+    ori, up, right = view_frame()
+
+    def frame():
+        return sc.vol.Render((W, W), ori, up, right, LIGHT, M.VolumeRender.MRPNN, sc.g, sc.alpha, sampleNum=1,
+                             seed=3).reshape(-1, 4)
+    ref = frame()
+    hit = ref[:, 3] > 0
+    sc.vol.SetPrecision(getattr(M, prec))
+    try:
+        for hw in (True, False):
+            sc.vol.SetGatherFilter(hw)
+            got = frame()
+            np.testing.assert_array_equal(got[:, 3], ref[:, 3])
+            rms = np.sqrt(np.mean((got[hit, :3] - ref[hit, :3]) ** 2)) / np.sqrt(np.mean(ref[hit, :3] ** 2))
+            print(f"{prec} gather_filter={int(hw)}: rel RMS vs FP32 {rms:.4f} over {hit.sum()} hit pixels")
+            assert rms < TC_REL_RMS[prec]
+            np.testing.assert_array_equal(got[~hit], ref[~hit])   # sky pixels: the same constant
+    finally:
+        sc.vol.SetPrecision(M.FP32)
+        sc.vol.SetGatherFilter(True)
+
+
 def test_tracer_workload_zscore():
     import mrpnn_b200 as M
     sc = Scene(R=128, seed=0, freq=4.0, alpha=64.0, g=0.857, sr=0.99, sky=0.05, bake_res=768)
