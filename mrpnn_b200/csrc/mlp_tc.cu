@@ -834,6 +834,10 @@ __global__ void __launch_bounds__(kGroups * kGroupThreads, 1) k_mlp_tc(const __g
         int tile = tile_slot[G.g];
         group_bar(G.g);
         if (tile >= total_tiles || (st & kStFailed)) break;
+        // staged records from the last tile down: the gather wrote its
+        // features in record order just before, so the last tiles' features
+        // are still in L2 when the first groups ask for them
+        if (STAGED) tile = total_tiles - 1 - tile;
         float o[3];
         if (STAGED) {
             int q = 0;
