@@ -926,7 +926,7 @@ MRP_D void hit_pixels(const VolumeDev& v, const ViewDev& w, const HitRecords& re
                       int pix) {
     Tally tally;
     int npix = w.width * w.height;
-    bool valid = pix < npix && pixel_selected(w, pix / w.width, pix % w.width);
+    bool valid = pix >= 0 && pix < npix && pixel_selected(w, pix / w.width, pix % w.width);
     bool active = false;
     f3 hit = mk3(0, 0, 0), X, Y, Z, LX;
     if (valid) {
@@ -974,20 +974,27 @@ MRP_D void hit_pixels(const VolumeDev& v, const ViewDev& w, const HitRecords& re
 #pragma unroll
     for (int k = 0; k < 16; ++k) f[k * cap] = vals[k];
 }
-// Persistent warps: each takes the next 32 consecutive pixels from a
+// Persistent warps: each takes the next tile of 8 x 4 pixels from a
 // counter (rec.count[1]) as soon as its previous 32 rays have ended, so a
 // long march holds one warp, not a whole block, and the SMs stay full until
-// the last pixels are handed out.
+// the last tiles are handed out; the rays of a square-ish tile march more
+// alike than 32 pixels of a row.  (Explicit rays, a width x 1 launch, come
+// 32 in a row.)
 template <bool COUNT, class DT, bool ENV = false>
 __global__ void __launch_bounds__(kHitThreads, 8) k_hit(VolumeDev v, ViewDev w, HitRecords rec, float4* __restrict__ accum) {
-    const int nchunks = (w.width * w.height + 31) >> 5;
-    const unsigned lane = threadIdx.x & 31;
+    const int tx = w.height > 1 ? (w.width + 7) >> 3 : (w.width + 31) >> 5;
+    const int ty = w.height > 1 ? (w.height + 3) >> 2 : 1;
+    const int nchunks = tx * ty;
+    const int lane = (int)(threadIdx.x & 31);
+    const int lx = w.height > 1 ? lane & 7 : lane, ly = w.height > 1 ? lane >> 3 : 0;
+    const int sx = w.height > 1 ? 8 : 32, sy = w.height > 1 ? 4 : 1;
     for (;;) {
         int c = 0;
         if (lane == 0) c = atomicAdd(rec.count + 1, 1);
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= nchunks) return;
-        hit_pixels<COUNT, DT, ENV>(v, w, rec, accum, (c << 5) + (int)lane);
+        const int col = (c % tx) * sx + lx, row = (c / tx) * sy + ly;
+        hit_pixels<COUNT, DT, ENV>(v, w, rec, accum, col < w.width && row < w.height ? row * w.width + col : -1);
     }
 }
 
