@@ -439,11 +439,15 @@ def run_serving(args, local):
     srv = M.Server(memory_budget=SERVE["budget"], max_slots=args.serve_slots, precision=M.BF16,
                    slot_pixels=1920 * 1080)
     try:
-        # warm-up: one request of each image size (LUT, slot buffers)
+        # warm-up: one request of each image size (LUT, slot buffers), then
+        # one small request per volume (its texture copy for the gather)
         for k, (Wq, Hq) in enumerate(SERVE["images"]):
             v = vols[k][0]
             vw = v.make_view((Wq, Hq), *view_vectors(), light(), SCENE["g"], vols[k][2])
             srv.wait(srv.submit(v, vw, pool[k][:Wq * Hq * 4]))
+        for k, (v, _, a) in enumerate(vols):
+            vw = v.make_view((64, 64), *view_vectors(), light(), SCENE["g"], a)
+            srv.wait(srv.submit(v, vw, pool[k % len(pool)][:64 * 64 * 4]))
         tickets = [None] * n_req
         done = [False] * n_req
         t_start = time.perf_counter()

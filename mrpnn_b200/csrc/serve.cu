@@ -573,7 +573,8 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
     if (cfg.precision != MRP_FP32 && cfg.precision != MRP_BF16 && cfg.precision != MRP_FP8)
         return fail(MRP_ERR_INVALID, "unknown precision %d", (int)cfg.precision);
     if (cfg.slot_pixels > (1ull << 26)) return fail(MRP_ERR_INVALID, "slot_pixels %zu too large", cfg.slot_pixels);
-    if (cfg.slot_pixels && (slot_bytes(cfg.slot_pixels) + kLutBytes) * (size_t)cfg.max_slots > cfg.memory_budget)
+    if (cfg.slot_pixels && (slot_bytes(cfg.slot_pixels) + kLutBytes + (cfg.precision != MRP_FP32 ? tr_tex_bytes() : 0)) *
+                                   (size_t)cfg.max_slots > cfg.memory_budget)
         return fail(MRP_ERR_BUDGET, "%d slots of %zu pixels exceed the budget of %zu bytes", cfg.max_slots,
                     cfg.slot_pixels, cfg.memory_budget);
     std::unique_ptr<mrp_server> S(new mrp_server());
@@ -622,8 +623,11 @@ mrp_status mrp_serve_open(const mrp_serve_config* cfg_in, mrp_server** out) {
         }
     }
     if (cfg.slot_pixels) {
+        // slots sized at open also get their texture copies now: array
+        // allocations are synchronous and would stall the worker mid-stream
         for (Slot& s : S->slots)
-            if ((e = S->grow(s, cfg.slot_pixels)) != cudaSuccess)
+            if ((e = S->grow(s, cfg.slot_pixels)) != cudaSuccess ||
+                (S->tex_mode && (e = S->ensure_tr_textures(s)) != cudaSuccess))
                 return cleanup(fail(MRP_ERR_OOM, "slot buffers: %s", cudaGetErrorString(e)));
         for (Slot& s : S->slots)
             if ((e = cudaStreamSynchronize(s.stream)) != cudaSuccess)
