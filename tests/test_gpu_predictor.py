@@ -256,3 +256,37 @@ def test_fp16_features(scene, prec, hw):
         # software filter's beyond fp16 rounding
         assert (err > 2e-3 * np.abs(r_feat[hit]) + 2e-5).any()
     np.testing.assert_array_equal(rgba.reshape(W, W, 4), img)
+
+
+def test_texture_gather_follows_updates():
+    """The texture copies of the BF16 gather are refreshed whenever a builder
+    rewrites the linear levels: after a change of light (TR levels), of g (the
+    LUT) and of the volume's data (pyramid), a render equals the render of a
+    fresh volume that never saw the earlier state, bit for bit."""
+    import mrpnn_b200 as M
+    M.init()
+    ori, up, right = view_frame()
+    W = 64
+    L2 = np.array([-0.5, 0.7, 0.2], np.float32)
+    L2 = (L2 / np.float32(np.linalg.norm(L2))).astype(np.float32)
+
+    def fresh(seed, L, g):
+        v = M.VolumeRender(64)
+        v.generate_fbm(seed, 4.0)
+        v.Update()
+        v.SetScatterRate(0.99)
+        v.SetSky(0.05)
+        v.SetPrecision(M.BF16)
+        return v, v.Render((W, W), ori, up, right, L, M.VolumeRender.MRPNN, g, 64.0, sampleNum=1, seed=5)
+
+    v, first = fresh(0, LIGHT, 0.857)
+    for seed, L, g in ((0, L2, 0.857), (0, L2, 0.5), (7, L2, 0.5)):
+        if seed != 0:
+            v.generate_fbm(seed, 4.0)
+            v.Update()
+        got = v.Render((W, W), ori, up, right, L, M.VolumeRender.MRPNN, g, 64.0, sampleNum=1, seed=5)
+        _, want = fresh(seed, L, g)
+        assert (want[..., 3] > 0).sum() > 100
+        np.testing.assert_array_equal(got, want)
+    assert not np.array_equal(first, got)
+
