@@ -220,8 +220,14 @@ mrp_status mrp_load_model(const char* path) {
     if (halton_perms(m, perm) != MRP_OK) return fail(MRP_ERR_IO, "%s: %s", path, t_err.c_str());
     CU(set_stencil_tables(st));
     CU(set_halton_permutations(perm));
-    if (!g.d_weights) CU(mrp::dev_malloc(&g.d_weights, sizeof(float) * kWeightCount));
-    CU(cudaMemcpy(g.d_weights, w.data(), sizeof(float) * kWeightCount, cudaMemcpyHostToDevice));
+    std::vector<float> wd(kWeightCountDev, 0.0f);
+    std::copy(w.begin(), w.end(), wd.begin());
+    for (int j = 0; j < 128; ++j)
+        for (int o = 0; o < 64; ++o) wd[kLC1T + j * 64 + o] = w[kLC1W + o * 128 + j];
+    for (int j = 0; j < 75; ++j)
+        for (int o = 0; o < 16; ++o) wd[kFin1T + j * 16 + o] = w[kLSEFin1W + o * 75 + j];
+    if (!g.d_weights) CU(mrp::dev_malloc(&g.d_weights, sizeof(float) * kWeightCountDev));
+    CU(cudaMemcpy(g.d_weights, wd.data(), sizeof(float) * kWeightCountDev, cudaMemcpyHostToDevice));
     CU(tc_prepare_weights(w.data(), g.tc));
     g.tc.d_fp32 = g.d_weights;
     g.model = std::move(m);

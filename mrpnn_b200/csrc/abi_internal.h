@@ -39,7 +39,7 @@ struct Lib {
     int sms = 148;
     cudaStream_t stream = nullptr;   // for handle-less calls
     std::map<std::string, std::vector<float>> model;
-    float* d_weights = nullptr;      // packed fp32 weights (common.cuh layout)
+    float* d_weights = nullptr;      // packed fp32 weights + transposed copies (common.cuh layout, kWeightCountDev)
     std::vector<float> h_weights;
     TcWeights tc;                    // tensor-core weight images
     // scratch for handle-less parity calls

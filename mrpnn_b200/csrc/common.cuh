@@ -644,5 +644,10 @@ constexpr int lxb(int k) { return kLXk + k * 272 + 256; }
 constexpr int kLX12W = kLXk + 12 * 272, kLX12B = kLX12W + 16;
 constexpr int kWeightCount = kLX12B + 1;
 static_assert(kWeightCount == 49673, "packed weight count must match core/NNWeight.cuh");
+// The device copy appends two transposed copies for the FP32 network:
+// LC1W as [128][64] and LSEFin1W as [75][16] (16-byte aligned rows).
+constexpr int kLC1T = (kWeightCount + 3) / 4 * 4;
+constexpr int kFin1T = kLC1T + 8192;
+constexpr int kWeightCountDev = kFin1T + 1200;
 
 }  // namespace mrp

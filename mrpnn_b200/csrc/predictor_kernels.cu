@@ -625,16 +625,14 @@ MRP_D void gather(const VolumeDev& v, const PixelFrame& f, float* out, int strid
     *gamma = gamma_of(f);
 }
 
-// Feature sources of the MLP: a block asks for its slice [FROM, FROM+W) of
-// the three channels just before it uses it, so no pixel ever holds all 576.
+// Feature sources of the MLP: a block asks for one channel's slice
+// [FROM, FROM+W) just before it uses it, so no pixel ever holds all 576.
 struct GlobalFeatures {
     const float* x;   // channel c at x[c * 192 + i]
     template <int FROM, int W>
-    MRP_D void load(float (&xs)[3][32]) const {
+    MRP_D void load(int c, float (&xs)[32]) const {
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int i = 0; i < W; ++i) xs[c][i] = __ldg(x + c * 192 + FROM + i);
+        for (int i = 0; i < W; ++i) xs[i] = __ldg(x + c * 192 + FROM + i);
     }
 };
 // Tiled feature layout of the staged predictor: record r, channel c, sample
@@ -643,53 +641,91 @@ struct GlobalFeatures {
 struct TiledFeatures {
     const float* x;   // already offset to (r / 32) * 576 * 32 + r % 32
     template <int FROM, int W>
-    MRP_D void load(float (&xs)[3][32]) const {
+    MRP_D void load(int c, float (&xs)[32]) const {
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int i = 0; i < W; ++i) xs[c][i] = __ldg(x + (c * 192 + FROM + i) * 32);
-    }
-};
-struct GatheredFeatures {
-    const VolumeDev* v;
-    PixelFrame f;
-    template <int FROM, int W>
-    MRP_D void load(float (&xs)[3][32]) const {
-        float t[3][32];
-#pragma unroll 1
-        for (int i = 0; i < W; ++i) gather_sample(*v, f, FROM + i, &t[0][i], &t[1][i], &t[2][i]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int i = 0; i < W; ++i) xs[c][i] = t[c][i];
+        for (int i = 0; i < W; ++i) xs[i] = __ldg(x + (c * 192 + FROM + i) * 32);
     }
 };
 
 // ---------------------------------------------------------------------------
-// FP32 MLP, RadiancePredictInternal (core/radiancePredict.cu:301-422).
+// FP32 MLP, RadiancePredictInternal (core/radiancePredict.cu:301-422), one
+// pixel per thread with every activation in registers.
 // Blocks: in_c = X_c[slice]*gate_c + prev_c; out = relu(b + W in) (bias
 // first); then ADD3 (out += slice) or, for the widening blocks 1 and 4, REP3
-// (next residual = concat(out, slice)).  Weights: packed layout of common.cuh.
+// (next residual = concat(out, slice)).  Weights: packed layout of common.cuh
+// (plus the transposed LC1 and LSEFin1 copies after it).
+//
+// Every output is the reference's own sum: its bias (or 0) first, then the
+// inputs in index order, one fmaf each; only the loop nesting differs where
+// that keeps the arrays in registers (LC1 takes each LC0 output as soon as
+// it is made; LSEFin1 sums its 74 channel-independent inputs once).  The
+// two arrays that must outlive a phase -- the 72 SE pool statistics and the
+// 120 concatenated branch outputs -- sit in shared memory, one slot column
+// per thread (kMlpSlots x kMlpThreads floats a block).
 // ---------------------------------------------------------------------------
 MRP_D float wld(const float* __restrict__ w, int i) { return __ldg(w + i); }
 
 MRP_D float sigmoid_ref(float o) { return (float)(1.0 / (1.0 + (double)expf(-o))); }
 
-template <int W, int FROM, bool WIDEN, bool HAS_PREV, class Src>
-MRP_D void mlp_block(const Src& src, float g, float gamma, float* pool, int pid, float (&prev)[3][32],
-                     float (&nxt)[3][32], const float* __restrict__ wt) {
-    float xs[3][32];
-    src.template load<FROM, W>(xs);
+constexpr int kMlpThreads = 128;
+constexpr int kPoolSlot = 0, kCombSlot = 72, kMlpSlots = 192;
+constexpr size_t kMlpSmem = (size_t)kMlpSlots * kMlpThreads * sizeof(float);
+struct Slots {
+    float* s;   // this thread's column: slot k at s[k * kMlpThreads]
+    MRP_D float& operator[](int k) const { return s[k * kMlpThreads]; }
+};
+
+// out[o] = relu(b[o] + sum_j in[j] w[o][j]); rows of FROM floats, 16-byte aligned.
+template <int FROM, int TO, int NI, int NO>
+MRP_D void dense_relu(const float (&in)[NI], float (&out)[NO], const float* __restrict__ w, const float* __restrict__ b) {
+    static_assert(FROM <= NI && TO <= NO && FROM % 4 == 0, "dense_relu shape");
+#pragma unroll
+    for (int o = 0; o < TO; ++o) {
+        float a = wld(b, o);
+        const float4* w4 = reinterpret_cast<const float4*>(w + o * FROM);
+#pragma unroll
+        for (int j = 0; j < FROM / 4; ++j) {
+            const float4 q = __ldg(w4 + j);
+            a = fmaf(in[4 * j], q.x, a);
+            a = fmaf(in[4 * j + 1], q.y, a);
+            a = fmaf(in[4 * j + 2], q.z, a);
+            a = fmaf(in[4 * j + 3], q.w, a);
+        }
+        out[o] = a >= 0.0f ? a : 0.0f;
+    }
+}
+
+// Residual state of the SE blocks, channel c, element i: in registers (the
+// 8-wide direct-illumination chain) or in this thread's shared-memory slots
+// (the main chain, 3 x 32 wide, whose two idle channels would otherwise
+// crowd the registers of the one being computed).
+struct RegState {
+    float (&st)[3][32];
+    MRP_D float get(int c, int i) const { return st[c][i]; }
+    MRP_D void set(int c, int i, float v) const { st[c][i] = v; }
+};
+struct SlotState {
+    Slots s;   // channel c, element i at slot kCombSlot + 32 c + i
+    MRP_D float get(int c, int i) const { return s[kCombSlot + 32 * c + i]; }
+    MRP_D void set(int c, int i, float v) const { s[kCombSlot + 32 * c + i] = v; }
+};
+
+// One SE block; the state's channel c is updated in place.
+template <int W, int FROM, bool WIDEN, bool HAS_PREV, class Src, class State>
+MRP_D void mlp_block(const Src& src, float g, float gamma, Slots pool, int pid, const State& st,
+                     const float* __restrict__ wt) {
     // SE gate: pool (avg, max) of each channel's slice, 8->8 relu, 8->3 sigmoid
     float p8[8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+        float xs[32];
+        src.template load<FROM, W>(c, xs);
         float s = 0.0f, m = -10000.0f;
 #pragma unroll
-        for (int i = 0; i < W; ++i) { float xv = xs[c][i]; s += xv; m = fmaxf(m, xv); }
+        for (int i = 0; i < W; ++i) { s += xs[i]; m = fmaxf(m, xs[i]); }
         s = s / (float)W;
-        pool[pid + c] = s;
-        pool[36 + pid + c] = m;
+        pool[kPoolSlot + pid + c] = s;
+        pool[kPoolSlot + 36 + pid + c] = m;
         p8[c] = s;
         p8[3 + c] = m;
     }
@@ -712,100 +748,88 @@ MRP_D void mlp_block(const Src& src, float g, float gamma, float* pool, int pid,
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+        float xs[32];
+        src.template load<FROM, W>(c, xs);   // the slice again: the pooling pass kept none of it
         const float* wc = wt + 88 + c * (W * W + W);
         float in[W];
 #pragma unroll
         for (int i = 0; i < W; ++i) {
-            float t = xs[c][i] * gate[c];
-            in[i] = HAS_PREV ? t + prev[c][i] : t;
+            const float t = xs[i] * gate[c];
+            in[i] = HAS_PREV ? t + st.get(c, i) : t;
         }
-#pragma unroll 4
-        for (int o = 0; o < W; ++o) {
-            float a = wld(wc, W * W + o);
+        float out[W];
+        dense_relu<W, W>(in, out, wc, wc + W * W);
 #pragma unroll
-            for (int j = 0; j < W; ++j) a = fmaf(in[j], wld(wc, o * W + j), a);
-            a = a >= 0.0f ? a : 0.0f;
-            if (WIDEN) nxt[c][o] = a;
-            else nxt[c][o] = a + xs[c][o];
-        }
+        for (int o = 0; o < W; ++o) st.set(c, o, WIDEN ? out[o] : out[o] + xs[o]);
         if (WIDEN) {
 #pragma unroll
-            for (int i = 0; i < W; ++i) nxt[c][W + i] = xs[c][i];
+            for (int i = 0; i < W; ++i) st.set(c, W + i, xs[i]);
         }
     }
-}
-
-template <int FROM, int TO>
-MRP_D void dense_relu(const float* in, float* out, const float* __restrict__ w, const float* __restrict__ b) {
-#pragma unroll 2
-    for (int o = 0; o < TO; ++o) {
-        float a = wld(b, o);
-        const float4* w4 = reinterpret_cast<const float4*>(w + o * FROM);
-#pragma unroll
-        for (int j = 0; j < FROM / 4; ++j) {
-            float4 q = __ldg(w4 + j);
-            a = fmaf(in[4 * j], q.x, a);
-            a = fmaf(in[4 * j + 1], q.y, a);
-            a = fmaf(in[4 * j + 2], q.z, a);
-            a = fmaf(in[4 * j + 3], q.w, a);
-        }
-        out[o] = a >= 0.0f ? a : 0.0f;
-    }
-}
-
-template <int K>
-MRP_D void copy_state(float (&dst)[3][32], const float (&src)[3][32]) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int i = 0; i < K; ++i) dst[c][i] = src[c][i];
 }
 
 template <class Src>
-MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __restrict__ wt, float out[3]) {
-    float pool[75];
-    pool[72] = g;
-    pool[73] = gamma;
-    float comb[120];
+MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __restrict__ wt_, Slots sm, float out[3]) {
+    const float* __restrict__ wt = wt_;
     {
-        float a[3][32], b[3][32];
-        mlp_block<8, 0, false, false>(x, g, gamma, pool, 0, a, b, wt + main_block_off(0));
-        copy_state<8>(a, b);
-        mlp_block<8, 8, true, true>(x, g, gamma, pool, 3, a, b, wt + main_block_off(1));
-        copy_state<16>(a, b);
-        mlp_block<16, 16, false, true>(x, g, gamma, pool, 6, a, b, wt + main_block_off(2));
-        copy_state<16>(a, b);
-        mlp_block<16, 32, false, true>(x, g, gamma, pool, 9, a, b, wt + main_block_off(3));
-        copy_state<16>(a, b);
-        mlp_block<16, 48, true, true>(x, g, gamma, pool, 12, a, b, wt + main_block_off(4));
-        copy_state<32>(a, b);
-        mlp_block<32, 64, false, true>(x, g, gamma, pool, 15, a, b, wt + main_block_off(5));
-        copy_state<32>(a, b);
-        mlp_block<32, 96, false, true>(x, g, gamma, pool, 18, a, b, wt + main_block_off(6));
-        copy_state<32>(a, b);
-        mlp_block<32, 128, false, true>(x, g, gamma, pool, 21, a, b, wt + main_block_off(7));
+        const SlotState st{sm};
+        mlp_block<8, 0, false, false>(x, g, gamma, sm, 0, st, wt + main_block_off(0));
+        mlp_block<8, 8, true, true>(x, g, gamma, sm, 3, st, wt + main_block_off(1));
+        mlp_block<16, 16, false, true>(x, g, gamma, sm, 6, st, wt + main_block_off(2));
+        mlp_block<16, 32, false, true>(x, g, gamma, sm, 9, st, wt + main_block_off(3));
+        mlp_block<16, 48, true, true>(x, g, gamma, sm, 12, st, wt + main_block_off(4));
+        mlp_block<32, 64, false, true>(x, g, gamma, sm, 15, st, wt + main_block_off(5));
+        mlp_block<32, 96, false, true>(x, g, gamma, sm, 18, st, wt + main_block_off(6));
+        mlp_block<32, 128, false, true>(x, g, gamma, sm, 21, st, wt + main_block_off(7));
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float* wf = wt + kMainFinalOff + c * (1024 + 32);
-            dense_relu<32, 32>(b[c], comb + 32 * c, wf, wf + 1024);
+            float s32[32], o32[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) s32[i] = st.get(c, i);
+            dense_relu<32, 32>(s32, o32, wf, wf + 1024);   // channel c's state slots become its comb slots
+#pragma unroll
+            for (int i = 0; i < 32; ++i) sm[kCombSlot + 32 * c + i] = o32[i];
         }
     }
     {
-        float a[3][32], b[3][32];
-        mlp_block<8, 160, false, false>(x, g, gamma, pool, 24, a, b, wt + di_block_off(0));
-        copy_state<8>(a, b);
-        mlp_block<8, 168, false, true>(x, g, gamma, pool, 27, a, b, wt + di_block_off(1));
-        copy_state<8>(a, b);
-        mlp_block<8, 176, false, true>(x, g, gamma, pool, 30, a, b, wt + di_block_off(2));
-        copy_state<8>(a, b);
-        mlp_block<8, 184, false, true>(x, g, gamma, pool, 33, a, b, wt + di_block_off(3));
+        float di[3][32];
+        const RegState st{di};
+        mlp_block<8, 160, false, false>(x, g, gamma, sm, 24, st, wt + di_block_off(0));
+        mlp_block<8, 168, false, true>(x, g, gamma, sm, 27, st, wt + di_block_off(1));
+        mlp_block<8, 176, false, true>(x, g, gamma, sm, 30, st, wt + di_block_off(2));
+        mlp_block<8, 184, false, true>(x, g, gamma, sm, 33, st, wt + di_block_off(3));
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float* wf = wt + kDiFinalOff + c * (64 + 8);
-            dense_relu<8, 8>(b[c], comb + 96 + 8 * c, wf, wf + 64);
+            float o8[8];
+            dense_relu<8, 8>(di[c], o8, wf, wf + 64);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) sm[kCombSlot + 96 + 8 * c + i] = o8[i];
         }
     }
-    float srv[3] = {sr.x, sr.y, sr.z};
+    // LSEFin1 over pool = (36 averages, 36 maxima, g, gamma, albedo^4): the
+    // first 74 terms do not depend on the albedo channel, so each output's
+    // sum runs through them once here and takes its 75th term per channel.
+    float fin1[16];
+#pragma unroll
+    for (int o = 0; o < 16; ++o) fin1[o] = 0.0f;
+    const float4* f1t = reinterpret_cast<const float4*>(wt + kFin1T);   // [75][16]
+#pragma unroll 4
+    for (int j = 0; j < 74; ++j) {
+        const float p = j < 72 ? sm[kPoolSlot + j] : (j == 72 ? g : gamma);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float4 w = __ldg(f1t + j * 4 + q);
+            fin1[4 * q] = fmaf(p, w.x, fin1[4 * q]);
+            fin1[4 * q + 1] = fmaf(p, w.y, fin1[4 * q + 1]);
+            fin1[4 * q + 2] = fmaf(p, w.z, fin1[4 * q + 2]);
+            fin1[4 * q + 3] = fmaf(p, w.w, fin1[4 * q + 3]);
+        }
+    }
+#pragma unroll
+    for (int o = 0; o < 16; ++o) sm[kPoolSlot + o] = fin1[o];   // the pool statistics are used up
+    const float srv[3] = {sr.x, sr.y, sr.z};
     float srp[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) srp[c] = powf(srv[c], 4.0f);
@@ -815,25 +839,16 @@ MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __re
         if (ch == 1 && srv[1] == srv[0]) { P[1] = P[0]; continue; }
         if (ch == 2 && srv[2] == srv[0]) { P[2] = P[0]; continue; }
         if (ch == 2 && srv[2] == srv[1]) { P[2] = P[1]; continue; }
-        pool[74] = srp[ch];
-        float xa[128], xb[128];
-#pragma unroll
-        for (int i = 0; i < 120; ++i) xa[i] = comb[i];
-        // LGGS 3->8: sum first, bias last (LinearReLU, :41-56)
-#pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            float a = 0.0f;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) a = fmaf(pool[72 + j], wld(wt, kLGGSW + o * 3 + j), a);
-            a += wld(wt, kLGGSB + o);
-            xa[120 + o] = a >= 0.0f ? a : 0.0f;
-        }
+        const float s4 = srp[ch];
+        // The weight pointer made opaque per pass: otherwise the tail's
+        // weight loads, the same for every albedo channel, are hoisted out of
+        // this loop and held in registers that the pass itself needs.
+        const float* wt;
+        asm volatile("mov.b64 %0, %1;" : "=l"(wt) : "l"(wt_));
         float hf[16], gf[6];
-#pragma unroll 2
-        for (int o = 0; o < 16; ++o) {
-            float a = 0.0f;
 #pragma unroll
-            for (int j = 0; j < 75; ++j) a = fmaf(pool[j], wld(wt, kLSEFin1W + o * 75 + j), a);
+        for (int o = 0; o < 16; ++o) {
+            const float a = fmaf(s4, wld(wt, kLSEFin1W + o * 75 + 74), sm[kPoolSlot + o]);
             hf[o] = a >= 0.0f ? a : 0.0f;
         }
 #pragma unroll
@@ -843,25 +858,64 @@ MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __re
             for (int j = 0; j < 16; ++j) a = fmaf(hf[j], wld(wt, kLSEFin2W + o * 16 + j), a);
             gf[o] = sigmoid_ref(a);
         }
+        // x = concat(main_c * gate_c, di_c * gate_{3+c}, LGGS(g, gamma, albedo^4))
+        float xa[128];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) { xa[i] *= gf[0]; xa[32 + i] *= gf[1]; xa[64 + i] *= gf[2]; }
+        for (int i = 0; i < 120; ++i) xa[i] = sm[kCombSlot + i] * gf[i < 96 ? i / 32 : 3 + (i - 96) / 8];
+        // LGGS 3->8: sum first, bias last (LinearReLU, :41-56)
+        const float p3[3] = {g, gamma, s4};
 #pragma unroll
-        for (int i = 0; i < 8; ++i) { xa[96 + i] *= gf[3]; xa[104 + i] *= gf[4]; xa[112 + i] *= gf[5]; }
-        dense_relu<128, 128>(xa, xb, wt + kLC0W, wt + kLC0B);
-        dense_relu<128, 64>(xb, xa, wt + kLC1W, wt + kLC1B);
-        dense_relu<64, 32>(xa, xb, wt + kLC2W, wt + kLC2B);
-        dense_relu<32, 16>(xb, xa, wt + kLXW, wt + kLXB);
+        for (int o = 0; o < 8; ++o) {
+            float a = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) a = fmaf(p3[j], wld(wt, kLGGSW + o * 3 + j), a);
+            a += wld(wt, kLGGSB + o);
+            xa[120 + o] = a >= 0.0f ? a : 0.0f;
+        }
+        // LC0 128->128 with LC1 128->64 folded in: LC0 output j joins every
+        // LC1 sum as its j-th term (transposed LC1 rows: [128][64]).
+        float acc1[64];
+#pragma unroll
+        for (int o = 0; o < 64; ++o) acc1[o] = wld(wt, kLC1B + o);
+        const float4* l1t = reinterpret_cast<const float4*>(wt + kLC1T);
+#pragma unroll 1
+        for (int j = 0; j < 128; ++j) {
+            float a = wld(wt, kLC0B + j);
+            const float4* w4 = reinterpret_cast<const float4*>(wt + kLC0W + j * 128);
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const float4 w = __ldg(w4 + q);
+                a = fmaf(xa[4 * q], w.x, a);
+                a = fmaf(xa[4 * q + 1], w.y, a);
+                a = fmaf(xa[4 * q + 2], w.z, a);
+                a = fmaf(xa[4 * q + 3], w.w, a);
+            }
+            const float h0 = a >= 0.0f ? a : 0.0f;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const float4 w = __ldg(l1t + j * 16 + q);
+                acc1[4 * q] = fmaf(h0, w.x, acc1[4 * q]);
+                acc1[4 * q + 1] = fmaf(h0, w.y, acc1[4 * q + 1]);
+                acc1[4 * q + 2] = fmaf(h0, w.z, acc1[4 * q + 2]);
+                acc1[4 * q + 3] = fmaf(h0, w.w, acc1[4 * q + 3]);
+            }
+        }
+#pragma unroll
+        for (int o = 0; o < 64; ++o) acc1[o] = acc1[o] >= 0.0f ? acc1[o] : 0.0f;
+        float h2[32], h3[16];
+        dense_relu<64, 32>(acc1, h2, wt + kLC2W, wt + kLC2B);
+        dense_relu<32, 16>(h2, h3, wt + kLXW, wt + kLXB);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             float y[16], z[16];
-            dense_relu<16, 16>(xa, y, wt + lxw(2 * k), wt + lxb(2 * k));
+            dense_relu<16, 16>(h3, y, wt + lxw(2 * k), wt + lxb(2 * k));
             dense_relu<16, 16>(y, z, wt + lxw(2 * k + 1), wt + lxb(2 * k + 1));
 #pragma unroll
-            for (int i = 0; i < 16; ++i) xa[i] += z[i];
+            for (int i = 0; i < 16; ++i) h3[i] += z[i];
         }
         float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) a = fmaf(xa[j], wld(wt, kLX12W + j), a);
+        for (int j = 0; j < 16; ++j) a = fmaf(h3[j], wld(wt, kLX12W + j), a);
         a += wld(wt, kLX12B);
         P[ch] = a >= 0.0f ? a : 0.0f;
     }
@@ -892,13 +946,14 @@ __global__ void k_gather(VolumeDev v, const float* __restrict__ pos, const float
     gather(v, f, feat + (size_t)576 * i, 192, gamma + i);
 }
 
-__global__ void __launch_bounds__(128) k_mlp_fp32(const float* __restrict__ wt, const float* __restrict__ feat,
-                                                  const float* __restrict__ gamma, float g, f3 sr, int n,
-                                                  float* __restrict__ out3) {
+__global__ void __launch_bounds__(kMlpThreads, 2) k_mlp_fp32(const float* __restrict__ wt, const float* __restrict__ feat,
+                                                              const float* __restrict__ gamma, float g, f3 sr, int n,
+                                                              float* __restrict__ out3) {
+    extern __shared__ float mlp_slots[];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float o[3];
-    mlp_fp32(GlobalFeatures{feat + (size_t)576 * i}, gamma[i], g, sr, wt, o);
+    mlp_fp32(GlobalFeatures{feat + (size_t)576 * i}, gamma[i], g, sr, wt, Slots{mlp_slots + threadIdx.x}, o);
     out3[3 * i] = o[0]; out3[3 * i + 1] = o[1]; out3[3 * i + 2] = o[2];
 }
 
@@ -1022,14 +1077,17 @@ __global__ void __launch_bounds__(128) k_gather_rec(VolumeDev v, ViewDev w, HitR
     else gather_all_fast<FP16>(v, pf, feat, r);
 }
 
-__global__ void __launch_bounds__(128) k_mlp_rec(VolumeDev v, ViewDev w, HitRecords rec, const float* __restrict__ feat,
-                                                const float* __restrict__ wt, float4* __restrict__ accum) {
+__global__ void __launch_bounds__(kMlpThreads, 2) k_mlp_rec(VolumeDev v, ViewDev w, HitRecords rec,
+                                                            const float* __restrict__ feat, const float* __restrict__ wt,
+                                                            float4* __restrict__ accum) {
+    extern __shared__ float mlp_slots[];
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *rec.count) return;
     float gamma = rec.f[15 * rec.cap + r];
     f3 sr = div(v.scatter_rate, 1.001f);
     float o[3];
-    mlp_fp32(TiledFeatures{feat + (size_t)(r >> 5) * 576 * 32 + (r & 31)}, gamma, w.g, sr, wt, o);
+    mlp_fp32(TiledFeatures{feat + (size_t)(r >> 5) * 576 * 32 + (r & 31)}, gamma, w.g, sr, wt,
+             Slots{mlp_slots + threadIdx.x}, o);
     int pix = rec.pix[r];
     f3 hit = mk3(rec.f[r], rec.f[rec.cap + r], rec.f[2 * rec.cap + r]);
     f3 pr = mul(mk3(o[0], o[1], o[2]), 1.0f);   // alphaMult == 1 (core/render.cuh:844-848)
@@ -1079,7 +1137,10 @@ cudaError_t launch_gather(const VolumeDev& v, const float* pos, const float* bas
 cudaError_t launch_mlp_fp32(const float* weights, const float* feat, const float* gamma, float g, const float sr[3],
                             int n, float* out3, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    k_mlp_fp32<<<(n + 127) / 128, 128, 0, s>>>(weights, feat, gamma, g, mk3(sr[0], sr[1], sr[2]), n, out3);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem);
+    if (e != cudaSuccess) return e;
+    k_mlp_fp32<<<(n + kMlpThreads - 1) / kMlpThreads, kMlpThreads, kMlpSmem, s>>>(weights, feat, gamma, g,
+                                                                               mk3(sr[0], sr[1], sr[2]), n, out3);
     return cudaGetLastError();
 }
 cudaError_t launch_hit(const VolumeDev& v, const ViewDev& view, HitRecords rec, float4* accum, cudaStream_t s) {
@@ -1355,7 +1416,9 @@ cudaError_t launch_mlp_rec_fp32(const VolumeDev& v, const ViewDev& view, HitReco
                                 const float* weights, float4* accum, cudaStream_t s) {
     int n = view.width * view.height;
     if (n <= 0) return cudaSuccess;
-    k_mlp_rec<<<(n + 127) / 128, 128, 0, s>>>(v, view, rec, feat, weights, accum);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem);
+    if (e != cudaSuccess) return e;
+    k_mlp_rec<<<(n + kMlpThreads - 1) / kMlpThreads, kMlpThreads, kMlpSmem, s>>>(v, view, rec, feat, weights, accum);
     return cudaGetLastError();
 }
 cudaError_t launch_debug_scatter(HitRecords rec, const float* feat, bool fp16, int npix, float* aux, float* feat_out,
