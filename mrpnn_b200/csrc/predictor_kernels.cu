@@ -629,10 +629,11 @@ MRP_D void gather(const VolumeDev& v, const PixelFrame& f, float* out, int strid
 // [FROM, FROM+W) just before it uses it, so no pixel ever holds all 576.
 struct GlobalFeatures {
     const float* x;   // channel c at x[c * 192 + i]
-    template <int FROM, int W>
-    MRP_D void load(int c, float (&xs)[32]) const {
+    template <int W>
+    MRP_D void load(int from, int c, float (&xs)[32]) const {
+        const float* p = x + c * 192 + from;
 #pragma unroll
-        for (int i = 0; i < W; ++i) xs[i] = __ldg(x + c * 192 + FROM + i);
+        for (int i = 0; i < W; ++i) xs[i] = __ldg(p + i);
     }
 };
 // Tiled feature layout of the staged predictor: record r, channel c, sample
@@ -640,10 +641,11 @@ struct GlobalFeatures {
 // records reads or writes 128 contiguous bytes per feature.
 struct TiledFeatures {
     const float* x;   // already offset to (r / 32) * 576 * 32 + r % 32
-    template <int FROM, int W>
-    MRP_D void load(int c, float (&xs)[32]) const {
+    template <int W>
+    MRP_D void load(int from, int c, float (&xs)[32]) const {
+        const float* p = x + (c * 192 + from) * 32;
 #pragma unroll
-        for (int i = 0; i < W; ++i) xs[i] = __ldg(x + (c * 192 + FROM + i) * 32);
+        for (int i = 0; i < W; ++i) xs[i] = __ldg(p + i * 32);
     }
 };
 
@@ -695,31 +697,27 @@ MRP_D void dense_relu(const float (&in)[NI], float (&out)[NO], const float* __re
     }
 }
 
-// Residual state of the SE blocks, channel c, element i: in registers (the
-// 8-wide direct-illumination chain) or in this thread's shared-memory slots
-// (the main chain, 3 x 32 wide, whose two idle channels would otherwise
-// crowd the registers of the one being computed).
-struct RegState {
-    float (&st)[3][32];
-    MRP_D float get(int c, int i) const { return st[c][i]; }
-    MRP_D void set(int c, int i, float v) const { st[c][i] = v; }
-};
+// Residual state of the SE blocks, channel c, element i, in this thread's
+// shared-memory slots: the main chain (3 x 32) at the slots its final
+// layers' outputs take later, the direct-illumination chain (3 x 8) at
+// those of its own final layers.
 struct SlotState {
-    Slots s;   // channel c, element i at slot kCombSlot + 32 c + i
-    MRP_D float get(int c, int i) const { return s[kCombSlot + 32 * c + i]; }
-    MRP_D void set(int c, int i, float v) const { s[kCombSlot + 32 * c + i] = v; }
+    Slots s;
+    int base, stride;   // channel c, element i at slot base + stride c + i
+    MRP_D float get(int c, int i) const { return s[base + stride * c + i]; }
+    MRP_D void set(int c, int i, float v) const { s[base + stride * c + i] = v; }
 };
 
 // One SE block; the state's channel c is updated in place.
-template <int W, int FROM, bool WIDEN, bool HAS_PREV, class Src, class State>
-MRP_D void mlp_block(const Src& src, float g, float gamma, Slots pool, int pid, const State& st,
+template <int W, bool WIDEN, bool HAS_PREV, class Src, class State>
+MRP_D void mlp_block(const Src& src, int from, float g, float gamma, Slots pool, int pid, const State& st,
                      const float* __restrict__ wt) {
     // SE gate: pool (avg, max) of each channel's slice, 8->8 relu, 8->3 sigmoid
     float p8[8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float xs[32];
-        src.template load<FROM, W>(c, xs);
+        src.template load<W>(from, c, xs);
         float s = 0.0f, m = -10000.0f;
 #pragma unroll
         for (int i = 0; i < W; ++i) { s += xs[i]; m = fmaxf(m, xs[i]); }
@@ -746,15 +744,18 @@ MRP_D void mlp_block(const Src& src, float g, float gamma, Slots pool, int pid, 
         for (int j = 0; j < 8; ++j) a = fmaf(h[j], wld(wt, 64 + o * 8 + j), a);
         gate[o] = sigmoid_ref(a);
     }
-#pragma unroll
+    // one copy of the channel body, run three times (the state is in shared
+    // memory, so the channel may be a run-time index): a third of the code
+#pragma unroll 1
     for (int c = 0; c < 3; ++c) {
         float xs[32];
-        src.template load<FROM, W>(c, xs);   // the slice again: the pooling pass kept none of it
+        src.template load<W>(from, c, xs);   // the slice again: the pooling pass kept none of it
         const float* wc = wt + 88 + c * (W * W + W);
+        const float gc = c == 0 ? gate[0] : (c == 1 ? gate[1] : gate[2]);
         float in[W];
 #pragma unroll
         for (int i = 0; i < W; ++i) {
-            const float t = xs[i] * gate[c];
+            const float t = xs[i] * gc;
             in[i] = HAS_PREV ? t + st.get(c, i) : t;
         }
         float out[W];
@@ -772,16 +773,18 @@ template <class Src>
 MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __restrict__ wt_, Slots sm, float out[3]) {
     const float* __restrict__ wt = wt_;
     {
-        const SlotState st{sm};
-        mlp_block<8, 0, false, false>(x, g, gamma, sm, 0, st, wt + main_block_off(0));
-        mlp_block<8, 8, true, true>(x, g, gamma, sm, 3, st, wt + main_block_off(1));
-        mlp_block<16, 16, false, true>(x, g, gamma, sm, 6, st, wt + main_block_off(2));
-        mlp_block<16, 32, false, true>(x, g, gamma, sm, 9, st, wt + main_block_off(3));
-        mlp_block<16, 48, true, true>(x, g, gamma, sm, 12, st, wt + main_block_off(4));
-        mlp_block<32, 64, false, true>(x, g, gamma, sm, 15, st, wt + main_block_off(5));
-        mlp_block<32, 96, false, true>(x, g, gamma, sm, 18, st, wt + main_block_off(6));
-        mlp_block<32, 128, false, true>(x, g, gamma, sm, 21, st, wt + main_block_off(7));
-#pragma unroll
+        const SlotState st{sm, kCombSlot, 32};
+        mlp_block<8, false, false>(x, 0, g, gamma, sm, 0, st, wt + main_block_off(0));
+        mlp_block<8, true, true>(x, 8, g, gamma, sm, 3, st, wt + main_block_off(1));
+        // blocks of one width share one copy of the code
+#pragma unroll 1
+        for (int k = 2; k < 4; ++k)
+            mlp_block<16, false, true>(x, 16 * (k - 1), g, gamma, sm, 3 * k, st, wt + main_block_off(2) + (k - 2) * block_size(16));
+        mlp_block<16, true, true>(x, 48, g, gamma, sm, 12, st, wt + main_block_off(4));
+#pragma unroll 1
+        for (int k = 5; k < 8; ++k)
+            mlp_block<32, false, true>(x, 64 + 32 * (k - 5), g, gamma, sm, 3 * k, st, wt + main_block_off(5) + (k - 5) * block_size(32));
+#pragma unroll 1
         for (int c = 0; c < 3; ++c) {
             const float* wf = wt + kMainFinalOff + c * (1024 + 32);
             float s32[32], o32[32];
@@ -793,17 +796,18 @@ MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __re
         }
     }
     {
-        float di[3][32];
-        const RegState st{di};
-        mlp_block<8, 160, false, false>(x, g, gamma, sm, 24, st, wt + di_block_off(0));
-        mlp_block<8, 168, false, true>(x, g, gamma, sm, 27, st, wt + di_block_off(1));
-        mlp_block<8, 176, false, true>(x, g, gamma, sm, 30, st, wt + di_block_off(2));
-        mlp_block<8, 184, false, true>(x, g, gamma, sm, 33, st, wt + di_block_off(3));
-#pragma unroll
+        const SlotState st{sm, kCombSlot + 96, 8};
+        mlp_block<8, false, false>(x, 160, g, gamma, sm, 24, st, wt + di_block_off(0));
+#pragma unroll 1
+        for (int k = 1; k < 4; ++k)
+            mlp_block<8, false, true>(x, 160 + 8 * k, g, gamma, sm, 24 + 3 * k, st, wt + di_block_off(0) + k * block_size(8));
+#pragma unroll 1
         for (int c = 0; c < 3; ++c) {
             const float* wf = wt + kDiFinalOff + c * (64 + 8);
-            float o8[8];
-            dense_relu<8, 8>(di[c], o8, wf, wf + 64);
+            float s8[8], o8[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) s8[i] = st.get(c, i);
+            dense_relu<8, 8>(s8, o8, wf, wf + 64);   // channel c's state slots become its comb slots
 #pragma unroll
             for (int i = 0; i < 8; ++i) sm[kCombSlot + 96 + 8 * c + i] = o8[i];
         }
@@ -905,7 +909,7 @@ MRP_D void mlp_fp32(const Src& x, float gamma, float g, f3 sr, const float* __re
         float h2[32], h3[16];
         dense_relu<64, 32>(acc1, h2, wt + kLC2W, wt + kLC2B);
         dense_relu<32, 16>(h2, h3, wt + kLXW, wt + kLXB);
-#pragma unroll
+#pragma unroll 1
         for (int k = 0; k < 6; ++k) {
             float y[16], z[16];
             dense_relu<16, 16>(h3, y, wt + lxw(2 * k), wt + lxb(2 * k));
