@@ -649,5 +649,8 @@ static_assert(kWeightCount == 49673, "packed weight count must match core/NNWeig
 constexpr int kLC1T = (kWeightCount + 3) / 4 * 4;
 constexpr int kFin1T = kLC1T + 8192;
 constexpr int kWeightCountDev = kFin1T + 1200;
+static_assert(kLC1T % 4 == 0 && kFin1T % 4 == 0 && kLC0W % 4 == 0 && kLC2W % 4 == 0 && kLXW % 4 == 0 &&
+                  kMainFinalOff % 4 == 0 && kDiOff % 4 == 0 && kLXk % 4 == 0,
+              "rows read as float4 start on 16-byte boundaries");
 
 }  // namespace mrp
