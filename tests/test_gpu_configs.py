@@ -102,13 +102,23 @@ def test_headline_frame_tensor_core_forms(prec):
         sc.vol.SetGatherFilter(True)
 
 
-def test_tracer_workload_zscore():
+@pytest.mark.parametrize("hw_filter", [False, True], ids=["software", "texture"])
+def test_tracer_workload_zscore(hw_filter):
+    """The C1 tracer workload against the oracle's tracer, per pixel.  With
+    the texture unit's filters (tracer_filter) the GPU's density and NEE
+    values differ from the oracle's by the unit's 8-bit weights, so its
+    paths part from the oracle's and the comparison is between two
+    independent estimates: the same bars hold."""
     import mrpnn_b200 as M
     sc = Scene(R=128, seed=0, freq=4.0, alpha=64.0, g=0.857, sr=0.99, sky=0.05, bake_res=768)
     W, spp, bounces = 256, 16, 256
     ori, up, right = view_frame()
-    got = sc.vol.Render((W, W), ori, up, right, LIGHT, M.VolumeRender.PT, sc.g, sc.alpha, multiScatter=bounces,
-                        sampleNum=1, spp=spp, seed=9).reshape(-1, 4)
+    sc.vol.SetTracerFilter(hw_filter)
+    try:
+        got = sc.vol.Render((W, W), ori, up, right, LIGHT, M.VolumeRender.PT, sc.g, sc.alpha, multiScatter=bounces,
+                            sampleNum=1, spp=spp, seed=9).reshape(-1, 4)
+    finally:
+        sc.vol.SetTracerFilter(False)
     view = O.make_view(W, W, ori, up, right, LIGHT, alpha=sc.alpha, g=sc.g, multi_scatter=bounces, spp=spp,
                        seed=9, frame=0)
     rgba, s, s2 = O.trace_pixels(sc.orc, view, np.arange(W * W, dtype=np.int32))
