@@ -80,12 +80,14 @@ typedef struct mrp_params {
     int gather_filter;       /* the stencil gather of the BF16 / FP8 forms
                                 (fp16 features): 1 (default) the texture
                                 unit's trilinear and bilinear filters on the
-                                mip, TR and HG-LUT levels, as the reference's
-                                own tex3D / tex2D sampling in SetupInputData
-                                (weights quantised to 1/256); 0 software
-                                filters with fp32 weights.  The FP32 form
-                                always filters in software (the oracle's
-                                features to ~1e-6). */
+                                mip and TR levels and, for the light ray's
+                                points, the HG-LUT, as the reference's own
+                                tex3D / tex2D sampling in SetupInputData
+                                (weights quantised to 1/256; the rotated
+                                directions' LUT factor is read in software);
+                                0 software filters with fp32 weights.  The
+                                FP32 form always filters in software (the
+                                oracle's features to ~1e-6). */
 } mrp_params;
 
 /* One camera: VolumeRender::Render(int2 size, ori, up, right, lightDir, rt,

@@ -481,7 +481,8 @@ class VolumeRender:
 
     def SetGatherFilter(self, hardware):
         """The stencil gather of the BF16 / FP8 forms: True (default) the
-        texture unit's trilinear / bilinear filters, as the reference's own
+        texture unit's trilinear / bilinear filters on the mip and TR levels
+        (and the LUT for the light ray's points), as the reference's own
         tex3D / tex2D sampling; False software filters with fp32 weights.  The
         FP32 form always filters in software."""
         self._params.gather_filter = 1 if hardware else 0
