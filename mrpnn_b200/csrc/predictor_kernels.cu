@@ -657,7 +657,7 @@ struct TiledFeatures {
 
 // ---------------------------------------------------------------------------
 // FP32 MLP, RadiancePredictInternal (core/radiancePredict.cu:301-422), one
-// pixel per thread with every activation in registers.
+// pixel per thread, no local-memory arrays.
 // Blocks: in_c = X_c[slice]*gate_c + prev_c; out = relu(b + W in) (bias
 // first); then ADD3 (out += slice) or, for the widening blocks 1 and 4, REP3
 // (next residual = concat(out, slice)).  Weights: packed layout of common.cuh
@@ -666,10 +666,13 @@ struct TiledFeatures {
 // Every output is the reference's own sum: its bias (or 0) first, then the
 // inputs in index order, one fmaf each; only the loop nesting differs where
 // that keeps the arrays in registers (LC1 takes each LC0 output as soon as
-// it is made; LSEFin1 sums its 74 channel-independent inputs once).  The
-// two arrays that must outlive a phase -- the 72 SE pool statistics and the
-// 120 concatenated branch outputs -- sit in shared memory, one slot column
-// per thread (kMlpSlots x kMlpThreads floats a block).
+// it is made; LSEFin1 sums its 74 channel-independent inputs once).  What
+// must outlive one layer -- the SE chains' residuals (which then become the
+// 120 concatenated branch outputs) and the 72 SE pool statistics -- sits in
+// shared memory, one slot column per thread (kMlpSlots x kMlpThreads floats
+// a block); with the residual there, an SE block's channel body and the
+// blocks of one width are single copies of code, which keeps the network's
+// instruction footprint small enough for the instruction caches.
 // ---------------------------------------------------------------------------
 MRP_D float wld(const float* __restrict__ w, int i) { return __ldg(w + i); }
 
